@@ -1,0 +1,167 @@
+"""dustyfargoadsg_b200 -- the gas time step of Dusty FARGO-ADSG (AlgoGas) on a
+single NVIDIA B200, behind the C ABI of include/fargo_b200.h.
+
+Python here is a thin binding over libfargo_b200.so for tests, benchmarks and
+scripting; the step itself runs in the library's CUDA kernels.  The C host
+(dustyfargoadsg_b200/host) and the reference's own main (through the AlgoGas
+drop-in) use the same library.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _ffi
+from ._ffi import (FB_F_ALL, FB_F_DENS, FB_F_ENERGY, FB_F_VRAD, FB_F_VTHETA, FbError, FbParams,
+                   FbProfiles, FbState, FbStepReport, check, load)
+
+__all__ = ["Disc", "read_par", "FbError", "load", "CONFIG_DIR"]
+
+CONFIG_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "configs")
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def read_par(path, **overrides):
+    """Parse a reference .par file (ReadVariables rules) into FbParams.
+
+    PLANETCONFIG is resolved like the reference does (relative to the
+    current directory) and, failing that, relative to the .par file.
+    """
+    lib = load()
+    p = FbParams()
+    check(lib.fb_params_read_par(C.byref(p), os.fsencode(path)), "fb_params_read_par(%s)" % path)
+    cfg = p.planetconfig.decode()
+    if cfg and not os.path.isabs(cfg) and not os.path.exists(cfg):
+        alt = os.path.join(os.path.dirname(os.path.abspath(path)), cfg)
+        if os.path.exists(alt):
+            p.planetconfig = alt.encode()
+    for key, val in overrides.items():
+        if key == "planetconfig":
+            val = os.fsencode(val)
+        setattr(p, key, val)
+    return p
+
+
+class Disc:
+    """One disc on the GPU: parameters, device context and host mirrors."""
+
+    def __init__(self, params, noise=0.0, seed=0, state=None):
+        self.lib = load()
+        if isinstance(params, (str, os.PathLike)):
+            params = read_par(params)
+        self.p = params
+        if self.p.unsupported:
+            raise FbError(-2, "Disc", self.lib.fb_unsupported_name(C.byref(self.p)).decode())
+        self.nr, self.ns = self.p.nrad, self.p.nsec
+        self.nf = (self.nr + 1) * self.ns
+        self.ctx = C.c_void_p()
+        check(self.lib.fb_create(C.byref(self.p), None, C.byref(self.ctx)), "fb_create")
+        self.fields = {k: np.zeros(self.nf) for k in ("dens", "vrad", "vtheta", "energy")}
+        self.prof = {k: np.zeros(self.nr) for k in
+                     ("sigma_med", "sigma_inf", "energy_med", "vtheta_med", "vrad_med", "global_soundspeed")}
+        self.st = FbState()
+        for k, a in self.fields.items():
+            setattr(self.st, k, _ptr(a))
+        self.pr = FbProfiles(*[_ptr(self.prof[k]) for k in
+                               ("sigma_med", "sigma_inf", "energy_med", "vtheta_med", "vrad_med",
+                                "global_soundspeed")])
+        if state is None:
+            check(self.lib.fb_init_state(C.byref(self.p), self.ctx, float(noise), int(seed),
+                                         C.byref(self.st), C.byref(self.pr)), "fb_init_state", self.ctx)
+        else:
+            self.set_state(state)
+            return
+        check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx)
+
+    # -- state ----------------------------------------------------------
+    def set_state(self, state):
+        """Upload a state dict: fields (dens, vrad, vtheta, energy) of
+        (nrad+1)*nsec doubles, profiles (SigmaMed, ...) and scalars."""
+        for k in ("dens", "vrad", "vtheta", "energy"):
+            if k in state:
+                self.fields[k][:] = np.asarray(state[k], dtype=np.float64).ravel()[: self.nf]
+        names = {"SigmaMed": "sigma_med", "SigmaInf": "sigma_inf", "EnergyMed": "energy_med",
+                 "VthetaMed": "vtheta_med", "VradMed": "vrad_med", "GLOBAL_SoundSpeed": "global_soundspeed"}
+        for src, dst in names.items():
+            if src in state:
+                self.prof[dst][:] = np.asarray(state[src], dtype=np.float64)[: self.nr]
+        st = self.st
+        st.physical_time = float(state.get("PhysicalTime", 0.0))
+        st.physical_time_initial = float(state.get("PhysicalTimeInitial", 0.0))
+        st.omega_frame = float(state.get("OmegaFrame", self.p.omegaframe))
+        st.lost_mass = float(state.get("LostMass", 0.0))
+        st.mindt = float(state.get("MINDT", self.p.mindt))
+        st.maxdt = float(state.get("MAXDT", self.p.maxdt))
+        for q in range(3):
+            st.stardiscbarycenter_x[q] = float(np.asarray(state.get("stardiscbarycenter_x", [0, 0, 0]))[q])
+            st.stardiscbarycenter_y[q] = float(np.asarray(state.get("stardiscbarycenter_y", [0, 0, 0]))[q])
+        if "pl_x" in state:
+            n = len(np.atleast_1d(state["pl_x"]))
+            pl = st.planets
+            pl.nb = n
+            cfg = _ffi.FbPlanets()
+            check(self.lib.fb_planets_read_cfg(C.byref(self.p), self.p.planetconfig, C.byref(cfg)),
+                  "fb_planets_read_cfg")
+            for q in range(n):
+                pl.mass[q] = float(np.atleast_1d(state["pl_mass"])[q])
+                pl.x[q] = float(np.atleast_1d(state["pl_x"])[q])
+                pl.y[q] = float(np.atleast_1d(state["pl_y"])[q])
+                pl.vx[q] = float(np.atleast_1d(state["pl_vx"])[q])
+                pl.vy[q] = float(np.atleast_1d(state["pl_vy"])[q])
+                pl.acc[q] = cfg.acc[q]
+                pl.initial_mass[q] = cfg.initial_mass[q]
+                pl.final_mass[q] = cfg.final_mass[q]
+                pl.feeldisk[q] = cfg.feeldisk[q]
+                pl.feelothers[q] = cfg.feelothers[q]
+                pl.binary[q] = cfg.binary[q]
+        check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx)
+
+    def step(self):
+        """One DT (AlgoGas) on the device; returns the step report."""
+        rep = FbStepReport()
+        check(self.lib.fb_algogas(self.ctx, C.byref(rep)), "fb_algogas", self.ctx)
+        return rep
+
+    def stage(self, stage, dt):
+        check(self.lib.fb_stage(self.ctx, int(stage), float(dt)), "fb_stage", self.ctx)
+
+    def download(self, mask=FB_F_ALL):
+        check(self.lib.fb_download(self.ctx, C.byref(self.st), C.c_uint(mask)), "fb_download", self.ctx)
+        out = {k: v.copy() for k, v in self.fields.items()}
+        st = self.st
+        out.update(PhysicalTime=st.physical_time, LostMass=st.lost_mass, MINDT=st.mindt, MAXDT=st.maxdt,
+                   OmegaFrame=st.omega_frame)
+        n = st.planets.nb
+        for name in ("mass", "x", "y", "vx", "vy"):
+            out["pl_" + name] = np.array([getattr(st.planets, name)[q] for q in range(n)])
+        return out
+
+    def derived(self, which):
+        out = np.zeros(self.nf)
+        check(self.lib.fb_download_derived(self.ctx, int(which), _ptr(out)), "fb_download_derived", self.ctx)
+        return out
+
+    def diagnostics(self):
+        m, p = C.c_double(), C.c_double()
+        check(self.lib.fb_diagnostics(self.ctx, C.byref(m), C.byref(p)), "fb_diagnostics", self.ctx)
+        return m.value, p.value
+
+    def close(self):
+        if self.ctx:
+            self.lib.fb_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -1,0 +1,162 @@
+"""ctypes view of the C ABI declared in include/fargo_b200.h.
+
+The structures mirror the C layout field for field; `check_layout()` compares
+their sizes with the library's own `fb_struct_size`.  Loading fails loudly
+when libfargo_b200.so has not been built: there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+FB_MAX_PLANETS = 16
+FB_OK = 0
+FB_ERR = {
+    -1: "FB_ERR_INVALID", -2: "FB_ERR_UNSUPPORTED", -3: "FB_ERR_CUDA", -4: "FB_ERR_NOMEM",
+    -5: "FB_ERR_NAN", -6: "FB_ERR_NEGATIVE", -7: "FB_ERR_SUBSTEPS", -8: "FB_ERR_TIMEOUT",
+    -9: "FB_ERR_IO", -10: "FB_ERR_STATE", -11: "FB_ERR_NODEVICE",
+}
+FB_F_DENS, FB_F_VRAD, FB_F_VTHETA, FB_F_ENERGY, FB_F_ALL = 1, 2, 4, 8, 15
+FB_STAGE_TRANSPORT, FB_STAGE_VISCOSITY, FB_STAGE_BOUNDARY, FB_STAGE_DAMPING, FB_STAGE_SELFGRAV = 1, 2, 3, 4, 5
+
+_D = C.c_double
+_I = C.c_int
+_P = C.POINTER(C.c_double)
+_NP = FB_MAX_PLANETS
+
+
+class FbParams(C.Structure):
+    _fields_ = [
+        ("nrad", _I), ("nsec", _I), ("rmin", _D), ("rmax", _D), ("log_grid", _I),
+        ("pmin", _D), ("pmax", _D),
+        ("dt", _D), ("ntot", _I), ("ninterm", _I),
+        ("sigma0", _D), ("sigmaslope", _D), ("aspectratio", _D), ("flaringindex", _D),
+        ("alphaviscosity", _D), ("viscosity", _D),
+        ("adiabaticindex", _D), ("energy_equation", _I), ("viscous_heating", _I),
+        ("beta_cooling", _I), ("betacoolingtime", _D), ("betacoolingslope", _D),
+        ("self_gravity", _I), ("sgthicknesssmoothing", _D),
+        ("thicknesssmoothing", _D), ("rochesmoothing", _D), ("indirecttermsmoothing", _D),
+        ("masstaper", _D), ("omegaframe", _D),
+        ("indirect_term", _I), ("discard_gas_indirect_term", _I), ("alternative_gas_indirect_term", _I),
+        ("forced_circular", _I), ("exclude_hill", _I),
+        ("excludehillfactor", _D), ("eccentricity", _D), ("releasedate", _D), ("releaseradius", _D),
+        ("fast_transport", _I), ("wall_boundary", _I), ("evanescent", _I),
+        ("wkzrmin", _D), ("wkzrmax", _D), ("dampingtodynamicaltimeratio", _D),
+        ("damp_to_axi", _I), ("damp_to_ini", _I), ("add_floors", _I),
+        ("densityfloor", _D), ("zero_vrad_bc", _I),
+        ("mindt", _D), ("maxdt", _D), ("imposeddiskdrift", _D),
+        ("factorunitmass", _D), ("factorunitlength", _D), ("factormmw", _D),
+        ("nbpart", _I),
+        ("sizeminpart", _D), ("sizemaxpart", _D), ("sizepartslope", _D), ("rhopart", _D), ("dustslope", _D),
+        ("rmindust", _D), ("rmaxdust", _D),
+        ("dust_feel_disk", _I), ("dust_feel_planets", _I), ("dust_feel_turb", _I), ("dust_feedback", _I),
+        ("sfta", _I), ("interpolation", _I),
+        ("unsupported", C.c_ulonglong),
+        ("planetconfig", C.c_char * 512), ("outputdir", C.c_char * 512),
+    ]
+
+
+class FbPlanets(C.Structure):
+    _fields_ = [
+        ("nb", _I),
+        ("mass", _D * _NP), ("x", _D * _NP), ("y", _D * _NP),
+        ("vx", _D * _NP), ("vy", _D * _NP), ("acc", _D * _NP),
+        ("initial_mass", _D * _NP), ("final_mass", _D * _NP),
+        ("feeldisk", _I * _NP), ("feelothers", _I * _NP), ("binary", _I * _NP),
+    ]
+
+
+class FbState(C.Structure):
+    _fields_ = [
+        ("dens", _P), ("vrad", _P), ("vtheta", _P), ("energy", _P),
+        ("physical_time", _D), ("physical_time_initial", _D),
+        ("omega_frame", _D), ("lost_mass", _D), ("mindt", _D), ("maxdt", _D),
+        ("stardiscbarycenter_x", _D * 3), ("stardiscbarycenter_y", _D * 3),
+        ("planets", FbPlanets),
+    ]
+
+
+class FbProfiles(C.Structure):
+    _fields_ = [
+        ("sigma_med", _P), ("sigma_inf", _P), ("energy_med", _P), ("vtheta_med", _P),
+        ("vrad_med", _P), ("global_soundspeed", _P),
+    ]
+
+
+class FbStepReport(C.Structure):
+    _fields_ = [
+        ("substeps", _I), ("status", _I), ("physical_time", _D), ("mindt", _D), ("maxdt", _D),
+        ("lost_mass", _D), ("gpu_ms", _D),
+    ]
+
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libfargo_b200.so")
+
+#: every symbol include/fargo_b200.h declares
+EXPORTS = (
+    "fb_params_default", "fb_params_read_par", "fb_unsupported_name", "fb_planets_read_cfg",
+    "fb_init_state", "fb_create", "fb_destroy", "fb_upload", "fb_algogas", "fb_download",
+    "fb_download_derived", "fb_diagnostics", "fb_strerror", "fb_last_error", "fb_stage",
+    "fb_build_info", "fb_struct_size",
+)
+
+_lib = None
+
+
+def load():
+    """Load libfargo_b200.so (built by `make -C dustyfargoadsg_b200`)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            "libfargo_b200.so is not built (%s); run `make -C dustyfargoadsg_b200` or "
+            "__graft_entry__.build()" % LIB_PATH)
+    lib = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    sig = {
+        "fb_params_default": (_I, [C.POINTER(FbParams)]),
+        "fb_params_read_par": (_I, [C.POINTER(FbParams), C.c_char_p]),
+        "fb_unsupported_name": (C.c_char_p, [C.POINTER(FbParams)]),
+        "fb_planets_read_cfg": (_I, [C.POINTER(FbParams), C.c_char_p, C.POINTER(FbPlanets)]),
+        "fb_init_state": (_I, [C.POINTER(FbParams), vp, _D, C.c_long, C.POINTER(FbState), C.POINTER(FbProfiles)]),
+        "fb_create": (_I, [C.POINTER(FbParams), _P, C.POINTER(vp)]),
+        "fb_destroy": (_I, [vp]),
+        "fb_upload": (_I, [vp, C.POINTER(FbState), C.POINTER(FbProfiles)]),
+        "fb_algogas": (_I, [vp, C.POINTER(FbStepReport)]),
+        "fb_download": (_I, [vp, C.POINTER(FbState), C.c_uint]),
+        "fb_download_derived": (_I, [vp, _I, _P]),
+        "fb_diagnostics": (_I, [vp, _P, _P]),
+        "fb_strerror": (C.c_char_p, [_I]),
+        "fb_last_error": (C.c_char_p, [vp]),
+        "fb_stage": (_I, [vp, _I, _D]),
+        "fb_build_info": (C.c_char_p, []),
+        "fb_struct_size": (_I, [_I]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    check_layout(lib)
+    return lib
+
+
+def check_layout(lib):
+    for idx, cls in enumerate((FbParams, FbPlanets, FbState, FbProfiles, FbStepReport)):
+        want = lib.fb_struct_size(idx)
+        if want != C.sizeof(cls):
+            raise RuntimeError("ABI mismatch for %s: C %d bytes, ctypes %d" % (cls.__name__, want, C.sizeof(cls)))
+
+
+class FbError(RuntimeError):
+    def __init__(self, code, where, detail=""):
+        self.code = code
+        name = FB_ERR.get(code, str(code))
+        super().__init__("%s failed: %s%s" % (where, name, (" (" + detail + ")") if detail else ""))
+
+
+def check(code, where, ctx=None):
+    if code != FB_OK:
+        detail = ""
+        if ctx is not None and _lib is not None:
+            detail = (_lib.fb_last_error(ctx) or b"").decode(errors="replace")
+        raise FbError(code, where, detail)

@@ -1,0 +1,556 @@
+// fb_api.cu -- the C ABI of libfargo_b200.so: device context, upload /
+// download, and the substep sequence of AlgoGas (src/SourceEuler.c:326-719).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+#include "fb_dev.cuh"
+
+struct fb_ctx {
+  fb_params p;
+  fb_geom g;
+  int nr, ns;
+  size_t nf;
+  cudaStream_t st;
+  cudaEvent_t ev0, ev1;
+  KP k;
+  std::vector<void *> allocs;
+  fb_ctl *d_ctl;
+  fb_ctl *h_ctl;  // pinned mirror
+  double *d_diag;
+  double *h_diag; // pinned
+  fb_sg *sg;
+  int uploaded;
+  char err[512];
+  // host copies of the tables that depend on uploaded profiles
+  std::vector<double> h_supp;
+};
+
+static void set_err(fb_ctx *c, const char *fmt, ...)
+{
+  if (!c) return;
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(c->err, sizeof c->err, fmt, ap);
+  va_end(ap);
+}
+
+#define CK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t _e = (call);                                                        \
+    if (_e != cudaSuccess) {                                                        \
+      set_err(ctx, "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e)); \
+      return FB_ERR_CUDA;                                                           \
+    }                                                                               \
+  } while (0)
+
+static double *dalloc(fb_ctx *ctx, size_t n)
+{
+  void *p = NULL;
+  if (cudaMalloc(&p, n * sizeof(double)) != cudaSuccess) return NULL;
+  cudaMemset(p, 0, n * sizeof(double));
+  ctx->allocs.push_back(p);
+  return (double *)p;
+}
+
+static const double *dtable(fb_ctx *ctx, const double *h, size_t n)
+{
+  double *d = dalloc(ctx, n);
+  if (d && h) cudaMemcpy(d, h, n * sizeof(double), cudaMemcpyHostToDevice);
+  return d;
+}
+
+extern "C" const fb_geom *fb_ctx_geom(const fb_ctx *ctx) { return ctx ? &ctx->g : NULL; }
+
+extern "C" const char *fb_strerror(int code)
+{
+  switch (code) {
+    case FB_OK: return "ok";
+    case FB_ERR_INVALID: return "invalid argument or parameter";
+    case FB_ERR_UNSUPPORTED: return "feature not supported by this build";
+    case FB_ERR_CUDA: return "CUDA error";
+    case FB_ERR_NOMEM: return "out of memory";
+    case FB_ERR_NAN: return "non-finite value in the gas state";
+    case FB_ERR_NEGATIVE: return "negative density or energy";
+    case FB_ERR_SUBSTEPS: return "CFL substep count out of range";
+    case FB_ERR_TIMEOUT: return "bounded device wait timed out";
+    case FB_ERR_IO: return "I/O error";
+    case FB_ERR_STATE: return "call made in the wrong order";
+    case FB_ERR_NODEVICE: return "no CUDA device";
+    default: return "unknown error";
+  }
+}
+
+extern "C" const char *fb_last_error(const fb_ctx *ctx) { return ctx ? ctx->err : "no context"; }
+
+extern "C" const char *fb_build_info(void)
+{
+  return "libfargo_b200 sm_100a fp64 --fmad=false abi " "1";
+}
+
+// ------------------------------------------------------------------ create
+extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
+{
+  if (!p || !out) return FB_ERR_INVALID;
+  *out = NULL;
+  if (p->unsupported) return FB_ERR_UNSUPPORTED;
+  if (p->nrad < 4 || p->nsec < 2) return FB_ERR_INVALID;
+  if (p->self_gravity && !p->log_grid) return FB_ERR_INVALID;  // sginit.c:6-7
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return FB_ERR_NODEVICE;
+  fb_ctx *ctx = new fb_ctx();
+  ctx->p = *p;
+  ctx->nr = p->nrad;
+  ctx->ns = p->nsec;
+  ctx->nf = (size_t)(p->nrad + 1) * p->nsec;
+  ctx->err[0] = 0;
+  int rc = fb_geom_fill(p, radii, &ctx->g);
+  if (rc) { delete ctx; return rc; }
+  rc = fb_gas_prepare(ctx->ns, p->energy_equation);
+  if (rc) { set_err(ctx, "ring of %d doubles does not fit in shared memory", ctx->ns); fb_geom_free(&ctx->g); delete ctx; return rc; }
+  if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return FB_ERR_CUDA; }
+  cudaEventCreate(&ctx->ev0);
+  cudaEventCreate(&ctx->ev1);
+  const int nr = ctx->nr, ns = ctx->ns;
+  const size_t nf = ctx->nf;
+  KP &k = ctx->k;
+  memset(&k, 0, sizeof k);
+  k.nr = nr;
+  k.ns = ns;
+  k.nf = nf;
+  double **fields[] = {&k.rho, &k.vr, &k.vt, &k.e, &k.cs, &k.pres, &k.pot, &k.vri, &k.vti,
+                       &k.divv, &k.trr, &k.tpp, &k.trp, &k.vischeat, &k.q[0], &k.q[1], &k.q[2],
+                       &k.q[3], &k.q[4], &k.q[5], &k.rho_t, &k.sg_accr, &k.sg_acct};
+  for (size_t f = 0; f < sizeof fields / sizeof fields[0]; f++) {
+    *fields[f] = dalloc(ctx, nf);
+    if (!*fields[f]) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+  }
+  k.lost0 = dalloc(ctx, ns);
+  // 1-D tables (host, glibc libm; see fb_host.c)
+  const fb_geom &g = ctx->g;
+  std::vector<double> cs_ring(nr), p15(nr), dxrad(nr), dxth(nr), invdxth(nr), dxth_cfl(nr), mindx2(nr);
+  std::vector<double> beta(nr), dlam(nr, 0.0), dtau(nr, 1.0);
+  std::vector<int> drings;
+  for (int i = 0; i < nr; i++) {
+    const double r = g.rmed[i];
+    cs_ring[i] = fb_host_aspect_ratio(p, r) * sqrt(FB_G * 1.0 / r) * pow(r, p->flaringindex);
+    p15[i] = pow(r, 1.5);
+    dxrad[i] = g.rsup[i] - g.rinf[i];
+    dxth[i] = (p->pmax - p->pmin) / (double)ns * g.rmed[i];   // SourceEuler.c:928, TransportEuler.c:405
+    invdxth[i] = 1.0 / dxth[i];
+    dxth_cfl[i] = g.rmed[i] * (p->pmax - p->pmin) / (double)ns;  // SourceEuler.c:1344
+    {
+      double a = dxrad[i], b = dxth_cfl[i];
+      double m = (b < a) ? b : a;
+      mindx2[i] = pow(m, 2.0);
+    }
+    beta[i] = p->betacoolingtime * pow(r, -p->betacoolingslope);  // Theo.c:216-222
+    if (p->evanescent && ((r < p->wkzrmin) || (r > p->wkzrmax))) {
+      double damping = 0.0, T = 1.0;
+      if (r < p->wkzrmin) {
+        damping = (r - p->wkzrmin) / (g.rmed[0] - p->wkzrmin);
+        T = p->dampingtodynamicaltimeratio * pow(r, 1.5);
+      }
+      if (r > p->wkzrmax) {
+        damping = (r - p->wkzrmax) / (g.rmed[nr - 1] - p->wkzrmax);
+        T = p->dampingtodynamicaltimeratio * pow(r, 1.5);
+      }
+      dlam[i] = damping * damping;
+      dtau[i] = T;
+      drings.push_back(i);
+    }
+  }
+  k.rinf = dtable(ctx, g.rinf, nr + 1);
+  k.rsup = dtable(ctx, g.rsup, nr);
+  k.rmed = dtable(ctx, g.rmed, nr + 1);
+  k.surf = dtable(ctx, g.surf, nr);
+  k.invrmed = dtable(ctx, g.invrmed, nr);
+  k.invsurf = dtable(ctx, g.invsurf, nr);
+  k.invdiffrsup = dtable(ctx, g.invdiffrsup, nr);
+  k.invrinf = dtable(ctx, g.invrinf, nr);
+  k.invdiffrmed = dtable(ctx, g.invdiffrmed, nr + 1);
+  k.cosaz = dtable(ctx, g.cosaz, ns);
+  k.sinaz = dtable(ctx, g.sinaz, ns);
+  k.cs_ring = dtable(ctx, cs_ring.data(), nr);
+  k.gcs = dalloc(ctx, nr);
+  k.p15 = dtable(ctx, p15.data(), nr);
+  k.dxrad = dtable(ctx, dxrad.data(), nr);
+  k.dxtheta = dtable(ctx, dxth.data(), nr);
+  k.invdxtheta = dtable(ctx, invdxth.data(), nr);
+  k.dxtheta_cfl = dtable(ctx, dxth_cfl.data(), nr);
+  k.mindx2 = dtable(ctx, mindx2.data(), nr);
+  k.supp_torque = dalloc(ctx, nr);
+  k.sigmamed = dalloc(ctx, nr);
+  k.energymed = dalloc(ctx, nr);
+  k.vthetamed = dalloc(ctx, nr);
+  k.vradmed = dalloc(ctx, nr);
+  k.betatab = dtable(ctx, beta.data(), nr);
+  k.damp_lam = dtable(ctx, dlam.data(), nr);
+  k.damp_tau = dtable(ctx, dtau.data(), nr);
+  {
+    int *d = NULL;
+    if (!drings.empty()) {
+      cudaMalloc(&d, drings.size() * sizeof(int));
+      cudaMemcpy(d, drings.data(), drings.size() * sizeof(int), cudaMemcpyHostToDevice);
+      ctx->allocs.push_back(d);
+    }
+    k.damp_rings = d;
+    k.n_damp_rings = (int)drings.size();
+  }
+  k.vh_l1 = log(g.rmed[0] / g.rmed[1]);
+  k.vh_l2 = log(g.rmed[1] / g.rmed[2]);
+  k.ringmin = dalloc(ctx, nr);
+  k.vmoy = dalloc(ctx, nr);
+  {
+    size_t cells = (size_t)nr * ns;
+    int nb = (int)((cells + 255) / 256);
+    if (nb > 296) nb = 296;
+    k.n_partial_blocks = nb;
+    k.partials = dalloc(ctx, (size_t)nb * 5);
+    ctx->d_diag = dalloc(ctx, (size_t)nb * 2);
+    if (cudaMallocHost((void **)&ctx->h_diag, (size_t)nb * 2 * sizeof(double)) != cudaSuccess) {
+      fb_destroy(ctx);
+      return FB_ERR_NOMEM;
+    }
+  }
+  if (cudaMalloc((void **)&ctx->d_ctl, sizeof(fb_ctl)) != cudaSuccess ||
+      cudaMallocHost((void **)&ctx->h_ctl, sizeof(fb_ctl)) != cudaSuccess) {
+    fb_destroy(ctx);
+    return FB_ERR_NOMEM;
+  }
+  cudaMemset(ctx->d_ctl, 0, sizeof(fb_ctl));
+  memset(ctx->h_ctl, 0, sizeof(fb_ctl));
+  k.ctl = ctx->d_ctl;
+  // scalars
+  k.pmin = p->pmin;
+  k.pmax = p->pmax;
+  k.dphi = (p->pmax - p->pmin) / (double)ns;
+  k.invdphi = 1.0 / k.dphi;
+  k.omega_frame = p->omegaframe;
+  k.gamma = p->adiabaticindex;
+  k.alpha = p->alphaviscosity;
+  k.nu_const = p->viscosity;
+  k.visc_mode = (p->alphaviscosity != 0.0) ? 1 : (p->viscosity != 0.0 ? 2 : 0);
+  k.energy = p->energy_equation;
+  k.viscous_heating = p->viscous_heating;
+  k.beta_cooling = p->beta_cooling;
+  k.fast_transport = p->fast_transport;
+  k.wall = p->wall_boundary;
+  k.evanescent = p->evanescent;
+  k.add_floors = p->add_floors;
+  k.damp_axi = p->damp_to_axi;
+  k.zero_vrad = p->zero_vrad_bc;
+  k.floordens = p->densityfloor;
+  k.wkzrmin = p->wkzrmin;
+  k.wkzrmax = p->wkzrmax;
+  k.indirect_term = p->indirect_term;
+  k.discard_gas_it = p->discard_gas_indirect_term;
+  k.alt_gas_it = p->alternative_gas_indirect_term;
+  k.exclude_hill = p->exclude_hill;
+  k.roche = (p->rochesmoothing != 0.0);
+  k.forced_circular = p->forced_circular;
+  k.indirect_smoothing = p->indirecttermsmoothing;
+  k.rochesmoothing = p->rochesmoothing;
+  k.thicksmoothing = p->thicknesssmoothing;
+  k.aspectratio = p->aspectratio;
+  k.flaringindex = p->flaringindex;
+  k.masstaper = p->masstaper;
+  k.self_gravity = p->self_gravity;
+  k.transport_only = 0;
+  if (p->self_gravity) {
+    rc = fb_sg_create(&ctx->sg, p, &ctx->g, ctx->st);
+    if (rc) { set_err(ctx, "self-gravity setup failed (%d)", rc); fb_destroy(ctx); return rc; }
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) { fb_destroy(ctx); return FB_ERR_CUDA; }
+  *out = ctx;
+  return FB_OK;
+}
+
+extern "C" int fb_destroy(fb_ctx *ctx)
+{
+  if (!ctx) return FB_OK;
+  if (ctx->st) cudaStreamSynchronize(ctx->st);
+  if (ctx->sg) fb_sg_destroy(ctx->sg);
+  for (void *p : ctx->allocs) cudaFree(p);
+  if (ctx->d_ctl) cudaFree(ctx->d_ctl);
+  if (ctx->h_ctl) cudaFreeHost(ctx->h_ctl);
+  if (ctx->h_diag) cudaFreeHost(ctx->h_diag);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->st) cudaStreamDestroy(ctx->st);
+  fb_geom_free(&ctx->g);
+  delete ctx;
+  return FB_OK;
+}
+
+// ------------------------------------------------------------ upload
+__global__ void k_fill_cs_iso(KP k)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  for (size_t l = (size_t)blockIdx.x * blockDim.x + threadIdx.x; l < n; l += (size_t)gridDim.x * blockDim.x)
+    k.cs[l] = k.cs_ring[l / k.ns];
+}
+
+extern "C" int fb_upload(fb_ctx *ctx, const fb_state *s, const fb_profiles *prof)
+{
+  if (!ctx || !s) return FB_ERR_INVALID;
+  KP &k = ctx->k;
+  const size_t bytes = ctx->nf * sizeof(double);
+  const int nr = ctx->nr;
+  if (s->dens) CK(cudaMemcpyAsync(k.rho, s->dens, bytes, cudaMemcpyHostToDevice, ctx->st));
+  if (s->vrad) CK(cudaMemcpyAsync(k.vr, s->vrad, bytes, cudaMemcpyHostToDevice, ctx->st));
+  if (s->vtheta) CK(cudaMemcpyAsync(k.vt, s->vtheta, bytes, cudaMemcpyHostToDevice, ctx->st));
+  if (s->energy) CK(cudaMemcpyAsync(k.e, s->energy, bytes, cudaMemcpyHostToDevice, ctx->st));
+  if (prof) {
+    if (prof->sigma_med) {
+      CK(cudaMemcpyAsync((void *)k.sigmamed, prof->sigma_med, nr * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+      ctx->h_supp.assign(nr, 0.0);
+      for (int i = 0; i < nr; i++)  // SourceEuler.c:933
+        ctx->h_supp[i] = ctx->p.imposeddiskdrift * 0.5 * pow(ctx->g.rmed[i], -2.5) * ctx->p.sigma0 / prof->sigma_med[i];
+      CK(cudaMemcpyAsync((void *)k.supp_torque, ctx->h_supp.data(), nr * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    }
+    if (prof->energy_med) CK(cudaMemcpyAsync((void *)k.energymed, prof->energy_med, nr * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    if (prof->vtheta_med) CK(cudaMemcpyAsync((void *)k.vthetamed, prof->vtheta_med, nr * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    if (prof->vrad_med) CK(cudaMemcpyAsync((void *)k.vradmed, prof->vrad_med, nr * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+    if (prof->global_soundspeed) CK(cudaMemcpyAsync(k.gcs, prof->global_soundspeed, nr * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  }
+  if (!ctx->p.energy_equation) {
+    k_fill_cs_iso<<<256, 256, 0, ctx->st>>>(k);
+  } else {
+    fb_launch_soundspeed(k, 0, ctx->st);
+  }
+  // scalar state
+  fb_ctl *c = ctx->h_ctl;
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaMemcpy(c, ctx->d_ctl, sizeof(fb_ctl), cudaMemcpyDeviceToHost));
+  c->physical_time = s->physical_time;
+  c->physical_time_initial = s->physical_time_initial;
+  c->omega_frame = s->omega_frame;
+  c->lost_mass = s->lost_mass;
+  c->mindt = s->mindt;
+  c->maxdt = s->maxdt;
+  for (int q = 0; q < 3; q++) {
+    c->bary_x[q] = s->stardiscbarycenter_x[q];
+    c->bary_y[q] = s->stardiscbarycenter_y[q];
+  }
+  const fb_planets &pl = s->planets;
+  if (pl.nb < 0 || pl.nb > FB_MAX_PLANETS) return FB_ERR_INVALID;
+  c->np = pl.nb;
+  for (int q = 0; q < pl.nb; q++) {
+    if (pl.acc[q] > 1e-10) { set_err(ctx, "planet accretion is not supported"); return FB_ERR_UNSUPPORTED; }
+    if (pl.feeldisk[q]) { set_err(ctx, "planets feeling the disc are not supported"); return FB_ERR_UNSUPPORTED; }
+    if (pl.binary[q]) { set_err(ctx, "binary planets are not supported"); return FB_ERR_UNSUPPORTED; }
+    c->pm[q] = pl.mass[q];
+    c->px[q] = pl.x[q];
+    c->py[q] = pl.y[q];
+    c->pvx[q] = pl.vx[q];
+    c->pvy[q] = pl.vy[q];
+    c->pacc[q] = pl.acc[q];
+    c->pinit[q] = pl.initial_mass[q];
+    c->pfinal[q] = pl.final_mass[q];
+    c->pfeelothers[q] = pl.feelothers[q];
+  }
+  if (ctx->p.omegaframe != s->omega_frame) {
+    set_err(ctx, "OmegaFrame must stay OMEGAFRAME (non-rotating frame)");
+    return FB_ERR_UNSUPPORTED;
+  }
+  CK(cudaMemcpy(ctx->d_ctl, c, sizeof(fb_ctl), cudaMemcpyHostToDevice));
+  ctx->uploaded = 1;
+  return FB_OK;
+}
+
+// ------------------------------------------------------------ one DT
+static void enqueue_substep(fb_ctx *ctx)
+{
+  KP &k = ctx->k;
+  cudaStream_t s = ctx->st;
+  fb_launch_cfl(k, s);
+  fb_launch_force_sums(k, s);
+  fb_launch_controller(k, s);
+  if (k.energy) fb_launch_soundspeed(k, k.visc_mode == 1, s);
+  fb_launch_potential(k, s);
+  fb_launch_substep1(k, s);
+  if (k.self_gravity) {
+    fb_sg_accel(ctx->sg, k, k.rho, s);
+    fb_sg_update_velocities(k, s);
+  }
+  if (k.visc_mode) {
+    fb_launch_viscous_terms(k, k.vri, k.vti, s);
+    fb_launch_viscous_update(k, k.vri, k.vti, 0.0, s);
+  }
+  fb_launch_substep2(k, s);
+  if (k.energy) {
+    if (k.viscous_heating)
+      fb_launch_viscous_terms(k, k.vr, k.vt, s);
+    else
+      fb_launch_divergence(k, s);
+    fb_launch_substep3(k, s);
+  }
+  fb_launch_transport(k, 0.0, s);
+  if (k.evanescent) fb_launch_damping(k, 0.0, s);
+}
+
+extern "C" int fb_algogas(fb_ctx *ctx, fb_step_report *rep)
+{
+  if (!ctx) return FB_ERR_INVALID;
+  if (!ctx->uploaded) return FB_ERR_STATE;
+  KP &k = ctx->k;
+  cudaStream_t s = ctx->st;
+  CK(cudaEventRecord(ctx->ev0, s));
+  fb_launch_begin_dt(k, ctx->p.dt, s);
+  if (k.energy) fb_launch_soundspeed(k, 0, s);  // SourceEuler.c:344-350
+  int status = FB_OK;
+  const int cap = 1000000;
+  for (int it = 0; it < cap; it++) {
+    enqueue_substep(ctx);
+    CK(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(fb_ctl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (ctx->h_ctl->status) { status = ctx->h_ctl->status; break; }
+    if (ctx->h_ctl->done) break;
+    if (it == cap - 1) status = FB_ERR_SUBSTEPS;
+  }
+  CK(cudaEventRecord(ctx->ev1, s));
+  CK(cudaEventSynchronize(ctx->ev1));
+  CK(cudaGetLastError());
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+  const fb_ctl *c = ctx->h_ctl;
+  if (rep) {
+    rep->substeps = c->substeps;
+    rep->status = status;
+    rep->physical_time = c->physical_time;
+    rep->mindt = c->mindt;
+    rep->maxdt = c->maxdt;
+    rep->lost_mass = c->lost_mass;
+    rep->gpu_ms = ms;
+  }
+  if (status) set_err(ctx, "AlgoGas stopped: %s", fb_strerror(status));
+  return status;
+}
+
+// ------------------------------------------------------------ download
+extern "C" int fb_download(fb_ctx *ctx, fb_state *s, unsigned mask)
+{
+  if (!ctx || !s) return FB_ERR_INVALID;
+  KP &k = ctx->k;
+  const size_t bytes = ctx->nf * sizeof(double);
+  if ((mask & FB_F_DENS) && s->dens) CK(cudaMemcpyAsync(s->dens, k.rho, bytes, cudaMemcpyDeviceToHost, ctx->st));
+  if ((mask & FB_F_VRAD) && s->vrad) CK(cudaMemcpyAsync(s->vrad, k.vr, bytes, cudaMemcpyDeviceToHost, ctx->st));
+  if ((mask & FB_F_VTHETA) && s->vtheta) CK(cudaMemcpyAsync(s->vtheta, k.vt, bytes, cudaMemcpyDeviceToHost, ctx->st));
+  if ((mask & FB_F_ENERGY) && s->energy) CK(cudaMemcpyAsync(s->energy, k.e, bytes, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(fb_ctl), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  const fb_ctl *c = ctx->h_ctl;
+  s->physical_time = c->physical_time;
+  s->physical_time_initial = c->physical_time_initial;
+  s->omega_frame = c->omega_frame;
+  s->lost_mass = c->lost_mass;
+  s->mindt = c->mindt;
+  s->maxdt = c->maxdt;
+  for (int q = 0; q < 3; q++) {
+    s->stardiscbarycenter_x[q] = c->bary_x[q];
+    s->stardiscbarycenter_y[q] = c->bary_y[q];
+  }
+  s->planets.nb = c->np;
+  for (int q = 0; q < c->np; q++) {
+    s->planets.mass[q] = c->pm[q];
+    s->planets.x[q] = c->px[q];
+    s->planets.y[q] = c->py[q];
+    s->planets.vx[q] = c->pvx[q];
+    s->planets.vy[q] = c->pvy[q];
+  }
+  return FB_OK;
+}
+
+extern "C" int fb_download_derived(fb_ctx *ctx, int which, double *out)
+{
+  if (!ctx || !out || which < 0 || which > 5) return FB_ERR_INVALID;
+  double *tmp = NULL;
+  CK(cudaMallocAsync((void **)&tmp, ctx->nf * sizeof(double), ctx->st));
+  CK(cudaMemsetAsync(tmp, 0, ctx->nf * sizeof(double), ctx->st));
+  fb_launch_derived(ctx->k, which, tmp, ctx->st);
+  CK(cudaMemcpyAsync(out, tmp, ctx->nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaFreeAsync(tmp, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return FB_OK;
+}
+
+extern "C" int fb_diagnostics(fb_ctx *ctx, double *mass, double *momentum)
+{
+  if (!ctx) return FB_ERR_INVALID;
+  const int nb = ctx->k.n_partial_blocks;
+  fb_launch_diag(ctx->k, ctx->d_diag, ctx->st);
+  CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag, (size_t)nb * 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  double m = 0.0, p = 0.0;
+  for (int b = 0; b < nb; b++) {
+    m += ctx->h_diag[2 * b];
+    p += ctx->h_diag[2 * b + 1];
+  }
+  if (mass) *mass = m;
+  if (momentum) *momentum = p;
+  return FB_OK;
+}
+
+// ------------------------------------------------------------ stages
+extern "C" int fb_stage(fb_ctx *ctx, int stage, double dt)
+{
+  if (!ctx) return FB_ERR_INVALID;
+  if (!ctx->uploaded) return FB_ERR_STATE;
+  KP k = ctx->k;
+  cudaStream_t s = ctx->st;
+  switch (stage) {
+    case FB_STAGE_TRANSPORT:
+      if (!(dt > 0.0)) return FB_ERR_INVALID;
+      k.transport_only = 1;
+      fb_launch_transport(k, dt, s);
+      break;
+    case FB_STAGE_VISCOSITY:
+      if (!(dt > 0.0)) return FB_ERR_INVALID;
+      if (k.energy) fb_launch_soundspeed(k, k.visc_mode == 1, s);
+      fb_launch_viscous_terms(k, k.vr, k.vt, s);
+      fb_launch_viscous_update(k, k.vr, k.vt, dt, s);
+      break;
+    case FB_STAGE_BOUNDARY:
+      fb_launch_boundary_only(k, s);
+      break;
+    case FB_STAGE_DAMPING:
+      if (!(dt > 0.0)) return FB_ERR_INVALID;
+      fb_launch_damping(k, dt, s);
+      break;
+    case FB_STAGE_SELFGRAV:
+      if (!ctx->sg) return FB_ERR_STATE;
+      fb_sg_accel(ctx->sg, k, k.rho, s);
+      break;
+    default:
+      return FB_ERR_INVALID;
+  }
+  CK(cudaStreamSynchronize(s));
+  CK(cudaGetLastError());
+  return FB_OK;
+}
+
+// Initial-state helper for self-gravity: SG acceleration of a host density
+// and its azimuthal means (mpi_make1Dprofile of SG_Accr, sgsysinit.c:13-14).
+extern "C" int fb_sg_axisym_accel(fb_ctx *ctx, const double *dens, double *axi_out)
+{
+  if (!ctx || !dens || !axi_out) return FB_ERR_INVALID;
+  if (!ctx->sg) return FB_ERR_STATE;
+  KP &k = ctx->k;
+  const int nr = ctx->nr, ns = ctx->ns;
+  CK(cudaMemcpyAsync(k.rho, dens, ctx->nf * sizeof(double), cudaMemcpyHostToDevice, ctx->st));
+  fb_sg_accel(ctx->sg, k, k.rho, ctx->st);
+  std::vector<double> acc((size_t)nr * ns);
+  CK(cudaMemcpyAsync(acc.data(), k.sg_accr, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  for (int i = 0; i < nr; i++) {
+    double a = 0.0;
+    for (int j = 0; j < ns; j++) a += acc[(size_t)i * ns + j];
+    a /= (double)ns;
+    axi_out[i] = a;
+  }
+  return FB_OK;
+}

@@ -1,0 +1,111 @@
+// fb_dev.cuh -- device-side data structures of libfargo_b200.so (internal).
+//
+// Memory layout in HBM: every 2-D field is one array of (nr+1)*ns doubles in
+// the reference's ring-major order l = j + i*ns (src/LowTasks.c:97-112), so
+// a ring is a contiguous, 8-byte aligned run of ns doubles and a warp reading
+// 32 consecutive azimuths issues fully coalesced 256-byte transactions.
+// Ring nr exists for the outer radial-velocity interface.  All scratch
+// fields are zeroed once at creation; rings that the reference never writes
+// in a scratch field therefore read as zero here too, which the step relies
+// on (e.g. VradInt ring 0 and ring nr, src/SourceEuler.c:866 loops 1..nr-1).
+#pragma once
+#include <cuda_runtime.h>
+#include "fb_internal.h"
+
+// Device-resident control block: the scalar state of AlgoGas
+// (src/SourceEuler.c:333-460), advanced by a one-thread kernel so that the
+// whole substep stays on the device.
+struct fb_ctl {
+  double DT, dtemp, dt, dthydro, dtnbody;
+  double physical_time, physical_time_initial, omega_frame;
+  double mindt, maxdt, lost_mass;
+  double disk_acc_x, disk_acc_y, disk_acc_alt_x, disk_acc_alt_y;
+  double ind_x, ind_y;                       // IndirectTerm (Pframeforce.c:25)
+  double bary_x[3], bary_y[3];               // stardiscbarycenter_{x,y}
+  double mdisc;
+  int substeps, done, status, crash_count, nonfinite;
+  int np;
+  double pm[FB_MAX_PLANETS], px[FB_MAX_PLANETS], py[FB_MAX_PLANETS];
+  double pvx[FB_MAX_PLANETS], pvy[FB_MAX_PLANETS], pacc[FB_MAX_PLANETS];
+  double pinit[FB_MAX_PLANETS], pfinal[FB_MAX_PLANETS];
+  int pfeelothers[FB_MAX_PLANETS];
+  // planets as seen by FillForcesArrays in the current substep
+  double pot_m[FB_MAX_PLANETS], pot_x[FB_MAX_PLANETS], pot_y[FB_MAX_PLANETS];
+  double pot_smooth2[FB_MAX_PLANETS], pot_invd3[FB_MAX_PLANETS];
+};
+
+// Everything a kernel needs, passed by value (well under the 32 KB limit).
+struct KP {
+  int nr, ns;
+  size_t nf;
+  // state
+  double *rho, *vr, *vt, *e;
+  // derived / scratch fields
+  double *cs, *pres, *pot;
+  double *vri, *vti;
+  double *divv, *trr, *tpp, *trp, *vischeat;
+  double *q[6];        // transport: RadMomP, RadMomM, ThetaMomP, ThetaMomM, Energy, Rho
+  double *rho_t;       // density after transport, before floors
+  double *lost0;       // ns: ring-0 radial mass fluxes of the last substep
+  double *sg_accr, *sg_acct;  // SG accelerations (nf)
+  // per-ring tables (nr or nr+1 entries)
+  const double *rinf, *rsup, *rmed, *surf, *invrmed, *invsurf, *invdiffrsup, *invrinf, *invdiffrmed;
+  const double *cosaz, *sinaz;
+  const double *cs_ring;   // isothermal sound speed per ring
+  double *gcs;             // GLOBAL_SoundSpeed (ring means of cs)
+  const double *p15;       // pow(Rmed, 1.5)
+  const double *dxrad, *dxtheta, *invdxtheta, *mindx2;
+  const double *dxtheta_cfl; // Rmed*(PMAX-PMIN)/ns as ConditionCFL forms it (SourceEuler.c:1344)
+  const double *supp_torque;
+  const double *sigmamed, *energymed, *vthetamed, *vradmed;
+  const double *betatab;   // ComputeBetaCooling(Rmed)
+  const double *damp_lam;  // damping*damping per ring (0 outside the zones)
+  const double *damp_tau;  // DAMPINGTODYNAMICALTIMERATIO*pow(Rmed,1.5)
+  const int *damp_rings;   // list of rings inside the wave-killing zones
+  int n_damp_rings;
+  double vh_l1, vh_l2;     // log(r/rip), log(rip/ri2p) for ViscHeat at i=0
+  // CFL / reductions
+  double *ringmin, *vmoy;
+  double *partials;
+  int n_partial_blocks;
+  fb_ctl *ctl;
+  // scalars
+  double pmin, pmax, dphi, invdphi, omega_frame;
+  double gamma, alpha, nu_const;
+  int visc_mode;           // 0 inviscid, 1 alpha, 2 constant nu
+  int energy, viscous_heating, beta_cooling, fast_transport;
+  int wall, evanescent, add_floors, damp_axi, zero_vrad;
+  double floordens, wkzrmin, wkzrmax;
+  int indirect_term, discard_gas_it, alt_gas_it, exclude_hill, roche, forced_circular;
+  double indirect_smoothing, rochesmoothing, thicksmoothing, aspectratio, flaringindex;
+  double masstaper;
+  int self_gravity;
+  int transport_only;      // stage test: Transport without floors/boundaries
+};
+
+// launchers (fb_gas.cu)
+void fb_launch_cfl(const KP &k, cudaStream_t s);
+void fb_launch_force_sums(const KP &k, cudaStream_t s);
+void fb_launch_controller(const KP &k, cudaStream_t s);
+void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s);
+void fb_launch_potential(const KP &k, cudaStream_t s);
+void fb_launch_substep1(const KP &k, cudaStream_t s);
+void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s);
+void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s);
+void fb_launch_substep2(const KP &k, cudaStream_t s);
+void fb_launch_divergence(const KP &k, cudaStream_t s);
+void fb_launch_substep3(const KP &k, cudaStream_t s);
+void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s);
+void fb_launch_floors_boundary(const KP &k, cudaStream_t s);
+void fb_launch_damping(const KP &k, double dt_override, cudaStream_t s);
+void fb_launch_diag(const KP &k, double *out2, cudaStream_t s);
+void fb_launch_derived(const KP &k, int which, double *out, cudaStream_t s);
+void fb_launch_boundary_only(const KP &k, cudaStream_t s);
+int  fb_gas_prepare(int ns, int energy);  // kernel attributes (shared memory)
+void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s);
+// self-gravity (fb_sg.cu)
+struct fb_sg;
+int  fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t s);
+void fb_sg_destroy(fb_sg *sg);
+void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
+void fb_sg_update_velocities(const KP &k, cudaStream_t s);

@@ -1,0 +1,1205 @@
+// fb_gas.cu -- FP64 kernels of one gas substep of AlgoGas
+// (src/SourceEuler.c:398-716) for sm_100a.
+//
+// Every kernel restates the reference expression it replaces with the same
+// operand order (the library is built with --fmad=false so that no multiply
+// is fused into an add), citing the reference file:line.  Ring reductions
+// (azimuthal means) use a fixed tree order inside one CTA: deterministic,
+// but rounded differently from the reference's sequential sums (~1e-16
+// relative).  All of these kernels are bound by memory traffic; their
+// algorithmic bytes per cell are listed in DESIGN.md.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "fb_dev.cuh"
+
+#define FB_BS 256
+
+static __device__ __forceinline__ double min2(double a, double b) { return (b < a) ? b : a; }  // SourceEuler.c:293
+static __device__ __forceinline__ double max2(double a, double b) { return (b > a) ? b : a; }  // SourceEuler.c:300
+
+static __device__ __forceinline__ double dt_of(const KP &k, double dtov) { return dtov > 0.0 ? dtov : k.ctl->dt; }
+
+// ------------------------------------------------------------ reductions
+template <int BS>
+static __device__ double block_sum(double v, double *sh)
+{
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (lane < BS / 32) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[0] = v;
+  }
+  __syncthreads();
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+template <int BS>
+static __device__ double block_min(double v, double *sh)
+{
+  for (int o = 16; o > 0; o >>= 1) {
+    double u = __shfl_down_sync(0xffffffffu, v, o);
+    v = (u < v) ? u : v;
+  }
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (lane < BS / 32) ? sh[lane] : 1e300;
+    for (int o = 16; o > 0; o >>= 1) {
+      double u = __shfl_down_sync(0xffffffffu, v, o);
+      v = (u < v) ? u : v;
+    }
+    if (lane == 0) sh[0] = v;
+  }
+  __syncthreads();
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+static __device__ __forceinline__ double nu_ring(const KP &k, int i)
+{
+  // FViscosity(Rmed[i]) (Viscosity.c:23-69) for the supported laws:
+  // ALPHAVISCOSITY*GLOBAL_SoundSpeed[i]^2*pow(r,1.5), or VISCOSITY.
+  if (k.visc_mode == 1) return k.alpha * k.gcs[i] * k.gcs[i] * k.p15[i];
+  if (k.visc_mode == 2) return k.nu_const;
+  return 0.0;
+}
+
+// ---------------------------------------------------------------- CFL
+// ConditionCFL (SourceEuler.c:1304-1552): one CTA per ring computes the
+// azimuthal mean Vmoy[i] and the smallest per-cell limit of the ring; the
+// controller takes the minimum over rings, adds the shear limit and returns
+// ceil(deltaT/newdt).  DetectCrash (SourceEuler.c:51-69) rides along.
+__global__ void __launch_bounds__(FB_BS) k_cfl(KP k)
+{
+  __shared__ double sh[32];
+  const int i = blockIdx.x, ns = k.ns, nr = k.nr;
+  const size_t base = (size_t)i * ns;
+  const double *vt = k.vt + base, *vr = k.vr + base;
+  double s = 0.0;
+  int neg = 0, bad = 0;
+  for (int j = threadIdx.x; j < ns; j += FB_BS) {
+    s += vt[j];
+    double d = k.rho[base + j];
+    if (d < 0.0) neg = 1;
+    if (!isfinite(d) || !isfinite(vt[j]) || !isfinite(vr[j])) bad = 1;
+    if (k.energy) {
+      double e = k.e[base + j];
+      if (e < 0.0) neg = 1;
+      if (!isfinite(e)) bad = 1;
+    }
+  }
+  s = block_sum<FB_BS>(s, sh);
+  const double vmoy = s / (double)ns;
+  if (threadIdx.x == 0) k.vmoy[i] = vmoy;
+  neg = __syncthreads_or(neg);
+  bad = __syncthreads_or(bad);
+  if (threadIdx.x == 0) {
+    if (neg) atomicAdd(&k.ctl->crash_count, 1);
+    if (bad) atomicOr(&k.ctl->nonfinite, 1);
+  }
+  if (i < 1) return;  // per-cell limits over i = One_or_active..Max_or_active-1
+  const double viscosity = nu_ring(k, i);
+  const double dxrad = k.dxrad[i], dxtheta = k.dxtheta_cfl[i];
+  double m = 1e30;
+  for (int j = threadIdx.x; j < ns; j += FB_BS) {
+    const int jp = (j == ns - 1) ? 0 : j + 1;
+    double vres = k.fast_transport ? vt[j] - vmoy : vt[j];
+    double cs = k.cs[base + j];
+    double invdt1 = cs / (min2(dxrad, dxtheta));
+    double invdt2 = fabs(vr[j]) / dxrad;
+    double invdt3 = fabs(vres) / dxtheta;
+    double dvr = vr[ns + j] - vr[j];
+    double dvt = vt[jp] - vt[j];
+    if (dvr >= 0.0) dvr = 1e-10; else dvr = -dvr;
+    if (dvt >= 0.0) dvt = 1e-10; else dvt = -dvt;
+    double invdt4 = max2(dvr / dxrad, dvt / dxtheta);
+    invdt4 *= 4.0 * FB_CVNR * FB_CVNR;
+    double invdt5 = (viscosity != 0.0) ? viscosity * 4.0 / k.mindx2[i] : 1e-10;
+    double invdt6 = 1e-10;
+    double dt = FB_CFLSECURITY / sqrt(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 +
+                                      invdt4 * invdt4 + invdt5 * invdt5 + invdt6 * invdt6);
+    if (dt < m) m = dt;
+  }
+  m = block_min<FB_BS>(m, sh);
+  if (threadIdx.x == 0) k.ringmin[i] = m;
+  (void)nr;
+}
+
+void fb_launch_cfl(const KP &k, cudaStream_t s) { k_cfl<<<k.nr, FB_BS, 0, s>>>(k); }
+
+// ------------------------------------------------------- disc force sums
+// ComputeForce (Force.c:77-253) for the star (x = y = 0, mass 0) with
+// rsmoothing = INDIRECTTERMSMOOTHING, as called from SourceEuler.c:482, plus
+// GasTotalMass (SideEuler.c:15) and the barycentre sums of
+// ComputeBarycenterPosition (SideEuler.c:42-89).  Per-CTA partials are
+// summed by the controller in CTA order (deterministic).
+__global__ void __launch_bounds__(FB_BS) k_force_sums(KP k)
+{
+  __shared__ double sh[32];
+  const int ns = k.ns;
+  const size_t n = (size_t)k.nr * ns;
+  const double rs = k.indirect_smoothing;
+  double fx = 0.0, fy = 0.0, mass = 0.0, xb = 0.0, yb = 0.0;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    const double xc = k.rmed[i] * k.cosaz[j];
+    const double yc = k.rmed[i] * k.sinaz[j];
+    const double dens = k.rho[l];
+    const double cellmass = k.surf[i] * dens;
+    const double dx = xc - 0.0, dy = yc - 0.0;
+    const double d2 = dx * dx + dy * dy;
+    const double dist2 = d2 + rs * rs;
+    const double distance = sqrt(dist2);
+    const double InvDist3 = 1.0 / dist2 / distance;
+    fx += FB_G * cellmass * dx * InvDist3 * 1.0;
+    fy += FB_G * cellmass * dy * InvDist3 * 1.0;
+    mass += k.surf[i] * dens;
+    xb += k.surf[i] * dens * xc;
+    yb += k.surf[i] * dens * yc;
+  }
+  fx = block_sum<FB_BS>(fx, sh);
+  fy = block_sum<FB_BS>(fy, sh);
+  mass = block_sum<FB_BS>(mass, sh);
+  xb = block_sum<FB_BS>(xb, sh);
+  yb = block_sum<FB_BS>(yb, sh);
+  if (threadIdx.x == 0) {
+    double *p = k.partials + (size_t)blockIdx.x * 5;
+    p[0] = fx; p[1] = fy; p[2] = mass; p[3] = xb; p[4] = yb;
+  }
+}
+
+void fb_launch_force_sums(const KP &k, cudaStream_t s)
+{
+  k_force_sums<<<k.n_partial_blocks, FB_BS, 0, s>>>(k);
+}
+
+// ------------------------------------------------------------ controller
+static __device__ double dev_aspect_ratio(const KP &k, double rad)
+{
+  // AspectRatio (Viscosity.c:107-123) with TRANSITION* at their defaults
+  double aspectratio = k.aspectratio;
+  double rmin = 0.0 - 1.0 * k.aspectratio, rmax = 0.0 + 1.0 * k.aspectratio;
+  if ((rad >= rmin) && (rad <= rmax)) aspectratio *= exp((rmax - rad) / (rmax - rmin) * log(1.0));
+  return aspectratio;
+}
+
+// DerivMotionRK5 (RungeKunta.c:13-53)
+static __device__ void rk5_deriv(const double *q, const double *masses, double *deriv, int n,
+                                 double dt, const int *feelothers, int indirect)
+{
+  const double *x = q, *y = q + n, *vx = q + 2 * n, *vy = q + 3 * n;
+  double *dx = deriv, *dy = deriv + n, *dvx = deriv + 2 * n, *dvy = deriv + 3 * n;
+  double Dist[FB_MAX_PLANETS];
+  for (int i = 0; i < n; i++) Dist[i] = sqrt(x[i] * x[i] + y[i] * y[i]);
+  for (int i = 0; i < n; i++) {
+    dx[i] = vx[i];
+    dy[i] = vy[i];
+    dvx[i] = -FB_G * 1.0 / Dist[i] / Dist[i] / Dist[i] * x[i];
+    dvy[i] = -FB_G * 1.0 / Dist[i] / Dist[i] / Dist[i] * y[i];
+    for (int j = 0; j < n; j++) {
+      if (indirect) {
+        dvx[i] -= FB_G * masses[j] / Dist[j] / Dist[j] / Dist[j] * x[j];
+        dvy[i] -= FB_G * masses[j] / Dist[j] / Dist[j] / Dist[j] * y[j];
+      }
+      if ((j != i) && feelothers[i]) {
+        double dist = (x[i] - x[j]) * (x[i] - x[j]) + (y[i] - y[j]) * (y[i] - y[j]);
+        dist = sqrt(dist);
+        dvx[i] += FB_G * masses[j] / dist / dist / dist * (x[j] - x[i]);
+        dvy[i] += FB_G * masses[j] / dist / dist / dist * (y[j] - y[i]);
+      }
+    }
+  }
+  for (int i = 0; i < 4 * n; i++) deriv[i] *= dt;
+}
+
+// RungeKunta (RungeKunta.c:64-91)
+static __device__ void rk5(const double *q0, double dt, const double *masses, double *q1, int n,
+                           const int *feelothers, int indirect)
+{
+  // k2..k5 enter the first translations multiplied by 0.0; the reference
+  // seeds them with the previous call's k6 (RungeKunta.c:73-75), which is
+  // finite, so zeros give the same sums.
+  double k1[4 * FB_MAX_PLANETS] = {0}, k2[4 * FB_MAX_PLANETS] = {0}, k3[4 * FB_MAX_PLANETS] = {0};
+  double k4[4 * FB_MAX_PLANETS] = {0}, k5[4 * FB_MAX_PLANETS] = {0}, k6[4 * FB_MAX_PLANETS] = {0};
+  const int m = 4 * n;
+  rk5_deriv(q0, masses, k1, n, dt, feelothers, indirect);
+  for (int i = 0; i < m; i++) q1[i] = q0[i] + 0.2 * k1[i] + 0.0 * k2[i] + 0.0 * k3[i] + 0.0 * k4[i] + 0.0 * k5[i];
+  rk5_deriv(q1, masses, k2, n, dt, feelothers, indirect);
+  for (int i = 0; i < m; i++) q1[i] = q0[i] + 0.075 * k1[i] + 0.225 * k2[i] + 0.0 * k3[i] + 0.0 * k4[i] + 0.0 * k5[i];
+  rk5_deriv(q1, masses, k3, n, dt, feelothers, indirect);
+  for (int i = 0; i < m; i++) q1[i] = q0[i] + 0.3 * k1[i] + -0.9 * k2[i] + 1.2 * k3[i] + 0.0 * k4[i] + 0.0 * k5[i];
+  rk5_deriv(q1, masses, k4, n, dt, feelothers, indirect);
+  for (int i = 0; i < m; i++)
+    q1[i] = q0[i] + -11.0 / 54.0 * k1[i] + 2.5 * k2[i] + -70.0 / 27.0 * k3[i] + 35.0 / 27.0 * k4[i] + 0.0 * k5[i];
+  rk5_deriv(q1, masses, k5, n, dt, feelothers, indirect);
+  for (int i = 0; i < m; i++)
+    q1[i] = q0[i] + 1631.0 / 55296.0 * k1[i] + 175.0 / 512.0 * k2[i] + 575.0 / 13824.0 * k3[i] +
+            44275.0 / 110592.0 * k4[i] + 253.0 / 4096.0 * k5[i];
+  rk5_deriv(q1, masses, k6, n, dt, feelothers, indirect);
+  for (int i = 0; i < m; i++)
+    q1[i] = q0[i] + 37.0 / 378.0 * k1[i] + 250.0 / 621.0 * k3[i] + 125.0 / 594.0 * k4[i] + 512.0 / 1771.0 * k6[i];
+}
+
+// The scalar part of one substep of AlgoGas, SourceEuler.c:398-531, run by
+// one thread after k_cfl and k_force_sums.
+__global__ void k_controller(KP k)
+{
+  fb_ctl *c = k.ctl;
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int np = c->np, nr = k.nr;
+  // planet masses (SourceEuler.c:402-418)
+  if (k.masstaper > 1e-2) {
+    double mt = (c->physical_time - c->physical_time_initial) / (k.masstaper * 2.0 * M_PI);
+    mt = (mt > 1.0 ? 1.0 : pow(sin(mt * M_PI / 2.0), 2.0));
+    if (mt < 1.0)
+      for (int p = 0; p < np; p++) c->pm[p] = c->pinit[p] + (c->pfinal[p] - c->pinit[p]) * mt;
+  } else {
+    for (int p = 0; p < np; p++)
+      if (c->pacc[p] < 1e-10) c->pm[p] = c->pfinal[p];
+  }
+  // n-body limit (SourceEuler.c:421-440)
+  double dtnbody;
+  if (np > 1) {
+    dtnbody = 1e5;
+    for (int a = 0; a < np; a++)
+      for (int b = a + 1; b < np; b++) {
+        double xk = c->px[a], xj = c->px[b], yk = c->py[a], yj = c->py[b];
+        double mk = c->pm[a], mj = c->pm[b];
+        double dist = sqrt((xk - xj) * (xk - xj) + (yk - yj) * (yk - yj));
+        double buf = 2.0 * M_PI * sqrt(dist * dist * dist / (mk + mj + 1e-8)) / FB_BINARYSECURITY;
+        dtnbody = min2(dtnbody, buf);
+      }
+  } else {
+    dtnbody = 100.0;
+  }
+  // ConditionCFL reduction (SourceEuler.c:1336-1497) and substep count
+  const double deltaT = c->DT - c->dtemp;
+  double newdt = 1e30;
+  for (int i = 1; i < nr; i++) {
+    double d = k.ringmin[i];
+    if (d < newdt) newdt = d;
+  }
+  for (int i = 0; i < nr - 1; i++) {
+    double d = (k.pmax - k.pmin) * FB_CFLSECURITY / (double)k.ns /
+               fabs(k.vmoy[i] * k.invrmed[i] - k.vmoy[i + 1] * k.invrmed[i + 1]);
+    if (d < newdt) newdt = d;
+  }
+  if (deltaT < newdt) newdt = deltaT;
+  const double ncfl = ceil(deltaT / newdt);
+  if (!(ncfl >= 1.0) || ncfl > 2.0e9) {
+    c->status = FB_ERR_SUBSTEPS;
+    c->done = 1;
+    return;
+  }
+  const int gastimestepcfl = (int)ncfl;
+  const double dthydro = (c->DT - c->dtemp) / (double)gastimestepcfl;
+  const double dt = min2(dthydro, dtnbody);
+  c->dthydro = dthydro;
+  c->dtnbody = dtnbody;
+  c->dt = dt;
+  c->dtemp += dt;
+  if (dt < c->mindt) c->mindt = dt;
+  if (dt > c->maxdt) c->maxdt = dt;
+  // DiskOnPrimaryAcceleration = ComputeAccel(...) (SourceEuler.c:482)
+  double fx = 0.0, fy = 0.0, mass = 0.0, xb = 0.0, yb = 0.0;
+  for (int b = 0; b < k.n_partial_blocks; b++) {
+    const double *p = k.partials + (size_t)b * 5;
+    fx += p[0]; fy += p[1]; mass += p[2]; xb += p[3]; yb += p[4];
+  }
+  c->disk_acc_x = 0.0 + fx;
+  c->disk_acc_y = 0.0 + fy;
+  c->mdisc = mass;
+  // ComputeOppositeAccelerationOfBarycenter (SideEuler.c:91-112)
+  c->bary_x[2] = xb / (1.0 + mass);
+  c->bary_y[2] = yb / (1.0 + mass);
+  c->disk_acc_alt_x = -(c->bary_x[2] - 2.0 * c->bary_x[1] + c->bary_x[0]) / (dt * dt);
+  c->disk_acc_alt_y = -(c->bary_y[2] - 2.0 * c->bary_y[1] + c->bary_y[0]) / (dt * dt);
+  c->bary_x[0] = c->bary_x[1]; c->bary_x[1] = c->bary_x[2];
+  c->bary_y[0] = c->bary_y[1]; c->bary_y[1] = c->bary_y[2];
+  // FillForcesArrays prelude (Pframeforce.c:44-90): indirect term and the
+  // planets' potential parameters at the current positions.
+  double planetmass_taper = 1.0;
+  if (k.masstaper > 1e-2) {
+    double mt = (c->physical_time - c->physical_time_initial) / (k.masstaper * 2.0 * M_PI);
+    planetmass_taper = (mt > 1.0 ? 1.0 : .5 * (1.0 - cos(M_PI * mt)));
+  }
+  c->ind_x = -c->disk_acc_x;
+  c->ind_y = -c->disk_acc_y;
+  if (k.alt_gas_it) { c->ind_x = -c->disk_acc_alt_x; c->ind_y = -c->disk_acc_alt_y; }
+  if (!k.indirect_term) { c->ind_x = 0.0; c->ind_y = 0.0; }
+  for (int p = 0; p < np; p++) {
+    double xplanet = c->px[p], yplanet = c->py[p];
+    double mplanet = c->pm[p] * planetmass_taper;
+    double PlanetDistance = sqrt(xplanet * xplanet + yplanet * yplanet);
+    double InvPlanetDistance3 = 1.0 / PlanetDistance / PlanetDistance / PlanetDistance;
+    double smoothing;
+    if (k.roche) {
+      double RRoche = PlanetDistance * pow((1.0 / 3.0 * mplanet), 1.0 / 3.0);
+      smoothing = RRoche * k.rochesmoothing;
+    } else {
+      smoothing = k.thicksmoothing * dev_aspect_ratio(k, PlanetDistance) * pow(PlanetDistance, 1.0 + k.flaringindex);
+    }
+    c->pot_m[p] = mplanet;
+    c->pot_x[p] = xplanet;
+    c->pot_y[p] = yplanet;
+    c->pot_smooth2[p] = smoothing * smoothing;
+    c->pot_invd3[p] = InvPlanetDistance3;
+  }
+  // AdvanceSystemRK5 (Pframeforce.c:163-266)
+  if (!k.forced_circular) {
+    double q0[4 * FB_MAX_PLANETS], q1[4 * FB_MAX_PLANETS], masses[FB_MAX_PLANETS];
+    for (int i = 0; i < np; i++) {
+      q0[i] = c->px[i]; q0[i + np] = c->py[i]; q0[i + 2 * np] = c->pvx[i]; q0[i + 3 * np] = c->pvy[i];
+      masses[i] = c->pm[i];
+    }
+    if (np > 0) rk5(q0, dt, masses, q1, np, c->pfeelothers, k.indirect_term);
+    for (int i = 0; i < np; i++) {
+      c->px[i] = q1[i]; c->py[i] = q1[i + np]; c->pvx[i] = q1[i + 2 * np]; c->pvy[i] = q1[i + 3 * np];
+    }
+  } else {
+    for (int i = 0; i < np; i++) {
+      double x = c->px[i], y = c->py[i];
+      double theta = atan2(y, x);
+      double vx = c->pvx[i], vy = c->pvy[i];
+      double r = sqrt(x * x + y * y);
+      double v = sqrt(vx * vx + vy * vy);
+      double omega = (-y * vx + x * vy) / r / r;
+      double dtheta = omega * dt;
+      c->px[i] = r * cos(theta + dtheta);
+      c->py[i] = r * sin(theta + dtheta);
+      c->pvx[i] = -v * sin(theta + dtheta);
+      c->pvy[i] = v * cos(theta + dtheta);
+    }
+  }
+  // RotatePsys (Psys.c:352-372) with angle OmegaFrame*dt
+  {
+    double angle = c->omega_frame * dt;
+    double sint = sin(angle), cost = cos(angle);
+    for (int i = 0; i < np; i++) {
+      double xt = c->px[i], yt = c->py[i];
+      c->px[i] = xt * cost + yt * sint;
+      c->py[i] = -xt * sint + yt * cost;
+      xt = c->pvx[i]; yt = c->pvy[i];
+      c->pvx[i] = xt * cost + yt * sint;
+      c->pvy[i] = -xt * sint + yt * cost;
+    }
+  }
+  // LostMass of the previous substep's ring-0 radial mass fluxes
+  // (VanLeerRadial's LostByDisk, TransportEuler.c:213-216).
+  c->physical_time += dt;  // SourceEuler.c:714 (no kernel in this substep reads it)
+  c->substeps += 1;
+  c->done = (c->dtemp < 0.999999999 * c->DT) ? 0 : 1;
+  if (c->nonfinite) { c->status = FB_ERR_NAN; c->done = 1; }
+}
+
+void fb_launch_controller(const KP &k, cudaStream_t s) { k_controller<<<1, 32, 0, s>>>(k); }
+
+// ------------------------------------------------------------ sound speed
+// ComputeSoundSpeed (SourceEuler.c:2323-2343), energy equation, and the
+// ring means GLOBAL_SoundSpeed that mpi_make1Dprofile (axilib.c:5-60) makes
+// inside ComputeViscousTerms (Viscosity.c:247-248).
+__global__ void __launch_bounds__(FB_BS) k_soundspeed(KP k, int update_gcs)
+{
+  __shared__ double sh[32];
+  const int i = blockIdx.x, ns = k.ns;
+  const size_t base = (size_t)i * ns;
+  double s = 0.0;
+  for (int j = threadIdx.x; j < ns; j += FB_BS) {
+    const size_t l = base + j;
+    double c = sqrt(k.gamma * (k.gamma - 1.0) * k.e[l] / k.rho[l]);
+    k.cs[l] = c;
+    s += c;
+  }
+  if (update_gcs) {
+    s = block_sum<FB_BS>(s, sh);
+    if (threadIdx.x == 0) k.gcs[i] = s / (double)ns;
+  }
+}
+
+void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s)
+{
+  k_soundspeed<<<k.nr, FB_BS, 0, s>>>(k, update_gcs);
+}
+
+// ----------------------------------------------------------- potential
+// FillForcesArrays (Pframeforce.c:44-129): star + planets + indirect terms.
+__global__ void __launch_bounds__(FB_BS) k_potential(KP k)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  const fb_ctl *c = k.ctl;
+  const int np = c->np;
+  const int use_ind = (!k.discard_gas_it) && (fabs(k.pmax - k.pmin - 2. * M_PI) < 0.01);
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / k.ns), j = (int)(l - (size_t)i * k.ns);
+    const double x = k.rmed[i] * k.cosaz[j];
+    const double y = k.rmed[i] * k.sinaz[j];
+    double P = 0.0;
+    for (int p = 0; p < np; p++) {
+      const double xplanet = c->pot_x[p], yplanet = c->pot_y[p], mplanet = c->pot_m[p];
+      double distance = (x - xplanet) * (x - xplanet) + (y - yplanet) * (y - yplanet);
+      double distancesmooth = sqrt(distance + c->pot_smooth2[p]);
+      double pot = -FB_G * mplanet / distancesmooth;
+      if (k.indirect_term) pot += FB_G * mplanet * c->pot_invd3[p] * (x * xplanet + y * yplanet);
+      P += pot;
+    }
+    {
+      const double InvDistance = 1.0 / k.rmed[i];
+      double pot = -FB_G * 1.0 * InvDistance;
+      if (use_ind) pot -= c->ind_x * x + c->ind_y * y;
+      P += pot;
+    }
+    k.pot[l] = P;
+  }
+}
+
+void fb_launch_potential(const KP &k, cudaStream_t s)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  int blocks = (int)((n + FB_BS - 1) / FB_BS);
+  k_potential<<<blocks, FB_BS, 0, s>>>(k);
+}
+
+// ------------------------------------------------------------ SubStep1
+static __device__ __forceinline__ double pressure_at(const KP &k, size_t l)
+{
+  // ComputePressureField (SourceEuler.c:2414-2438)
+  if (!k.energy) return k.rho[l] * k.cs[l] * k.cs[l];
+  return (k.gamma - 1.0) * k.e[l];
+}
+
+// SubStep1 (SourceEuler.c:765-1009) without dust: pressure, potential and
+// curvature terms into VradInt (i >= 1) and VthetaInt (all rings).
+__global__ void __launch_bounds__(FB_BS) k_substep1(KP k)
+{
+  const int ns = k.ns;
+  const size_t n = (size_t)k.nr * ns;
+  const double dt = k.ctl->dt;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+    const double Pl = pressure_at(k, l);
+    k.pres[l] = Pl;
+    if (i >= 1) {
+      const size_t lim = l - ns;
+      const double Plim = pressure_at(k, lim);
+      double gradp = (Pl - Plim) * 2.0 / (k.rho[l] + k.rho[lim]) * k.invdiffrmed[i];
+      double gradphi = (k.pot[l] - k.pot[lim]) * k.invdiffrmed[i];
+      double vt2 = k.vt[l] + k.vt[ljp] + k.vt[lim] + k.vt[ljp - ns];
+      vt2 = vt2 / 4.0 + k.rinf[i] * k.omega_frame;
+      vt2 = vt2 * vt2;
+      k.vri[l] = k.vr[l] + dt * (-gradp - gradphi + vt2 * k.invrinf[i]);
+    }
+    {
+      const double Pjm = pressure_at(k, ljm);
+      const double invdxtheta = k.invdxtheta[i];
+      double gradp = (Pl - Pjm) * 2.0 / (k.rho[l] + k.rho[ljm]) * invdxtheta;
+      double gradphi = (k.pot[l] - k.pot[ljm]) * invdxtheta;
+      double vti = k.vt[l] - dt * (gradp + gradphi);
+      vti += dt * k.supp_torque[i];
+      k.vti[l] = vti;
+    }
+  }
+}
+
+void fb_launch_substep1(const KP &k, cudaStream_t s)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  k_substep1<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
+}
+
+// ------------------------------------------------------- viscous stresses
+// ComputeViscousTerms (Viscosity.c:159-303) incl. ComputeDivergenceVelocity
+// (SourceEuler.c:2373-2412): DivV, TAUrr, TAUpp (all rings), TAUrp (i >= 1).
+__global__ void __launch_bounds__(FB_BS) k_viscous_terms(KP k, const double *__restrict__ vr,
+                                                         const double *__restrict__ vt)
+{
+  const int ns = k.ns;
+  const size_t n = (size_t)k.nr * ns;
+  const double invdphi = k.invdphi, onethird = 1.0 / 3.0;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    const size_t lip = l + ns;
+    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+    double div = (vr[lip] * k.rsup[i] - vr[l] * k.rinf[i]) * k.invdiffrsup[i] * k.invrmed[i];
+    div += (vt[ljp] - vt[l]) * invdphi * k.invrmed[i];
+    k.divv[l] = div;
+    const double Drr = (vr[lip] - vr[l]) * k.invdiffrsup[i];
+    const double Dpp = (vt[ljp] - vt[l]) * invdphi * k.invrmed[i] + 0.5 * (vr[lip] + vr[l]) * k.invrmed[i];
+    const double viscosity = nu_ring(k, i);
+    k.trr[l] = 2.0 * k.rho[l] * viscosity * (Drr - onethird * div);
+    k.tpp[l] = 2.0 * k.rho[l] * viscosity * (Dpp - onethird * div);
+    if (i >= 1) {
+      const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+      const size_t lim = l - ns;
+      const size_t ljmim = ljm - ns;
+      const double Drp = 0.5 * (k.rinf[i] * (vt[l] * k.invrmed[i] - vt[lim] * k.invrmed[i - 1]) * k.invdiffrmed[i] +
+                                (vr[l] - vr[ljm]) * invdphi * k.invrinf[i]);
+      k.trp[l] = 2.0 * 0.25 * (k.rho[l] + k.rho[lim] + k.rho[ljm] + k.rho[ljmim]) * viscosity * Drp;
+    }
+  }
+}
+
+void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  k_viscous_terms<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k, vr, vt);
+}
+
+// UpdateVelocitiesWithViscosity (Viscosity.c:305-378)
+__global__ void __launch_bounds__(FB_BS) k_viscous_update(KP k, double *vr, double *vt, double dtov)
+{
+  const int ns = k.ns, nr = k.nr;
+  const size_t n = (size_t)nr * ns;
+  const double DeltaT = dt_of(k, dtov), invdphi = k.invdphi;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    if (i < 1) continue;
+    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+    const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+    const size_t lim = l - ns, lip = l + ns;
+    if (i < nr - 1) {
+      vt[l] += DeltaT * k.invrmed[i] *
+               ((k.rsup[i] * k.trp[lip] - k.rinf[i] * k.trp[l]) * k.invdiffrsup[i] +
+                (k.tpp[l] - k.tpp[ljm]) * invdphi + 0.5 * (k.trp[l] + k.trp[lip])) /
+               (0.5 * (k.rho[l] + k.rho[ljm]));
+    }
+    vr[l] += DeltaT * k.invrinf[i] *
+             ((k.rmed[i] * k.trr[l] - k.rmed[i - 1] * k.trr[lim]) * k.invdiffrmed[i] +
+              (k.trp[ljp] - k.trp[l]) * invdphi - 0.5 * (k.tpp[l] + k.tpp[lim])) /
+             (0.5 * (k.rho[l] + k.rho[lim]));
+  }
+}
+
+void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  k_viscous_update<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k, vr, vt, dt_override);
+}
+
+// ------------------------------------------------------------ SubStep2
+// SubStep2 (SourceEuler.c:1012-1116) followed by the copies of
+// SourceEuler.c:617-622: artificial viscosity from VradInt/VthetaInt into
+// Vrad/Vtheta (and EnergyInt into Energy).  Rings the reference never
+// writes in VradNew/VthetaNew/EnergyInt (ring 0 and ring nr of VradNew, ring
+// nr of the others) are zero, and the copies spread those zeros.
+static __device__ __forceinline__ double q_r(const KP &k, size_t l, size_t lip)
+{
+  double dv = k.vri[lip] - k.vri[l];
+  return (dv < 0.0) ? FB_CVNR * FB_CVNR * k.rho[l] * dv * dv : 0.0;
+}
+static __device__ __forceinline__ double q_t(const KP &k, size_t l, size_t ljp)
+{
+  double dv = k.vti[ljp] - k.vti[l];
+  return (dv < 0.0) ? FB_CVNR * FB_CVNR * k.rho[l] * dv * dv : 0.0;
+}
+
+__global__ void __launch_bounds__(FB_BS) k_substep2(KP k)
+{
+  const int ns = k.ns, nr = k.nr;
+  const size_t n = (size_t)(nr + 1) * ns;
+  const double dt = k.ctl->dt;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    if (i == nr) {
+      k.vr[l] = 0.0;
+      k.vt[l] = 0.0;
+      if (k.energy) k.e[l] = 0.0;
+      continue;
+    }
+    const size_t lip = l + ns;
+    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+    const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+    const double qr = q_r(k, l, lip);
+    const double qt = q_t(k, l, ljp);
+    if (i >= 1) {
+      const size_t lim = l - ns;
+      const double qrim = q_r(k, lim, l);
+      k.vr[l] = k.vri[l] - dt * 2.0 / (k.rho[l] + k.rho[lim]) * (qr - qrim) * k.invdiffrmed[i];
+    } else {
+      k.vr[l] = 0.0;
+    }
+    {
+      const double qtjm = q_t(k, ljm, l);
+      const double invdxtheta = k.invdxtheta[i];
+      k.vt[l] = k.vti[l] - dt * 2.0 / (k.rho[l] + k.rho[ljm]) * (qt - qtjm) * invdxtheta;
+      if (k.energy) {
+        k.e[l] = k.e[l] - dt * qr * (k.vri[lip] - k.vri[l]) * k.invdiffrsup[i] -
+                 dt * qt * (k.vti[ljp] - k.vti[l]) * invdxtheta;
+      }
+    }
+  }
+}
+
+void fb_launch_substep2(const KP &k, cudaStream_t s)
+{
+  const size_t n = (size_t)(k.nr + 1) * k.ns;
+  k_substep2<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
+}
+
+// ComputeDivergenceVelocity (SourceEuler.c:2373-2412) on (Vrad, Vtheta)
+__global__ void __launch_bounds__(FB_BS) k_divergence(KP k)
+{
+  const int ns = k.ns;
+  const size_t n = (size_t)k.nr * ns;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    const size_t lip = l + ns;
+    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+    double div = (k.vr[lip] * k.rsup[i] - k.vr[l] * k.rinf[i]) * k.invdiffrsup[i] * k.invrmed[i];
+    div += (k.vt[ljp] - k.vt[l]) * k.invdphi * k.invrmed[i];
+    k.divv[l] = div;
+  }
+}
+
+void fb_launch_divergence(const KP &k, cudaStream_t s)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  k_divergence<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
+}
+
+// ------------------------------------------------------------ SubStep3
+static __device__ __forceinline__ double vischeat_at(const KP &k, int i, size_t l)
+{
+  // ComputeViscousHeating, SourceEuler.c:1570-1583 (i >= 1)
+  const double viscosity = nu_ring(k, i);
+  if (viscosity != 0.0) {
+    double vh = 0.5 / viscosity / k.rho[l] *
+                (k.trr[l] * k.trr[l] + 2.0 * k.trp[l] * k.trp[l] + k.tpp[l] * k.tpp[l]);
+    vh += (2.0 / 9.0) * viscosity * k.rho[l] * k.divv[l] * k.divv[l];
+    return vh;
+  }
+  return 0.0;
+}
+
+// ComputeViscousHeating (SourceEuler.c:1554-1606) and SubStep3
+// (SourceEuler.c:1119-1302; pdV, viscous heating, beta cooling), one CTA
+// per ring because beta cooling needs the ring mean of vtheta.  Writes
+// Energy = EnergyNew (ring nr of EnergyNew is never written: zero).
+__global__ void __launch_bounds__(FB_BS) k_substep3(KP k)
+{
+  __shared__ double sh[32];
+  const int i = blockIdx.x, ns = k.ns, nr = k.nr;
+  const double dt = k.ctl->dt;
+  const size_t base = (size_t)i * ns;
+  if (i == nr) {
+    for (int j = threadIdx.x; j < ns; j += FB_BS) k.e[base + j] = 0.0;
+    return;
+  }
+  double coolfac = 0.0;
+  if (k.beta_cooling) {
+    double s = 0.0;
+    for (int j = threadIdx.x; j < ns; j += FB_BS) s += (k.vt[base + j] + k.rmed[i] * k.omega_frame);
+    double omega = block_sum<FB_BS>(s, sh);
+    omega /= (double)ns;
+    omega /= k.rmed[i];
+    double coolingtime = k.betatab[i] / omega;
+    coolfac = coolingtime;
+  }
+  // the i = 0 extrapolation tests the viscosity of the last ring visited by
+  // the i >= 1 loop (ring nr-1), SourceEuler.c:1598
+  const double visc_last = nu_ring(k, nr - 1);
+  for (int j = threadIdx.x; j < ns; j += FB_BS) {
+    const size_t l = base + j;
+    double vh = 0.0;
+    if (k.viscous_heating) {
+      if (i >= 1) {
+        vh = vischeat_at(k, i, l);
+      } else {
+        const double qpip = vischeat_at(k, 1, l + ns);
+        const double qpi2p = vischeat_at(k, 2, l + 2 * ns);
+        vh = (visc_last != 0.0) ? qpip * exp(log(qpip / qpi2p) * k.vh_l1 / k.vh_l2) : 0.0;
+      }
+      k.vischeat[l] = vh;
+    }
+    double num = k.e[l] + (double)(k.viscous_heating ? 1 : 0) * vh * dt;
+    double den = 1.0 + (k.gamma - 1.0) * dt * k.divv[l];
+    double en = num / den;
+    if (k.beta_cooling) {
+      double d2 = 1.0 + dt / coolfac;
+      en = en / d2;
+    }
+    k.e[l] = en;
+  }
+}
+
+void fb_launch_substep3(const KP &k, cudaStream_t s) { k_substep3<<<k.nr + 1, FB_BS, 0, s>>>(k); }
+
+// ------------------------------------------------------------ Transport
+// Radial pass of the van Leer transport (OneWindRad, TransportEuler.c:124-220
+// with ComputeLRMomenta :89-119, ComputeStarRad :141-184, DivisePolarGrid
+// SideEuler.c:244-261).  One thread owns one azimuth column and marches
+// through a chunk of rings, keeping the slopes and interface values of the
+// last rings in registers, so each input is read once and no interface is
+// evaluated twice.  Outputs the five (six) transported quantities.
+template <int NQ>
+__global__ void __launch_bounds__(128) k_transport_radial(KP k, double dtov, int chunk)
+{
+  const double dt = dt_of(k, dtov);
+  const int ns = k.ns, nr = k.nr;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const int i0 = blockIdx.y * chunk;
+  const int i1 = min(nr, i0 + chunk);
+  const int jp = (j == ns - 1) ? 0 : j + 1;
+  const double Om = k.omega_frame;
+  const double dtheta = (k.pmax - k.pmin) / (double)ns;
+  // window: index 0 = ring k-1, 1 = ring k, 2 = ring k+1
+  double W[NQ][3], Qo[NQ][3], R[3];
+  double DQ[NQ][2], DR[2], QS[NQ][2], RS[2], VR[2];
+  auto load = [&](int kk, int slot) {
+    if (kk < 0 || kk > nr - 1) {
+#pragma unroll
+      for (int q = 0; q < NQ; q++) { W[q][slot] = 0.0; Qo[q][slot] = 0.0; }
+      R[slot] = 0.0;
+      return;
+    }
+    const size_t l = (size_t)kk * ns + j;
+    const double r = k.rho[l];
+    const double Rm = k.rmed[kk];
+    double qv[NQ];
+    qv[0] = r * k.vr[l + ns];                       // rp = rho*vr[lip]
+    qv[1] = r * k.vr[l];                            // rm = rho*vr[l]
+    qv[2] = r * (k.vt[(size_t)kk * ns + jp] + Rm * Om) * Rm;  // tp
+    qv[3] = r * (k.vt[l] + Rm * Om) * Rm;           // tm
+    if (NQ == 6) qv[4] = k.e[l];
+    qv[NQ - 1] = r;
+    const double den = r + 1e-20;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) { Qo[q][slot] = qv[q]; W[q][slot] = qv[q] / den; }
+    R[slot] = r;
+  };
+  auto slope = [&](double am, double a0, double ap, int kk) -> double {
+    if (kk <= 0 || kk >= nr - 1) return 0.0;
+    double dqm = (a0 - am) * k.invdiffrmed[kk];
+    double dqp = (ap - a0) * k.invdiffrmed[kk + 1];
+    if (dqp * dqm > 0.0) return 2.0 * dqp * dqm / (dqp + dqm);
+    return 0.0;
+  };
+  int kstart = max(i0 - 1, 0);
+  load(kstart - 1, 0);
+  load(kstart, 1);
+#pragma unroll
+  for (int q = 0; q < NQ; q++) { DQ[q][0] = 0.0; QS[q][0] = 0.0; }
+  DR[0] = 0.0; RS[0] = 0.0; VR[0] = 0.0;
+  for (int kk = kstart; kk <= i1; kk++) {
+    load(kk + 1, 2);
+    const double vrk = k.vr[(size_t)kk * ns + j];
+    const double rmk = k.rmed[kk];
+    const double rmkm = (kk >= 1) ? k.rmed[kk - 1] : 0.0;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) DQ[q][1] = slope(W[q][0], W[q][1], W[q][2], kk);
+    DR[1] = slope(R[0], R[1], R[2], kk);
+    if (kk == 0 || kk >= nr) {
+#pragma unroll
+      for (int q = 0; q < NQ; q++) QS[q][1] = 0.0;
+      RS[1] = 0.0;
+    } else if (vrk > 0.0) {
+      const double f = (rmk - rmkm - vrk * dt) * 0.5;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) QS[q][1] = W[q][0] + (rmk - rmkm - vrk * dt) * 0.5 * DQ[q][0];
+      RS[1] = R[0] + f * DR[0];
+    } else {
+      const double rmkp = k.rmed[kk + 1];
+      const double f = (rmkp - rmk + vrk * dt) * 0.5;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) QS[q][1] = W[q][1] - (rmkp - rmk + vrk * dt) * 0.5 * DQ[q][1];
+      RS[1] = R[1] - f * DR[1];
+    }
+    VR[1] = vrk;
+    const int io = kk - 1;
+    if (io >= i0 && io < i1) {
+      const size_t l = (size_t)io * ns + j;
+      const double a = dt * dtheta * k.rinf[io];
+      const double b = dt * dtheta * k.rsup[io];
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        double varq = a * QS[q][0] * RS[0] * VR[0];
+        varq -= b * QS[q][1] * RS[1] * VR[1];
+        k.q[q][l] = Qo[q][0] + varq * k.invsurf[io];
+        if (q == NQ - 1 && io == 0) k.lost0[j] = varq;
+      }
+    }
+    // shift windows
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      W[q][0] = W[q][1]; W[q][1] = W[q][2];
+      Qo[q][0] = Qo[q][1]; Qo[q][1] = Qo[q][2];
+      DQ[q][0] = DQ[q][1];
+      QS[q][0] = QS[q][1];
+    }
+    R[0] = R[1]; R[1] = R[2];
+    DR[0] = DR[1];
+    RS[0] = RS[1];
+    VR[0] = VR[1];
+  }
+}
+
+// Azimuthal pass (OneWindTheta, TransportEuler.c:226-247): ring mean,
+// residual and integer FARGO shift (:249-373), van Leer on the residual and
+// on the uniform part (:375-465), the shift itself, then ComputeVelocities'
+// vtheta (:515-547), the energy floor (SourceEuler.c:2524) and the
+// sub-Keplerian edge rings (SideEuler.c:1008-1044).  One CTA per ring with
+// the whole ring of every quantity in shared memory, so the periodic
+// azimuthal stencil needs no halo exchange.
+template <int NQ>
+__global__ void __launch_bounds__(256) k_transport_azimuthal(KP k, double dtov)
+{
+  const double dt = dt_of(k, dtov);
+  extern __shared__ double smem[];
+  __shared__ double sh[32];
+  const int i = blockIdx.x, ns = k.ns, nr = k.nr;
+  const size_t base = (size_t)i * ns;
+  double *Q = smem;                 // NQ*ns
+  double *vres = Q + NQ * ns;       // ns
+  double *rhos = vres + ns;         // ns
+  double *rhoi = rhos + ns;         // ns
+  double *work = rhoi + ns;         // ns
+  double *dq = work + ns;           // ns
+  double *qrs = dq + ns;            // ns
+  for (int j = threadIdx.x; j < ns; j += blockDim.x)
+    for (int q = 0; q < NQ; q++) Q[q * ns + j] = k.q[q][base + j];
+  // ComputeThetaElongations / ComputeAverageThetaVelocities / ComputeResiduals
+  const double invdt = 1.0 / dt;
+  double s = 0.0;
+  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+    double elong = k.vt[base + j] * dt;
+    s += elong * invdt;
+  }
+  s = block_sum<256>(s, sh);
+  const double VMed = s / (double)ns;
+  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+    double elong = k.vt[base + j] * dt;
+    vres[j] = elong * invdt - VMed;
+  }
+  // ComputeConstantResidual (TransportEuler.c:310-348)
+  const double dpinvns = (k.pmax - k.pmin) / (double)ns;
+  const double Ntilde = VMed * k.invrmed[i] * dt * (double)ns / (k.pmax - k.pmin);
+  const double Nround = floor(Ntilde + 0.5);
+  const long nshift = (long)Nround;
+  double vconst = (Ntilde - Nround) * k.rmed[i] * invdt * dpinvns;
+  if (!k.fast_transport) {
+    for (int j = threadIdx.x; j < ns; j += blockDim.x) vres[j] = vconst + vres[j];
+    vconst = 0.0;
+  }
+  __syncthreads();
+  const double dxtheta = k.dxtheta[i], invdxtheta = k.invdxtheta[i];
+  const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
+  const double invsurf = 1.0 / k.surf[i];
+  const double *rho = Q + (NQ - 1) * ns;
+  for (int pass = 0; pass < 2; pass++) {
+    const bool uniform = (pass == 1);
+    if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
+    // ComputeStarTheta(Rho, V, RhoStar) and RhoInt = Rho
+    for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+      const int jm = (j == 0) ? ns - 1 : j - 1, jp = (j == ns - 1) ? 0 : j + 1;
+      double dqm = (rho[j] - rho[jm]);
+      double dqp = (rho[jp] - rho[j]);
+      dq[j] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+      rhoi[j] = rho[j];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+      const int jm = (j == 0) ? ns - 1 : j - 1;
+      const double v = uniform ? vconst : vres[j];
+      const double ksi = v * dt;
+      rhos[j] = (ksi > 0.0) ? rho[jm] + (dxtheta - ksi) * dq[jm] : rho[j] - (dxtheta + ksi) * dq[j];
+    }
+    __syncthreads();
+    for (int q = 0; q < NQ; q++) {
+      double *qb = Q + q * ns;
+      for (int j = threadIdx.x; j < ns; j += blockDim.x) work[j] = qb[j] / (rhoi[j] + 1e-20);
+      __syncthreads();
+      for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+        const int jm = (j == 0) ? ns - 1 : j - 1, jp = (j == ns - 1) ? 0 : j + 1;
+        double dqm = (work[j] - work[jm]);
+        double dqp = (work[jp] - work[j]);
+        dq[j] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+        const int jm = (j == 0) ? ns - 1 : j - 1;
+        const double v = uniform ? vconst : vres[j];
+        const double ksi = v * dt;
+        qrs[j] = (ksi > 0.0) ? work[jm] + (dxtheta - ksi) * dq[jm] : work[j] - (dxtheta + ksi) * dq[j];
+      }
+      __syncthreads();
+      for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+        const int jp = (j == ns - 1) ? 0 : j + 1;
+        const double v = uniform ? vconst : vres[j];
+        const double vp = uniform ? vconst : vres[jp];
+        double varq = dxrad * qrs[j] * rhos[j] * v;
+        varq -= dxrad * qrs[jp] * rhos[jp] * vp;
+        qb[j] += varq * invsurf;
+      }
+      __syncthreads();
+    }
+  }
+  // AdvectSHIFT (TransportEuler.c:350-373) for every quantity
+  for (int q = 0; q < NQ; q++) {
+    double *qb = Q + q * ns;
+    for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+      long ji = ((long)j - nshift) % ns;
+      if (ji < 0) ji += ns;
+      work[j] = qb[ji];
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < ns; j += blockDim.x) qb[j] = work[j];
+    __syncthreads();
+  }
+  // ComputeVelocities, vtheta part; floors on energy; sub-Keplerian edges
+  const double *tp = Q + 2 * ns, *tm = Q + 3 * ns;
+  const int subkep = (!k.transport_only) && (i == 0 || i == nr - 1);
+  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+    const int jm = (j == 0) ? ns - 1 : j - 1;
+    double v = (tp[jm] + tm[j]) / (rho[j] + rho[jm] + 1e-20) / k.rmed[i] - k.rmed[i] * k.omega_frame;
+    if (subkep) v = k.vthetamed[i] - k.rmed[i] * k.omega_frame;
+    k.vt[base + j] = v;
+    k.rho_t[base + j] = rho[j];
+    k.q[0][base + j] = Q[j];
+    k.q[1][base + j] = Q[ns + j];
+    if (NQ == 6) {
+      double e = Q[4 * ns + j];
+      if (k.add_floors && !k.transport_only) {
+        double e_bottom = 1e-3 * k.energymed[i];
+        if (e < e_bottom) e = e_bottom;
+      }
+      k.e[base + j] = e;
+    }
+  }
+}
+
+// ComputeVelocities' radial part (TransportEuler.c:531-536) needs the
+// neighbouring ring after both passes; fused with AddFloorDensity
+// (SourceEuler.c:2506) and ApplyWallBoundaries (SideEuler.c:1047-1099).
+__global__ void __launch_bounds__(FB_BS) k_transport_vr(KP k)
+{
+  const int ns = k.ns, nr = k.nr;
+  const size_t n = (size_t)(nr + 1) * ns;
+  const int wall = k.wall && !k.transport_only;
+  const int floors = k.add_floors && !k.transport_only;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    auto vr_at = [&](int ii) -> double {
+      if (ii == 0) return 0.0;
+      const size_t m = (size_t)ii * ns + j;
+      return (k.q[0][m - ns] + k.q[1][m]) / (k.rho_t[m] + k.rho_t[m - ns] + 1e-20);
+    };
+    if (i == nr) {
+      if (wall) k.vr[l] = -vr_at(nr - 2);
+      continue;
+    }
+    double d = k.rho_t[l];
+    double v = vr_at(i);
+    if (floors && d < k.floordens) d = k.floordens;
+    if (wall) {
+      if (i == 1) { v = 0.0; d = k.sigmamed[1]; }
+      if (i == 0) { v = -vr_at(2); d = k.sigmamed[0]; }
+      if (i == nr - 1) { v = 0.0; d = k.sigmamed[nr - 1]; }
+      if (i == nr - 2) d = k.sigmamed[nr - 2];
+    }
+    k.rho[l] = d;
+    k.vr[l] = v;
+  }
+}
+
+// LostMass += LostByDisk of the density's VanLeerRadial (TransportEuler.c:137,
+// :213-216): the ring-0 radial fluxes summed over azimuth.
+__global__ void k_lostmass(KP k)
+{
+  double s = 0.0;
+  for (int j = threadIdx.x; j < k.ns; j += 32) s += k.lost0[j];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) k.ctl->lost_mass += 0.0 + s;
+}
+
+void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s)
+{
+  const double dt = dt_override;  // <= 0: kernels read the substep dt from the control block
+  const int chunk = 16;
+  dim3 gr((k.ns + 127) / 128, (k.nr + chunk - 1) / chunk);
+  const int NQ = k.energy ? 6 : 5;
+  const size_t smem = (size_t)(NQ + 6) * k.ns * sizeof(double);
+  if (k.energy) {
+    k_transport_radial<6><<<gr, 128, 0, s>>>(k, dt, chunk);
+    k_transport_azimuthal<6><<<k.nr, 256, smem, s>>>(k, dt);
+  } else {
+    k_transport_radial<5><<<gr, 128, 0, s>>>(k, dt, chunk);
+    k_transport_azimuthal<5><<<k.nr, 256, smem, s>>>(k, dt);
+  }
+  const size_t n = (size_t)(k.nr + 1) * k.ns;
+  k_transport_vr<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
+  k_lostmass<<<1, 32, 0, s>>>(k);
+}
+
+void fb_launch_floors_boundary(const KP &k, cudaStream_t s) { (void)k; (void)s; }
+
+// ApplyBoundaryCondition alone (SideEuler.c:1102-1131): walls and the
+// sub-Keplerian edge rings on the current state (stage tests).
+__global__ void k_boundary_only(KP k)
+{
+  const int ns = k.ns, nr = k.nr;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  if (k.wall) {
+    k.vr[(size_t)1 * ns + j] = 0.0;
+    k.vr[j] = -k.vr[(size_t)2 * ns + j];
+    k.rho[(size_t)1 * ns + j] = k.sigmamed[1];
+    k.rho[j] = k.sigmamed[0];
+    k.vr[(size_t)(nr - 1) * ns + j] = 0.0;
+    k.vr[(size_t)nr * ns + j] = -k.vr[(size_t)(nr - 2) * ns + j];
+    k.rho[(size_t)(nr - 2) * ns + j] = k.sigmamed[nr - 2];
+    k.rho[(size_t)(nr - 1) * ns + j] = k.sigmamed[nr - 1];
+  }
+  k.vt[j] = k.vthetamed[0] - k.rmed[0] * k.omega_frame;
+  k.vt[(size_t)(nr - 1) * ns + j] = k.vthetamed[nr - 1] - k.rmed[nr - 1] * k.omega_frame;
+}
+
+void fb_launch_boundary_only(const KP &k, cudaStream_t s)
+{
+  k_boundary_only<<<(k.ns + 127) / 128, 128, 0, s>>>(k);
+}
+
+// ------------------------------------------------------------ damping
+// EvanescentBoundary (SideEuler.c:796-950), default DampToAxi or DampToIni.
+__global__ void __launch_bounds__(FB_BS) k_damping(KP k, double dtov)
+{
+  __shared__ double sh[32];
+  const int i = k.damp_rings[blockIdx.x], ns = k.ns, nr = k.nr;
+  const size_t base = (size_t)i * ns;
+  const double step = dt_of(k, dtov);
+  const double lambda = k.damp_lam[i] * step / k.damp_tau[i];
+  double vrad0, vtheta0, dens0, energ0;
+  if (k.damp_axi) {
+    double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
+    for (int j = threadIdx.x; j < ns; j += FB_BS) {
+      a += k.vr[base + j];
+      b += k.vt[base + j];
+      c += k.rho[base + j];
+      d += k.e[base + j];
+    }
+    vrad0 = block_sum<FB_BS>(a, sh) / (double)ns;
+    vtheta0 = block_sum<FB_BS>(b, sh) / (double)ns;
+    dens0 = block_sum<FB_BS>(c, sh) / (double)ns;
+    energ0 = block_sum<FB_BS>(d, sh) / (double)ns;
+  } else {
+    vtheta0 = k.vthetamed[i] - k.rmed[i] * k.omega_frame;
+    vrad0 = k.vradmed[i];
+    dens0 = k.sigmamed[i];
+    energ0 = k.energymed[i];
+  }
+  const int zero_here = k.zero_vrad &&
+      (((k.rmed[i] < k.wkzrmin) && (i == 0 || i == 1)) || ((k.rmed[i] > k.wkzrmax) && (i == nr - 1)));
+  for (int j = threadIdx.x; j < ns; j += FB_BS) {
+    const size_t l = base + j;
+    k.vr[l] = (k.vr[l] + lambda * vrad0) / (1.0 + lambda);
+    k.vt[l] = (k.vt[l] + lambda * vtheta0) / (1.0 + lambda);
+    k.rho[l] = (k.rho[l] + lambda * dens0) / (1.0 + lambda);
+    if (k.energy) k.e[l] = (k.e[l] + lambda * energ0) / (1.0 + lambda);
+    if (zero_here) {
+      k.vr[l] = 0.0;
+      k.rho[l] = dens0;
+      k.vt[l] = vtheta0;
+    }
+  }
+}
+
+void fb_launch_damping(const KP &k, double dt_override, cudaStream_t s)
+{
+  if (k.n_damp_rings > 0) k_damping<<<k.n_damp_rings, FB_BS, 0, s>>>(k, dt_override);
+}
+
+// ------------------------------------------------------------ diagnostics
+// GasTotalMass (SideEuler.c:15-40) and GasMomentum (SideEuler.c:114-147)
+__global__ void __launch_bounds__(FB_BS) k_diag(KP k, double *out)
+{
+  __shared__ double sh[32];
+  const int ns = k.ns;
+  const size_t n = (size_t)k.nr * ns;
+  double m = 0.0, p = 0.0;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    m += k.surf[i] * k.rho[l];
+    double vt_cent;
+    if (j < ns - 1)
+      vt_cent = 0.5 * (k.vt[l] + k.vt[l + 1]) + k.rmed[i] * k.omega_frame;
+    else
+      vt_cent = 0.5 * (k.vt[l] + k.vt[(size_t)i * ns]) + k.rmed[i] * k.omega_frame;
+    p += k.surf[i] * k.rho[l] * k.rmed[i] * vt_cent;
+  }
+  m = block_sum<FB_BS>(m, sh);
+  p = block_sum<FB_BS>(p, sh);
+  if (threadIdx.x == 0) {
+    out[2 * blockIdx.x] = m;
+    out[2 * blockIdx.x + 1] = p;
+  }
+}
+
+void fb_launch_diag(const KP &k, double *out2, cudaStream_t s)
+{
+  k_diag<<<k.n_partial_blocks, FB_BS, 0, s>>>(k, out2);
+}
+
+// Derived output fields (layout (nr+1)*ns; ring nr zero)
+__global__ void __launch_bounds__(FB_BS) k_derived(KP k, int which, double *out)
+{
+  const int ns = k.ns;
+  const size_t n = (size_t)k.nr * ns;
+  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
+    double v = 0.0;
+    switch (which) {
+      case 0:  // ComputeTemperatureField (SourceEuler.c:2440-2460)
+        v = k.energy ? 1.0 / 1.0 * (k.gamma - 1.0) * k.e[l] / k.rho[l] : 1.0 / 1.0 * k.pres[l] / k.rho[l];
+        break;
+      case 1: v = k.pot[l]; break;
+      case 2: v = k.pres[l]; break;
+      case 3: v = k.cs[l]; break;
+      case 4: v = k.divv[l]; break;
+      case 5: v = k.vischeat[l]; break;
+      default: v = 0.0;
+    }
+    out[l] = v;
+  }
+}
+
+void fb_launch_derived(const KP &k, int which, double *out, cudaStream_t s)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  k_derived<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k, which, out);
+}
+
+// Start of one AlgoGas call: dtemp = 0 (SourceEuler.c:333) and the loop flags.
+__global__ void k_begin_dt(KP k, double DT)
+{
+  fb_ctl *c = k.ctl;
+  c->DT = DT;
+  c->dtemp = 0.0;
+  c->done = 0;
+  c->substeps = 0;
+  c->status = 0;
+  c->nonfinite = 0;
+}
+
+void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s) { k_begin_dt<<<1, 1, 0, s>>>(k, DT); }
+
+int fb_gas_prepare(int ns, int energy)
+{
+  const int NQ = energy ? 6 : 5;
+  const size_t smem = (size_t)(NQ + 6) * ns * sizeof(double);
+  int dev = 0, maxopt = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (smem + 32 * sizeof(double) > (size_t)maxopt) return FB_ERR_UNSUPPORTED;
+  cudaError_t e1 = cudaFuncSetAttribute(k_transport_azimuthal<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e2 = cudaFuncSetAttribute(k_transport_azimuthal<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  return (e1 == cudaSuccess && e2 == cudaSuccess) ? FB_OK : FB_ERR_CUDA;
+}

@@ -1,0 +1,224 @@
+/*
+ * fargo_b200.h -- C ABI of libfargo_b200.so, a B200 (sm_100a) implementation
+ * of the gas time step of Dusty FARGO-ADSG.
+ *
+ * The boundary replaced is the reference's
+ *     void AlgoGas(Force*, PolarGrid *Rho, *Vrad, *Vtheta, *Energy, *Label,
+ *                  PolarGrid *DRho, *dustpcdens, *DVrad, *DVtheta,
+ *                  PlanetarySystem*, DustSystem*)
+ * (src/SourceEuler.c:326-331, prototype src/proto.h:82), called once per DT
+ * from src/main.c:387.  Here the state lives on the GPU between calls;
+ * the host uploads it once, calls fb_algogas() once per DT and downloads
+ * fields only when it writes outputs.
+ *
+ * Conventions
+ *  - Every entry point returns FB_OK (0) or a negative FB_ERR_* code.  The
+ *    library never calls exit(); fb_last_error() gives a one-line reason.
+ *  - Fields use the reference's PolarGrid layout: ring-major, index
+ *    l = j + i*nsec, with nrad+1 rings (ring nrad holds the outer radial
+ *    velocity interface, src/LowTasks.c:97-112).  Host buffers passed to
+ *    fb_upload / fb_download have (nrad+1)*nsec doubles.
+ *  - FP64 throughout.  A context is not thread-safe; use one per host thread.
+ *  - Features of the reference that this build does not implement are
+ *    rejected by fb_create with FB_ERR_UNSUPPORTED, never silently ignored.
+ */
+#ifndef FARGO_B200_H
+#define FARGO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FB_ABI_VERSION 1
+
+#define FB_OK               0
+#define FB_ERR_INVALID     -1   /* bad argument or parameter value          */
+#define FB_ERR_UNSUPPORTED -2   /* .par feature outside this build          */
+#define FB_ERR_CUDA        -3   /* CUDA runtime error                        */
+#define FB_ERR_NOMEM       -4   /* device or host allocation failed          */
+#define FB_ERR_NAN         -5   /* NaN/Inf found in the gas state            */
+#define FB_ERR_NEGATIVE    -6   /* negative density or energy (the reference's
+                                   DetectCrash, src/SourceEuler.c:51-69)     */
+#define FB_ERR_SUBSTEPS    -7   /* CFL substep count above the cap           */
+#define FB_ERR_TIMEOUT     -8   /* a bounded device wait gave up             */
+#define FB_ERR_IO          -9   /* file could not be read or written         */
+#define FB_ERR_STATE      -10   /* call made in the wrong order              */
+#define FB_ERR_NODEVICE   -11   /* no CUDA device visible                    */
+
+#define FB_MAX_PLANETS 16
+
+/* Hot-path parameters.  Field names follow the reference's .par keys
+ * (src/var.c:13-202); defaults are the reference's (fb_params_default).
+ * String switches are decoded by first letter as src/Interpret.c:165-479
+ * does. */
+typedef struct fb_params {
+  /* grid: NRAD, NSEC, RMIN, RMAX, RADIALSPACING (L/A), PMIN, PMAX */
+  int nrad, nsec;
+  double rmin, rmax;
+  int log_grid;
+  double pmin, pmax;
+  /* time: DT, NTOT, NINTERM */
+  double dt;
+  int ntot, ninterm;
+  /* disc: SIGMA0, SIGMASLOPE, ASPECTRATIO, FLARINGINDEX */
+  double sigma0, sigmaslope, aspectratio, flaringindex;
+  /* ALPHAVISCOSITY, VISCOSITY */
+  double alphaviscosity, viscosity;
+  /* thermodynamics: ADIABATICINDEX, ENERGYEQUATION, VISCOUSHEATING,
+     BETACOOLING, BETACOOLINGTIME, BETACOOLINGSLOPE */
+  double adiabaticindex;
+  int energy_equation, viscous_heating, beta_cooling;
+  double betacoolingtime, betacoolingslope;
+  /* self-gravity: SELFGRAVITY (Yes), SGTHICKNESSSMOOTHING */
+  int self_gravity;
+  double sgthicknesssmoothing;
+  /* planets and frame: THICKNESSSMOOTHING, ROCHESMOOTHING,
+     INDIRECTTERMSMOOTHING, MASSTAPER, OMEGAFRAME, INDIRECTTERM,
+     DISCARDGASINDIRECTTERM, ALTERNATIVEGASINDIRECTTERM, FORCEDCIRCULAR,
+     EXCLUDEHILL, EXCLUDEHILLFACTOR, ECCENTRICITY, RELEASEDATE,
+     RELEASERADIUS */
+  double thicknesssmoothing, rochesmoothing, indirecttermsmoothing;
+  double masstaper, omegaframe;
+  int indirect_term, discard_gas_indirect_term, alternative_gas_indirect_term;
+  int forced_circular, exclude_hill;
+  double excludehillfactor, eccentricity, releasedate, releaseradius;
+  /* transport and boundaries: TRANSPORT (FARGO/Standard), INNERBOUNDARY
+     (Wall), WAVEKILLINGZONES, WKZRMIN, WKZRMAX,
+     DAMPINGTODYNAMICALTIMERATIO, DAMPTOAXI/DAMPTOINI, ADDFLOORS,
+     DENSITYFLOOR, ZEROVRADBC */
+  int fast_transport, wall_boundary, evanescent;
+  double wkzrmin, wkzrmax, dampingtodynamicaltimeratio;
+  int damp_to_axi, damp_to_ini, add_floors;
+  double densityfloor;
+  int zero_vrad_bc;
+  /* MINDT, MAXDT: initial values of the running min/max substep (the
+     reference keeps them as .par variables, src/var.c:145-146) */
+  double mindt, maxdt;
+  /* IMPOSEDDISKDRIFT */
+  double imposeddiskdrift;
+  /* units: FACTORUNITMASS, FACTORUNITLENGTH, FACTORMMW */
+  double factorunitmass, factorunitlength, factormmw;
+  /* Lagrangian dust particles: NBPART, SIZEMINPART, SIZEMAXPART,
+     SIZEPARTSLOPE, RHOPART, DUSTSLOPE, RMINDUST, RMAXDUST, DUSTFEELDISK,
+     DUSTFEELPLANETS, DUSTFEELTURB, DUSTFEEDBACK, SFTAPPROX, INTERPOLATION */
+  int nbpart;
+  double sizeminpart, sizemaxpart, sizepartslope, rhopart, dustslope;
+  double rmindust, rmaxdust;
+  int dust_feel_disk, dust_feel_planets, dust_feel_turb, dust_feedback;
+  int sfta, interpolation; /* interpolation: 0 NGP, 1 CIC, 2 TSC */
+  /* bit mask of .par features that were set but that this build does not
+     implement (fb_create refuses a non-zero mask); see fb_unsupported_name */
+  unsigned long long unsupported;
+  /* PLANETCONFIG and OUTPUTDIR, as written in the .par file */
+  char planetconfig[512];
+  char outputdir[512];
+} fb_params;
+
+/* Planetary system (src/types.h:96-108).  initial_mass/final_mass are the
+   reference's InitialPlanetMass/FinalPlanetMass (src/global.h). */
+typedef struct fb_planets {
+  int nb;
+  double mass[FB_MAX_PLANETS], x[FB_MAX_PLANETS], y[FB_MAX_PLANETS];
+  double vx[FB_MAX_PLANETS], vy[FB_MAX_PLANETS], acc[FB_MAX_PLANETS];
+  double initial_mass[FB_MAX_PLANETS], final_mass[FB_MAX_PLANETS];
+  int feeldisk[FB_MAX_PLANETS], feelothers[FB_MAX_PLANETS], binary[FB_MAX_PLANETS];
+} fb_planets;
+
+/* Host view of the state that AlgoGas reads and writes.  Field pointers
+   refer to caller-owned arrays of (nrad+1)*nsec doubles; a NULL field is
+   skipped by fb_upload / fb_download. */
+typedef struct fb_state {
+  double *dens, *vrad, *vtheta, *energy;
+  double physical_time, physical_time_initial;
+  double omega_frame, lost_mass, mindt, maxdt;
+  double stardiscbarycenter_x[3], stardiscbarycenter_y[3];
+  fb_planets planets;
+} fb_state;
+
+/* Axisymmetric profiles the step reads (src/global.h: SigmaMed, SigmaInf,
+   EnergyMed, VthetaMed, VradMed, GLOBAL_SoundSpeed), nrad doubles each. */
+typedef struct fb_profiles {
+  double *sigma_med, *sigma_inf, *energy_med, *vtheta_med, *vrad_med;
+  double *global_soundspeed;
+} fb_profiles;
+
+/* What one fb_algogas call did. */
+typedef struct fb_step_report {
+  int substeps;          /* CFL substeps taken in this DT                 */
+  int status;            /* FB_OK or the first error seen                 */
+  double physical_time;  /* PhysicalTime after the DT                      */
+  double mindt, maxdt;   /* MINDT / MAXDT (src/SourceEuler.c:457-460)     */
+  double lost_mass;      /* LostMass (src/TransportEuler.c:137)            */
+  double gpu_ms;         /* device time of the DT (CUDA events)            */
+} fb_step_report;
+
+/* Download masks */
+#define FB_F_DENS    0x01u
+#define FB_F_VRAD    0x02u
+#define FB_F_VTHETA  0x04u
+#define FB_F_ENERGY  0x08u
+#define FB_F_ALL     0x0Fu
+
+typedef struct fb_ctx fb_ctx;
+
+/* ---- parameters (host only, no GPU needed) --------------------------- */
+/* Defaults of src/var.c:13-202 and src/Interpret.c:23-50. */
+int fb_params_default(fb_params *p);
+/* Reads a .par file with the rules of ReadVariables (src/Interpret.c:82-480):
+   case-insensitive keys, '#' comments, separators "\t :=>_".  Unknown keys
+   are ignored like the reference does (it warns). */
+int fb_params_read_par(fb_params *p, const char *path);
+/* Name of the first unsupported feature in p->unsupported, or "" */
+const char *fb_unsupported_name(const fb_params *p);
+
+/* ---- initial conditions (host only) ------------------------------------ */
+/* Reads the planet .cfg file (InitPlanetarySystem, src/Psys.c:96-203). */
+int fb_planets_read_cfg(const fb_params *p, const char *path, fb_planets *out);
+/* Fills state and profiles exactly as the reference's main.c:145-291 does
+   for the supported features: FillPolar1DArrays, InitGasDensity (+ optional
+   seeded white noise of relative amplitude noise_amp, drawn with the POSIX
+   drand48 stream seeded by noise_seed, in the reference's loop order),
+   InitGasEnergy, InitEuler/InitGasVelocities.  With self-gravity the
+   initial SG acceleration is needed, which is computed on the GPU of ctx;
+   pass ctx = NULL otherwise.  Field arrays must be allocated by the caller. */
+int fb_init_state(const fb_params *p, fb_ctx *ctx, double noise_amp,
+                  long noise_seed, fb_state *st, fb_profiles *prof);
+
+/* ---- device context ------------------------------------------------------ */
+/* radii: optional nrad+1 interface radii (the reference's Radii array,
+   src/SourceEuler.c:88-104); NULL computes them from rmin/rmax/log_grid. */
+int fb_create(const fb_params *p, const double *radii, fb_ctx **out);
+int fb_destroy(fb_ctx *ctx);
+int fb_upload(fb_ctx *ctx, const fb_state *st, const fb_profiles *prof);
+/* One DT of AlgoGas (src/SourceEuler.c:326-719) on device-resident state. */
+int fb_algogas(fb_ctx *ctx, fb_step_report *rep);
+int fb_download(fb_ctx *ctx, fb_state *st, unsigned mask);
+/* Derived output fields at the current state (reference layout, (nrad+1)*nsec):
+   which = 0 Temperature (src/SourceEuler.c:2440), 1 Potential, 2 Pressure,
+   3 SoundSpeed, 4 DivergenceVelocity, 5 ViscHeat. */
+int fb_download_derived(fb_ctx *ctx, int which, double *out);
+/* Diagnostics on the device state: GasTotalMass (src/SideEuler.c:15) and
+   GasMomentum (src/SideEuler.c:114). */
+int fb_diagnostics(fb_ctx *ctx, double *mass, double *momentum);
+const char *fb_strerror(int code);
+const char *fb_last_error(const fb_ctx *ctx);
+
+/* ---- single stages (parity tests and profiling) ------------------------ */
+#define FB_STAGE_TRANSPORT  1  /* Transport (src/TransportEuler.c:65)       */
+#define FB_STAGE_VISCOSITY  2  /* ComputeViscousTerms + UpdateVelocitiesWithViscosity
+                                  on (vrad, vtheta, dens) (src/Viscosity.c:159-378) */
+#define FB_STAGE_BOUNDARY   3  /* ApplyBoundaryCondition (src/SideEuler.c:1102) */
+#define FB_STAGE_DAMPING    4  /* EvanescentBoundary (src/SideEuler.c:796)  */
+#define FB_STAGE_SELFGRAV   5  /* compute_sgacc only: fills SG accelerations */
+int fb_stage(fb_ctx *ctx, int stage, double dt);
+
+/* Build information: "sm_100a fp64 ..." */
+const char *fb_build_info(void);
+/* sizeof of the ABI structs (0 fb_params, 1 fb_planets, 2 fb_state,
+   3 fb_profiles, 4 fb_step_report), for bindings to check their layout. */
+int fb_struct_size(int which);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FARGO_B200_H */

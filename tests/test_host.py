@@ -1,0 +1,88 @@
+"""CPU tests: the C ABI loads, the .par reader follows the reference's rules,
+and the host-side initial state is bit-identical to the reference's."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from tests import _oracle
+
+REPO = _oracle.REPO
+CFG = _oracle.CONFIG_DIR
+
+
+def test_library_exports_every_declared_symbol():
+    from dustyfargoadsg_b200 import _ffi
+    lib = _ffi.load()
+    header = open(os.path.join(REPO, "include", "fargo_b200.h")).read()
+    declared = set(re.findall(r"\b(fb_[a-z0-9_]+)\s*\(", header))
+    assert declared, "no declarations parsed"
+    for name in sorted(declared):
+        assert hasattr(lib, name), name
+    assert set(_ffi.EXPORTS) == declared
+    assert b"sm_100a" in lib.fb_build_info()
+
+
+def test_struct_layout_matches_ctypes():
+    from dustyfargoadsg_b200 import _ffi
+    _ffi.check_layout(_ffi.load())
+
+
+def test_params_defaults_and_switches():
+    from dustyfargoadsg_b200 import read_par
+    p = read_par(os.path.join(CFG, "iso_128x384.par"))
+    assert (p.nrad, p.nsec) == (128, 384)
+    assert p.log_grid == 1 and p.fast_transport == 1 and p.wall_boundary == 1
+    assert p.evanescent == 1 and abs(p.wkzrmin - 0.5) < 1e-15
+    assert p.forced_circular == 1 and p.energy_equation == 0
+    assert p.unsupported == 0
+    assert abs(p.densityfloor - 1e-9) < 1e-24 and p.add_floors == 1
+    assert p.masstaper == 0.0000001 and p.mindt == 100.0
+
+
+def test_unsupported_features_are_refused(tmp_path):
+    from dustyfargoadsg_b200 import Disc, FbError, read_par
+    src = os.path.join(CFG, "iso_128x384.par")
+    for key, val in (("InnerBoundary", "Non-Reflecting"), ("Frame", "C"), ("DustFluid", "Yes"),
+                     ("ThermalCooling", "Yes")):
+        par = _oracle.write_par(src, str(tmp_path), **{key: val})
+        p = read_par(par)
+        assert p.unsupported != 0, key
+        with pytest.raises(FbError):
+            Disc(p)
+
+
+@pytest.mark.skipif(not _oracle.have_oracle(), reason="oracle not built")
+@pytest.mark.parametrize("noise,seed", [(0.0, 0), (1e-4, 0), (1e-3, 7)])
+def test_initial_state_bit_identical(tmp_path, noise, seed):
+    """fb_init_state == the reference's main.c initialisation, bit for bit."""
+    from dustyfargoadsg_b200 import _ffi, read_par
+    src = os.path.join(CFG, "iso_128x384.par")
+    par = _oracle.write_par(src, str(tmp_path), Nrad=48, Nsec=96)
+    dumps, _, _ = _oracle.run_oracle(par, steps=1, noise=noise, seed=seed, dump_every=1000)
+    ref = dumps["state_init"]
+    lib = _ffi.load()
+    p = read_par(par)
+    nr, ns = p.nrad, p.nsec
+    nf = (nr + 1) * ns
+    f = {k: np.zeros(nf) for k in ("dens", "vrad", "vtheta", "energy")}
+    pr = {k: np.zeros(nr) for k in ("sigma_med", "sigma_inf", "energy_med", "vtheta_med", "vrad_med",
+                                    "global_soundspeed")}
+    ptr = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+    st = _ffi.FbState()
+    for k, a in f.items():
+        setattr(st, k, ptr(a))
+    prof = _ffi.FbProfiles(*[ptr(pr[k]) for k in ("sigma_med", "sigma_inf", "energy_med", "vtheta_med",
+                                                   "vrad_med", "global_soundspeed")])
+    _ffi.check(lib.fb_init_state(C.byref(p), None, noise, seed, C.byref(st), C.byref(prof)), "init")
+    for k in ("dens", "vrad", "vtheta", "energy"):
+        np.testing.assert_array_equal(f[k], ref[k], err_msg=k)
+    np.testing.assert_array_equal(pr["sigma_med"], ref["SigmaMed"])
+    np.testing.assert_array_equal(pr["vtheta_med"], ref["VthetaMed"])
+    np.testing.assert_array_equal(pr["vrad_med"], ref["VradMed"])
+    np.testing.assert_array_equal(pr["global_soundspeed"], ref["GLOBAL_SoundSpeed"])
+    assert st.planets.nb == 1
+    assert st.planets.x[0] == ref["pl_x"][0] and st.planets.vy[0] == ref["pl_vy"][0]
+    assert st.planets.mass[0] == ref["pl_mass"][0]
