@@ -60,6 +60,7 @@ static long h_substeps = 0;
 static long h_calls = 0;
 static int h_atexit_set = 0;
 static int h_stage_done = 0;
+static int h_in_algogas = 0;
 
 static double now_s(void)
 {
@@ -268,7 +269,7 @@ void __wrap_ComputeViscousTerms(PolarGrid *Vr, PolarGrid *Vt, PolarGrid *Rho,
   const char *nm[3] = {"vrad", "vtheta", "dens"};
   PolarGrid *g[3];
   g[0] = Vr; g[1] = Vt; g[2] = Rho;
-  if (stage && h_substeps == 0) {
+  if (stage && h_substeps == 0 && h_in_algogas) {
     static int once = 0;
     if (!once) { once = 1; dump_fields("stage_visc_in", 3, nm, g); }
   }
@@ -284,7 +285,7 @@ void __wrap_UpdateVelocitiesWithViscosity(PolarGrid *Vr, PolarGrid *Vt, PolarGri
   PolarGrid *g[3];
   g[0] = Vr; g[1] = Vt; g[2] = Rho;
   __real_UpdateVelocitiesWithViscosity(Vr, Vt, Rho, DVr, DVt, DRho, dt);
-  if (stage && h_substeps == 0) {
+  if (stage && h_substeps == 0 && h_in_algogas) {
     static int once = 0;
     if (!once) { once = 1; dump_fields("stage_visc_out", 3, nm, g); }
   }
@@ -329,6 +330,7 @@ void __wrap_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad,
   ensure_atexit();
   if (h_calls == 0) dump_state("state_init", Rho, Vrad, Vtheta, Energy, sys, dsys);
   h_call_start = now_s();
+  h_in_algogas = 1;
 #ifdef FB_DROPIN
   fb_dropin_AlgoGas(force, Rho, Vrad, Vtheta, Energy, Label, DRho, dustpcdens,
                     DVrad, DVtheta, sys, dsys);
@@ -337,6 +339,7 @@ void __wrap_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad,
                  DVrad, DVtheta, sys, dsys);
 #endif
   h_time_in_algogas += now_s() - h_call_start;
+  h_in_algogas = 0;
   h_calls++;
   if (every > 0 && (h_calls % every) == 0) {
     snprintf(tag, sizeof tag, "state_%05ld", h_calls);
