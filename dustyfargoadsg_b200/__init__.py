@@ -15,13 +15,18 @@ from . import _ffi
 from ._ffi import (FB_F_ALL, FB_F_DENS, FB_F_ENERGY, FB_F_VRAD, FB_F_VTHETA, FbError, FbParams,
                    FbProfiles, FbState, FbStepReport, check, load)
 
-__all__ = ["Disc", "read_par", "FbError", "load", "CONFIG_DIR"]
+__all__ = ["Disc", "read_par", "select_device", "FbError", "load", "CONFIG_DIR"]
 
 CONFIG_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "configs")
 
 
 def _ptr(a):
     return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def select_device(device):
+    """Make `device` current for the library's CUDA runtime (this thread)."""
+    check(load().fb_select_device(int(device)), "fb_select_device")
 
 
 def read_par(path, **overrides):
@@ -137,6 +142,22 @@ class Disc:
         n = st.planets.nb
         for name in ("mass", "x", "y", "vx", "vy"):
             out["pl_" + name] = np.array([getattr(st.planets, name)[q] for q in range(n)])
+        return out
+
+    def kernel_launches(self):
+        return int(self.lib.fb_kernel_launches(self.ctx))
+
+    def profile(self, enable=True):
+        check(self.lib.fb_profile(self.ctx, 1 if enable else 0), "fb_profile", self.ctx)
+
+    def profile_read(self):
+        """{stage name: (device ms, launches)} accumulated since profile()."""
+        out = {}
+        n = self.lib.fb_profile_read(self.ctx, 0, None, None, None)
+        for idx in range(n):
+            name, ms, cnt = C.c_char_p(), C.c_double(), C.c_longlong()
+            self.lib.fb_profile_read(self.ctx, idx, C.byref(name), C.byref(ms), C.byref(cnt))
+            out[name.value.decode()] = (ms.value, cnt.value)
         return out
 
     def derived(self, which):

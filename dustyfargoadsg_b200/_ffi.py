@@ -95,7 +95,8 @@ EXPORTS = (
     "fb_params_default", "fb_params_read_par", "fb_unsupported_name", "fb_planets_read_cfg",
     "fb_init_state", "fb_create", "fb_destroy", "fb_upload", "fb_algogas", "fb_download",
     "fb_download_derived", "fb_diagnostics", "fb_strerror", "fb_last_error", "fb_stage",
-    "fb_build_info", "fb_struct_size",
+    "fb_build_info", "fb_struct_size", "fb_kernel_launches", "fb_profile", "fb_profile_read",
+    "fb_select_device",
 )
 
 _lib = None
@@ -130,6 +131,10 @@ def load():
         "fb_stage": (_I, [vp, _I, _D]),
         "fb_build_info": (C.c_char_p, []),
         "fb_struct_size": (_I, [_I]),
+        "fb_kernel_launches": (C.c_longlong, [vp]),
+        "fb_profile": (_I, [vp, _I]),
+        "fb_profile_read": (_I, [vp, _I, C.POINTER(C.c_char_p), _P, C.POINTER(C.c_longlong)]),
+        "fb_select_device": (_I, [_I]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

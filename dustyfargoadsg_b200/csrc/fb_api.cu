@@ -9,6 +9,15 @@
 #include <vector>
 #include "fb_dev.cuh"
 
+enum {
+  ST_CFL, ST_FORCE, ST_CONTROL, ST_SOUND, ST_POT, ST_SUB1, ST_SG, ST_VTERMS, ST_VUPDATE,
+  ST_SUB2, ST_EVTERMS, ST_SUB3, ST_TRAD, ST_TAZI, ST_TVR, ST_DAMP, FB_NSTAGE
+};
+static const char *stage_names[FB_NSTAGE] = {
+  "cfl", "force_sums", "controller", "soundspeed", "potential", "substep1", "selfgravity",
+  "viscous_terms", "viscous_update", "substep2", "energy_viscous_terms", "substep3",
+  "transport_radial", "transport_azimuthal", "transport_vr_boundary", "damping"};
+
 struct fb_ctx {
   fb_params p;
   fb_geom g;
@@ -27,6 +36,13 @@ struct fb_ctx {
   char err[512];
   // host copies of the tables that depend on uploaded profiles
   std::vector<double> h_supp;
+  // launch accounting and optional per-stage profiling
+  long long launches;
+  int profiling;
+  std::vector<cudaEvent_t> pev;   // one per recorded point of a substep
+  std::vector<int> pseq;          // stage id of each recorded interval
+  double pms[FB_NSTAGE];
+  long long pcount[FB_NSTAGE];
 };
 
 static void set_err(fb_ctx *c, const char *fmt, ...)
@@ -61,6 +77,14 @@ static const double *dtable(fb_ctx *ctx, const double *h, size_t n)
   double *d = dalloc(ctx, n);
   if (d && h) cudaMemcpy(d, h, n * sizeof(double), cudaMemcpyHostToDevice);
   return d;
+}
+
+extern "C" int fb_select_device(int device)
+{
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) return FB_ERR_NODEVICE;
+  if (device < 0 || device >= n) return FB_ERR_INVALID;
+  return cudaSetDevice(device) == cudaSuccess ? FB_OK : FB_ERR_CUDA;
 }
 
 extern "C" const fb_geom *fb_ctx_geom(const fb_ctx *ctx) { return ctx ? &ctx->g : NULL; }
@@ -280,6 +304,7 @@ extern "C" int fb_destroy(fb_ctx *ctx)
   if (ctx->h_diag) cudaFreeHost(ctx->h_diag);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   fb_geom_free(&ctx->g);
   delete ctx;
@@ -363,34 +388,92 @@ extern "C" int fb_upload(fb_ctx *ctx, const fb_state *s, const fb_profiles *prof
 }
 
 // ------------------------------------------------------------ one DT
-static void enqueue_substep(fb_ctx *ctx)
+// One substep (SourceEuler.c:398-716).  STAGE() records an event before a
+// stage when profiling and counts the kernel launches it issues.
+#define STAGE(id, nlaunch, call)                                 \
+  do {                                                           \
+    if (ctx->profiling) {                                        \
+      cudaEventRecord(ctx->pev[npt], s);                         \
+      ctx->pseq[npt] = (id);                                     \
+      npt++;                                                     \
+    }                                                            \
+    call;                                                        \
+    ctx->launches += (nlaunch);                                  \
+    ctx->pcount[id] += (nlaunch);                                \
+  } while (0)
+
+static int enqueue_substep(fb_ctx *ctx)
 {
   KP &k = ctx->k;
   cudaStream_t s = ctx->st;
-  fb_launch_cfl(k, s);
-  fb_launch_force_sums(k, s);
-  fb_launch_controller(k, s);
-  if (k.energy) fb_launch_soundspeed(k, k.visc_mode == 1, s);
-  fb_launch_potential(k, s);
-  fb_launch_substep1(k, s);
+  int npt = 0;
+  STAGE(ST_CFL, 1, fb_launch_cfl(k, s));
+  STAGE(ST_FORCE, 1, fb_launch_force_sums(k, s));
+  STAGE(ST_CONTROL, 1, fb_launch_controller(k, s));
+  if (k.energy) STAGE(ST_SOUND, 1, fb_launch_soundspeed(k, k.visc_mode == 1, s));
+  STAGE(ST_POT, 1, fb_launch_potential(k, s));
+  STAGE(ST_SUB1, 1, fb_launch_substep1(k, s));
   if (k.self_gravity) {
-    fb_sg_accel(ctx->sg, k, k.rho, s);
-    fb_sg_update_velocities(k, s);
+    STAGE(ST_SG, 0, (fb_sg_accel(ctx->sg, k, k.rho, s), fb_sg_update_velocities(k, s)));
+    ctx->launches += fb_sg_launches(ctx->sg);
+    ctx->pcount[ST_SG] += fb_sg_launches(ctx->sg);
   }
   if (k.visc_mode) {
-    fb_launch_viscous_terms(k, k.vri, k.vti, s);
-    fb_launch_viscous_update(k, k.vri, k.vti, 0.0, s);
+    STAGE(ST_VTERMS, 1, fb_launch_viscous_terms(k, k.vri, k.vti, s));
+    STAGE(ST_VUPDATE, 1, fb_launch_viscous_update(k, k.vri, k.vti, 0.0, s));
   }
-  fb_launch_substep2(k, s);
+  STAGE(ST_SUB2, 1, fb_launch_substep2(k, s));
   if (k.energy) {
     if (k.viscous_heating)
-      fb_launch_viscous_terms(k, k.vr, k.vt, s);
+      STAGE(ST_EVTERMS, 1, fb_launch_viscous_terms(k, k.vr, k.vt, s));
     else
-      fb_launch_divergence(k, s);
-    fb_launch_substep3(k, s);
+      STAGE(ST_EVTERMS, 1, fb_launch_divergence(k, s));
+    STAGE(ST_SUB3, 1, fb_launch_substep3(k, s));
   }
-  fb_launch_transport(k, 0.0, s);
-  if (k.evanescent) fb_launch_damping(k, 0.0, s);
+  STAGE(ST_TRAD, 1, fb_launch_transport_radial(k, 0.0, s));
+  STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s));
+  STAGE(ST_TVR, 2, fb_launch_transport_vr(k, s));
+  if (k.evanescent && k.n_damp_rings > 0) STAGE(ST_DAMP, 1, fb_launch_damping(k, 0.0, s));
+  if (ctx->profiling) {
+    cudaEventRecord(ctx->pev[npt], s);
+    ctx->pseq[npt] = -1;
+    npt++;
+  }
+  return npt;
+}
+
+static void profile_collect(fb_ctx *ctx, int npt)
+{
+  for (int q = 0; q + 1 < npt; q++) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, ctx->pev[q], ctx->pev[q + 1]) == cudaSuccess && ctx->pseq[q] >= 0)
+      ctx->pms[ctx->pseq[q]] += ms;
+  }
+}
+
+extern "C" long long fb_kernel_launches(const fb_ctx *ctx) { return ctx ? ctx->launches : -1; }
+
+extern "C" int fb_profile(fb_ctx *ctx, int enable)
+{
+  if (!ctx) return FB_ERR_INVALID;
+  if (enable && ctx->pev.empty()) {
+    ctx->pev.resize(FB_NSTAGE + 2);
+    ctx->pseq.resize(FB_NSTAGE + 2);
+    for (auto &e : ctx->pev) CK(cudaEventCreate(&e));
+  }
+  ctx->profiling = enable ? 1 : 0;
+  for (int q = 0; q < FB_NSTAGE; q++) { ctx->pms[q] = 0.0; ctx->pcount[q] = 0; }
+  return FB_OK;
+}
+
+extern "C" int fb_profile_read(const fb_ctx *ctx, int idx, const char **name, double *ms, long long *launches)
+{
+  if (!ctx) return FB_ERR_INVALID;
+  if (idx < 0 || idx >= FB_NSTAGE) return FB_NSTAGE;
+  if (name) *name = stage_names[idx];
+  if (ms) *ms = ctx->pms[idx];
+  if (launches) *launches = ctx->pcount[idx];
+  return FB_NSTAGE;
 }
 
 extern "C" int fb_algogas(fb_ctx *ctx, fb_step_report *rep)
@@ -401,13 +484,15 @@ extern "C" int fb_algogas(fb_ctx *ctx, fb_step_report *rep)
   cudaStream_t s = ctx->st;
   CK(cudaEventRecord(ctx->ev0, s));
   fb_launch_begin_dt(k, ctx->p.dt, s);
-  if (k.energy) fb_launch_soundspeed(k, 0, s);  // SourceEuler.c:344-350
+  ctx->launches += 1;
+  if (k.energy) { fb_launch_soundspeed(k, 0, s); ctx->launches += 1; }  // SourceEuler.c:344-350
   int status = FB_OK;
   const int cap = 1000000;
   for (int it = 0; it < cap; it++) {
-    enqueue_substep(ctx);
+    int npt = enqueue_substep(ctx);
     CK(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(fb_ctl), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (ctx->profiling) profile_collect(ctx, npt);
     if (ctx->h_ctl->status) { status = ctx->h_ctl->status; break; }
     if (ctx->h_ctl->done) break;
     if (it == cap - 1) status = FB_ERR_SUBSTEPS;

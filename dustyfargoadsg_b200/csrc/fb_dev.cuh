@@ -96,6 +96,9 @@ void fb_launch_substep2(const KP &k, cudaStream_t s);
 void fb_launch_divergence(const KP &k, cudaStream_t s);
 void fb_launch_substep3(const KP &k, cudaStream_t s);
 void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s);
+void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s);
+void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s);
+void fb_launch_transport_vr(const KP &k, cudaStream_t s);
 void fb_launch_floors_boundary(const KP &k, cudaStream_t s);
 void fb_launch_damping(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_diag(const KP &k, double *out2, cudaStream_t s);
@@ -109,3 +112,4 @@ int  fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_
 void fb_sg_destroy(fb_sg *sg);
 void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
 void fb_sg_update_velocities(const KP &k, cudaStream_t s);
+int  fb_sg_launches(const fb_sg *sg);  // kernels per fb_sg_accel + update

@@ -1022,23 +1022,39 @@ __global__ void k_lostmass(KP k)
   if (threadIdx.x == 0) k.ctl->lost_mass += 0.0 + s;
 }
 
-void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s)
+void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
 {
-  const double dt = dt_override;  // <= 0: kernels read the substep dt from the control block
   const int chunk = 16;
   dim3 gr((k.ns + 127) / 128, (k.nr + chunk - 1) / chunk);
+  if (k.energy)
+    k_transport_radial<6><<<gr, 128, 0, s>>>(k, dt_override, chunk);
+  else
+    k_transport_radial<5><<<gr, 128, 0, s>>>(k, dt_override, chunk);
+}
+
+void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s)
+{
   const int NQ = k.energy ? 6 : 5;
   const size_t smem = (size_t)(NQ + 6) * k.ns * sizeof(double);
-  if (k.energy) {
-    k_transport_radial<6><<<gr, 128, 0, s>>>(k, dt, chunk);
-    k_transport_azimuthal<6><<<k.nr, 256, smem, s>>>(k, dt);
-  } else {
-    k_transport_radial<5><<<gr, 128, 0, s>>>(k, dt, chunk);
-    k_transport_azimuthal<5><<<k.nr, 256, smem, s>>>(k, dt);
-  }
+  if (k.energy)
+    k_transport_azimuthal<6><<<k.nr, 256, smem, s>>>(k, dt_override);
+  else
+    k_transport_azimuthal<5><<<k.nr, 256, smem, s>>>(k, dt_override);
+}
+
+void fb_launch_transport_vr(const KP &k, cudaStream_t s)
+{
   const size_t n = (size_t)(k.nr + 1) * k.ns;
   k_transport_vr<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
   k_lostmass<<<1, 32, 0, s>>>(k);
+}
+
+// Transport (TransportEuler.c:65-87) + floors + boundaries: 4 launches
+void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s)
+{
+  fb_launch_transport_radial(k, dt_override, s);
+  fb_launch_transport_azimuthal(k, dt_override, s);
+  fb_launch_transport_vr(k, s);
 }
 
 void fb_launch_floors_boundary(const KP &k, cudaStream_t s) { (void)k; (void)s; }

@@ -185,6 +185,9 @@ int fb_init_state(const fb_params *p, fb_ctx *ctx, double noise_amp,
                   long noise_seed, fb_state *st, fb_profiles *prof);
 
 /* ---- device context ------------------------------------------------------ */
+/* Selects the CUDA device used by contexts created afterwards on this host
+   thread (cudaSetDevice of the library's runtime). */
+int fb_select_device(int device);
 /* radii: optional nrad+1 interface radii (the reference's Radii array,
    src/SourceEuler.c:88-104); NULL computes them from rmin/rmax/log_grid. */
 int fb_create(const fb_params *p, const double *radii, fb_ctx **out);
@@ -211,6 +214,17 @@ const char *fb_last_error(const fb_ctx *ctx);
 #define FB_STAGE_DAMPING    4  /* EvanescentBoundary (src/SideEuler.c:796)  */
 #define FB_STAGE_SELFGRAV   5  /* compute_sgacc only: fills SG accelerations */
 int fb_stage(fb_ctx *ctx, int stage, double dt);
+
+/* ---- profiling ----------------------------------------------------------- */
+/* Number of kernel launches this context has issued. */
+long long fb_kernel_launches(const fb_ctx *ctx);
+/* enable = 1: record CUDA events between the stages of every substep and
+   accumulate each stage's device time (adds event records to the stream,
+   for profiling runs); enable = 0 stops.  Resets the accumulators. */
+int fb_profile(fb_ctx *ctx, int enable);
+/* Stage idx (0 .. n-1) of the profile: its name, accumulated device ms and
+   number of launches; returns the number of stages, or a negative code. */
+int fb_profile_read(const fb_ctx *ctx, int idx, const char **name, double *ms, long long *launches);
 
 /* Build information: "sm_100a fp64 ..." */
 const char *fb_build_info(void);
