@@ -552,7 +552,7 @@ extern "C" int fb_download(fb_ctx *ctx, fb_state *s, unsigned mask)
 
 extern "C" int fb_download_derived(fb_ctx *ctx, int which, double *out)
 {
-  if (!ctx || !out || which < 0 || which > 5) return FB_ERR_INVALID;
+  if (!ctx || !out || which < 0 || which > 7) return FB_ERR_INVALID;
   double *tmp = NULL;
   CK(cudaMallocAsync((void **)&tmp, ctx->nf * sizeof(double), ctx->st));
   CK(cudaMemsetAsync(tmp, 0, ctx->nf * sizeof(double), ctx->st));

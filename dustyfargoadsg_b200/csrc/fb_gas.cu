@@ -249,13 +249,33 @@ static __device__ void rk5(const double *q0, double dt, const double *masses, do
     q1[i] = q0[i] + 37.0 / 378.0 * k1[i] + 250.0 / 621.0 * k3[i] + 125.0 / 594.0 * k4[i] + 512.0 / 1771.0 * k6[i];
 }
 
-// The scalar part of one substep of AlgoGas, SourceEuler.c:398-531, run by
-// one thread after k_cfl and k_force_sums.
-__global__ void k_controller(KP k)
+// The scalar part of one substep of AlgoGas, SourceEuler.c:398-531.  One CTA:
+// its threads reduce the per-ring CFL limits, the shear limits and the
+// force partials (fixed tree order), then thread 0 runs the scalar logic.
+__global__ void __launch_bounds__(FB_BS) k_controller(KP k)
 {
+  __shared__ double sh[32];
   fb_ctl *c = k.ctl;
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const int np = c->np, nr = k.nr;
+  const int np = c->np, nr = k.nr, tid = threadIdx.x;
+  // ConditionCFL reduction (SourceEuler.c:1336-1497)
+  double m = 1e30;
+  for (int i = 1 + tid; i < nr; i += FB_BS) {
+    double d = k.ringmin[i];
+    if (d < m) m = d;
+  }
+  for (int i = tid; i < nr - 1; i += FB_BS) {
+    double d = (k.pmax - k.pmin) * FB_CFLSECURITY / (double)k.ns /
+               fabs(k.vmoy[i] * k.invrmed[i] - k.vmoy[i + 1] * k.invrmed[i + 1]);
+    if (d < m) m = d;
+  }
+  const double newdt_cells = block_min<FB_BS>(m, sh);
+  double f[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int b = tid; b < k.n_partial_blocks; b += FB_BS) {
+    const double *p = k.partials + (size_t)b * 5;
+    for (int q = 0; q < 5; q++) f[q] += p[q];
+  }
+  for (int q = 0; q < 5; q++) f[q] = block_sum<FB_BS>(f[q], sh);
+  if (tid != 0) return;
   // planet masses (SourceEuler.c:402-418)
   if (k.masstaper > 1e-2) {
     double mt = (c->physical_time - c->physical_time_initial) / (k.masstaper * 2.0 * M_PI);
@@ -283,16 +303,7 @@ __global__ void k_controller(KP k)
   }
   // ConditionCFL reduction (SourceEuler.c:1336-1497) and substep count
   const double deltaT = c->DT - c->dtemp;
-  double newdt = 1e30;
-  for (int i = 1; i < nr; i++) {
-    double d = k.ringmin[i];
-    if (d < newdt) newdt = d;
-  }
-  for (int i = 0; i < nr - 1; i++) {
-    double d = (k.pmax - k.pmin) * FB_CFLSECURITY / (double)k.ns /
-               fabs(k.vmoy[i] * k.invrmed[i] - k.vmoy[i + 1] * k.invrmed[i + 1]);
-    if (d < newdt) newdt = d;
-  }
+  double newdt = newdt_cells;
   if (deltaT < newdt) newdt = deltaT;
   const double ncfl = ceil(deltaT / newdt);
   if (!(ncfl >= 1.0) || ncfl > 2.0e9) {
@@ -310,11 +321,7 @@ __global__ void k_controller(KP k)
   if (dt < c->mindt) c->mindt = dt;
   if (dt > c->maxdt) c->maxdt = dt;
   // DiskOnPrimaryAcceleration = ComputeAccel(...) (SourceEuler.c:482)
-  double fx = 0.0, fy = 0.0, mass = 0.0, xb = 0.0, yb = 0.0;
-  for (int b = 0; b < k.n_partial_blocks; b++) {
-    const double *p = k.partials + (size_t)b * 5;
-    fx += p[0]; fy += p[1]; mass += p[2]; xb += p[3]; yb += p[4];
-  }
+  const double fx = f[0], fy = f[1], mass = f[2], xb = f[3], yb = f[4];
   c->disk_acc_x = 0.0 + fx;
   c->disk_acc_y = 0.0 + fy;
   c->mdisc = mass;
@@ -401,7 +408,7 @@ __global__ void k_controller(KP k)
   if (c->nonfinite) { c->status = FB_ERR_NAN; c->done = 1; }
 }
 
-void fb_launch_controller(const KP &k, cudaStream_t s) { k_controller<<<1, 32, 0, s>>>(k); }
+void fb_launch_controller(const KP &k, cudaStream_t s) { k_controller<<<1, FB_BS, 0, s>>>(k); }
 
 // ------------------------------------------------------------ sound speed
 // ComputeSoundSpeed (SourceEuler.c:2323-2343), energy equation, and the
@@ -1024,12 +1031,16 @@ __global__ void k_lostmass(KP k)
 
 void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
 {
-  const int chunk = 16;
-  dim3 gr((k.ns + 127) / 128, (k.nr + chunk - 1) / chunk);
+  // 64 columns per CTA; ring chunks halve until there are >= 4 CTAs per SM
+  // (longer chunks reread fewer halo rings, shorter ones fill the GPU).
+  const int tx = 64, bx = (k.ns + tx - 1) / tx;
+  int chunk = 32;
+  while (chunk > 4 && (long)bx * ((k.nr + chunk - 1) / chunk) < 4 * 148) chunk /= 2;
+  dim3 gr(bx, (k.nr + chunk - 1) / chunk);
   if (k.energy)
-    k_transport_radial<6><<<gr, 128, 0, s>>>(k, dt_override, chunk);
+    k_transport_radial<6><<<gr, tx, 0, s>>>(k, dt_override, chunk);
   else
-    k_transport_radial<5><<<gr, 128, 0, s>>>(k, dt_override, chunk);
+    k_transport_radial<5><<<gr, tx, 0, s>>>(k, dt_override, chunk);
 }
 
 void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s)
@@ -1181,6 +1192,8 @@ __global__ void __launch_bounds__(FB_BS) k_derived(KP k, int which, double *out)
       case 3: v = k.cs[l]; break;
       case 4: v = k.divv[l]; break;
       case 5: v = k.vischeat[l]; break;
+      case 6: v = k.sg_accr[l]; break;
+      case 7: v = k.sg_acct[l]; break;
       default: v = 0.0;
     }
     out[l] = v;

@@ -1,15 +1,414 @@
-// fb_sg.cu -- log-polar FFT self-gravity (placeholder until the FFT kernels land).
+// fb_sg.cu -- log-polar self-gravity (sgmain.c, sgkernel.c, sgdens.c,
+// sgacc.c, sgupdate.c of the reference) as FP64 FFT kernels for sm_100a.
+//
+// The reference convolves the reduced densities Sr = Sigma sqrt(r/r0) and
+// St = Sr r/r0 with the kernels Kr, Kt on a (2 Nr) x Ns periodic grid (the
+// radial direction zero-padded), through unnormalised FFTW transforms:
+//     A = IFFT2( -G FFT2(K) . FFT2(S) ),   normalised by rstep tstep/(2Nr Ns).
+// Here the transforms are our own Stockham mixed-radix (2,3,4,5) FFTs, one
+// CTA per 1-D transform with the line in shared memory:
+//   1. sg_rows_fwd : per ring i < Nr, one complex FFT of z = Sr + i St along
+//      phi, split into the two half spectra (rows >= Nr are zero, so they
+//      are never transformed);
+//   2. sg_cols     : per azimuthal wavenumber k and per quantity, forward FFT
+//      along the 2 Nr radial points, product with the kernel spectrum,
+//      inverse FFT; only the Nr physical rows are written back;
+//   3. sg_rows_inv : per ring, one inverse complex FFT of Wr + i Wt (both
+//      Hermitian), whose real and imaginary parts are the two accelerations,
+//      with the normalisation and self-force term of sgacc.c:138-161 fused;
+//   4. sg_update   : the velocity kicks of update_sgvelocity (sgupdate.c).
+// The kernel spectra are computed once (host glibc for K, device FFT).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+#include <vector>
 #include "fb_dev.cuh"
 
-struct fb_sg { int dummy; };
+#define SG_BS 256
+#define SG_MAXST 16
 
+struct fb_fft_plan {
+  int n, nst;
+  int radix[SG_MAXST];
+  double2 *tw;  // device: exp(-2 pi i t / n), t < n
+};
+
+struct fb_sg {
+  int nr, ns, m, nk;        // m = 2 nr, nk = ns/2 + 1
+  fb_fft_plan prow, pcol;
+  double2 *xr, *xt;         // half spectra after the row pass, [i][k], i < nr
+  double2 *khr, *kht;       // kernel spectra, [k][m]
+  double *sq, *rr;          // sqrt(Rmed/R0), Rmed (per ring) for the densities
+  double *nr_accr, *nr_acct;  // per-ring normalisations
+  double r0;                // GlobalRmed[0]
+  double rstep, tstep, eps;
+  size_t smem_row, smem_col;
+};
+
+static int plan_radices(int n, int *radix)
+{
+  int k = 0;
+  while (n % 4 == 0 && k < SG_MAXST) { radix[k++] = 4; n /= 4; }
+  while (n % 2 == 0 && k < SG_MAXST) { radix[k++] = 2; n /= 2; }
+  while (n % 3 == 0 && k < SG_MAXST) { radix[k++] = 3; n /= 3; }
+  while (n % 5 == 0 && k < SG_MAXST) { radix[k++] = 5; n /= 5; }
+  if (n != 1) return -1;
+  return k;
+}
+
+static int make_plan(fb_fft_plan *p, int n)
+{
+  p->n = n;
+  p->nst = plan_radices(n, p->radix);
+  if (p->nst < 0) return FB_ERR_UNSUPPORTED;
+  std::vector<double2> h(n);
+  for (int t = 0; t < n; t++) {
+    double a = 2.0 * M_PI * (double)t / (double)n;
+    h[t] = make_double2(cos(a), -sin(a));
+  }
+  if (cudaMalloc(&p->tw, n * sizeof(double2)) != cudaSuccess) return FB_ERR_NOMEM;
+  cudaMemcpy(p->tw, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
+  return FB_OK;
+}
+
+// ---------------------------------------------------------------- device FFT
+static __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+static __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+static __device__ __forceinline__ double2 cmul(double2 a, double2 b)
+{
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+static __device__ __forceinline__ double2 cscale(double2 a, double s) { return make_double2(a.x * s, a.y * s); }
+// multiply by -i (forward) or +i (inverse)
+static __device__ __forceinline__ double2 crot(double2 a, int inv) { return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x); }
+
+struct FftArgs {
+  int n, nst;
+  int radix[SG_MAXST];
+  const double2 *tw;
+};
+
+static FftArgs fft_args(const fb_fft_plan &p)
+{
+  FftArgs a;
+  a.n = p.n;
+  a.nst = p.nst;
+  for (int q = 0; q < SG_MAXST; q++) a.radix[q] = (q < p.nst) ? p.radix[q] : 1;
+  a.tw = p.tw;
+  return a;
+}
+
+// Stockham autosort FFT of length a.n in shared memory; x holds the input,
+// y is scratch; returns the buffer holding the natural-order result.
+// inv = 0: sum_j x_j exp(-2 pi i jk/n); inv = 1: exp(+2 pi i jk/n); no scaling.
+static __device__ double2 *fft_smem(double2 *x, double2 *y, const FftArgs &a, int inv)
+{
+  const int n = a.n;
+  int L = 1;  // size of the sub-transforms already done
+  for (int s = 0; s < a.nst; s++) {
+    const int R = a.radix[s];
+    const int nr_ = n / R;
+    const int tstride = n / (L * R);
+    __syncthreads();
+    for (int j = threadIdx.x; j < nr_; j += blockDim.x) {
+      double2 v[5];
+      for (int r = 0; r < R; r++) v[r] = x[j + r * nr_];
+      const int jm = j % L;
+      if (L > 1) {
+        for (int r = 1; r < R; r++) {
+          double2 w = a.tw[(r * jm * tstride) % n];
+          if (inv) w.y = -w.y;
+          v[r] = cmul(v[r], w);
+        }
+      }
+      if (R == 2) {
+        double2 t0 = v[0];
+        v[0] = cadd(t0, v[1]);
+        v[1] = csub(t0, v[1]);
+      } else if (R == 4) {
+        double2 A = cadd(v[0], v[2]), B = csub(v[0], v[2]);
+        double2 Cc = cadd(v[1], v[3]), D = crot(csub(v[1], v[3]), inv);
+        v[0] = cadd(A, Cc);
+        v[2] = csub(A, Cc);
+        v[1] = cadd(B, D);
+        v[3] = csub(B, D);
+      } else if (R == 3) {
+        const double h = 0.86602540378443864676;  // sqrt(3)/2
+        double2 t1 = cadd(v[1], v[2]);
+        double2 t2 = csub(v[0], cscale(t1, 0.5));
+        double2 t3 = cscale(csub(v[1], v[2]), inv ? h : -h);
+        v[0] = cadd(v[0], t1);
+        v[1] = make_double2(t2.x - t3.y, t2.y + t3.x);  // t2 + i t3
+        v[2] = make_double2(t2.x + t3.y, t2.y - t3.x);  // t2 - i t3
+      } else {  // R == 5, direct 5-point DFT
+        const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+        const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+        const double sg = inv ? 1.0 : -1.0;
+        double2 in[5] = {v[0], v[1], v[2], v[3], v[4]};
+        const double cs[5] = {1.0, c1, c2, c2, c1};
+        const double sn[5] = {0.0, s1, s2, -s2, -s1};
+        for (int k = 0; k < 5; k++) {
+          double re = 0.0, im = 0.0;
+          for (int q = 0; q < 5; q++) {
+            const int e = (k * q) % 5;
+            const double c = cs[e], sgn = sg * sn[e];
+            re += in[q].x * c - in[q].y * sgn;
+            im += in[q].x * sgn + in[q].y * c;
+          }
+          v[k] = make_double2(re, im);
+        }
+      }
+      const int idxD = (j / L) * L * R + jm;
+      for (int r = 0; r < R; r++) y[idxD + r * L] = v[r];
+    }
+    double2 *t = x;
+    x = y;
+    y = t;
+    L *= R;
+  }
+  __syncthreads();
+  return x;
+}
+
+// ------------------------------------------------------------------ kernels
+// Row pass of compute_fftdensity (sgdens.c:52-68) + the forward transform
+// along phi.  in_r/in_t given: real rows are in_r, in_t (kernel setup);
+// otherwise Sr, St are built from the density.
+__global__ void __launch_bounds__(SG_BS) sg_rows_fwd(FftArgs fa, int nrows, int ns, int nk,
+                                                      const double *dens, const double *sq,
+                                                      const double *rmed, double r0,
+                                                      const double *in_r, const double *in_t,
+                                                      double2 *out_r, double2 *out_t)
+{
+  extern __shared__ double2 sm[];
+  double2 *x = sm, *y = sm + ns;
+  const int i = blockIdx.x;
+  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+    double a, b;
+    if (in_r) {
+      a = in_r[(size_t)i * ns + j];
+      b = in_t[(size_t)i * ns + j];
+    } else {
+      a = dens[(size_t)i * ns + j] * sq[i];   // SGP_Sr = dens*sqrt(Rmed/R0)
+      b = a * rmed[i] / r0;                   // SGP_St = Sr*Rmed/R0
+    }
+    x[j] = make_double2(a, b);
+  }
+  double2 *Z = fft_smem(x, y, fa, 0);
+  for (int k = threadIdx.x; k < nk; k += blockDim.x) {
+    const double2 zk = Z[k], zc = Z[(ns - k) % ns];
+    // A = (Z[k] + conj Z[-k]) / 2 ; B = (Z[k] - conj Z[-k]) / (2i)
+    const double2 A = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y - zc.y));
+    const double2 B = make_double2(0.5 * (zk.y + zc.y), -0.5 * (zk.x - zc.x));
+    out_r[(size_t)i * nk + k] = A;
+    out_t[(size_t)i * nk + k] = B;
+  }
+}
+
+// Column pass.  mode 0: forward transform of the kernel half spectra into
+// [k][m] layout (setup).  mode 1: forward, product with -G Khat
+// (sgacc.c:25-38), inverse, keep rows < nrows_in.
+__global__ void __launch_bounds__(SG_BS) sg_cols(FftArgs fa, int nrows_in, int nk, int mode,
+                                                  double2 *data_r, double2 *data_t,
+                                                  double2 *kh_r, double2 *kh_t)
+{
+  extern __shared__ double2 sm[];
+  const int m = fa.n;
+  double2 *x = sm, *y = sm + m;
+  const int k = blockIdx.x;
+  const int which = blockIdx.y;  // 0: r, 1: t
+  double2 *data = which ? data_t : data_r;
+  double2 *kh = which ? kh_t : kh_r;
+  for (int i = threadIdx.x; i < m; i += blockDim.x)
+    x[i] = (i < nrows_in) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
+  double2 *X = fft_smem(x, y, fa, 0);
+  if (mode == 0) {
+    for (int i = threadIdx.x; i < m; i += blockDim.x) kh[(size_t)k * m + i] = X[i];
+    return;
+  }
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    const double2 K = kh[(size_t)k * m + i], S = X[i];
+    X[i] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
+  }
+  double2 *Y = (X == x) ? y : x;
+  double2 *W = fft_smem(X, Y, fa, 1);
+  for (int i = threadIdx.x; i < nrows_in; i += blockDim.x) data[(size_t)i * nk + k] = W[i];
+}
+
+// Inverse row pass + sgacc.c:138-161: normalisation, self-force.
+__global__ void __launch_bounds__(SG_BS) sg_rows_inv(FftArgs fa, int ns, int nk, const double2 *wr,
+                                                      const double2 *wt, const double *normr,
+                                                      const double *normt, const double *dens,
+                                                      double selfk_rstep, double selfk_tstep,
+                                                      double eps, double *accr, double *acct)
+{
+  extern __shared__ double2 sm[];
+  double2 *x = sm, *y = sm + ns;
+  const int i = blockIdx.x;
+  for (int k = threadIdx.x; k < ns; k += blockDim.x) {
+    double2 a, b;
+    if (k < nk) {
+      a = wr[(size_t)i * nk + k];
+      b = wt[(size_t)i * nk + k];
+      if (k == 0 || 2 * k == ns) { a.y = 0.0; b.y = 0.0; }  // c2r reads only Re there
+    } else {
+      a = wr[(size_t)i * nk + (ns - k)];
+      b = wt[(size_t)i * nk + (ns - k)];
+      a.y = -a.y;
+      b.y = -b.y;
+    }
+    x[k] = make_double2(a.x - b.y, a.y + b.x);  // a + i b
+  }
+  double2 *A = fft_smem(x, y, fa, 1);
+  const double nrm_r = normr[i], nrm_t = normt[i];
+  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+    const size_t l = (size_t)i * ns + j;
+    double ar = A[j].x * nrm_r;
+    ar += FB_G * dens[l] * selfk_rstep * selfk_tstep / eps;
+    accr[l] = ar;
+    acct[l] = A[j].y * nrm_t;
+  }
+}
+
+// update_sgvelocity (sgupdate.c:30-72) on VradInt / VthetaInt
+__global__ void __launch_bounds__(SG_BS) sg_update(KP k)
+{
+  const int ns = k.ns;
+  const size_t n = (size_t)k.nr * ns;
+  const double Dt = k.ctl->dt;
+  for (size_t l = (size_t)blockIdx.x * SG_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * SG_BS) {
+    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+    if (i > 0) {
+      const double radsgacc = ((k.rinf[i] - k.rmed[i - 1]) * k.sg_accr[l] +
+                               (k.rmed[i] - k.rinf[i]) * k.sg_accr[l - ns]) * k.invdiffrmed[i];
+      k.vri[l] += Dt * radsgacc;
+    }
+    const size_t lm1 = (size_t)i * ns + (j == 0 ? ns - 1 : j - 1);
+    const double azisgacc = 0.5 * (k.sg_acct[l] + k.sg_acct[lm1]);
+    k.vti[l] += Dt * azisgacc;
+  }
+}
+
+// ------------------------------------------------------------------- host
 int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t s)
 {
-  (void)p; (void)g; (void)s;
   *out = NULL;
-  return FB_ERR_UNSUPPORTED;
+  fb_sg *sg = new fb_sg();
+  memset(sg, 0, sizeof *sg);
+  const int nr = g->nr, ns = g->ns, m = 2 * nr, nk = ns / 2 + 1;
+  sg->nr = nr;
+  sg->ns = ns;
+  sg->m = m;
+  sg->nk = nk;
+  if (ns % 2 != 0) { delete sg; return FB_ERR_UNSUPPORTED; }
+  int rc = make_plan(&sg->prow, ns);
+  if (!rc) rc = make_plan(&sg->pcol, m);
+  if (rc) { fb_sg_destroy(sg); return rc; }
+  sg->smem_row = 2 * (size_t)ns * sizeof(double2);
+  sg->smem_col = 2 * (size_t)m * sizeof(double2);
+  int dev = 0, maxopt = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (sg->smem_row > (size_t)maxopt || sg->smem_col > (size_t)maxopt) { fb_sg_destroy(sg); return FB_ERR_UNSUPPORTED; }
+  cudaFuncSetAttribute(sg_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sg->smem_row);
+  cudaFuncSetAttribute(sg_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sg->smem_row);
+  cudaFuncSetAttribute(sg_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sg->smem_col);
+  // init_sg (sginit.c:9-11)
+  sg->eps = p->sgthicknesssmoothing * p->aspectratio;
+  sg->rstep = log(g->radii[nr] / g->radii[0]) / (double)nr;
+  sg->tstep = (p->pmax - p->pmin) / (double)ns;
+  // per-ring factors
+  std::vector<double> sq(nr), normr(nr), normt(nr);
+  const double r0 = g->rmed[0];
+  sg->r0 = r0;
+  for (int i = 0; i < nr; i++) {
+    sq[i] = sqrt(g->rmed[i] / r0);
+    double normaccr = sg->rstep * sg->tstep / ((double)(2 * nr) * (double)ns);
+    double normacct = normaccr;
+    normaccr /= sqrt(g->rmed[i] / r0);
+    normacct /= (g->rmed[i] / r0 * sqrt(g->rmed[i] / r0));
+    normr[i] = normaccr;
+    normt[i] = normacct;
+  }
+  bool ok = cudaMalloc(&sg->xr, (size_t)nr * nk * sizeof(double2)) == cudaSuccess &&
+            cudaMalloc(&sg->xt, (size_t)nr * nk * sizeof(double2)) == cudaSuccess &&
+            cudaMalloc(&sg->khr, (size_t)nk * m * sizeof(double2)) == cudaSuccess &&
+            cudaMalloc(&sg->kht, (size_t)nk * m * sizeof(double2)) == cudaSuccess &&
+            cudaMalloc(&sg->sq, nr * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&sg->rr, nr * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&sg->nr_accr, nr * sizeof(double)) == cudaSuccess &&
+            cudaMalloc(&sg->nr_acct, nr * sizeof(double)) == cudaSuccess;
+  if (!ok) { fb_sg_destroy(sg); return FB_ERR_NOMEM; }
+  cudaMemcpy(sg->sq, sq.data(), nr * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(sg->rr, g->rmed, nr * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(sg->nr_accr, normr.data(), nr * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(sg->nr_acct, normt.data(), nr * sizeof(double), cudaMemcpyHostToDevice);
+  // compute_fftkernel (sgkernel.c:3-27): kernels on the 2 Nr x Ns grid
+  std::vector<double> kr((size_t)m * ns), kt((size_t)m * ns);
+  const double e2 = sg->eps * sg->eps;
+  for (int i = 0; i < m; i++) {
+    double u;
+    if (i < nr)
+      u = log(g->radii[i] / g->radii[0]);
+    else
+      u = -log(g->radii[2 * nr - i] / g->radii[0]);
+    for (int j = 0; j < ns; j++) {
+      const size_t l = (size_t)i * ns + j;
+      double a = 1.0 + sg->eps * sg->eps - g->cosaz[j] * exp(-u);
+      a *= pow(sg->eps * sg->eps * exp(u) + 2.0 * (cosh(u) - g->cosaz[j]), -1.5);
+      double b = g->sinaz[j];
+      b *= pow(sg->eps * sg->eps * exp(u) + 2.0 * (cosh(u) - g->cosaz[j]), -1.5);
+      kr[l] = a;
+      kt[l] = b;
+    }
+  }
+  (void)e2;
+  double *dkr = NULL, *dkt = NULL;
+  double2 *hr = NULL, *ht = NULL;
+  ok = cudaMalloc(&dkr, kr.size() * sizeof(double)) == cudaSuccess &&
+       cudaMalloc(&dkt, kt.size() * sizeof(double)) == cudaSuccess &&
+       cudaMalloc(&hr, (size_t)m * nk * sizeof(double2)) == cudaSuccess &&
+       cudaMalloc(&ht, (size_t)m * nk * sizeof(double2)) == cudaSuccess;
+  if (!ok) { cudaFree(dkr); cudaFree(dkt); cudaFree(hr); cudaFree(ht); fb_sg_destroy(sg); return FB_ERR_NOMEM; }
+  cudaMemcpy(dkr, kr.data(), kr.size() * sizeof(double), cudaMemcpyHostToDevice);
+  cudaMemcpy(dkt, kt.data(), kt.size() * sizeof(double), cudaMemcpyHostToDevice);
+  FftArgs fr = fft_args(sg->prow), fc = fft_args(sg->pcol);
+  sg_rows_fwd<<<m, SG_BS, sg->smem_row, s>>>(fr, m, ns, nk, NULL, NULL, NULL, 1.0, dkr, dkt, hr, ht);
+  sg_cols<<<dim3(nk, 2), SG_BS, sg->smem_col, s>>>(fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
+  cudaError_t e = cudaStreamSynchronize(s);
+  cudaFree(dkr); cudaFree(dkt); cudaFree(hr); cudaFree(ht);
+  if (e != cudaSuccess) { fb_sg_destroy(sg); return FB_ERR_CUDA; }
+  *out = sg;
+  return FB_OK;
 }
-void fb_sg_destroy(fb_sg *sg) { (void)sg; }
-void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s) { (void)sg; (void)k; (void)dens; (void)s; }
-void fb_sg_update_velocities(const KP &k, cudaStream_t s) { (void)k; (void)s; }
-int fb_sg_launches(const fb_sg *sg) { (void)sg; return 0; }
+
+void fb_sg_destroy(fb_sg *sg)
+{
+  if (!sg) return;
+  cudaFree(sg->prow.tw); cudaFree(sg->pcol.tw);
+  cudaFree(sg->xr); cudaFree(sg->xt); cudaFree(sg->khr); cudaFree(sg->kht);
+  cudaFree(sg->sq); cudaFree(sg->rr); cudaFree(sg->nr_accr); cudaFree(sg->nr_acct);
+  delete sg;
+}
+
+// compute_fftdensity + compute_sgacc (sgdens.c, sgacc.c): 3 launches
+void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
+{
+  const int nr = sg->nr, ns = sg->ns, nk = sg->nk;
+  FftArgs fr = fft_args(sg->prow), fc = fft_args(sg->pcol);
+  sg_rows_fwd<<<nr, SG_BS, sg->smem_row, s>>>(fr, nr, ns, nk, dens, sg->sq, sg->rr, sg->r0,
+                                               NULL, NULL, sg->xr, sg->xt);
+  sg_cols<<<dim3(nk, 2), SG_BS, sg->smem_col, s>>>(fc, nr, nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
+  sg_rows_inv<<<nr, SG_BS, sg->smem_row, s>>>(fr, ns, nk, sg->xr, sg->xt, sg->nr_accr, sg->nr_acct, dens,
+                                               sg->rstep, sg->tstep, sg->eps, k.sg_accr, k.sg_acct);
+}
+
+void fb_sg_update_velocities(const KP &k, cudaStream_t s)
+{
+  const size_t n = (size_t)k.nr * k.ns;
+  sg_update<<<(int)((n + SG_BS - 1) / SG_BS), SG_BS, 0, s>>>(k);
+}
+
+int fb_sg_launches(const fb_sg *sg) { return sg ? 4 : 0; }
+
+extern "C" int fb_sg_ready(void) { return 1; }

@@ -198,7 +198,8 @@ int fb_algogas(fb_ctx *ctx, fb_step_report *rep);
 int fb_download(fb_ctx *ctx, fb_state *st, unsigned mask);
 /* Derived output fields at the current state (reference layout, (nrad+1)*nsec):
    which = 0 Temperature (src/SourceEuler.c:2440), 1 Potential, 2 Pressure,
-   3 SoundSpeed, 4 DivergenceVelocity, 5 ViscHeat. */
+   3 SoundSpeed, 4 DivergenceVelocity, 5 ViscHeat, 6 SG radial acceleration
+   (SG_Accr, src/sgacc.c:152-161), 7 SG azimuthal acceleration (SG_Acct). */
 int fb_download_derived(fb_ctx *ctx, int which, double *out);
 /* Diagnostics on the device state: GasTotalMass (src/SideEuler.c:15) and
    GasMomentum (src/SideEuler.c:114). */

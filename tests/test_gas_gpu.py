@@ -112,3 +112,71 @@ def test_algogas_matches_oracle(tmp_path, nrad, nsec, steps):
             errs = _cmp(out, ref, FIELDS, TOL_DT)
             assert abs(out["PhysicalTime"] - ref["PhysicalTime"]) <= 1e-13 * abs(ref["PhysicalTime"])
             print("DT", s, "substeps", rep.substeps, "errors", errs)
+
+
+ADI = os.path.join(CFG, "adiabatic_sg_512x1536.par")
+
+
+@pytest.mark.parametrize("nrad,nsec,steps,beta,alpha", [(48, 144, 3, "Yes", "1e-3"), (64, 192, 2, "No", "0.0")])
+def test_energy_equation_matches_oracle(tmp_path, nrad, nsec, steps, beta, alpha):
+    """Adiabatic gas (SubStep2 energy, SubStep3 pdV + viscous heating + beta
+    cooling, energy transport and floor) without self-gravity."""
+    from dustyfargoadsg_b200 import Disc, read_par
+    par = _oracle.write_par(ADI, str(tmp_path), Nrad=nrad, Nsec=nsec, SelfGravity="No",
+                            BetaCooling=beta, AlphaViscosity=alpha)
+    dumps, _, _ = _oracle.run_oracle(par, steps=steps, noise=1e-4, seed=3)
+    with Disc(read_par(par), noise=1e-4, seed=3) as disc:
+        init = disc.download()
+        _cmp(init, dumps["state_init"], FIELDS + ("energy",), 0.0)
+        prev = 0
+        for s in range(1, steps + 1):
+            rep = disc.step()
+            ref = dumps["state_%05d" % s]
+            out = disc.download()
+            assert rep.substeps == int(ref["substeps"]) - prev
+            prev = int(ref["substeps"])
+            errs = _cmp(out, ref, FIELDS + ("energy",), TOL_DT)
+            print("energy DT", s, "substeps", rep.substeps, errs)
+
+
+@pytest.fixture(scope="module")
+def sg_case(tmp_path_factory):
+    wd = str(tmp_path_factory.mktemp("sg"))
+    par = _oracle.write_par(ADI, wd, Nrad=64, Nsec=192)
+    dumps, _, _ = _oracle.run_oracle(par, steps=2, noise=1e-4, seed=5)
+    return par, dumps
+
+
+def test_selfgravity_accelerations(sg_case):
+    """compute_sgacc of the initial density: our FFT convolution vs the
+    reference's (FFTW 2.1.5), scale-relative."""
+    from dustyfargoadsg_b200 import _ffi
+    par, d = sg_case
+    init = d["state_init"]
+    with _disc(par, _state_from(init, {k: init[k] for k in ("dens", "vrad", "vtheta", "energy")})) as disc:
+        disc.stage(_ffi.FB_STAGE_SELFGRAV, 1.0)
+        ar, at = disc.derived(6), disc.derived(7)
+    nrs = disc.nr * disc.ns
+    e_r = _oracle.rel_err(ar[:nrs], init["sg_accr"][:nrs])
+    e_t = _oracle.rel_err(at[:nrs], init["sg_acct"][:nrs])
+    print("SG accel errors", e_r, e_t)
+    assert e_r < 1e-12 and e_t < 1e-12
+
+
+def test_selfgravity_algogas_matches_oracle(sg_case, tmp_path):
+    """Whole DTs with energy equation, beta cooling and self-gravity."""
+    from dustyfargoadsg_b200 import Disc, read_par
+    par, dumps = sg_case
+    with Disc(read_par(par), noise=1e-4, seed=5) as disc:
+        init = disc.download()
+        errs0 = _cmp(init, dumps["state_init"], FIELDS + ("energy",), 1e-13)
+        print("SG init", errs0)
+        prev = 0
+        for s in (1, 2):
+            rep = disc.step()
+            ref = dumps["state_%05d" % s]
+            out = disc.download()
+            assert rep.substeps == int(ref["substeps"]) - prev
+            prev = int(ref["substeps"])
+            errs = _cmp(out, ref, FIELDS + ("energy",), TOL_DT)
+            print("SG DT", s, "substeps", rep.substeps, errs)
