@@ -10,11 +10,13 @@
 #include "fb_dev.cuh"
 
 enum {
-  ST_CFL, ST_FORCE, ST_CONTROL, ST_SOUND, ST_POT, ST_SUB1, ST_SG, ST_VTERMS, ST_VUPDATE,
+  ST_CFL, ST_FORCE, ST_CONTROL, ST_SOUND, ST_POT, ST_SUB1, ST_SG, ST_SGCOLS, ST_SGINV, ST_SGUPD,
+  ST_VTERMS, ST_VUPDATE,
   ST_SUB2, ST_EVTERMS, ST_SUB3, ST_TRAD, ST_TAZI, ST_TVR, ST_DAMP, FB_NSTAGE
 };
 static const char *stage_names[FB_NSTAGE] = {
-  "cfl", "force_sums", "controller", "soundspeed", "potential", "substep1", "selfgravity",
+  "cfl", "force_sums", "controller", "soundspeed", "potential", "substep1", "sg_rows_fwd",
+  "sg_cols", "sg_rows_inv", "sg_update",
   "viscous_terms", "viscous_update", "substep2", "energy_viscous_terms", "substep3",
   "transport_radial", "transport_azimuthal", "transport_vr_boundary", "damping"};
 
@@ -43,6 +45,12 @@ struct fb_ctx {
   std::vector<int> pseq;          // stage id of each recorded interval
   double pms[FB_NSTAGE];
   long long pcount[FB_NSTAGE];
+  // one DT as a CUDA graph: a conditional WHILE node around the substep
+  cudaGraph_t gdt;
+  cudaGraphExec_t gdt_exec;
+  int graph_state;            // 0 not built, 1 ready, -1 unavailable
+  long long launches_per_substep;
+  int substep_cap;
 };
 
 static void set_err(fb_ctx *c, const char *fmt, ...)
@@ -284,6 +292,12 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.masstaper = p->masstaper;
   k.self_gravity = p->self_gravity;
   k.transport_only = 0;
+  ctx->substep_cap = 1000000;
+  {
+    const char *cap = getenv("FB_MAX_SUBSTEPS");
+    if (cap && atoi(cap) > 0) ctx->substep_cap = atoi(cap);
+  }
+  if (getenv("FB_NO_GRAPH")) ctx->graph_state = -1;
   if (p->self_gravity) {
     rc = fb_sg_create(&ctx->sg, p, &ctx->g, ctx->st);
     if (rc) { set_err(ctx, "self-gravity setup failed (%d)", rc); fb_destroy(ctx); return rc; }
@@ -305,6 +319,8 @@ extern "C" int fb_destroy(fb_ctx *ctx)
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
+  if (ctx->gdt_exec) cudaGraphExecDestroy(ctx->gdt_exec);
+  if (ctx->gdt) cudaGraphDestroy(ctx->gdt);
   if (ctx->st) cudaStreamDestroy(ctx->st);
   fb_geom_free(&ctx->g);
   delete ctx;
@@ -414,9 +430,10 @@ static int enqueue_substep(fb_ctx *ctx)
   STAGE(ST_POT, 1, fb_launch_potential(k, s));
   STAGE(ST_SUB1, 1, fb_launch_substep1(k, s));
   if (k.self_gravity) {
-    STAGE(ST_SG, 0, (fb_sg_accel(ctx->sg, k, k.rho, s), fb_sg_update_velocities(k, s)));
-    ctx->launches += fb_sg_launches(ctx->sg);
-    ctx->pcount[ST_SG] += fb_sg_launches(ctx->sg);
+    STAGE(ST_SG, 1, fb_sg_rows_fwd(ctx->sg, k, k.rho, s));
+    STAGE(ST_SGCOLS, 1, fb_sg_cols(ctx->sg, s));
+    STAGE(ST_SGINV, 1, fb_sg_rows_inv(ctx->sg, k, k.rho, s));
+    STAGE(ST_SGUPD, 1, fb_sg_update_velocities(k, s));
   }
   if (k.visc_mode) {
     STAGE(ST_VTERMS, 1, fb_launch_viscous_terms(k, k.vri, k.vti, s));
@@ -440,6 +457,56 @@ static int enqueue_substep(fb_ctx *ctx)
     npt++;
   }
   return npt;
+}
+
+// Captures one DT as a graph: WHILE(cond) { substep; cond = !done }.  The
+// kernels read dt and the planets from the device control block, so one
+// capture serves every substep and every DT.
+static int build_dt_graph(fb_ctx *ctx)
+{
+  cudaGraph_t g = NULL, body = NULL;
+  cudaGraphConditionalHandle h;
+  cudaGraphNode_t node;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return FB_ERR_CUDA;
+  if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return FB_ERR_CUDA;
+  }
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  if (cudaGraphAddNode(&node, g, NULL, 0, &cp) != cudaSuccess) {
+    cudaGraphDestroy(g);
+    return FB_ERR_CUDA;
+  }
+  body = cp.conditional.phGraph_out[0];
+  const long long l0 = ctx->launches;
+  const int prof = ctx->profiling;
+  ctx->profiling = 0;
+  cudaError_t e = cudaStreamBeginCaptureToGraph(ctx->st, body, NULL, NULL, 0, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    enqueue_substep(ctx);
+    fb_launch_loop_cond(ctx->k, h, ctx->substep_cap, ctx->st);
+    e = cudaStreamEndCapture(ctx->st, &body);
+  }
+  ctx->profiling = prof;
+  ctx->launches_per_substep = ctx->launches - l0 + 1;
+  ctx->launches = l0;
+  for (int q = 0; q < FB_NSTAGE; q++) ctx->pcount[q] = 0;
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return FB_ERR_CUDA;
+  }
+  if (cudaGraphInstantiate(&ctx->gdt_exec, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    return FB_ERR_CUDA;
+  }
+  ctx->gdt = g;
+  return FB_OK;
 }
 
 static void profile_collect(fb_ctx *ctx, int npt)
@@ -487,8 +554,15 @@ extern "C" int fb_algogas(fb_ctx *ctx, fb_step_report *rep)
   ctx->launches += 1;
   if (k.energy) { fb_launch_soundspeed(k, 0, s); ctx->launches += 1; }  // SourceEuler.c:344-350
   int status = FB_OK;
-  const int cap = 1000000;
-  for (int it = 0; it < cap; it++) {
+  const int cap = ctx->substep_cap;
+  if (!ctx->profiling && ctx->graph_state == 0) ctx->graph_state = (build_dt_graph(ctx) == FB_OK) ? 1 : -1;
+  if (!ctx->profiling && ctx->graph_state == 1) {
+    CK(cudaGraphLaunch(ctx->gdt_exec, s));
+    CK(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(fb_ctl), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    status = ctx->h_ctl->status;
+    ctx->launches += ctx->launches_per_substep * (long long)ctx->h_ctl->substeps;
+  } else for (int it = 0; it < cap; it++) {
     int npt = enqueue_substep(ctx);
     CK(cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(fb_ctl), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));

@@ -106,6 +106,7 @@ void fb_launch_derived(const KP &k, int which, double *out, cudaStream_t s);
 void fb_launch_boundary_only(const KP &k, cudaStream_t s);
 int  fb_gas_prepare(int ns, int energy);  // kernel attributes (shared memory)
 void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s);
+void fb_launch_loop_cond(const KP &k, cudaGraphConditionalHandle h, int cap, cudaStream_t s);
 // self-gravity (fb_sg.cu)
 struct fb_sg;
 int  fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t s);
@@ -113,3 +114,6 @@ void fb_sg_destroy(fb_sg *sg);
 void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
 void fb_sg_update_velocities(const KP &k, cudaStream_t s);
 int  fb_sg_launches(const fb_sg *sg);  // kernels per fb_sg_accel + update
+void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
+void fb_sg_cols(fb_sg *sg, cudaStream_t s);
+void fb_sg_rows_inv(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);

@@ -851,28 +851,50 @@ __global__ void __launch_bounds__(128) k_transport_radial(KP k, double dtov, int
   }
 }
 
+// Sum over the block for any blockDim that is a multiple of 32.
+static __device__ double block_sum_dyn(double v, double *sh)
+{
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (lane < nw) ? sh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0) sh[0] = v;
+  }
+  __syncthreads();
+  double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+static __device__ __forceinline__ int wrapj(int j, int ns) { return j < 0 ? j + ns : (j >= ns ? j - ns : j); }
+
 // Azimuthal pass (OneWindTheta, TransportEuler.c:226-247): ring mean,
 // residual and integer FARGO shift (:249-373), van Leer on the residual and
 // on the uniform part (:375-465), the shift itself, then ComputeVelocities'
 // vtheta (:515-547), the energy floor (SourceEuler.c:2524) and the
-// sub-Keplerian edge rings (SideEuler.c:1008-1044).  One CTA per ring with
-// the whole ring of every quantity in shared memory, so the periodic
-// azimuthal stencil needs no halo exchange.
-template <int NQ>
-__global__ void __launch_bounds__(256) k_transport_azimuthal(KP k, double dtov)
+// sub-Keplerian edge rings (SideEuler.c:1008-1044).
+//
+// One CTA per ring holds the ring of every transported quantity in shared
+// memory (the periodic azimuthal stencil needs no halo exchange).  Each
+// thread owns E consecutive azimuths and evaluates the whole van Leer
+// chain of a quantity for them in registers (ratios, slopes, interface
+// values, flux difference), reading its +-2 neighbours from shared memory;
+// one barrier per quantity separates the reads from the in-place writes.
+template <int NQ, int E>
+__global__ void __launch_bounds__(512) k_transport_azimuthal(KP k, double dtov)
 {
-  const double dt = dt_of(k, dtov);
   extern __shared__ double smem[];
   __shared__ double sh[32];
+  const double dt = dt_of(k, dtov);
   const int i = blockIdx.x, ns = k.ns, nr = k.nr;
   const size_t base = (size_t)i * ns;
-  double *Q = smem;                 // NQ*ns
-  double *vres = Q + NQ * ns;       // ns
-  double *rhos = vres + ns;         // ns
-  double *rhoi = rhos + ns;         // ns
-  double *work = rhoi + ns;         // ns
-  double *dq = work + ns;           // ns
-  double *qrs = dq + ns;            // ns
+  double *Q = smem;             // NQ rings
+  double *vres = Q + NQ * ns;   // residual azimuthal velocity
+  const int a = threadIdx.x * E;
   for (int j = threadIdx.x; j < ns; j += blockDim.x)
     for (int q = 0; q < NQ; q++) Q[q * ns + j] = k.q[q][base + j];
   // ComputeThetaElongations / ComputeAverageThetaVelocities / ComputeResiduals
@@ -882,22 +904,21 @@ __global__ void __launch_bounds__(256) k_transport_azimuthal(KP k, double dtov)
     double elong = k.vt[base + j] * dt;
     s += elong * invdt;
   }
-  s = block_sum<256>(s, sh);
+  s = block_sum_dyn(s, sh);
   const double VMed = s / (double)ns;
-  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-    double elong = k.vt[base + j] * dt;
-    vres[j] = elong * invdt - VMed;
-  }
   // ComputeConstantResidual (TransportEuler.c:310-348)
   const double dpinvns = (k.pmax - k.pmin) / (double)ns;
   const double Ntilde = VMed * k.invrmed[i] * dt * (double)ns / (k.pmax - k.pmin);
   const double Nround = floor(Ntilde + 0.5);
   const long nshift = (long)Nround;
   double vconst = (Ntilde - Nround) * k.rmed[i] * invdt * dpinvns;
-  if (!k.fast_transport) {
-    for (int j = threadIdx.x; j < ns; j += blockDim.x) vres[j] = vconst + vres[j];
-    vconst = 0.0;
+  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+    double elong = k.vt[base + j] * dt;
+    double v = elong * invdt - VMed;
+    if (!k.fast_transport) v = vconst + v;
+    vres[j] = v;
   }
+  if (!k.fast_transport) vconst = 0.0;
   __syncthreads();
   const double dxtheta = k.dxtheta[i], invdxtheta = k.invdxtheta[i];
   const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
@@ -906,63 +927,71 @@ __global__ void __launch_bounds__(256) k_transport_azimuthal(KP k, double dtov)
   for (int pass = 0; pass < 2; pass++) {
     const bool uniform = (pass == 1);
     if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
-    // ComputeStarTheta(Rho, V, RhoStar) and RhoInt = Rho
-    for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-      const int jm = (j == 0) ? ns - 1 : j - 1, jp = (j == ns - 1) ? 0 : j + 1;
-      double dqm = (rho[j] - rho[jm]);
-      double dqp = (rho[jp] - rho[j]);
-      dq[j] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
-      rhoi[j] = rho[j];
+    // RhoStar (ComputeStarTheta(Rho, V, RhoStar)) for j = a .. a+E; RhoInt is
+    // the density before this pass, i.e. Q[rho] until the last quantity.
+    double R_[E + 4], DR[E + 2], RS[E + 1], V[E + 1];
+#pragma unroll
+    for (int t = 0; t < E + 4; t++) R_[t] = (a < ns) ? rho[wrapj(a - 2 + t, ns)] : 0.0;
+#pragma unroll
+    for (int t = 0; t < E + 2; t++) {
+      double dqm = (R_[t + 1] - R_[t]);
+      double dqp = (R_[t + 2] - R_[t + 1]);
+      DR[t] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
     }
-    __syncthreads();
-    for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-      const int jm = (j == 0) ? ns - 1 : j - 1;
-      const double v = uniform ? vconst : vres[j];
+#pragma unroll
+    for (int t = 0; t < E + 1; t++) {
+      const double v = uniform ? vconst : ((a < ns) ? vres[wrapj(a + t, ns)] : 0.0);
+      V[t] = v;
       const double ksi = v * dt;
-      rhos[j] = (ksi > 0.0) ? rho[jm] + (dxtheta - ksi) * dq[jm] : rho[j] - (dxtheta + ksi) * dq[j];
+      RS[t] = (ksi > 0.0) ? R_[t + 1] + (dxtheta - ksi) * DR[t] : R_[t + 2] - (dxtheta + ksi) * DR[t + 1];
     }
-    __syncthreads();
     for (int q = 0; q < NQ; q++) {
       double *qb = Q + q * ns;
-      for (int j = threadIdx.x; j < ns; j += blockDim.x) work[j] = qb[j] / (rhoi[j] + 1e-20);
-      __syncthreads();
-      for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-        const int jm = (j == 0) ? ns - 1 : j - 1, jp = (j == ns - 1) ? 0 : j + 1;
-        double dqm = (work[j] - work[jm]);
-        double dqp = (work[jp] - work[j]);
-        dq[j] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+      double W[E + 4], q0[E];
+#pragma unroll
+      for (int t = 0; t < E + 4; t++) W[t] = (a < ns) ? qb[wrapj(a - 2 + t, ns)] / (R_[t] + 1e-20) : 0.0;
+#pragma unroll
+      for (int t = 0; t < E; t++) q0[t] = (a + t < ns) ? qb[a + t] : 0.0;
+      __syncthreads();  // every read of this quantity precedes its updates
+      double DQ[E + 2], QS[E + 1];
+#pragma unroll
+      for (int t = 0; t < E + 2; t++) {
+        double dqm = (W[t + 1] - W[t]);
+        double dqp = (W[t + 2] - W[t + 1]);
+        DQ[t] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
       }
-      __syncthreads();
-      for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-        const int jm = (j == 0) ? ns - 1 : j - 1;
-        const double v = uniform ? vconst : vres[j];
-        const double ksi = v * dt;
-        qrs[j] = (ksi > 0.0) ? work[jm] + (dxtheta - ksi) * dq[jm] : work[j] - (dxtheta + ksi) * dq[j];
+#pragma unroll
+      for (int t = 0; t < E + 1; t++) {
+        const double ksi = V[t] * dt;
+        QS[t] = (ksi > 0.0) ? W[t + 1] + (dxtheta - ksi) * DQ[t] : W[t + 2] - (dxtheta + ksi) * DQ[t + 1];
       }
-      __syncthreads();
-      for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-        const int jp = (j == ns - 1) ? 0 : j + 1;
-        const double v = uniform ? vconst : vres[j];
-        const double vp = uniform ? vconst : vres[jp];
-        double varq = dxrad * qrs[j] * rhos[j] * v;
-        varq -= dxrad * qrs[jp] * rhos[jp] * vp;
-        qb[j] += varq * invsurf;
+#pragma unroll
+      for (int t = 0; t < E; t++) {
+        if (a + t < ns) {
+          double varq = dxrad * QS[t] * RS[t] * V[t];
+          varq -= dxrad * QS[t + 1] * RS[t + 1] * V[t + 1];
+          qb[a + t] = q0[t] + varq * invsurf;
+        }
       }
-      __syncthreads();
     }
+    __syncthreads();
   }
   // AdvectSHIFT (TransportEuler.c:350-373) for every quantity
   for (int q = 0; q < NQ; q++) {
     double *qb = Q + q * ns;
-    for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-      long ji = ((long)j - nshift) % ns;
+    double tmp[E];
+#pragma unroll
+    for (int t = 0; t < E; t++) {
+      long ji = ((long)(a + t) - nshift) % ns;
       if (ji < 0) ji += ns;
-      work[j] = qb[ji];
+      tmp[t] = (a + t < ns) ? qb[ji] : 0.0;
     }
     __syncthreads();
-    for (int j = threadIdx.x; j < ns; j += blockDim.x) qb[j] = work[j];
-    __syncthreads();
+#pragma unroll
+    for (int t = 0; t < E; t++)
+      if (a + t < ns) qb[a + t] = tmp[t];
   }
+  __syncthreads();
   // ComputeVelocities, vtheta part; floors on energy; sub-Keplerian edges
   const double *tp = Q + 2 * ns, *tm = Q + 3 * ns;
   const int subkep = (!k.transport_only) && (i == 0 || i == nr - 1);
@@ -984,6 +1013,8 @@ __global__ void __launch_bounds__(256) k_transport_azimuthal(KP k, double dtov)
     }
   }
 }
+
+#define FB_AZI_E 6
 
 // ComputeVelocities' radial part (TransportEuler.c:531-536) needs the
 // neighbouring ring after both passes; fused with AddFloorDensity
@@ -1043,14 +1074,17 @@ void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
     k_transport_radial<5><<<gr, tx, 0, s>>>(k, dt_override, chunk);
 }
 
+static int azi_threads(int ns) { return (((ns + FB_AZI_E - 1) / FB_AZI_E) + 31) / 32 * 32; }
+
 void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s)
 {
   const int NQ = k.energy ? 6 : 5;
-  const size_t smem = (size_t)(NQ + 6) * k.ns * sizeof(double);
+  const size_t smem = (size_t)(NQ + 1) * k.ns * sizeof(double);
+  const int th = azi_threads(k.ns);
   if (k.energy)
-    k_transport_azimuthal<6><<<k.nr, 256, smem, s>>>(k, dt_override);
+    k_transport_azimuthal<6, FB_AZI_E><<<k.nr, th, smem, s>>>(k, dt_override);
   else
-    k_transport_azimuthal<5><<<k.nr, 256, smem, s>>>(k, dt_override);
+    k_transport_azimuthal<5, FB_AZI_E><<<k.nr, th, smem, s>>>(k, dt_override);
 }
 
 void fb_launch_transport_vr(const KP &k, cudaStream_t s)
@@ -1223,12 +1257,32 @@ void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s) { k_begin_dt<<<1
 int fb_gas_prepare(int ns, int energy)
 {
   const int NQ = energy ? 6 : 5;
-  const size_t smem = (size_t)(NQ + 6) * ns * sizeof(double);
+  const size_t smem = (size_t)(NQ + 1) * ns * sizeof(double);
   int dev = 0, maxopt = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem + 32 * sizeof(double) > (size_t)maxopt) return FB_ERR_UNSUPPORTED;
-  cudaError_t e1 = cudaFuncSetAttribute(k_transport_azimuthal<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaError_t e2 = cudaFuncSetAttribute(k_transport_azimuthal<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (azi_threads(ns) > 512 || ns < 16) return FB_ERR_UNSUPPORTED;
+  cudaError_t e1 = cudaFuncSetAttribute(k_transport_azimuthal<5, FB_AZI_E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e2 = cudaFuncSetAttribute(k_transport_azimuthal<6, FB_AZI_E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   return (e1 == cudaSuccess && e2 == cudaSuccess) ? FB_OK : FB_ERR_CUDA;
+}
+
+// Loop condition of the captured substep graph: keep going while the
+// controller has not reached DT (SourceEuler.c:398) and nothing failed; the
+// cap bounds the loop even if the time step collapses.
+__global__ void k_loop_cond(KP k, cudaGraphConditionalHandle h, int cap)
+{
+  fb_ctl *c = k.ctl;
+  int go = (!c->done && !c->status) ? 1 : 0;
+  if (go && c->substeps >= cap) {
+    c->status = FB_ERR_SUBSTEPS;
+    go = 0;
+  }
+  cudaGraphSetConditional(h, go);
+}
+
+void fb_launch_loop_cond(const KP &k, cudaGraphConditionalHandle h, int cap, cudaStream_t s)
+{
+  k_loop_cond<<<1, 1, 0, s>>>(k, h, cap);
 }

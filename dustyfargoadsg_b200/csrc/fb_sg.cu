@@ -98,68 +98,89 @@ static FftArgs fft_args(const fb_fft_plan &p)
   return a;
 }
 
+// One radix-R pass of a Stockham autosort FFT (all of v[] in registers).
+template <int R, int INV>
+static __device__ __forceinline__ void fft_pass(const double2 *__restrict__ x, double2 *__restrict__ y,
+                                                int n, int L, const double2 *__restrict__ tw)
+{
+  const int nr_ = n / R;
+  const int tstride = n / (L * R);
+  for (int j = threadIdx.x; j < nr_; j += blockDim.x) {
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = x[j + r * nr_];
+    const int jm = j % L;
+    if (L > 1) {
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        double2 w = tw[r * jm * tstride];  // r*jm*tstride < n
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    if (R == 2) {
+      double2 t0 = v[0];
+      v[0] = cadd(t0, v[1]);
+      v[1] = csub(t0, v[1]);
+    } else if (R == 4) {
+      double2 A = cadd(v[0], v[2]), B = csub(v[0], v[2]);
+      double2 Cc = cadd(v[1], v[3]), D = crot(csub(v[1], v[3]), INV);
+      v[0] = cadd(A, Cc);
+      v[2] = csub(A, Cc);
+      v[1] = cadd(B, D);
+      v[3] = csub(B, D);
+    } else if (R == 3) {
+      const double h = 0.86602540378443864676;  // sqrt(3)/2
+      double2 t1 = cadd(v[1], v[2]);
+      double2 t2 = csub(v[0], cscale(t1, 0.5));
+      double2 t3 = cscale(csub(v[1], v[2]), INV ? h : -h);
+      v[0] = cadd(v[0], t1);
+      v[1] = make_double2(t2.x - t3.y, t2.y + t3.x);  // t2 + i t3
+      v[2] = make_double2(t2.x + t3.y, t2.y - t3.x);  // t2 - i t3
+    } else if (R == 5) {  // direct 5-point DFT
+      const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+      const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+      const double sg = INV ? 1.0 : -1.0;
+      const double cs[5] = {1.0, c1, c2, c2, c1};
+      const double sn[5] = {0.0, s1, s2, -s2, -s1};
+      double2 in[5];
+#pragma unroll
+      for (int q = 0; q < 5; q++) in[q] = v[q];
+#pragma unroll
+      for (int k = 0; k < 5; k++) {
+        double re = 0.0, im = 0.0;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+          const int e = (k * q) % 5;
+          const double c = cs[e], sgn = sg * sn[e];
+          re += in[q].x * c - in[q].y * sgn;
+          im += in[q].x * sgn + in[q].y * c;
+        }
+        v[k] = make_double2(re, im);
+      }
+    }
+    const int idxD = (j - jm) * R + jm;
+#pragma unroll
+    for (int r = 0; r < R; r++) y[idxD + r * L] = v[r];
+  }
+}
+
 // Stockham autosort FFT of length a.n in shared memory; x holds the input,
 // y is scratch; returns the buffer holding the natural-order result.
 // inv = 0: sum_j x_j exp(-2 pi i jk/n); inv = 1: exp(+2 pi i jk/n); no scaling.
-static __device__ double2 *fft_smem(double2 *x, double2 *y, const FftArgs &a, int inv)
+template <int INV>
+static __device__ double2 *fft_smem_t(double2 *x, double2 *y, const FftArgs &a)
 {
   const int n = a.n;
-  int L = 1;  // size of the sub-transforms already done
+  int L = 1;
   for (int s = 0; s < a.nst; s++) {
     const int R = a.radix[s];
-    const int nr_ = n / R;
-    const int tstride = n / (L * R);
     __syncthreads();
-    for (int j = threadIdx.x; j < nr_; j += blockDim.x) {
-      double2 v[5];
-      for (int r = 0; r < R; r++) v[r] = x[j + r * nr_];
-      const int jm = j % L;
-      if (L > 1) {
-        for (int r = 1; r < R; r++) {
-          double2 w = a.tw[(r * jm * tstride) % n];
-          if (inv) w.y = -w.y;
-          v[r] = cmul(v[r], w);
-        }
-      }
-      if (R == 2) {
-        double2 t0 = v[0];
-        v[0] = cadd(t0, v[1]);
-        v[1] = csub(t0, v[1]);
-      } else if (R == 4) {
-        double2 A = cadd(v[0], v[2]), B = csub(v[0], v[2]);
-        double2 Cc = cadd(v[1], v[3]), D = crot(csub(v[1], v[3]), inv);
-        v[0] = cadd(A, Cc);
-        v[2] = csub(A, Cc);
-        v[1] = cadd(B, D);
-        v[3] = csub(B, D);
-      } else if (R == 3) {
-        const double h = 0.86602540378443864676;  // sqrt(3)/2
-        double2 t1 = cadd(v[1], v[2]);
-        double2 t2 = csub(v[0], cscale(t1, 0.5));
-        double2 t3 = cscale(csub(v[1], v[2]), inv ? h : -h);
-        v[0] = cadd(v[0], t1);
-        v[1] = make_double2(t2.x - t3.y, t2.y + t3.x);  // t2 + i t3
-        v[2] = make_double2(t2.x + t3.y, t2.y - t3.x);  // t2 - i t3
-      } else {  // R == 5, direct 5-point DFT
-        const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-        const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
-        const double sg = inv ? 1.0 : -1.0;
-        double2 in[5] = {v[0], v[1], v[2], v[3], v[4]};
-        const double cs[5] = {1.0, c1, c2, c2, c1};
-        const double sn[5] = {0.0, s1, s2, -s2, -s1};
-        for (int k = 0; k < 5; k++) {
-          double re = 0.0, im = 0.0;
-          for (int q = 0; q < 5; q++) {
-            const int e = (k * q) % 5;
-            const double c = cs[e], sgn = sg * sn[e];
-            re += in[q].x * c - in[q].y * sgn;
-            im += in[q].x * sgn + in[q].y * c;
-          }
-          v[k] = make_double2(re, im);
-        }
-      }
-      const int idxD = (j / L) * L * R + jm;
-      for (int r = 0; r < R; r++) y[idxD + r * L] = v[r];
+    switch (R) {
+      case 4: fft_pass<4, INV>(x, y, n, L, a.tw); break;
+      case 2: fft_pass<2, INV>(x, y, n, L, a.tw); break;
+      case 3: fft_pass<3, INV>(x, y, n, L, a.tw); break;
+      default: fft_pass<5, INV>(x, y, n, L, a.tw); break;
     }
     double2 *t = x;
     x = y;
@@ -168,6 +189,11 @@ static __device__ double2 *fft_smem(double2 *x, double2 *y, const FftArgs &a, in
   }
   __syncthreads();
   return x;
+}
+
+static __device__ __forceinline__ double2 *fft_smem(double2 *x, double2 *y, const FftArgs &a, int inv)
+{
+  return inv ? fft_smem_t<1>(x, y, a) : fft_smem_t<0>(x, y, a);
 }
 
 // ------------------------------------------------------------------ kernels
@@ -392,15 +418,32 @@ void fb_sg_destroy(fb_sg *sg)
 }
 
 // compute_fftdensity + compute_sgacc (sgdens.c, sgacc.c): 3 launches
+void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
+{
+  (void)k;
+  FftArgs fr = fft_args(sg->prow);
+  sg_rows_fwd<<<sg->nr, SG_BS, sg->smem_row, s>>>(fr, sg->nr, sg->ns, sg->nk, dens, sg->sq, sg->rr, sg->r0,
+                                                   NULL, NULL, sg->xr, sg->xt);
+}
+
+void fb_sg_cols(fb_sg *sg, cudaStream_t s)
+{
+  FftArgs fc = fft_args(sg->pcol);
+  sg_cols<<<dim3(sg->nk, 2), SG_BS, sg->smem_col, s>>>(fc, sg->nr, sg->nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
+}
+
+void fb_sg_rows_inv(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
+{
+  FftArgs fr = fft_args(sg->prow);
+  sg_rows_inv<<<sg->nr, SG_BS, sg->smem_row, s>>>(fr, sg->ns, sg->nk, sg->xr, sg->xt, sg->nr_accr, sg->nr_acct,
+                                                   dens, sg->rstep, sg->tstep, sg->eps, k.sg_accr, k.sg_acct);
+}
+
 void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 {
-  const int nr = sg->nr, ns = sg->ns, nk = sg->nk;
-  FftArgs fr = fft_args(sg->prow), fc = fft_args(sg->pcol);
-  sg_rows_fwd<<<nr, SG_BS, sg->smem_row, s>>>(fr, nr, ns, nk, dens, sg->sq, sg->rr, sg->r0,
-                                               NULL, NULL, sg->xr, sg->xt);
-  sg_cols<<<dim3(nk, 2), SG_BS, sg->smem_col, s>>>(fc, nr, nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
-  sg_rows_inv<<<nr, SG_BS, sg->smem_row, s>>>(fr, ns, nk, sg->xr, sg->xt, sg->nr_accr, sg->nr_acct, dens,
-                                               sg->rstep, sg->tstep, sg->eps, k.sg_accr, k.sg_acct);
+  fb_sg_rows_fwd(sg, k, dens, s);
+  fb_sg_cols(sg, s);
+  fb_sg_rows_inv(sg, k, dens, s);
 }
 
 void fb_sg_update_velocities(const KP &k, cudaStream_t s)
