@@ -49,7 +49,7 @@ FALLBACK_HBM_GBS = 6650.0
 # Algorithmic bytes per cell of each stage (distinct fields read + written,
 # 8 B each), isothermal / with energy equation.  See DESIGN.md.
 STAGE_BYTES = {
-    "cfl": (32, 40), "force_sums": (8, 8), "potential": (8, 8), "soundspeed": (0, 24),
+    "cfl_forces": (32, 40), "potential": (8, 8), "soundspeed": (0, 24),
     "substep1": (64, 64), "viscous_terms": (56, 56), "viscous_update": (64, 64),
     "substep2": (40, 56), "energy_viscous_terms": (56, 56), "substep3": (0, 56),
     "transport_radial": (64, 80), "transport_azimuthal": (80, 96),

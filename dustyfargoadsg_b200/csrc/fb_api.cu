@@ -15,7 +15,7 @@ enum {
   ST_SUB2, ST_EVTERMS, ST_SUB3, ST_TRAD, ST_TAZI, ST_TVR, ST_DAMP, FB_NSTAGE
 };
 static const char *stage_names[FB_NSTAGE] = {
-  "cfl", "force_sums", "controller", "soundspeed", "potential", "substep1", "sg_rows_fwd",
+  "cfl_forces", "unused", "controller", "soundspeed", "potential", "substep1", "sg_rows_fwd",
   "sg_cols", "sg_rows_inv", "sg_update",
   "viscous_terms", "viscous_update", "substep2", "energy_viscous_terms", "substep3",
   "transport_radial", "transport_azimuthal", "transport_vr_boundary", "damping"};
@@ -237,9 +237,8 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.ringmin = dalloc(ctx, nr);
   k.vmoy = dalloc(ctx, nr);
   {
-    size_t cells = (size_t)nr * ns;
-    int nb = (int)((cells + 255) / 256);
-    if (nb > 296) nb = 296;
+    // the CFL kernel leaves one set of force/mass partials per ring
+    const int nb = nr;
     k.n_partial_blocks = nb;
     k.partials = dalloc(ctx, (size_t)nb * 5);
     ctx->d_diag = dalloc(ctx, (size_t)nb * 2);
@@ -424,7 +423,6 @@ static int enqueue_substep(fb_ctx *ctx)
   cudaStream_t s = ctx->st;
   int npt = 0;
   STAGE(ST_CFL, 1, fb_launch_cfl(k, s));
-  STAGE(ST_FORCE, 1, fb_launch_force_sums(k, s));
   STAGE(ST_CONTROL, 1, fb_launch_controller(k, s));
   if (k.energy) STAGE(ST_SOUND, 1, fb_launch_soundspeed(k, k.visc_mode == 1, s));
   STAGE(ST_POT, 1, fb_launch_potential(k, s));

@@ -85,7 +85,6 @@ struct KP {
 
 // launchers (fb_gas.cu)
 void fb_launch_cfl(const KP &k, cudaStream_t s);
-void fb_launch_force_sums(const KP &k, cudaStream_t s);
 void fb_launch_controller(const KP &k, cudaStream_t s);
 void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s);
 void fb_launch_potential(const KP &k, cudaStream_t s);

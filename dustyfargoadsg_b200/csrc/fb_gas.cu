@@ -13,6 +13,10 @@
 #include "fb_dev.cuh"
 
 #define FB_BS 256
+#define FB_BS2 128  // threads per CTA of the per-cell kernels: one ring row of 128 azimuths
+
+// per-cell kernels: blockIdx.y = ring, 128 consecutive azimuths per CTA
+static inline dim3 grid2d(const KP &k, int rings) { return dim3((k.ns + FB_BS2 - 1) / FB_BS2, rings); }
 
 static __device__ __forceinline__ double min2(double a, double b) { return (b < a) ? b : a; }  // SourceEuler.c:293
 static __device__ __forceinline__ double max2(double a, double b) { return (b > a) ? b : a; }  // SourceEuler.c:300
@@ -100,6 +104,39 @@ __global__ void __launch_bounds__(FB_BS) k_cfl(KP k)
   s = block_sum<FB_BS>(s, sh);
   const double vmoy = s / (double)ns;
   if (threadIdx.x == 0) k.vmoy[i] = vmoy;
+  // ComputeForce (Force.c:77-253) for the star (x = y = 0, mass 0) with
+  // rsmoothing = INDIRECTTERMSMOOTHING (SourceEuler.c:482), GasTotalMass
+  // (SideEuler.c:15) and the barycentre sums (SideEuler.c:42-89): ring
+  // partials, summed by the controller in ring order.
+  {
+    const double rs = k.indirect_smoothing;
+    double fx = 0.0, fy = 0.0, mass = 0.0, xb = 0.0, yb = 0.0;
+    for (int j = threadIdx.x; j < ns; j += FB_BS) {
+      const double xc = k.rmed[i] * k.cosaz[j];
+      const double yc = k.rmed[i] * k.sinaz[j];
+      const double dens = k.rho[base + j];
+      const double cellmass = k.surf[i] * dens;
+      const double dx = xc - 0.0, dy = yc - 0.0;
+      const double d2 = dx * dx + dy * dy;
+      const double dist2 = d2 + rs * rs;
+      const double distance = sqrt(dist2);
+      const double InvDist3 = 1.0 / dist2 / distance;
+      fx += FB_G * cellmass * dx * InvDist3 * 1.0;
+      fy += FB_G * cellmass * dy * InvDist3 * 1.0;
+      mass += k.surf[i] * dens;
+      xb += k.surf[i] * dens * xc;
+      yb += k.surf[i] * dens * yc;
+    }
+    fx = block_sum<FB_BS>(fx, sh);
+    fy = block_sum<FB_BS>(fy, sh);
+    mass = block_sum<FB_BS>(mass, sh);
+    xb = block_sum<FB_BS>(xb, sh);
+    yb = block_sum<FB_BS>(yb, sh);
+    if (threadIdx.x == 0) {
+      double *pp = k.partials + (size_t)i * 5;
+      pp[0] = fx; pp[1] = fy; pp[2] = mass; pp[3] = xb; pp[4] = yb;
+    }
+  }
   neg = __syncthreads_or(neg);
   bad = __syncthreads_or(bad);
   if (threadIdx.x == 0) {
@@ -135,52 +172,6 @@ __global__ void __launch_bounds__(FB_BS) k_cfl(KP k)
 }
 
 void fb_launch_cfl(const KP &k, cudaStream_t s) { k_cfl<<<k.nr, FB_BS, 0, s>>>(k); }
-
-// ------------------------------------------------------- disc force sums
-// ComputeForce (Force.c:77-253) for the star (x = y = 0, mass 0) with
-// rsmoothing = INDIRECTTERMSMOOTHING, as called from SourceEuler.c:482, plus
-// GasTotalMass (SideEuler.c:15) and the barycentre sums of
-// ComputeBarycenterPosition (SideEuler.c:42-89).  Per-CTA partials are
-// summed by the controller in CTA order (deterministic).
-__global__ void __launch_bounds__(FB_BS) k_force_sums(KP k)
-{
-  __shared__ double sh[32];
-  const int ns = k.ns;
-  const size_t n = (size_t)k.nr * ns;
-  const double rs = k.indirect_smoothing;
-  double fx = 0.0, fy = 0.0, mass = 0.0, xb = 0.0, yb = 0.0;
-  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
-    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
-    const double xc = k.rmed[i] * k.cosaz[j];
-    const double yc = k.rmed[i] * k.sinaz[j];
-    const double dens = k.rho[l];
-    const double cellmass = k.surf[i] * dens;
-    const double dx = xc - 0.0, dy = yc - 0.0;
-    const double d2 = dx * dx + dy * dy;
-    const double dist2 = d2 + rs * rs;
-    const double distance = sqrt(dist2);
-    const double InvDist3 = 1.0 / dist2 / distance;
-    fx += FB_G * cellmass * dx * InvDist3 * 1.0;
-    fy += FB_G * cellmass * dy * InvDist3 * 1.0;
-    mass += k.surf[i] * dens;
-    xb += k.surf[i] * dens * xc;
-    yb += k.surf[i] * dens * yc;
-  }
-  fx = block_sum<FB_BS>(fx, sh);
-  fy = block_sum<FB_BS>(fy, sh);
-  mass = block_sum<FB_BS>(mass, sh);
-  xb = block_sum<FB_BS>(xb, sh);
-  yb = block_sum<FB_BS>(yb, sh);
-  if (threadIdx.x == 0) {
-    double *p = k.partials + (size_t)blockIdx.x * 5;
-    p[0] = fx; p[1] = fy; p[2] = mass; p[3] = xb; p[4] = yb;
-  }
-}
-
-void fb_launch_force_sums(const KP &k, cudaStream_t s)
-{
-  k_force_sums<<<k.n_partial_blocks, FB_BS, 0, s>>>(k);
-}
 
 // ------------------------------------------------------------ controller
 static __device__ double dev_aspect_ratio(const KP &k, double rad)
@@ -439,14 +430,15 @@ void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s)
 
 // ----------------------------------------------------------- potential
 // FillForcesArrays (Pframeforce.c:44-129): star + planets + indirect terms.
-__global__ void __launch_bounds__(FB_BS) k_potential(KP k)
+__global__ void __launch_bounds__(FB_BS2) k_potential(KP k)
 {
-  const size_t n = (size_t)k.nr * k.ns;
   const fb_ctl *c = k.ctl;
   const int np = c->np;
   const int use_ind = (!k.discard_gas_it) && (fabs(k.pmax - k.pmin - 2. * M_PI) < 0.01);
-  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
-    const int i = (int)(l / k.ns), j = (int)(l - (size_t)i * k.ns);
+  {
+    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= k.ns) return;
+    const size_t l = (size_t)i * k.ns + j;
     const double x = k.rmed[i] * k.cosaz[j];
     const double y = k.rmed[i] * k.sinaz[j];
     double P = 0.0;
@@ -470,9 +462,7 @@ __global__ void __launch_bounds__(FB_BS) k_potential(KP k)
 
 void fb_launch_potential(const KP &k, cudaStream_t s)
 {
-  const size_t n = (size_t)k.nr * k.ns;
-  int blocks = (int)((n + FB_BS - 1) / FB_BS);
-  k_potential<<<blocks, FB_BS, 0, s>>>(k);
+  k_potential<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k);
 }
 
 // ------------------------------------------------------------ SubStep1
@@ -485,13 +475,14 @@ static __device__ __forceinline__ double pressure_at(const KP &k, size_t l)
 
 // SubStep1 (SourceEuler.c:765-1009) without dust: pressure, potential and
 // curvature terms into VradInt (i >= 1) and VthetaInt (all rings).
-__global__ void __launch_bounds__(FB_BS) k_substep1(KP k)
+__global__ void __launch_bounds__(FB_BS2) k_substep1(KP k)
 {
   const int ns = k.ns;
-  const size_t n = (size_t)k.nr * ns;
   const double dt = k.ctl->dt;
-  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
-    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+  {
+    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const size_t l = (size_t)i * ns + j;
     const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
     const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
     const double Pl = pressure_at(k, l);
@@ -520,21 +511,21 @@ __global__ void __launch_bounds__(FB_BS) k_substep1(KP k)
 
 void fb_launch_substep1(const KP &k, cudaStream_t s)
 {
-  const size_t n = (size_t)k.nr * k.ns;
-  k_substep1<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
+  k_substep1<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k);
 }
 
 // ------------------------------------------------------- viscous stresses
 // ComputeViscousTerms (Viscosity.c:159-303) incl. ComputeDivergenceVelocity
 // (SourceEuler.c:2373-2412): DivV, TAUrr, TAUpp (all rings), TAUrp (i >= 1).
-__global__ void __launch_bounds__(FB_BS) k_viscous_terms(KP k, const double *__restrict__ vr,
+__global__ void __launch_bounds__(FB_BS2) k_viscous_terms(KP k, const double *__restrict__ vr,
                                                          const double *__restrict__ vt)
 {
   const int ns = k.ns;
-  const size_t n = (size_t)k.nr * ns;
   const double invdphi = k.invdphi, onethird = 1.0 / 3.0;
-  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
-    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+  {
+    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const size_t l = (size_t)i * ns + j;
     const size_t lip = l + ns;
     const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
     double div = (vr[lip] * k.rsup[i] - vr[l] * k.rinf[i]) * k.invdiffrsup[i] * k.invrmed[i];
@@ -558,19 +549,19 @@ __global__ void __launch_bounds__(FB_BS) k_viscous_terms(KP k, const double *__r
 
 void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s)
 {
-  const size_t n = (size_t)k.nr * k.ns;
-  k_viscous_terms<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k, vr, vt);
+  k_viscous_terms<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k, vr, vt);
 }
 
 // UpdateVelocitiesWithViscosity (Viscosity.c:305-378)
-__global__ void __launch_bounds__(FB_BS) k_viscous_update(KP k, double *vr, double *vt, double dtov)
+__global__ void __launch_bounds__(FB_BS2) k_viscous_update(KP k, double *vr, double *vt, double dtov)
 {
   const int ns = k.ns, nr = k.nr;
-  const size_t n = (size_t)nr * ns;
   const double DeltaT = dt_of(k, dtov), invdphi = k.invdphi;
-  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
-    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
-    if (i < 1) continue;
+  {
+    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const size_t l = (size_t)i * ns + j;
+    if (i < 1) return;
     const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
     const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
     const size_t lim = l - ns, lip = l + ns;
@@ -589,8 +580,7 @@ __global__ void __launch_bounds__(FB_BS) k_viscous_update(KP k, double *vr, doub
 
 void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s)
 {
-  const size_t n = (size_t)k.nr * k.ns;
-  k_viscous_update<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k, vr, vt, dt_override);
+  k_viscous_update<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k, vr, vt, dt_override);
 }
 
 // ------------------------------------------------------------ SubStep2
@@ -610,18 +600,19 @@ static __device__ __forceinline__ double q_t(const KP &k, size_t l, size_t ljp)
   return (dv < 0.0) ? FB_CVNR * FB_CVNR * k.rho[l] * dv * dv : 0.0;
 }
 
-__global__ void __launch_bounds__(FB_BS) k_substep2(KP k)
+__global__ void __launch_bounds__(FB_BS2) k_substep2(KP k)
 {
   const int ns = k.ns, nr = k.nr;
-  const size_t n = (size_t)(nr + 1) * ns;
   const double dt = k.ctl->dt;
-  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
-    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+  {
+    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const size_t l = (size_t)i * ns + j;
     if (i == nr) {
       k.vr[l] = 0.0;
       k.vt[l] = 0.0;
       if (k.energy) k.e[l] = 0.0;
-      continue;
+      return;
     }
     const size_t lip = l + ns;
     const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
@@ -649,17 +640,17 @@ __global__ void __launch_bounds__(FB_BS) k_substep2(KP k)
 
 void fb_launch_substep2(const KP &k, cudaStream_t s)
 {
-  const size_t n = (size_t)(k.nr + 1) * k.ns;
-  k_substep2<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
+  k_substep2<<<grid2d(k, k.nr + 1), FB_BS2, 0, s>>>(k);
 }
 
 // ComputeDivergenceVelocity (SourceEuler.c:2373-2412) on (Vrad, Vtheta)
-__global__ void __launch_bounds__(FB_BS) k_divergence(KP k)
+__global__ void __launch_bounds__(FB_BS2) k_divergence(KP k)
 {
   const int ns = k.ns;
-  const size_t n = (size_t)k.nr * ns;
-  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
-    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+  {
+    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const size_t l = (size_t)i * ns + j;
     const size_t lip = l + ns;
     const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
     double div = (k.vr[lip] * k.rsup[i] - k.vr[l] * k.rinf[i]) * k.invdiffrsup[i] * k.invrmed[i];
@@ -670,8 +661,7 @@ __global__ void __launch_bounds__(FB_BS) k_divergence(KP k)
 
 void fb_launch_divergence(const KP &k, cudaStream_t s)
 {
-  const size_t n = (size_t)k.nr * k.ns;
-  k_divergence<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
+  k_divergence<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k);
 }
 
 // ------------------------------------------------------------ SubStep3
@@ -1019,14 +1009,15 @@ __global__ void __launch_bounds__(512) k_transport_azimuthal(KP k, double dtov)
 // ComputeVelocities' radial part (TransportEuler.c:531-536) needs the
 // neighbouring ring after both passes; fused with AddFloorDensity
 // (SourceEuler.c:2506) and ApplyWallBoundaries (SideEuler.c:1047-1099).
-__global__ void __launch_bounds__(FB_BS) k_transport_vr(KP k)
+__global__ void __launch_bounds__(FB_BS2) k_transport_vr(KP k)
 {
   const int ns = k.ns, nr = k.nr;
-  const size_t n = (size_t)(nr + 1) * ns;
   const int wall = k.wall && !k.transport_only;
   const int floors = k.add_floors && !k.transport_only;
-  for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
-    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
+  {
+    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ns) return;
+    const size_t l = (size_t)i * ns + j;
     auto vr_at = [&](int ii) -> double {
       if (ii == 0) return 0.0;
       const size_t m = (size_t)ii * ns + j;
@@ -1034,7 +1025,7 @@ __global__ void __launch_bounds__(FB_BS) k_transport_vr(KP k)
     };
     if (i == nr) {
       if (wall) k.vr[l] = -vr_at(nr - 2);
-      continue;
+      return;
     }
     double d = k.rho_t[l];
     double v = vr_at(i);
@@ -1089,8 +1080,7 @@ void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t
 
 void fb_launch_transport_vr(const KP &k, cudaStream_t s)
 {
-  const size_t n = (size_t)(k.nr + 1) * k.ns;
-  k_transport_vr<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k);
+  k_transport_vr<<<grid2d(k, k.nr + 1), FB_BS2, 0, s>>>(k);
   k_lostmass<<<1, 32, 0, s>>>(k);
 }
 
