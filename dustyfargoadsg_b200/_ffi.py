@@ -96,7 +96,7 @@ EXPORTS = (
     "fb_init_state", "fb_create", "fb_destroy", "fb_upload", "fb_algogas", "fb_download",
     "fb_download_derived", "fb_diagnostics", "fb_strerror", "fb_last_error", "fb_stage",
     "fb_build_info", "fb_struct_size", "fb_kernel_launches", "fb_profile", "fb_profile_read",
-    "fb_select_device",
+    "fb_select_device", "fb_transport_noalloc", "fb_noalloc_last_error",
 )
 
 _lib = None
@@ -135,6 +135,8 @@ def load():
         "fb_profile": (_I, [vp, _I]),
         "fb_profile_read": (_I, [vp, _I, C.POINTER(C.c_char_p), _P, C.POINTER(C.c_longlong)]),
         "fb_select_device": (_I, [_I]),
+        "fb_transport_noalloc": (_I, [C.POINTER(FbParams), vp, vp, vp, vp, _D, vp, _P]),
+        "fb_noalloc_last_error": (C.c_char_p, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

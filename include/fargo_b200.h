@@ -216,6 +216,31 @@ const char *fb_last_error(const fb_ctx *ctx);
 #define FB_STAGE_SELFGRAV   5  /* compute_sgacc only: fills SG accelerations */
 int fb_stage(fb_ctx *ctx, int stage, double dt);
 
+/* ---- allocation-free transport -------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc:
+   host codes embedded in a GPU application that owns the whole device-memory
+   budget, or that call from regions where an allocation (which may also
+   synchronize the device) is not acceptable.  Runs the same kernels as
+   fb_stage(ctx, FB_STAGE_TRANSPORT, dt) (Transport, src/TransportEuler.c:65)
+   without a context and without allocating anything: the inter-pass scratch
+   is a fixed file-scope device array of at most FB_NOALLOC_MAX_CELLS cells
+   (about 7.4 MB), held on every GPU that loads the library until exit.
+   dens, vrad, vtheta, energy are DEVICE pointers to (nrad+1)*nsec doubles in
+   the PolarGrid layout, updated in place (energy only with the energy
+   equation); stream is a cudaStream_t (NULL: default stream); lost_mass, if
+   not NULL, receives the ring-0 outflow of this call (the stream is then
+   synchronized).  Grids with (nrad+1)*nsec > FB_NOALLOC_MAX_CELLS, nrad >
+   4096 or nsec > 3072 are refused with FB_ERR_INVALID.  The first call on a
+   device (and the first with a larger nsec) sets up the device addresses and
+   kernel attributes; make it before any stream capture.  Every call
+   synchronizes the stream once after uploading the grid tables.  All calls
+   share the scratch, so calls that overlap on the GPU race.  The reason for
+   a failure is in fb_noalloc_last_error(). */
+#define FB_NOALLOC_MAX_CELLS 131072
+int fb_transport_noalloc(const fb_params *p, double *dens, double *vrad, double *vtheta,
+                         double *energy, double dt, void *stream, double *lost_mass);
+const char *fb_noalloc_last_error(void);
+
 /* ---- profiling ----------------------------------------------------------- */
 /* Number of kernel launches this context has issued. */
 long long fb_kernel_launches(const fb_ctx *ctx);
