@@ -40,6 +40,8 @@ sys.path.insert(0, REPO)
 WORKLOADS = {
     # isothermal 128 x 384 disc, q=1e-3 planet on a fixed circular orbit
     "iso_128x384": dict(par="iso_128x384.par", noise=1e-4, seed=0),
+    # isothermal disc on the largest grid of the batched sweep (HBM-resident)
+    "iso_768x2304": dict(par="iso_768x2304.par", noise=1e-4, seed=0),
     # adiabatic + beta cooling + self-gravity 512 x 1536 disc, q=5e-4 planet
     "adiabatic_sg_512x1536": dict(par="adiabatic_sg_512x1536.par", noise=1e-4, seed=0),
 }
