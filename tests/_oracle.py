@@ -14,6 +14,7 @@ import numpy as np
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_BIN = os.path.join(REPO, "oracle", "_ref", "fargo_oracle")
+DROPIN_BIN = os.path.join(REPO, "oracle", "_ref", "fargo_dropin")
 CONFIG_DIR = os.path.join(REPO, "dustyfargoadsg_b200", "configs")
 
 
@@ -67,15 +68,18 @@ def write_par(src_par, dst_dir, **keys):
 
 
 def run_oracle(par, steps, noise=0.0, seed=0, dump_every=1, stage=False, workdir=None,
-               timeout=3600, max_substeps=None, keep=False, extra_keys=None):
+               timeout=3600, max_substeps=None, keep=False, extra_keys=None, binary=None):
     """Run the reference for `steps` AlgoGas calls (NTOT = steps-1) and
     return (dumps, timing, workdir).  dumps maps tag -> dict of arrays."""
-    if not have_oracle():
-        raise RuntimeError("oracle binary missing: run `make -C oracle` where the reference is present")
+    binary = binary or ORACLE_BIN
+    if not os.path.exists(binary):
+        raise RuntimeError("%s missing: run `make -C oracle all dropin` where the reference is present" % binary)
     wd = workdir or tempfile.mkdtemp(prefix="fb_oracle_")
     out = os.path.join(wd, "out")
     os.makedirs(out, exist_ok=True)
     keys = {"Ntot": max(steps - 1, 0), "OutputDir": out, "Ninterm": max(steps, 1) * 1000}
+    if extra_keys and "Ninterm" in extra_keys:
+        keys.pop("Ninterm")
     keys.update(extra_keys or {})
     p = write_par(par, wd, **keys)
     env = dict(os.environ)
@@ -87,7 +91,7 @@ def run_oracle(par, steps, noise=0.0, seed=0, dump_every=1, stage=False, workdir
         env["ORACLE_STAGE_DUMP"] = "1"
     if max_substeps:
         env["ORACLE_MAX_SUBSTEPS"] = str(int(max_substeps))
-    r = subprocess.run([ORACLE_BIN, p], cwd=wd, env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
+    r = subprocess.run([binary, p], cwd=wd, env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
                        timeout=timeout)
     if r.returncode != 0:
         raise RuntimeError("oracle failed (%d): %s" % (r.returncode, r.stderr[-2000:].decode(errors="replace")))

@@ -1,0 +1,49 @@
+"""The drop-in proof: the reference's own main(), init, SendOutput and planet
+logs, with AlgoGas answered by libfargo_b200.so through
+dustyfargoadsg_b200/host/algogas_dropin.c, against the reference's own
+AlgoGas on the same seeded run.  Compares the state after every DT and the
+gas*N.dat output files the reference writes."""
+import os
+
+import numpy as np
+import pytest
+
+from tests import _oracle
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (_oracle.have_oracle() and os.path.exists(_oracle.DROPIN_BIN)),
+                                 reason="oracle / drop-in binaries not built")]
+
+
+@pytest.mark.parametrize("par_name,keys", [
+    ("iso_128x384.par", dict(Nrad=64, Nsec=192)),
+    ("adiabatic_sg_512x1536.par", dict(Nrad=64, Nsec=192)),
+])
+def test_dropin_matches_reference(tmp_path, par_name, keys):
+    src = os.path.join(_oracle.CONFIG_DIR, par_name)
+    steps = 5
+    par = _oracle.write_par(src, str(tmp_path), **keys)
+    wa, wb = str(tmp_path / "ref"), str(tmp_path / "gpu")
+    os.makedirs(wa)
+    os.makedirs(wb)
+    extra = {"Ninterm": 2}
+    ref, _, _ = _oracle.run_oracle(par, steps, noise=1e-4, seed=2, workdir=wa, keep=True, extra_keys=extra)
+    gpu, _, _ = _oracle.run_oracle(par, steps, noise=1e-4, seed=2, workdir=wb, keep=True, extra_keys=extra,
+                                   binary=_oracle.DROPIN_BIN)
+    for s in range(1, steps + 1):
+        a, b = gpu["state_%05d" % s], ref["state_%05d" % s]
+        for k in ("dens", "vrad", "vtheta", "energy"):
+            assert _oracle.rel_err(a[k], b[k]) <= 1e-11, (s, k)
+        assert abs(a["PhysicalTime"] - b["PhysicalTime"]) <= 1e-13 * b["PhysicalTime"]
+    # output files written by the reference's SendOutput (Output.c:178-218)
+    nr, ns = keys["Nrad"], keys["Nsec"]
+    for n in (0, 1, 2):
+        for name in ("gasdens", "gasvrad", "gasvtheta"):
+            fa = os.path.join(wa, "out", "%s%d.dat" % (name, n))
+            fb = os.path.join(wb, "out", "%s%d.dat" % (name, n))
+            xa, xb = np.fromfile(fa), np.fromfile(fb)
+            assert xa.size == nr * ns and xb.size == nr * ns
+            assert _oracle.rel_err(xb, xa) <= 1e-11, (name, n)
+    pa = np.loadtxt(os.path.join(wa, "out", "planet0.dat"))
+    pb = np.loadtxt(os.path.join(wb, "out", "planet0.dat"))
+    np.testing.assert_allclose(pb, pa, rtol=1e-10, atol=1e-14)
