@@ -12,8 +12,8 @@ import os
 import numpy as np
 
 from . import _ffi
-from ._ffi import (FB_F_ALL, FB_F_DENS, FB_F_ENERGY, FB_F_VRAD, FB_F_VTHETA, FbError, FbParams,
-                   FbProfiles, FbState, FbStepReport, check, load)
+from ._ffi import (FB_F_ALL, FB_F_DENS, FB_F_ENERGY, FB_F_VRAD, FB_F_VTHETA, FbDustState, FbError,
+                   FbParams, FbProfiles, FbState, FbStepReport, check, load)
 
 __all__ = ["Disc", "read_par", "select_device", "FbError", "load", "CONFIG_DIR"]
 
@@ -53,7 +53,9 @@ def read_par(path, **overrides):
 class Disc:
     """One disc on the GPU: parameters, device context and host mirrors."""
 
-    def __init__(self, params, noise=0.0, seed=0, state=None):
+    DUST_ARRAYS = ("r", "th", "vr", "vth", "l", "size", "stokes")
+
+    def __init__(self, params, noise=0.0, seed=0, state=None, dust_seed=None):
         self.lib = load()
         if isinstance(params, (str, os.PathLike)):
             params = read_par(params)
@@ -73,13 +75,52 @@ class Disc:
         self.pr = FbProfiles(*[_ptr(self.prof[k]) for k in
                                ("sigma_med", "sigma_inf", "energy_med", "vtheta_med", "vrad_med",
                                 "global_soundspeed")])
+        self.npart = int(self.p.nbpart)
+        if self.npart > 0:
+            self.dust_arrays = {k: np.zeros(self.npart) for k in self.DUST_ARRAYS}
+            self.dst = FbDustState()
+            self.dst.n = self.npart
+            for k, a in self.dust_arrays.items():
+                setattr(self.dst, k, _ptr(a))
         if state is None:
             check(self.lib.fb_init_state(C.byref(self.p), self.ctx, float(noise), int(seed),
                                          C.byref(self.st), C.byref(self.pr)), "fb_init_state", self.ctx)
         else:
             self.set_state(state)
+            if self.npart > 0 and "pc_r" in state:
+                self.set_dust(state)
             return
         check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx)
+        if self.npart > 0:
+            # InitDustSystem reseeds the stream (Dsys.c:173)
+            check(self.lib.fb_init_dust(C.byref(self.p), self.ctx, int(seed if dust_seed is None else dust_seed),
+                                        C.byref(self.dst)), "fb_init_dust", self.ctx)
+            check(self.lib.fb_dust_upload(self.ctx, C.byref(self.dst)), "fb_dust_upload", self.ctx)
+
+    # -- particles ------------------------------------------------------
+    def set_dust(self, state):
+        """Upload particles: pc_r, pc_th, pc_vr, pc_vth, pc_size (+ pc_l,
+        pc_stokes; pc_rng_x / pc_kicks / pc_carry for the random stream)."""
+        for k in self.DUST_ARRAYS:
+            key = "pc_" + k
+            if key in state:
+                self.dust_arrays[k][:] = np.asarray(state[key], dtype=np.float64)[: self.npart]
+        if "pc_l" not in state:
+            self.dust_arrays["l"][:] = self.dust_arrays["r"] * self.dust_arrays["vth"]
+        self.dst.rng_x = int(state.get("pc_rng_x", self.dst.rng_x))
+        self.dst.kicks = int(state.get("pc_kicks", 0))
+        carry = state.get("pc_carry", (0.0, 0.0))
+        self.dst.carry[0], self.dst.carry[1] = float(carry[0]), float(carry[1])
+        self.dst.particles_mass = 0.0
+        check(self.lib.fb_dust_upload(self.ctx, C.byref(self.dst)), "fb_dust_upload", self.ctx)
+
+    def dust(self):
+        """Download the particles: {pc_r, ..., pc_stokes, pc_rng_x, pc_kicks}."""
+        check(self.lib.fb_dust_download(self.ctx, C.byref(self.dst)), "fb_dust_download", self.ctx)
+        out = {"pc_" + k: v.copy() for k, v in self.dust_arrays.items()}
+        out.update(pc_rng_x=int(self.dst.rng_x), pc_kicks=int(self.dst.kicks),
+                   pc_carry=(self.dst.carry[0], self.dst.carry[1]))
+        return out
 
     # -- state ----------------------------------------------------------
     def set_state(self, state):

@@ -48,7 +48,8 @@ class FbParams(C.Structure):
         ("sizeminpart", _D), ("sizemaxpart", _D), ("sizepartslope", _D), ("rhopart", _D), ("dustslope", _D),
         ("rmindust", _D), ("rmaxdust", _D),
         ("dust_feel_disk", _I), ("dust_feel_planets", _I), ("dust_feel_turb", _I), ("dust_feedback", _I),
-        ("sfta", _I), ("interpolation", _I),
+        ("dust_feel_sg", _I),
+        ("sfta", _I), ("interpolation", _I), ("write_dust_density", _I),
         ("unsupported", C.c_ulonglong),
         ("planetconfig", C.c_char * 512), ("outputdir", C.c_char * 512),
     ]
@@ -81,6 +82,13 @@ class FbProfiles(C.Structure):
     ]
 
 
+class FbDustState(C.Structure):
+    _fields_ = [
+        ("n", _I), ("r", _P), ("th", _P), ("vr", _P), ("vth", _P), ("l", _P), ("size", _P), ("stokes", _P),
+        ("rng_x", C.c_ulonglong), ("kicks", C.c_longlong), ("carry", _D * 2), ("particles_mass", _D),
+    ]
+
+
 class FbStepReport(C.Structure):
     _fields_ = [
         ("substeps", _I), ("status", _I), ("physical_time", _D), ("mindt", _D), ("maxdt", _D),
@@ -96,7 +104,8 @@ EXPORTS = (
     "fb_init_state", "fb_create", "fb_destroy", "fb_upload", "fb_algogas", "fb_download",
     "fb_download_derived", "fb_diagnostics", "fb_strerror", "fb_last_error", "fb_stage",
     "fb_build_info", "fb_struct_size", "fb_kernel_launches", "fb_profile", "fb_profile_read",
-    "fb_select_device", "fb_transport_noalloc", "fb_noalloc_last_error",
+    "fb_select_device", "fb_transport_noalloc", "fb_noalloc_last_error", "fb_init_dust",
+    "fb_dust_upload", "fb_dust_download",
 )
 
 _lib = None
@@ -137,6 +146,9 @@ def load():
         "fb_select_device": (_I, [_I]),
         "fb_transport_noalloc": (_I, [C.POINTER(FbParams), vp, vp, vp, vp, _D, vp, _P]),
         "fb_noalloc_last_error": (C.c_char_p, []),
+        "fb_init_dust": (_I, [C.POINTER(FbParams), vp, C.c_long, C.POINTER(FbDustState)]),
+        "fb_dust_upload": (_I, [vp, C.POINTER(FbDustState)]),
+        "fb_dust_download": (_I, [vp, C.POINTER(FbDustState)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -148,7 +160,7 @@ def load():
 
 
 def check_layout(lib):
-    for idx, cls in enumerate((FbParams, FbPlanets, FbState, FbProfiles, FbStepReport)):
+    for idx, cls in enumerate((FbParams, FbPlanets, FbState, FbProfiles, FbStepReport, FbDustState)):
         want = lib.fb_struct_size(idx)
         if want != C.sizeof(cls):
             raise RuntimeError("ABI mismatch for %s: C %d bytes, ctypes %d" % (cls.__name__, want, C.sizeof(cls)))

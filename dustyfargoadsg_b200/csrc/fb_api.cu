@@ -12,13 +12,13 @@
 enum {
   ST_CFL, ST_FORCE, ST_CONTROL, ST_SOUND, ST_POT, ST_SUB1, ST_SG, ST_SGCOLS, ST_SGINV, ST_SGUPD,
   ST_VTERMS, ST_VUPDATE,
-  ST_SUB2, ST_EVTERMS, ST_SUB3, ST_TRAD, ST_TAZI, ST_TVR, ST_DAMP, FB_NSTAGE
+  ST_SUB2, ST_EVTERMS, ST_SUB3, ST_TRAD, ST_TAZI, ST_TVR, ST_DAMP, ST_DUST, FB_NSTAGE
 };
 static const char *stage_names[FB_NSTAGE] = {
   "cfl_forces", "unused", "controller", "soundspeed", "potential", "substep1", "sg_rows_fwd",
   "sg_cols", "sg_rows_inv", "sg_update",
   "viscous_terms", "viscous_update", "substep2", "energy_viscous_terms", "substep3",
-  "transport_radial", "transport_azimuthal", "transport_vr_boundary", "damping"};
+  "transport_radial", "transport_azimuthal", "transport_vr_boundary", "damping", "dust_particles"};
 
 struct fb_ctx {
   fb_params p;
@@ -51,6 +51,10 @@ struct fb_ctx {
   int graph_state;            // 0 not built, 1 ready, -1 unavailable
   long long launches_per_substep;
   int substep_cap;
+  // Lagrangian particles (nbpart > 0)
+  PP pp;
+  int has_dust, dust_uploaded;
+  fb_dust_ctl *h_dc;  // pinned mirror of pp.dc
 };
 
 static void set_err(fb_ctx *c, const char *fmt, ...)
@@ -121,6 +125,91 @@ extern "C" const char *fb_last_error(const fb_ctx *ctx) { return ctx ? ctx->err 
 extern "C" const char *fb_build_info(void)
 {
   return "libfargo_b200 sm_100a fp64 --fmad=false abi " "1";
+}
+
+// Particle arrays, the grids the gas step leaves for them, and the constants
+// of the particle update (Dsys.c:308-331).
+static int dust_create(fb_ctx *ctx)
+{
+  const fb_params *p = &ctx->p;
+  KP &k = ctx->k;
+  PP &pp = ctx->pp;
+  const int n = p->nbpart, ns = ctx->ns;
+  const size_t nf = ctx->nf;
+  if (p->omegaframe != 0.0) {
+    set_err(ctx, "particles need a non-rotating frame (OMEGAFRAME = 0)");
+    return FB_ERR_UNSUPPORTED;
+  }
+  double **grids[] = {&k.indpot, &k.rgp, &k.agp, &k.rind, &k.aind, &k.rsga, &k.asga};
+  for (size_t f = 0; f < sizeof grids / sizeof grids[0]; f++)
+    if (!(*grids[f] = dalloc(ctx, nf))) return FB_ERR_NOMEM;
+  k.particles = 1;
+  k.dust_feel_planets = p->dust_feel_planets;
+  k.dust_feel_disk = p->dust_feel_disk;
+  memset(&pp, 0, sizeof pp);
+  pp.n = n;
+  // candidate uniform pairs per substep: accepted ones (rate pi/4) must cover
+  // one Gaussian pair per kicked particle plus the odd one
+  pp.ncand = (int)((long long)(n + 4) * 27 / 20 + 2048 + 256);
+  double **arrays[] = {&pp.r, &pp.th, &pp.vr, &pp.vth, &pp.l, &pp.size, &pp.st};
+  for (size_t f = 0; f < sizeof arrays / sizeof arrays[0]; f++)
+    if (!(*arrays[f] = dalloc(ctx, n))) return FB_ERR_NOMEM;
+  const int nsb = (n + 1023) / 1024, ncb = (pp.ncand + 255) / 256;
+  int **ints[] = {&pp.flag, &pp.kidx, &pp.kick_bsum, &pp.cand_flag, &pp.cand_bsum};
+  const size_t isz[] = {(size_t)n, (size_t)n, (size_t)nsb, (size_t)pp.ncand, (size_t)ncb};
+  for (size_t f = 0; f < 5; f++) {
+    void *d = NULL;
+    if (cudaMalloc(&d, isz[f] * sizeof(int)) != cudaSuccess) return FB_ERR_NOMEM;
+    cudaMemset(d, 0, isz[f] * sizeof(int));
+    ctx->allocs.push_back(d);
+    *ints[f] = (int *)d;
+  }
+  {
+    void *d = NULL;
+    if (cudaMalloc(&d, ((size_t)n + 4) * sizeof(double2)) != cudaSuccess) return FB_ERR_NOMEM;
+    ctx->allocs.push_back(d);
+    pp.pairs = (double2 *)d;
+    if (cudaMalloc(&d, sizeof(fb_dust_ctl)) != cudaSuccess) return FB_ERR_NOMEM;
+    cudaMemset(d, 0, sizeof(fb_dust_ctl));
+    ctx->allocs.push_back(d);
+    pp.dc = (fb_dust_ctl *)d;
+    if (cudaMallocHost((void **)&ctx->h_dc, sizeof(fb_dust_ctl)) != cudaSuccess) return FB_ERR_NOMEM;
+    memset(ctx->h_dc, 0, sizeof(fb_dust_ctl));
+  }
+  // azimuths of the cell centres and interfaces (SourceEuler.c:162-174)
+  const fb_geom &g = ctx->g;
+  const double half = 0.5 * (p->pmax - p->pmin) / (double)ns;
+  std::vector<double> aziinf(ns);
+  for (int j = 0; j < ns; j++) aziinf[j] = g.azimuth[j] - half;
+  pp.azimuth = dtable(ctx, g.azimuth, ns);
+  pp.aziinf = dtable(ctx, aziinf.data(), ns);
+  pp.aziinf0 = aziinf[0];
+  pp.azisupl = g.azimuth[ns - 1] + half;
+  pp.delta_r = p->log_grid ? log(g.rsup[0] / g.rinf[0]) : g.rsup[0] - g.rinf[0];
+  pp.delta_phi = (g.azimuth[0] + half) - (g.azimuth[0] - half);
+  pp.rmin = p->rmin;
+  pp.rmax = p->rmax;
+  const double unit_length = fb_unit_length(p), unit_mass = fb_unit_mass(p);
+  pp.unit_mass = unit_mass;
+  pp.inv_unit_length2 = pow(unit_length, -2.0);
+  pp.dust_density_cu = p->rhopart * 1000.0 * pow(unit_length, 3.) / unit_mass;
+  pp.aspectratio = p->aspectratio;
+  pp.thicksmoothing = p->thicknesssmoothing;
+  pp.flaringindex = p->flaringindex;
+  pp.log_grid = p->log_grid;
+  pp.feel_disk = p->dust_feel_disk;
+  pp.feel_planets = p->dust_feel_planets;
+  pp.feel_sg = p->dust_feel_sg;
+  pp.feel_turb = p->dust_feel_turb;
+  pp.sfta = p->sfta;
+  pp.restokes = p->write_dust_density;
+  // DUSTFEEDBACK with the particle mass of a run without a dust fluid (zero,
+  // main.c:187-201): the feedback accelerations and heating are exact zeros
+  // and only the stopping-time bound on the substep remains
+  if (p->dust_feedback) k.dust_min_ts = &pp.dc->min_ts;
+  if (!pp.azimuth || !pp.aziinf) return FB_ERR_NOMEM;
+  ctx->has_dust = 1;
+  return FB_OK;
 }
 
 // ------------------------------------------------------------------ create
@@ -297,6 +386,10 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
     if (cap && atoi(cap) > 0) ctx->substep_cap = atoi(cap);
   }
   if (getenv("FB_NO_GRAPH")) ctx->graph_state = -1;
+  if (p->nbpart > 0) {
+    rc = dust_create(ctx);
+    if (rc) { fb_destroy(ctx); return rc; }
+  }
   if (p->self_gravity) {
     rc = fb_sg_create(&ctx->sg, p, &ctx->g, ctx->st);
     if (rc) { set_err(ctx, "self-gravity setup failed (%d)", rc); fb_destroy(ctx); return rc; }
@@ -310,6 +403,7 @@ extern "C" int fb_destroy(fb_ctx *ctx)
 {
   if (!ctx) return FB_OK;
   if (ctx->st) cudaStreamSynchronize(ctx->st);
+  if (ctx->h_dc) cudaFreeHost(ctx->h_dc);
   if (ctx->sg) fb_sg_destroy(ctx->sg);
   for (void *p : ctx->allocs) cudaFree(p);
   if (ctx->d_ctl) cudaFree(ctx->d_ctl);
@@ -424,6 +518,9 @@ static int enqueue_substep(fb_ctx *ctx)
   int npt = 0;
   STAGE(ST_CFL, 1, fb_launch_cfl(k, s));
   STAGE(ST_CONTROL, 1, fb_launch_controller(k, s));
+  // particles after the planets' RK5 step and before the gas update
+  // (SourceEuler.c:504-531)
+  if (ctx->has_dust) STAGE(ST_DUST, fb_dust_launches(ctx->pp), fb_launch_dust_substep(k, ctx->pp, s));
   if (k.energy) STAGE(ST_SOUND, 1, fb_launch_soundspeed(k, k.visc_mode == 1, s));
   STAGE(ST_POT, 1, fb_launch_potential(k, s));
   STAGE(ST_SUB1, 1, fb_launch_substep1(k, s));
@@ -545,11 +642,23 @@ extern "C" int fb_algogas(fb_ctx *ctx, fb_step_report *rep)
 {
   if (!ctx) return FB_ERR_INVALID;
   if (!ctx->uploaded) return FB_ERR_STATE;
+  if (ctx->has_dust && !ctx->dust_uploaded) {
+    set_err(ctx, "NBPART > 0: upload the particles (fb_dust_upload) before the first DT");
+    return FB_ERR_STATE;
+  }
   KP &k = ctx->k;
   cudaStream_t s = ctx->st;
   CK(cudaEventRecord(ctx->ev0, s));
   fb_launch_begin_dt(k, ctx->p.dt, s);
   ctx->launches += 1;
+  if (ctx->has_dust && ctx->sg) {
+    // main.c:307-316: before every DT the reference's main loop recomputes
+    // the self-gravity field (SoftWriting = No), which sets the RadSGAcc /
+    // AziSGAcc grids the first substep's particles read
+    fb_sg_accel(ctx->sg, k, k.rho, s);
+    fb_sg_update_velocities(k, s, 1);
+    ctx->launches += fb_sg_launches(ctx->sg);
+  }
   if (k.energy) { fb_launch_soundspeed(k, 0, s); ctx->launches += 1; }  // SourceEuler.c:344-350
   int status = FB_OK;
   const int cap = ctx->substep_cap;
@@ -709,5 +818,87 @@ extern "C" int fb_sg_axisym_accel(fb_ctx *ctx, const double *dens, double *axi_o
     a /= (double)ns;
     axi_out[i] = a;
   }
+  return FB_OK;
+}
+
+// Same as fb_sg_axisym_accel for the density already on the device.
+extern "C" int fb_sg_axisym_accel_device(fb_ctx *ctx, double *axi_out)
+{
+  if (!ctx || !axi_out) return FB_ERR_INVALID;
+  if (!ctx->sg) return FB_ERR_STATE;
+  if (!ctx->uploaded) return FB_ERR_STATE;
+  KP &k = ctx->k;
+  const int nr = ctx->nr, ns = ctx->ns;
+  fb_sg_accel(ctx->sg, k, k.rho, ctx->st);
+  std::vector<double> acc((size_t)nr * ns);
+  CK(cudaMemcpyAsync(acc.data(), k.sg_accr, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  for (int i = 0; i < nr; i++) {
+    double a = 0.0;
+    for (int j = 0; j < ns; j++) a += acc[(size_t)i * ns + j];
+    a /= (double)ns;
+    axi_out[i] = a;
+  }
+  return FB_OK;
+}
+
+// ------------------------------------------------------------ particles
+extern "C" int fb_dust_upload(fb_ctx *ctx, const fb_dust_state *st)
+{
+  if (!ctx || !st) return FB_ERR_INVALID;
+  if (!ctx->has_dust) { set_err(ctx, "context created with NBPART = 0"); return FB_ERR_STATE; }
+  if (!ctx->uploaded) { set_err(ctx, "upload the gas state (fb_upload) first"); return FB_ERR_STATE; }
+  PP &pp = ctx->pp;
+  if (st->n != pp.n || !st->r || !st->th || !st->vr || !st->vth || !st->l || !st->size || !st->stokes)
+    return FB_ERR_INVALID;
+  if (st->kicks < 0 || st->rng_x > 0xFFFFFFFFFFFFull) return FB_ERR_INVALID;
+  if (st->particles_mass != 0.0) {
+    set_err(ctx, "a non-zero particle mass needs the dust feedback / dust-fluid paths, not in this build");
+    return FB_ERR_UNSUPPORTED;
+  }
+  const size_t b = (size_t)pp.n * sizeof(double);
+  const double *src[] = {st->r, st->th, st->vr, st->vth, st->l, st->size, st->stokes};
+  double *dst[] = {pp.r, pp.th, pp.vr, pp.vth, pp.l, pp.size, pp.st};
+  for (int f = 0; f < 7; f++) CK(cudaMemcpyAsync(dst[f], src[f], b, cudaMemcpyHostToDevice, ctx->st));
+  fb_dust_ctl *h = ctx->h_dc;
+  memset(h, 0, sizeof *h);
+  h->x = st->rng_x;
+  h->kicks = st->kicks;
+  h->carry_rad = st->carry[0];
+  h->carry_phi = st->carry[1];
+  h->min_ts = 1e6;
+  CK(cudaMemcpyAsync(pp.dc, h, sizeof *h, cudaMemcpyHostToDevice, ctx->st));
+  // the interpolation call of main.c:287: Stokes numbers at the uploaded state
+  fb_launch_dust_interpolation_only(ctx->k, pp, ctx->st);
+  ctx->launches += 1;
+  CK(cudaStreamSynchronize(ctx->st));
+  CK(cudaGetLastError());
+  ctx->dust_uploaded = 1;
+  return FB_OK;
+}
+
+extern "C" int fb_dust_download(fb_ctx *ctx, fb_dust_state *st)
+{
+  if (!ctx || !st) return FB_ERR_INVALID;
+  if (!ctx->has_dust) return FB_ERR_STATE;
+  PP &pp = ctx->pp;
+  if (st->n != pp.n) return FB_ERR_INVALID;
+  const size_t b = (size_t)pp.n * sizeof(double);
+  double *dst[] = {st->r, st->th, st->vr, st->vth, st->l, st->size, st->stokes};
+  const double *src[] = {pp.r, pp.th, pp.vr, pp.vth, pp.l, pp.size, pp.st};
+  for (int f = 0; f < 7; f++)
+    if (dst[f]) CK(cudaMemcpyAsync(dst[f], src[f], b, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaMemcpyAsync(ctx->h_dc, pp.dc, sizeof(fb_dust_ctl), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  const fb_dust_ctl *h = ctx->h_dc;
+  if (h->err) {
+    set_err(ctx, "particle random stream: too few candidate pairs");
+    return FB_ERR_INVALID;
+  }
+  st->rng_x = h->x;
+  st->kicks = h->kicks;
+  st->carry[0] = h->carry_rad;
+  st->carry[1] = h->carry_phi;
+  st->particles_mass = 0.0;
   return FB_OK;
 }

@@ -81,6 +81,40 @@ struct KP {
   double masstaper;
   int self_gravity;
   int transport_only;      // stage test: Transport without floors/boundaries
+  // Lagrangian particles: grids the gas substep leaves for the next particle
+  // update (IndPotential, RadGradP, AziGradP, RadIndAcc, AziIndAcc,
+  // RadSGAcc, AziSGAcc of src/SourceEuler.c:210-216); NULL without particles
+  double *indpot, *rgp, *agp, *rind, *aind, *rsga, *asga;
+  int particles, dust_feel_planets, dust_feel_disk;
+  // DUSTFEEDBACK: the substep is also bounded by half the particles' minimum
+  // stopping time (SourceEuler.c:1501-1507); NULL otherwise
+  const double *dust_min_ts;
+};
+
+// Device state of the particles' random stream (src/DustUpdate.c:438-485).
+struct fb_dust_ctl {
+  unsigned long long x;        // drand48 state after the last draw
+  long long kicks;             // calls made so far by each Gaussian generator
+  double carry_rad, carry_phi; // their cached second deviates (kicks odd)
+  long long t_start, c_last;   // first pair event of this substep, last candidate used
+  int K, npairs, err, pad;     // kicked particles, accepted pairs needed, shortfall flag
+  double min_ts;               // Minimum_Stopping_Time of the last interpolation (Dsys.c:336,758)
+};
+
+// Particle arrays (structure of arrays in the reference's index order) and
+// the constants of the particle update, passed by value.
+struct PP {
+  int n, ncand;
+  double *r, *th, *vr, *vth, *l, *size, *st;
+  int *flag, *kidx, *kick_bsum, *cand_flag, *cand_bsum;
+  double2 *pairs;
+  fb_dust_ctl *dc;
+  const double *azimuth, *aziinf;  // ns
+  double aziinf0, azisupl, delta_r, delta_phi;
+  double rmin, rmax, unit_mass, inv_unit_length2, dust_density_cu;
+  double aspectratio, thicksmoothing, flaringindex;
+  int log_grid, feel_disk, feel_planets, feel_sg, feel_turb, sfta;
+  int restokes;  // WRITEDUSTDENSITY: interpolation again after the update (SourceEuler.c:526-531)
 };
 
 // launchers (fb_gas.cu)
@@ -111,7 +145,12 @@ struct fb_sg;
 int  fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t s);
 void fb_sg_destroy(fb_sg *sg);
 void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
-void fb_sg_update_velocities(const KP &k, cudaStream_t s);
+// refresh = 1: the Dt = 0 call of main.c:316 on Vrad/Vtheta (fields only)
+void fb_sg_update_velocities(const KP &k, cudaStream_t s, int refresh = 0);
+// Lagrangian particles (fb_dust.cu)
+void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s);
+void fb_launch_dust_interpolation_only(const KP &k, const PP &pp, cudaStream_t s);
+int  fb_dust_launches(const PP &pp);
 int  fb_sg_launches(const fb_sg *sg);  // kernels per fb_sg_accel + update
 void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
 void fb_sg_cols(fb_sg *sg, cudaStream_t s);

@@ -1,0 +1,529 @@
+// fb_dust.cu -- Lagrangian dust particles of AlgoGas (src/SourceEuler.c:504-531)
+// on the GPU: SemiUpdateDustPositions (src/DustUpdate.c:6-265), the TSC
+// interpolation of the gas onto the particles (src/Dsys.c:265-1149) and
+// UpdateDustVelocities (src/DustUpdate.c:267-435).  FP64, one thread per
+// particle, particles kept as a structure of arrays in the reference's index
+// order.  The gas grids are read through L2 (a 256x768 ring set is 1.5 MB a
+// field), so the per-particle stencil gathers are L2 hits.
+//
+// Turbulent kicks and their random stream.  The reference draws the kicks
+// in particle order from the one drand48 stream through two Gaussian
+// generators (myrandn_rad, myrandn_phi, src/DustUpdate.c:438-485), each a
+// Marsaglia polar method that hands out the second deviate of its pair on
+// its next call.  Both are called once per kicked particle, so kick number m
+// (counted over the whole run) takes its radial deviate from accepted pair
+// 2*(m/2) and its azimuthal one from accepted pair 2*(m/2)+1 -- x1 for even
+// m, x2 for odd m -- where "accepted pairs" are the Marsaglia acceptances
+// among consecutive uniform pairs of the stream.  The GPU reproduces that
+// stream exactly: a scan ranks the kicked particles, candidate uniform pairs
+// are drawn in parallel with the LCG's closed-form skip-ahead
+// (X_{n+m} = a^m X_n + c (a^m - 1)/(a - 1) mod 2^48, evaluated by binary
+// powering), the accepted candidates are compacted in stream order, and the
+// stream position is advanced past the last candidate used.
+#include <cuda_runtime.h>
+#include <math.h>
+#include "fb_dev.cuh"
+
+#define D_BS 256
+#define SCAN_BS 1024
+
+static const unsigned long long LCG_A = 0x5DEECE66Dull, LCG_C = 0xBull, M48 = 0xFFFFFFFFFFFFull;
+
+// X_{n+m} from X_n for the drand48 recurrence X <- (a X + c) mod 2^48
+static __device__ __forceinline__ unsigned long long lcg_skip(unsigned long long x, unsigned long long m)
+{
+  unsigned long long A = 1, C = 0, a = LCG_A, c = LCG_C;
+  while (m) {
+    if (m & 1ull) {
+      A = (A * a) & M48;
+      C = (C * a + c) & M48;
+    }
+    c = ((a + 1) * c) & M48;
+    a = (a * a) & M48;
+    m >>= 1;
+  }
+  return (A * x + C) & M48;
+}
+
+// drand48's value of a state: X / 2^48, exact in double
+static __device__ __forceinline__ double u48(unsigned long long x) { return (double)x * 0x1p-48; }
+
+static __device__ __forceinline__ double wrap_azimuth(const PP &pp, double th)
+{
+  // src/DustUpdate.c:44-47 and 130-133
+  if (th < pp.aziinf0) th += (pp.azisupl - pp.aziinf0);
+  if (th > pp.azisupl) th -= (pp.azisupl - pp.aziinf0);
+  return th;
+}
+
+// TSC weight of one axis (src/Dsys.c:451-463)
+static __device__ __forceinline__ double tsc_weight(double d, double delta)
+{
+  double w = 0.0;
+  if (d < 0.5 * delta) w = 0.75 - d * d / delta / delta;
+  if ((d >= 0.5 * delta) && (d <= 1.5 * delta)) w = 0.5 * (1.5 - d / delta) * (1.5 - d / delta);
+  if (d > 1.5 * delta) w = 0.0;
+  return w;
+}
+
+// FViscosity (src/Viscosity.c:23-69) at a particle radius.  The reference's
+// search `while (GlobalRmed[i] < rad) i++` has no upper bound and runs past
+// the last ring for radii beyond Rmed[nr-1]; here it stops at the last ring.
+static __device__ double viscosity_at(const KP &k, double rad)
+{
+  if (k.visc_mode == 1) {
+    int i = 0;
+    while (i < k.nr - 1 && k.rmed[i] < rad) i++;
+    return k.alpha * k.gcs[i] * k.gcs[i] * pow(rad, 1.5);
+  }
+  return (k.visc_mode == 2) ? k.nu_const : 0.0;
+}
+
+// Stokes number with the Paardekooper (2007) drag law (src/Dsys.c:724-764).
+// pow(x,2.0) and pow(x,-1.0) are written as the product and the reciprocal
+// the reference's compiler turns them into.  AspectRatio(rp) is ASPECTRATIO
+// for the supported parameter set (TRANSITIONRATIO = 1, LAMBDADOUBLING = 0).
+static __device__ double stokes_number(const PP &pp, double size, double rp, double vrp, double vtp,
+                                       double vrg, double vtg, double csg, double densg)
+{
+  const double densg_cgs = 0.1 * densg * pp.unit_mass * pp.inv_unit_length2;
+  const double lambda = 3.34e-8 * (1.0 / densg_cgs) * pp.aspectratio * rp;
+  const double Kn = 0.5 * lambda / size;
+  const double Mach = sqrt((vrp - vrg) * (vrp - vrg) + (vtp - vtg) * (vtp - vtg)) / csg;
+  const double f_D = sqrt(1.0 + 9.0 * M_PI * Mach * Mach / 128.0);
+  const double Re = 3.0 * sqrt(FB_PI / 8.0) * Mach / Kn;
+  double k_D = 0.0;
+  if (Re <= 500.0) {
+    k_D = 1.0 + 0.15 * pow(Re, 0.687);
+  } else {
+    if ((Re > 500.0) && (Re <= 1500.0)) k_D = 3.96e-6 * pow(Re, 2.4);
+    if (Re > 1500.0) k_D = 0.11 * Re;
+  }
+  const double a3 = 3.0 * Kn + 1.0;
+  const double Cdrag = (a3 * a3) * (1.0 / (9.0 * Kn * Kn * f_D + 3.0 * Kn * k_D));
+  return 0.5 * M_PI * Cdrag * size * pp.dust_density_cu / densg;
+}
+
+// ---------------------------------------------------- 1. drift and flags
+// SemiUpdateDustPositions with timestep = 2 dt, drift part (DustUpdate.c:30-56).
+// flag = the particle gets a turbulent kick in this substep.
+__global__ void __launch_bounds__(D_BS) k_dust_drift(KP k, PP pp)
+{
+  const int q = blockIdx.x * D_BS + threadIdx.x;
+  if (q == 0) pp.dc->min_ts = 1e6;  // reset by every interpolation call (Dsys.c:336)
+  if (q >= pp.n) return;
+  const double timestep = 2.0 * k.ctl->dt;
+  const double rinf0 = k.rinf[0], rsupl = k.rsup[k.nr - 1];
+  const double r = pp.r[q];
+  int flag = 0;
+  if ((r >= rinf0) && (r < rsupl)) {
+    const double rn = r + pp.vr[q] * 0.5 * timestep;
+    double th = pp.th[q] + pp.vth[q] * r * 0.25 * timestep * (pow(r, -2.) + pow(rn, -2.));
+    th = wrap_azimuth(pp, th);
+    flag = (pp.feel_turb && (rn >= rinf0) && (rn <= rsupl)) ? 1 : 0;
+    if (!flag) th = wrap_azimuth(pp, th);
+    pp.r[q] = rn;
+    pp.th[q] = th;
+  }
+  pp.flag[q] = flag;
+}
+
+// ------------------------------------------------------- 2. scans
+static __device__ __forceinline__ int warp_incl_scan(int x)
+{
+  const int lane = threadIdx.x & 31;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  return x;
+}
+
+// exclusive scan of SCAN_BS ints per block; block totals to blocksum
+__global__ void __launch_bounds__(SCAN_BS) k_scan_block(const int *in, int *out, int *blocksum, int n)
+{
+  __shared__ int sh[SCAN_BS / 32];
+  const int g = blockIdx.x * SCAN_BS + threadIdx.x;
+  const int v = (g < n) ? in[g] : 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int x = warp_incl_scan(v);
+  if (lane == 31) sh[w] = x;
+  __syncthreads();
+  if (w == 0) sh[lane] = warp_incl_scan(sh[lane]);  // SCAN_BS / 32 == 32 warps
+  __syncthreads();
+  const int warp_off = (w > 0) ? sh[w - 1] : 0;
+  if (g < n) out[g] = warp_off + x - v;
+  if (threadIdx.x == SCAN_BS - 1) blocksum[blockIdx.x] = sh[SCAN_BS / 32 - 1];
+}
+
+// exclusive scan of nb block sums in place by one CTA of SCAN_BS threads;
+// returns the total (valid in every thread)
+static __device__ int scan_top(int *blocksum, int nb)
+{
+  __shared__ int sh[SCAN_BS / 32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int base = 0; base < nb; base += SCAN_BS) {
+    const int g = base + threadIdx.x;
+    const int v = (g < nb) ? blocksum[g] : 0;
+    const int x = warp_incl_scan(v);
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) sh[lane] = warp_incl_scan(sh[lane]);
+    __syncthreads();
+    const int warp_off = (w > 0) ? sh[w - 1] : 0;
+    const int c0 = carry;
+    if (g < nb) blocksum[g] = c0 + warp_off + x - v;
+    __syncthreads();
+    if (threadIdx.x == 0) carry = c0 + sh[SCAN_BS / 32 - 1];
+    __syncthreads();
+  }
+  return carry;
+}
+
+// Number of kicked particles K of this substep and the accepted pairs it needs.
+__global__ void __launch_bounds__(SCAN_BS) k_kick_top(PP pp, int nb)
+{
+  const int K = scan_top(pp.kick_bsum, nb);
+  if (threadIdx.x == 0) {
+    fb_dust_ctl *d = pp.dc;
+    const long long G = d->kicks;
+    d->K = K;
+    d->t_start = (G + 1) / 2;  // first pair event not served by the carry
+    long long E = 0;
+    if (K > 0) {
+      E = (G + K - 1) / 2 - d->t_start + 1;
+      if (E < 0) E = 0;
+    }
+    d->npairs = (int)(2 * E);
+  }
+}
+
+// ------------------------------------------------ 3. Gaussian pairs
+// Candidate c takes the uniforms X_{cur+2c+1}, X_{cur+2c+2} of the stream;
+// Marsaglia's test of src/DustUpdate.c:449-454 (pow(u,2.0) is u*u).
+static __device__ __forceinline__ bool candidate(unsigned long long xcur, long long c, double *u1, double *u2, double *w)
+{
+  const unsigned long long x1 = lcg_skip(xcur, (unsigned long long)(2 * c + 1));
+  const unsigned long long x2 = (LCG_A * x1 + LCG_C) & M48;
+  *u1 = 2.0 * u48(x1) - 1.0;
+  *u2 = 2.0 * u48(x2) - 1.0;
+  *w = (*u1) * (*u1) + (*u2) * (*u2);
+  return !(*w >= 1.0 || *w == 0.0);
+}
+
+// Candidates examined this substep: enough that the accepted ones (rate pi/4)
+// cover npairs with a margin of many standard deviations.
+static __device__ __forceinline__ long long candidate_limit(const PP &pp, int npairs)
+{
+  const long long lim = (long long)npairs * 27 / 20 + 2048;
+  return lim < pp.ncand ? lim : pp.ncand;
+}
+
+__global__ void __launch_bounds__(D_BS) k_rng_count(PP pp)
+{
+  __shared__ int sh[D_BS / 32];
+  const long long c = (long long)blockIdx.x * D_BS + threadIdx.x;
+  const int npairs = pp.dc->npairs;
+  int acc = 0;
+  if (npairs > 0 && c < candidate_limit(pp, npairs)) {
+    double u1, u2, w;
+    acc = candidate(pp.dc->x, c, &u1, &u2, &w) ? 1 : 0;
+  }
+  if (c < pp.ncand) pp.cand_flag[c] = acc;
+  const int cnt = __popc(__ballot_sync(0xffffffffu, acc));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int s = 0;
+    for (int q = 0; q < D_BS / 32; q++) s += sh[q];
+    pp.cand_bsum[blockIdx.x] = s;
+  }
+}
+
+__global__ void __launch_bounds__(SCAN_BS) k_rng_top(KP k, PP pp, int nb)
+{
+  const int total = scan_top(pp.cand_bsum, nb);
+  if (threadIdx.x == 0) {
+    fb_dust_ctl *d = pp.dc;
+    if (d->npairs > total) {
+      // never silently wrong: the step stops with an error status
+      d->err = 1;
+      d->npairs = total;
+      k.ctl->status = FB_ERR_INVALID;
+    }
+  }
+}
+
+// Accepted candidate number g (in stream order) becomes pair g.
+__global__ void __launch_bounds__(D_BS) k_rng_scatter(PP pp)
+{
+  __shared__ int wc[D_BS / 32];
+  const long long c = (long long)blockIdx.x * D_BS + threadIdx.x;
+  const int npairs = pp.dc->npairs;
+  const int acc = (npairs > 0 && c < pp.ncand) ? pp.cand_flag[c] : 0;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const unsigned b = __ballot_sync(0xffffffffu, acc);
+  if (lane == 0) wc[w] = __popc(b);
+  __syncthreads();
+  int off = 0;
+  for (int q = 0; q < w; q++) off += wc[q];
+  const int g = pp.cand_bsum[blockIdx.x] + off + __popc(b & ((1u << lane) - 1u));
+  if (acc && g < npairs) {
+    double u1, u2, ww;
+    candidate(pp.dc->x, c, &u1, &u2, &ww);
+    const double mult = sqrt((-2.0 * log(ww)) / ww);
+    pp.pairs[g] = make_double2(u1 * mult, u2 * mult);
+    if (g == npairs - 1) pp.dc->c_last = c;
+  }
+}
+
+// Minimum_Stopping_Time (Dsys.c:757-759): positive doubles order like their
+// bit patterns, so an integer atomicMin on the bits is a min on the values.
+static __device__ __forceinline__ void record_stopping_time(const PP &pp, double Ts)
+{
+  if (Ts >= 0.0) atomicMin((long long *)&pp.dc->min_ts, __double_as_longlong(Ts));
+}
+
+// ----------------------------------- 4. kicks, interpolation, velocities
+// mode 0: one substep (kick, interpolation, UpdateDustVelocities, and the
+// second interpolation of SourceEuler.c:529-530 when WRITEDUSTDENSITY);
+// mode 1: the interpolation call of main.c:287 (Stokes numbers only).
+__global__ void __launch_bounds__(D_BS) k_dust_update(KP k, PP pp, int mode)
+{
+  const int q = blockIdx.x * D_BS + threadIdx.x;
+  if (q >= pp.n) return;
+  const int ns = k.ns, nr = k.nr;
+  const double rinf0 = k.rinf[0], rsupl = k.rsup[nr - 1];
+  double r = pp.r[q], th = pp.th[q];
+  // ---- turbulent kick (DustUpdate.c:56-105, Charnoz et al. 2011 eq. 21)
+  if (mode == 0 && pp.flag[q]) {
+    const double timestep = 2.0 * k.ctl->dt;
+    const double St = pp.st[q];
+    const double visc = viscosity_at(k, r);
+    const double D_dust = visc * (1.0 + 4.0 * (St * St)) * pow(1. + St * St, -2.0);
+    int ip = 0;
+    if (r >= k.rinf[ip]) {
+      while ((r >= k.rinf[ip]) && (ip <= nr - 1)) ip++;
+    }
+    ip--;
+    int jp = (int)floor(ns * (th - pp.aziinf0) / (pp.azisupl - pp.aziinf0));
+    if (jp == ns) jp = 0;
+    jp = min(max(jp, 0), ns - 1);
+    const size_t lp = (size_t)ip * ns + jp;
+    const size_t lpm1 = (ip != 0) ? lp - ns : lp;
+    const size_t lpjm = (jp == 0) ? (size_t)ip * ns + ns - 1 : lp - 1;
+    // this particle's deviates (see the head of the file)
+    const fb_dust_ctl *d = pp.dc;
+    const long long M = d->kicks + pp.kidx[q] + pp.kick_bsum[q / SCAN_BS];
+    const long long t = M / 2;
+    const int odd = (int)(M & 1ll);
+    double xr, xp;
+    if (t < d->t_start) {
+      xr = d->carry_rad;
+      xp = d->carry_phi;
+    } else {
+      const long long e = t - d->t_start;
+      const double2 pr = pp.pairs[2 * e], pf = pp.pairs[2 * e + 1];
+      xr = odd ? pr.y : pr.x;
+      xp = odd ? pf.y : pf.x;
+    }
+    const double dens_lp = k.rho[lp];
+    const double dr_mean = D_dust / dens_lp * (dens_lp - k.rho[lpm1]) * k.invdiffrmed[ip] * timestep;
+    const double sigma_r_squared = 2.0 * D_dust * timestep;
+    r = r + (dr_mean + sqrt(sigma_r_squared) * xr);
+    const double dxtheta = (k.pmax - k.pmin) / (double)ns * k.rmed[ip];
+    const double invdxtheta = 1.0 / dxtheta;
+    const double dphi_mean = D_dust / dens_lp * (dens_lp - k.rho[lpjm]) * invdxtheta * timestep / r;
+    th = th + (dphi_mean + sqrt(sigma_r_squared) / r * xp);
+    th = wrap_azimuth(pp, th);
+    pp.r[q] = r;
+    pp.th[q] = th;
+  }
+  if (!((r >= rinf0) && (r < rsupl))) return;
+  // ---- 1) cell of the particle (Dsys.c:363-372)
+  const double rp = r, tp = th;
+  int ip = 0;
+  while (rp >= k.rinf[ip]) ip++;
+  ip--;
+  int jp = (int)floor(ns * (tp - pp.aziinf0) / (pp.azisupl - pp.aziinf0));
+  if (jp == ns) jp = 0;
+  jp = min(max(jp, 0), ns - 1);
+  const double delta_phi = pp.delta_phi, delta_r = pp.delta_r;
+  const int want_sg = k.self_gravity && pp.feel_sg;
+  double vrg = 0.0, rgp = 0.0, rind = 0.0, rsg = 0.0;
+  double vtg = 0.0, agp = 0.0, aind = 0.0, asg = 0.0;
+  double densg = 0.0, csg = 0.0;
+  // ---- 2a) vrad-staggered values: (Rinf[i], Azimuth[j]) (Dsys.c:397-487)
+  for (int j = jp - 1; j <= jp + 1; j++) {
+    int myj;
+    double myaz;
+    if (j >= 0 && j < ns) { myj = j; myaz = pp.azimuth[j]; }
+    else if (j < 0) { myj = j + ns; myaz = pp.azimuth[0] + j * delta_phi; }
+    else { myj = j - ns; myaz = pp.azimuth[ns - 1] + (j + 1 - ns) * delta_phi; }
+    const double wt = tsc_weight(fabs(tp - myaz), delta_phi);
+    for (int i = ip - 1; i <= ip + 1; i++) {
+      if (i < 0 || i > nr - 1) continue;
+      const double dr = pp.log_grid ? fabs(log(rp / k.rinf[i])) : fabs(rp - k.rinf[i]);
+      const double wr = tsc_weight(dr, delta_r);
+      const size_t l = (size_t)i * ns + myj;
+      vrg += (wr * wt * k.vr[l]);
+      rgp += (wr * wt * k.rgp[l]);
+      if (k.indirect_term) rind += (wr * wt * k.rind[l]);
+      if (want_sg) rsg += (wr * wt * k.rsga[l]);
+    }
+  }
+  // ---- 2b) vtheta-staggered values: (Rmed[i], AziInf[j]) (Dsys.c:510-588)
+  {
+    const int myjp = (tp > pp.azimuth[jp]) ? jp + 1 : jp;
+    for (int j = myjp - 1; j <= myjp + 1; j++) {
+      int myj;
+      double myaz;
+      if (j >= 0 && j < ns) { myj = j; myaz = pp.aziinf[j]; }
+      else if (j < 0) { myj = j + ns; myaz = pp.aziinf[0] + j * delta_phi; }
+      else { myj = j - ns; myaz = pp.aziinf[ns - 1] + (j + 1 - ns) * delta_phi; }
+      const double wt = tsc_weight(fabs(tp - myaz), delta_phi);
+      for (int i = ip - 1; i <= ip + 1; i++) {
+        if (i < 0 || i > nr - 1) continue;
+        const double dr = pp.log_grid ? fabs(log(rp / k.rmed[i])) : fabs(rp - k.rmed[i]);
+        const double wr = tsc_weight(dr, delta_r);
+        const size_t l = (size_t)i * ns + myj;
+        // the reference adds Rmed*OmegaFrame to vtheta around the call; the
+        // supported frame is non-rotating (OmegaFrame = 0)
+        vtg += (wr * wt * k.vt[l]);
+        agp += (wr * wt * k.agp[l]);
+        if (k.indirect_term) aind += (wr * wt * k.aind[l]);
+        if (want_sg) asg += (wr * wt * k.asga[l]);
+      }
+    }
+  }
+  // ---- 2c) cell-centred values: (Rmed[i], Azimuth[j]) (Dsys.c:617-711).
+  // The dust deposit of this loop is Particles_Mass times the weights; the
+  // particle mass is zero without a dust fluid (main.c:187-200), so there
+  // is nothing to deposit.
+  for (int j = jp - 1; j <= jp + 1; j++) {
+    int myj;
+    double myaz;
+    if (j >= 0 && j < ns) { myj = j; myaz = pp.azimuth[j]; }
+    else if (j < 0) { myj = j + ns; myaz = pp.azimuth[0] + j * delta_phi; }
+    else { myj = j - ns; myaz = pp.azimuth[ns - 1] + (j + 1 - ns) * delta_phi; }
+    const double wt = tsc_weight(fabs(tp - myaz), delta_phi);
+    for (int i = ip - 1; i <= ip + 1; i++) {
+      if (i < 0 || i > nr - 1) continue;
+      const double dr = pp.log_grid ? fabs(log(rp / k.rmed[i])) : fabs(rp - k.rmed[i]);
+      const double wr = tsc_weight(dr, delta_r);
+      const size_t l = (size_t)i * ns + myj;
+      densg += (wr * wt * k.rho[l]);
+      csg += (wr * wt * k.cs[l]);
+    }
+  }
+  const double size = pp.size[q];
+  const double vrd = pp.vr[q], vtd = pp.vth[q];
+  const double St = stokes_number(pp, size, rp, vrd, vtd, vrg, vtg, csg, densg);
+  if (mode == 1) {
+    pp.st[q] = St;
+    record_stopping_time(pp, St * pow(rp, 1.5));
+    return;
+  }
+  // ---- UpdateDustVelocities (DustUpdate.c:301-428), first-order integrator
+  const double dt = k.ctl->dt;
+  const double rd = rp, td = tp;
+  int LocalDustFeelDisk = pp.feel_disk;
+  if ((rd < pp.rmin) || (rd > pp.rmax)) LocalDustFeelDisk = 0;
+  const double stoptime = St * pow(rd, 1.5);
+  double vr_new, vth_new;
+  if ((stoptime < dt) && pp.sfta) {
+    // short-friction-time approximation
+    vr_new = vrg + stoptime * rgp / densg;
+    vth_new = vtg + stoptime * agp / densg;
+    pp.l[q] = rd * vth_new;
+  } else {
+    // semi-implicit integrator
+    double FgravR = -pow(rd, -2.);
+    double FgravTh = 0.;
+    if ((fabs(FgravR + vtd * vtd / rd) < 1e-15) && (!pp.feel_planets) && (!pp.feel_disk) && (!pp.feel_sg))
+      FgravR = -vtd * vtd / rd;
+    if (pp.feel_planets) {
+      const fb_ctl *c = k.ctl;
+      for (int p = 0; p < c->np; p++) {
+        const double xp = c->px[p], yp = c->py[p];
+        const double rpl = sqrt(xp * xp + yp * yp);
+        const double tpl = atan2(yp, xp);
+        const double mp = c->pm[p];
+        const double eps = pp.thicksmoothing * pp.aspectratio * pow(0.5 * rpl, 1.0 + pp.flaringindex) *
+                           pow(2.0, 1.0 + pp.flaringindex);
+        const double d = sqrt(rd * rd + rpl * rpl - 2.0 * rd * rpl * cos(td - tpl) + eps * eps);
+        FgravR += mp * (rpl * cos(td - tpl) - rd) * pow(d, -3.0);
+        FgravTh += -mp * rpl * sin(td - tpl) * pow(d, -3.0);
+      }
+    }
+    if (k.indirect_term) {
+      FgravR += rind;
+      FgravTh += aind;
+    }
+    if (k.self_gravity && pp.feel_sg) {
+      FgravR += rsg;
+      FgravTh += asg;
+    }
+    const double den = 1.0 + LocalDustFeelDisk * dt / stoptime;
+    const double numTh = (vtd - vtg) + dt * (FgravTh - vrd * vtd / rd);
+    vth_new = vtg + numTh / den;
+    const double numR = (vrd - vrg) + dt * (FgravR + (vth_new * vth_new) / rd);
+    vr_new = vrg + numR / den;
+  }
+  pp.vr[q] = vr_new;
+  pp.vth[q] = vth_new;
+  // the interpolation after RotateDsys recomputes the Stokes number with the
+  // updated velocities; the next substep's kick uses that one
+  const double St_out = pp.restokes ? stokes_number(pp, size, rp, vr_new, vth_new, vrg, vtg, csg, densg) : St;
+  pp.st[q] = St_out;
+  record_stopping_time(pp, pp.restokes ? St_out * pow(rp, 1.5) : stoptime);
+}
+
+// ----------------------------------------------------- 5. bookkeeping
+__global__ void k_dust_finish(PP pp)
+{
+  fb_dust_ctl *d = pp.dc;
+  const long long G = d->kicks, K = d->K;
+  if (d->npairs > 0) d->x = lcg_skip(d->x, (unsigned long long)(2 * (d->c_last + 1)));
+  if (K > 0 && ((G + K) & 1ll)) {
+    // an odd number of calls in total: each generator keeps the second
+    // deviate of its last pair for its next call
+    const long long e = (G + K - 1) / 2 - d->t_start;
+    if (e >= 0) {
+      d->carry_rad = pp.pairs[2 * e].y;
+      d->carry_phi = pp.pairs[2 * e + 1].y;
+    }
+  }
+  d->kicks = G + K;
+  d->K = 0;
+  d->npairs = 0;
+}
+
+// ---------------------------------------------------------- launchers
+int fb_dust_launches(const PP &pp) { return pp.feel_turb ? 8 : 2; }
+
+void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s)
+{
+  const int nb = (pp.n + D_BS - 1) / D_BS;
+  k_dust_drift<<<nb, D_BS, 0, s>>>(k, pp);
+  if (pp.feel_turb) {
+    const int nsb = (pp.n + SCAN_BS - 1) / SCAN_BS;
+    k_scan_block<<<nsb, SCAN_BS, 0, s>>>(pp.flag, pp.kidx, pp.kick_bsum, pp.n);
+    k_kick_top<<<1, SCAN_BS, 0, s>>>(pp, nsb);
+    const int ncb = (pp.ncand + D_BS - 1) / D_BS;
+    k_rng_count<<<ncb, D_BS, 0, s>>>(pp);
+    k_rng_top<<<1, SCAN_BS, 0, s>>>(k, pp, ncb);
+    k_rng_scatter<<<ncb, D_BS, 0, s>>>(pp);
+  }
+  k_dust_update<<<nb, D_BS, 0, s>>>(k, pp, 0);
+  if (pp.feel_turb) k_dust_finish<<<1, 1, 0, s>>>(pp);
+}
+
+void fb_launch_dust_interpolation_only(const KP &k, const PP &pp, cudaStream_t s)
+{
+  const int nb = (pp.n + D_BS - 1) / D_BS;
+  k_dust_update<<<nb, D_BS, 0, s>>>(k, pp, 1);
+}

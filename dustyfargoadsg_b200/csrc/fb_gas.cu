@@ -295,6 +295,11 @@ __global__ void __launch_bounds__(FB_BS) k_controller(KP k)
   // ConditionCFL reduction (SourceEuler.c:1336-1497) and substep count
   const double deltaT = c->DT - c->dtemp;
   double newdt = newdt_cells;
+  if (k.dust_min_ts) {  // SourceEuler.c:1501-1507
+    double dt_fb = 0.5 * *k.dust_min_ts;
+    if (dt_fb == 0.0) dt_fb = 1e10;
+    if (dt_fb < newdt) newdt = dt_fb;
+  }
   if (deltaT < newdt) newdt = deltaT;
   const double ncfl = ceil(deltaT / newdt);
   if (!(ncfl >= 1.0) || ncfl > 2.0e9) {
@@ -441,22 +446,30 @@ __global__ void __launch_bounds__(FB_BS2) k_potential(KP k)
     const size_t l = (size_t)i * k.ns + j;
     const double x = k.rmed[i] * k.cosaz[j];
     const double y = k.rmed[i] * k.sinaz[j];
-    double P = 0.0;
+    double P = 0.0, IP = 0.0;
     for (int p = 0; p < np; p++) {
       const double xplanet = c->pot_x[p], yplanet = c->pot_y[p], mplanet = c->pot_m[p];
       double distance = (x - xplanet) * (x - xplanet) + (y - yplanet) * (y - yplanet);
       double distancesmooth = sqrt(distance + c->pot_smooth2[p]);
       double pot = -FB_G * mplanet / distancesmooth;
-      if (k.indirect_term) pot += FB_G * mplanet * c->pot_invd3[p] * (x * xplanet + y * yplanet);
+      if (k.indirect_term) {
+        const double ind = FB_G * mplanet * c->pot_invd3[p] * (x * xplanet + y * yplanet);
+        pot += ind;
+        if (k.dust_feel_planets) IP = ind;  // Pframeforce.c:102-103 assigns, last planet wins
+      }
       P += pot;
     }
     {
       const double InvDistance = 1.0 / k.rmed[i];
       double pot = -FB_G * 1.0 * InvDistance;
-      if (use_ind) pot -= c->ind_x * x + c->ind_y * y;
+      if (use_ind) {
+        pot -= c->ind_x * x + c->ind_y * y;
+        if (k.dust_feel_disk) IP -= c->ind_x * x + c->ind_y * y;
+      }
       P += pot;
     }
     k.pot[l] = P;
+    if (k.particles) k.indpot[l] = IP;  // IndPotential (Pframeforce.c:55-121)
   }
 }
 
@@ -496,6 +509,10 @@ __global__ void __launch_bounds__(FB_BS2) k_substep1(KP k)
       vt2 = vt2 / 4.0 + k.rinf[i] * k.omega_frame;
       vt2 = vt2 * vt2;
       k.vri[l] = k.vr[l] + dt * (-gradp - gradphi + vt2 * k.invrinf[i]);
+      if (k.particles) {  // RadGradP, RadIndAcc (SourceEuler.c:875-877)
+        k.rgp[l] = (Pl - Plim) * k.invdiffrmed[i];
+        k.rind[l] = -(k.indpot[l] - k.indpot[lim]) * k.invdiffrmed[i];
+      }
     }
     {
       const double Pjm = pressure_at(k, ljm);
@@ -505,6 +522,10 @@ __global__ void __launch_bounds__(FB_BS2) k_substep1(KP k)
       double vti = k.vt[l] - dt * (gradp + gradphi);
       vti += dt * k.supp_torque[i];
       k.vti[l] = vti;
+      if (k.particles) {  // AziGradP, AziIndAcc (SourceEuler.c:944-951)
+        k.agp[l] = (Pl - Pjm) * invdxtheta;
+        k.aind[l] = -(k.indpot[l] - k.indpot[ljm]) * invdxtheta;
+      }
     }
   }
 }

@@ -104,7 +104,9 @@ int fb_params_default(fb_params *p)
   p->dust_feel_planets = 1;
   p->dust_feel_turb = 0;
   p->dust_feedback = 0;
+  p->dust_feel_sg = 1;
   p->sfta = 1;
+  p->write_dust_density = 0;
   p->interpolation = 2;
   strcpy(p->planetconfig, "Systems/SolarSystem.cfg");
   strcpy(p->outputdir, "~masset");
@@ -324,9 +326,21 @@ int fb_params_read_par(fb_params *p, const char *path)
   if (is_c(c, 'N')) p->interpolation = 0;
   if (is_c(c, 'C')) p->interpolation = 1;
   if (is_c(c, 'T')) p->interpolation = 2;
-  if (p->nbpart != 0) p->unsupported |= FB_U_PARTICLES;
   if (p->nbpart != 0 && is_c(kv_c(&set, "NODTCONSTRAINTBYPCS", 'Y'), 'N'))
     p->unsupported |= FB_U_DUSTTIMESTEP;
+  if (p->nbpart != 0) {
+    /* particle options outside this build */
+    if (is_c(kv_c(&set, "ZZINTEGRATOR", 'N'), 'Y')) p->unsupported |= FB_U_ZZINTEGRATOR;
+    if (is_c(kv_c(&set, "DUSTGROWTH", 'N'), 'Y')) p->unsupported |= FB_U_DUSTGROWTH;
+    if (is_c(kv_c(&set, "REMOVEDUSTFROMPLANETSHILLRADIUS", 'N'), 'Y')) p->unsupported |= FB_U_HILLREMOVAL;
+    if (p->interpolation != 2) p->unsupported |= FB_U_INTERPOLATION;
+    if (is_c(kv_c(&set, "DUSTFEELSG", 'Y'), 'Z')) p->unsupported |= FB_U_DUSTSGZERO;
+    if (p->omegaframe != 0.0) p->unsupported |= FB_U_COROTATING;
+  }
+  if (is_c(kv_c(&set, "DUSTFEELSG", 'Y'), 'N')) p->dust_feel_sg = 0;
+  if (!is_c(kv_c(&set, "WRITEDUSTDENSITY", 'N'), 'N')) p->write_dust_density = 1;  /* Interpret.c:255-258 */
+  if (p->nbpart != 0 && p->self_gravity && is_c(kv_c(&set, "SOFTWRITING", 'N'), 'Y'))
+    p->unsupported |= FB_U_SOFTWRITING;
   if (p->alphaviscosity != 0.0 && p->viscosity != 0.0) ok = FB_ERR_INVALID; /* Interpret.c:453-459 */
   if (p->self_gravity && p->sgthicknesssmoothing == 0.0) ok = FB_ERR_INVALID;
   if (p->evanescent && (p->wkzrmin == 0.0 || p->wkzrmax == 0.0)) ok = FB_ERR_INVALID;
@@ -357,6 +371,10 @@ const char *fb_unsupported_name(const fb_params *p)
     {FB_U_ADDNOISE, "AddNoise (wall-clock seeded)"}, {FB_U_PLANETACCRETION, "planet accretion"},
     {FB_U_FEELDISK, "planets feeling the disc"}, {FB_U_BINARY, "binary planets"},
     {FB_U_FEELOTHERS_FC, "FeelOthers with ForcedCircular"},
+    {FB_U_ZZINTEGRATOR, "ZZIntegrator"},
+    {FB_U_DUSTGROWTH, "DustGrowth"}, {FB_U_HILLREMOVAL, "RemoveDustFromPlanetsHillRadius"},
+    {FB_U_INTERPOLATION, "NGP/CIC particle interpolation"}, {FB_U_DUSTSGZERO, "DustFeelSG Z"},
+    {FB_U_SOFTWRITING, "SoftWriting with particles and self-gravity"},
   };
   size_t k;
   if (!p) return "";
@@ -696,6 +714,97 @@ done:
   return rc;
 }
 
+/* ComputeCodeUnits (src/LowTasks.c:202-213) */
+double fb_unit_length(const fb_params *p) { return 1.49598e11 * p->factorunitlength; }
+double fb_unit_mass(const fb_params *p) { return 1.9891e30 * p->factorunitmass; }
+
+/* InitDustSystem (src/Dsys.c:128-262), new particles, one process. */
+int fb_init_dust(const fb_params *p, fb_ctx *ctx, long seed, fb_dust_state *st)
+{
+  fb_geom gl, *g;
+  const fb_geom *gc = ctx ? fb_ctx_geom(ctx) : NULL;
+  fb_rand48 r48;
+  double C1, C2, rmindust, rmaxdust, aziinf0, azisupl, unit_length;
+  double *axisg = NULL;
+  int i, n, rc;
+  if (!p || !st || !st->r || !st->th || !st->vr || !st->vth || !st->l || !st->size || !st->stokes)
+    return FB_ERR_INVALID;
+  n = p->nbpart;
+  if (n <= 0 || st->n != n) return FB_ERR_INVALID;
+  if (p->self_gravity && !ctx) return FB_ERR_INVALID;
+  if (p->sizeminpart == p->sizemaxpart && p->sizepartslope != 0.0) return FB_ERR_INVALID;  /* Dsys.c:151-155 */
+  if (gc) {
+    g = (fb_geom *)gc;
+  } else {
+    rc = fb_geom_fill(p, NULL, &gl);
+    if (rc) return rc;
+    g = &gl;
+  }
+  unit_length = fb_unit_length(p);
+  rmindust = (p->rmindust == 0.0) ? p->rmin : p->rmindust;
+  rmaxdust = (p->rmaxdust == 0.0) ? p->rmax : p->rmaxdust;
+  /* AziInf[0], AziSup[NSEC-1] (src/SourceEuler.c:176-179) */
+  aziinf0 = g->azimuth[0] - 0.5 * (p->pmax - p->pmin) / (double)p->nsec;
+  azisupl = g->azimuth[p->nsec - 1] + 0.5 * (p->pmax - p->pmin) / (double)p->nsec;
+  fb_srand48(&r48, seed);
+  if (p->sizeminpart != p->sizemaxpart) {
+    if (p->sizepartslope != 1.0) {
+      C1 = pow(p->sizemaxpart, 1.0 - p->sizepartslope);
+      C2 = pow(p->sizeminpart, 1.0 - p->sizepartslope);
+      for (i = 0; i < n; i++)
+        st->size[i] = pow(C2 + (C1 - C2) * fb_drand48(&r48), 1.0 / (1.0 - p->sizepartslope)) / unit_length;
+    } else {
+      for (i = 0; i < n; i++)
+        st->size[i] = p->sizeminpart * exp(fb_drand48(&r48) * log(p->sizemaxpart / p->sizeminpart)) / unit_length;
+    }
+  } else {
+    for (i = 0; i < n; i++) st->size[i] = p->sizeminpart / unit_length;
+  }
+  if (p->dustslope != 1.0) {
+    C1 = pow(rmaxdust, 1.0 - p->dustslope);
+    C2 = pow(rmindust, 1.0 - p->dustslope);
+    for (i = 0; i < n; i++) st->r[i] = pow(C2 + (C1 - C2) * fb_drand48(&r48), 1.0 / (1.0 - p->dustslope));
+  } else {
+    for (i = 0; i < n; i++) st->r[i] = rmindust * exp(fb_drand48(&r48) * log(rmaxdust / rmindust));
+  }
+  for (i = 0; i < n; i++) st->th[i] = aziinf0 + fb_drand48(&r48) * (azisupl - aziinf0);
+  if (p->self_gravity) {
+    axisg = (double *)calloc(p->nrad, sizeof(double));
+    if (!axisg) { rc = FB_ERR_NOMEM; goto done; }
+    rc = fb_sg_axisym_accel_device(ctx, axisg);
+    if (rc) goto done;
+  }
+  for (i = 0; i < n; i++) {
+    st->vr[i] = 0.0;
+    st->stokes[i] = 0.0;
+    if (!p->self_gravity) {
+      st->vth[i] = pow(st->r[i], -0.5);
+    } else {
+      double dist = st->r[i], ri, rip1, dr, sgacc;
+      int ipl = 0;
+      while ((g->rmed[ipl] <= dist) && (ipl < p->nrad - 2)) ipl++;
+      ri = g->rmed[ipl];
+      rip1 = g->rmed[ipl + 1];
+      dr = rip1 - ri;
+      sgacc = (dist - ri) * axisg[ipl + 1] + (rip1 - dist) * axisg[ipl];
+      sgacc /= dr;
+      st->vth[i] = pow(st->r[i], -0.5) * sqrt(1.0 - dist * dist * sgacc);
+    }
+    st->l[i] = st->r[i] * st->vth[i];
+  }
+  st->rng_x = r48.x;
+  st->kicks = 0;
+  st->carry[0] = st->carry[1] = 0.0;
+  /* Particles_Mass: the dust surface density is only initialised with a
+     dust fluid, so it is zero here (main.c:167-200) */
+  st->particles_mass = 0.0;
+  rc = FB_OK;
+done:
+  free(axisg);
+  if (!gc) fb_geom_free(&gl);
+  return rc;
+}
+
 int fb_struct_size(int which)
 {
   switch (which) {
@@ -704,6 +813,7 @@ int fb_struct_size(int which)
     case 2: return (int)sizeof(fb_state);
     case 3: return (int)sizeof(fb_profiles);
     case 4: return (int)sizeof(fb_step_report);
+    case 5: return (int)sizeof(fb_dust_state);
     default: return -1;
   }
 }

@@ -53,6 +53,12 @@ extern "C" {
 #define FB_U_FEELDISK         (1ull << 33)
 #define FB_U_BINARY           (1ull << 34)
 #define FB_U_FEELOTHERS_FC    (1ull << 35)
+#define FB_U_ZZINTEGRATOR     (1ull << 37)
+#define FB_U_DUSTGROWTH       (1ull << 38)
+#define FB_U_HILLREMOVAL      (1ull << 39)
+#define FB_U_INTERPOLATION    (1ull << 40)
+#define FB_U_DUSTSGZERO       (1ull << 41)
+#define FB_U_SOFTWRITING      (1ull << 42)
 
 /* 1-D geometry of FillPolar1DArrays (src/SourceEuler.c:71-188) for one
  * process holding all rings (IMIN = 0, GLOBALNRAD = NRAD). */
@@ -84,6 +90,11 @@ double fb_drand48(fb_rand48 *s);
  * radial SG acceleration of dens (host array) on the device and returns its
  * azimuthal means (GLOBAL_AxiSGAccr, nr doubles). */
 int fb_sg_axisym_accel(fb_ctx *ctx, const double *dens, double *axi_out);
+/* Same, for the density already on the device (the context's state). */
+int fb_sg_axisym_accel_device(fb_ctx *ctx, double *axi_out);
+/* Units of ComputeCodeUnits (src/LowTasks.c:202-229). */
+double fb_unit_length(const fb_params *p);
+double fb_unit_mass(const fb_params *p);
 /* Geometry held by a context (NULL if none). */
 const fb_geom *fb_ctx_geom(const fb_ctx *ctx);
 

@@ -296,22 +296,29 @@ __global__ void __launch_bounds__(SG_BS) sg_rows_inv(FftArgs fa, int ns, int nk,
   }
 }
 
-// update_sgvelocity (sgupdate.c:30-72) on VradInt / VthetaInt
-__global__ void __launch_bounds__(SG_BS) sg_update(KP k)
+// update_sgvelocity (sgupdate.c:30-72) on VradInt / VthetaInt.  refresh = 1
+// is the call the reference's main loop makes before every DT
+// (main.c:316, Dt = 0, on Vrad / Vtheta), which matters only for the
+// RadSGAcc / AziSGAcc grids the particles read.
+__global__ void __launch_bounds__(SG_BS) sg_update(KP k, int refresh)
 {
   const int ns = k.ns;
   const size_t n = (size_t)k.nr * ns;
-  const double Dt = k.ctl->dt;
+  const double Dt = refresh ? 0.0 : k.ctl->dt;
+  double *vr = refresh ? k.vr : k.vri;
+  double *vt = refresh ? k.vt : k.vti;
   for (size_t l = (size_t)blockIdx.x * SG_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * SG_BS) {
     const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
     if (i > 0) {
       const double radsgacc = ((k.rinf[i] - k.rmed[i - 1]) * k.sg_accr[l] +
                                (k.rmed[i] - k.rinf[i]) * k.sg_accr[l - ns]) * k.invdiffrmed[i];
-      k.vri[l] += Dt * radsgacc;
+      vr[l] += Dt * radsgacc;
+      if (k.particles) k.rsga[l] = radsgacc;
     }
     const size_t lm1 = (size_t)i * ns + (j == 0 ? ns - 1 : j - 1);
     const double azisgacc = 0.5 * (k.sg_acct[l] + k.sg_acct[lm1]);
-    k.vti[l] += Dt * azisgacc;
+    vt[l] += Dt * azisgacc;
+    if (k.particles) k.asga[l] = azisgacc;
   }
 }
 
@@ -446,10 +453,10 @@ void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
   fb_sg_rows_inv(sg, k, dens, s);
 }
 
-void fb_sg_update_velocities(const KP &k, cudaStream_t s)
+void fb_sg_update_velocities(const KP &k, cudaStream_t s, int refresh)
 {
   const size_t n = (size_t)k.nr * k.ns;
-  sg_update<<<(int)((n + SG_BS - 1) / SG_BS), SG_BS, 0, s>>>(k);
+  sg_update<<<(int)((n + SG_BS - 1) / SG_BS), SG_BS, 0, s>>>(k, refresh);
 }
 
 int fb_sg_launches(const fb_sg *sg) { return sg ? 4 : 0; }

@@ -11,10 +11,11 @@
  *
  * First call: translate the globals into fb_params, create the context with
  * the reference's own Radii, upload the fields, profiles and planets.  Every
- * call: one DT on the GPU, then the host PolarGrids, planets and the scalar
- * globals (PhysicalTime, LostMass, MINDT, MAXDT, stardiscbarycenter) are
- * refreshed so that the reference's SendOutput, planet logs and -a monitor
- * see the state they expect.  Errors print a message and call prs_exit(1),
+ * call: one DT on the GPU, then the host PolarGrids, planets, particles, the
+ * drand48 stream and the scalar globals (PhysicalTime, LostMass, MINDT,
+ * MAXDT, stardiscbarycenter) are refreshed so that the reference's
+ * SendOutput, planet and particle logs and -a monitor see the state they
+ * expect.  Errors print a message and call prs_exit(1),
  * the reference's own way of stopping (src/LowTasks.c:32).
  */
 #include "mp.h"
@@ -30,6 +31,9 @@ extern boolean OpenInner, NonReflecting, AccBoundary, OuterSourceMass, Corotatin
 extern boolean AdvecteLabel, ZMPlus, MHDLSA, EntropyDiffusion, RadiativeDiffusion, ThermalCooling;
 extern boolean TempPresc, AddMass, DiscEvaporation, PhotoEvaporation, CavityTorque, ComputeCPDMass;
 extern boolean BM08, DustFeedback, Write_Temperature, Write_Potential;
+extern boolean DustFeelDisk, DustFeelPlanets, DustFeelTurb, DustFeelSG, DustFeelSGZeroMode;
+extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensity, ZZIntegrator;
+extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
 
 static fb_ctx *g_ctx = NULL;
 
@@ -122,7 +126,67 @@ static void params_from_globals(fb_params *p)
   if (TRANSITIONRADIUS != 0.0 || TRANSITIONRATIO != 1.0) p->unsupported |= FB_U_TRANSITION;
   if (LAMBDADOUBLING != 0.0) p->unsupported |= FB_U_LAMBDADOUBLING;
   if (RELEASEDATE != 0.0) p->unsupported |= FB_U_RELEASE;
-  if (NBPART != 0) p->unsupported |= FB_U_PARTICLES;
+  /* Lagrangian particles (Dsys.c, DustUpdate.c) */
+  p->sizeminpart = SIZEMINPART;
+  p->sizemaxpart = SIZEMAXPART;
+  p->sizepartslope = SIZEPARTSLOPE;
+  p->rhopart = RHOPART;
+  p->dustslope = DUSTSLOPE;
+  p->rmindust = RMINDUST;
+  p->rmaxdust = RMAXDUST;
+  p->dust_feel_disk = DustFeelDisk;
+  p->dust_feel_planets = DustFeelPlanets;
+  p->dust_feel_turb = DustFeelTurb;
+  p->dust_feedback = DustFeedback;
+  p->dust_feel_sg = DustFeelSG;
+  p->sfta = ShortFrictionTimeApproximation;
+  p->interpolation = TSCInterpolation ? 2 : 0;
+  p->write_dust_density = Write_DustDensity;
+  if (NBPART != 0) {
+    if (ZZIntegrator) p->unsupported |= FB_U_ZZINTEGRATOR;
+    if (DustGrowth) p->unsupported |= FB_U_DUSTGROWTH;
+    if (RemoveDustFromPlanetsHillRadius) p->unsupported |= FB_U_HILLREMOVAL;
+    if (!TSCInterpolation) p->unsupported |= FB_U_INTERPOLATION;
+    if (DustFeelSGZeroMode) p->unsupported |= FB_U_DUSTSGZERO;
+    if (!NoTimestepConstraintByParticles) p->unsupported |= FB_U_DUSTTIMESTEP;
+    if (SelfGravity && SoftWriting) p->unsupported |= FB_U_SOFTWRITING;
+  }
+}
+
+/* The libc drand48 state (X = x[2]:x[1]:x[0]) read and written through
+   seed48, which also resets the multiplier and increment to the defaults
+   that drand48 uses anyway. */
+static unsigned long long rand48_get(void)
+{
+  unsigned short probe[3] = {0, 0, 0}, keep[3];
+  unsigned short *old = seed48(probe);
+  keep[0] = old[0];
+  keep[1] = old[1];
+  keep[2] = old[2];
+  seed48(keep);
+  return (unsigned long long)keep[0] | ((unsigned long long)keep[1] << 16) | ((unsigned long long)keep[2] << 32);
+}
+
+static void rand48_set(unsigned long long x)
+{
+  unsigned short s[3];
+  s[0] = (unsigned short)(x & 0xFFFFu);
+  s[1] = (unsigned short)((x >> 16) & 0xFFFFu);
+  s[2] = (unsigned short)((x >> 32) & 0xFFFFu);
+  seed48(s);
+}
+
+static void dust_views(fb_dust_state *d, DustSystem *dsys)
+{
+  memset(d, 0, sizeof *d);
+  d->n = NBPART;
+  d->r = dsys->r;
+  d->th = dsys->th;
+  d->vr = dsys->vr;
+  d->vth = dsys->vth;
+  d->l = dsys->l;
+  d->size = dsys->dustsize;
+  d->stokes = dsys->stokesnb;
 }
 
 static void state_views(fb_state *st, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid *Vtheta,
@@ -143,7 +207,8 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
   fb_state st;
   fb_step_report rep;
   int rc, k;
-  (void)force; (void)Label; (void)DRho; (void)dustpcdens; (void)DVrad; (void)DVtheta; (void)dsys;
+  fb_dust_state dst;
+  (void)force; (void)Label; (void)DRho; (void)dustpcdens; (void)DVrad; (void)DVtheta;
   state_views(&st, Rho, Vrad, Vtheta, Energy);
   if (!g_ctx) {
     fb_params p;
@@ -184,6 +249,17 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
     prof.global_soundspeed = GLOBAL_SoundSpeed;
     rc = fb_upload(g_ctx, &st, &prof);
     if (rc) dropin_fail("fb_upload", rc);
+    if (NBPART != 0) {
+      /* the particles as main.c left them, and the position of the drand48
+         stream the turbulent kicks continue; the Gaussian generators have not
+         been called before the first AlgoGas */
+      dust_views(&dst, dsys);
+      dst.rng_x = rand48_get();
+      dst.kicks = 0;
+      dst.particles_mass = Particles_Mass;
+      rc = fb_dust_upload(g_ctx, &dst);
+      if (rc) dropin_fail("fb_dust_upload", rc);
+    }
   }
   rc = fb_algogas(g_ctx, &rep);
   if (rc) dropin_fail("fb_algogas", rc);
@@ -198,6 +274,12 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
   for (k = 0; k < 3; k++) {
     stardiscbarycenter_x[k] = st.stardiscbarycenter_x[k];
     stardiscbarycenter_y[k] = st.stardiscbarycenter_y[k];
+  }
+  if (NBPART != 0) {
+    dust_views(&dst, dsys);
+    rc = fb_dust_download(g_ctx, &dst);
+    if (rc) dropin_fail("fb_dust_download", rc);
+    rand48_set(dst.rng_x);
   }
   for (k = 0; k < sys->nb; k++) {
     sys->mass[k] = st.planets.mass[k];

@@ -100,12 +100,16 @@ typedef struct fb_params {
   double factorunitmass, factorunitlength, factormmw;
   /* Lagrangian dust particles: NBPART, SIZEMINPART, SIZEMAXPART,
      SIZEPARTSLOPE, RHOPART, DUSTSLOPE, RMINDUST, RMAXDUST, DUSTFEELDISK,
-     DUSTFEELPLANETS, DUSTFEELTURB, DUSTFEEDBACK, SFTAPPROX, INTERPOLATION */
+     DUSTFEELPLANETS, DUSTFEELTURB, DUSTFEEDBACK, DUSTFEELSG, SFTAPPROX,
+     INTERPOLATION, WRITEDUSTDENSITY (which makes AlgoGas interpolate the
+     gas onto the particles a second time each substep, src/SourceEuler.c:529,
+     and so changes the Stokes numbers the next turbulent kick uses) */
   int nbpart;
   double sizeminpart, sizemaxpart, sizepartslope, rhopart, dustslope;
   double rmindust, rmaxdust;
-  int dust_feel_disk, dust_feel_planets, dust_feel_turb, dust_feedback;
+  int dust_feel_disk, dust_feel_planets, dust_feel_turb, dust_feedback, dust_feel_sg;
   int sfta, interpolation; /* interpolation: 0 NGP, 1 CIC, 2 TSC */
+  int write_dust_density;
   /* bit mask of .par features that were set but that this build does not
      implement (fb_create refuses a non-zero mask); see fb_unsupported_name */
   unsigned long long unsupported;
@@ -152,6 +156,21 @@ typedef struct fb_step_report {
   double gpu_ms;         /* device time of the DT (CUDA events)            */
 } fb_step_report;
 
+/* Lagrangian dust particles (src/types.h:114-146, the fields the step
+   carries between DTs).  Arrays are caller-owned, n doubles each.  rng_x
+   is the 48-bit drand48 state after every draw made so far; kicks counts
+   the turbulent-kick calls made so far by each of the two Gaussian
+   generators of src/DustUpdate.c:438-485, and carry holds their cached
+   second deviates (radial, azimuthal) when kicks is odd. */
+typedef struct fb_dust_state {
+  int n;
+  double *r, *th, *vr, *vth, *l, *size, *stokes;
+  unsigned long long rng_x;
+  long long kicks;
+  double carry[2];
+  double particles_mass;   /* Particles_Mass (main.c:190-224) */
+} fb_dust_state;
+
 /* Download masks */
 #define FB_F_DENS    0x01u
 #define FB_F_VRAD    0x02u
@@ -184,6 +203,13 @@ int fb_planets_read_cfg(const fb_params *p, const char *path, fb_planets *out);
 int fb_init_state(const fb_params *p, fb_ctx *ctx, double noise_amp,
                   long noise_seed, fb_state *st, fb_profiles *prof);
 
+/* Draws the initial particles exactly as InitDustSystem does
+   (src/Dsys.c:128-262): sizes, then radii, then azimuths from the POSIX
+   drand48 stream seeded with `seed`; Keplerian azimuthal velocities (with
+   the self-gravity correction when ctx holds self-gravity).  Arrays of
+   st->n = p->nbpart doubles must be allocated by the caller. */
+int fb_init_dust(const fb_params *p, fb_ctx *ctx, long seed, fb_dust_state *st);
+
 /* ---- device context ------------------------------------------------------ */
 /* Selects the CUDA device used by contexts created afterwards on this host
    thread (cudaSetDevice of the library's runtime). */
@@ -196,6 +222,11 @@ int fb_upload(fb_ctx *ctx, const fb_state *st, const fb_profiles *prof);
 /* One DT of AlgoGas (src/SourceEuler.c:326-719) on device-resident state. */
 int fb_algogas(fb_ctx *ctx, fb_step_report *rep);
 int fb_download(fb_ctx *ctx, fb_state *st, unsigned mask);
+/* Particles (NBPART > 0): upload once after fb_upload (computes the
+   particles' gas values and Stokes numbers as the reference's first
+   interpolation call, src/main.c:287), download when writing outputs. */
+int fb_dust_upload(fb_ctx *ctx, const fb_dust_state *st);
+int fb_dust_download(fb_ctx *ctx, fb_dust_state *st);
 /* Derived output fields at the current state (reference layout, (nrad+1)*nsec):
    which = 0 Temperature (src/SourceEuler.c:2440), 1 Potential, 2 Pressure,
    3 SoundSpeed, 4 DivergenceVelocity, 5 ViscHeat, 6 SG radial acceleration

@@ -122,6 +122,19 @@ static void write_dump(const char *path, darr *a, int na, double *sc, int nsc,
   fclose(f);
 }
 
+/* Position of the libc drand48 stream (48-bit, exact in a double), read
+   through seed48 and put back unchanged. */
+static unsigned long long rand48_state(void)
+{
+  unsigned short probe[3] = {0, 0, 0}, keep[3];
+  unsigned short *old = seed48(probe);
+  keep[0] = old[0];
+  keep[1] = old[1];
+  keep[2] = old[2];
+  seed48(keep);
+  return (unsigned long long)keep[0] | ((unsigned long long)keep[1] << 16) | ((unsigned long long)keep[2] << 32);
+}
+
 static void dump_state(const char *tag, PolarGrid *Rho, PolarGrid *Vrad,
                        PolarGrid *Vtheta, PolarGrid *Energy,
                        PlanetarySystem *sys, DustSystem *dsys)
@@ -144,6 +157,7 @@ static void dump_state(const char *tag, PolarGrid *Rho, PolarGrid *Vrad,
   scn[nsc] = "substeps"; sc[nsc++] = (double)h_substeps;
   scn[nsc] = "nplanets"; sc[nsc++] = (double)(sys ? sys->nb : 0);
   scn[nsc] = "nbpart"; sc[nsc++] = (double)NBPART;
+  scn[nsc] = "rng_state"; sc[nsc++] = (double)rand48_state();
   a[na].name = "dens"; a[na].p = Rho->Field; a[na++].n = nf;
   a[na].name = "vrad"; a[na].p = Vrad->Field; a[na++].n = nf;
   a[na].name = "vtheta"; a[na].p = Vtheta->Field; a[na++].n = nf;

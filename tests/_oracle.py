@@ -18,7 +18,8 @@ DROPIN_BIN = os.path.join(REPO, "oracle", "_ref", "fargo_dropin")
 CONFIG_DIR = os.path.join(REPO, "dustyfargoadsg_b200", "configs")
 
 
-SCALARS = {"PhysicalTime", "OmegaFrame", "LostMass", "MINDT", "MAXDT", "substeps", "nplanets", "nbpart"}
+SCALARS = {"PhysicalTime", "OmegaFrame", "LostMass", "MINDT", "MAXDT", "substeps", "nplanets", "nbpart",
+           "rng_state"}
 
 
 def have_oracle():

@@ -86,3 +86,38 @@ def test_initial_state_bit_identical(tmp_path, noise, seed):
     assert st.planets.nb == 1
     assert st.planets.x[0] == ref["pl_x"][0] and st.planets.vy[0] == ref["pl_vy"][0]
     assert st.planets.mass[0] == ref["pl_mass"][0]
+
+
+DUST_PAR = os.path.join(CFG, "dust_256x768.par")
+
+
+@pytest.mark.skipif(not _oracle.have_oracle(), reason="oracle not built")
+@pytest.mark.parametrize("keys", [
+    dict(),                                                   # s^-3.5 sizes, uniform radii
+    dict(SizePartSlope=1.0, DustSlope=1.0, SizeMaxPart=1e-1),  # the exp/log branches of Dsys.c:182-197
+    dict(SizeMinPart=1e-3, SizeMaxPart=1e-3, SizePartSlope=0.0, DustSlope=0.5, RminDust=0.0),
+])
+def test_initial_particles_bit_identical(tmp_path, keys):
+    """fb_init_dust == InitDustSystem (Dsys.c:128-262) bit for bit, and the
+    drand48 stream is left at the same position."""
+    from dustyfargoadsg_b200 import _ffi, read_par
+    args = dict(Nrad=32, Nsec=64, NbPart=3000)
+    args.update(keys)
+    par = _oracle.write_par(DUST_PAR, str(tmp_path), **args)
+    dumps, _, _ = _oracle.run_oracle(par, steps=1, noise=0.0, seed=1, dump_every=1000)
+    ref = dumps["state_init"]
+    lib = _ffi.load()
+    p = read_par(par)
+    assert p.unsupported == 0, lib.fb_unsupported_name(C.byref(p))
+    n = p.nbpart
+    arrays = {k: np.zeros(n) for k in ("r", "th", "vr", "vth", "l", "size", "stokes")}
+    st = _ffi.FbDustState()
+    st.n = n
+    for k, a in arrays.items():
+        setattr(st, k, a.ctypes.data_as(C.POINTER(C.c_double)))
+    _ffi.check(lib.fb_init_dust(C.byref(p), None, 1, C.byref(st)), "fb_init_dust")
+    for k in ("r", "th", "vr", "vth", "size"):
+        np.testing.assert_array_equal(arrays[k], ref["pc_" + k], err_msg=k)
+    np.testing.assert_array_equal(arrays["l"], arrays["r"] * arrays["vth"])
+    assert st.rng_x == int(ref["rng_state"])
+    assert st.kicks == 0
