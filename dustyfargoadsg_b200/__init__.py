@@ -15,7 +15,7 @@ from . import _ffi
 from ._ffi import (FB_F_ALL, FB_F_DENS, FB_F_ENERGY, FB_F_VRAD, FB_F_VTHETA, FbDustState, FbError,
                    FbParams, FbProfiles, FbState, FbStepReport, check, load)
 
-__all__ = ["Disc", "read_par", "select_device", "FbError", "load", "CONFIG_DIR"]
+__all__ = ["Disc", "Batch", "read_par", "select_device", "FbError", "load", "CONFIG_DIR"]
 
 CONFIG_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "configs")
 
@@ -206,6 +206,15 @@ class Disc:
         check(self.lib.fb_download_derived(self.ctx, int(which), _ptr(out)), "fb_download_derived", self.ctx)
         return out
 
+    def vortensity(self, field=False):
+        """Azimuthal means of Sigma (per ring) and of the vortensity (per
+        interface ring), and optionally the vortensity field."""
+        sm, vm = np.zeros(self.nr), np.zeros(self.nr)
+        f = np.zeros(self.nf) if field else None
+        check(self.lib.fb_vortensity(self.ctx, _ptr(f) if field else None, _ptr(sm), _ptr(vm)),
+              "fb_vortensity", self.ctx)
+        return (sm, vm, f) if field else (sm, vm)
+
     def diagnostics(self):
         m, p = C.c_double(), C.c_double()
         check(self.lib.fb_diagnostics(self.ctx, C.byref(m), C.byref(p)), "fb_diagnostics", self.ctx)
@@ -215,6 +224,42 @@ class Disc:
         if self.ctx:
             self.lib.fb_destroy(self.ctx)
             self.ctx = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+class Batch:
+    """Several discs advanced one DT each by a single graph launch
+    (fb_batch_*); the discs stay usable on their own."""
+
+    def __init__(self, discs):
+        self.lib = load()
+        self.discs = list(discs)
+        n = len(self.discs)
+        arr = (C.c_void_p * n)(*[d.ctx for d in self.discs])
+        self.b = C.c_void_p()
+        check(self.lib.fb_batch_create(arr, n, C.byref(self.b)), "fb_batch_create")
+        self.reps = (FbStepReport * n)()
+
+    def step(self):
+        """One DT of every disc; returns the per-disc step reports."""
+        check(self.lib.fb_batch_algogas(self.b, self.reps), "fb_batch_algogas")
+        return list(self.reps)
+
+    def close(self):
+        if self.b:
+            self.lib.fb_batch_destroy(self.b)
+            self.b = C.c_void_p()
 
     def __del__(self):
         try:

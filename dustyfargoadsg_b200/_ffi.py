@@ -105,7 +105,8 @@ EXPORTS = (
     "fb_download_derived", "fb_diagnostics", "fb_strerror", "fb_last_error", "fb_stage",
     "fb_build_info", "fb_struct_size", "fb_kernel_launches", "fb_profile", "fb_profile_read",
     "fb_select_device", "fb_transport_noalloc", "fb_noalloc_last_error", "fb_init_dust",
-    "fb_dust_upload", "fb_dust_download",
+    "fb_dust_upload", "fb_dust_download", "fb_vortensity", "fb_batch_create", "fb_batch_algogas",
+    "fb_batch_destroy",
 )
 
 _lib = None
@@ -149,6 +150,10 @@ def load():
         "fb_init_dust": (_I, [C.POINTER(FbParams), vp, C.c_long, C.POINTER(FbDustState)]),
         "fb_dust_upload": (_I, [vp, C.POINTER(FbDustState)]),
         "fb_dust_download": (_I, [vp, C.POINTER(FbDustState)]),
+        "fb_vortensity": (_I, [vp, _P, _P, _P]),
+        "fb_batch_create": (_I, [C.POINTER(vp), _I, C.POINTER(vp)]),
+        "fb_batch_algogas": (_I, [vp, C.POINTER(FbStepReport)]),
+        "fb_batch_destroy": (_I, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -554,6 +554,28 @@ static int enqueue_substep(fb_ctx *ctx)
   return npt;
 }
 
+// The start of one DT, before the substep loop; returns the kernel launches.
+static int enqueue_dt_prelude(fb_ctx *ctx)
+{
+  KP &k = ctx->k;
+  cudaStream_t s = ctx->st;
+  int n = 1;
+  fb_launch_begin_dt(k, ctx->p.dt, s);
+  if (ctx->has_dust && ctx->sg) {
+    // main.c:307-316: before every DT the reference's main loop recomputes
+    // the self-gravity field (SoftWriting = No), which sets the RadSGAcc /
+    // AziSGAcc grids the first substep's particles read
+    fb_sg_accel(ctx->sg, k, k.rho, s);
+    fb_sg_update_velocities(k, s, 1);
+    n += fb_sg_launches(ctx->sg);
+  }
+  if (k.energy) {  // SourceEuler.c:344-350
+    fb_launch_soundspeed(k, 0, s);
+    n += 1;
+  }
+  return n;
+}
+
 // Captures one DT as a graph: WHILE(cond) { substep; cond = !done }.  The
 // kernels read dt and the planets from the device control block, so one
 // capture serves every substep and every DT.
@@ -646,20 +668,9 @@ extern "C" int fb_algogas(fb_ctx *ctx, fb_step_report *rep)
     set_err(ctx, "NBPART > 0: upload the particles (fb_dust_upload) before the first DT");
     return FB_ERR_STATE;
   }
-  KP &k = ctx->k;
   cudaStream_t s = ctx->st;
   CK(cudaEventRecord(ctx->ev0, s));
-  fb_launch_begin_dt(k, ctx->p.dt, s);
-  ctx->launches += 1;
-  if (ctx->has_dust && ctx->sg) {
-    // main.c:307-316: before every DT the reference's main loop recomputes
-    // the self-gravity field (SoftWriting = No), which sets the RadSGAcc /
-    // AziSGAcc grids the first substep's particles read
-    fb_sg_accel(ctx->sg, k, k.rho, s);
-    fb_sg_update_velocities(k, s, 1);
-    ctx->launches += fb_sg_launches(ctx->sg);
-  }
-  if (k.energy) { fb_launch_soundspeed(k, 0, s); ctx->launches += 1; }  // SourceEuler.c:344-350
+  ctx->launches += enqueue_dt_prelude(ctx);
   int status = FB_OK;
   const int cap = ctx->substep_cap;
   if (!ctx->profiling && ctx->graph_state == 0) ctx->graph_state = (build_dt_graph(ctx) == FB_OK) ? 1 : -1;
@@ -901,4 +912,167 @@ extern "C" int fb_dust_download(fb_ctx *ctx, fb_dust_state *st)
   st->carry[1] = h->carry_phi;
   st->particles_mass = 0.0;
   return FB_OK;
+}
+
+// ------------------------------------------------------------ diagnostics
+extern "C" int fb_vortensity(fb_ctx *ctx, double *field, double *sigma_mean, double *vort_mean)
+{
+  if (!ctx) return FB_ERR_INVALID;
+  if (!ctx->uploaded) return FB_ERR_STATE;
+  const int nr = ctx->nr, ns = ctx->ns;
+  double *xi = NULL, *means = NULL;
+  CK(cudaMallocAsync((void **)&xi, ctx->nf * sizeof(double), ctx->st));
+  CK(cudaMallocAsync((void **)&means, 2 * (size_t)nr * sizeof(double), ctx->st));
+  CK(cudaMemsetAsync(xi, 0, ctx->nf * sizeof(double), ctx->st));
+  fb_launch_vortensity(ctx->k, xi, ctx->st);
+  fb_launch_ring_mean(ctx->k.rho, nr, ns, means, ctx->st);
+  fb_launch_ring_mean(xi, nr, ns, means + nr, ctx->st);
+  ctx->launches += 3;
+  if (field) CK(cudaMemcpyAsync(field, xi, ctx->nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  if (sigma_mean) CK(cudaMemcpyAsync(sigma_mean, means, nr * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  if (vort_mean) CK(cudaMemcpyAsync(vort_mean, means + nr, nr * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaFreeAsync(xi, ctx->st));
+  CK(cudaFreeAsync(means, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return FB_OK;
+}
+
+// ------------------------------------------------------------ batches
+// Many discs (contexts of any grid size and parameters on one device)
+// advanced one DT each by a single graph launch: per disc, the DT prelude
+// followed by a conditional WHILE node around its substep, all discs as
+// independent branches of one graph so that their kernels overlap on the
+// GPU.  No counterpart in the reference, which runs one disc per process.
+struct fb_batch {
+  std::vector<fb_ctx *> ctxs;
+  std::vector<int> prelude;  // kernel launches of each disc's DT prelude
+  std::vector<long long> per_substep;
+  cudaStream_t st;
+  cudaEvent_t ev0, ev1;
+  cudaGraph_t g;
+  cudaGraphExec_t ge;
+};
+
+extern "C" int fb_batch_destroy(fb_batch *b)
+{
+  if (!b) return FB_OK;
+  if (b->st) cudaStreamSynchronize(b->st);
+  if (b->ge) cudaGraphExecDestroy(b->ge);
+  if (b->g) cudaGraphDestroy(b->g);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return FB_OK;
+}
+
+// One disc of the batch graph: its DT prelude as a child graph, then the
+// conditional WHILE node around its substep (captured into the node's body).
+static int batch_add_disc(fb_batch *b, fb_ctx *ctx)
+{
+  cudaStream_t s = ctx->st;
+  const long long l0 = ctx->launches;
+  const int prof = ctx->profiling;
+  ctx->profiling = 0;
+  int rc = FB_ERR_CUDA;
+  cudaGraph_t pre = NULL;
+  cudaGraphNode_t pre_node, loop_node;
+  cudaGraphConditionalHandle h;
+  cudaGraphNodeParams cp = {};
+  int npre = 0;
+  if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) goto out;
+  npre = enqueue_dt_prelude(ctx);
+  if (cudaStreamEndCapture(s, &pre) != cudaSuccess || !pre) goto out;
+  if (cudaGraphAddChildGraphNode(&pre_node, b->g, NULL, 0, pre) != cudaSuccess) goto out;
+  if (cudaGraphConditionalHandleCreate(&h, b->g, 1, cudaGraphCondAssignDefault) != cudaSuccess) goto out;
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  if (cudaGraphAddNode(&loop_node, b->g, &pre_node, 1, &cp) != cudaSuccess) goto out;
+  {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    const long long l1 = ctx->launches;
+    if (cudaStreamBeginCaptureToGraph(s, body, NULL, NULL, 0, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+      goto out;
+    enqueue_substep(ctx);
+    fb_launch_loop_cond(ctx->k, h, ctx->substep_cap, s);
+    if (cudaStreamEndCapture(s, &body) != cudaSuccess) goto out;
+    b->prelude.push_back(npre);
+    b->per_substep.push_back(ctx->launches - l1 + 1);
+  }
+  rc = FB_OK;
+out:
+  if (rc) cudaGetLastError();
+  if (pre) cudaGraphDestroy(pre);
+  ctx->launches = l0;
+  for (int q = 0; q < FB_NSTAGE; q++) ctx->pcount[q] = 0;
+  ctx->profiling = prof;
+  return rc;
+}
+
+extern "C" int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out)
+{
+  if (!ctxs || n <= 0 || !out) return FB_ERR_INVALID;
+  *out = NULL;
+  for (int d = 0; d < n; d++) {
+    if (!ctxs[d]) return FB_ERR_INVALID;
+    if (!ctxs[d]->uploaded || (ctxs[d]->has_dust && !ctxs[d]->dust_uploaded)) return FB_ERR_STATE;
+    for (int e = 0; e < d; e++)
+      if (ctxs[e] == ctxs[d]) return FB_ERR_INVALID;  // a disc may appear once
+  }
+  fb_batch *b = new fb_batch();
+  b->ctxs.assign(ctxs, ctxs + n);
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+      cudaGraphCreate(&b->g, 0) != cudaSuccess) {
+    fb_batch_destroy(b);
+    return FB_ERR_CUDA;
+  }
+  for (int d = 0; d < n; d++) {
+    int rc = batch_add_disc(b, ctxs[d]);
+    if (rc) { fb_batch_destroy(b); return rc; }
+  }
+  if (cudaGraphInstantiate(&b->ge, b->g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    fb_batch_destroy(b);
+    return FB_ERR_CUDA;
+  }
+  *out = b;
+  return FB_OK;
+}
+
+extern "C" int fb_batch_algogas(fb_batch *b, fb_step_report *reps)
+{
+  if (!b) return FB_ERR_INVALID;
+  const int n = (int)b->ctxs.size();
+  fb_ctx *ctx = b->ctxs[0];  // for CK error messages
+  // the discs' own streams may still hold work (uploads, single DTs)
+  for (fb_ctx *c : b->ctxs) CK(cudaStreamSynchronize(c->st));
+  CK(cudaEventRecord(b->ev0, b->st));
+  CK(cudaGraphLaunch(b->ge, b->st));
+  CK(cudaEventRecord(b->ev1, b->st));
+  for (fb_ctx *c : b->ctxs) CK(cudaMemcpyAsync(c->h_ctl, c->d_ctl, sizeof(fb_ctl), cudaMemcpyDeviceToHost, b->st));
+  CK(cudaStreamSynchronize(b->st));
+  CK(cudaGetLastError());
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  int status = FB_OK;
+  for (int d = 0; d < n; d++) {
+    fb_ctx *c = b->ctxs[d];
+    const fb_ctl *h = c->h_ctl;
+    c->launches += b->prelude[d] + b->per_substep[d] * (long long)h->substeps;
+    if (h->status && !status) status = h->status;
+    if (h->status) set_err(c, "AlgoGas stopped: %s", fb_strerror(h->status));
+    if (reps) {
+      reps[d].substeps = h->substeps;
+      reps[d].status = h->status;
+      reps[d].physical_time = h->physical_time;
+      reps[d].mindt = h->mindt;
+      reps[d].maxdt = h->maxdt;
+      reps[d].lost_mass = h->lost_mass;
+      reps[d].gpu_ms = ms;  // the whole batch
+    }
+  }
+  return status;
 }

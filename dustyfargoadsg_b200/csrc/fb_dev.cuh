@@ -138,6 +138,7 @@ void fb_launch_diag(const KP &k, double *out2, cudaStream_t s);
 void fb_launch_derived(const KP &k, int which, double *out, cudaStream_t s);
 void fb_launch_boundary_only(const KP &k, cudaStream_t s);
 int  fb_gas_prepare(int ns, int energy);  // kernel attributes (shared memory)
+int  fb_allow_max_dynamic_smem(const void *func);
 void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s);
 void fb_launch_loop_cond(const KP &k, cudaGraphConditionalHandle h, int cap, cudaStream_t s);
 // self-gravity (fb_sg.cu)
@@ -147,6 +148,9 @@ void fb_sg_destroy(fb_sg *sg);
 void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
 // refresh = 1: the Dt = 0 call of main.c:316 on Vrad/Vtheta (fields only)
 void fb_sg_update_velocities(const KP &k, cudaStream_t s, int refresh = 0);
+// diagnostics (fb_diag.cu)
+void fb_launch_vortensity(const KP &k, double *xi, cudaStream_t s);
+void fb_launch_ring_mean(const double *f, int nr, int ns, double *out, cudaStream_t s);
 // Lagrangian particles (fb_dust.cu)
 void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s);
 void fb_launch_dust_interpolation_only(const KP &k, const PP &pp, cudaStream_t s);

@@ -1265,6 +1265,23 @@ __global__ void k_begin_dt(KP k, double DT)
 
 void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s) { k_begin_dt<<<1, 1, 0, s>>>(k, DT); }
 
+// Lets a kernel take all the dynamic shared memory the device offers beside
+// its static part.  The limit is a per-function attribute shared by every
+// context in the process, so it is raised once to the device maximum rather
+// than set to one grid's need (contexts of different sizes coexist).
+int fb_allow_max_dynamic_smem(const void *func)
+{
+  int dev = 0, maxopt = 0;
+  cudaFuncAttributes fa;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+      cudaFuncGetAttributes(&fa, func) != cudaSuccess)
+    return FB_ERR_CUDA;
+  const int dyn = maxopt - (int)fa.sharedSizeBytes;
+  return cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) == cudaSuccess ? FB_OK
+                                                                                                    : FB_ERR_CUDA;
+}
+
 int fb_gas_prepare(int ns, int energy)
 {
   const int NQ = energy ? 6 : 5;
@@ -1274,9 +1291,9 @@ int fb_gas_prepare(int ns, int energy)
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem + 32 * sizeof(double) > (size_t)maxopt) return FB_ERR_UNSUPPORTED;
   if (azi_threads(ns) > 512 || ns < 16) return FB_ERR_UNSUPPORTED;
-  cudaError_t e1 = cudaFuncSetAttribute(k_transport_azimuthal<5, FB_AZI_E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaError_t e2 = cudaFuncSetAttribute(k_transport_azimuthal<6, FB_AZI_E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  return (e1 == cudaSuccess && e2 == cudaSuccess) ? FB_OK : FB_ERR_CUDA;
+  int rc = fb_allow_max_dynamic_smem((const void *)k_transport_azimuthal<5, FB_AZI_E>);
+  if (!rc) rc = fb_allow_max_dynamic_smem((const void *)k_transport_azimuthal<6, FB_AZI_E>);
+  return rc;
 }
 
 // Loop condition of the captured substep graph: keep going while the

@@ -343,9 +343,11 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (sg->smem_row > (size_t)maxopt || sg->smem_col > (size_t)maxopt) { fb_sg_destroy(sg); return FB_ERR_UNSUPPORTED; }
-  cudaFuncSetAttribute(sg_rows_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sg->smem_row);
-  cudaFuncSetAttribute(sg_rows_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sg->smem_row);
-  cudaFuncSetAttribute(sg_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sg->smem_col);
+  if (fb_allow_max_dynamic_smem((const void *)sg_rows_fwd) || fb_allow_max_dynamic_smem((const void *)sg_rows_inv) ||
+      fb_allow_max_dynamic_smem((const void *)sg_cols)) {
+    fb_sg_destroy(sg);
+    return FB_ERR_CUDA;
+  }
   // init_sg (sginit.c:9-11)
   sg->eps = p->sgthicknesssmoothing * p->aspectratio;
   sg->rstep = log(g->radii[nr] / g->radii[0]) / (double)nr;

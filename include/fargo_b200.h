@@ -235,6 +235,28 @@ int fb_download_derived(fb_ctx *ctx, int which, double *out);
 /* Diagnostics on the device state: GasTotalMass (src/SideEuler.c:15) and
    GasMomentum (src/SideEuler.c:114). */
 int fb_diagnostics(fb_ctx *ctx, double *mass, double *momentum);
+/* ---- batches of discs (no counterpart in the reference) ----------------- */
+/* Many discs -- contexts of any grid size and parameters on the current
+   device, each uploaded -- advanced one DT each by one graph launch, their
+   substep loops running side by side on the GPU.  A context may belong to
+   one batch at a time and keeps working on its own with fb_algogas. */
+typedef struct fb_batch fb_batch;
+int fb_batch_create(fb_ctx *const *ctxs, int n, fb_batch **out);
+/* One DT of every disc; reps (n entries, may be NULL) as fb_algogas reports
+   them, gpu_ms being the whole batch's device time.  Returns the first
+   non-zero disc status. */
+int fb_batch_algogas(fb_batch *b, fb_step_report *reps);
+int fb_batch_destroy(fb_batch *b);
+
+/* No counterpart in the reference (it has no vortensity routine): the
+   vortensity xi = omega_z / Sigma at the cell corners (R_inf[i], phi_inf[j]),
+   i = 1..nrad-1, with omega_z = [d(R vtheta)/dR - d(vrad)/dphi] / R_inf
+   + 2 OmegaFrame from centred differences of the staggered velocities and
+   Sigma the mean of the four cells around the corner (ring 0 and ring nrad
+   are 0); and the azimuthal means of Sigma (per ring) and of xi (per
+   interface ring).  Any output may be NULL: field (nrad+1)*nsec doubles,
+   sigma_mean and vort_mean nrad doubles. */
+int fb_vortensity(fb_ctx *ctx, double *field, double *sigma_mean, double *vort_mean);
 const char *fb_strerror(int code);
 const char *fb_last_error(const fb_ctx *ctx);
 
