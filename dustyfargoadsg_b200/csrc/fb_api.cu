@@ -516,8 +516,7 @@ static int enqueue_substep(fb_ctx *ctx)
   KP &k = ctx->k;
   cudaStream_t s = ctx->st;
   int npt = 0;
-  STAGE(ST_CFL, 1, fb_launch_cfl(k, s));
-  STAGE(ST_CONTROL, 1, fb_launch_controller(k, s));
+  STAGE(ST_CFL, 1, fb_launch_cfl(k, s));  // ConditionCFL + the controller (last CTA)
   // particles after the planets' RK5 step and before the gas update
   // (SourceEuler.c:504-531)
   if (ctx->has_dust) STAGE(ST_DUST, fb_dust_launches(ctx->pp), fb_launch_dust_substep(k, ctx->pp, s));

@@ -25,6 +25,7 @@ struct fb_ctl {
   double mdisc;
   int substeps, done, status, crash_count, nonfinite;
   int np;
+  unsigned int cfl_done;                     // CTAs of the CFL kernel finished this substep
   double pm[FB_MAX_PLANETS], px[FB_MAX_PLANETS], py[FB_MAX_PLANETS];
   double pvx[FB_MAX_PLANETS], pvy[FB_MAX_PLANETS], pacc[FB_MAX_PLANETS];
   double pinit[FB_MAX_PLANETS], pfinal[FB_MAX_PLANETS];
@@ -119,7 +120,6 @@ struct PP {
 
 // launchers (fb_gas.cu)
 void fb_launch_cfl(const KP &k, cudaStream_t s);
-void fb_launch_controller(const KP &k, cudaStream_t s);
 void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s);
 void fb_launch_potential(const KP &k, cudaStream_t s);
 void fb_launch_substep1(const KP &k, cudaStream_t s);

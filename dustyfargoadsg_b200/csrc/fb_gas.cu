@@ -77,6 +77,9 @@ static __device__ __forceinline__ double nu_ring(const KP &k, int i)
   return 0.0;
 }
 
+static __device__ void cfl_ring_limit(const KP &k, int i, double vmoy, double *sh);
+static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c);
+
 // ---------------------------------------------------------------- CFL
 // ConditionCFL (SourceEuler.c:1304-1552): one CTA per ring computes the
 // azimuthal mean Vmoy[i] and the smallest per-cell limit of the ring; the
@@ -85,7 +88,7 @@ static __device__ __forceinline__ double nu_ring(const KP &k, int i)
 __global__ void __launch_bounds__(FB_BS) k_cfl(KP k)
 {
   __shared__ double sh[32];
-  const int i = blockIdx.x, ns = k.ns, nr = k.nr;
+  const int i = blockIdx.x, ns = k.ns;
   const size_t base = (size_t)i * ns;
   const double *vt = k.vt + base, *vr = k.vr + base;
   double s = 0.0;
@@ -143,7 +146,37 @@ __global__ void __launch_bounds__(FB_BS) k_cfl(KP k)
     if (neg) atomicAdd(&k.ctl->crash_count, 1);
     if (bad) atomicOr(&k.ctl->nonfinite, 1);
   }
-  if (i < 1) return;  // per-cell limits over i = One_or_active..Max_or_active-1
+  if (i >= 1) cfl_ring_limit(k, i, vmoy, sh);  // i = One_or_active..Max_or_active-1
+  // the last CTA to finish runs the controller (no waiting: whoever comes
+  // last sees every other ring's results)
+  __shared__ int last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last = (atomicAdd(&k.ctl->cfl_done, 1u) == gridDim.x - 1) ? 1 : 0;
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __shared__ fb_ctl cs;
+  unsigned long long *dst = (unsigned long long *)&cs;
+  const unsigned long long *src = (const unsigned long long *)k.ctl;
+  for (int w = threadIdx.x; w < (int)(sizeof(fb_ctl) / 8); w += FB_BS) dst[w] = __ldcg(src + w);
+  __syncthreads();
+  controller_body(k, sh, &cs);
+  __syncthreads();
+  if (threadIdx.x == 0) cs.cfl_done = 0;
+  __syncthreads();
+  unsigned long long *out = (unsigned long long *)k.ctl;
+  for (int w = threadIdx.x; w < (int)(sizeof(fb_ctl) / 8); w += FB_BS) out[w] = dst[w];
+}
+
+// ConditionCFL's per-cell limits of ring i (SourceEuler.c:1390-1485)
+static __device__ void cfl_ring_limit(const KP &k, int i, double vmoy, double *sh)
+{
+  const int ns = k.ns;
+  const size_t base = (size_t)i * ns;
+  const double *vt = k.vt + base, *vr = k.vr + base;
   const double viscosity = nu_ring(k, i);
   const double dxrad = k.dxrad[i], dxtheta = k.dxtheta_cfl[i];
   double m = 1e30;
@@ -168,7 +201,6 @@ __global__ void __launch_bounds__(FB_BS) k_cfl(KP k)
   }
   m = block_min<FB_BS>(m, sh);
   if (threadIdx.x == 0) k.ringmin[i] = m;
-  (void)nr;
 }
 
 void fb_launch_cfl(const KP &k, cudaStream_t s) { k_cfl<<<k.nr, FB_BS, 0, s>>>(k); }
@@ -240,30 +272,29 @@ static __device__ void rk5(const double *q0, double dt, const double *masses, do
     q1[i] = q0[i] + 37.0 / 378.0 * k1[i] + 250.0 / 621.0 * k3[i] + 125.0 / 594.0 * k4[i] + 512.0 / 1771.0 * k6[i];
 }
 
-// The scalar part of one substep of AlgoGas, SourceEuler.c:398-531.  One CTA:
-// its threads reduce the per-ring CFL limits, the shear limits and the
-// force partials (fixed tree order), then thread 0 runs the scalar logic.
-__global__ void __launch_bounds__(FB_BS) k_controller(KP k)
+// The scalar part of one substep of AlgoGas, SourceEuler.c:398-531, run by
+// the last CTA of k_cfl: its threads reduce the per-ring CFL limits, the
+// shear limits and the force partials (fixed tree order), then thread 0 runs
+// the scalar logic on a shared-memory copy of the control block.
+static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
 {
-  __shared__ double sh[32];
-  fb_ctl *c = k.ctl;
   const int np = c->np, nr = k.nr, tid = threadIdx.x;
   // ConditionCFL reduction (SourceEuler.c:1336-1497)
   double m = 1e30;
   for (int i = 1 + tid; i < nr; i += FB_BS) {
-    double d = k.ringmin[i];
+    double d = __ldcg(k.ringmin + i);
     if (d < m) m = d;
   }
   for (int i = tid; i < nr - 1; i += FB_BS) {
     double d = (k.pmax - k.pmin) * FB_CFLSECURITY / (double)k.ns /
-               fabs(k.vmoy[i] * k.invrmed[i] - k.vmoy[i + 1] * k.invrmed[i + 1]);
+               fabs(__ldcg(k.vmoy + i) * k.invrmed[i] - __ldcg(k.vmoy + i + 1) * k.invrmed[i + 1]);
     if (d < m) m = d;
   }
   const double newdt_cells = block_min<FB_BS>(m, sh);
   double f[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   for (int b = tid; b < k.n_partial_blocks; b += FB_BS) {
     const double *p = k.partials + (size_t)b * 5;
-    for (int q = 0; q < 5; q++) f[q] += p[q];
+    for (int q = 0; q < 5; q++) f[q] += __ldcg(p + q);
   }
   for (int q = 0; q < 5; q++) f[q] = block_sum<FB_BS>(f[q], sh);
   if (tid != 0) return;
@@ -403,8 +434,6 @@ __global__ void __launch_bounds__(FB_BS) k_controller(KP k)
   c->done = (c->dtemp < 0.999999999 * c->DT) ? 0 : 1;
   if (c->nonfinite) { c->status = FB_ERR_NAN; c->done = 1; }
 }
-
-void fb_launch_controller(const KP &k, cudaStream_t s) { k_controller<<<1, FB_BS, 0, s>>>(k); }
 
 // ------------------------------------------------------------ sound speed
 // ComputeSoundSpeed (SourceEuler.c:2323-2343), energy equation, and the
@@ -889,29 +918,37 @@ static __device__ __forceinline__ int wrapj(int j, int ns) { return j < 0 ? j + 
 // vtheta (:515-547), the energy floor (SourceEuler.c:2524) and the
 // sub-Keplerian edge rings (SideEuler.c:1008-1044).
 //
-// One CTA per ring holds the ring of every transported quantity in shared
-// memory (the periodic azimuthal stencil needs no halo exchange).  Each
-// thread owns E consecutive azimuths and evaluates the whole van Leer
-// chain of a quantity for them in registers (ratios, slopes, interface
-// values, flux difference), reading its +-2 neighbours from shared memory;
-// one barrier per quantity separates the reads from the in-place writes.
+// One CTA per ring with the ring's NQ quantities in shared memory.  Thread t
+// owns the E cells t, t+T, t+2T, ... (T = blockDim.x), so every shared-memory
+// sweep is bank-conflict free and a ring of up to 1024*E cells keeps 24-32
+// warps busy.  Per pass and quantity the face values go through two
+// shared-memory stages: W = q/(RhoInt+1e-20) for the own cells, then the van
+// Leer slope DQ of the own cells; each thread then forms the upwind values at
+// both faces of its cells and updates them.  W and DQ are double-buffered
+// across quantities, so a quantity costs two barriers.  The arithmetic is
+// the reference's, term for term (ComputeStarTheta :392-433, VanLeerTheta
+// :435-465); only the work split differs.
+//
+// shared memory: NQ rings of quantities, the residual velocity, W[2], DQ[2]
+#define FB_AZI_RINGS(NQ) ((NQ) + 5)
+template <int E> struct AziMaxThreads { static const int value = (E <= 2) ? 1024 : 768; };
 template <int NQ, int E>
-__global__ void __launch_bounds__(512) k_transport_azimuthal(KP k, double dtov)
+__global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal(KP k, double dtov)
 {
   extern __shared__ double smem[];
   __shared__ double sh[32];
   const double dt = dt_of(k, dtov);
-  const int i = blockIdx.x, ns = k.ns, nr = k.nr;
+  const int i = blockIdx.x, ns = k.ns, nr = k.nr, T = blockDim.x, tid = threadIdx.x;
   const size_t base = (size_t)i * ns;
-  double *Q = smem;             // NQ rings
-  double *vres = Q + NQ * ns;   // residual azimuthal velocity
-  const int a = threadIdx.x * E;
-  for (int j = threadIdx.x; j < ns; j += blockDim.x)
+  double *Q = smem;              // NQ rings
+  double *vres = Q + NQ * ns;    // residual azimuthal velocity
+  double *DR = vres + 4 * ns;    // density slopes: the second DQ buffer
+  for (int j = tid; j < ns; j += T)
     for (int q = 0; q < NQ; q++) Q[q * ns + j] = k.q[q][base + j];
   // ComputeThetaElongations / ComputeAverageThetaVelocities / ComputeResiduals
   const double invdt = 1.0 / dt;
   double s = 0.0;
-  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+  for (int j = tid; j < ns; j += T) {
     double elong = k.vt[base + j] * dt;
     s += elong * invdt;
   }
@@ -923,90 +960,109 @@ __global__ void __launch_bounds__(512) k_transport_azimuthal(KP k, double dtov)
   const double Nround = floor(Ntilde + 0.5);
   const long nshift = (long)Nround;
   double vconst = (Ntilde - Nround) * k.rmed[i] * invdt * dpinvns;
-  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+  for (int j = tid; j < ns; j += T) {
     double elong = k.vt[base + j] * dt;
     double v = elong * invdt - VMed;
     if (!k.fast_transport) v = vconst + v;
     vres[j] = v;
   }
   if (!k.fast_transport) vconst = 0.0;
-  __syncthreads();
   const double dxtheta = k.dxtheta[i], invdxtheta = k.invdxtheta[i];
   const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
   const double invsurf = 1.0 / k.surf[i];
   const double *rho = Q + (NQ - 1) * ns;
+#define jc(e) (tid + (e) * T)  // own cells (valid while < ns)
   for (int pass = 0; pass < 2; pass++) {
     const bool uniform = (pass == 1);
     if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
-    // RhoStar (ComputeStarTheta(Rho, V, RhoStar)) for j = a .. a+E; RhoInt is
-    // the density before this pass, i.e. Q[rho] until the last quantity.
-    double R_[E + 4], DR[E + 2], RS[E + 1], V[E + 1];
+    __syncthreads();  // Q and vres complete
+    // RhoStar (ComputeStarTheta(Rho, V, RhoStar)); RhoInt is the density
+    // before this pass, kept in registers for the own cells.
+    double R[E], RSl[E], RSh[E], Vl[E], Vh[E];
 #pragma unroll
-    for (int t = 0; t < E + 4; t++) R_[t] = (a < ns) ? rho[wrapj(a - 2 + t, ns)] : 0.0;
-#pragma unroll
-    for (int t = 0; t < E + 2; t++) {
-      double dqm = (R_[t + 1] - R_[t]);
-      double dqp = (R_[t + 2] - R_[t + 1]);
-      DR[t] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
-    }
-#pragma unroll
-    for (int t = 0; t < E + 1; t++) {
-      const double v = uniform ? vconst : ((a < ns) ? vres[wrapj(a + t, ns)] : 0.0);
-      V[t] = v;
-      const double ksi = v * dt;
-      RS[t] = (ksi > 0.0) ? R_[t + 1] + (dxtheta - ksi) * DR[t] : R_[t + 2] - (dxtheta + ksi) * DR[t + 1];
-    }
-    for (int q = 0; q < NQ; q++) {
-      double *qb = Q + q * ns;
-      double W[E + 4], q0[E];
-#pragma unroll
-      for (int t = 0; t < E + 4; t++) W[t] = (a < ns) ? qb[wrapj(a - 2 + t, ns)] / (R_[t] + 1e-20) : 0.0;
-#pragma unroll
-      for (int t = 0; t < E; t++) q0[t] = (a + t < ns) ? qb[a + t] : 0.0;
-      __syncthreads();  // every read of this quantity precedes its updates
-      double DQ[E + 2], QS[E + 1];
-#pragma unroll
-      for (int t = 0; t < E + 2; t++) {
-        double dqm = (W[t + 1] - W[t]);
-        double dqp = (W[t + 2] - W[t + 1]);
-        DQ[t] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
-      }
-#pragma unroll
-      for (int t = 0; t < E + 1; t++) {
-        const double ksi = V[t] * dt;
-        QS[t] = (ksi > 0.0) ? W[t + 1] + (dxtheta - ksi) * DQ[t] : W[t + 2] - (dxtheta + ksi) * DQ[t + 1];
-      }
-#pragma unroll
-      for (int t = 0; t < E; t++) {
-        if (a + t < ns) {
-          double varq = dxrad * QS[t] * RS[t] * V[t];
-          varq -= dxrad * QS[t + 1] * RS[t + 1] * V[t + 1];
-          qb[a + t] = q0[t] + varq * invsurf;
-        }
+    for (int e = 0; e < E; e++) {
+      const int j = jc(e);
+      if (j < ns) {
+        const double rm = rho[wrapj(j - 1, ns)], r0 = rho[j], rp = rho[wrapj(j + 1, ns)];
+        R[e] = r0;
+        const double dqm = (r0 - rm), dqp = (rp - r0);
+        DR[j] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
       }
     }
     __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const int j = jc(e);
+      if (j < ns) {
+        const int jm = wrapj(j - 1, ns), jp = wrapj(j + 1, ns);
+        const double vl = uniform ? vconst : vres[j], vh = uniform ? vconst : vres[jp];
+        Vl[e] = vl;
+        Vh[e] = vh;
+        const double kl = vl * dt, kh = vh * dt;
+        RSl[e] = (kl > 0.0) ? rho[jm] + (dxtheta - kl) * DR[jm] : R[e] - (dxtheta + kl) * DR[j];
+        RSh[e] = (kh > 0.0) ? R[e] + (dxtheta - kh) * DR[j] : rho[jp] - (dxtheta + kh) * DR[jp];
+      }
+    }
+    for (int q = 0; q < NQ; q++) {
+      double *qb = Q + q * ns;
+      double *W = vres + (1 + (q & 1)) * ns, *D = vres + (3 + (q & 1)) * ns;
+      double q0[E];
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int j = jc(e);
+        if (j < ns) {
+          q0[e] = qb[j];
+          W[j] = q0[e] / (R[e] + 1e-20);
+        }
+      }
+      __syncthreads();  // W complete (and, for q = 1, every read of DR done)
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int j = jc(e);
+        if (j < ns) {
+          const double w0 = W[j];
+          const double dqm = (w0 - W[wrapj(j - 1, ns)]), dqp = (W[wrapj(j + 1, ns)] - w0);
+          D[j] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+        }
+      }
+      __syncthreads();  // DQ complete
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const int j = jc(e);
+        if (j < ns) {
+          const int jm = wrapj(j - 1, ns), jp = wrapj(j + 1, ns);
+          const double kl = Vl[e] * dt, kh = Vh[e] * dt;
+          const double qsl = (kl > 0.0) ? W[jm] + (dxtheta - kl) * D[jm] : W[j] - (dxtheta + kl) * D[j];
+          const double qsh = (kh > 0.0) ? W[j] + (dxtheta - kh) * D[j] : W[jp] - (dxtheta + kh) * D[jp];
+          double varq = dxrad * qsl * RSl[e] * Vl[e];
+          varq -= dxrad * qsh * RSh[e] * Vh[e];
+          qb[j] = q0[e] + varq * invsurf;
+        }
+      }
+    }
   }
+  __syncthreads();
   // AdvectSHIFT (TransportEuler.c:350-373) for every quantity
   for (int q = 0; q < NQ; q++) {
     double *qb = Q + q * ns;
     double tmp[E];
 #pragma unroll
-    for (int t = 0; t < E; t++) {
-      long ji = ((long)(a + t) - nshift) % ns;
+    for (int e = 0; e < E; e++) {
+      const int j = jc(e);
+      long ji = ((long)j - nshift) % ns;
       if (ji < 0) ji += ns;
-      tmp[t] = (a + t < ns) ? qb[ji] : 0.0;
+      tmp[e] = (j < ns) ? qb[ji] : 0.0;
     }
     __syncthreads();
 #pragma unroll
-    for (int t = 0; t < E; t++)
-      if (a + t < ns) qb[a + t] = tmp[t];
+    for (int e = 0; e < E; e++)
+      if (jc(e) < ns) qb[jc(e)] = tmp[e];
   }
   __syncthreads();
   // ComputeVelocities, vtheta part; floors on energy; sub-Keplerian edges
   const double *tp = Q + 2 * ns, *tm = Q + 3 * ns;
   const int subkep = (!k.transport_only) && (i == 0 || i == nr - 1);
-  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
+  for (int j = tid; j < ns; j += T) {
     const int jm = (j == 0) ? ns - 1 : j - 1;
     double v = (tp[jm] + tm[j]) / (rho[j] + rho[jm] + 1e-20) / k.rmed[i] - k.rmed[i] * k.omega_frame;
     if (subkep) v = k.vthetamed[i] - k.rmed[i] * k.omega_frame;
@@ -1023,9 +1079,21 @@ __global__ void __launch_bounds__(512) k_transport_azimuthal(KP k, double dtov)
       k.e[base + j] = e;
     }
   }
+#undef jc
 }
 
-#define FB_AZI_E 6
+// cells per thread of the azimuthal pass (1..4): 1024 threads for up to 2
+// cells each, 768 threads above (more registers per thread)
+static int azi_cells_per_thread(int ns)
+{
+  if (ns <= 2048) return (ns + 1023) / 1024;
+  return (ns + 767) / 768;
+}
+static int azi_threads(int ns)
+{
+  const int E = azi_cells_per_thread(ns);
+  return (((ns + E - 1) / E) + 31) / 32 * 32;
+}
 
 // ComputeVelocities' radial part (TransportEuler.c:531-536) needs the
 // neighbouring ring after both passes; fused with AddFloorDensity
@@ -1086,17 +1154,25 @@ void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
     k_transport_radial<5><<<gr, tx, 0, s>>>(k, dt_override, chunk);
 }
 
-static int azi_threads(int ns) { return (((ns + FB_AZI_E - 1) / FB_AZI_E) + 31) / 32 * 32; }
+template <int NQ>
+static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
+{
+  const size_t smem = (size_t)FB_AZI_RINGS(NQ) * k.ns * sizeof(double);
+  const int th = azi_threads(k.ns);
+  switch (azi_cells_per_thread(k.ns)) {
+    case 1: k_transport_azimuthal<NQ, 1><<<k.nr, th, smem, s>>>(k, dt_override); break;
+    case 2: k_transport_azimuthal<NQ, 2><<<k.nr, th, smem, s>>>(k, dt_override); break;
+    case 3: k_transport_azimuthal<NQ, 3><<<k.nr, th, smem, s>>>(k, dt_override); break;
+    default: k_transport_azimuthal<NQ, 4><<<k.nr, th, smem, s>>>(k, dt_override); break;
+  }
+}
 
 void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s)
 {
-  const int NQ = k.energy ? 6 : 5;
-  const size_t smem = (size_t)(NQ + 1) * k.ns * sizeof(double);
-  const int th = azi_threads(k.ns);
   if (k.energy)
-    k_transport_azimuthal<6, FB_AZI_E><<<k.nr, th, smem, s>>>(k, dt_override);
+    launch_azimuthal<6>(k, dt_override, s);
   else
-    k_transport_azimuthal<5, FB_AZI_E><<<k.nr, th, smem, s>>>(k, dt_override);
+    launch_azimuthal<5>(k, dt_override, s);
 }
 
 void fb_launch_transport_vr(const KP &k, cudaStream_t s)
@@ -1285,15 +1361,21 @@ int fb_allow_max_dynamic_smem(const void *func)
 int fb_gas_prepare(int ns, int energy)
 {
   const int NQ = energy ? 6 : 5;
-  const size_t smem = (size_t)(NQ + 1) * ns * sizeof(double);
+  const size_t smem = (size_t)FB_AZI_RINGS(NQ) * ns * sizeof(double);
   int dev = 0, maxopt = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem + 32 * sizeof(double) > (size_t)maxopt) return FB_ERR_UNSUPPORTED;
-  if (azi_threads(ns) > 512 || ns < 16) return FB_ERR_UNSUPPORTED;
-  int rc = fb_allow_max_dynamic_smem((const void *)k_transport_azimuthal<5, FB_AZI_E>);
-  if (!rc) rc = fb_allow_max_dynamic_smem((const void *)k_transport_azimuthal<6, FB_AZI_E>);
-  return rc;
+  if (azi_cells_per_thread(ns) > 4 || ns < 16) return FB_ERR_UNSUPPORTED;
+  const void *fns[] = {(const void *)k_transport_azimuthal<5, 1>, (const void *)k_transport_azimuthal<5, 2>,
+                       (const void *)k_transport_azimuthal<5, 3>, (const void *)k_transport_azimuthal<5, 4>,
+                       (const void *)k_transport_azimuthal<6, 1>, (const void *)k_transport_azimuthal<6, 2>,
+                       (const void *)k_transport_azimuthal<6, 3>, (const void *)k_transport_azimuthal<6, 4>};
+  for (const void *f : fns) {
+    int rc = fb_allow_max_dynamic_smem(f);
+    if (rc) return rc;
+  }
+  return FB_OK;
 }
 
 // Loop condition of the captured substep graph: keep going while the

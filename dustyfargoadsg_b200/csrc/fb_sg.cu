@@ -99,13 +99,18 @@ static FftArgs fft_args(const fb_fft_plan &p)
 }
 
 // One radix-R pass of a Stockham autosort FFT (all of v[] in registers).
-template <int R, int INV>
-static __device__ __forceinline__ void fft_pass(const double2 *__restrict__ x, double2 *__restrict__ y,
+// NL lines of length n lie back to back in x and y.
+template <int R, int INV, int NL>
+static __device__ __forceinline__ void fft_pass(const double2 *__restrict__ x0, double2 *__restrict__ y0,
                                                 int n, int L, const double2 *__restrict__ tw)
 {
   const int nr_ = n / R;
   const int tstride = n / (L * R);
-  for (int j = threadIdx.x; j < nr_; j += blockDim.x) {
+  for (int jj = threadIdx.x; jj < NL * nr_; jj += blockDim.x) {
+    const int line = (NL == 1) ? 0 : jj / nr_;
+    const int j = jj - line * nr_;
+    const double2 *__restrict__ x = x0 + (size_t)line * n;
+    double2 *__restrict__ y = y0 + (size_t)line * n;
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) v[r] = x[j + r * nr_];
@@ -168,7 +173,7 @@ static __device__ __forceinline__ void fft_pass(const double2 *__restrict__ x, d
 // Stockham autosort FFT of length a.n in shared memory; x holds the input,
 // y is scratch; returns the buffer holding the natural-order result.
 // inv = 0: sum_j x_j exp(-2 pi i jk/n); inv = 1: exp(+2 pi i jk/n); no scaling.
-template <int INV>
+template <int INV, int NL>
 static __device__ double2 *fft_smem_t(double2 *x, double2 *y, const FftArgs &a)
 {
   const int n = a.n;
@@ -177,10 +182,10 @@ static __device__ double2 *fft_smem_t(double2 *x, double2 *y, const FftArgs &a)
     const int R = a.radix[s];
     __syncthreads();
     switch (R) {
-      case 4: fft_pass<4, INV>(x, y, n, L, a.tw); break;
-      case 2: fft_pass<2, INV>(x, y, n, L, a.tw); break;
-      case 3: fft_pass<3, INV>(x, y, n, L, a.tw); break;
-      default: fft_pass<5, INV>(x, y, n, L, a.tw); break;
+      case 4: fft_pass<4, INV, NL>(x, y, n, L, a.tw); break;
+      case 2: fft_pass<2, INV, NL>(x, y, n, L, a.tw); break;
+      case 3: fft_pass<3, INV, NL>(x, y, n, L, a.tw); break;
+      default: fft_pass<5, INV, NL>(x, y, n, L, a.tw); break;
     }
     double2 *t = x;
     x = y;
@@ -193,7 +198,7 @@ static __device__ double2 *fft_smem_t(double2 *x, double2 *y, const FftArgs &a)
 
 static __device__ __forceinline__ double2 *fft_smem(double2 *x, double2 *y, const FftArgs &a, int inv)
 {
-  return inv ? fft_smem_t<1>(x, y, a) : fft_smem_t<0>(x, y, a);
+  return inv ? fft_smem_t<1, 1>(x, y, a) : fft_smem_t<0, 1>(x, y, a);
 }
 
 // ------------------------------------------------------------------ kernels
@@ -234,31 +239,45 @@ __global__ void __launch_bounds__(SG_BS) sg_rows_fwd(FftArgs fa, int nrows, int 
 // Column pass.  mode 0: forward transform of the kernel half spectra into
 // [k][m] layout (setup).  mode 1: forward, product with -G Khat
 // (sgacc.c:25-38), inverse, keep rows < nrows_in.
+// KC adjacent wavenumbers per CTA: a warp's loads and stores then cover
+// whole 32-byte sectors of the [ring][k] spectra (KC*16 bytes per ring)
+// instead of half sectors, and the KC transforms share each FFT pass.
+#define SG_KC 2
 __global__ void __launch_bounds__(SG_BS) sg_cols(FftArgs fa, int nrows_in, int nk, int mode,
                                                   double2 *data_r, double2 *data_t,
                                                   double2 *kh_r, double2 *kh_t)
 {
   extern __shared__ double2 sm[];
   const int m = fa.n;
-  double2 *x = sm, *y = sm + m;
-  const int k = blockIdx.x;
+  double2 *x = sm, *y = sm + SG_KC * m;  // SG_KC lines each
+  const int k0 = blockIdx.x * SG_KC;
   const int which = blockIdx.y;  // 0: r, 1: t
   double2 *data = which ? data_t : data_r;
   double2 *kh = which ? kh_t : kh_r;
-  for (int i = threadIdx.x; i < m; i += blockDim.x)
-    x[i] = (i < nrows_in) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
-  double2 *X = fft_smem(x, y, fa, 0);
+  for (int t = threadIdx.x; t < SG_KC * m; t += blockDim.x) {
+    const int i = t / SG_KC, c = t - i * SG_KC, k = k0 + c;
+    x[(size_t)c * m + i] = (i < nrows_in && k < nk) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
+  }
+  double2 *X = fft_smem_t<0, SG_KC>(x, y, fa);
   if (mode == 0) {
-    for (int i = threadIdx.x; i < m; i += blockDim.x) kh[(size_t)k * m + i] = X[i];
+    for (int c = 0; c < SG_KC; c++)
+      if (k0 + c < nk)
+        for (int i = threadIdx.x; i < m; i += blockDim.x) kh[(size_t)(k0 + c) * m + i] = X[(size_t)c * m + i];
     return;
   }
-  for (int i = threadIdx.x; i < m; i += blockDim.x) {
-    const double2 K = kh[(size_t)k * m + i], S = X[i];
-    X[i] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
+  for (int t = threadIdx.x; t < SG_KC * m; t += blockDim.x) {
+    const int c = t / m, i = t - c * m, k = k0 + c;
+    if (k < nk) {
+      const double2 K = kh[(size_t)k * m + i], S = X[t];
+      X[t] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
+    }
   }
   double2 *Y = (X == x) ? y : x;
-  double2 *W = fft_smem(X, Y, fa, 1);
-  for (int i = threadIdx.x; i < nrows_in; i += blockDim.x) data[(size_t)i * nk + k] = W[i];
+  double2 *W = fft_smem_t<1, SG_KC>(X, Y, fa);
+  for (int t = threadIdx.x; t < SG_KC * nrows_in; t += blockDim.x) {
+    const int i = t / SG_KC, c = t - i * SG_KC, k = k0 + c;
+    if (k < nk) data[(size_t)i * nk + k] = W[(size_t)c * m + i];
+  }
 }
 
 // Inverse row pass + sgacc.c:138-161: normalisation, self-force.
@@ -338,7 +357,7 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   if (!rc) rc = make_plan(&sg->pcol, m);
   if (rc) { fb_sg_destroy(sg); return rc; }
   sg->smem_row = 2 * (size_t)ns * sizeof(double2);
-  sg->smem_col = 2 * (size_t)m * sizeof(double2);
+  sg->smem_col = 2 * (size_t)SG_KC * m * sizeof(double2);
   int dev = 0, maxopt = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
@@ -409,7 +428,7 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   cudaMemcpy(dkt, kt.data(), kt.size() * sizeof(double), cudaMemcpyHostToDevice);
   FftArgs fr = fft_args(sg->prow), fc = fft_args(sg->pcol);
   sg_rows_fwd<<<m, SG_BS, sg->smem_row, s>>>(fr, m, ns, nk, NULL, NULL, NULL, 1.0, dkr, dkt, hr, ht);
-  sg_cols<<<dim3(nk, 2), SG_BS, sg->smem_col, s>>>(fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
+  sg_cols<<<dim3((nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s>>>(fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
   cudaError_t e = cudaStreamSynchronize(s);
   cudaFree(dkr); cudaFree(dkt); cudaFree(hr); cudaFree(ht);
   if (e != cudaSuccess) { fb_sg_destroy(sg); return FB_ERR_CUDA; }
@@ -438,7 +457,8 @@ void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 void fb_sg_cols(fb_sg *sg, cudaStream_t s)
 {
   FftArgs fc = fft_args(sg->pcol);
-  sg_cols<<<dim3(sg->nk, 2), SG_BS, sg->smem_col, s>>>(fc, sg->nr, sg->nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
+  sg_cols<<<dim3((sg->nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s>>>(fc, sg->nr, sg->nk, 1, sg->xr, sg->xt,
+                                                                         sg->khr, sg->kht);
 }
 
 void fb_sg_rows_inv(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
