@@ -55,7 +55,7 @@ class Disc:
 
     DUST_ARRAYS = ("r", "th", "vr", "vth", "l", "size", "stokes")
 
-    def __init__(self, params, noise=0.0, seed=0, state=None, dust_seed=None):
+    def __init__(self, params, noise=0.0, seed=0, state=None, dust_seed=None, tuning=None):
         self.lib = load()
         if isinstance(params, (str, os.PathLike)):
             params = read_par(params)
@@ -66,6 +66,8 @@ class Disc:
         self.nf = (self.nr + 1) * self.ns
         self.ctx = C.c_void_p()
         check(self.lib.fb_create(C.byref(self.p), None, C.byref(self.ctx)), "fb_create")
+        if tuning is not None:
+            self.set_tuning(tuning)
         self.fields = {k: np.zeros(self.nf) for k in ("dens", "vrad", "vtheta", "energy")}
         self.prof = {k: np.zeros(self.nr) for k in
                      ("sigma_med", "sigma_inf", "energy_med", "vtheta_med", "vrad_med", "global_soundspeed")}
@@ -96,6 +98,26 @@ class Disc:
             check(self.lib.fb_init_dust(C.byref(self.p), self.ctx, int(seed if dust_seed is None else dust_seed),
                                         C.byref(self.dst)), "fb_init_dust", self.ctx)
             check(self.lib.fb_dust_upload(self.ctx, C.byref(self.dst)), "fb_dust_upload", self.ctx)
+
+    # -- launch shapes --------------------------------------------------
+    def set_tuning(self, tuning):
+        """Apply launch shapes: a dict of fb_tuning fields, or a tuning table
+        ({"iso"|"energy": {"NrxNs": entry}}) looked up for this grid."""
+        entry = tuning
+        if "iso" in tuning or "energy" in tuning:
+            kind = "energy" if self.p.energy_equation else "iso"
+            entry = tuning.get(kind, {}).get("%dx%d" % (self.p.nrad, self.p.nsec))
+            if entry is None:
+                return False
+        t = _ffi.FbTuning(*[int(entry.get(f, 0)) for f in
+                            ("cell_block", "azi_cells_per_thread", "rad_columns", "rad_rings")])
+        check(self.lib.fb_set_tuning(self.ctx, C.byref(t)), "fb_set_tuning", self.ctx)
+        return True
+
+    def tuning(self):
+        t = _ffi.FbTuning()
+        check(self.lib.fb_get_tuning(self.ctx, C.byref(t)), "fb_get_tuning", self.ctx)
+        return {f: getattr(t, f) for f, _ in t._fields_}
 
     # -- particles ------------------------------------------------------
     def set_dust(self, state):

@@ -89,6 +89,10 @@ class FbDustState(C.Structure):
     ]
 
 
+class FbTuning(C.Structure):
+    _fields_ = [("cell_block", _I), ("azi_cells_per_thread", _I), ("rad_columns", _I), ("rad_rings", _I)]
+
+
 class FbStepReport(C.Structure):
     _fields_ = [
         ("substeps", _I), ("status", _I), ("physical_time", _D), ("mindt", _D), ("maxdt", _D),
@@ -106,7 +110,7 @@ EXPORTS = (
     "fb_build_info", "fb_struct_size", "fb_kernel_launches", "fb_profile", "fb_profile_read",
     "fb_select_device", "fb_transport_noalloc", "fb_noalloc_last_error", "fb_init_dust",
     "fb_dust_upload", "fb_dust_download", "fb_vortensity", "fb_batch_create", "fb_batch_algogas",
-    "fb_batch_destroy",
+    "fb_batch_destroy", "fb_get_tuning", "fb_set_tuning", "fb_tune",
 )
 
 _lib = None
@@ -154,6 +158,9 @@ def load():
         "fb_batch_create": (_I, [C.POINTER(vp), _I, C.POINTER(vp)]),
         "fb_batch_algogas": (_I, [vp, C.POINTER(FbStepReport)]),
         "fb_batch_destroy": (_I, [vp]),
+        "fb_get_tuning": (_I, [vp, C.POINTER(FbTuning)]),
+        "fb_set_tuning": (_I, [vp, C.POINTER(FbTuning)]),
+        "fb_tune": (_I, [vp, _I, C.POINTER(FbTuning), C.POINTER(_D)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -165,7 +172,7 @@ def load():
 
 
 def check_layout(lib):
-    for idx, cls in enumerate((FbParams, FbPlanets, FbState, FbProfiles, FbStepReport, FbDustState)):
+    for idx, cls in enumerate((FbParams, FbPlanets, FbState, FbProfiles, FbStepReport, FbDustState, FbTuning)):
         want = lib.fb_struct_size(idx)
         if want != C.sizeof(cls):
             raise RuntimeError("ABI mismatch for %s: C %d bytes, ctypes %d" % (cls.__name__, want, C.sizeof(cls)))

@@ -380,6 +380,10 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.masstaper = p->masstaper;
   k.self_gravity = p->self_gravity;
   k.transport_only = 0;
+  k.cell_bs = 128;  // launch shapes: automatic until tuned
+  k.azi_E = 0;
+  k.rad_tx = 0;
+  k.rad_chunk = 0;
   ctx->substep_cap = 1000000;
   {
     const char *cap = getenv("FB_MAX_SUBSTEPS");
@@ -1074,4 +1078,185 @@ extern "C" int fb_batch_algogas(fb_batch *b, fb_step_report *reps)
     }
   }
   return status;
+}
+
+// ------------------------------------------------------------ tuning
+// Launch shapes of the per-cell, azimuthal and radial kernels.  No
+// counterpart in the reference.  fb_tune times candidates on this context's
+// own disc (a few substeps each, per-stage CUDA events) from a saved state,
+// which it restores afterwards, so tuning does not advance the disc.
+static void invalidate_graph(fb_ctx *ctx)
+{
+  if (ctx->gdt_exec) cudaGraphExecDestroy(ctx->gdt_exec);
+  if (ctx->gdt) cudaGraphDestroy(ctx->gdt);
+  ctx->gdt_exec = NULL;
+  ctx->gdt = NULL;
+  if (ctx->graph_state == 1) ctx->graph_state = 0;
+}
+
+extern "C" int fb_get_tuning(const fb_ctx *ctx, fb_tuning *t)
+{
+  if (!ctx || !t) return FB_ERR_INVALID;
+  const KP &k = ctx->k;
+  t->cell_block = k.cell_bs;
+  t->azi_cells_per_thread = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
+  t->rad_columns = k.rad_tx > 0 ? k.rad_tx : 64;
+  t->rad_rings = k.rad_chunk > 0 ? k.rad_chunk : fb_rad_chunk_auto(k);
+  return FB_OK;
+}
+
+extern "C" int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t)
+{
+  if (!ctx || !t) return FB_ERR_INVALID;
+  KP &k = ctx->k;
+  const int cb = t->cell_block ? t->cell_block : 128;
+  if (cb < 32 || cb > 256 || cb % 32) return FB_ERR_INVALID;
+  if (t->azi_cells_per_thread && !fb_azi_E_valid(k.ns, k.energy, t->azi_cells_per_thread)) return FB_ERR_INVALID;
+  if (t->rad_columns && (t->rad_columns < 32 || t->rad_columns > 128 || t->rad_columns % 32)) return FB_ERR_INVALID;
+  if (t->rad_rings < 0 || t->rad_rings > k.nr) return FB_ERR_INVALID;
+  k.cell_bs = cb;
+  k.azi_E = t->azi_cells_per_thread;
+  k.rad_tx = t->rad_columns;
+  k.rad_chunk = t->rad_rings;
+  invalidate_graph(ctx);
+  return FB_OK;
+}
+
+namespace {
+struct Snapshot {
+  std::vector<std::pair<void *, size_t>> regions;
+  std::vector<void *> copies;
+};
+}  // namespace
+
+static int snapshot_take(fb_ctx *ctx, Snapshot &sn)
+{
+  KP &k = ctx->k;
+  const size_t nf = ctx->nf * sizeof(double), nr = (size_t)ctx->nr * sizeof(double);
+  sn.regions = {{k.rho, nf}, {k.vr, nf}, {k.vt, nf}, {k.e, nf}, {k.cs, nf}, {k.gcs, nr},
+                {k.lost0, (size_t)ctx->ns * sizeof(double)}, {ctx->d_ctl, sizeof(fb_ctl)}};
+  if (ctx->has_dust) {
+    PP &pp = ctx->pp;
+    const size_t np = (size_t)pp.n * sizeof(double);
+    double *g[] = {k.indpot, k.rgp, k.agp, k.rind, k.aind, k.rsga, k.asga};
+    for (double *f : g) sn.regions.push_back({f, nf});
+    double *a[] = {pp.r, pp.th, pp.vr, pp.vth, pp.l, pp.st};
+    for (double *f : a) sn.regions.push_back({f, np});
+    sn.regions.push_back({pp.dc, sizeof(fb_dust_ctl)});
+  }
+  for (auto &r : sn.regions) {
+    void *c = NULL;
+    if (cudaMalloc(&c, r.second) != cudaSuccess) return FB_ERR_NOMEM;
+    sn.copies.push_back(c);
+    CK(cudaMemcpyAsync(c, r.first, r.second, cudaMemcpyDeviceToDevice, ctx->st));
+  }
+  return FB_OK;
+}
+
+static int snapshot_restore(fb_ctx *ctx, const Snapshot &sn)
+{
+  for (size_t q = 0; q < sn.copies.size(); q++)
+    CK(cudaMemcpyAsync(sn.regions[q].first, sn.copies[q], sn.regions[q].second, cudaMemcpyDeviceToDevice, ctx->st));
+  return FB_OK;
+}
+
+static void snapshot_free(Snapshot &sn)
+{
+  for (void *c : sn.copies) cudaFree(c);
+  sn.copies.clear();
+}
+
+// Runs `substeps` substeps from the snapshot with per-stage events; returns
+// the summed device ms of the stages in `stages` (per substep), or < 0.
+static double tune_measure(fb_ctx *ctx, const Snapshot &sn, int substeps, const int *stages, int nst)
+{
+  if (snapshot_restore(ctx, sn)) return -1.0;
+  for (int q = 0; q < FB_NSTAGE; q++) { ctx->pms[q] = 0.0; ctx->pcount[q] = 0; }
+  cudaStream_t s = ctx->st;
+  const long long l0 = ctx->launches;
+  enqueue_dt_prelude(ctx);
+  for (int it = 0; it < substeps + 1; it++) {
+    if (it == 1)  // the first substep warms caches and is not counted
+      for (int q = 0; q < FB_NSTAGE; q++) { ctx->pms[q] = 0.0; ctx->pcount[q] = 0; }
+    const int npt = enqueue_substep(ctx);
+    if (cudaMemcpyAsync(ctx->h_ctl, ctx->d_ctl, sizeof(fb_ctl), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      cudaGetLastError();
+      return -1.0;
+    }
+    profile_collect(ctx, npt);
+    if (ctx->h_ctl->status) return -1.0;
+    if (ctx->h_ctl->done) enqueue_dt_prelude(ctx);  // start another DT from here
+  }
+  ctx->launches = l0;
+  double ms = 0.0;
+  for (int q = 0; q < nst; q++) ms += ctx->pms[stages[q]];
+  return ms / substeps;
+}
+
+extern "C" int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_out)
+{
+  if (!ctx || substeps < 1) return FB_ERR_INVALID;
+  if (!ctx->uploaded || (ctx->has_dust && !ctx->dust_uploaded)) return FB_ERR_STATE;
+  KP &k = ctx->k;
+  int rc = fb_profile(ctx, 1);
+  if (rc) return rc;
+  Snapshot sn;
+  rc = snapshot_take(ctx, sn);
+  if (rc) { snapshot_free(sn); fb_profile(ctx, 0); return rc; }
+  const int cell_stages[] = {ST_POT, ST_SUB1, ST_VTERMS, ST_VUPDATE, ST_SUB2, ST_EVTERMS, ST_TVR};
+  const int azi_stage[] = {ST_TAZI};
+  const int rad_stage[] = {ST_TRAD};
+  double total = 0.0;
+  // 1. per-cell CTA width
+  {
+    const int cand[] = {64, 128, 256};
+    int bestv = k.cell_bs;
+    double bestms = 1e300;
+    for (int c : cand) {
+      k.cell_bs = c;
+      const double ms = tune_measure(ctx, sn, substeps, cell_stages, 7);
+      if (ms >= 0.0 && ms < bestms) { bestms = ms; bestv = c; }
+    }
+    k.cell_bs = bestv;
+    total += bestms;
+  }
+  // 2. cells per thread of the azimuthal pass
+  {
+    int bestv = k.azi_E;
+    double bestms = 1e300;
+    for (int E = 1; E <= 4; E++) {
+      if (!fb_azi_E_valid(k.ns, k.energy, E)) continue;
+      k.azi_E = E;
+      const double ms = tune_measure(ctx, sn, substeps, azi_stage, 1);
+      if (ms >= 0.0 && ms < bestms) { bestms = ms; bestv = E; }
+    }
+    k.azi_E = bestv;
+    total += bestms;
+  }
+  // 3. columns x rings per CTA of the radial pass
+  {
+    const int txs[] = {32, 64, 128}, chunks[] = {4, 8, 16, 32};
+    int btx = k.rad_tx, bch = k.rad_chunk;
+    double bestms = 1e300;
+    for (int tx : txs)
+      for (int ch : chunks) {
+        if (ch > k.nr) continue;
+        k.rad_tx = tx;
+        k.rad_chunk = ch;
+        const double ms = tune_measure(ctx, sn, substeps, rad_stage, 1);
+        if (ms >= 0.0 && ms < bestms) { bestms = ms; btx = tx; bch = ch; }
+      }
+    k.rad_tx = btx;
+    k.rad_chunk = bch;
+    total += bestms;
+  }
+  rc = snapshot_restore(ctx, sn);
+  if (!rc) rc = (cudaStreamSynchronize(ctx->st) == cudaSuccess) ? FB_OK : FB_ERR_CUDA;
+  snapshot_free(sn);
+  fb_profile(ctx, 0);
+  invalidate_graph(ctx);
+  if (best) fb_get_tuning(ctx, best);
+  if (ms_out) *ms_out = total;
+  return rc;
 }

@@ -90,6 +90,10 @@ struct KP {
   // DUSTFEEDBACK: the substep is also bounded by half the particles' minimum
   // stopping time (SourceEuler.c:1501-1507); NULL otherwise
   const double *dust_min_ts;
+  // launch shapes (tuning): per-cell CTA width, cells per thread of the
+  // azimuthal pass (0 = automatic), columns per CTA and rings per CTA of the
+  // radial pass (0 = automatic)
+  int cell_bs, azi_E, rad_tx, rad_chunk;
 };
 
 // Device state of the particles' random stream (src/DustUpdate.c:438-485).
@@ -138,6 +142,10 @@ void fb_launch_diag(const KP &k, double *out2, cudaStream_t s);
 void fb_launch_derived(const KP &k, int which, double *out, cudaStream_t s);
 void fb_launch_boundary_only(const KP &k, cudaStream_t s);
 int  fb_gas_prepare(int ns, int energy);  // kernel attributes (shared memory)
+// launch-shape candidates the tuner may try (fb_gas.cu)
+int  fb_azi_E_valid(int ns, int energy, int E);   // 1 if E cells/thread fit this ring
+int  fb_azi_E_auto(int ns);
+int  fb_rad_chunk_auto(const KP &k);
 int  fb_allow_max_dynamic_smem(const void *func);
 void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s);
 void fb_launch_loop_cond(const KP &k, cudaGraphConditionalHandle h, int cap, cudaStream_t s);

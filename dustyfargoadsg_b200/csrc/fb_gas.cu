@@ -13,10 +13,11 @@
 #include "fb_dev.cuh"
 
 #define FB_BS 256
-#define FB_BS2 128  // threads per CTA of the per-cell kernels: one ring row of 128 azimuths
+#define FB_BS2 256  // most threads per CTA of the per-cell kernels (k.cell_bs <= FB_BS2)
 
 // per-cell kernels: blockIdx.y = ring, 128 consecutive azimuths per CTA
-static inline dim3 grid2d(const KP &k, int rings) { return dim3((k.ns + FB_BS2 - 1) / FB_BS2, rings); }
+// per-cell kernels: CTAs of k.cell_bs azimuths (a ring segment) times rings
+static inline dim3 grid2d(const KP &k, int rings) { return dim3((k.ns + k.cell_bs - 1) / k.cell_bs, rings); }
 
 static __device__ __forceinline__ double min2(double a, double b) { return (b < a) ? b : a; }  // SourceEuler.c:293
 static __device__ __forceinline__ double max2(double a, double b) { return (b > a) ? b : a; }  // SourceEuler.c:300
@@ -504,7 +505,7 @@ __global__ void __launch_bounds__(FB_BS2) k_potential(KP k)
 
 void fb_launch_potential(const KP &k, cudaStream_t s)
 {
-  k_potential<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k);
+  k_potential<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k);
 }
 
 // ------------------------------------------------------------ SubStep1
@@ -561,7 +562,7 @@ __global__ void __launch_bounds__(FB_BS2) k_substep1(KP k)
 
 void fb_launch_substep1(const KP &k, cudaStream_t s)
 {
-  k_substep1<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k);
+  k_substep1<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k);
 }
 
 // ------------------------------------------------------- viscous stresses
@@ -599,7 +600,7 @@ __global__ void __launch_bounds__(FB_BS2) k_viscous_terms(KP k, const double *__
 
 void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s)
 {
-  k_viscous_terms<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k, vr, vt);
+  k_viscous_terms<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k, vr, vt);
 }
 
 // UpdateVelocitiesWithViscosity (Viscosity.c:305-378)
@@ -630,7 +631,7 @@ __global__ void __launch_bounds__(FB_BS2) k_viscous_update(KP k, double *vr, dou
 
 void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s)
 {
-  k_viscous_update<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k, vr, vt, dt_override);
+  k_viscous_update<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k, vr, vt, dt_override);
 }
 
 // ------------------------------------------------------------ SubStep2
@@ -690,7 +691,7 @@ __global__ void __launch_bounds__(FB_BS2) k_substep2(KP k)
 
 void fb_launch_substep2(const KP &k, cudaStream_t s)
 {
-  k_substep2<<<grid2d(k, k.nr + 1), FB_BS2, 0, s>>>(k);
+  k_substep2<<<grid2d(k, k.nr + 1), k.cell_bs, 0, s>>>(k);
 }
 
 // ComputeDivergenceVelocity (SourceEuler.c:2373-2412) on (Vrad, Vtheta)
@@ -711,7 +712,7 @@ __global__ void __launch_bounds__(FB_BS2) k_divergence(KP k)
 
 void fb_launch_divergence(const KP &k, cudaStream_t s)
 {
-  k_divergence<<<grid2d(k, k.nr), FB_BS2, 0, s>>>(k);
+  k_divergence<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k);
 }
 
 // ------------------------------------------------------------ SubStep3
@@ -1082,17 +1083,25 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
 #undef jc
 }
 
-// cells per thread of the azimuthal pass (1..4): 1024 threads for up to 2
-// cells each, 768 threads above (more registers per thread)
-static int azi_cells_per_thread(int ns)
+// cells per thread of the azimuthal pass (1..4): at most 1024 threads for
+// 1-2 cells each, 768 threads for 3-4 (more registers per thread).  The
+// automatic choice is the fewest cells per thread; the tuner may pick more.
+static int azi_max_threads(int E) { return E <= 2 ? 1024 : 768; }
+static int azi_threads_for(int ns, int E) { return (((ns + E - 1) / E) + 31) / 32 * 32; }
+int fb_azi_E_auto(int ns)
 {
-  if (ns <= 2048) return (ns + 1023) / 1024;
-  return (ns + 767) / 768;
+  for (int E = 1; E <= 4; E++)
+    if (azi_threads_for(ns, E) <= azi_max_threads(E)) return E;
+  return 5;  // ring too long
 }
-static int azi_threads(int ns)
+int fb_azi_E_valid(int ns, int energy, int E)
 {
-  const int E = azi_cells_per_thread(ns);
-  return (((ns + E - 1) / E) + 31) / 32 * 32;
+  if (E < 1 || E > 4 || azi_threads_for(ns, E) > azi_max_threads(E)) return 0;
+  const int NQ = energy ? 6 : 5;
+  int dev = 0, maxopt = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return (size_t)FB_AZI_RINGS(NQ) * ns * sizeof(double) + 32 * sizeof(double) <= (size_t)maxopt;
 }
 
 // ComputeVelocities' radial part (TransportEuler.c:531-536) needs the
@@ -1140,13 +1149,21 @@ __global__ void k_lostmass(KP k)
   if (threadIdx.x == 0) k.ctl->lost_mass += 0.0 + s;
 }
 
-void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
+// Rings per CTA of the radial pass when not tuned: 64-column CTAs, chunks
+// halving from 32 until there are >= 4 CTAs per SM (longer chunks reread
+// fewer halo rings, shorter ones fill the GPU).
+int fb_rad_chunk_auto(const KP &k)
 {
-  // 64 columns per CTA; ring chunks halve until there are >= 4 CTAs per SM
-  // (longer chunks reread fewer halo rings, shorter ones fill the GPU).
-  const int tx = 64, bx = (k.ns + tx - 1) / tx;
+  const int tx = k.rad_tx > 0 ? k.rad_tx : 64, bx = (k.ns + tx - 1) / tx;
   int chunk = 32;
   while (chunk > 4 && (long)bx * ((k.nr + chunk - 1) / chunk) < 4 * 148) chunk /= 2;
+  return chunk;
+}
+
+void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
+{
+  const int tx = k.rad_tx > 0 ? k.rad_tx : 64, bx = (k.ns + tx - 1) / tx;
+  const int chunk = k.rad_chunk > 0 ? k.rad_chunk : fb_rad_chunk_auto(k);
   dim3 gr(bx, (k.nr + chunk - 1) / chunk);
   if (k.energy)
     k_transport_radial<6><<<gr, tx, 0, s>>>(k, dt_override, chunk);
@@ -1158,8 +1175,9 @@ template <int NQ>
 static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
 {
   const size_t smem = (size_t)FB_AZI_RINGS(NQ) * k.ns * sizeof(double);
-  const int th = azi_threads(k.ns);
-  switch (azi_cells_per_thread(k.ns)) {
+  const int E = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
+  const int th = azi_threads_for(k.ns, E);
+  switch (E) {
     case 1: k_transport_azimuthal<NQ, 1><<<k.nr, th, smem, s>>>(k, dt_override); break;
     case 2: k_transport_azimuthal<NQ, 2><<<k.nr, th, smem, s>>>(k, dt_override); break;
     case 3: k_transport_azimuthal<NQ, 3><<<k.nr, th, smem, s>>>(k, dt_override); break;
@@ -1177,7 +1195,7 @@ void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t
 
 void fb_launch_transport_vr(const KP &k, cudaStream_t s)
 {
-  k_transport_vr<<<grid2d(k, k.nr + 1), FB_BS2, 0, s>>>(k);
+  k_transport_vr<<<grid2d(k, k.nr + 1), k.cell_bs, 0, s>>>(k);
   k_lostmass<<<1, 32, 0, s>>>(k);
 }
 
@@ -1366,7 +1384,7 @@ int fb_gas_prepare(int ns, int energy)
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem + 32 * sizeof(double) > (size_t)maxopt) return FB_ERR_UNSUPPORTED;
-  if (azi_cells_per_thread(ns) > 4 || ns < 16) return FB_ERR_UNSUPPORTED;
+  if (fb_azi_E_auto(ns) > 4 || ns < 16) return FB_ERR_UNSUPPORTED;
   const void *fns[] = {(const void *)k_transport_azimuthal<5, 1>, (const void *)k_transport_azimuthal<5, 2>,
                        (const void *)k_transport_azimuthal<5, 3>, (const void *)k_transport_azimuthal<5, 4>,
                        (const void *)k_transport_azimuthal<6, 1>, (const void *)k_transport_azimuthal<6, 2>,

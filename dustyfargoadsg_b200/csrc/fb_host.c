@@ -814,6 +814,7 @@ int fb_struct_size(int which)
     case 3: return (int)sizeof(fb_profiles);
     case 4: return (int)sizeof(fb_step_report);
     case 5: return (int)sizeof(fb_dust_state);
+    case 6: return (int)sizeof(fb_tuning);
     default: return -1;
   }
 }

@@ -141,6 +141,7 @@ extern "C" int fb_transport_noalloc(const fb_params *p, double *dens, double *vr
   k.nr = nr;
   k.ns = ns;
   k.nf = (size_t)(nr + 1) * ns;
+  k.cell_bs = 128;
   k.rho = dens;
   k.vr = vrad;
   k.vt = vtheta;

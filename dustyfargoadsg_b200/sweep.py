@@ -64,12 +64,13 @@ def write_disc_files(draw, workdir, tag, base_par=ISO_PAR):
     return par
 
 
-def make_discs(draws, workdir, noise=1e-4, seed=0):
-    """One Disc (device context, initial state uploaded) per draw."""
+def make_discs(draws, workdir, noise=1e-4, seed=0, tuning=None):
+    """One Disc (device context, initial state uploaded) per draw, with the
+    launch shapes of `tuning` (a table of tune.py) where it has the grid."""
     discs = []
     for d, draw in enumerate(draws):
         par = write_disc_files(draw, workdir, "disc%03d" % d)
-        discs.append(Disc(read_par(par), noise=noise, seed=seed))
+        discs.append(Disc(read_par(par), noise=noise, seed=seed, tuning=tuning))
     return discs
 
 

@@ -235,6 +235,21 @@ int fb_download_derived(fb_ctx *ctx, int which, double *out);
 /* Diagnostics on the device state: GasTotalMass (src/SideEuler.c:15) and
    GasMomentum (src/SideEuler.c:114). */
 int fb_diagnostics(fb_ctx *ctx, double *mass, double *momentum);
+/* ---- launch shapes (no counterpart in the reference) ---------------------
+   CTA width of the per-cell kernels (32..256, multiple of 32), cells per
+   thread of the azimuthal transport (1..4), columns (32/64/128) and rings
+   per CTA of the radial transport.  0 in fb_set_tuning means automatic;
+   fb_get_tuning reports the values in effect.  fb_tune times the candidates
+   on the context's own disc, `substeps` substeps each from a saved state
+   that it restores (the disc does not advance), keeps the fastest and
+   reports the summed ms per substep of the tuned stages. */
+typedef struct fb_tuning {
+  int cell_block, azi_cells_per_thread, rad_columns, rad_rings;
+} fb_tuning;
+int fb_get_tuning(const fb_ctx *ctx, fb_tuning *t);
+int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t);
+int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_per_substep);
+
 /* ---- batches of discs (no counterpart in the reference) ----------------- */
 /* Many discs -- contexts of any grid size and parameters on the current
    device, each uploaded -- advanced one DT each by one graph launch, their
@@ -308,7 +323,8 @@ int fb_profile_read(const fb_ctx *ctx, int idx, const char **name, double *ms, l
 /* Build information: "sm_100a fp64 ..." */
 const char *fb_build_info(void);
 /* sizeof of the ABI structs (0 fb_params, 1 fb_planets, 2 fb_state,
-   3 fb_profiles, 4 fb_step_report), for bindings to check their layout. */
+   3 fb_profiles, 4 fb_step_report, 5 fb_dust_state, 6 fb_tuning), for
+   bindings to check their layout. */
 int fb_struct_size(int which);
 
 #ifdef __cplusplus

@@ -1,0 +1,47 @@
+"""Launch-shape tuning (fb_tune / fb_set_tuning): the tuner must leave the
+disc exactly where it was, and a tuned disc must follow the same trajectory
+as an untuned one (shapes change the work split, not the arithmetic; only
+the order of the ring-mean sum of the azimuthal pass may differ)."""
+import os
+
+import numpy as np
+import pytest
+
+from tests import _oracle
+
+pytestmark = pytest.mark.gpu
+FIELDS = ("dens", "vrad", "vtheta")
+
+
+def test_tune_restores_state_and_keeps_results(tmp_path):
+    from dustyfargoadsg_b200 import Disc, read_par, tune
+    par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "iso_128x384.par"), str(tmp_path),
+                            Nrad=96, Nsec=288)
+    with Disc(read_par(par), noise=1e-4, seed=0) as a, Disc(read_par(par), noise=1e-4, seed=0) as b:
+        a.step()
+        b.step()
+        before = a.download()
+        entry = tune.tune_disc(a, substeps=2)
+        after = a.download()
+        for k in FIELDS:
+            np.testing.assert_array_equal(before[k], after[k], err_msg=k)
+        assert before["PhysicalTime"] == after["PhysicalTime"]
+        assert a.tuning() == {k: entry[k] for k in tune.FIELDS}
+        for _ in range(2):
+            ra, rb = a.step(), b.step()
+            assert ra.substeps == rb.substeps
+        sa, sb = a.download(), b.download()
+        for k in FIELDS:
+            assert _oracle.rel_err(sa[k], sb[k]) <= 1e-13, k
+
+
+def test_tuning_table_lookup(tmp_path):
+    from dustyfargoadsg_b200 import Disc, FbError, read_par
+    par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "iso_128x384.par"), str(tmp_path),
+                            Nrad=64, Nsec=192)
+    table = {"iso": {"64x192": {"cell_block": 64, "azi_cells_per_thread": 2, "rad_columns": 32, "rad_rings": 8}}}
+    with Disc(read_par(par), tuning=table) as d:
+        assert d.tuning() == {"cell_block": 64, "azi_cells_per_thread": 2, "rad_columns": 32, "rad_rings": 8}
+        with pytest.raises(FbError):
+            d.set_tuning({"cell_block": 48})
+        d.step()
