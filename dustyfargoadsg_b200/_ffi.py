@@ -20,6 +20,7 @@ FB_STAGE_TRANSPORT, FB_STAGE_VISCOSITY, FB_STAGE_BOUNDARY, FB_STAGE_DAMPING, FB_
 _D = C.c_double
 _I = C.c_int
 _P = C.POINTER(C.c_double)
+_FP = C.POINTER(C.c_float)
 _NP = FB_MAX_PLANETS
 
 
@@ -111,6 +112,9 @@ EXPORTS = (
     "fb_select_device", "fb_transport_noalloc", "fb_noalloc_last_error", "fb_init_dust",
     "fb_dust_upload", "fb_dust_download", "fb_vortensity", "fb_batch_create", "fb_batch_algogas",
     "fb_batch_destroy", "fb_get_tuning", "fb_set_tuning", "fb_tune",
+    "fb_closure_create", "fb_closure_destroy", "fb_closure_num_params", "fb_closure_params",
+    "fb_closure_scales", "fb_closure_autoscale", "fb_closure_record", "fb_closure_set_sample",
+    "fb_closure_loss_grad", "fb_closure_train", "fb_closure_infer", "fb_closure_apply", "fb_downsample",
 )
 
 _lib = None
@@ -161,6 +165,19 @@ def load():
         "fb_get_tuning": (_I, [vp, C.POINTER(FbTuning)]),
         "fb_set_tuning": (_I, [vp, C.POINTER(FbTuning)]),
         "fb_tune": (_I, [vp, _I, C.POINTER(FbTuning), C.POINTER(_D)]),
+        "fb_closure_create": (_I, [vp, _I, _I, C.c_ulonglong, C.POINTER(vp)]),
+        "fb_closure_destroy": (_I, [vp]),
+        "fb_closure_num_params": (_I, [vp, C.POINTER(_I), C.POINTER(_I)]),
+        "fb_closure_params": (_I, [vp, _FP, _FP, _I]),
+        "fb_closure_scales": (_I, [vp, _P, _P, _I]),
+        "fb_closure_autoscale": (_I, [vp, _I]),
+        "fb_closure_record": (_I, [vp, vp, _I, _I]),
+        "fb_closure_set_sample": (_I, [vp, _I, _FP, _FP]),
+        "fb_closure_loss_grad": (_I, [vp, _I, _I, C.POINTER(_D), _FP, _FP]),
+        "fb_closure_train": (_I, [vp, _I, _I, _I, _I, _D, C.c_ulonglong, _P]),
+        "fb_closure_infer": (_I, [vp, vp, _I, _FP]),
+        "fb_closure_apply": (_I, [vp, vp]),
+        "fb_downsample": (_I, [vp, vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -1,0 +1,293 @@
+"""Learned coarse-grid closure: data generation from fine runs, training on
+the GPU, the corrected coarse solver and its check against the plain fine
+method.
+
+The network and its kernels live in libfargo_b200.so (fb_closure_*); this
+module drives them:
+
+* samples (`record_samples`): a fine disc and a coarse disc with the same
+  radii and parameters; per sample the coarse disc is set to the
+  coarse-grained fine state, its features are recorded, the plain method
+  advances it one DT, the fine disc advances one DT too, and the target is
+  the coarse-graining of the fine result minus the plain coarse result, in
+  the conservative variables (mass, angular momentum, radial momentum);
+* training (`Closure.train`): Adam on random minibatches, the loss being the
+  weighted squared error of the correction the network's face fluxes imply;
+* the corrected solver (`run_coarse`): after every DT of the plain coarse
+  method, one correction by the network (fb_closure_apply);
+* the judge (`evaluate`): azimuthally averaged surface density and vortensity
+  of the corrected coarse run, the plain coarse run and the coarse-grained
+  plain fine run (the reference); the corrected run is accepted only when
+  both errors are within 1%, otherwise the fine method is the answer.
+
+    python -m dustyfargoadsg_b200.closure --help
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import tempfile
+import time
+
+import numpy as np
+
+from . import Disc, FbError, read_par, sweep
+from ._ffi import check, load
+
+TOLERANCE = 0.01  # accepted azimuthally averaged Sigma / vortensity error
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Closure:
+    """The network and its device-side training set (fb_closure)."""
+
+    def __init__(self, coarse_disc, capacity=256, batch=8, seed=0):
+        self.lib = load()
+        self.c = C.c_void_p()
+        check(self.lib.fb_closure_create(coarse_disc.ctx, int(capacity), int(batch), int(seed), C.byref(self.c)),
+              "fb_closure_create")
+        self.capacity, self.batch, self.count = capacity, batch, 0
+        nw, nb = C.c_int(), C.c_int()
+        self.lib.fb_closure_num_params(self.c, C.byref(nw), C.byref(nb))
+        self.nw, self.nb = nw.value, nb.value
+
+    # -- parameters -------------------------------------------------------
+    def get_params(self):
+        w, b = np.zeros(self.nw, dtype=np.float32), np.zeros(self.nb, dtype=np.float32)
+        check(self.lib.fb_closure_params(self.c, _fp(w), _fp(b), 1), "fb_closure_params")
+        s, q = np.zeros(3), np.zeros(3)
+        check(self.lib.fb_closure_scales(self.c, _dp(s), _dp(q), 1), "fb_closure_scales")
+        return {"w": w, "b": b, "scale": s, "wq": q}
+
+    def set_params(self, d):
+        w = np.ascontiguousarray(d["w"], dtype=np.float32)
+        b = np.ascontiguousarray(d["b"], dtype=np.float32)
+        check(self.lib.fb_closure_params(self.c, _fp(w), _fp(b), 0), "fb_closure_params")
+        s = np.ascontiguousarray(d["scale"], dtype=np.float64)
+        q = np.ascontiguousarray(d["wq"], dtype=np.float64)
+        check(self.lib.fb_closure_scales(self.c, _dp(s), _dp(q), 0), "fb_closure_scales")
+
+    def save(self, path, meta=None):
+        d = self.get_params()
+        np.savez(path, meta=json.dumps(meta or {}), **d)
+
+    def load(self, path):
+        z = np.load(path)
+        self.set_params({k: z[k] for k in ("w", "b", "scale", "wq")})
+        return json.loads(str(z["meta"]))
+
+    # -- data, training, use --------------------------------------------
+    def record(self, coarse_disc, slot, what):
+        check(self.lib.fb_closure_record(self.c, coarse_disc.ctx, int(slot), int(what)), "fb_closure_record")
+        if what == 2:
+            self.count = max(self.count, slot + 1)
+
+    def autoscale(self, count=None):
+        check(self.lib.fb_closure_autoscale(self.c, int(count or self.count)), "fb_closure_autoscale")
+
+    def loss(self, first, nb):
+        L = C.c_double()
+        check(self.lib.fb_closure_loss_grad(self.c, int(first), int(nb), C.byref(L), None, None),
+              "fb_closure_loss_grad")
+        return L.value
+
+    def train(self, first, count, iters, lr=1e-3, seed=0, batch=None):
+        losses = np.zeros(max(iters, 1))
+        check(self.lib.fb_closure_train(self.c, int(first), int(count), int(batch or self.batch), int(iters),
+                                        float(lr), int(seed), _dp(losses)), "fb_closure_train")
+        return losses[:iters]
+
+    def apply(self, coarse_disc):
+        check(self.lib.fb_closure_apply(self.c, coarse_disc.ctx), "fb_closure_apply")
+
+    def close(self):
+        if self.c:
+            self.lib.fb_closure_destroy(self.c)
+            self.c = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def downsample(fine, coarse):
+    check(fine.lib.fb_downsample(fine.ctx, coarse.ctx), "fb_downsample")
+
+
+def disc_pair(draw, workdir, tag, coarse_nr, factor, noise=1e-4, seed=0, coarse_ns=None):
+    """Fine and coarse Discs of one parameter draw (same radii); the coarse
+    grid has nsec = 3 nrad unless given."""
+    coarse_ns = coarse_ns or 3 * coarse_nr
+    fine_draw = dict(draw, Nrad=coarse_nr * factor, Nsec=coarse_ns * factor)
+    coarse_draw = dict(draw, Nrad=coarse_nr, Nsec=coarse_ns)
+    fine = Disc(read_par(sweep.write_disc_files(fine_draw, workdir, tag + "_fine")), noise=noise, seed=seed)
+    coarse = Disc(read_par(sweep.write_disc_files(coarse_draw, workdir, tag + "_coarse")))
+    return fine, coarse
+
+
+def record_samples(net, fine, coarse, first_slot, nsamples, every=1):
+    """Samples first_slot.. from the fine run; the fine disc advances
+    nsamples*every DTs."""
+    slot = first_slot
+    downsample(fine, coarse)
+    for _ in range(nsamples):
+        net.record(coarse, slot, 0)
+        coarse.step()
+        net.record(coarse, slot, 1)
+        for _ in range(every):
+            fine.step()
+        downsample(fine, coarse)
+        net.record(coarse, slot, 2)
+        slot += 1
+    return slot
+
+
+def train_small(workdir, coarse_nr=16, coarse_ns=64, factor=4, samples=6, iters=60, seed=0):
+    """A small end-to-end training run (tests): one disc, a few samples."""
+    draw = dict(q=1e-3, AlphaViscosity=1e-3, AspectRatio=0.05, SigmaSlope=0.5)
+    fine, coarse = disc_pair(draw, workdir, "small", coarse_nr, factor, noise=1e-3, seed=seed, coarse_ns=coarse_ns)
+    net = Closure(coarse, capacity=samples, batch=2, seed=seed)
+    try:
+        for _ in range(3):
+            fine.step()
+        record_samples(net, fine, coarse, 0, samples)
+        net.autoscale()
+        first = net.loss(0, 2)
+        losses = net.train(0, samples, iters, lr=3e-3, seed=seed, batch=2)
+        last = net.loss(0, 2)
+        return {"loss_first": first, "loss_last": last, "train_losses": losses[::10].tolist()}
+    finally:
+        net.close()
+        fine.close()
+        coarse.close()
+
+
+# ------------------------------------------------------------ evaluation
+def profiles(disc):
+    """Azimuthal means of Sigma and of the vortensity."""
+    sm, vm = disc.vortensity()
+    return sm, vm
+
+
+def profile_errors(test, ref):
+    """Largest relative deviation over rings of the Sigma profile and of the
+    vortensity profile (interface rings 1..nr-1)."""
+    es = float(np.max(np.abs(test[0] - ref[0]) / np.abs(ref[0])))
+    ev = float(np.max(np.abs(test[1][1:] - ref[1][1:]) / np.abs(ref[1][1:])))
+    return es, ev
+
+
+def run_coarse(coarse, ndt, net=None):
+    """ndt DTs of the coarse disc, corrected by `net` after each; GPU time (s)."""
+    t = 0.0
+    for _ in range(ndt):
+        t0 = time.perf_counter()
+        coarse.step()
+        if net is not None:
+            net.apply(coarse)
+        t += time.perf_counter() - t0
+    return t
+
+
+def evaluate(net, draw, workdir, tag, coarse_nr, factor, ndt, seed=0):
+    """Fine, plain coarse and corrected coarse runs of one draw from the
+    same start; returns errors, times and whether the corrected run stands."""
+    fine, coarse = disc_pair(draw, workdir, tag, coarse_nr, factor, seed=seed)
+    plain = Disc(coarse.p)
+    try:
+        downsample(fine, coarse)
+        downsample(fine, plain)
+        t0 = time.perf_counter()
+        for _ in range(ndt):
+            fine.step()
+        t_fine = time.perf_counter() - t0
+        t_plain = run_coarse(plain, ndt)
+        t_cnn = run_coarse(coarse, ndt, net)
+        p_cnn, p_plain = profiles(coarse), profiles(plain)
+        downsample(fine, coarse)  # the reference on the coarse grid
+        p_ref = profiles(coarse)
+        e_cnn, e_plain = profile_errors(p_cnn, p_ref), profile_errors(p_plain, p_ref)
+        accepted = max(e_cnn) <= TOLERANCE
+        return {"draw": draw, "dt": ndt, "err_sigma_cnn": e_cnn[0], "err_vort_cnn": e_cnn[1],
+                "err_sigma_plain": e_plain[0], "err_vort_plain": e_plain[1],
+                "t_fine_s": t_fine, "t_coarse_plain_s": t_plain, "t_coarse_cnn_s": t_cnn,
+                "speedup_cnn_vs_fine": t_fine / t_cnn, "accepted": accepted,
+                "answer": "coarse+cnn" if accepted else "fine (fallback)"}
+    finally:
+        fine.close()
+        coarse.close()
+        plain.close()
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="train and judge the learned closure")
+    ap.add_argument("--coarse-nr", type=int, default=128)
+    ap.add_argument("--factor", type=int, default=4)
+    ap.add_argument("--train-discs", type=int, default=8)
+    ap.add_argument("--spinup-dt", type=int, default=100, help="fine DTs before the first sample")
+    ap.add_argument("--samples-per-disc", type=int, default=24)
+    ap.add_argument("--every", type=int, default=10, help="fine DTs between samples")
+    ap.add_argument("--iters", type=int, default=2000)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--eval-discs", type=int, default=4)
+    ap.add_argument("--eval-dt", type=int, default=400)
+    ap.add_argument("--out", default=None, help="model .npz")
+    ap.add_argument("--report", default=None, help="JSON report")
+    args = ap.parse_args(argv)
+    wd = tempfile.mkdtemp(prefix="fb_closure_")
+    draws = sweep.draw_discs(args.train_discs, seed=3)
+    cap = args.train_discs * args.samples_per_disc
+    report = {"coarse": [args.coarse_nr, 3 * args.coarse_nr], "factor": args.factor}
+    t0 = time.perf_counter()
+    net = None
+    slot = 0
+    for d, draw in enumerate(draws):
+        draw = dict(draw)
+        draw.pop("Nrad"), draw.pop("Nsec")
+        fine, coarse = disc_pair(draw, wd, "train%02d" % d, args.coarse_nr, args.factor)
+        if net is None:
+            net = Closure(coarse, capacity=cap, batch=8, seed=3)
+        for _ in range(args.spinup_dt):
+            fine.step()
+        slot = record_samples(net, fine, coarse, slot, args.samples_per_disc, args.every)
+        fine.close()
+        coarse.close()
+        print("disc", d, "samples", slot, "%.1f s" % (time.perf_counter() - t0), flush=True)
+    report["t_data_s"] = time.perf_counter() - t0
+    nval = max(8, slot // 8)
+    ntrain = slot - nval
+    net.autoscale(ntrain)
+    report["loss_val_before"] = net.loss(ntrain, min(8, nval))
+    t1 = time.perf_counter()
+    losses = net.train(0, ntrain, args.iters, lr=args.lr, seed=4)
+    report["t_train_s"] = time.perf_counter() - t1
+    report["loss_train_first"], report["loss_train_last"] = float(losses[0]), float(np.mean(losses[-50:]))
+    report["loss_val_after"] = net.loss(ntrain, min(8, nval))
+    print("training", report, flush=True)
+    evals = []
+    for d, draw in enumerate(sweep.draw_discs(args.eval_discs, seed=4)):
+        draw = dict(draw)
+        draw.pop("Nrad"), draw.pop("Nsec")
+        r = evaluate(net, draw, wd, "eval%02d" % d, args.coarse_nr, args.factor, args.eval_dt)
+        evals.append(r)
+        print("eval", d, r, flush=True)
+    report["evaluations"] = evals
+    if args.out:
+        net.save(args.out, meta={k: v for k, v in report.items() if k != "evaluations"})
+    if args.report:
+        with open(args.report, "w") as f:
+            json.dump(report, f, indent=1)
+    net.close()
+
+
+if __name__ == "__main__":
+    main()

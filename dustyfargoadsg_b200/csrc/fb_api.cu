@@ -100,6 +100,10 @@ extern "C" int fb_select_device(int device)
 }
 
 extern "C" const fb_geom *fb_ctx_geom(const fb_ctx *ctx) { return ctx ? &ctx->g : NULL; }
+const KP *fb_ctx_kp(const fb_ctx *ctx) { return ctx ? &ctx->k : NULL; }
+KP *fb_ctx_kp_mut(fb_ctx *ctx) { return ctx ? &ctx->k : NULL; }
+cudaStream_t fb_ctx_stream(const fb_ctx *ctx) { return ctx ? ctx->st : NULL; }
+void fb_ctx_count_launches(fb_ctx *ctx, int n) { if (ctx) ctx->launches += n; }
 
 extern "C" const char *fb_strerror(int code)
 {

@@ -156,6 +156,11 @@ void fb_sg_destroy(fb_sg *sg);
 void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
 // refresh = 1: the Dt = 0 call of main.c:316 on Vrad/Vtheta (fields only)
 void fb_sg_update_velocities(const KP &k, cudaStream_t s, int refresh = 0);
+// context accessors for the other modules (fb_api.cu)
+const KP *fb_ctx_kp(const fb_ctx *ctx);
+KP *fb_ctx_kp_mut(fb_ctx *ctx);
+cudaStream_t fb_ctx_stream(const fb_ctx *ctx);
+void fb_ctx_count_launches(fb_ctx *ctx, int n);
 // diagnostics (fb_diag.cu)
 void fb_launch_vortensity(const KP &k, double *xi, cudaStream_t s);
 void fb_launch_ring_mean(const double *f, int nr, int ns, double *out, cudaStream_t s);
