@@ -44,7 +44,11 @@ WORKLOADS = {
     "iso_768x2304": dict(par="iso_768x2304.par", noise=1e-4, seed=0),
     # adiabatic + beta cooling + self-gravity 512 x 1536 disc, q=5e-4 planet
     "adiabatic_sg_512x1536": dict(par="adiabatic_sg_512x1536.par", noise=1e-4, seed=0),
+    # gas of the 128x384 disc on 256 x 768 with 200,000 Lagrangian particles
+    # (turbulent kicks), particles drawn from the drand48 stream seeded with 1
+    "dust_256x768": dict(par="dust_256x768.par", noise=1e-4, seed=0, dust_seed=1),
 }
+BATCH_DISCS, BATCH_SEED = 64, 2  # the batched sweep: 64 discs drawn from seed 2
 DEFAULT_WORKLOAD = "adiabatic_sg_512x1536"
 FALLBACK_HBM_GBS = 6650.0
 
@@ -220,6 +224,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=None, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -249,7 +254,9 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    disc = fb.Disc(p, noise=wl["noise"], seed=wl["seed"])
+    from dustyfargoadsg_b200 import tune
+    table = tune.load_table()
+    disc = fb.Disc(p, noise=wl["noise"], seed=wl["seed"], dust_seed=wl.get("dust_seed"), tuning=table)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
     def barrier():
@@ -311,6 +318,15 @@ def main():
         e2e_wall, e2e_sub = float(tm[0]), float(t[1])
     e2e_value = e2e_sub * cells / e2e_wall
     fbytes = disc.nf * 8 * len(arrays)
+    d2h_extra = 0
+    if disc.npart > 0:
+        # the particles are outputs too: time their download once per step
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            disc.dust()
+        e2e_wall_d = time.perf_counter() - t0
+        e2e_value = e2e_sub * cells / (e2e_wall + e2e_wall_d)
+        d2h_extra = disc.npart * 8 * len(disc.DUST_ARRAYS)
 
     # --- profiled pass: per-stage CUDA events -> roofline ------------------
     disc.profile(True)
@@ -351,6 +367,10 @@ def main():
         else:
             cpu = {"value": None, "unit": "cell-updates/s", "cores": 1, "kind": "reference", "sample": desc}
 
+    batch = None
+    if rank == 0 and world == 1 and not args.no_batch:
+        batch = measure_batch(fb, table, flush)
+
     if rank == 0:
         line = {
             "metric": "gas cell-updates/s FP64", "value": value, "unit": "cell-updates/s",
@@ -362,18 +382,53 @@ def main():
                        "parallelism": "replicas%d" % world,
                        "l2": "flushed (256 MB write) before every timed step"},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": fbytes,
-                    "d2h_bytes_per_step": fbytes},
+                    "d2h_bytes_per_step": fbytes + d2h_extra},
             "gpu_launches": launches,
             "roofline": roofline,
             "stages": stages,
             "cpu_baseline": cpu,
             "clocks": clk,
         }
+        if disc.npart > 0:
+            line["config"]["particles"] = disc.npart
+            line["particle_updates_per_s"] = disc.npart * sub_all / t_max
+        if batch is not None:
+            line["batched"] = batch
         print(json.dumps(line))
     disc.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def measure_batch(fb, table, flush, warmup=2, steps=3):
+    """The batched sweep: 64 discs of uneven grids and parameters (seed 2),
+    one graph launch per DT for all of them; orbits/s summed over discs."""
+    import torch
+    from dustyfargoadsg_b200 import sweep
+    wd = tempfile.mkdtemp(prefix="fb_batch_")
+    discs = sweep.make_discs(sweep.draw_discs(BATCH_DISCS, BATCH_SEED), wd, tuning=table)
+    try:
+        with fb.Batch(discs) as batch:
+            for _ in range(warmup):
+                batch.step()
+            ms, cell_updates, launches0 = 0.0, 0, sum(d.kernel_launches() for d in discs)
+            for _ in range(steps):
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                reps = batch.step()
+                ms += reps[0].gpu_ms
+                cell_updates += sum(r.substeps * d.nr * d.ns for r, d in zip(reps, discs))
+            launches = sum(d.kernel_launches() for d in discs) - launches0
+        orbits = BATCH_DISCS * steps * sweep.orbits_per_dt(discs[0].p)
+        return {"metric": "batched orbits/s", "value": orbits / (ms / 1e3), "unit": "orbits/s",
+                "discs": BATCH_DISCS, "seed": BATCH_SEED, "steps": steps, "warmup": warmup,
+                "cell_updates_per_s": cell_updates / (ms / 1e3), "ms_per_step": ms / steps,
+                "gpu_launches": launches, "graph_launches_per_step": 1,
+                "grids": sorted({"%dx%d" % (d.nr, d.ns) for d in discs})}
+    finally:
+        for d in discs:
+            d.close()
 
 
 def _supported(fb, name):

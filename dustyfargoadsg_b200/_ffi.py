@@ -115,6 +115,7 @@ EXPORTS = (
     "fb_closure_create", "fb_closure_destroy", "fb_closure_num_params", "fb_closure_params",
     "fb_closure_scales", "fb_closure_autoscale", "fb_closure_record", "fb_closure_set_sample",
     "fb_closure_loss_grad", "fb_closure_train", "fb_closure_infer", "fb_closure_apply", "fb_downsample",
+    "fb_closure_set_gain",
 )
 
 _lib = None
@@ -172,12 +173,13 @@ def load():
         "fb_closure_scales": (_I, [vp, _P, _P, _I]),
         "fb_closure_autoscale": (_I, [vp, _I]),
         "fb_closure_record": (_I, [vp, vp, _I, _I]),
-        "fb_closure_set_sample": (_I, [vp, _I, _FP, _FP]),
+        "fb_closure_set_sample": (_I, [vp, _I, _FP, _FP, _FP]),
         "fb_closure_loss_grad": (_I, [vp, _I, _I, C.POINTER(_D), _FP, _FP]),
         "fb_closure_train": (_I, [vp, _I, _I, _I, _I, _D, C.c_ulonglong, _P]),
         "fb_closure_infer": (_I, [vp, vp, _I, _FP]),
         "fb_closure_apply": (_I, [vp, vp]),
         "fb_downsample": (_I, [vp, vp]),
+        "fb_closure_set_gain": (_I, [vp, _D]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -107,6 +107,9 @@ class Closure:
     def apply(self, coarse_disc):
         check(self.lib.fb_closure_apply(self.c, coarse_disc.ctx), "fb_closure_apply")
 
+    def set_gain(self, gain):
+        check(self.lib.fb_closure_set_gain(self.c, float(gain)), "fb_closure_set_gain")
+
     def close(self):
         if self.c:
             self.lib.fb_closure_destroy(self.c)
@@ -135,19 +138,22 @@ def disc_pair(draw, workdir, tag, coarse_nr, factor, noise=1e-4, seed=0, coarse_
 
 
 def record_samples(net, fine, coarse, first_slot, nsamples, every=1):
-    """Samples first_slot.. from the fine run; the fine disc advances
-    nsamples*every DTs."""
+    """Samples first_slot.. from the fine run, one every `every` DTs of the
+    fine disc: each is one DT of the plain coarse method from the
+    coarse-grained fine state against the coarse-graining of the fine
+    disc's own DT."""
     slot = first_slot
-    downsample(fine, coarse)
     for _ in range(nsamples):
+        downsample(fine, coarse)
         net.record(coarse, slot, 0)
         coarse.step()
         net.record(coarse, slot, 1)
-        for _ in range(every):
-            fine.step()
+        fine.step()
         downsample(fine, coarse)
         net.record(coarse, slot, 2)
         slot += 1
+        for _ in range(every - 1):
+            fine.step()
     return slot
 
 
@@ -198,34 +204,58 @@ def run_coarse(coarse, ndt, net=None):
     return t
 
 
-def evaluate(net, draw, workdir, tag, coarse_nr, factor, ndt, seed=0):
+def evaluate(net, draw, workdir, tag, coarse_nr, factor, ndt, seed=0, gains=(1.0,)):
     """Fine, plain coarse and corrected coarse runs of one draw from the
-    same start; returns errors, times and whether the corrected run stands."""
+    same start; returns errors, times and whether the corrected run stands
+    (a corrected run that fails counts as not within tolerance)."""
     fine, coarse = disc_pair(draw, workdir, tag, coarse_nr, factor, seed=seed)
     plain = Disc(coarse.p)
+    runs = []
     try:
-        downsample(fine, coarse)
         downsample(fine, plain)
         t0 = time.perf_counter()
         for _ in range(ndt):
             fine.step()
         t_fine = time.perf_counter() - t0
         t_plain = run_coarse(plain, ndt)
-        t_cnn = run_coarse(coarse, ndt, net)
-        p_cnn, p_plain = profiles(coarse), profiles(plain)
-        downsample(fine, coarse)  # the reference on the coarse grid
-        p_ref = profiles(coarse)
-        e_cnn, e_plain = profile_errors(p_cnn, p_ref), profile_errors(p_plain, p_ref)
-        accepted = max(e_cnn) <= TOLERANCE
-        return {"draw": draw, "dt": ndt, "err_sigma_cnn": e_cnn[0], "err_vort_cnn": e_cnn[1],
-                "err_sigma_plain": e_plain[0], "err_vort_plain": e_plain[1],
-                "t_fine_s": t_fine, "t_coarse_plain_s": t_plain, "t_coarse_cnn_s": t_cnn,
-                "speedup_cnn_vs_fine": t_fine / t_cnn, "accepted": accepted,
-                "answer": "coarse+cnn" if accepted else "fine (fallback)"}
-    finally:
+        ref = Disc(coarse.p)
+        downsample(fine, ref)  # the reference on the coarse grid
+        p_ref = profiles(ref)
+        ref.close()
+        e_plain = profile_errors(profiles(plain), p_ref)
         fine.close()
-        coarse.close()
-        plain.close()
+        fine = None
+        for gain in gains:
+            fresh_fine, _ = None, None
+            run = {"gain": gain}
+            try:
+                net.set_gain(gain)
+                # restart the corrected run from the same coarse start
+                start, _c = disc_pair(draw, workdir, tag + "_g", coarse_nr, factor, seed=seed)
+                downsample(start, coarse)
+                start.close()
+                _c.close()
+                run["t_s"] = run_coarse(coarse, ndt, net)
+                e = profile_errors(profiles(coarse), p_ref)
+                run["err_sigma"], run["err_vort"] = e
+                run["ok"] = bool(np.all(np.isfinite(e)))
+            except FbError as exc:
+                run["ok"], run["error"] = False, str(exc)
+            runs.append(run)
+        good = [r for r in runs if r["ok"]]
+        best = min(good, key=lambda r: max(r["err_sigma"], r["err_vort"])) if good else None
+        accepted = best is not None and max(best["err_sigma"], best["err_vort"]) <= TOLERANCE
+        out = {"draw": draw, "dt": ndt, "err_sigma_plain": e_plain[0], "err_vort_plain": e_plain[1],
+               "t_fine_s": t_fine, "t_coarse_plain_s": t_plain, "runs": runs, "accepted": accepted,
+               "answer": "coarse+cnn" if accepted else "fine (fallback)"}
+        if best is not None:
+            out.update(gain=best["gain"], err_sigma_cnn=best["err_sigma"], err_vort_cnn=best["err_vort"],
+                       t_coarse_cnn_s=best["t_s"], speedup_cnn_vs_fine=t_fine / best["t_s"])
+        return out
+    finally:
+        for d in (fine, coarse, plain):
+            if d is not None:
+                d.close()
 
 
 def main(argv=None):
@@ -233,6 +263,7 @@ def main(argv=None):
     ap.add_argument("--coarse-nr", type=int, default=128)
     ap.add_argument("--factor", type=int, default=4)
     ap.add_argument("--train-discs", type=int, default=8)
+    ap.add_argument("--val-discs", type=int, default=2, help="of the training discs, held out for early stopping")
     ap.add_argument("--spinup-dt", type=int, default=100, help="fine DTs before the first sample")
     ap.add_argument("--samples-per-disc", type=int, default=24)
     ap.add_argument("--every", type=int, default=10, help="fine DTs between samples")
@@ -240,6 +271,7 @@ def main(argv=None):
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-discs", type=int, default=4)
     ap.add_argument("--eval-dt", type=int, default=400)
+    ap.add_argument("--gains", default="1.0,0.5,0.25", help="correction strengths tried in the evaluation")
     ap.add_argument("--out", default=None, help="model .npz")
     ap.add_argument("--report", default=None, help="JSON report")
     args = ap.parse_args(argv)
@@ -263,21 +295,37 @@ def main(argv=None):
         coarse.close()
         print("disc", d, "samples", slot, "%.1f s" % (time.perf_counter() - t0), flush=True)
     report["t_data_s"] = time.perf_counter() - t0
-    nval = max(8, slot // 8)
+    # the last `val_discs` discs are held out for validation (early stopping)
+    nval = args.val_discs * args.samples_per_disc
     ntrain = slot - nval
     net.autoscale(ntrain)
-    report["loss_val_before"] = net.loss(ntrain, min(8, nval))
+
+    def val_loss():
+        return float(np.mean([net.loss(ntrain + q, 1) for q in range(0, nval, max(1, nval // 8))]))
+
+    report["loss_val_before"] = best_val = val_loss()
+    best = net.get_params()
     t1 = time.perf_counter()
-    losses = net.train(0, ntrain, args.iters, lr=args.lr, seed=4)
+    losses, curve = [], []
+    chunk = max(1, args.iters // 12)
+    for it in range(0, args.iters, chunk):
+        losses.extend(net.train(0, ntrain, min(chunk, args.iters - it), lr=args.lr, seed=4 + it).tolist())
+        v = val_loss()
+        curve.append([it + chunk, float(np.mean(losses[-chunk:])), v])
+        if v < best_val:
+            best_val, best = v, net.get_params()
+    net.set_params(best)
     report["t_train_s"] = time.perf_counter() - t1
     report["loss_train_first"], report["loss_train_last"] = float(losses[0]), float(np.mean(losses[-50:]))
-    report["loss_val_after"] = net.loss(ntrain, min(8, nval))
+    report["loss_val_best"] = best_val
+    report["curve_iter_train_val"] = curve
     print("training", report, flush=True)
     evals = []
     for d, draw in enumerate(sweep.draw_discs(args.eval_discs, seed=4)):
         draw = dict(draw)
         draw.pop("Nrad"), draw.pop("Nsec")
-        r = evaluate(net, draw, wd, "eval%02d" % d, args.coarse_nr, args.factor, args.eval_dt)
+        r = evaluate(net, draw, wd, "eval%02d" % d, args.coarse_nr, args.factor, args.eval_dt,
+                     gains=[float(g) for g in args.gains.split(",")])
         evals.append(r)
         print("eval", d, r, flush=True)
     report["evaluations"] = evals

@@ -14,17 +14,21 @@
 // [out][tap][in] with tap = (dy+1)*3 + (dx+1).  Azimuth is periodic, the
 // radial direction zero-padded.
 //
-// Conservative quantities on the coarse staggered grid (cell (i,j)):
-//   m = Sigma(i,j)
-//   J = (Sigma(i,j-1) + Sigma(i,j))/2 * Rmed[i] * vtheta(i,j)      (at the vtheta face)
-//   P = (Sigma(i-1,j) + Sigma(i,j))/2 * vrad(i,j), i >= 1          (at the vrad face)
-// and the correction of one of them from the network's two face-flux
-// channels (Fr through the inner radial face, Ft through the lower
-// azimuthal face of each cell), scale s:
-//   dq(i,j) = s * [Fr(i,j) mr(i) - Fr(i+1,j) mr(i+1) + (Ft(i,j) - Ft(i,j+1)) mt(i)] / Surf[i]
-// with mr(i) = 1 on interior faces (1..nr-1 for m and J, 2..nr-1 for P) and
-// mt(i) = 1 (i >= 1 for P): sum_ij Surf[i] dq(i,j) = 0 exactly in exact
-// arithmetic.
+// What the network corrects: the mass of every coarse cell, through two
+// face fluxes per cell (Fr through its inner radial face, Ft through its
+// lower azimuthal face), in units of scale * Sigma0(face) where Sigma0 is
+// the disc's initial density profile (geometric mean of the two rings at a
+// radial face):
+//   dSigma(i,j) = [Fr(i,j) mr(i) - Fr(i+1,j) mr(i+1) + Ft(i,j) - Ft(i,j+1)] / Surf[i]
+// with mr(i) = 1 on the interior radial faces 1..nr-1, so sum Surf dSigma = 0.
+// The corrected mass carries its angular momentum: each vtheta face's
+// control volume (half of the cells j-1 and j) exchanges, through its four
+// boundaries, the mass fluxes of the cells averaged onto those boundaries
+// times the upwind specific angular momentum R vtheta, so the staggered
+// angular momentum J = (Sigma(i,j-1) + Sigma(i,j))/2 R vtheta(i,j) changes
+// only by round-off and a uniform rotation is left unchanged.  vrad is not
+// modified.  The training set stores the conservative quantities m, J, P of
+// the targets; the loss uses m.
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <math.h>
@@ -35,8 +39,8 @@
 
 #define CL_LAYERS 4
 #define CL_C 32      // hidden channels
-#define CL_CIN 16    // input feature channels (5 used)
-#define CL_COUT 16   // output channels (6 used: Fr, Ft for m, J, P)
+#define CL_CIN 16    // input feature channels (7 used)
+#define CL_COUT 16   // output channels (2 used: the mass fluxes Fr, Ft)
 #define CL_TILE 64   // pixels per CTA in the convolutions
 #define CL_BS 128
 
@@ -261,6 +265,7 @@ __global__ void __launch_bounds__(CL_BS) k_conv_wgrad(const bf16 *__restrict__ x
 //   0: Sigma / SigmaMed(r) - 1          1: vrad / cs(r)
 //   2: (vtheta - VthetaMed(r)) / cs(r)  3: (log r - mean) / half-width of log r
 //   4: planets' smoothed potential / cs(r)^2 at their current positions
+//   5: log10(alpha) + 3                 6: (aspect ratio - 0.065) / 0.035
 __global__ void k_features(KP k, bf16 *out, double lmid, double lhalf)
 {
   const int i = blockIdx.y, ns = k.ns;
@@ -282,6 +287,8 @@ __global__ void k_features(KP k, bf16 *out, double lmid, double lhalf)
   f[2] = (float)((k.vt[l] - k.vthetamed[i]) / cs);
   f[3] = (float)((log(r) - lmid) / lhalf);
   f[4] = (float)(phi / (cs * cs));
+  f[5] = (float)(k.alpha > 0.0 ? log10(k.alpha) + 3.0 : -2.0);  // log10 alpha, about -1..1
+  f[6] = (float)((k.aspectratio - 0.065) / 0.035);               // h, about -1..1
   unsigned *o = reinterpret_cast<unsigned *>(out + l * CL_CIN);
 #pragma unroll
   for (int c = 0; c < CL_CIN; c += 2) o[c / 2] = pack_bf16x2(f[c], f[c + 1]);
@@ -308,30 +315,29 @@ __global__ void k_conservative(KP k, float *out, float sign, int accumulate)
 }
 
 // ------------------------------------------------------------ flux differences
-static __device__ __forceinline__ int mask_r(int q, int i, int nr)
-{
-  // interior radial faces: 1..nr-1 (m, J), 2..nr-1 (P, whose ring 0 is a boundary)
-  return (i >= (q == 2 ? 2 : 1) && i <= nr - 1) ? 1 : 0;
-}
-static __device__ __forceinline__ int mask_t(int q, int i) { return (q == 2 && i == 0) ? 0 : 1; }
-
-// dq of quantity q at (i,j) from the network output O (NHWC f32, sample b)
+// interior radial faces 1..nr-1
+static __device__ __forceinline__ int mask_r(int i, int nr) { return (i >= 1 && i <= nr - 1) ? 1 : 0; }
+// Sigma0 at radial face i (between rings i-1 and i)
 template <typename T>
-static __device__ __forceinline__ T flux_diff(const float *O, const T *scale, const T *surf, int q, int i, int j,
+static __device__ __forceinline__ T sig_face(const T *sig, int i) { return sqrt(sig[i - 1] * sig[i]); }
+
+// dSigma at (i,j) from the network output O (NHWC f32, one sample)
+template <typename T, typename S>
+static __device__ __forceinline__ T mass_diff(const float *O, T scale, const T *surf, const S *sig, int i, int j,
                                               int nr, int ns)
 {
   const size_t row = (size_t)i * ns;
   const int jp = (j == ns - 1) ? 0 : j + 1;
-  const T fr0 = mask_r(q, i, nr) ? (T)O[(row + j) * CL_COUT + 2 * q] : (T)0;
-  const T fr1 = mask_r(q, i + 1, nr) ? (T)O[(row + ns + j) * CL_COUT + 2 * q] : (T)0;
-  const T ft = mask_t(q, i) ? ((T)O[(row + j) * CL_COUT + 2 * q + 1] - (T)O[(row + jp) * CL_COUT + 2 * q + 1]) : (T)0;
-  return scale[q] * ((fr0 - fr1) + ft) / surf[i];
+  const T fr0 = mask_r(i, nr) ? (T)O[(row + j) * CL_COUT] * (T)sig_face(sig, i) : (T)0;
+  const T fr1 = mask_r(i + 1, nr) ? (T)O[(row + ns + j) * CL_COUT] * (T)sig_face(sig, i + 1) : (T)0;
+  const T ft = ((T)O[(row + j) * CL_COUT + 1] - (T)O[(row + jp) * CL_COUT + 1]) * (T)sig[i];
+  return scale * ((fr0 - fr1) + ft) / surf[i];
 }
 
-// Loss of a minibatch: L = sum_b sum_q w_q sum_ij (dq_pred - Y_q)^2 / (B nr ns);
-// G = dL/d(dq_pred).  One thread per cell and sample; loss partials per CTA.
-__global__ void k_loss(const float *O, const float *Y, const int *idx, const float *scale, const float *wq,
-                       const float *surf, float *G, double *loss_part, int nr, int ns, int nb)
+// Loss of a minibatch: L = w sum_b sum_ij (dSigma_pred - Y_m)^2 / (B nr ns);
+// G = dL/d(dSigma_pred).  One thread per cell and sample; partials per CTA.
+__global__ void k_loss(const float *O, const float *Y, const float *sig, const int *idx, const float *scale,
+                       const float *wq, const float *surf, float *G, double *loss_part, int nr, int ns, int nb)
 {
   __shared__ double sh[256];
   const size_t n = (size_t)nr * ns;
@@ -343,12 +349,11 @@ __global__ void k_loss(const float *O, const float *Y, const int *idx, const flo
     const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
     const float *Ob = O + (size_t)b * n * CL_COUT;
     const float *Yb = Y + (size_t)idx[b] * 3 * n;
+    const float *sb = sig + (size_t)idx[b] * nr;
     const float norm = 1.0f / (float)(n * nb);
-    for (int q = 0; q < 3; q++) {
-      const float d = flux_diff<float>(Ob, scale, surf, q, i, j, nr, ns) - Yb[q * n + l];
-      e += (double)wq[q] * d * d;
-      G[((size_t)b * 3 + q) * n + l] = 2.0f * wq[q] * d * norm;
-    }
+    const float d = mass_diff<float, float>(Ob, scale[0], surf, sb, i, j, nr, ns) - Yb[l];
+    e = (double)wq[0] * d * d;
+    G[(size_t)b * n + l] = 2.0f * wq[0] * d * norm;
   }
   sh[threadIdx.x] = e;
   __syncthreads();
@@ -359,10 +364,10 @@ __global__ void k_loss(const float *O, const float *Y, const int *idx, const flo
   if (threadIdx.x == 0) loss_part[blockIdx.x] = sh[0] / (double)(n * nb);
 }
 
-// dL/dO from G (adjoint of flux_diff); channels >= 6 get 0.  Output bf16
+// dL/dO from G (adjoint of mass_diff); channels >= 2 get 0.  Output bf16
 // (the last layer's pre-activation gradient).
-__global__ void k_loss_adjoint(const float *G, const float *scale, const float *surf, bf16 *dO, int nr, int ns,
-                               int nb)
+__global__ void k_loss_adjoint(const float *G, const float *sig, const int *idx, const float *scale,
+                               const float *surf, bf16 *dO, int nr, int ns, int nb)
 {
   const size_t n = (size_t)nr * ns;
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -371,52 +376,88 @@ __global__ void k_loss_adjoint(const float *G, const float *scale, const float *
   const size_t l = t - (size_t)b * n;
   const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
   const int jm = (j == 0) ? ns - 1 : j - 1;
+  const float *Gb = G + (size_t)b * n;
+  const float *sb = sig + (size_t)idx[b] * nr;
+  const float s = scale[0];
   float d[CL_COUT];
 #pragma unroll
   for (int c = 0; c < CL_COUT; c++) d[c] = 0.f;
-  for (int q = 0; q < 3; q++) {
-    const float *Gq = G + ((size_t)b * 3 + q) * n;
-    const float s = scale[q];
-    // Fr(i,j) enters dq(i,j) with +s/Surf[i] and dq(i-1,j) with -s/Surf[i-1]
-    if (mask_r(q, i, nr)) d[2 * q] = s * (Gq[l] / surf[i] - Gq[l - ns] / surf[i - 1]);
-    // Ft(i,j) enters dq(i,j) with +s/Surf[i] and dq(i,j-1) with -s/Surf[i]
-    if (mask_t(q, i)) d[2 * q + 1] = s / surf[i] * (Gq[l] - Gq[(size_t)i * ns + jm]);
-  }
+  // Fr(i,j) enters dSigma(i,j) with +s sf/Surf[i] and dSigma(i-1,j) with -s sf/Surf[i-1]
+  if (mask_r(i, nr)) d[0] = s * sig_face(sb, i) * (Gb[l] / surf[i] - Gb[l - ns] / surf[i - 1]);
+  // Ft(i,j) enters dSigma(i,j) with +s sig/Surf[i] and dSigma(i,j-1) with -s sig/Surf[i]
+  d[1] = s * sb[i] / surf[i] * (Gb[l] - Gb[(size_t)i * ns + jm]);
   unsigned *o = reinterpret_cast<unsigned *>(dO + t * CL_COUT);
 #pragma unroll
   for (int c = 0; c < CL_COUT; c += 2) o[c / 2] = pack_bf16x2(d[c], d[c + 1]);
 }
 
 // ------------------------------------------------------------ apply (inference)
-// New density of every cell (FP64), from the mass fluxes.
-__global__ void k_apply_density(KP k, const float *O, const double *scale, const double *surf, double *rho_new)
+// At inference each face flux is saturated, F -> Fmax tanh(F/Fmax) with Fmax
+// = CL_FMAX in units of the output scale: a pointwise map of the one value
+// both cells of a face read, so the correction stays conservative, while an
+// output far outside the training range cannot push the disc off.
+#define CL_FMAX 3.0
+__global__ void k_saturate(const float *O, float *Os, size_t n)
 {
-  const int i = blockIdx.y, ns = k.ns, nr = k.nr;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ns) return;
-  const size_t l = (size_t)i * ns + j;
-  double r = k.rho[l] + flux_diff<double>(O, scale, surf, 0, i, j, nr, ns);
-  if (r < k.floordens) r = k.floordens;  // AddFloorDensity's floor, never reached in practice
-  rho_new[l] = r;
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+    Os[t] = (float)(CL_FMAX * tanh((double)O[t] / CL_FMAX));
 }
 
-// Velocities from the corrected J and P and the new density; then the
-// density itself.  Reads only the old density and rho_new.
-__global__ void k_apply_velocities(KP k, const float *O, const double *scale, const double *surf,
-                                   const double *rho_new)
+// Physical face mass fluxes (FP64) of the saturated outputs: Fr at the
+// inner radial face of every cell (ring nr: 0), Ft at its lower azimuthal face.
+__global__ void k_face_flux(KP k, const float *O, double scale, double *fr, double *ft)
 {
   const int i = blockIdx.y, ns = k.ns, nr = k.nr;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ns) return;
   const size_t l = (size_t)i * ns + j;
-  const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
-  const double J = 0.5 * (k.rho[ljm] + k.rho[l]) * k.rmed[i] * k.vt[l] +
-                   flux_diff<double>(O, scale, surf, 1, i, j, nr, ns);
-  k.vt[l] = J / (0.5 * (rho_new[ljm] + rho_new[l]) * k.rmed[i]);
-  if (i >= 1) {
-    const double P = 0.5 * (k.rho[l - ns] + k.rho[l]) * k.vr[l] + flux_diff<double>(O, scale, surf, 2, i, j, nr, ns);
-    k.vr[l] = P / (0.5 * (rho_new[l - ns] + rho_new[l]));
+  if (i == nr) {
+    fr[l] = 0.0;
+    return;
   }
+  fr[l] = mask_r(i, nr) ? scale * (double)O[l * CL_COUT] * sig_face(k.sigmamed, i) : 0.0;
+  ft[l] = scale * (double)O[l * CL_COUT + 1] * k.sigmamed[i];
+}
+
+static __device__ __forceinline__ double dsigma(const KP &k, const double *fr, const double *ft, const double *surf,
+                                                int i, int j)
+{
+  const int ns = k.ns;
+  const size_t l = (size_t)i * ns + j;
+  const int jp = (j == ns - 1) ? 0 : j + 1;
+  return ((fr[l] - fr[l + ns]) + (ft[l] - ft[(size_t)i * ns + jp])) / surf[i];
+}
+
+// New density and vtheta (into scratch): mass by the flux differences, the
+// angular momentum of every vtheta face's control volume by the same mass
+// fluxes carrying the upwind R vtheta.
+__global__ void k_apply_mass(KP k, const double *fr, const double *ft, const double *surf, double *rho_new,
+                             double *vt_new)
+{
+  const int i = blockIdx.y, ns = k.ns, nr = k.nr;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const size_t l = (size_t)i * ns + j;
+  const int jm = (j == 0) ? ns - 1 : j - 1, jp = (j == ns - 1) ? 0 : j + 1;
+  const size_t ljm = (size_t)i * ns + jm, ljp = (size_t)i * ns + jp;
+  const double ds = dsigma(k, fr, ft, surf, i, j), dsm = dsigma(k, fr, ft, surf, i, jm);
+  const double R = k.rmed[i];
+  const double *vt = k.vt;
+  // mass through the radial boundaries of the face control volume (i,j)
+  const double gin = 0.5 * (fr[ljm] + fr[l]);
+  const double gout = 0.5 * (fr[ljm + ns] + fr[l + ns]);
+  const double lin = (gin > 0.0) ? k.rmed[i - 1 >= 0 ? i - 1 : 0] * vt[(i >= 1 ? l - ns : l)] : R * vt[l];
+  const double lout = (gout > 0.0) ? R * vt[l] : (i + 1 < nr ? k.rmed[i + 1] * vt[l + ns] : R * vt[l]);
+  // mass through the cell centres (i,j-1) (in) and (i,j) (out)
+  const double tin = 0.5 * (ft[ljm] + ft[l]);
+  const double tout = 0.5 * (ft[l] + ft[ljp]);
+  const double ltin = (tin > 0.0) ? R * vt[ljm] : R * vt[l];
+  const double ltout = (tout > 0.0) ? R * vt[l] : R * vt[ljp];
+  const double dJ = ((gin * lin - gout * lout) + (tin * ltin - tout * ltout)) / surf[i];
+  const double J = 0.5 * (k.rho[ljm] + k.rho[l]) * R * vt[l] + dJ;
+  const double rho_l = k.rho[l] + ds, rho_jm = k.rho[ljm] + dsm;
+  rho_new[l] = rho_l;
+  vt_new[l] = J / (0.5 * (rho_jm + rho_l) * R);
 }
 
 __global__ void k_copy(double *dst, const double *src, size_t n)
@@ -475,30 +516,40 @@ __global__ void k_pack_weights(const float *w, bf16 *wf, bf16 *wb, int cin, int 
   wb[((size_t)c * 9 + (8 - tap)) * cout + o] = v;
 }
 
-__global__ void k_stats(const float *Y, const float *surf, int nr, int ns, int count, double *acc)
+__global__ void k_stats(const float *Y, const float *sig, const float *surf, int nr, int ns, int count, double *acc)
 {
-  // acc[q] += Y_q^2, acc[3+q] += (Y_q Surf)^2
-  __shared__ double sh[6][256];
+  // acc[0] += Y_m^2, acc[1] += (Y_m Surf / Sigma0)^2
+  __shared__ double sh[2][256];
   const size_t n = (size_t)nr * ns;
-  double s[6] = {0, 0, 0, 0, 0, 0};
+  double s0 = 0.0, s1 = 0.0;
   for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < n * count; t += (size_t)gridDim.x * blockDim.x) {
     const size_t smp = t / n, l = t - smp * n;
     const int i = (int)(l / ns);
-    for (int q = 0; q < 3; q++) {
-      const double y = Y[(smp * 3 + q) * n + l];
-      s[q] += y * y;
-      s[3 + q] += (y * surf[i]) * (y * surf[i]);
-    }
+    const double y = Y[smp * 3 * n + l];
+    const double u = y * surf[i] / sig[smp * nr + i];
+    s0 += y * y;
+    s1 += u * u;
   }
-  for (int q = 0; q < 6; q++) sh[q][threadIdx.x] = s[q];
+  sh[0][threadIdx.x] = s0;
+  sh[1][threadIdx.x] = s1;
   __syncthreads();
   for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-    if (threadIdx.x < w)
-      for (int q = 0; q < 6; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + w];
+    if (threadIdx.x < w) {
+      sh[0][threadIdx.x] += sh[0][threadIdx.x + w];
+      sh[1][threadIdx.x] += sh[1][threadIdx.x + w];
+    }
     __syncthreads();
   }
-  if (threadIdx.x == 0)
-    for (int q = 0; q < 6; q++) atomicAdd(acc + q, sh[q][0]);
+  if (threadIdx.x == 0) {
+    atomicAdd(acc, sh[0][0]);
+    atomicAdd(acc + 1, sh[1][0]);
+  }
+}
+
+__global__ void k_store_sig(KP k, float *out)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < k.nr) out[i] = (float)k.sigmamed[i];
 }
 
 // ================================================================== host
@@ -514,11 +565,15 @@ struct fb_closure {
   // output scales and loss weights (float for training, double for apply)
   float *scale_f, *wq_f;
   double *scale_d, *surf_d;
+  double *scale_apply;  // scale * gain, used by fb_closure_apply
+  double gain;
+  float *out_sat;       // saturated outputs (inference)
   float *surf_f;
   float h_scale[3], h_wq[3];
   // dataset
   bf16 *X;
   float *Y;
+  float *sig;  // initial density profile of each sample's disc [cap][nr]
   // minibatch work buffers (bmax samples)
   int bmax;
   bf16 *act[CL_LAYERS];   // act[l] = output of layer l (bf16), l < 3
@@ -531,7 +586,7 @@ struct fb_closure {
   double *stats;
   // inference scratch
   bf16 *xin;
-  double *rho_new;
+  double *rho_new, *fr, *ft, *vt_new;
   double lmid, lhalf;
   char err[256];
 };
@@ -591,12 +646,12 @@ extern "C" int fb_closure_create(const fb_ctx *coarse, int capacity, int batch, 
     c->nw[l] = nw;
     // He initialisation over the used input channels; the last layer small,
     // so that training starts near "no correction"
-    const int cin_used = (l == 0) ? 5 : cin;
+    const int cin_used = (l == 0) ? 7 : cin;
     const double sd = sqrt(2.0 / (9.0 * cin_used)) * (l == CL_LAYERS - 1 ? 0.05 : 1.0);
     std::vector<float> hw(nw);
     for (int t = 0; t < nw; t++) {
       const int ci = t % cin, o = t / (9 * cin);
-      const bool used = (ci < cin_used) && (l < CL_LAYERS - 1 || o < 6);
+      const bool used = (ci < cin_used) && (l < CL_LAYERS - 1 || o < 2);
       hw[t] = used ? (float)(sd * cl_gauss(&s)) : 0.0f;
     }
     rc |= cl_alloc((void **)&c->w[l], nw * 4) | cl_alloc((void **)&c->b[l], cout * 4);
@@ -608,8 +663,12 @@ extern "C" int fb_closure_create(const fb_ctx *coarse, int capacity, int batch, 
   }
   rc |= cl_alloc((void **)&c->scale_f, 4 * 4) | cl_alloc((void **)&c->wq_f, 4 * 4);
   rc |= cl_alloc((void **)&c->scale_d, 4 * 8) | cl_alloc((void **)&c->surf_d, c->nr * 8);
+  rc |= cl_alloc((void **)&c->scale_apply, 4 * 8) | cl_alloc((void **)&c->out_sat, n * CL_COUT * 4);
   rc |= cl_alloc((void **)&c->surf_f, c->nr * 4);
   rc |= cl_alloc((void **)&c->X, (size_t)capacity * n * CL_CIN * 2) | cl_alloc((void **)&c->Y, (size_t)capacity * 3 * n * 4);
+  rc |= cl_alloc((void **)&c->sig, (size_t)capacity * c->nr * 4);
+  rc |= cl_alloc((void **)&c->fr, (n + c->ns) * 8) | cl_alloc((void **)&c->ft, n * 8) |
+        cl_alloc((void **)&c->vt_new, n * 8);
   for (int l = 0; l < CL_LAYERS - 1 && !rc; l++) {
     rc |= cl_alloc((void **)&c->act[l], (size_t)batch * n * CL_C * 2);
     rc |= cl_alloc((void **)&c->z[l], (size_t)batch * n * CL_C * 4);
@@ -633,6 +692,8 @@ extern "C" int fb_closure_create(const fb_ctx *coarse, int capacity, int batch, 
   cudaMemcpy(c->wq_f, c->h_wq, 12, cudaMemcpyHostToDevice);
   double sdd[3] = {1.0, 1.0, 1.0};
   cudaMemcpy(c->scale_d, sdd, 24, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->scale_apply, sdd, 24, cudaMemcpyHostToDevice);
+  c->gain = 1.0;
   cl_pack(c);
   if (cudaStreamSynchronize(c->st) != cudaSuccess) { fb_closure_destroy(c); return FB_ERR_CUDA; }
   *out = c;
@@ -648,8 +709,8 @@ extern "C" int fb_closure_destroy(fb_closure *c)
                  c->act[l], c->z[l], c->dz[l]};
     for (void *q : p) cudaFree(q);
   }
-  void *p[] = {c->scale_f, c->wq_f, c->scale_d, c->surf_d, c->surf_f, c->X, c->Y, c->out, c->G,
-               c->loss_part, c->idx, c->stats, c->xin, c->rho_new};
+  void *p[] = {c->scale_f, c->wq_f, c->scale_d, c->scale_apply, c->out_sat, c->surf_d, c->surf_f, c->X, c->Y, c->out, c->G,
+               c->loss_part, c->idx, c->stats, c->xin, c->rho_new, c->sig, c->fr, c->ft, c->vt_new};
   for (void *q : p) cudaFree(q);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -707,27 +768,36 @@ extern "C" int fb_closure_scales(fb_closure *c, double *scale, double *wq, int g
   cudaMemcpy(c->scale_f, c->h_scale, 12, cudaMemcpyHostToDevice);
   cudaMemcpy(c->wq_f, c->h_wq, 12, cudaMemcpyHostToDevice);
   cudaMemcpy(c->scale_d, scale, 24, cudaMemcpyHostToDevice);
+  double sa[3] = {scale[0] * c->gain, scale[1] * c->gain, scale[2] * c->gain};
+  cudaMemcpy(c->scale_apply, sa, 24, cudaMemcpyHostToDevice);
   return FB_OK;
 }
 
-// Scales from the first `count` samples: scale_q = rms(Y_q Surf) (so the
-// network's fluxes are O(1)), w_q = 1 / mean(Y_q^2).
+// Strength of the applied correction (1 = as trained); training is unaffected.
+extern "C" int fb_closure_set_gain(fb_closure *c, double gain)
+{
+  if (!c || !(gain >= 0.0) || gain > 10.0) return FB_ERR_INVALID;
+  c->gain = gain;
+  double sa[3] = {c->h_scale[0] * gain, c->h_scale[1] * gain, c->h_scale[2] * gain};
+  return cudaMemcpy(c->scale_apply, sa, 24, cudaMemcpyHostToDevice) == cudaSuccess ? FB_OK : FB_ERR_CUDA;
+}
+
+// Scale and loss weight of the mass correction from the first `count`
+// samples: scale = rms(Y_m Surf / Sigma0) (the network's fluxes are then
+// O(1)), w = 1 / mean(Y_m^2).  The momentum entries are kept at 1.
 extern "C" int fb_closure_autoscale(fb_closure *c, int count)
 {
   if (!c || count < 1 || count > c->count) return FB_ERR_INVALID;
   cudaMemsetAsync(c->stats, 0, 8 * 8, c->st);
-  k_stats<<<148 * 4, 256, 0, c->st>>>(c->Y, c->surf_f, c->nr, c->ns, count, c->stats);
-  double h[6];
-  if (cudaMemcpyAsync(h, c->stats, 48, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
+  k_stats<<<148 * 4, 256, 0, c->st>>>(c->Y, c->sig, c->surf_f, c->nr, c->ns, count, c->stats);
+  double h[2];
+  if (cudaMemcpyAsync(h, c->stats, 16, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
       cudaStreamSynchronize(c->st) != cudaSuccess)
     return FB_ERR_CUDA;
   const double n = (double)c->nr * c->ns * count;
-  double scale[3], wq[3];
-  for (int q = 0; q < 3; q++) {
-    const double ms = h[q] / n, mss = h[3 + q] / n;
-    scale[q] = mss > 0.0 ? sqrt(mss) : 1.0;
-    wq[q] = ms > 0.0 ? 1.0 / ms : 1.0;
-  }
+  double scale[3] = {1.0, 1.0, 1.0}, wq[3] = {1.0, 1.0, 1.0};
+  scale[0] = h[1] > 0.0 ? sqrt(h[1] / n) : 1.0;
+  wq[0] = h[0] > 0.0 ? n / h[0] : 1.0;
   return fb_closure_scales(c, scale, wq, 0);
 }
 
@@ -749,6 +819,7 @@ extern "C" int fb_closure_record(fb_closure *c, fb_ctx *coarse, int slot, int wh
   const size_t n = (size_t)c->nr * c->ns;
   if (what == 0) {
     cl_features(c, coarse, c->X + (size_t)slot * n * CL_CIN, s);
+    k_store_sig<<<(c->nr + 127) / 128, 128, 0, s>>>(*kp, c->sig + (size_t)slot * c->nr);
   } else {
     dim3 gr((c->ns + 127) / 128, c->nr);
     k_conservative<<<gr, 128, 0, s>>>(*kp, c->Y + (size_t)slot * 3 * n, what == 1 ? -1.0f : 1.0f, what == 2);
@@ -758,15 +829,17 @@ extern "C" int fb_closure_record(fb_closure *c, fb_ctx *coarse, int slot, int wh
   return cudaGetLastError() == cudaSuccess ? FB_OK : FB_ERR_CUDA;
 }
 
-// Host-provided sample (features as floats, rounded to BF16; targets).
-extern "C" int fb_closure_set_sample(fb_closure *c, int slot, const float *x, const float *y)
+// Host-provided sample (features as floats, rounded to BF16; targets;
+// initial density profile of the sample's disc).
+extern "C" int fb_closure_set_sample(fb_closure *c, int slot, const float *x, const float *y, const float *sig)
 {
-  if (!c || !x || !y || slot < 0 || slot >= c->cap) return FB_ERR_INVALID;
+  if (!c || !x || !y || !sig || slot < 0 || slot >= c->cap) return FB_ERR_INVALID;
   const size_t n = (size_t)c->nr * c->ns;
   std::vector<bf16> hx(n * CL_CIN);
   for (size_t t = 0; t < hx.size(); t++) hx[t] = __float2bfloat16(x[t]);
   if (cudaMemcpy(c->X + (size_t)slot * n * CL_CIN, hx.data(), hx.size() * 2, cudaMemcpyHostToDevice) != cudaSuccess ||
-      cudaMemcpy(c->Y + (size_t)slot * 3 * n, y, 3 * n * 4, cudaMemcpyHostToDevice) != cudaSuccess)
+      cudaMemcpy(c->Y + (size_t)slot * 3 * n, y, 3 * n * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->sig + (size_t)slot * c->nr, sig, c->nr * 4, cudaMemcpyHostToDevice) != cudaSuccess)
     return FB_ERR_CUDA;
   if (slot + 1 > c->count) c->count = slot + 1;
   return FB_OK;
@@ -805,8 +878,9 @@ static int cl_loss_grad(fb_closure *c, const int *hidx, int nb, double *loss)
   cudaMemcpyAsync(c->idx, hidx, nb * 4, cudaMemcpyHostToDevice, s);
   cl_forward(c, xb, nb, 1, s);
   const int nblk = (int)((n * nb + 255) / 256);
-  k_loss<<<nblk, 256, 0, s>>>(c->out, c->Y, c->idx, c->scale_f, c->wq_f, c->surf_f, c->G, c->loss_part, nr, ns, nb);
-  k_loss_adjoint<<<nblk, 256, 0, s>>>(c->G, c->scale_f, c->surf_f, c->dz[3], nr, ns, nb);
+  k_loss<<<nblk, 256, 0, s>>>(c->out, c->Y, c->sig, c->idx, c->scale_f, c->wq_f, c->surf_f, c->G, c->loss_part, nr, ns,
+                              nb);
+  k_loss_adjoint<<<nblk, 256, 0, s>>>(c->G, c->sig, c->idx, c->scale_f, c->surf_f, c->dz[3], nr, ns, nb);
   dim3 gr(ns / CL_TILE, nr, nb);
   // backward data: dz[l-1] = conv^T(dz[l]) * GELU'(z[l-1])
   k_conv<CL_COUT, CL_C, 2><<<gr, CL_BS, 0, s>>>(c->dz[3], c->wbk[3], NULL, c->z[2], c->dz[2], NULL, NULL, nr, ns);
@@ -925,11 +999,13 @@ extern "C" int fb_closure_apply(fb_closure *c, fb_ctx *coarse)
   k_conv<CL_C, CL_C, 0><<<gr, CL_BS, 0, s>>>(c->act[0], c->wf[1], c->b[1], NULL, c->act[1], NULL, NULL, nr, ns);
   k_conv<CL_C, CL_C, 0><<<gr, CL_BS, 0, s>>>(c->act[1], c->wf[2], c->b[2], NULL, c->act[2], NULL, NULL, nr, ns);
   k_conv<CL_C, CL_COUT, 1><<<gr, CL_BS, 0, s>>>(c->act[2], c->wf[3], c->b[3], NULL, NULL, c->out, NULL, nr, ns);
-  dim3 g2((ns + 127) / 128, nr);
-  k_apply_density<<<g2, 128, 0, s>>>(*kp, c->out, c->scale_d, c->surf_d, c->rho_new);
-  k_apply_velocities<<<g2, 128, 0, s>>>(*kp, c->out, c->scale_d, c->surf_d, c->rho_new);
+  k_saturate<<<256, 256, 0, s>>>(c->out, c->out_sat, (size_t)nr * ns * CL_COUT);
+  k_face_flux<<<dim3((ns + 127) / 128, nr + 1), 128, 0, s>>>(*kp, c->out_sat, (double)c->h_scale[0] * c->gain, c->fr,
+                                                               c->ft);
+  k_apply_mass<<<dim3((ns + 127) / 128, nr), 128, 0, s>>>(*kp, c->fr, c->ft, c->surf_d, c->rho_new, c->vt_new);
   k_copy<<<256, 256, 0, s>>>(kp->rho, c->rho_new, (size_t)nr * ns);
-  fb_ctx_count_launches(coarse, 8);
+  k_copy<<<256, 256, 0, s>>>(kp->vt, c->vt_new, (size_t)nr * ns);
+  fb_ctx_count_launches(coarse, 10);
   if (cudaStreamSynchronize(s) != cudaSuccess) return FB_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? FB_OK : FB_ERR_CUDA;
 }

@@ -258,6 +258,19 @@ __global__ void __launch_bounds__(SG_BS) sg_cols(FftArgs fa, int nrows_in, int n
     const int i = t / SG_KC, c = t - i * SG_KC, k = k0 + c;
     x[(size_t)c * m + i] = (i < nrows_in && k < nk) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
   }
+  // the kernel spectrum of these wavenumbers goes to registers now, so that
+  // its loads complete while the forward transform runs
+  constexpr int KPT = 8;
+  const bool pref = (mode == 1) && (SG_KC * m <= KPT * SG_BS);
+  double2 kpre[KPT];
+  if (pref) {
+#pragma unroll
+    for (int q = 0; q < KPT; q++) {
+      const int t = threadIdx.x + q * SG_BS;
+      const int c = t / m, i = t - c * m, k = k0 + c;
+      kpre[q] = (t < SG_KC * m && k < nk) ? kh[(size_t)k * m + i] : make_double2(0.0, 0.0);
+    }
+  }
   double2 *X = fft_smem_t<0, SG_KC>(x, y, fa);
   if (mode == 0) {
     for (int c = 0; c < SG_KC; c++)
@@ -265,11 +278,23 @@ __global__ void __launch_bounds__(SG_BS) sg_cols(FftArgs fa, int nrows_in, int n
         for (int i = threadIdx.x; i < m; i += blockDim.x) kh[(size_t)(k0 + c) * m + i] = X[(size_t)c * m + i];
     return;
   }
-  for (int t = threadIdx.x; t < SG_KC * m; t += blockDim.x) {
-    const int c = t / m, i = t - c * m, k = k0 + c;
-    if (k < nk) {
-      const double2 K = kh[(size_t)k * m + i], S = X[t];
-      X[t] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
+  if (pref) {
+#pragma unroll
+    for (int q = 0; q < KPT; q++) {
+      const int t = threadIdx.x + q * SG_BS;
+      const int c = t / m, k = k0 + c;
+      if (t < SG_KC * m && k < nk) {
+        const double2 K = kpre[q], S = X[t];
+        X[t] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
+      }
+    }
+  } else {
+    for (int t = threadIdx.x; t < SG_KC * m; t += blockDim.x) {
+      const int c = t / m, i = t - c * m, k = k0 + c;
+      if (k < nk) {
+        const double2 K = kh[(size_t)k * m + i], S = X[t];
+        X[t] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
+      }
     }
   }
   double2 *Y = (X == x) ? y : x;

@@ -266,14 +266,15 @@ int fb_batch_destroy(fb_batch *b);
 /* ---- learned coarse-grid closure (no counterpart in the reference) -------
    A 4-layer periodic-in-azimuth CNN (3x3 convolutions, 32 channels, GELU;
    BF16 weights and activations, FP32 accumulation on the tensor cores) that
-   reads a coarse disc and returns face-flux corrections of mass, angular
-   momentum and radial momentum, applied as flux differences (mass and
-   angular momentum change only by round-off).  The coarse grid's nsec must
-   be a multiple of 64; isothermal discs.  Training samples live on the
-   device: for sample s, fb_closure_record(.., s, 0) stores the input
-   features of the coarse disc, (.., s, 1) subtracts the conservative
-   variables after the plain method's DT, (.., s, 2) adds those of the
-   coarse-grained fine disc one DT later (the target correction). */
+   reads a coarse disc and returns two face fluxes of mass per cell (in units
+   of scale x the disc's initial density at the face), applied as flux
+   differences; the corrected mass carries its upwind angular momentum, so
+   mass and angular momentum change only by round-off.  The coarse grid's
+   nsec must be a multiple of 64; isothermal discs.  Training samples live
+   on the device: for sample s, fb_closure_record(.., s, 0) stores the input
+   features (and the initial density profile) of the coarse disc, (.., s, 1)
+   subtracts its conservative variables after the plain method's DT, (.., s,
+   2) adds those of the coarse-grained fine disc one DT later (the target). */
 typedef struct fb_closure fb_closure;
 int fb_closure_create(const fb_ctx *coarse, int capacity, int batch, unsigned long long seed, fb_closure **out);
 int fb_closure_destroy(fb_closure *c);
@@ -281,14 +282,16 @@ int fb_closure_num_params(const fb_closure *c, int *nweights, int *nbiases);
 /* get = 1 copies FP32 weights ([out][tap][in] per layer) and biases out,
    get = 0 sets them */
 int fb_closure_params(fb_closure *c, float *w, float *b, int get);
-/* 3 output scales (flux units) and 3 loss weights, get or set */
+/* 3 output scales and 3 loss weights (entry 0: mass; 1, 2 unused), get or set */
 int fb_closure_scales(fb_closure *c, double *scale, double *wq, int get);
-/* scales from the first `count` samples: rms(target * Surf), 1/mean(target^2) */
+/* scale and weight from the first `count` samples:
+   rms(target * Surf / Sigma0), 1/mean(target^2) */
 int fb_closure_autoscale(fb_closure *c, int count);
 int fb_closure_record(fb_closure *c, fb_ctx *coarse, int slot, int what);
 /* host-provided sample: x = nrad*nsec*16 feature floats (rounded to BF16),
-   y = 3*nrad*nsec targets */
-int fb_closure_set_sample(fb_closure *c, int slot, const float *x, const float *y);
+   y = 3*nrad*nsec targets (mass, angular and radial momentum; the loss
+   uses the mass), sig = nrad initial densities of the sample's disc */
+int fb_closure_set_sample(fb_closure *c, int slot, const float *x, const float *y, const float *sig);
 /* loss and gradients (same layout as fb_closure_params) of samples
    [first, first+nb), no update; gw/gb may be NULL */
 int fb_closure_loss_grad(fb_closure *c, int first, int nb, double *loss, float *gw, float *gb);
@@ -296,11 +299,14 @@ int fb_closure_loss_grad(fb_closure *c, int first, int nb, double *loss, float *
    first+count); loss_out[iters] optional */
 int fb_closure_train(fb_closure *c, int first, int count, int nb, int iters, double lr, unsigned long long seed,
                      double *loss_out);
-/* network output (nrad*nsec*16 floats, channels 0..5 = Fr,Ft of m, J, P)
+/* network output (nrad*nsec*16 floats, channels 0, 1 = the mass fluxes)
    for sample slot, or for the coarse disc's state when slot < 0 */
 int fb_closure_infer(fb_closure *c, const fb_ctx *coarse, int slot, float *out);
-/* one correction of the coarse disc's state, in place */
+/* one correction of the coarse disc's state (density and vtheta), in
+   place; each face flux is saturated at 3 output scales (3 tanh(F/3), a
+   conservative map) and multiplied by the gain (default 1) */
 int fb_closure_apply(fb_closure *c, fb_ctx *coarse);
+int fb_closure_set_gain(fb_closure *c, double gain);
 /* coarse disc := coarse-graining of a fine disc on the same radii whose
    grid is an integer multiple in both directions (isothermal) */
 int fb_downsample(const fb_ctx *fine, fb_ctx *coarse);

@@ -3,9 +3,9 @@ checker of the GPU kernels in dustyfargoadsg_b200/csrc/fb_closure.cu).
 
 Network: 4 layers of 3x3 convolutions on NHWC arrays [sample][ring][azimuth]
 [channel], periodic in azimuth, zero-padded in radius; channels 16 -> 32 ->
-32 -> 32 -> 16; GELU after the first three.  Loss: the correction of the
-conservative quantities m, J, P built from the six output face fluxes by the
-flux-difference operator, against targets, weighted per quantity.
+32 -> 32 -> 16; GELU after the first three.  Loss: the mass correction built
+from the two output face fluxes (scaled by the disc's initial density at the
+face) by the flux-difference operator, against targets.
 
 `bf16=True` rounds to bfloat16 where the GPU stores bfloat16 (weights, the
 input, hidden activations, every back-propagated pre-activation gradient),
@@ -77,43 +77,37 @@ def conv_data_grad(dz, w):
     return dx_
 
 
-def masks(nr):
-    mr = np.zeros((3, nr + 1))
-    mr[0, 1:nr] = 1.0
-    mr[1, 1:nr] = 1.0
-    mr[2, 2:nr] = 1.0
-    mt = np.ones((3, nr))
-    mt[2, 0] = 0.0
-    return mr, mt
+def sig_face(sig):
+    """Sigma0 at the radial faces 0..nr (geometric mean; 0 at the edges)."""
+    nr = sig.shape[-1]
+    f = np.zeros(sig.shape[:-1] + (nr + 1,))
+    f[..., 1:nr] = np.sqrt(sig[..., :-1] * sig[..., 1:])
+    return f
 
 
-def flux_diff(O, scale, surf):
-    """dq [B,3,nr,ns] from the network output O [B,nr,ns,16]."""
+def flux_diff(O, scale, surf, sig):
+    """dSigma [B,nr,ns] from the network output O [B,nr,ns,16]: channel 0 is
+    the flux through each cell's inner radial face, channel 1 through its
+    lower azimuthal face, in units of scale * Sigma0(face); sig [B,nr]."""
     B, nr, ns, _ = O.shape
-    mr, mt = masks(nr)
-    dq = np.zeros((B, 3, nr, ns))
-    for q in range(3):
-        fr = O[..., 2 * q]
-        ft = O[..., 2 * q + 1]
-        fr_in = fr * mr[q, :nr][None, :, None]
-        fr_out = np.zeros_like(fr)
-        fr_out[:, :-1] = fr[:, 1:] * mr[q, 1:nr][None, :, None]
-        dft = (ft - np.roll(ft, -1, axis=2)) * mt[q][None, :, None]
-        dq[:, q] = scale[q] * ((fr_in - fr_out) + dft) / surf[None, :, None]
-    return dq
+    sf = sig_face(sig)  # [B, nr+1]
+    fr = O[..., 0] * sf[:, :nr, None]
+    fr_out = np.zeros_like(fr)
+    fr_out[:, :-1] = O[:, 1:, :, 0] * sf[:, 1:nr, None]
+    dft = (O[..., 1] - np.roll(O[..., 1], -1, axis=2)) * sig[:, :, None]
+    return scale * ((fr - fr_out) + dft) / surf[None, :, None]
 
 
-def flux_diff_adjoint(G, scale, surf):
-    """dL/dO [B,nr,ns,16] from G = dL/d(dq) [B,3,nr,ns]."""
-    B, _, nr, ns = G.shape
-    mr, mt = masks(nr)
+def flux_diff_adjoint(G, scale, surf, sig):
+    """dL/dO [B,nr,ns,16] from G = dL/d(dSigma) [B,nr,ns]."""
+    B, nr, ns = G.shape
+    sf = sig_face(sig)
+    g = G / surf[None, :, None]
+    gm = np.zeros_like(g)
+    gm[:, 1:] = g[:, :-1]
     dO = np.zeros((B, nr, ns, 16))
-    for q in range(3):
-        g = G[:, q] / surf[None, :, None]
-        gm = np.zeros_like(g)
-        gm[:, 1:] = g[:, :-1]
-        dO[..., 2 * q] = scale[q] * (g - gm) * mr[q, :nr][None, :, None]
-        dO[..., 2 * q + 1] = scale[q] * (g - np.roll(g, 1, axis=2)) * mt[q][None, :, None]
+    dO[..., 0] = scale * sf[:, :nr, None] * (g - gm)
+    dO[..., 1] = scale * sig[:, :, None] * (g - np.roll(g, 1, axis=2))
     return dO
 
 
@@ -132,22 +126,23 @@ def forward(params, x, bf16=True):
     return out, acts, zs
 
 
-def loss_and_grads(params, x, y, scale, wq, surf, bf16=True):
-    """Loss and [(dW, db)] per layer for samples x [B,nr,ns,16], y [B,3,nr,ns]."""
+def loss_and_grads(params, x, y, scale, w, surf, sig, bf16=True):
+    """Loss and [(dW, db)] per layer for samples x [B,nr,ns,16], mass targets
+    y [B,nr,ns], initial density profiles sig [B,nr]."""
     r = bf16_round if bf16 else (lambda a: a)
     out, acts, zs = forward(params, x, bf16)
     B, nr, ns, _ = out.shape
-    d = flux_diff(out, scale, surf) - y
+    d = flux_diff(out, scale, surf, sig) - y
     n = B * nr * ns
-    L = sum(wq[q] * np.sum(d[:, q] ** 2) for q in range(3)) / n
-    G = np.stack([2.0 * wq[q] * d[:, q] / n for q in range(3)], axis=1)
-    dz = r(flux_diff_adjoint(G, scale, surf))
+    L = w * np.sum(d ** 2) / n
+    G = 2.0 * w * d / n
+    dz = r(flux_diff_adjoint(G, scale, surf, sig))
     grads = [None] * len(params)
     for l in range(len(params) - 1, -1, -1):
-        w = r(params[l][0])
+        wl = r(params[l][0])
         grads[l] = (conv_wgrad(acts[l], dz), dz.sum(axis=(0, 1, 2)))
         if l > 0:
-            dz = r(conv_data_grad(dz, w) * gelu_grad(zs[l - 1]))
+            dz = r(conv_data_grad(dz, wl) * gelu_grad(zs[l - 1]))
     return L, grads
 
 

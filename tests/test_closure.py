@@ -18,10 +18,10 @@ def test_reference_gradients_match_finite_differences():
     _, surf = _geometry(nr, ns)
     params = R.init_params(seed=2, scale=0.5)
     x = rng.uniform(-1, 1, (B, nr, ns, 16))
-    y = rng.standard_normal((B, 3, nr, ns)) * 0.1
-    scale = np.array([0.02, 0.03, 0.01])
-    wq = np.array([1.0, 2.0, 0.5])
-    L, grads = R.loss_and_grads(params, x, y, scale, wq, surf, bf16=False)
+    y = rng.standard_normal((B, nr, ns)) * 0.1
+    sig = rng.uniform(0.5, 2.0, (B, nr))
+    scale, wq = 0.02, 1.7
+    L, grads = R.loss_and_grads(params, x, y, scale, wq, surf, sig, bf16=False)
     eps = 1e-6
     for l in range(len(params)):
         w, b = params[l]
@@ -32,9 +32,9 @@ def test_reference_gradients_match_finite_differences():
             wm[idx] -= eps
             pp = list(params)
             pp[l] = (wp, b)
-            Lp, _ = R.loss_and_grads(pp, x, y, scale, wq, surf, bf16=False)
+            Lp, _ = R.loss_and_grads(pp, x, y, scale, wq, surf, sig, bf16=False)
             pp[l] = (wm, b)
-            Lm, _ = R.loss_and_grads(pp, x, y, scale, wq, surf, bf16=False)
+            Lm, _ = R.loss_and_grads(pp, x, y, scale, wq, surf, sig, bf16=False)
             num = (Lp - Lm) / (2 * eps)
             ana = grads[l][0][idx]
             assert abs(num - ana) <= 1e-6 * max(1.0, abs(num)) + 1e-9, (l, idx, num, ana)
@@ -45,9 +45,9 @@ def test_reference_gradients_match_finite_differences():
             bm[o] -= eps
             pp = list(params)
             pp[l] = (w, bp)
-            Lp, _ = R.loss_and_grads(pp, x, y, scale, wq, surf, bf16=False)
+            Lp, _ = R.loss_and_grads(pp, x, y, scale, wq, surf, sig, bf16=False)
             pp[l] = (w, bm)
-            Lm, _ = R.loss_and_grads(pp, x, y, scale, wq, surf, bf16=False)
+            Lm, _ = R.loss_and_grads(pp, x, y, scale, wq, surf, sig, bf16=False)
             num = (Lp - Lm) / (2 * eps)
             assert abs(num - grads[l][1][o]) <= 1e-6 * max(1.0, abs(num)) + 1e-9, (l, o)
 
@@ -55,13 +55,12 @@ def test_reference_gradients_match_finite_differences():
 def test_flux_difference_conserves():
     nr, ns = 7, 16
     _, surf = _geometry(nr, ns)
-    O = np.random.RandomState(3).standard_normal((1, nr, ns, 16))
-    dq = R.flux_diff(O, np.array([1.0, 2.0, 3.0]), surf)
-    for q in range(3):
-        total = np.sum(dq[0, q] * surf[:, None])
-        assert abs(total) < 1e-12 * np.sum(np.abs(dq[0, q] * surf[:, None]))
-    # P (q = 2) never touches its boundary ring 0
-    assert np.all(dq[0, 2, 0] == 0.0)
+    rng = np.random.RandomState(3)
+    O = rng.standard_normal((1, nr, ns, 16))
+    sig = rng.uniform(0.5, 2.0, (1, nr))
+    dq = R.flux_diff(O, 1.3, surf, sig)
+    total = np.sum(dq[0] * surf[:, None])
+    assert abs(total) < 1e-12 * np.sum(np.abs(dq[0] * surf[:, None]))
 
 
 def test_adjoint_is_the_transpose():
@@ -69,11 +68,11 @@ def test_adjoint_is_the_transpose():
     _, surf = _geometry(nr, ns)
     rng = np.random.RandomState(4)
     O = rng.standard_normal((2, nr, ns, 16))
-    O[..., 6:] = 0.0
-    G = rng.standard_normal((2, 3, nr, ns))
-    scale = np.array([0.5, 1.5, 2.0])
-    lhs = np.sum(R.flux_diff(O, scale, surf) * G)
-    rhs = np.sum(O * R.flux_diff_adjoint(G, scale, surf))
+    O[..., 2:] = 0.0
+    G = rng.standard_normal((2, nr, ns))
+    sig = rng.uniform(0.5, 2.0, (2, nr))
+    lhs = np.sum(R.flux_diff(O, 0.7, surf, sig) * G)
+    rhs = np.sum(O * R.flux_diff_adjoint(G, 0.7, surf, sig))
     assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
 
 
