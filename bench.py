@@ -351,11 +351,17 @@ def main():
     if best is not None:
         bpc = STAGE_BYTES.get(best, (None, None))[energy]
         ms, cnt = prof[best]
-        achieved = (bpc * cells / (ms / cnt * 1e-3) / 1e9) if bpc else None
+        units = cells
+        if best == "dust_particles":
+            # per particle and substep: read r, th, vr, vth, size, St, flag and
+            # write r, th, vr, vth, St (96 B); the grid gathers are L2 hits
+            bpc, units = 96, disc.npart
+            cnt = cnt / (8 if p.dust_feel_turb else 2)  # launches per substep
+        achieved = (bpc * units / (ms / cnt * 1e-3) / 1e9) if bpc else None
         roofline = {"bound": "hbm", "kernel": best, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": (achieved / peak) if achieved else None,
                     "traffic": traffic_per_launch(args.workload, best),
-                    "algorithmic_bytes_per_launch": bpc * cells if bpc else None,
+                    "algorithmic_bytes_per_launch": bpc * units if bpc else None,
                     "peak_kind": peak_kind + " HBM copy bandwidth",
                     "share_of_step": ms / sum(v[0] for v in prof.values())}
 

@@ -159,9 +159,12 @@ static int dust_create(fb_ctx *ctx)
   for (size_t f = 0; f < sizeof arrays / sizeof arrays[0]; f++)
     if (!(*arrays[f] = dalloc(ctx, n))) return FB_ERR_NOMEM;
   const int nsb = (n + 1023) / 1024, ncb = (pp.ncand + 255) / 256;
-  int **ints[] = {&pp.flag, &pp.kidx, &pp.kick_bsum, &pp.cand_flag, &pp.cand_bsum};
-  const size_t isz[] = {(size_t)n, (size_t)n, (size_t)nsb, (size_t)pp.ncand, (size_t)ncb};
-  for (size_t f = 0; f < 5; f++) {
+  pp.ncells = ctx->nr * ctx->ns + 1;
+  int **ints[] = {&pp.flag, &pp.kidx, &pp.kick_bsum, &pp.cand_flag, &pp.cand_bsum,
+                  &pp.perm, &pp.key, &pp.cell_count, &pp.cell_bsum};
+  const size_t isz[] = {(size_t)n, (size_t)n, (size_t)nsb, (size_t)pp.ncand, (size_t)ncb,
+                        (size_t)n, (size_t)n, (size_t)pp.ncells, (size_t)(pp.ncells + 1023) / 1024};
+  for (size_t f = 0; f < 9; f++) {
     void *d = NULL;
     if (cudaMalloc(&d, isz[f] * sizeof(int)) != cudaSuccess) return FB_ERR_NOMEM;
     cudaMemset(d, 0, isz[f] * sizeof(int));
@@ -212,6 +215,12 @@ static int dust_create(fb_ctx *ctx)
   // and only the stopping-time bound on the substep remains
   if (p->dust_feedback) k.dust_min_ts = &pp.dc->min_ts;
   if (!pp.azimuth || !pp.aziinf) return FB_ERR_NOMEM;
+  {
+    std::vector<int> id(n);
+    for (int q = 0; q < n; q++) id[q] = q;
+    if (cudaMemcpy(pp.perm, id.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
+      return FB_ERR_CUDA;
+  }
   ctx->has_dust = 1;
   return FB_OK;
 }
@@ -580,6 +589,7 @@ static int enqueue_dt_prelude(fb_ctx *ctx)
     fb_launch_soundspeed(k, 0, s);
     n += 1;
   }
+  if (ctx->has_dust) n += fb_launch_dust_sort(k, ctx->pp, s);  // processing order only
   return n;
 }
 
@@ -887,6 +897,7 @@ extern "C" int fb_dust_upload(fb_ctx *ctx, const fb_dust_state *st)
   h->min_ts = 1e6;
   CK(cudaMemcpyAsync(pp.dc, h, sizeof *h, cudaMemcpyHostToDevice, ctx->st));
   // the interpolation call of main.c:287: Stokes numbers at the uploaded state
+  ctx->launches += fb_launch_dust_sort(ctx->k, pp, ctx->st);
   fb_launch_dust_interpolation_only(ctx->k, pp, ctx->st);
   ctx->launches += 1;
   CK(cudaStreamSynchronize(ctx->st));

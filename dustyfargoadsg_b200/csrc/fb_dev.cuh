@@ -104,6 +104,9 @@ struct fb_dust_ctl {
   long long t_start, c_last;   // first pair event of this substep, last candidate used
   int K, npairs, err, pad;     // kicked particles, accepted pairs needed, shortfall flag
   double min_ts;               // Minimum_Stopping_Time of the last interpolation (Dsys.c:336,758)
+  // per planet, for the substep's velocity update (DustUpdate.c:342-352):
+  // radius, azimuth and smoothing length, the same for every particle
+  double pl_r[FB_MAX_PLANETS], pl_t[FB_MAX_PLANETS], pl_eps[FB_MAX_PLANETS];
 };
 
 // Particle arrays (structure of arrays in the reference's index order) and
@@ -120,6 +123,10 @@ struct PP {
   double aspectratio, thicksmoothing, flaringindex;
   int log_grid, feel_disk, feel_planets, feel_sg, feel_turb, sfta;
   int restokes;  // WRITEDUSTDENSITY: interpolation again after the update (SourceEuler.c:526-531)
+  // processing order: particles sorted by cell once per DT, so that a warp's
+  // grid gathers hit neighbouring cells (results do not depend on the order)
+  int *perm, *key, *cell_count, *cell_bsum;
+  int ncells;  // nr*ns + 1 (the last bucket holds particles off the grid)
 };
 
 // launchers (fb_gas.cu)
@@ -168,6 +175,7 @@ void fb_launch_ring_mean(const double *f, int nr, int ns, double *out, cudaStrea
 void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s);
 void fb_launch_dust_interpolation_only(const KP &k, const PP &pp, cudaStream_t s);
 int  fb_dust_launches(const PP &pp);
+int  fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s);  // returns launches
 int  fb_sg_launches(const fb_sg *sg);  // kernels per fb_sg_accel + update
 void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
 void fb_sg_cols(fb_sg *sg, cudaStream_t s);

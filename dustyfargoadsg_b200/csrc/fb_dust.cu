@@ -29,20 +29,31 @@
 
 static const unsigned long long LCG_A = 0x5DEECE66Dull, LCG_C = 0xBull, M48 = 0xFFFFFFFFFFFFull;
 
-// X_{n+m} from X_n for the drand48 recurrence X <- (a X + c) mod 2^48
+// The recurrence applied 2^i times is again affine, X <- (A_i X + C_i) mod
+// 2^48, with A_0 = a, C_0 = c, A_{i+1} = A_i^2, C_{i+1} = (A_i + 1) C_i.
+struct LcgJumps {
+  unsigned long long A[48], C[48];
+  constexpr LcgJumps() : A(), C()
+  {
+    unsigned long long a = LCG_A, c = LCG_C;
+    for (int i = 0; i < 48; i++) {
+      A[i] = a;
+      C[i] = c;
+      c = ((a + 1) * c) & M48;
+      a = (a * a) & M48;
+    }
+  }
+};
+__constant__ LcgJumps c_jumps = LcgJumps();
+
+// X_{n+m} from X_n: one affine map per set bit of m (the maps commute).  The
+// loop runs over the bit positions, so a warp whose threads skip by similar
+// m reads the same table entry in each iteration.
 static __device__ __forceinline__ unsigned long long lcg_skip(unsigned long long x, unsigned long long m)
 {
-  unsigned long long A = 1, C = 0, a = LCG_A, c = LCG_C;
-  while (m) {
-    if (m & 1ull) {
-      A = (A * a) & M48;
-      C = (C * a + c) & M48;
-    }
-    c = ((a + 1) * c) & M48;
-    a = (a * a) & M48;
-    m >>= 1;
-  }
-  return (A * x + C) & M48;
+  for (int i = 0; m; i++, m >>= 1)
+    if (m & 1ull) x = (c_jumps.A[i] * x + c_jumps.C[i]) & M48;
+  return x;
 }
 
 // drand48's value of a state: X / 2^48, exact in double
@@ -66,14 +77,37 @@ static __device__ __forceinline__ double tsc_weight(double d, double delta)
   return w;
 }
 
+// The reference finds rings by linear searches over the radii (Dsys.c:364,
+// DustUpdate.c:73, Viscosity.c:31); the same indices come from binary
+// searches over the sorted tables here.
+// first index in [0, n) with a[idx] > x, or n (x >= a[idx] keeps searching)
+static __device__ __forceinline__ int first_above(const double *a, int n, double x)
+{
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (x >= a[mid]) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+// first index in [0, n) with a[idx] >= x, or n
+static __device__ __forceinline__ int first_not_below(const double *a, int n, double x)
+{
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (a[mid] < x) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
 // FViscosity (src/Viscosity.c:23-69) at a particle radius.  The reference's
 // search `while (GlobalRmed[i] < rad) i++` has no upper bound and runs past
 // the last ring for radii beyond Rmed[nr-1]; here it stops at the last ring.
 static __device__ double viscosity_at(const KP &k, double rad)
 {
   if (k.visc_mode == 1) {
-    int i = 0;
-    while (i < k.nr - 1 && k.rmed[i] < rad) i++;
+    const int i = first_not_below(k.rmed, k.nr - 1, rad);  // <= nr-1
     return k.alpha * k.gcs[i] * k.gcs[i] * pow(rad, 1.5);
   }
   return (k.visc_mode == 2) ? k.nu_const : 0.0;
@@ -111,6 +145,17 @@ __global__ void __launch_bounds__(D_BS) k_dust_drift(KP k, PP pp)
 {
   const int q = blockIdx.x * D_BS + threadIdx.x;
   if (q == 0) pp.dc->min_ts = 1e6;  // reset by every interpolation call (Dsys.c:336)
+  if (pp.feel_planets && blockIdx.x == 0 && threadIdx.x < k.ctl->np) {
+    // the planet terms of UpdateDustVelocities, evaluated once per substep
+    const fb_ctl *c = k.ctl;
+    const int p = threadIdx.x;
+    const double xp = c->px[p], yp = c->py[p];
+    const double rpl = sqrt(xp * xp + yp * yp);
+    pp.dc->pl_r[p] = rpl;
+    pp.dc->pl_t[p] = atan2(yp, xp);
+    pp.dc->pl_eps[p] = pp.thicksmoothing * pp.aspectratio * pow(0.5 * rpl, 1.0 + pp.flaringindex) *
+                       pow(2.0, 1.0 + pp.flaringindex);
+  }
   if (q >= pp.n) return;
   const double timestep = 2.0 * k.ctl->dt;
   const double rinf0 = k.rinf[0], rsupl = k.rsup[k.nr - 1];
@@ -291,10 +336,11 @@ static __device__ __forceinline__ void record_stopping_time(const PP &pp, double
 // mode 0: one substep (kick, interpolation, UpdateDustVelocities, and the
 // second interpolation of SourceEuler.c:529-530 when WRITEDUSTDENSITY);
 // mode 1: the interpolation call of main.c:287 (Stokes numbers only).
-__global__ void __launch_bounds__(D_BS) k_dust_update(KP k, PP pp, int mode)
+__global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
 {
-  const int q = blockIdx.x * D_BS + threadIdx.x;
-  if (q >= pp.n) return;
+  const int t = blockIdx.x * D_BS + threadIdx.x;
+  if (t >= pp.n) return;
+  const int q = pp.perm[t];
   const int ns = k.ns, nr = k.nr;
   const double rinf0 = k.rinf[0], rsupl = k.rsup[nr - 1];
   double r = pp.r[q], th = pp.th[q];
@@ -304,11 +350,8 @@ __global__ void __launch_bounds__(D_BS) k_dust_update(KP k, PP pp, int mode)
     const double St = pp.st[q];
     const double visc = viscosity_at(k, r);
     const double D_dust = visc * (1.0 + 4.0 * (St * St)) * pow(1. + St * St, -2.0);
-    int ip = 0;
-    if (r >= k.rinf[ip]) {
-      while ((r >= k.rinf[ip]) && (ip <= nr - 1)) ip++;
-    }
-    ip--;
+    // `while (r >= Rinf[ip] && ip <= nr-1) ip++; ip--` (r >= Rinf[0] here)
+    const int ip = first_above(k.rinf, nr, r) - 1;
     int jp = (int)floor(ns * (th - pp.aziinf0) / (pp.azisupl - pp.aziinf0));
     if (jp == ns) jp = 0;
     jp = min(max(jp, 0), ns - 1);
@@ -345,9 +388,8 @@ __global__ void __launch_bounds__(D_BS) k_dust_update(KP k, PP pp, int mode)
   if (!((r >= rinf0) && (r < rsupl))) return;
   // ---- 1) cell of the particle (Dsys.c:363-372)
   const double rp = r, tp = th;
-  int ip = 0;
-  while (rp >= k.rinf[ip]) ip++;
-  ip--;
+  // `while (rp >= Rinf[ip]) ip++; ip--` with Rinf[0] <= rp < Rinf[nr]
+  const int ip = first_above(k.rinf, nr + 1, rp) - 1;
   int jp = (int)floor(ns * (tp - pp.aziinf0) / (pp.azisupl - pp.aziinf0));
   if (jp == ns) jp = 0;
   jp = min(max(jp, 0), ns - 1);
@@ -356,65 +398,86 @@ __global__ void __launch_bounds__(D_BS) k_dust_update(KP k, PP pp, int mode)
   double vrg = 0.0, rgp = 0.0, rind = 0.0, rsg = 0.0;
   double vtg = 0.0, agp = 0.0, aind = 0.0, asg = 0.0;
   double densg = 0.0, csg = 0.0;
+  // The stencils' weights: radial ones at Rinf (2a) and Rmed (2b, 2c),
+  // azimuthal ones at the cell centres (2a, 2c) and interfaces (2b); each
+  // is computed once and reused, as the same values enter the sums.
+  double wr_inf[3], wr_med[3], wt_c[3], wt_i[3];
+  int jc[3], ji[3];
+#pragma unroll
+  for (int t = 0; t < 3; t++) {
+    const int i = ip - 1 + t;
+    if (i >= 0 && i <= nr - 1) {
+      wr_inf[t] = tsc_weight(pp.log_grid ? fabs(log(rp / k.rinf[i])) : fabs(rp - k.rinf[i]), delta_r);
+      wr_med[t] = tsc_weight(pp.log_grid ? fabs(log(rp / k.rmed[i])) : fabs(rp - k.rmed[i]), delta_r);
+    } else {
+      wr_inf[t] = wr_med[t] = 0.0;
+    }
+    const int j = jp - 1 + t;
+    double az;
+    if (j >= 0 && j < ns) { jc[t] = j; az = pp.azimuth[j]; }
+    else if (j < 0) { jc[t] = j + ns; az = pp.azimuth[0] + j * delta_phi; }
+    else { jc[t] = j - ns; az = pp.azimuth[ns - 1] + (j + 1 - ns) * delta_phi; }
+    wt_c[t] = tsc_weight(fabs(tp - az), delta_phi);
+  }
+  {
+    const int myjp = (tp > pp.azimuth[jp]) ? jp + 1 : jp;
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+      const int j = myjp - 1 + t;
+      double az;
+      if (j >= 0 && j < ns) { ji[t] = j; az = pp.aziinf[j]; }
+      else if (j < 0) { ji[t] = j + ns; az = pp.aziinf[0] + j * delta_phi; }
+      else { ji[t] = j - ns; az = pp.aziinf[ns - 1] + (j + 1 - ns) * delta_phi; }
+      wt_i[t] = tsc_weight(fabs(tp - az), delta_phi);
+    }
+  }
   // ---- 2a) vrad-staggered values: (Rinf[i], Azimuth[j]) (Dsys.c:397-487)
-  for (int j = jp - 1; j <= jp + 1; j++) {
-    int myj;
-    double myaz;
-    if (j >= 0 && j < ns) { myj = j; myaz = pp.azimuth[j]; }
-    else if (j < 0) { myj = j + ns; myaz = pp.azimuth[0] + j * delta_phi; }
-    else { myj = j - ns; myaz = pp.azimuth[ns - 1] + (j + 1 - ns) * delta_phi; }
-    const double wt = tsc_weight(fabs(tp - myaz), delta_phi);
-    for (int i = ip - 1; i <= ip + 1; i++) {
+#pragma unroll
+  for (int tj = 0; tj < 3; tj++) {
+    const double wt = wt_c[tj];
+#pragma unroll
+    for (int ti = 0; ti < 3; ti++) {
+      const int i = ip - 1 + ti;
       if (i < 0 || i > nr - 1) continue;
-      const double dr = pp.log_grid ? fabs(log(rp / k.rinf[i])) : fabs(rp - k.rinf[i]);
-      const double wr = tsc_weight(dr, delta_r);
-      const size_t l = (size_t)i * ns + myj;
+      const double wr = wr_inf[ti];
+      const size_t l = (size_t)i * ns + jc[tj];
       vrg += (wr * wt * k.vr[l]);
       rgp += (wr * wt * k.rgp[l]);
       if (k.indirect_term) rind += (wr * wt * k.rind[l]);
       if (want_sg) rsg += (wr * wt * k.rsga[l]);
     }
   }
-  // ---- 2b) vtheta-staggered values: (Rmed[i], AziInf[j]) (Dsys.c:510-588)
-  {
-    const int myjp = (tp > pp.azimuth[jp]) ? jp + 1 : jp;
-    for (int j = myjp - 1; j <= myjp + 1; j++) {
-      int myj;
-      double myaz;
-      if (j >= 0 && j < ns) { myj = j; myaz = pp.aziinf[j]; }
-      else if (j < 0) { myj = j + ns; myaz = pp.aziinf[0] + j * delta_phi; }
-      else { myj = j - ns; myaz = pp.aziinf[ns - 1] + (j + 1 - ns) * delta_phi; }
-      const double wt = tsc_weight(fabs(tp - myaz), delta_phi);
-      for (int i = ip - 1; i <= ip + 1; i++) {
-        if (i < 0 || i > nr - 1) continue;
-        const double dr = pp.log_grid ? fabs(log(rp / k.rmed[i])) : fabs(rp - k.rmed[i]);
-        const double wr = tsc_weight(dr, delta_r);
-        const size_t l = (size_t)i * ns + myj;
-        // the reference adds Rmed*OmegaFrame to vtheta around the call; the
-        // supported frame is non-rotating (OmegaFrame = 0)
-        vtg += (wr * wt * k.vt[l]);
-        agp += (wr * wt * k.agp[l]);
-        if (k.indirect_term) aind += (wr * wt * k.aind[l]);
-        if (want_sg) asg += (wr * wt * k.asga[l]);
-      }
+  // ---- 2b) vtheta-staggered values: (Rmed[i], AziInf[j]) (Dsys.c:510-588);
+  // the reference adds Rmed*OmegaFrame to vtheta around the call, and the
+  // supported frame is non-rotating (OmegaFrame = 0)
+#pragma unroll
+  for (int tj = 0; tj < 3; tj++) {
+    const double wt = wt_i[tj];
+#pragma unroll
+    for (int ti = 0; ti < 3; ti++) {
+      const int i = ip - 1 + ti;
+      if (i < 0 || i > nr - 1) continue;
+      const double wr = wr_med[ti];
+      const size_t l = (size_t)i * ns + ji[tj];
+      vtg += (wr * wt * k.vt[l]);
+      agp += (wr * wt * k.agp[l]);
+      if (k.indirect_term) aind += (wr * wt * k.aind[l]);
+      if (want_sg) asg += (wr * wt * k.asga[l]);
     }
   }
   // ---- 2c) cell-centred values: (Rmed[i], Azimuth[j]) (Dsys.c:617-711).
   // The dust deposit of this loop is Particles_Mass times the weights; the
   // particle mass is zero without a dust fluid (main.c:187-200), so there
   // is nothing to deposit.
-  for (int j = jp - 1; j <= jp + 1; j++) {
-    int myj;
-    double myaz;
-    if (j >= 0 && j < ns) { myj = j; myaz = pp.azimuth[j]; }
-    else if (j < 0) { myj = j + ns; myaz = pp.azimuth[0] + j * delta_phi; }
-    else { myj = j - ns; myaz = pp.azimuth[ns - 1] + (j + 1 - ns) * delta_phi; }
-    const double wt = tsc_weight(fabs(tp - myaz), delta_phi);
-    for (int i = ip - 1; i <= ip + 1; i++) {
+#pragma unroll
+  for (int tj = 0; tj < 3; tj++) {
+    const double wt = wt_c[tj];
+#pragma unroll
+    for (int ti = 0; ti < 3; ti++) {
+      const int i = ip - 1 + ti;
       if (i < 0 || i > nr - 1) continue;
-      const double dr = pp.log_grid ? fabs(log(rp / k.rmed[i])) : fabs(rp - k.rmed[i]);
-      const double wr = tsc_weight(dr, delta_r);
-      const size_t l = (size_t)i * ns + myj;
+      const double wr = wr_med[ti];
+      const size_t l = (size_t)i * ns + jc[tj];
       densg += (wr * wt * k.rho[l]);
       csg += (wr * wt * k.cs[l]);
     }
@@ -432,7 +495,8 @@ __global__ void __launch_bounds__(D_BS) k_dust_update(KP k, PP pp, int mode)
   const double rd = rp, td = tp;
   int LocalDustFeelDisk = pp.feel_disk;
   if ((rd < pp.rmin) || (rd > pp.rmax)) LocalDustFeelDisk = 0;
-  const double stoptime = St * pow(rd, 1.5);
+  const double rp15 = pow(rd, 1.5);
+  const double stoptime = St * rp15;
   double vr_new, vth_new;
   if ((stoptime < dt) && pp.sfta) {
     // short-friction-time approximation
@@ -447,16 +511,14 @@ __global__ void __launch_bounds__(D_BS) k_dust_update(KP k, PP pp, int mode)
       FgravR = -vtd * vtd / rd;
     if (pp.feel_planets) {
       const fb_ctl *c = k.ctl;
+      const fb_dust_ctl *dc = pp.dc;  // radius, azimuth, smoothing from k_dust_drift
       for (int p = 0; p < c->np; p++) {
-        const double xp = c->px[p], yp = c->py[p];
-        const double rpl = sqrt(xp * xp + yp * yp);
-        const double tpl = atan2(yp, xp);
+        const double rpl = dc->pl_r[p], tpl = dc->pl_t[p], eps = dc->pl_eps[p];
         const double mp = c->pm[p];
-        const double eps = pp.thicksmoothing * pp.aspectratio * pow(0.5 * rpl, 1.0 + pp.flaringindex) *
-                           pow(2.0, 1.0 + pp.flaringindex);
-        const double d = sqrt(rd * rd + rpl * rpl - 2.0 * rd * rpl * cos(td - tpl) + eps * eps);
-        FgravR += mp * (rpl * cos(td - tpl) - rd) * pow(d, -3.0);
-        FgravTh += -mp * rpl * sin(td - tpl) * pow(d, -3.0);
+        const double cdt = cos(td - tpl), d = sqrt(rd * rd + rpl * rpl - 2.0 * rd * rpl * cdt + eps * eps);
+        const double d3 = pow(d, -3.0);
+        FgravR += mp * (rpl * cdt - rd) * d3;
+        FgravTh += -mp * rpl * sin(td - tpl) * d3;
       }
     }
     if (k.indirect_term) {
@@ -479,7 +541,7 @@ __global__ void __launch_bounds__(D_BS) k_dust_update(KP k, PP pp, int mode)
   // updated velocities; the next substep's kick uses that one
   const double St_out = pp.restokes ? stokes_number(pp, size, rp, vr_new, vth_new, vrg, vtg, csg, densg) : St;
   pp.st[q] = St_out;
-  record_stopping_time(pp, pp.restokes ? St_out * pow(rp, 1.5) : stoptime);
+  record_stopping_time(pp, pp.restokes ? St_out * rp15 : stoptime);
 }
 
 // ----------------------------------------------------- 5. bookkeeping
@@ -500,6 +562,55 @@ __global__ void k_dust_finish(PP pp)
   d->kicks = G + K;
   d->K = 0;
   d->npairs = 0;
+}
+
+// ------------------------------------------------------ 6. cell sort
+// Counting sort of the particles by cell (once per DT): key = ip*ns + jp of
+// the particles on the grid, nr*ns for the others.
+__global__ void __launch_bounds__(D_BS) k_cell_key(KP k, PP pp)
+{
+  const int q = blockIdx.x * D_BS + threadIdx.x;
+  if (q >= pp.n) return;
+  const double r = pp.r[q], th = pp.th[q];
+  const int nr = k.nr, ns = k.ns;
+  int key = nr * ns;
+  if (r >= k.rinf[0] && r < k.rsup[nr - 1]) {
+    const int ip = first_above(k.rinf, nr + 1, r) - 1;
+    int jp = (int)floor(ns * (th - pp.aziinf0) / (pp.azisupl - pp.aziinf0));
+    jp = min(max(jp, 0), ns - 1);
+    key = ip * ns + jp;
+  }
+  pp.key[q] = key;
+  atomicAdd(pp.cell_count + key, 1);
+}
+
+// exclusive block offsets -> global offsets
+__global__ void __launch_bounds__(SCAN_BS) k_scan_add(int *v, const int *bsum, int n)
+{
+  const int g = blockIdx.x * SCAN_BS + threadIdx.x;
+  if (g < n) v[g] += bsum[blockIdx.x];
+}
+
+__global__ void __launch_bounds__(SCAN_BS) k_scan_top_only(int *blocksum, int nb) { scan_top(blocksum, nb); }
+
+__global__ void __launch_bounds__(D_BS) k_cell_scatter(PP pp)
+{
+  const int q = blockIdx.x * D_BS + threadIdx.x;
+  if (q >= pp.n) return;
+  const int pos = atomicAdd(pp.cell_count + pp.key[q], 1);  // the offsets, consumed as cursors
+  pp.perm[pos] = q;
+}
+
+int fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s)
+{
+  const int nb = (pp.n + D_BS - 1) / D_BS, nc = pp.ncells, ncb = (nc + SCAN_BS - 1) / SCAN_BS;
+  cudaMemsetAsync(pp.cell_count, 0, (size_t)nc * sizeof(int), s);
+  k_cell_key<<<nb, D_BS, 0, s>>>(k, pp);
+  k_scan_block<<<ncb, SCAN_BS, 0, s>>>(pp.cell_count, pp.cell_count, pp.cell_bsum, nc);
+  k_scan_top_only<<<1, SCAN_BS, 0, s>>>(pp.cell_bsum, ncb);
+  k_scan_add<<<ncb, SCAN_BS, 0, s>>>(pp.cell_count, pp.cell_bsum, nc);
+  k_cell_scatter<<<nb, D_BS, 0, s>>>(pp);
+  return 5;
 }
 
 // ---------------------------------------------------------- launchers

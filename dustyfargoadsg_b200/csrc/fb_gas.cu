@@ -925,13 +925,14 @@ static __device__ __forceinline__ int wrapj(int j, int ns) { return j < 0 ? j + 
 // warps busy.  Per pass and quantity the face values go through two
 // shared-memory stages: W = q/(RhoInt+1e-20) for the own cells, then the van
 // Leer slope DQ of the own cells; each thread then forms the upwind values at
-// both faces of its cells and updates them.  W and DQ are double-buffered
-// across quantities, so a quantity costs two barriers.  The arithmetic is
-// the reference's, term for term (ComputeStarTheta :392-433, VanLeerTheta
+// both faces of its cells and updates them (three barriers per quantity).
+// The density slopes of RhoStar share the DQ ring.  The arithmetic is the
+// reference's, term for term (ComputeStarTheta :392-433, VanLeerTheta
 // :435-465); only the work split differs.
 //
-// shared memory: NQ rings of quantities, the residual velocity, W[2], DQ[2]
-#define FB_AZI_RINGS(NQ) ((NQ) + 5)
+// shared memory: NQ rings of quantities, the residual velocity, W, DQ --
+// 110.6 KB for six quantities of 1536 cells, so that two CTAs share an SM
+#define FB_AZI_RINGS(NQ) ((NQ) + 3)
 template <int E> struct AziMaxThreads { static const int value = (E <= 2) ? 1024 : 768; };
 template <int NQ, int E>
 __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal(KP k, double dtov)
@@ -943,7 +944,9 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
   const size_t base = (size_t)i * ns;
   double *Q = smem;              // NQ rings
   double *vres = Q + NQ * ns;    // residual azimuthal velocity
-  double *DR = vres + 4 * ns;    // density slopes: the second DQ buffer
+  double *W = vres + ns;         // q / RhoInt
+  double *D = vres + 2 * ns;     // van Leer slopes of W
+  double *DR = D;                // density slopes (RhoStar), read before D is rewritten
   for (int j = tid; j < ns; j += T)
     for (int q = 0; q < NQ; q++) Q[q * ns + j] = k.q[q][base + j];
   // ComputeThetaElongations / ComputeAverageThetaVelocities / ComputeResiduals
@@ -1006,8 +1009,8 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
     }
     for (int q = 0; q < NQ; q++) {
       double *qb = Q + q * ns;
-      double *W = vres + (1 + (q & 1)) * ns, *D = vres + (3 + (q & 1)) * ns;
       double q0[E];
+      if (q > 0) __syncthreads();  // every read of the previous W and DQ done
 #pragma unroll
       for (int e = 0; e < E; e++) {
         const int j = jc(e);
@@ -1016,7 +1019,7 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
           W[j] = q0[e] / (R[e] + 1e-20);
         }
       }
-      __syncthreads();  // W complete (and, for q = 1, every read of DR done)
+      __syncthreads();  // W complete (and, for q = 0, every read of DR done)
 #pragma unroll
       for (int e = 0; e < E; e++) {
         const int j = jc(e);
@@ -1043,14 +1046,17 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
     }
   }
   __syncthreads();
-  // AdvectSHIFT (TransportEuler.c:350-373) for every quantity
+  // AdvectSHIFT (TransportEuler.c:350-373) for every quantity: cell j takes
+  // cell (j - nshift) mod ns
+  int shift = (int)(nshift % ns);
+  if (shift < 0) shift += ns;
   for (int q = 0; q < NQ; q++) {
     double *qb = Q + q * ns;
     double tmp[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
       const int j = jc(e);
-      long ji = ((long)j - nshift) % ns;
+      int ji = j - shift;
       if (ji < 0) ji += ns;
       tmp[e] = (j < ns) ? qb[ji] : 0.0;
     }
@@ -1392,6 +1398,9 @@ int fb_gas_prepare(int ns, int energy)
   for (const void *f : fns) {
     int rc = fb_allow_max_dynamic_smem(f);
     if (rc) return rc;
+    // the whole unified L1 as shared memory: two rings' CTAs per SM where they fit
+    if (cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess)
+      return FB_ERR_CUDA;
   }
   return FB_OK;
 }
