@@ -27,6 +27,8 @@ struct fb_ctx {
   size_t nf;
   cudaStream_t st;
   cudaEvent_t ev0, ev1;
+  cudaStream_t st_planets;            // branch of the planets' step (k_planets)
+  cudaEvent_t ev_fork, ev_planets;    // its start and end within a substep
   KP k;
   std::vector<void *> allocs;
   fb_ctl *d_ctl;
@@ -248,6 +250,12 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return FB_ERR_CUDA; }
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
+  if (cudaStreamCreateWithFlags(&ctx->st_planets, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_planets, cudaEventDisableTiming) != cudaSuccess) {
+    fb_destroy(ctx);
+    return FB_ERR_CUDA;
+  }
   const int nr = ctx->nr, ns = ctx->ns;
   const size_t nf = ctx->nf;
   KP &k = ctx->k;
@@ -428,6 +436,9 @@ extern "C" int fb_destroy(fb_ctx *ctx)
   if (ctx->h_diag) cudaFreeHost(ctx->h_diag);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
   if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+  if (ctx->ev_planets) cudaEventDestroy(ctx->ev_planets);
+  if (ctx->st_planets) cudaStreamDestroy(ctx->st_planets);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->gdt_exec) cudaGraphExecDestroy(ctx->gdt_exec);
   if (ctx->gdt) cudaGraphDestroy(ctx->gdt);
@@ -534,9 +545,19 @@ static int enqueue_substep(fb_ctx *ctx)
   cudaStream_t s = ctx->st;
   int npt = 0;
   STAGE(ST_CFL, 1, fb_launch_cfl(k, s));  // ConditionCFL + the controller (last CTA)
+  // the planets' step on a branch of its own: no gas kernel of the substep
+  // reads the positions it writes; joined before the particles' velocity
+  // update, else at the end of the substep
+  cudaEventRecord(ctx->ev_fork, s);
+  cudaStreamWaitEvent(ctx->st_planets, ctx->ev_fork, 0);
+  fb_launch_planets(k, ctx->has_dust ? &ctx->pp : NULL, ctx->st_planets);
+  cudaEventRecord(ctx->ev_planets, ctx->st_planets);
+  ctx->launches += 1;
+  ctx->pcount[ST_CFL] += 1;
   // particles after the planets' RK5 step and before the gas update
   // (SourceEuler.c:504-531)
-  if (ctx->has_dust) STAGE(ST_DUST, fb_dust_launches(ctx->pp), fb_launch_dust_substep(k, ctx->pp, s));
+  if (ctx->has_dust)
+    STAGE(ST_DUST, fb_dust_launches(ctx->pp), fb_launch_dust_substep(k, ctx->pp, s, ctx->ev_planets));
   if (k.energy) STAGE(ST_SOUND, 1, fb_launch_soundspeed(k, k.visc_mode == 1, s));
   STAGE(ST_POT, 1, fb_launch_potential(k, s));
   STAGE(ST_SUB1, 1, fb_launch_substep1(k, s));
@@ -562,6 +583,7 @@ static int enqueue_substep(fb_ctx *ctx)
   STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s));
   STAGE(ST_TVR, 2, fb_launch_transport_vr(k, s));
   if (k.evanescent && k.n_damp_rings > 0) STAGE(ST_DAMP, 1, fb_launch_damping(k, 0.0, s));
+  if (!ctx->has_dust) cudaStreamWaitEvent(s, ctx->ev_planets, 0);
   if (ctx->profiling) {
     cudaEventRecord(ctx->pev[npt], s);
     ctx->pseq[npt] = -1;
@@ -967,6 +989,8 @@ struct fb_batch {
   std::vector<long long> per_substep;
   cudaStream_t st;
   cudaEvent_t ev0, ev1;
+  cudaStream_t st_planets;            // branch of the planets' step (k_planets)
+  cudaEvent_t ev_fork, ev_planets;    // its start and end within a substep
   cudaGraph_t g;
   cudaGraphExec_t ge;
 };

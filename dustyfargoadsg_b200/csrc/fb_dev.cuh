@@ -131,6 +131,7 @@ struct PP {
 
 // launchers (fb_gas.cu)
 void fb_launch_cfl(const KP &k, cudaStream_t s);
+void fb_launch_planets(const KP &k, const PP *pp, cudaStream_t s);
 void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s);
 void fb_launch_potential(const KP &k, cudaStream_t s);
 void fb_launch_substep1(const KP &k, cudaStream_t s);
@@ -172,7 +173,7 @@ void fb_ctx_count_launches(fb_ctx *ctx, int n);
 void fb_launch_vortensity(const KP &k, double *xi, cudaStream_t s);
 void fb_launch_ring_mean(const double *f, int nr, int ns, double *out, cudaStream_t s);
 // Lagrangian particles (fb_dust.cu)
-void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s);
+void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s, cudaEvent_t planets_done);
 void fb_launch_dust_interpolation_only(const KP &k, const PP &pp, cudaStream_t s);
 int  fb_dust_launches(const PP &pp);
 int  fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s);  // returns launches

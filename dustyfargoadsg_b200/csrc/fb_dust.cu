@@ -145,17 +145,6 @@ __global__ void __launch_bounds__(D_BS) k_dust_drift(KP k, PP pp)
 {
   const int q = blockIdx.x * D_BS + threadIdx.x;
   if (q == 0) pp.dc->min_ts = 1e6;  // reset by every interpolation call (Dsys.c:336)
-  if (pp.feel_planets && blockIdx.x == 0 && threadIdx.x < k.ctl->np) {
-    // the planet terms of UpdateDustVelocities, evaluated once per substep
-    const fb_ctl *c = k.ctl;
-    const int p = threadIdx.x;
-    const double xp = c->px[p], yp = c->py[p];
-    const double rpl = sqrt(xp * xp + yp * yp);
-    pp.dc->pl_r[p] = rpl;
-    pp.dc->pl_t[p] = atan2(yp, xp);
-    pp.dc->pl_eps[p] = pp.thicksmoothing * pp.aspectratio * pow(0.5 * rpl, 1.0 + pp.flaringindex) *
-                       pow(2.0, 1.0 + pp.flaringindex);
-  }
   if (q >= pp.n) return;
   const double timestep = 2.0 * k.ctl->dt;
   const double rinf0 = k.rinf[0], rsupl = k.rsup[k.nr - 1];
@@ -511,7 +500,7 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
       FgravR = -vtd * vtd / rd;
     if (pp.feel_planets) {
       const fb_ctl *c = k.ctl;
-      const fb_dust_ctl *dc = pp.dc;  // radius, azimuth, smoothing from k_dust_drift
+      const fb_dust_ctl *dc = pp.dc;  // radius, azimuth, smoothing from k_planets
       for (int p = 0; p < c->np; p++) {
         const double rpl = dc->pl_r[p], tpl = dc->pl_t[p], eps = dc->pl_eps[p];
         const double mp = c->pm[p];
@@ -616,7 +605,7 @@ int fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s)
 // ---------------------------------------------------------- launchers
 int fb_dust_launches(const PP &pp) { return pp.feel_turb ? 8 : 2; }
 
-void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s)
+void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s, cudaEvent_t planets_done)
 {
   const int nb = (pp.n + D_BS - 1) / D_BS;
   k_dust_drift<<<nb, D_BS, 0, s>>>(k, pp);
@@ -629,6 +618,7 @@ void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s)
     k_rng_top<<<1, SCAN_BS, 0, s>>>(k, pp, ncb);
     k_rng_scatter<<<ncb, D_BS, 0, s>>>(pp);
   }
+  if (planets_done) cudaStreamWaitEvent(s, planets_done, 0);  // positions after the planets' step
   k_dust_update<<<nb, D_BS, 0, s>>>(k, pp, 0);
   if (pp.feel_turb) k_dust_finish<<<1, 1, 0, s>>>(pp);
 }

@@ -14,6 +14,7 @@
 
 #define FB_BS 256
 #define FB_BS2 256  // most threads per CTA of the per-cell kernels (k.cell_bs <= FB_BS2)
+#define RING_U 6    // cells per thread and batch of k_soundspeed
 
 // per-cell kernels: blockIdx.y = ring, 128 consecutive azimuths per CTA
 // per-cell kernels: CTAs of k.cell_bs azimuths (a ring segment) times rings
@@ -78,81 +79,167 @@ static __device__ __forceinline__ double nu_ring(const KP &k, int i)
   return 0.0;
 }
 
-static __device__ void cfl_ring_limit(const KP &k, int i, double vmoy, double *sh);
+// Sums of NV values over a CTA of any multiple of 32 threads (<= 1024);
+// every thread gets the totals.  sh holds NV * 32 doubles.
+template <int NV>
+static __device__ void block_sums(double (&v)[NV], double *sh)
+{
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; q++)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_down_sync(0xffffffffu, v[q], o);
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < NV; q++) sh[q * 32 + w] = v[q];
+  __syncthreads();
+  if (w == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      double x = (lane < nw) ? sh[q * 32 + lane] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) sh[q * 32] = x;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int q = 0; q < NV; q++) v[q] = sh[q * 32];
+  __syncthreads();
+}
+
+static __device__ double block_min_dyn(double v, double *sh)
+{
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double u = __shfl_down_sync(0xffffffffu, v, o);
+    v = (u < v) ? u : v;
+  }
+  __syncthreads();
+  if (lane == 0) sh[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = (lane < nw) ? sh[lane] : 1e300;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double u = __shfl_down_sync(0xffffffffu, v, o);
+      v = (u < v) ? u : v;
+    }
+    if (lane == 0) sh[0] = v;
+  }
+  __syncthreads();
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
 static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c);
+static __device__ void planet_prelude(const KP &k, fb_ctl *c);
+static __device__ void rk5(const double *q0, double dt, const double *masses, double *q1, int n,
+                           const int *feelothers, int indirect);
 
 // ---------------------------------------------------------------- CFL
 // ConditionCFL (SourceEuler.c:1304-1552): one CTA per ring computes the
 // azimuthal mean Vmoy[i] and the smallest per-cell limit of the ring; the
 // controller takes the minimum over rings, adds the shear limit and returns
 // ceil(deltaT/newdt).  DetectCrash (SourceEuler.c:51-69) rides along.
-__global__ void __launch_bounds__(FB_BS) k_cfl(KP k)
+// One CTA per ring, CFL_E cells per thread, one pass over the ring: the
+// cells' values stay in registers between the ring sums (the mean azimuthal
+// velocity the CFL limits need) and the limits themselves.
+#define CFL_E 4
+static inline int cfl_threads(int ns) { return ((ns + CFL_E - 1) / CFL_E + 31) / 32 * 32; }
+__global__ void __launch_bounds__(1024) k_cfl(KP k)
 {
-  __shared__ double sh[32];
-  const int i = blockIdx.x, ns = k.ns;
+  __shared__ double sh[6 * 32];
+  const int i = blockIdx.x, ns = k.ns, T = blockDim.x, tid = threadIdx.x;
   const size_t base = (size_t)i * ns;
-  const double *vt = k.vt + base, *vr = k.vr + base;
-  double s = 0.0;
+  const double *vt = k.vt + base, *vr = k.vr + base, *rho = k.rho + base;
+  const bool cfl = (i >= 1);  // ConditionCFL's rings: One_or_active..Max_or_active-1
+  if (i == 0 && tid == 0) planet_prelude(k, k.ctl);
+  const double rmi = k.rmed[i], surf = k.surf[i], rs = k.indirect_smoothing;
+  // ring sums: vtheta; ComputeForce (Force.c:77-253) for the star (x = y = 0,
+  // mass 0) with rsmoothing = INDIRECTTERMSMOOTHING (SourceEuler.c:482);
+  // GasTotalMass (SideEuler.c:15) and the barycentre sums (SideEuler.c:42-89)
+  double v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  // ConditionCFL's per-cell limits (SourceEuler.c:1390-1485): all but the
+  // residual-velocity one are known before the ring mean; the sum under the
+  // square root is evaluated in the reference's order once it is
+  double vtc[CFL_E], s12[CFL_E], s4[CFL_E];
+  const double dxrad = k.dxrad[i], dxtheta = k.dxtheta_cfl[i];
   int neg = 0, bad = 0;
-  for (int j = threadIdx.x; j < ns; j += FB_BS) {
-    s += vt[j];
-    double d = k.rho[base + j];
-    if (d < 0.0) neg = 1;
-    if (!isfinite(d) || !isfinite(vt[j]) || !isfinite(vr[j])) bad = 1;
+#pragma unroll
+  for (int e = 0; e < CFL_E; e++) {
+    const int j = tid + e * T;
+    if (j >= ns) continue;
+    const double vtj = vt[j], vrj = vr[j], dens = rho[j];
+    v[0] += vtj;
+    if (dens < 0.0) neg = 1;
+    if (!isfinite(dens) || !isfinite(vtj) || !isfinite(vrj)) bad = 1;
     if (k.energy) {
-      double e = k.e[base + j];
-      if (e < 0.0) neg = 1;
-      if (!isfinite(e)) bad = 1;
+      const double en = k.e[base + j];
+      if (en < 0.0) neg = 1;
+      if (!isfinite(en)) bad = 1;
+    }
+    const double xc = rmi * k.cosaz[j];
+    const double yc = rmi * k.sinaz[j];
+    const double cellmass = surf * dens;
+    const double dx = xc - 0.0, dy = yc - 0.0;
+    const double d2 = dx * dx + dy * dy;
+    const double dist2 = d2 + rs * rs;
+    const double distance = sqrt(dist2);
+    const double InvDist3 = 1.0 / dist2 / distance;
+    v[1] += FB_G * cellmass * dx * InvDist3 * 1.0;
+    v[2] += FB_G * cellmass * dy * InvDist3 * 1.0;
+    v[3] += surf * dens;
+    v[4] += surf * dens * xc;
+    v[5] += surf * dens * yc;
+    if (cfl) {
+      const int jp = (j == ns - 1) ? 0 : j + 1;
+      double invdt1 = k.cs[base + j] / (min2(dxrad, dxtheta));
+      double invdt2 = fabs(vrj) / dxrad;
+      double dvr = vr[ns + j] - vrj;
+      double dvt = vt[jp] - vtj;
+      if (dvr >= 0.0) dvr = 1e-10; else dvr = -dvr;
+      if (dvt >= 0.0) dvt = 1e-10; else dvt = -dvt;
+      double invdt4 = max2(dvr / dxrad, dvt / dxtheta);
+      invdt4 *= 4.0 * FB_CVNR * FB_CVNR;
+      vtc[e] = vtj;
+      s12[e] = invdt1 * invdt1 + invdt2 * invdt2;
+      s4[e] = invdt4 * invdt4;
     }
   }
-  s = block_sum<FB_BS>(s, sh);
-  const double vmoy = s / (double)ns;
-  if (threadIdx.x == 0) k.vmoy[i] = vmoy;
-  // ComputeForce (Force.c:77-253) for the star (x = y = 0, mass 0) with
-  // rsmoothing = INDIRECTTERMSMOOTHING (SourceEuler.c:482), GasTotalMass
-  // (SideEuler.c:15) and the barycentre sums (SideEuler.c:42-89): ring
-  // partials, summed by the controller in ring order.
-  {
-    const double rs = k.indirect_smoothing;
-    double fx = 0.0, fy = 0.0, mass = 0.0, xb = 0.0, yb = 0.0;
-    for (int j = threadIdx.x; j < ns; j += FB_BS) {
-      const double xc = k.rmed[i] * k.cosaz[j];
-      const double yc = k.rmed[i] * k.sinaz[j];
-      const double dens = k.rho[base + j];
-      const double cellmass = k.surf[i] * dens;
-      const double dx = xc - 0.0, dy = yc - 0.0;
-      const double d2 = dx * dx + dy * dy;
-      const double dist2 = d2 + rs * rs;
-      const double distance = sqrt(dist2);
-      const double InvDist3 = 1.0 / dist2 / distance;
-      fx += FB_G * cellmass * dx * InvDist3 * 1.0;
-      fy += FB_G * cellmass * dy * InvDist3 * 1.0;
-      mass += k.surf[i] * dens;
-      xb += k.surf[i] * dens * xc;
-      yb += k.surf[i] * dens * yc;
-    }
-    fx = block_sum<FB_BS>(fx, sh);
-    fy = block_sum<FB_BS>(fy, sh);
-    mass = block_sum<FB_BS>(mass, sh);
-    xb = block_sum<FB_BS>(xb, sh);
-    yb = block_sum<FB_BS>(yb, sh);
-    if (threadIdx.x == 0) {
-      double *pp = k.partials + (size_t)i * 5;
-      pp[0] = fx; pp[1] = fy; pp[2] = mass; pp[3] = xb; pp[4] = yb;
-    }
+  block_sums<6>(v, sh);
+  const double vmoy = v[0] / (double)ns;
+  if (tid == 0) {
+    k.vmoy[i] = vmoy;
+    double *pp = k.partials + (size_t)i * 5;  // summed by the controller in ring order
+    for (int q = 0; q < 5; q++) pp[q] = v[1 + q];
   }
   neg = __syncthreads_or(neg);
   bad = __syncthreads_or(bad);
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     if (neg) atomicAdd(&k.ctl->crash_count, 1);
     if (bad) atomicOr(&k.ctl->nonfinite, 1);
   }
-  if (i >= 1) cfl_ring_limit(k, i, vmoy, sh);  // i = One_or_active..Max_or_active-1
+  if (cfl) {
+    const double viscosity = nu_ring(k, i);
+    const double invdt5 = (viscosity != 0.0) ? viscosity * 4.0 / k.mindx2[i] : 1e-10;
+    const double invdt6 = 1e-10;
+    double m = 1e30;
+#pragma unroll
+    for (int e = 0; e < CFL_E; e++) {
+      if (tid + e * T >= ns) continue;
+      double vres = k.fast_transport ? vtc[e] - vmoy : vtc[e];
+      double invdt3 = fabs(vres) / dxtheta;
+      double dt = FB_CFLSECURITY / sqrt(s12[e] + invdt3 * invdt3 + s4[e] + invdt5 * invdt5 + invdt6 * invdt6);
+      if (dt < m) m = dt;
+    }
+    m = block_min_dyn(m, sh);
+    if (tid == 0) k.ringmin[i] = m;
+  }
   // the last CTA to finish runs the controller (no waiting: whoever comes
   // last sees every other ring's results)
   __shared__ int last;
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     __threadfence();
     last = (atomicAdd(&k.ctl->cfl_done, 1u) == gridDim.x - 1) ? 1 : 0;
   }
@@ -162,49 +249,87 @@ __global__ void __launch_bounds__(FB_BS) k_cfl(KP k)
   __shared__ fb_ctl cs;
   unsigned long long *dst = (unsigned long long *)&cs;
   const unsigned long long *src = (const unsigned long long *)k.ctl;
-  for (int w = threadIdx.x; w < (int)(sizeof(fb_ctl) / 8); w += FB_BS) dst[w] = __ldcg(src + w);
+  for (int w = tid; w < (int)(sizeof(fb_ctl) / 8); w += T) dst[w] = __ldcg(src + w);
   __syncthreads();
   controller_body(k, sh, &cs);
   __syncthreads();
-  if (threadIdx.x == 0) cs.cfl_done = 0;
+  if (tid == 0) cs.cfl_done = 0;
   __syncthreads();
   unsigned long long *out = (unsigned long long *)k.ctl;
-  for (int w = threadIdx.x; w < (int)(sizeof(fb_ctl) / 8); w += FB_BS) out[w] = dst[w];
+  for (int w = tid; w < (int)(sizeof(fb_ctl) / 8); w += T) out[w] = dst[w];
 }
 
-// ConditionCFL's per-cell limits of ring i (SourceEuler.c:1390-1485)
-static __device__ void cfl_ring_limit(const KP &k, int i, double vmoy, double *sh)
+void fb_launch_cfl(const KP &k, cudaStream_t s) { k_cfl<<<k.nr, cfl_threads(k.ns), 0, s>>>(k); }
+
+// The planets' step of the substep, after the controller has set dt:
+// AdvanceSystemRK5 (Pframeforce.c:163-266) and RotatePsys (Psys.c:352-372).
+// One thread.  No other kernel of the substep reads the positions before the
+// particles' velocity update, so this kernel runs on a branch of its own
+// beside the gas kernels; with particles it also evaluates the planet terms
+// of UpdateDustVelocities (DustUpdate.c:342-352) at the new positions.
+__global__ void k_planets(KP k, fb_dust_ctl *dc, double thick, double aspect, double flaring)
 {
-  const int ns = k.ns;
-  const size_t base = (size_t)i * ns;
-  const double *vt = k.vt + base, *vr = k.vr + base;
-  const double viscosity = nu_ring(k, i);
-  const double dxrad = k.dxrad[i], dxtheta = k.dxtheta_cfl[i];
-  double m = 1e30;
-  for (int j = threadIdx.x; j < ns; j += FB_BS) {
-    const int jp = (j == ns - 1) ? 0 : j + 1;
-    double vres = k.fast_transport ? vt[j] - vmoy : vt[j];
-    double cs = k.cs[base + j];
-    double invdt1 = cs / (min2(dxrad, dxtheta));
-    double invdt2 = fabs(vr[j]) / dxrad;
-    double invdt3 = fabs(vres) / dxtheta;
-    double dvr = vr[ns + j] - vr[j];
-    double dvt = vt[jp] - vt[j];
-    if (dvr >= 0.0) dvr = 1e-10; else dvr = -dvr;
-    if (dvt >= 0.0) dvt = 1e-10; else dvt = -dvt;
-    double invdt4 = max2(dvr / dxrad, dvt / dxtheta);
-    invdt4 *= 4.0 * FB_CVNR * FB_CVNR;
-    double invdt5 = (viscosity != 0.0) ? viscosity * 4.0 / k.mindx2[i] : 1e-10;
-    double invdt6 = 1e-10;
-    double dt = FB_CFLSECURITY / sqrt(invdt1 * invdt1 + invdt2 * invdt2 + invdt3 * invdt3 +
-                                      invdt4 * invdt4 + invdt5 * invdt5 + invdt6 * invdt6);
-    if (dt < m) m = dt;
+  fb_ctl *c = k.ctl;
+  if (c->status != FB_OK) return;
+  const int np = c->np;
+  const double dt = c->dt;
+  // AdvanceSystemRK5 (Pframeforce.c:163-266)
+  if (!k.forced_circular) {
+    double q0[4 * FB_MAX_PLANETS], q1[4 * FB_MAX_PLANETS], masses[FB_MAX_PLANETS];
+    for (int i = 0; i < np; i++) {
+      q0[i] = c->px[i]; q0[i + np] = c->py[i]; q0[i + 2 * np] = c->pvx[i]; q0[i + 3 * np] = c->pvy[i];
+      masses[i] = c->pm[i];
+    }
+    if (np > 0) rk5(q0, dt, masses, q1, np, c->pfeelothers, k.indirect_term);
+    for (int i = 0; i < np; i++) {
+      c->px[i] = q1[i]; c->py[i] = q1[i + np]; c->pvx[i] = q1[i + 2 * np]; c->pvy[i] = q1[i + 3 * np];
+    }
+  } else {
+    for (int i = 0; i < np; i++) {
+      double x = c->px[i], y = c->py[i];
+      double theta = atan2(y, x);
+      double vx = c->pvx[i], vy = c->pvy[i];
+      double r = sqrt(x * x + y * y);
+      double v = sqrt(vx * vx + vy * vy);
+      double omega = (-y * vx + x * vy) / r / r;
+      double dtheta = omega * dt;
+      c->px[i] = r * cos(theta + dtheta);
+      c->py[i] = r * sin(theta + dtheta);
+      c->pvx[i] = -v * sin(theta + dtheta);
+      c->pvy[i] = v * cos(theta + dtheta);
+    }
   }
-  m = block_min<FB_BS>(m, sh);
-  if (threadIdx.x == 0) k.ringmin[i] = m;
+  // RotatePsys (Psys.c:352-372) with angle OmegaFrame*dt
+  {
+    double angle = c->omega_frame * dt;
+    double sint = sin(angle), cost = cos(angle);
+    for (int i = 0; i < np; i++) {
+      double xt = c->px[i], yt = c->py[i];
+      c->px[i] = xt * cost + yt * sint;
+      c->py[i] = -xt * sint + yt * cost;
+      xt = c->pvx[i]; yt = c->pvy[i];
+      c->pvx[i] = xt * cost + yt * sint;
+      c->pvy[i] = -xt * sint + yt * cost;
+    }
+  }
+  if (dc) {
+    for (int p = 0; p < np; p++) {
+      const double xp = c->px[p], yp = c->py[p];
+      const double rpl = sqrt(xp * xp + yp * yp);
+      dc->pl_r[p] = rpl;
+      dc->pl_t[p] = atan2(yp, xp);
+      dc->pl_eps[p] = thick * aspect * pow(0.5 * rpl, 1.0 + flaring) * pow(2.0, 1.0 + flaring);
+    }
+  }
 }
 
-void fb_launch_cfl(const KP &k, cudaStream_t s) { k_cfl<<<k.nr, FB_BS, 0, s>>>(k); }
+void fb_launch_planets(const KP &k, const PP *pp, cudaStream_t s)
+{
+  if (pp && pp->feel_planets)
+    k_planets<<<1, 1, 0, s>>>(k, pp->dc, pp->thicksmoothing, pp->aspectratio, pp->flaringindex);
+  else
+    k_planets<<<1, 1, 0, s>>>(k, nullptr, 0.0, 0.0, 0.0);
+}
 
 // ------------------------------------------------------------ controller
 static __device__ double dev_aspect_ratio(const KP &k, double rad)
@@ -277,29 +402,14 @@ static __device__ void rk5(const double *q0, double dt, const double *masses, do
 // the last CTA of k_cfl: its threads reduce the per-ring CFL limits, the
 // shear limits and the force partials (fixed tree order), then thread 0 runs
 // the scalar logic on a shared-memory copy of the control block.
-static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
+// The planet terms of the substep that do not depend on its time step:
+// masses (SourceEuler.c:402-418), the n-body limit (SourceEuler.c:421-440)
+// and FillForcesArrays' planet parameters at the current positions
+// (Pframeforce.c:44-90).  Run by one thread of CTA 0 of the CFL kernel while
+// the other CTAs work on their rings; the controller (last CTA) reads them.
+static __device__ void planet_prelude(const KP &k, fb_ctl *c)
 {
-  const int np = c->np, nr = k.nr, tid = threadIdx.x;
-  // ConditionCFL reduction (SourceEuler.c:1336-1497)
-  double m = 1e30;
-  for (int i = 1 + tid; i < nr; i += FB_BS) {
-    double d = __ldcg(k.ringmin + i);
-    if (d < m) m = d;
-  }
-  for (int i = tid; i < nr - 1; i += FB_BS) {
-    double d = (k.pmax - k.pmin) * FB_CFLSECURITY / (double)k.ns /
-               fabs(__ldcg(k.vmoy + i) * k.invrmed[i] - __ldcg(k.vmoy + i + 1) * k.invrmed[i + 1]);
-    if (d < m) m = d;
-  }
-  const double newdt_cells = block_min<FB_BS>(m, sh);
-  double f[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-  for (int b = tid; b < k.n_partial_blocks; b += FB_BS) {
-    const double *p = k.partials + (size_t)b * 5;
-    for (int q = 0; q < 5; q++) f[q] += __ldcg(p + q);
-  }
-  for (int q = 0; q < 5; q++) f[q] = block_sum<FB_BS>(f[q], sh);
-  if (tid != 0) return;
-  // planet masses (SourceEuler.c:402-418)
+  const int np = c->np;
   if (k.masstaper > 1e-2) {
     double mt = (c->physical_time - c->physical_time_initial) / (k.masstaper * 2.0 * M_PI);
     mt = (mt > 1.0 ? 1.0 : pow(sin(mt * M_PI / 2.0), 2.0));
@@ -309,7 +419,6 @@ static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
     for (int p = 0; p < np; p++)
       if (c->pacc[p] < 1e-10) c->pm[p] = c->pfinal[p];
   }
-  // n-body limit (SourceEuler.c:421-440)
   double dtnbody;
   if (np > 1) {
     dtnbody = 1e5;
@@ -324,6 +433,56 @@ static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
   } else {
     dtnbody = 100.0;
   }
+  c->dtnbody = dtnbody;
+  double planetmass_taper = 1.0;
+  if (k.masstaper > 1e-2) {
+    double mt = (c->physical_time - c->physical_time_initial) / (k.masstaper * 2.0 * M_PI);
+    planetmass_taper = (mt > 1.0 ? 1.0 : .5 * (1.0 - cos(M_PI * mt)));
+  }
+  for (int p = 0; p < np; p++) {
+    double xplanet = c->px[p], yplanet = c->py[p];
+    double mplanet = c->pm[p] * planetmass_taper;
+    double PlanetDistance = sqrt(xplanet * xplanet + yplanet * yplanet);
+    double InvPlanetDistance3 = 1.0 / PlanetDistance / PlanetDistance / PlanetDistance;
+    double smoothing;
+    if (k.roche) {
+      double RRoche = PlanetDistance * pow((1.0 / 3.0 * mplanet), 1.0 / 3.0);
+      smoothing = RRoche * k.rochesmoothing;
+    } else {
+      smoothing = k.thicksmoothing * dev_aspect_ratio(k, PlanetDistance) * pow(PlanetDistance, 1.0 + k.flaringindex);
+    }
+    c->pot_m[p] = mplanet;
+    c->pot_x[p] = xplanet;
+    c->pot_y[p] = yplanet;
+    c->pot_smooth2[p] = smoothing * smoothing;
+    c->pot_invd3[p] = InvPlanetDistance3;
+  }
+}
+
+static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
+{
+  const int nr = k.nr, tid = threadIdx.x, T = blockDim.x;
+  // ConditionCFL reduction (SourceEuler.c:1336-1497), the ring partials of
+  // the forces and sums; every load is issued before the reductions
+  double m = 1e30;
+  double f[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int i = tid; i < nr; i += T) {
+    const double rmin = (i >= 1) ? __ldcg(k.ringmin + i) : 1e30;
+    const double v0 = __ldcg(k.vmoy + i);
+    const double v1 = (i < nr - 1) ? __ldcg(k.vmoy + i + 1) : 0.0;
+    const double *p = k.partials + (size_t)i * 5;
+    for (int q = 0; q < 5; q++) f[q] += __ldcg(p + q);
+    if (rmin < m) m = rmin;
+    if (i < nr - 1) {
+      double d = (k.pmax - k.pmin) * FB_CFLSECURITY / (double)k.ns /
+                 fabs(v0 * k.invrmed[i] - v1 * k.invrmed[i + 1]);
+      if (d < m) m = d;
+    }
+  }
+  const double newdt_cells = block_min_dyn(m, sh);
+  block_sums<5>(f, sh);
+  if (tid != 0) return;
+  const double dtnbody = c->dtnbody;  // planet_prelude
   // ConditionCFL reduction (SourceEuler.c:1336-1497) and substep count
   const double deltaT = c->DT - c->dtemp;
   double newdt = newdt_cells;
@@ -343,7 +502,6 @@ static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
   const double dthydro = (c->DT - c->dtemp) / (double)gastimestepcfl;
   const double dt = min2(dthydro, dtnbody);
   c->dthydro = dthydro;
-  c->dtnbody = dtnbody;
   c->dt = dt;
   c->dtemp += dt;
   if (dt < c->mindt) c->mindt = dt;
@@ -360,74 +518,14 @@ static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
   c->disk_acc_alt_y = -(c->bary_y[2] - 2.0 * c->bary_y[1] + c->bary_y[0]) / (dt * dt);
   c->bary_x[0] = c->bary_x[1]; c->bary_x[1] = c->bary_x[2];
   c->bary_y[0] = c->bary_y[1]; c->bary_y[1] = c->bary_y[2];
-  // FillForcesArrays prelude (Pframeforce.c:44-90): indirect term and the
-  // planets' potential parameters at the current positions.
-  double planetmass_taper = 1.0;
-  if (k.masstaper > 1e-2) {
-    double mt = (c->physical_time - c->physical_time_initial) / (k.masstaper * 2.0 * M_PI);
-    planetmass_taper = (mt > 1.0 ? 1.0 : .5 * (1.0 - cos(M_PI * mt)));
-  }
+  // FillForcesArrays prelude (Pframeforce.c:44-90): the indirect term (the
+  // planets' parameters come from planet_prelude)
   c->ind_x = -c->disk_acc_x;
   c->ind_y = -c->disk_acc_y;
   if (k.alt_gas_it) { c->ind_x = -c->disk_acc_alt_x; c->ind_y = -c->disk_acc_alt_y; }
   if (!k.indirect_term) { c->ind_x = 0.0; c->ind_y = 0.0; }
-  for (int p = 0; p < np; p++) {
-    double xplanet = c->px[p], yplanet = c->py[p];
-    double mplanet = c->pm[p] * planetmass_taper;
-    double PlanetDistance = sqrt(xplanet * xplanet + yplanet * yplanet);
-    double InvPlanetDistance3 = 1.0 / PlanetDistance / PlanetDistance / PlanetDistance;
-    double smoothing;
-    if (k.roche) {
-      double RRoche = PlanetDistance * pow((1.0 / 3.0 * mplanet), 1.0 / 3.0);
-      smoothing = RRoche * k.rochesmoothing;
-    } else {
-      smoothing = k.thicksmoothing * dev_aspect_ratio(k, PlanetDistance) * pow(PlanetDistance, 1.0 + k.flaringindex);
-    }
-    c->pot_m[p] = mplanet;
-    c->pot_x[p] = xplanet;
-    c->pot_y[p] = yplanet;
-    c->pot_smooth2[p] = smoothing * smoothing;
-    c->pot_invd3[p] = InvPlanetDistance3;
-  }
-  // AdvanceSystemRK5 (Pframeforce.c:163-266)
-  if (!k.forced_circular) {
-    double q0[4 * FB_MAX_PLANETS], q1[4 * FB_MAX_PLANETS], masses[FB_MAX_PLANETS];
-    for (int i = 0; i < np; i++) {
-      q0[i] = c->px[i]; q0[i + np] = c->py[i]; q0[i + 2 * np] = c->pvx[i]; q0[i + 3 * np] = c->pvy[i];
-      masses[i] = c->pm[i];
-    }
-    if (np > 0) rk5(q0, dt, masses, q1, np, c->pfeelothers, k.indirect_term);
-    for (int i = 0; i < np; i++) {
-      c->px[i] = q1[i]; c->py[i] = q1[i + np]; c->pvx[i] = q1[i + 2 * np]; c->pvy[i] = q1[i + 3 * np];
-    }
-  } else {
-    for (int i = 0; i < np; i++) {
-      double x = c->px[i], y = c->py[i];
-      double theta = atan2(y, x);
-      double vx = c->pvx[i], vy = c->pvy[i];
-      double r = sqrt(x * x + y * y);
-      double v = sqrt(vx * vx + vy * vy);
-      double omega = (-y * vx + x * vy) / r / r;
-      double dtheta = omega * dt;
-      c->px[i] = r * cos(theta + dtheta);
-      c->py[i] = r * sin(theta + dtheta);
-      c->pvx[i] = -v * sin(theta + dtheta);
-      c->pvy[i] = v * cos(theta + dtheta);
-    }
-  }
-  // RotatePsys (Psys.c:352-372) with angle OmegaFrame*dt
-  {
-    double angle = c->omega_frame * dt;
-    double sint = sin(angle), cost = cos(angle);
-    for (int i = 0; i < np; i++) {
-      double xt = c->px[i], yt = c->py[i];
-      c->px[i] = xt * cost + yt * sint;
-      c->py[i] = -xt * sint + yt * cost;
-      xt = c->pvx[i]; yt = c->pvy[i];
-      c->pvx[i] = xt * cost + yt * sint;
-      c->pvy[i] = -xt * sint + yt * cost;
-    }
-  }
+  // AdvanceSystemRK5 and RotatePsys follow in k_planets, which runs beside
+  // the next kernels of the substep
   // LostMass of the previous substep's ring-0 radial mass fluxes
   // (VanLeerRadial's LostByDisk, TransportEuler.c:213-216).
   c->physical_time += dt;  // SourceEuler.c:714 (no kernel in this substep reads it)
@@ -446,11 +544,25 @@ __global__ void __launch_bounds__(FB_BS) k_soundspeed(KP k, int update_gcs)
   const int i = blockIdx.x, ns = k.ns;
   const size_t base = (size_t)i * ns;
   double s = 0.0;
-  for (int j = threadIdx.x; j < ns; j += FB_BS) {
-    const size_t l = base + j;
-    double c = sqrt(k.gamma * (k.gamma - 1.0) * k.e[l] / k.rho[l]);
-    k.cs[l] = c;
-    s += c;
+  for (int j0 = threadIdx.x; j0 < ns; j0 += RING_U * FB_BS) {
+    double ev[RING_U], dv[RING_U];
+#pragma unroll
+    for (int u = 0; u < RING_U; u++) {
+      const int j = j0 + u * FB_BS;
+      if (j < ns) {
+        ev[u] = k.e[base + j];
+        dv[u] = k.rho[base + j];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RING_U; u++) {
+      const int j = j0 + u * FB_BS;
+      if (j < ns) {
+        double c = sqrt(k.gamma * (k.gamma - 1.0) * ev[u] / dv[u]);
+        k.cs[base + j] = c;
+        s += c;
+      }
+    }
   }
   if (update_gcs) {
     s = block_sum<FB_BS>(s, sh);
