@@ -53,7 +53,7 @@ DEFAULT_WORKLOAD = "adiabatic_sg_512x1536"
 FALLBACK_HBM_GBS = 6650.0
 
 # Algorithmic bytes per cell of each stage (distinct fields read + written,
-# 8 B each), isothermal / with energy equation.  See DESIGN.md.
+# 8 B each), isothermal / with energy equation.
 STAGE_BYTES = {
     "cfl_forces": (32, 40), "potential": (8, 8), "soundspeed": (0, 24),
     "substep1": (64, 64), "viscous_terms": (56, 56), "viscous_update": (64, 64),

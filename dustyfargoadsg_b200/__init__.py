@@ -4,7 +4,7 @@ single NVIDIA B200, behind the C ABI of include/fargo_b200.h.
 Python here is a thin binding over libfargo_b200.so for tests, benchmarks and
 scripting; the step itself runs in the library's CUDA kernels.  The C host
 (dustyfargoadsg_b200/host) and the reference's own main (through the AlgoGas
-drop-in) use the same library.
+drop-in of host/algogas_dropin.c) use the same library.
 """
 import ctypes as C
 import os

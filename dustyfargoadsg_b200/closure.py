@@ -15,7 +15,7 @@ module drives them:
   weighted squared error of the correction the network's face fluxes imply;
 * the corrected solver (`run_coarse`): after every DT of the plain coarse
   method, one correction by the network (fb_closure_apply);
-* the judge (`evaluate`): azimuthally averaged surface density and vortensity
+* the evaluation (`evaluate`): azimuthally averaged surface density and vortensity
   of the corrected coarse run, the plain coarse run and the coarse-grained
   plain fine run (the reference); the corrected run is accepted only when
   both errors are within 1%, otherwise the fine method is the answer.
@@ -259,7 +259,7 @@ def evaluate(net, draw, workdir, tag, coarse_nr, factor, ndt, seed=0, gains=(1.0
 
 
 def main(argv=None):
-    ap = argparse.ArgumentParser(description="train and judge the learned closure")
+    ap = argparse.ArgumentParser(description="train and evaluate the learned closure")
     ap.add_argument("--coarse-nr", type=int, default=128)
     ap.add_argument("--factor", type=int, default=4)
     ap.add_argument("--train-discs", type=int, default=8)

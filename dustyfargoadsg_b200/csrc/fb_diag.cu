@@ -1,6 +1,6 @@
 // fb_diag.cu -- disc diagnostics with no counterpart in the reference (it has
 // no vortensity routine): vortensity on the staggered grid and azimuthal
-// means, used to judge coarse runs against fine ones.
+// means, used to compare coarse runs with fine ones.
 //
 // Vortensity at the cell corner (R_inf[i], phi_inf[j]), i = 1 .. nr-1, where
 // vtheta (at R_med, phi_inf) and vrad (at R_inf, phi_med) are both one

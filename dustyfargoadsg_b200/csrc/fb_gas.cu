@@ -6,8 +6,9 @@
 // is fused into an add), citing the reference file:line.  Ring reductions
 // (azimuthal means) use a fixed tree order inside one CTA: deterministic,
 // but rounded differently from the reference's sequential sums (~1e-16
-// relative).  All of these kernels are bound by memory traffic; their
-// algorithmic bytes per cell are listed in DESIGN.md.
+// relative).  Their algorithmic traffic is a few fields of 8 B per cell;
+// the transport passes carry enough FP64 work per cell (IEEE divisions in
+// every van Leer slope) that instruction issue, not HBM, bounds them.
 #include <cuda_runtime.h>
 #include <math.h>
 #include "fb_dev.cuh"

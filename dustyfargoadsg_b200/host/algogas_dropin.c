@@ -4,7 +4,7 @@
  * A maintainer links this file into the reference build and either names
  * the function AlgoGas (removing SourceEuler.c's), or keeps both and links
  * with -Wl,--wrap=AlgoGas and a one-line __wrap_AlgoGas that calls
- * fb_dropin_AlgoGas (INTEGRATION.md).  The signature is the reference's
+ * fb_dropin_AlgoGas.  The signature is the reference's
  * (src/SourceEuler.c:326-331, src/proto.h:82).  It is compiled against the
  * reference's headers (mp.h and the generated param.h / global_ex.h), so the
  * .par globals are read directly.

@@ -2,7 +2,7 @@
 oracle/_ref/fargo_oracle) and read its full-precision dumps.
 
 TEST INFRASTRUCTURE ONLY -- imported by tests/, bench.py's CPU baseline and
-__graft_entry__.smoke() as the checker, never by the product path.
+__graft_entry__.smoke() to check results, never by the product path.
 """
 import json
 import os

@@ -1,5 +1,5 @@
 """Float64 numpy restatement of the learned closure (test infrastructure: the
-checker of the GPU kernels in dustyfargoadsg_b200/csrc/fb_closure.cu).
+test reference of the GPU kernels in dustyfargoadsg_b200/csrc/fb_closure.cu).
 
 Network: 4 layers of 3x3 convolutions on NHWC arrays [sample][ring][azimuth]
 [channel], periodic in azimuth, zero-padded in radius; channels 16 -> 32 ->
