@@ -33,16 +33,24 @@ struct fb_fft_plan {
   double2 *tw;  // device: exp(-2 pi i t / n), t < n
 };
 
+struct FftArgs {
+  int n, nst;
+  int radix[SG_MAXST];
+  const double2 *tw;
+};
+
 struct fb_sg {
   int nr, ns, m, nk;        // m = 2 nr, nk = ns/2 + 1
   fb_fft_plan prow, pcol;
+  int p2;                   // m = 2^p, p >= 4: the radix-16 column kernel
+  FftArgs fc2;              // its passes (16, ..., 16, then 4 and/or 2)
   double2 *xr, *xt;         // half spectra after the row pass, [i][k], i < nr
   double2 *khr, *kht;       // kernel spectra, [k][m]
   double *sq, *rr;          // sqrt(Rmed/R0), Rmed (per ring) for the densities
   double *nr_accr, *nr_acct;  // per-ring normalisations
   double r0;                // GlobalRmed[0]
   double rstep, tstep, eps;
-  size_t smem_row, smem_col;
+  size_t smem_row, smem_col, smem_col2;
 };
 
 static int plan_radices(int n, int *radix)
@@ -82,11 +90,6 @@ static __device__ __forceinline__ double2 cscale(double2 a, double s) { return m
 // multiply by -i (forward) or +i (inverse)
 static __device__ __forceinline__ double2 crot(double2 a, int inv) { return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x); }
 
-struct FftArgs {
-  int n, nst;
-  int radix[SG_MAXST];
-  const double2 *tw;
-};
 
 static FftArgs fft_args(const fb_fft_plan &p)
 {
@@ -305,6 +308,149 @@ __global__ void __launch_bounds__(SG_BS) sg_cols(FftArgs fa, int nrows_in, int n
   }
 }
 
+// ------------------------------------------- column pass, powers of two
+// Columns of m = 2^p points (p >= 4): radix-16 passes (a 4 x 4 split with
+// the W16 twiddles in registers), then a radix-4 and/or radix-2 pass, so a
+// 1024-point column takes three passes each way instead of five.  Every
+// thread holds 16 points per pass: it loads them, the CTA synchronises, it
+// stores them -- one buffer, transformed in place.  Lines are padded by one
+// slot per 16 (index i at i + i/16), which keeps the stride-16 stores of
+// the first pass free of bank conflicts.  CTAs of SG_KC2 * m / 16 threads.
+#define SG_KC2 2
+static __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+
+template <int INV>
+static __device__ __forceinline__ void dft4(double2 &a, double2 &b, double2 &c, double2 &d)
+{
+  const double2 A = cadd(a, c), B = csub(a, c);
+  const double2 Cc = cadd(b, d), D = crot(csub(b, d), INV);
+  a = cadd(A, Cc);
+  c = csub(A, Cc);
+  b = cadd(B, D);
+  d = csub(B, D);
+}
+
+// 16-point DFT of v[0..15] in place; output k ends in v[4 (k % 4) + k / 4].
+template <int INV>
+static __device__ __forceinline__ void dft16(double2 *v)
+{
+  // exp(-2 pi i e / 16) for e = 1, 2, 3, 6, 9 (e = 4 is -i)
+  const double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;
+  const double h = 0.70710678118654752440;
+  const double sg = INV ? -1.0 : 1.0;  // conjugate for the inverse
+#pragma unroll
+  for (int s = 0; s < 4; s++) dft4<INV>(v[s], v[s + 4], v[s + 8], v[s + 12]);
+  // v[s + 4p] *= W16^(s p)
+  v[5] = cmul(v[5], make_double2(c1, -sg * s1));
+  v[9] = cmul(v[9], make_double2(h, -sg * h));
+  v[13] = cmul(v[13], make_double2(s1, -sg * c1));
+  v[6] = cmul(v[6], make_double2(h, -sg * h));
+  v[10] = crot(v[10], INV);
+  v[14] = cmul(v[14], make_double2(-h, -sg * h));
+  v[7] = cmul(v[7], make_double2(s1, -sg * c1));
+  v[11] = cmul(v[11], make_double2(-h, -sg * h));
+  v[15] = cmul(v[15], make_double2(-c1, sg * s1));
+#pragma unroll
+  for (int p = 0; p < 4; p++) dft4<INV>(v[4 * p], v[4 * p + 1], v[4 * p + 2], v[4 * p + 3]);
+}
+
+// One radix-R Stockham pass over nl padded lines of m points (stride mp).
+template <int R, int INV>
+static __device__ __forceinline__ void col_pass(double2 *X, int m, int mp, int L, const double2 *__restrict__ tw)
+{
+  constexpr int B = 16 / R;
+  const int nb = m / R, T = blockDim.x;
+  double2 v[16];
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int bf = threadIdx.x + b * T, line = bf / nb, j = bf - line * nb;
+    const double2 *x = X + (size_t)line * mp;
+#pragma unroll
+    for (int r = 0; r < R; r++) v[b * R + r] = x[pad16(j + r * nb)];
+    if (L > 1) {
+      const int jm = j & (L - 1), ts = m / (L * R);
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        double2 w = tw[r * jm * ts];  // r*jm*ts < m
+        if (INV) w.y = -w.y;
+        v[b * R + r] = cmul(v[b * R + r], w);
+      }
+    }
+    if (R == 16) {
+      dft16<INV>(v);
+    } else if (R == 4) {
+      dft4<INV>(v[b * 4], v[b * 4 + 1], v[b * 4 + 2], v[b * 4 + 3]);
+    } else {
+      const double2 t0 = v[b * 2];
+      v[b * 2] = cadd(t0, v[b * 2 + 1]);
+      v[b * 2 + 1] = csub(t0, v[b * 2 + 1]);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int b = 0; b < B; b++) {
+    const int bf = threadIdx.x + b * T, line = bf / nb, j = bf - line * nb;
+    const int jm = j & (L - 1), idxD = (j - jm) * R + jm;
+    double2 *x = X + (size_t)line * mp;
+#pragma unroll
+    for (int r = 0; r < R; r++) x[pad16(idxD + r * L)] = (R == 16) ? v[4 * (r & 3) + (r >> 2)] : v[b * R + r];
+  }
+  __syncthreads();
+}
+
+template <int INV>
+static __device__ void col_fft(double2 *X, int m, const FftArgs &a)
+{
+  const int mp = m + m / 16;
+  int L = 1;
+  for (int st = 0; st < a.nst; st++) {
+    const int R = a.radix[st];
+    if (R == 16) col_pass<16, INV>(X, m, mp, L, a.tw);
+    else if (R == 4) col_pass<4, INV>(X, m, mp, L, a.tw);
+    else col_pass<2, INV>(X, m, mp, L, a.tw);
+    L *= R;
+  }
+}
+
+__global__ void __launch_bounds__(256) sg_cols_p2(FftArgs fa, int nrows_in, int nk, int mode, double2 *data_r,
+                                                 double2 *data_t, double2 *kh_r, double2 *kh_t)
+{
+  extern __shared__ double2 sm[];
+  const int m = fa.n, mp = m + m / 16, T = blockDim.x;
+  const int k0 = blockIdx.x * SG_KC2;
+  const int which = blockIdx.y;  // 0: r, 1: t
+  double2 *data = which ? data_t : data_r;
+  double2 *kh = which ? kh_t : kh_r;
+  double2 *X = sm;
+  for (int t = threadIdx.x; t < SG_KC2 * m; t += T) {
+    const int i = t / SG_KC2, c = t - i * SG_KC2, k = k0 + c;
+    X[(size_t)c * mp + pad16(i)] = (i < nrows_in && k < nk) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  col_fft<0>(X, m, fa);
+  if (mode == 0) {
+    for (int t = threadIdx.x; t < SG_KC2 * m; t += T) {
+      const int c = t / m, i = t - c * m, k = k0 + c;
+      if (k < nk) kh[(size_t)k * m + i] = X[(size_t)c * mp + pad16(i)];
+    }
+    return;
+  }
+  // product with -G Khat (sgacc.c:25-38)
+  for (int t = threadIdx.x; t < SG_KC2 * m; t += T) {
+    const int c = t / m, i = t - c * m, k = k0 + c;
+    if (k < nk) {
+      const double2 K = kh[(size_t)k * m + i], S = X[(size_t)c * mp + pad16(i)];
+      X[(size_t)c * mp + pad16(i)] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
+    }
+  }
+  __syncthreads();
+  col_fft<1>(X, m, fa);
+  for (int t = threadIdx.x; t < SG_KC2 * nrows_in; t += T) {
+    const int i = t / SG_KC2, c = t - i * SG_KC2, k = k0 + c;
+    if (k < nk) data[(size_t)i * nk + k] = X[(size_t)c * mp + pad16(i)];
+  }
+}
+
 // Inverse row pass + sgacc.c:138-161: normalisation, self-force.
 __global__ void __launch_bounds__(SG_BS) sg_rows_inv(FftArgs fa, int ns, int nk, const double2 *wr,
                                                       const double2 *wt, const double *normr,
@@ -383,12 +529,25 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   if (rc) { fb_sg_destroy(sg); return rc; }
   sg->smem_row = 2 * (size_t)ns * sizeof(double2);
   sg->smem_col = 2 * (size_t)SG_KC * m * sizeof(double2);
+  sg->p2 = (m >= 16 && m <= 2048 && (m & (m - 1)) == 0);
+  if (sg->p2) {
+    FftArgs &a = sg->fc2;
+    a.n = m;
+    a.tw = sg->pcol.tw;
+    a.nst = 0;
+    int rem = m;
+    while (rem % 16 == 0) { a.radix[a.nst++] = 16; rem /= 16; }
+    if (rem >= 4) { a.radix[a.nst++] = 4; rem /= 4; }
+    if (rem == 2) { a.radix[a.nst++] = 2; rem /= 2; }
+    for (int q = a.nst; q < SG_MAXST; q++) a.radix[q] = 1;
+    sg->smem_col2 = (size_t)SG_KC2 * (m + m / 16) * sizeof(double2);
+  }
   int dev = 0, maxopt = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (sg->smem_row > (size_t)maxopt || sg->smem_col > (size_t)maxopt) { fb_sg_destroy(sg); return FB_ERR_UNSUPPORTED; }
   if (fb_allow_max_dynamic_smem((const void *)sg_rows_fwd) || fb_allow_max_dynamic_smem((const void *)sg_rows_inv) ||
-      fb_allow_max_dynamic_smem((const void *)sg_cols)) {
+      fb_allow_max_dynamic_smem((const void *)sg_cols) || fb_allow_max_dynamic_smem((const void *)sg_cols_p2)) {
     fb_sg_destroy(sg);
     return FB_ERR_CUDA;
   }
@@ -453,7 +612,11 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   cudaMemcpy(dkt, kt.data(), kt.size() * sizeof(double), cudaMemcpyHostToDevice);
   FftArgs fr = fft_args(sg->prow), fc = fft_args(sg->pcol);
   sg_rows_fwd<<<m, SG_BS, sg->smem_row, s>>>(fr, m, ns, nk, NULL, NULL, NULL, 1.0, dkr, dkt, hr, ht);
-  sg_cols<<<dim3((nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s>>>(fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
+  if (sg->p2)
+    sg_cols_p2<<<dim3((nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * m / 16, sg->smem_col2, s>>>(sg->fc2, m, nk, 0, hr, ht,
+                                                                                          sg->khr, sg->kht);
+  else
+    sg_cols<<<dim3((nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s>>>(fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
   cudaError_t e = cudaStreamSynchronize(s);
   cudaFree(dkr); cudaFree(dkt); cudaFree(hr); cudaFree(ht);
   if (e != cudaSuccess) { fb_sg_destroy(sg); return FB_ERR_CUDA; }
@@ -481,6 +644,11 @@ void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 
 void fb_sg_cols(fb_sg *sg, cudaStream_t s)
 {
+  if (sg->p2) {
+    sg_cols_p2<<<dim3((sg->nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * sg->m / 16, sg->smem_col2, s>>>(
+        sg->fc2, sg->nr, sg->nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
+    return;
+  }
   FftArgs fc = fft_args(sg->pcol);
   sg_cols<<<dim3((sg->nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s>>>(fc, sg->nr, sg->nk, 1, sg->xr, sg->xt,
                                                                          sg->khr, sg->kht);

@@ -163,6 +163,24 @@ def test_selfgravity_accelerations(sg_case):
     assert e_r < 1e-12 and e_t < 1e-12
 
 
+@pytest.mark.parametrize("nrad,nsec", [(256, 768), (512, 1536)])
+def test_selfgravity_accelerations_large(tmp_path, nrad, nsec):
+    """The convolution on the benchmark's grids (2 Nr = 512 and 1024 point
+    columns: radix-16 column passes) against FFTW 2.1.5."""
+    from dustyfargoadsg_b200 import _ffi
+    par = _oracle.write_par(ADI, str(tmp_path), Nrad=nrad, Nsec=nsec)
+    d, _, _ = _oracle.run_oracle(par, steps=1, noise=1e-4, seed=5, max_substeps=1)
+    init = d["state_init"]
+    with _disc(par, _state_from(init, {k: init[k] for k in ("dens", "vrad", "vtheta", "energy")})) as disc:
+        disc.stage(_ffi.FB_STAGE_SELFGRAV, 1.0)
+        ar, at = disc.derived(6), disc.derived(7)
+    nrs = disc.nr * disc.ns
+    e_r = _oracle.rel_err(ar[:nrs], init["sg_accr"][:nrs])
+    e_t = _oracle.rel_err(at[:nrs], init["sg_acct"][:nrs])
+    print("SG accel errors", nrad, nsec, e_r, e_t)
+    assert e_r < 1e-12 and e_t < 1e-12
+
+
 def test_selfgravity_algogas_matches_oracle(sg_case, tmp_path):
     """Whole DTs with energy equation, beta cooling and self-gravity."""
     from dustyfargoadsg_b200 import Disc, read_par
