@@ -42,7 +42,7 @@ struct FftArgs {
 struct fb_sg {
   int nr, ns, m, nk;        // m = 2 nr, nk = ns/2 + 1
   fb_fft_plan prow, pcol;
-  int p2;                   // m = 2^p, p >= 4: the radix-16 column kernel
+  int p2, lgm;              // m = 2^lgm, lgm >= 4: the radix-16 column kernel
   FftArgs fc2;              // its passes (16, ..., 16, then 4 and/or 2)
   double2 *xr, *xt;         // half spectra after the row pass, [i][k], i < nr
   double2 *khr, *kht;       // kernel spectra, [k][m]
@@ -354,21 +354,22 @@ static __device__ __forceinline__ void dft16(double2 *v)
   for (int p = 0; p < 4; p++) dft4<INV>(v[4 * p], v[4 * p + 1], v[4 * p + 2], v[4 * p + 3]);
 }
 
-// One radix-R Stockham pass over nl padded lines of m points (stride mp).
+// One radix-R Stockham pass over the padded lines of m = 2^lgm points
+// (stride mp); tw holds the m twiddles in shared memory.
 template <int R, int INV>
-static __device__ __forceinline__ void col_pass(double2 *X, int m, int mp, int L, const double2 *__restrict__ tw)
+static __device__ __forceinline__ void col_pass(double2 *X, int lgm, int mp, int L, const double2 *tw)
 {
-  constexpr int B = 16 / R;
-  const int nb = m / R, T = blockDim.x;
+  constexpr int B = 16 / R, LGR = (R == 16) ? 4 : (R == 4) ? 2 : 1;
+  const int lgnb = lgm - LGR, nb = 1 << lgnb, T = blockDim.x;
   double2 v[16];
 #pragma unroll
   for (int b = 0; b < B; b++) {
-    const int bf = threadIdx.x + b * T, line = bf / nb, j = bf - line * nb;
-    const double2 *x = X + (size_t)line * mp;
+    const int bf = threadIdx.x + b * T, line = bf >> lgnb, j = bf & (nb - 1);
+    const double2 *x = X + line * mp;
 #pragma unroll
     for (int r = 0; r < R; r++) v[b * R + r] = x[pad16(j + r * nb)];
     if (L > 1) {
-      const int jm = j & (L - 1), ts = m / (L * R);
+      const int jm = j & (L - 1), ts = nb / L;  // m / (L R)
 #pragma unroll
       for (int r = 1; r < R; r++) {
         double2 w = tw[r * jm * ts];  // r*jm*ts < m
@@ -389,9 +390,9 @@ static __device__ __forceinline__ void col_pass(double2 *X, int m, int mp, int L
   __syncthreads();
 #pragma unroll
   for (int b = 0; b < B; b++) {
-    const int bf = threadIdx.x + b * T, line = bf / nb, j = bf - line * nb;
+    const int bf = threadIdx.x + b * T, line = bf >> lgnb, j = bf & (nb - 1);
     const int jm = j & (L - 1), idxD = (j - jm) * R + jm;
-    double2 *x = X + (size_t)line * mp;
+    double2 *x = X + line * mp;
 #pragma unroll
     for (int r = 0; r < R; r++) x[pad16(idxD + r * L)] = (R == 16) ? v[4 * (r & 3) + (r >> 2)] : v[b * R + r];
   }
@@ -399,55 +400,71 @@ static __device__ __forceinline__ void col_pass(double2 *X, int m, int mp, int L
 }
 
 template <int INV>
-static __device__ void col_fft(double2 *X, int m, const FftArgs &a)
+static __device__ void col_fft(double2 *X, int lgm, const FftArgs &a, const double2 *tw)
 {
-  const int mp = m + m / 16;
+  const int m = 1 << lgm, mp = m + m / 16;
   int L = 1;
   for (int st = 0; st < a.nst; st++) {
     const int R = a.radix[st];
-    if (R == 16) col_pass<16, INV>(X, m, mp, L, a.tw);
-    else if (R == 4) col_pass<4, INV>(X, m, mp, L, a.tw);
-    else col_pass<2, INV>(X, m, mp, L, a.tw);
+    if (R == 16) col_pass<16, INV>(X, lgm, mp, L, tw);
+    else if (R == 4) col_pass<4, INV>(X, lgm, mp, L, tw);
+    else col_pass<2, INV>(X, lgm, mp, L, tw);
     L *= R;
   }
 }
 
-__global__ void __launch_bounds__(256) sg_cols_p2(FftArgs fa, int nrows_in, int nk, int mode, double2 *data_r,
-                                                 double2 *data_t, double2 *kh_r, double2 *kh_t)
+// Every thread moves 16 points in each phase (T = SG_KC2 m / 16), with all
+// of a phase's global loads issued before their first use.
+__global__ void __launch_bounds__(256) sg_cols_p2(FftArgs fa, int lgm, int nrows_in, int nk, int mode,
+                                                 double2 *data_r, double2 *data_t, double2 *kh_r, double2 *kh_t)
 {
   extern __shared__ double2 sm[];
-  const int m = fa.n, mp = m + m / 16, T = blockDim.x;
+  const int m = 1 << lgm, mp = m + m / 16, T = blockDim.x, tid = threadIdx.x;
   const int k0 = blockIdx.x * SG_KC2;
   const int which = blockIdx.y;  // 0: r, 1: t
   double2 *data = which ? data_t : data_r;
   double2 *kh = which ? kh_t : kh_r;
-  double2 *X = sm;
-  for (int t = threadIdx.x; t < SG_KC2 * m; t += T) {
-    const int i = t / SG_KC2, c = t - i * SG_KC2, k = k0 + c;
-    X[(size_t)c * mp + pad16(i)] = (i < nrows_in && k < nk) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
+  double2 *X = sm, *tw = sm + SG_KC2 * mp;
+  double2 v[16];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int t = tid + q * T, i = t >> 1, c = t & 1, k = k0 + c;  // SG_KC2 == 2
+    v[q] = (i < nrows_in && k < nk) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
+  }
+  for (int t = tid; t < m; t += T) tw[t] = fa.tw[t];
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int t = tid + q * T, i = t >> 1, c = t & 1;
+    X[c * mp + pad16(i)] = v[q];
   }
   __syncthreads();
-  col_fft<0>(X, m, fa);
+  col_fft<0>(X, lgm, fa, tw);
   if (mode == 0) {
-    for (int t = threadIdx.x; t < SG_KC2 * m; t += T) {
-      const int c = t / m, i = t - c * m, k = k0 + c;
-      if (k < nk) kh[(size_t)k * m + i] = X[(size_t)c * mp + pad16(i)];
+#pragma unroll
+    for (int q = 0; q < 16; q++) {
+      const int t = tid + q * T, c = t >> lgm, i = t & (m - 1), k = k0 + c;
+      if (k < nk) kh[(size_t)k * m + i] = X[c * mp + pad16(i)];
     }
     return;
   }
   // product with -G Khat (sgacc.c:25-38)
-  for (int t = threadIdx.x; t < SG_KC2 * m; t += T) {
-    const int c = t / m, i = t - c * m, k = k0 + c;
-    if (k < nk) {
-      const double2 K = kh[(size_t)k * m + i], S = X[(size_t)c * mp + pad16(i)];
-      X[(size_t)c * mp + pad16(i)] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
-    }
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int t = tid + q * T, c = t >> lgm, i = t & (m - 1), k = k0 + c;
+    v[q] = (k < nk) ? kh[(size_t)k * m + i] : make_double2(0.0, 0.0);
+  }
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int t = tid + q * T, c = t >> lgm, i = t & (m - 1);
+    const double2 K = v[q], S = X[c * mp + pad16(i)];
+    X[c * mp + pad16(i)] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
   }
   __syncthreads();
-  col_fft<1>(X, m, fa);
-  for (int t = threadIdx.x; t < SG_KC2 * nrows_in; t += T) {
-    const int i = t / SG_KC2, c = t - i * SG_KC2, k = k0 + c;
-    if (k < nk) data[(size_t)i * nk + k] = X[(size_t)c * mp + pad16(i)];
+  col_fft<1>(X, lgm, fa, tw);
+#pragma unroll
+  for (int q = 0; q < 16; q++) {
+    const int t = tid + q * T, i = t >> 1, c = t & 1, k = k0 + c;
+    if (i < nrows_in && k < nk) data[(size_t)i * nk + k] = X[c * mp + pad16(i)];
   }
 }
 
@@ -540,7 +557,9 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
     if (rem >= 4) { a.radix[a.nst++] = 4; rem /= 4; }
     if (rem == 2) { a.radix[a.nst++] = 2; rem /= 2; }
     for (int q = a.nst; q < SG_MAXST; q++) a.radix[q] = 1;
-    sg->smem_col2 = (size_t)SG_KC2 * (m + m / 16) * sizeof(double2);
+    sg->smem_col2 = ((size_t)SG_KC2 * (m + m / 16) + m) * sizeof(double2);
+    sg->lgm = 0;
+    while ((1 << sg->lgm) < m) sg->lgm++;
   }
   int dev = 0, maxopt = 0;
   cudaGetDevice(&dev);
@@ -613,8 +632,8 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   FftArgs fr = fft_args(sg->prow), fc = fft_args(sg->pcol);
   sg_rows_fwd<<<m, SG_BS, sg->smem_row, s>>>(fr, m, ns, nk, NULL, NULL, NULL, 1.0, dkr, dkt, hr, ht);
   if (sg->p2)
-    sg_cols_p2<<<dim3((nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * m / 16, sg->smem_col2, s>>>(sg->fc2, m, nk, 0, hr, ht,
-                                                                                          sg->khr, sg->kht);
+    sg_cols_p2<<<dim3((nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * m / 16, sg->smem_col2, s>>>(sg->fc2, sg->lgm, m, nk, 0,
+                                                                                          hr, ht, sg->khr, sg->kht);
   else
     sg_cols<<<dim3((nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s>>>(fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
   cudaError_t e = cudaStreamSynchronize(s);
@@ -646,7 +665,7 @@ void fb_sg_cols(fb_sg *sg, cudaStream_t s)
 {
   if (sg->p2) {
     sg_cols_p2<<<dim3((sg->nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * sg->m / 16, sg->smem_col2, s>>>(
-        sg->fc2, sg->nr, sg->nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
+        sg->fc2, sg->lgm, sg->nr, sg->nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
     return;
   }
   FftArgs fc = fft_args(sg->pcol);
