@@ -97,6 +97,19 @@ struct KP {
 };
 
 // Device state of the particles' random stream (src/DustUpdate.c:438-485).
+// a / d rounded to nearest, given r = 1/d rounded to nearest: y = RN(a r) is
+// within one ulp of a/d, its remainder a - d y is exact in one fma, and
+// RN(y + r (a - d y)) = RN(a / d) (Markstein's theorem: P. Markstein, IBM J.
+// Res. Dev. 34(1), 1990; J.-M. Muller et al., Handbook of Floating-Point
+// Arithmetic, ch. 4).  Valid away from overflow and underflow.  Lets several
+// quotients by one divisor share a single division.
+static __device__ __forceinline__ double fb_quot(double a, double d, double r)
+{
+  const double y = a * r;
+  const double e = fma(-d, y, a);
+  return fma(e, r, y);
+}
+
 struct fb_dust_ctl {
   unsigned long long x;        // drand48 state after the last draw
   long long kicks;             // calls made so far by each Gaussian generator

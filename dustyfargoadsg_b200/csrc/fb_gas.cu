@@ -1024,7 +1024,6 @@ static __device__ double block_sum_dyn(double v, double *sh)
   return r;
 }
 
-static __device__ __forceinline__ int wrapj(int j, int ns) { return j < 0 ? j + ns : (j >= ns ? j - ns : j); }
 
 // Azimuthal pass (OneWindTheta, TransportEuler.c:226-247): ring mean,
 // residual and integer FARGO shift (:249-373), van Leer on the residual and
@@ -1047,7 +1046,7 @@ static __device__ __forceinline__ int wrapj(int j, int ns) { return j < 0 ? j + 
 // 110.6 KB for six quantities of 1536 cells, so that two CTAs share an SM
 #define FB_AZI_RINGS(NQ) ((NQ) + 3)
 template <int E> struct AziMaxThreads { static const int value = (E <= 2) ? 1024 : 768; };
-template <int NQ, int E>
+template <int NQ, int E, bool FULL>
 __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal(KP k, double dtov)
 {
   extern __shared__ double smem[];
@@ -1088,76 +1087,88 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
   const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
   const double invsurf = 1.0 / k.surf[i];
   const double *rho = Q + (NQ - 1) * ns;
-#define jc(e) (tid + (e) * T)  // own cells (valid while < ns)
+  // own cells j = tid + e T (all valid when FULL: ns == E T) and their
+  // periodic neighbours
+  int jj[E], jjm[E], jjp[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int j = tid + e * T;
+    jj[e] = j;
+    jjm[e] = (j == 0) ? ns - 1 : j - 1;
+    jjp[e] = (j == ns - 1) ? 0 : j + 1;
+  }
+#define OWN(e) (FULL || jj[e] < ns)
   for (int pass = 0; pass < 2; pass++) {
     const bool uniform = (pass == 1);
     if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
     __syncthreads();  // Q and vres complete
     // RhoStar (ComputeStarTheta(Rho, V, RhoStar)); RhoInt is the density
     // before this pass, kept in registers for the own cells.
-    double R[E], RSl[E], RSh[E], Vl[E], Vh[E];
+    double R[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int j = jc(e);
-      if (j < ns) {
-        const double rm = rho[wrapj(j - 1, ns)], r0 = rho[j], rp = rho[wrapj(j + 1, ns)];
-        R[e] = r0;
-        const double dqm = (r0 - rm), dqp = (rp - r0);
-        DR[j] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
-      }
+      if (!OWN(e)) continue;
+      const double rm = rho[jjm[e]], r0 = rho[jj[e]], rp = rho[jjp[e]];
+      R[e] = r0;
+      const double dqm = (r0 - rm), dqp = (rp - r0);
+      DR[jj[e]] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
     }
     __syncthreads();
+    // Per face, the upwind cell u and the factor f of its star value:
+    // (kl > 0) ? q[j-1] + (dxtheta - kl) DQ[j-1] : q[j] - (dxtheta + kl) DQ[j]
+    // is q[u] + f DQ[u] with f = dxtheta - kl or -(dxtheta + kl) (the same
+    // value: negation and a + (-b) = a - b are exact).
+    double RSl[E], RSh[E], Vl[E], Vh[E], fl[E], fh[E], den[E], rden[E];
+    int ul[E], uh[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
-      const int j = jc(e);
-      if (j < ns) {
-        const int jm = wrapj(j - 1, ns), jp = wrapj(j + 1, ns);
-        const double vl = uniform ? vconst : vres[j], vh = uniform ? vconst : vres[jp];
-        Vl[e] = vl;
-        Vh[e] = vh;
-        const double kl = vl * dt, kh = vh * dt;
-        RSl[e] = (kl > 0.0) ? rho[jm] + (dxtheta - kl) * DR[jm] : R[e] - (dxtheta + kl) * DR[j];
-        RSh[e] = (kh > 0.0) ? R[e] + (dxtheta - kh) * DR[j] : rho[jp] - (dxtheta + kh) * DR[jp];
-      }
+      if (!OWN(e)) continue;
+      const double vl = uniform ? vconst : vres[jj[e]], vh = uniform ? vconst : vres[jjp[e]];
+      Vl[e] = vl;
+      Vh[e] = vh;
+      const double kl = vl * dt, kh = vh * dt;
+      ul[e] = (kl > 0.0) ? jjm[e] : jj[e];
+      fl[e] = (kl > 0.0) ? (dxtheta - kl) : -(dxtheta + kl);
+      uh[e] = (kh > 0.0) ? jj[e] : jjp[e];
+      fh[e] = (kh > 0.0) ? (dxtheta - kh) : -(dxtheta + kh);
+      RSl[e] = rho[ul[e]] + fl[e] * DR[ul[e]];
+      RSh[e] = rho[uh[e]] + fh[e] * DR[uh[e]];
+      den[e] = R[e] + 1e-20;
+      rden[e] = 1.0 / den[e];
     }
+#pragma unroll
     for (int q = 0; q < NQ; q++) {
       double *qb = Q + q * ns;
       double q0[E];
       if (q > 0) __syncthreads();  // every read of the previous W and DQ done
 #pragma unroll
       for (int e = 0; e < E; e++) {
-        const int j = jc(e);
-        if (j < ns) {
-          q0[e] = qb[j];
-          W[j] = q0[e] / (R[e] + 1e-20);
-        }
+        if (!OWN(e)) continue;
+        q0[e] = qb[jj[e]];
+        W[jj[e]] = fb_quot(q0[e], den[e], rden[e]);  // q0 / (RhoInt + 1e-20)
       }
       __syncthreads();  // W complete (and, for q = 0, every read of DR done)
 #pragma unroll
       for (int e = 0; e < E; e++) {
-        const int j = jc(e);
-        if (j < ns) {
-          const double w0 = W[j];
-          const double dqm = (w0 - W[wrapj(j - 1, ns)]), dqp = (W[wrapj(j + 1, ns)] - w0);
-          D[j] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
-        }
+        if (!OWN(e)) continue;
+        const double w0 = W[jj[e]];
+        const double dqm = (w0 - W[jjm[e]]), dqp = (W[jjp[e]] - w0);
+        D[jj[e]] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
       }
       __syncthreads();  // DQ complete
 #pragma unroll
       for (int e = 0; e < E; e++) {
-        const int j = jc(e);
-        if (j < ns) {
-          const int jm = wrapj(j - 1, ns), jp = wrapj(j + 1, ns);
-          const double kl = Vl[e] * dt, kh = Vh[e] * dt;
-          const double qsl = (kl > 0.0) ? W[jm] + (dxtheta - kl) * D[jm] : W[j] - (dxtheta + kl) * D[j];
-          const double qsh = (kh > 0.0) ? W[j] + (dxtheta - kh) * D[j] : W[jp] - (dxtheta + kh) * D[jp];
-          double varq = dxrad * qsl * RSl[e] * Vl[e];
-          varq -= dxrad * qsh * RSh[e] * Vh[e];
-          qb[j] = q0[e] + varq * invsurf;
-        }
+        if (!OWN(e)) continue;
+        const double qsl = W[ul[e]] + fl[e] * D[ul[e]];
+        const double qsh = W[uh[e]] + fh[e] * D[uh[e]];
+        double varq = dxrad * qsl * RSl[e] * Vl[e];
+        varq -= dxrad * qsh * RSh[e] * Vh[e];
+        qb[jj[e]] = q0[e] + varq * invsurf;
       }
     }
   }
+#undef OWN
+#define jc(e) (tid + (e) * T)  // own cells (valid while < ns)
   __syncthreads();
   // AdvectSHIFT (TransportEuler.c:350-373) for every quantity: cell j takes
   // cell (j - nshift) mod ns
@@ -1296,12 +1307,17 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
   const size_t smem = (size_t)FB_AZI_RINGS(NQ) * k.ns * sizeof(double);
   const int E = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
   const int th = azi_threads_for(k.ns, E);
+  const bool full = (th * E == k.ns);  // every thread owns E cells
+#define AZI_LAUNCH(EE)                                                            \
+  (full ? k_transport_azimuthal<NQ, EE, true><<<k.nr, th, smem, s>>>(k, dt_override) \
+        : k_transport_azimuthal<NQ, EE, false><<<k.nr, th, smem, s>>>(k, dt_override))
   switch (E) {
-    case 1: k_transport_azimuthal<NQ, 1><<<k.nr, th, smem, s>>>(k, dt_override); break;
-    case 2: k_transport_azimuthal<NQ, 2><<<k.nr, th, smem, s>>>(k, dt_override); break;
-    case 3: k_transport_azimuthal<NQ, 3><<<k.nr, th, smem, s>>>(k, dt_override); break;
-    default: k_transport_azimuthal<NQ, 4><<<k.nr, th, smem, s>>>(k, dt_override); break;
+    case 1: AZI_LAUNCH(1); break;
+    case 2: AZI_LAUNCH(2); break;
+    case 3: AZI_LAUNCH(3); break;
+    default: AZI_LAUNCH(4); break;
   }
+#undef AZI_LAUNCH
 }
 
 void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s)
@@ -1504,10 +1520,11 @@ int fb_gas_prepare(int ns, int energy)
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem + 32 * sizeof(double) > (size_t)maxopt) return FB_ERR_UNSUPPORTED;
   if (fb_azi_E_auto(ns) > 4 || ns < 16) return FB_ERR_UNSUPPORTED;
-  const void *fns[] = {(const void *)k_transport_azimuthal<5, 1>, (const void *)k_transport_azimuthal<5, 2>,
-                       (const void *)k_transport_azimuthal<5, 3>, (const void *)k_transport_azimuthal<5, 4>,
-                       (const void *)k_transport_azimuthal<6, 1>, (const void *)k_transport_azimuthal<6, 2>,
-                       (const void *)k_transport_azimuthal<6, 3>, (const void *)k_transport_azimuthal<6, 4>};
+#define AZI_FNS(NQ, F)                                                                                   \
+  (const void *)k_transport_azimuthal<NQ, 1, F>, (const void *)k_transport_azimuthal<NQ, 2, F>,          \
+      (const void *)k_transport_azimuthal<NQ, 3, F>, (const void *)k_transport_azimuthal<NQ, 4, F>
+  const void *fns[] = {AZI_FNS(5, false), AZI_FNS(5, true), AZI_FNS(6, false), AZI_FNS(6, true)};
+#undef AZI_FNS
   for (const void *f : fns) {
     int rc = fb_allow_max_dynamic_smem(f);
     if (rc) return rc;
