@@ -898,45 +898,67 @@ void fb_launch_substep3(const KP &k, cudaStream_t s) { k_substep3<<<k.nr + 1, FB
 // ------------------------------------------------------------ Transport
 // Radial pass of the van Leer transport (OneWindRad, TransportEuler.c:124-220
 // with ComputeLRMomenta :89-119, ComputeStarRad :141-184, DivisePolarGrid
-// SideEuler.c:244-261).  One thread owns one azimuth column and marches
+// SideEuler.c:244-261).  A thread owns one azimuth column and marches
 // through a chunk of rings, keeping the slopes and interface values of the
 // last rings in registers, so each input is read once and no interface is
 // evaluated twice.  Outputs the five (six) transported quantities.
-template <int NQ>
-__global__ void __launch_bounds__(128) k_transport_radial(KP k, double dtov, int chunk)
+// The quantities of a column are split over two halves of the CTA (warps
+// of the first half: RadMomP, RadMomM, ThetaMomP; of the second: ThetaMomM,
+// Energy, Rho), so each thread keeps the windows of at most three; both
+// halves evaluate the density's own slope and star value.
+template <int NQ, int H>
+static __device__ __forceinline__ void radial_column(const KP &k, double dt, int j, int i0, int i1)
 {
-  const double dt = dt_of(k, dtov);
+  constexpr int LO = H ? 3 : 0, NH = (H ? NQ : 3) - LO;
   const int ns = k.ns, nr = k.nr;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ns) return;
-  const int i0 = blockIdx.y * chunk;
-  const int i1 = min(nr, i0 + chunk);
   const int jp = (j == ns - 1) ? 0 : j + 1;
   const double Om = k.omega_frame;
   const double dtheta = (k.pmax - k.pmin) / (double)ns;
   // window: index 0 = ring k-1, 1 = ring k, 2 = ring k+1
-  double W[NQ][3], Qo[NQ][3], R[3];
-  double DQ[NQ][2], DR[2], QS[NQ][2], RS[2], VR[2];
-  auto load = [&](int kk, int slot) {
+  double W[NH][3], Qo[NH][3], R[3], VW[3];
+  double DQ[NH][2], DR[2], QS[NH][2], RS[2], VR[2];
+  // the inputs of one ring, loaded one iteration before they are used
+  struct Raw { double r, u0, u1, u2, v; };
+  auto fetch = [&](int kk) -> Raw {
+    Raw w = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (kk >= 0 && kk <= nr - 1) {
+      const size_t l = (size_t)kk * ns + j;
+      w.r = k.rho[l];
+      if (H == 0) {
+        w.u0 = k.vr[l + ns];
+        w.u1 = k.vr[l];
+        w.u2 = k.vt[(size_t)kk * ns + jp];
+      } else {
+        w.u0 = k.vt[l];
+        if (NQ == 6) w.u1 = k.e[l];
+      }
+    }
+    if (kk >= 0 && kk <= nr) w.v = k.vr[(size_t)kk * ns + j];
+    return w;
+  };
+  auto put = [&](const Raw &w, int kk, int slot) {
+    VW[slot] = w.v;
     if (kk < 0 || kk > nr - 1) {
 #pragma unroll
-      for (int q = 0; q < NQ; q++) { W[q][slot] = 0.0; Qo[q][slot] = 0.0; }
+      for (int q = 0; q < NH; q++) { W[q][slot] = 0.0; Qo[q][slot] = 0.0; }
       R[slot] = 0.0;
       return;
     }
-    const size_t l = (size_t)kk * ns + j;
-    const double r = k.rho[l];
+    const double r = w.r;
     const double Rm = k.rmed[kk];
-    double qv[NQ];
-    qv[0] = r * k.vr[l + ns];                       // rp = rho*vr[lip]
-    qv[1] = r * k.vr[l];                            // rm = rho*vr[l]
-    qv[2] = r * (k.vt[(size_t)kk * ns + jp] + Rm * Om) * Rm;  // tp
-    qv[3] = r * (k.vt[l] + Rm * Om) * Rm;           // tm
-    if (NQ == 6) qv[4] = k.e[l];
-    qv[NQ - 1] = r;
-    const double den = r + 1e-20;
+    double qv[NH];
+    if (H == 0) {
+      qv[0] = r * w.u0;                    // rp = rho*vr[lip]
+      qv[1] = r * w.u1;                    // rm = rho*vr[l]
+      qv[2] = r * (w.u2 + Rm * Om) * Rm;   // tp
+    } else {
+      qv[0] = r * (w.u0 + Rm * Om) * Rm;   // tm
+      if (NQ == 6) qv[1] = w.u1;
+      qv[NH - 1] = r;
+    }
+    const double den = r + 1e-20, rden = 1.0 / den;
 #pragma unroll
-    for (int q = 0; q < NQ; q++) { Qo[q][slot] = qv[q]; W[q][slot] = qv[q] / den; }
+    for (int q = 0; q < NH; q++) { Qo[q][slot] = qv[q]; W[q][slot] = fb_quot(qv[q], den, rden); }  // qv / den
     R[slot] = r;
   };
   auto slope = [&](double am, double a0, double ap, int kk) -> double {
@@ -947,33 +969,36 @@ __global__ void __launch_bounds__(128) k_transport_radial(KP k, double dtov, int
     return 0.0;
   };
   int kstart = max(i0 - 1, 0);
-  load(kstart - 1, 0);
-  load(kstart, 1);
+  Raw nxt = fetch(kstart + 1);
+  put(fetch(kstart - 1), kstart - 1, 0);
+  put(fetch(kstart), kstart, 1);
 #pragma unroll
-  for (int q = 0; q < NQ; q++) { DQ[q][0] = 0.0; QS[q][0] = 0.0; }
+  for (int q = 0; q < NH; q++) { DQ[q][0] = 0.0; QS[q][0] = 0.0; }
   DR[0] = 0.0; RS[0] = 0.0; VR[0] = 0.0;
   for (int kk = kstart; kk <= i1; kk++) {
-    load(kk + 1, 2);
-    const double vrk = k.vr[(size_t)kk * ns + j];
+    const Raw cur = nxt;
+    nxt = fetch(kk + 2);
+    put(cur, kk + 1, 2);
+    const double vrk = VW[1];  // vr of ring kk
     const double rmk = k.rmed[kk];
     const double rmkm = (kk >= 1) ? k.rmed[kk - 1] : 0.0;
 #pragma unroll
-    for (int q = 0; q < NQ; q++) DQ[q][1] = slope(W[q][0], W[q][1], W[q][2], kk);
+    for (int q = 0; q < NH; q++) DQ[q][1] = slope(W[q][0], W[q][1], W[q][2], kk);
     DR[1] = slope(R[0], R[1], R[2], kk);
     if (kk == 0 || kk >= nr) {
 #pragma unroll
-      for (int q = 0; q < NQ; q++) QS[q][1] = 0.0;
+      for (int q = 0; q < NH; q++) QS[q][1] = 0.0;
       RS[1] = 0.0;
     } else if (vrk > 0.0) {
       const double f = (rmk - rmkm - vrk * dt) * 0.5;
 #pragma unroll
-      for (int q = 0; q < NQ; q++) QS[q][1] = W[q][0] + (rmk - rmkm - vrk * dt) * 0.5 * DQ[q][0];
+      for (int q = 0; q < NH; q++) QS[q][1] = W[q][0] + (rmk - rmkm - vrk * dt) * 0.5 * DQ[q][0];
       RS[1] = R[0] + f * DR[0];
     } else {
       const double rmkp = k.rmed[kk + 1];
       const double f = (rmkp - rmk + vrk * dt) * 0.5;
 #pragma unroll
-      for (int q = 0; q < NQ; q++) QS[q][1] = W[q][1] - (rmkp - rmk + vrk * dt) * 0.5 * DQ[q][1];
+      for (int q = 0; q < NH; q++) QS[q][1] = W[q][1] - (rmkp - rmk + vrk * dt) * 0.5 * DQ[q][1];
       RS[1] = R[1] - f * DR[1];
     }
     VR[1] = vrk;
@@ -983,26 +1008,43 @@ __global__ void __launch_bounds__(128) k_transport_radial(KP k, double dtov, int
       const double a = dt * dtheta * k.rinf[io];
       const double b = dt * dtheta * k.rsup[io];
 #pragma unroll
-      for (int q = 0; q < NQ; q++) {
+      for (int q = 0; q < NH; q++) {
         double varq = a * QS[q][0] * RS[0] * VR[0];
         varq -= b * QS[q][1] * RS[1] * VR[1];
-        k.q[q][l] = Qo[q][0] + varq * k.invsurf[io];
-        if (q == NQ - 1 && io == 0) k.lost0[j] = varq;
+        k.q[LO + q][l] = Qo[q][0] + varq * k.invsurf[io];
+        if (LO + q == NQ - 1 && io == 0) k.lost0[j] = varq;
       }
     }
     // shift windows
 #pragma unroll
-    for (int q = 0; q < NQ; q++) {
+    for (int q = 0; q < NH; q++) {
       W[q][0] = W[q][1]; W[q][1] = W[q][2];
       Qo[q][0] = Qo[q][1]; Qo[q][1] = Qo[q][2];
       DQ[q][0] = DQ[q][1];
       QS[q][0] = QS[q][1];
     }
     R[0] = R[1]; R[1] = R[2];
+    VW[0] = VW[1]; VW[1] = VW[2];
     DR[0] = DR[1];
     RS[0] = RS[1];
     VR[0] = VR[1];
   }
+}
+
+// CTAs of 2 tx threads: columns blockIdx.x tx .. + tx, rings of one chunk
+template <int NQ>
+__global__ void __launch_bounds__(256) k_transport_radial(KP k, double dtov, int chunk)
+{
+  const double dt = dt_of(k, dtov);
+  const int tx = blockDim.x >> 1, h = (threadIdx.x >= tx) ? 1 : 0;  // tx % 32 == 0: warp-uniform
+  const int j = blockIdx.x * tx + threadIdx.x - h * tx;
+  if (j >= k.ns) return;
+  const int i0 = blockIdx.y * chunk;
+  const int i1 = min(k.nr, i0 + chunk);
+  if (h == 0)
+    radial_column<NQ, 0>(k, dt, j, i0, i1);
+  else
+    radial_column<NQ, 1>(k, dt, j, i0, i1);
 }
 
 // Sum over the block for any blockDim that is a multiple of 32.
@@ -1296,9 +1338,9 @@ void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
   const int chunk = k.rad_chunk > 0 ? k.rad_chunk : fb_rad_chunk_auto(k);
   dim3 gr(bx, (k.nr + chunk - 1) / chunk);
   if (k.energy)
-    k_transport_radial<6><<<gr, tx, 0, s>>>(k, dt_override, chunk);
+    k_transport_radial<6><<<gr, 2 * tx, 0, s>>>(k, dt_override, chunk);
   else
-    k_transport_radial<5><<<gr, tx, 0, s>>>(k, dt_override, chunk);
+    k_transport_radial<5><<<gr, 2 * tx, 0, s>>>(k, dt_override, chunk);
 }
 
 template <int NQ>
