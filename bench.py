@@ -147,7 +147,7 @@ def cpu_baseline_sample(par_path, noise, seed, budget_s, cells, cores=1):
     """Time the reference's own build (oracle/_ref) on a bounded sample.
 
     Returns (cell_updates_per_s, description) or (None, reason)."""
-    from tests import _oracle  # the checker/baseline only; never on the product path
+    from tests import _oracle  # test infrastructure: the CPU baseline only, never the product path
     if not _oracle.have_oracle():
         return None, "oracle binary not built"
     # a short probe run measures the substep rate, then one bounded sample
