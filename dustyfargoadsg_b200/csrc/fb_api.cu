@@ -163,10 +163,11 @@ static int dust_create(fb_ctx *ctx)
   const int nsb = (n + 1023) / 1024, ncb = (pp.ncand + 255) / 256;
   pp.ncells = ctx->nr * ctx->ns + 1;
   int **ints[] = {&pp.flag, &pp.kidx, &pp.kick_bsum, &pp.cand_flag, &pp.cand_bsum,
-                  &pp.perm, &pp.key, &pp.cell_count, &pp.cell_bsum};
+                  &pp.perm, &pp.key, &pp.cell_count, &pp.cell_bsum, &pp.orig, &pp.oscratch};
   const size_t isz[] = {(size_t)n, (size_t)n, (size_t)nsb, (size_t)pp.ncand, (size_t)ncb,
-                        (size_t)n, (size_t)n, (size_t)pp.ncells, (size_t)(pp.ncells + 1023) / 1024};
-  for (size_t f = 0; f < 9; f++) {
+                        (size_t)n, (size_t)n, (size_t)pp.ncells, (size_t)(pp.ncells + 1023) / 1024,
+                        (size_t)n, (size_t)n};
+  for (size_t f = 0; f < 11; f++) {
     void *d = NULL;
     if (cudaMalloc(&d, isz[f] * sizeof(int)) != cudaSuccess) return FB_ERR_NOMEM;
     cudaMemset(d, 0, isz[f] * sizeof(int));
@@ -217,12 +218,12 @@ static int dust_create(fb_ctx *ctx)
   // and only the stopping-time bound on the substep remains
   if (p->dust_feedback) k.dust_min_ts = &pp.dc->min_ts;
   if (!pp.azimuth || !pp.aziinf) return FB_ERR_NOMEM;
-  {
-    std::vector<int> id(n);
-    for (int q = 0; q < n; q++) id[q] = q;
-    if (cudaMemcpy(pp.perm, id.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess)
-      return FB_ERR_CUDA;
-  }
+  if (!(pp.pscratch = dalloc(ctx, 7 * (size_t)n))) return FB_ERR_NOMEM;
+  // first guess of a radius's ring: the grid law of the radii
+  pp.ring_r0 = g.rinf[0];
+  pp.ring_inv_r0 = 1.0 / g.rinf[0];
+  pp.ring_inv_step = p->log_grid ? (double)ctx->nr / log(g.rsup[ctx->nr - 1] / g.rinf[0])
+                                 : (double)ctx->nr / (g.rsup[ctx->nr - 1] - g.rinf[0]);
   ctx->has_dust = 1;
   return FB_OK;
 }
@@ -910,6 +911,8 @@ extern "C" int fb_dust_upload(fb_ctx *ctx, const fb_dust_state *st)
   const double *src[] = {st->r, st->th, st->vr, st->vth, st->l, st->size, st->stokes};
   double *dst[] = {pp.r, pp.th, pp.vr, pp.vth, pp.l, pp.size, pp.st};
   for (int f = 0; f < 7; f++) CK(cudaMemcpyAsync(dst[f], src[f], b, cudaMemcpyHostToDevice, ctx->st));
+  fb_launch_dust_iota(pp, ctx->st);  // slots in the reference's order until the first sort
+  ctx->launches += 1;
   fb_dust_ctl *h = ctx->h_dc;
   memset(h, 0, sizeof *h);
   h->x = st->rng_x;
@@ -937,8 +940,14 @@ extern "C" int fb_dust_download(fb_ctx *ctx, fb_dust_state *st)
   const size_t b = (size_t)pp.n * sizeof(double);
   double *dst[] = {st->r, st->th, st->vr, st->vth, st->l, st->size, st->stokes};
   const double *src[] = {pp.r, pp.th, pp.vr, pp.vth, pp.l, pp.size, pp.st};
-  for (int f = 0; f < 7; f++)
-    if (dst[f]) CK(cudaMemcpyAsync(dst[f], src[f], b, cudaMemcpyDeviceToHost, ctx->st));
+  // back in the reference's order through the scratch arrays
+  for (int f = 0; f < 7; f++) {
+    if (!dst[f]) continue;
+    double *tmp = pp.pscratch + (size_t)f * pp.n;
+    fb_launch_dust_to_reference_order(pp, src[f], tmp, ctx->st);
+    ctx->launches += 1;
+    CK(cudaMemcpyAsync(dst[f], tmp, b, cudaMemcpyDeviceToHost, ctx->st));
+  }
   CK(cudaMemcpyAsync(ctx->h_dc, pp.dc, sizeof(fb_dust_ctl), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   const fb_dust_ctl *h = ctx->h_dc;

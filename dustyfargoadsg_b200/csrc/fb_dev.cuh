@@ -136,10 +136,18 @@ struct PP {
   double aspectratio, thicksmoothing, flaringindex;
   int log_grid, feel_disk, feel_planets, feel_sg, feel_turb, sfta;
   int restokes;  // WRITEDUSTDENSITY: interpolation again after the update (SourceEuler.c:526-531)
-  // processing order: particles sorted by cell once per DT, so that a warp's
-  // grid gathers hit neighbouring cells (results do not depend on the order)
-  int *perm, *key, *cell_count, *cell_bsum;
-  int ncells;  // nr*ns + 1 (the last bucket holds particles off the grid)
+  // Storage order: once per DT the particles are moved into cell order (a
+  // counting sort), so that a warp's grid gathers hit neighbouring cells and
+  // its particle loads and stores stay coalesced.  orig[slot] is the
+  // reference's index of the particle in a slot: the random stream and the
+  // downloads follow it; no result depends on the storage order.
+  int *orig, *perm, *key, *cell_count, *cell_bsum;
+  double *pscratch;  // 7 n doubles: the moved arrays
+  int *oscratch;     // n: the moved orig
+  int ncells;        // nr*ns + 1 (the last bucket holds particles off the grid)
+  // first guess of a particle's ring from the grid law (log or arithmetic),
+  // corrected exactly against the radii
+  double ring_r0, ring_inv_r0, ring_inv_step;
 };
 
 // launchers (fb_gas.cu)
@@ -189,7 +197,9 @@ void fb_launch_ring_mean(const double *f, int nr, int ns, double *out, cudaStrea
 void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s, cudaEvent_t planets_done);
 void fb_launch_dust_interpolation_only(const KP &k, const PP &pp, cudaStream_t s);
 int  fb_dust_launches(const PP &pp);
-int  fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s);  // returns launches
+int fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s);  // returns launches
+void fb_launch_dust_iota(const PP &pp, cudaStream_t s);
+void fb_launch_dust_to_reference_order(const PP &pp, const double *src, double *dst, cudaStream_t s);
 int  fb_sg_launches(const fb_sg *sg);  // kernels per fb_sg_accel + update
 void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s);
 void fb_sg_cols(fb_sg *sg, cudaStream_t s);

@@ -78,36 +78,39 @@ static __device__ __forceinline__ double tsc_weight(double d, double delta)
 }
 
 // The reference finds rings by linear searches over the radii (Dsys.c:364,
-// DustUpdate.c:73, Viscosity.c:31); the same indices come from binary
-// searches over the sorted tables here.
-// first index in [0, n) with a[idx] > x, or n (x >= a[idx] keeps searching)
-static __device__ __forceinline__ int first_above(const double *a, int n, double x)
+// DustUpdate.c:73, Viscosity.c:31).  The same indices come from a first
+// guess by the grid law and a correction against the sorted radii.
+static __device__ __forceinline__ int ring_guess(const PP &pp, double x, int n)
 {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (x >= a[mid]) lo = mid + 1; else hi = mid;
-  }
-  return lo;
+  const double u = pp.log_grid ? log(x * pp.ring_inv_r0) * pp.ring_inv_step : (x - pp.ring_r0) * pp.ring_inv_step;
+  return (u > 0.0) ? (int)fmin(u, (double)(n - 1)) : 0;
 }
-// first index in [0, n) with a[idx] >= x, or n
-static __device__ __forceinline__ int first_not_below(const double *a, int n, double x)
+// largest index g in [0, n) with a[g] <= x, given a[0] <= x (the linear
+// search `while (x >= a[i] && i <= n-1) i++; i--`)
+static __device__ __forceinline__ int last_not_above(const PP &pp, const double *a, int n, double x)
 {
-  int lo = 0, hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (a[mid] < x) lo = mid + 1; else hi = mid;
-  }
-  return lo;
+  int g = ring_guess(pp, x, n);
+  while (g > 0 && a[g] > x) g--;
+  while (g < n - 1 && a[g + 1] <= x) g++;
+  return g;
+}
+// first index in [0, n - 1) with a[idx] >= x, else n - 1 (the search
+// `while (a[i] < x) i++` stopped at the last entry)
+static __device__ __forceinline__ int first_not_below_clamped(const PP &pp, const double *a, int n, double x)
+{
+  int g = ring_guess(pp, x, n);
+  while (g > 0 && a[g - 1] >= x) g--;
+  while (g < n - 1 && a[g] < x) g++;
+  return g;
 }
 
 // FViscosity (src/Viscosity.c:23-69) at a particle radius.  The reference's
 // search `while (GlobalRmed[i] < rad) i++` has no upper bound and runs past
 // the last ring for radii beyond Rmed[nr-1]; here it stops at the last ring.
-static __device__ double viscosity_at(const KP &k, double rad)
+static __device__ double viscosity_at(const KP &k, const PP &pp, double rad)
 {
   if (k.visc_mode == 1) {
-    const int i = first_not_below(k.rmed, k.nr - 1, rad);  // <= nr-1
+    const int i = first_not_below_clamped(pp, k.rmed, k.nr, rad);  // <= nr-1
     return k.alpha * k.gcs[i] * k.gcs[i] * pow(rad, 1.5);
   }
   return (k.visc_mode == 2) ? k.nu_const : 0.0;
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(D_BS) k_dust_drift(KP k, PP pp)
     pp.r[q] = rn;
     pp.th[q] = th;
   }
-  pp.flag[q] = flag;
+  pp.flag[pp.orig[q]] = flag;  // in the reference's order, for the kick ranks
 }
 
 // ------------------------------------------------------- 2. scans
@@ -327,20 +330,20 @@ static __device__ __forceinline__ void record_stopping_time(const PP &pp, double
 // mode 1: the interpolation call of main.c:287 (Stokes numbers only).
 __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
 {
-  const int t = blockIdx.x * D_BS + threadIdx.x;
-  if (t >= pp.n) return;
-  const int q = pp.perm[t];
+  const int q = blockIdx.x * D_BS + threadIdx.x;  // storage slot
+  if (q >= pp.n) return;
+  const int qr = (mode == 0) ? pp.orig[q] : 0;  // the reference's index: kick flag and rank
   const int ns = k.ns, nr = k.nr;
   const double rinf0 = k.rinf[0], rsupl = k.rsup[nr - 1];
   double r = pp.r[q], th = pp.th[q];
   // ---- turbulent kick (DustUpdate.c:56-105, Charnoz et al. 2011 eq. 21)
-  if (mode == 0 && pp.flag[q]) {
+  if (mode == 0 && pp.flag[qr]) {
     const double timestep = 2.0 * k.ctl->dt;
     const double St = pp.st[q];
-    const double visc = viscosity_at(k, r);
+    const double visc = viscosity_at(k, pp, r);
     const double D_dust = visc * (1.0 + 4.0 * (St * St)) * pow(1. + St * St, -2.0);
     // `while (r >= Rinf[ip] && ip <= nr-1) ip++; ip--` (r >= Rinf[0] here)
-    const int ip = first_above(k.rinf, nr, r) - 1;
+    const int ip = last_not_above(pp, k.rinf, nr, r);
     int jp = (int)floor(ns * (th - pp.aziinf0) / (pp.azisupl - pp.aziinf0));
     if (jp == ns) jp = 0;
     jp = min(max(jp, 0), ns - 1);
@@ -349,7 +352,7 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
     const size_t lpjm = (jp == 0) ? (size_t)ip * ns + ns - 1 : lp - 1;
     // this particle's deviates (see the head of the file)
     const fb_dust_ctl *d = pp.dc;
-    const long long M = d->kicks + pp.kidx[q] + pp.kick_bsum[q / SCAN_BS];
+    const long long M = d->kicks + pp.kidx[qr] + pp.kick_bsum[qr / SCAN_BS];
     const long long t = M / 2;
     const int odd = (int)(M & 1ll);
     double xr, xp;
@@ -378,7 +381,7 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
   // ---- 1) cell of the particle (Dsys.c:363-372)
   const double rp = r, tp = th;
   // `while (rp >= Rinf[ip]) ip++; ip--` with Rinf[0] <= rp < Rinf[nr]
-  const int ip = first_above(k.rinf, nr + 1, rp) - 1;
+  const int ip = last_not_above(pp, k.rinf, nr + 1, rp);
   int jp = (int)floor(ns * (tp - pp.aziinf0) / (pp.azisupl - pp.aziinf0));
   if (jp == ns) jp = 0;
   jp = min(max(jp, 0), ns - 1);
@@ -564,7 +567,7 @@ __global__ void __launch_bounds__(D_BS) k_cell_key(KP k, PP pp)
   const int nr = k.nr, ns = k.ns;
   int key = nr * ns;
   if (r >= k.rinf[0] && r < k.rsup[nr - 1]) {
-    const int ip = first_above(k.rinf, nr + 1, r) - 1;
+    const int ip = last_not_above(pp, k.rinf, nr + 1, r);
     int jp = (int)floor(ns * (th - pp.aziinf0) / (pp.azisupl - pp.aziinf0));
     jp = min(max(jp, 0), ns - 1);
     key = ip * ns + jp;
@@ -590,6 +593,40 @@ __global__ void __launch_bounds__(D_BS) k_cell_scatter(PP pp)
   pp.perm[pos] = q;
 }
 
+// Moves the particles into the sorted order: slot t takes old slot perm[t].
+__global__ void __launch_bounds__(D_BS) k_cell_gather(PP pp)
+{
+  const int t = blockIdx.x * D_BS + threadIdx.x;
+  if (t >= pp.n) return;
+  const int s = pp.perm[t];
+  const size_t n = pp.n;
+  double *x = pp.pscratch;
+  x[t] = pp.r[s];
+  x[n + t] = pp.th[s];
+  x[2 * n + t] = pp.vr[s];
+  x[3 * n + t] = pp.vth[s];
+  x[4 * n + t] = pp.l[s];
+  x[5 * n + t] = pp.size[s];
+  x[6 * n + t] = pp.st[s];
+  pp.oscratch[t] = pp.orig[s];
+}
+
+__global__ void __launch_bounds__(D_BS) k_cell_copy(PP pp)
+{
+  const int t = blockIdx.x * D_BS + threadIdx.x;
+  if (t >= pp.n) return;
+  const size_t n = pp.n;
+  const double *x = pp.pscratch;
+  pp.r[t] = x[t];
+  pp.th[t] = x[n + t];
+  pp.vr[t] = x[2 * n + t];
+  pp.vth[t] = x[3 * n + t];
+  pp.l[t] = x[4 * n + t];
+  pp.size[t] = x[5 * n + t];
+  pp.st[t] = x[6 * n + t];
+  pp.orig[t] = pp.oscratch[t];
+}
+
 int fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s)
 {
   const int nb = (pp.n + D_BS - 1) / D_BS, nc = pp.ncells, ncb = (nc + SCAN_BS - 1) / SCAN_BS;
@@ -599,7 +636,31 @@ int fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s)
   k_scan_top_only<<<1, SCAN_BS, 0, s>>>(pp.cell_bsum, ncb);
   k_scan_add<<<ncb, SCAN_BS, 0, s>>>(pp.cell_count, pp.cell_bsum, nc);
   k_cell_scatter<<<nb, D_BS, 0, s>>>(pp);
-  return 5;
+  k_cell_gather<<<nb, D_BS, 0, s>>>(pp);
+  k_cell_copy<<<nb, D_BS, 0, s>>>(pp);
+  return 7;
+}
+
+// storage slots in the reference's order (after an upload)
+__global__ void __launch_bounds__(D_BS) k_iota(int *v, int n)
+{
+  const int t = blockIdx.x * D_BS + threadIdx.x;
+  if (t < n) v[t] = t;
+}
+void fb_launch_dust_iota(const PP &pp, cudaStream_t s)
+{
+  k_iota<<<(pp.n + D_BS - 1) / D_BS, D_BS, 0, s>>>(pp.orig, pp.n);
+}
+
+// dst[orig[t]] = src[t]: one particle array back in the reference's order
+__global__ void __launch_bounds__(D_BS) k_to_reference_order(const int *orig, const double *src, double *dst, int n)
+{
+  const int t = blockIdx.x * D_BS + threadIdx.x;
+  if (t < n) dst[orig[t]] = src[t];
+}
+void fb_launch_dust_to_reference_order(const PP &pp, const double *src, double *dst, cudaStream_t s)
+{
+  k_to_reference_order<<<(pp.n + D_BS - 1) / D_BS, D_BS, 0, s>>>(pp.orig, src, dst, pp.n);
 }
 
 // ---------------------------------------------------------- launchers
