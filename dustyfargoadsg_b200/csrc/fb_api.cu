@@ -29,6 +29,8 @@ struct fb_ctx {
   cudaEvent_t ev0, ev1;
   cudaStream_t st_planets;            // branch of the planets' step (k_planets)
   cudaEvent_t ev_fork, ev_planets;    // its start and end within a substep
+  cudaStream_t st_sg;                 // branch of the self-gravity convolution
+  cudaEvent_t ev_sg_fork, ev_sg_done;
   KP k;
   std::vector<void *> allocs;
   fb_ctl *d_ctl;
@@ -253,7 +255,10 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   cudaEventCreate(&ctx->ev1);
   if (cudaStreamCreateWithFlags(&ctx->st_planets, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ctx->ev_planets, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&ctx->ev_planets, cudaEventDisableTiming) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&ctx->st_sg, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_sg_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_sg_done, cudaEventDisableTiming) != cudaSuccess) {
     fb_destroy(ctx);
     return FB_ERR_CUDA;
   }
@@ -440,6 +445,9 @@ extern "C" int fb_destroy(fb_ctx *ctx)
   if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
   if (ctx->ev_planets) cudaEventDestroy(ctx->ev_planets);
   if (ctx->st_planets) cudaStreamDestroy(ctx->st_planets);
+  if (ctx->ev_sg_fork) cudaEventDestroy(ctx->ev_sg_fork);
+  if (ctx->ev_sg_done) cudaEventDestroy(ctx->ev_sg_done);
+  if (ctx->st_sg) cudaStreamDestroy(ctx->st_sg);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->gdt_exec) cudaGraphExecDestroy(ctx->gdt_exec);
   if (ctx->gdt) cudaGraphDestroy(ctx->gdt);
@@ -545,6 +553,23 @@ static int enqueue_substep(fb_ctx *ctx)
   KP &k = ctx->k;
   cudaStream_t s = ctx->st;
   int npt = 0;
+  // The self-gravity convolution reads only the density, which no kernel
+  // changes before the transport: outside the per-stage profile it runs on
+  // a branch of its own from the start of the substep, beside the CFL,
+  // potential and SubStep1 kernels, and joins before its velocity kicks.
+  const bool sg_branch = k.self_gravity && !ctx->profiling;
+  if (sg_branch) {
+    cudaEventRecord(ctx->ev_sg_fork, s);
+    cudaStreamWaitEvent(ctx->st_sg, ctx->ev_sg_fork, 0);
+    fb_sg_rows_fwd(ctx->sg, k, k.rho, ctx->st_sg);
+    fb_sg_cols(ctx->sg, ctx->st_sg);
+    fb_sg_rows_inv(ctx->sg, k, k.rho, ctx->st_sg);
+    cudaEventRecord(ctx->ev_sg_done, ctx->st_sg);
+    ctx->launches += 3;
+    ctx->pcount[ST_SG] += 1;
+    ctx->pcount[ST_SGCOLS] += 1;
+    ctx->pcount[ST_SGINV] += 1;
+  }
   STAGE(ST_CFL, 1, fb_launch_cfl(k, s));  // ConditionCFL + the controller (last CTA)
   // the planets' step on a branch of its own: no gas kernel of the substep
   // reads the positions it writes; joined before the particles' velocity
@@ -563,9 +588,13 @@ static int enqueue_substep(fb_ctx *ctx)
   STAGE(ST_POT, 1, fb_launch_potential(k, s));
   STAGE(ST_SUB1, 1, fb_launch_substep1(k, s));
   if (k.self_gravity) {
-    STAGE(ST_SG, 1, fb_sg_rows_fwd(ctx->sg, k, k.rho, s));
-    STAGE(ST_SGCOLS, 1, fb_sg_cols(ctx->sg, s));
-    STAGE(ST_SGINV, 1, fb_sg_rows_inv(ctx->sg, k, k.rho, s));
+    if (sg_branch) {
+      cudaStreamWaitEvent(s, ctx->ev_sg_done, 0);
+    } else {
+      STAGE(ST_SG, 1, fb_sg_rows_fwd(ctx->sg, k, k.rho, s));
+      STAGE(ST_SGCOLS, 1, fb_sg_cols(ctx->sg, s));
+      STAGE(ST_SGINV, 1, fb_sg_rows_inv(ctx->sg, k, k.rho, s));
+    }
     STAGE(ST_SGUPD, 1, fb_sg_update_velocities(k, s));
   }
   if (k.visc_mode) {
@@ -1000,6 +1029,8 @@ struct fb_batch {
   cudaEvent_t ev0, ev1;
   cudaStream_t st_planets;            // branch of the planets' step (k_planets)
   cudaEvent_t ev_fork, ev_planets;    // its start and end within a substep
+  cudaStream_t st_sg;                 // branch of the self-gravity convolution
+  cudaEvent_t ev_sg_fork, ev_sg_done;
   cudaGraph_t g;
   cudaGraphExec_t ge;
 };
