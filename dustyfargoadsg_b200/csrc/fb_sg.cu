@@ -5,8 +5,10 @@
 // St = Sr r/r0 with the kernels Kr, Kt on a (2 Nr) x Ns periodic grid (the
 // radial direction zero-padded), through unnormalised FFTW transforms:
 //     A = IFFT2( -G FFT2(K) . FFT2(S) ),   normalised by rstep tstep/(2Nr Ns).
-// Here the transforms are our own Stockham mixed-radix (2,3,4,5) FFTs, one
-// CTA per 1-D transform with the line in shared memory:
+// Here the transforms are our own Stockham mixed-radix FFTs (radix 16 in
+// registers first, then 4, 2, 3, 5; lines padded by one slot per 16 in
+// shared memory against bank conflicts; per-pass twiddle tables read with
+// consecutive entries per warp), one CTA per 1-D transform or pair:
 //   1. sg_rows_fwd : per ring i < Nr, one complex FFT of z = Sr + i St along
 //      phi, split into the two half spectra (rows >= Nr are zero, so they
 //      are never transformed);
@@ -25,6 +27,7 @@
 #include "fb_dev.cuh"
 
 #define SG_BS 256
+#define SG_ROW_BS 128  // threads of a row transform (radix-16 passes: n/16 butterflies)
 #define SG_MAXST 16
 
 struct fb_fft_plan {
@@ -43,6 +46,9 @@ struct fb_sg {
   int nr, ns, m, nk;        // m = 2 nr, nk = ns/2 + 1
   fb_fft_plan prow, pcol;
   int p2, lgm;              // m = 2^lgm, lgm >= 4: the radix-16 column kernel
+  double2 *tw2;             // its per-pass twiddle tables
+  FftArgs frow;             // the row passes (radix 16 first) and their tables
+  double2 *twr;
   FftArgs fc2;              // its passes (16, ..., 16, then 4 and/or 2)
   double2 *xr, *xt;         // half spectra after the row pass, [i][k], i < nr
   double2 *khr, *kht;       // kernel spectra, [k][m]
@@ -76,6 +82,37 @@ static int make_plan(fb_fft_plan *p, int n)
   }
   if (cudaMalloc(&p->tw, n * sizeof(double2)) != cudaSuccess) return FB_ERR_NOMEM;
   cudaMemcpy(p->tw, h.data(), n * sizeof(double2), cudaMemcpyHostToDevice);
+  return FB_OK;
+}
+
+// Passes of a line of n points, radix 16 first and then 4, 2, 3, 5, with
+// their twiddle tables back to back: pass (R, L) holds exp(-2 pi i r jm /
+// (L R)) at [r][jm], r < R, jm < L.
+static int make_pass_tables(FftArgs *a, double2 **dtab, int n)
+{
+  a->n = n;
+  a->nst = 0;
+  int rem = n;
+  while (rem % 16 == 0 && a->nst < SG_MAXST) { a->radix[a->nst++] = 16; rem /= 16; }
+  int tail[SG_MAXST];
+  const int nt = plan_radices(rem, tail);
+  if (nt < 0 || a->nst + nt > SG_MAXST) return FB_ERR_UNSUPPORTED;
+  for (int q = 0; q < nt; q++) a->radix[a->nst++] = tail[q];
+  for (int q = a->nst; q < SG_MAXST; q++) a->radix[q] = 1;
+  std::vector<double2> tab;
+  int L = 1;
+  for (int st = 0; st < a->nst; st++) {
+    const int R = a->radix[st];
+    for (int r = 0; r < R; r++)
+      for (int jm = 0; jm < L; jm++) {
+        const double ang = 2.0 * M_PI * (double)(r * jm) / (double)(L * R);
+        tab.push_back(make_double2(cos(ang), -sin(ang)));
+      }
+    L *= R;
+  }
+  if (cudaMalloc(dtab, tab.size() * sizeof(double2)) != cudaSuccess) return FB_ERR_NOMEM;
+  cudaMemcpy(*dtab, tab.data(), tab.size() * sizeof(double2), cudaMemcpyHostToDevice);
+  a->tw = *dtab;
   return FB_OK;
 }
 
@@ -199,23 +236,124 @@ static __device__ double2 *fft_smem_t(double2 *x, double2 *y, const FftArgs &a)
   return x;
 }
 
-static __device__ __forceinline__ double2 *fft_smem(double2 *x, double2 *y, const FftArgs &a, int inv)
+
+// Radix-R DFT of v[0..R-1] in place (R = 2, 3, 4, 5), natural output order.
+template <int R, int INV>
+static __device__ __forceinline__ void dft_small(double2 *v)
 {
-  return inv ? fft_smem_t<1, 1>(x, y, a) : fft_smem_t<0, 1>(x, y, a);
+  if (R == 2) {
+    const double2 t0 = v[0];
+    v[0] = cadd(t0, v[1]);
+    v[1] = csub(t0, v[1]);
+  } else if (R == 4) {
+    const double2 A = cadd(v[0], v[2]), B = csub(v[0], v[2]);
+    const double2 Cc = cadd(v[1], v[3]), D = crot(csub(v[1], v[3]), INV);
+    v[0] = cadd(A, Cc);
+    v[2] = csub(A, Cc);
+    v[1] = cadd(B, D);
+    v[3] = csub(B, D);
+  } else if (R == 3) {
+    const double h = 0.86602540378443864676;  // sqrt(3)/2
+    const double2 t1 = cadd(v[1], v[2]);
+    const double2 t2 = csub(v[0], cscale(t1, 0.5));
+    const double2 t3 = cscale(csub(v[1], v[2]), INV ? h : -h);
+    v[0] = cadd(v[0], t1);
+    v[1] = make_double2(t2.x - t3.y, t2.y + t3.x);
+    v[2] = make_double2(t2.x + t3.y, t2.y - t3.x);
+  } else if (R == 5) {
+    const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
+    const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
+    const double sg = INV ? 1.0 : -1.0;
+    const double cs[5] = {1.0, c1, c2, c2, c1};
+    const double sn[5] = {0.0, s1, s2, -s2, -s1};
+    double2 in[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) in[q] = v[q];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+      double re = 0.0, im = 0.0;
+#pragma unroll
+      for (int q = 0; q < 5; q++) {
+        const int e = (k * q) % 5;
+        re += in[q].x * cs[e] - in[q].y * (sg * sn[e]);
+        im += in[q].x * (sg * sn[e]) + in[q].y * cs[e];
+      }
+      v[k] = make_double2(re, im);
+    }
+  }
+}
+
+static __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
+template <int INV> static __device__ __forceinline__ void dft16(double2 *v);
+
+// One radix-R Stockham pass of a line of n points between two buffers padded
+// by one slot per 16; twp is the pass's twiddle table, R rows of L entries
+// (exp(-2 pi i r jm / (L R)) at [r][jm], read with consecutive jm per warp).
+template <int R, int INV>
+static __device__ __forceinline__ void fft_pass_p(const double2 *__restrict__ x, double2 *__restrict__ y, int n,
+                                                  int L, const double2 *__restrict__ twp)
+{
+  const int nb = n / R;
+  for (int j = threadIdx.x; j < nb; j += blockDim.x) {
+    double2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = x[pad16(j + r * nb)];
+    const int jm = j % L;
+    if (L > 1) {
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        double2 w = twp[r * L + jm];
+        if (INV) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    if (R == 16) dft16<INV>(v); else dft_small<R, INV>(v);
+    const int idxD = (j - jm) * R + jm;
+#pragma unroll
+    for (int r = 0; r < R; r++) y[pad16(idxD + r * L)] = (R == 16) ? v[4 * (r & 3) + (r >> 2)] : v[r];
+  }
+}
+
+// Stockham FFT of one line in padded shared memory with the passes of a
+// (radix 16 first, then 4, 2, 3, 5); returns the buffer holding the result.
+template <int INV>
+static __device__ double2 *fft_line_p(double2 *x, double2 *y, const FftArgs &a)
+{
+  const int n = a.n;
+  int L = 1, off = 0;
+  for (int st = 0; st < a.nst; st++) {
+    const int R = a.radix[st];
+    const double2 *twp = a.tw + off;
+    __syncthreads();
+    switch (R) {
+      case 16: fft_pass_p<16, INV>(x, y, n, L, twp); break;
+      case 4: fft_pass_p<4, INV>(x, y, n, L, twp); break;
+      case 2: fft_pass_p<2, INV>(x, y, n, L, twp); break;
+      case 3: fft_pass_p<3, INV>(x, y, n, L, twp); break;
+      default: fft_pass_p<5, INV>(x, y, n, L, twp); break;
+    }
+    double2 *t = x;
+    x = y;
+    y = t;
+    off += R * L;
+    L *= R;
+  }
+  __syncthreads();
+  return x;
 }
 
 // ------------------------------------------------------------------ kernels
 // Row pass of compute_fftdensity (sgdens.c:52-68) + the forward transform
 // along phi.  in_r/in_t given: real rows are in_r, in_t (kernel setup);
 // otherwise Sr, St are built from the density.
-__global__ void __launch_bounds__(SG_BS) sg_rows_fwd(FftArgs fa, int nrows, int ns, int nk,
+__global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_fwd(FftArgs fa, int nrows, int ns, int nk,
                                                       const double *dens, const double *sq,
                                                       const double *rmed, double r0,
                                                       const double *in_r, const double *in_t,
                                                       double2 *out_r, double2 *out_t)
 {
   extern __shared__ double2 sm[];
-  double2 *x = sm, *y = sm + ns;
+  double2 *x = sm, *y = sm + ns + ns / 16;  // padded lines
   const int i = blockIdx.x;
   for (int j = threadIdx.x; j < ns; j += blockDim.x) {
     double a, b;
@@ -226,11 +364,11 @@ __global__ void __launch_bounds__(SG_BS) sg_rows_fwd(FftArgs fa, int nrows, int 
       a = dens[(size_t)i * ns + j] * sq[i];   // SGP_Sr = dens*sqrt(Rmed/R0)
       b = a * rmed[i] / r0;                   // SGP_St = Sr*Rmed/R0
     }
-    x[j] = make_double2(a, b);
+    x[pad16(j)] = make_double2(a, b);
   }
-  double2 *Z = fft_smem(x, y, fa, 0);
+  double2 *Z = fft_line_p<0>(x, y, fa);
   for (int k = threadIdx.x; k < nk; k += blockDim.x) {
-    const double2 zk = Z[k], zc = Z[(ns - k) % ns];
+    const double2 zk = Z[pad16(k)], zc = Z[pad16((ns - k) % ns)];
     // A = (Z[k] + conj Z[-k]) / 2 ; B = (Z[k] - conj Z[-k]) / (2i)
     const double2 A = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y - zc.y));
     const double2 B = make_double2(0.5 * (zk.y + zc.y), -0.5 * (zk.x - zc.x));
@@ -317,7 +455,6 @@ __global__ void __launch_bounds__(SG_BS) sg_cols(FftArgs fa, int nrows_in, int n
 // slot per 16 (index i at i + i/16), which keeps the stride-16 stores of
 // the first pass free of bank conflicts.  CTAs of SG_KC2 * m / 16 threads.
 #define SG_KC2 2
-static __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 
 template <int INV>
 static __device__ __forceinline__ void dft4(double2 &a, double2 &b, double2 &c, double2 &d)
@@ -355,7 +492,7 @@ static __device__ __forceinline__ void dft16(double2 *v)
 }
 
 // One radix-R Stockham pass over the padded lines of m = 2^lgm points
-// (stride mp); tw holds the m twiddles in shared memory.
+// (stride mp); tw is the pass's twiddle table, R rows of L entries.
 template <int R, int INV>
 static __device__ __forceinline__ void col_pass(double2 *X, int lgm, int mp, int L, const double2 *tw)
 {
@@ -369,10 +506,10 @@ static __device__ __forceinline__ void col_pass(double2 *X, int lgm, int mp, int
 #pragma unroll
     for (int r = 0; r < R; r++) v[b * R + r] = x[pad16(j + r * nb)];
     if (L > 1) {
-      const int jm = j & (L - 1), ts = nb / L;  // m / (L R)
+      const int jm = j & (L - 1);
 #pragma unroll
       for (int r = 1; r < R; r++) {
-        double2 w = tw[r * jm * ts];  // r*jm*ts < m
+        double2 w = tw[r * L + jm];  // exp(-2 pi i r jm / (L R)): consecutive in jm
         if (INV) w.y = -w.y;
         v[b * R + r] = cmul(v[b * R + r], w);
       }
@@ -400,22 +537,24 @@ static __device__ __forceinline__ void col_pass(double2 *X, int lgm, int mp, int
 }
 
 template <int INV>
-static __device__ void col_fft(double2 *X, int lgm, const FftArgs &a, const double2 *tw)
+static __device__ void col_fft(double2 *X, int lgm, const FftArgs &a)
 {
   const int m = 1 << lgm, mp = m + m / 16;
-  int L = 1;
+  int L = 1, off = 0;
   for (int st = 0; st < a.nst; st++) {
     const int R = a.radix[st];
+    const double2 *tw = a.tw + off;  // the per-pass tables follow each other
     if (R == 16) col_pass<16, INV>(X, lgm, mp, L, tw);
     else if (R == 4) col_pass<4, INV>(X, lgm, mp, L, tw);
     else col_pass<2, INV>(X, lgm, mp, L, tw);
+    off += R * L;
     L *= R;
   }
 }
 
 // Every thread moves 16 points in each phase (T = SG_KC2 m / 16), with all
 // of a phase's global loads issued before their first use.
-__global__ void __launch_bounds__(256) sg_cols_p2(FftArgs fa, int lgm, int nrows_in, int nk, int mode,
+__global__ void __launch_bounds__(128, 4) sg_cols_p2(FftArgs fa, int lgm, int nrows_in, int nk, int mode,
                                                  double2 *data_r, double2 *data_t, double2 *kh_r, double2 *kh_t)
 {
   extern __shared__ double2 sm[];
@@ -424,21 +563,20 @@ __global__ void __launch_bounds__(256) sg_cols_p2(FftArgs fa, int lgm, int nrows
   const int which = blockIdx.y;  // 0: r, 1: t
   double2 *data = which ? data_t : data_r;
   double2 *kh = which ? kh_t : kh_r;
-  double2 *X = sm, *tw = sm + SG_KC2 * mp;
+  double2 *X = sm;
   double2 v[16];
 #pragma unroll
   for (int q = 0; q < 16; q++) {
     const int t = tid + q * T, i = t >> 1, c = t & 1, k = k0 + c;  // SG_KC2 == 2
     v[q] = (i < nrows_in && k < nk) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
   }
-  for (int t = tid; t < m; t += T) tw[t] = fa.tw[t];
 #pragma unroll
   for (int q = 0; q < 16; q++) {
     const int t = tid + q * T, i = t >> 1, c = t & 1;
     X[c * mp + pad16(i)] = v[q];
   }
   __syncthreads();
-  col_fft<0>(X, lgm, fa, tw);
+  col_fft<0>(X, lgm, fa);
   if (mode == 0) {
 #pragma unroll
     for (int q = 0; q < 16; q++) {
@@ -460,7 +598,7 @@ __global__ void __launch_bounds__(256) sg_cols_p2(FftArgs fa, int lgm, int nrows
     X[c * mp + pad16(i)] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
   }
   __syncthreads();
-  col_fft<1>(X, lgm, fa, tw);
+  col_fft<1>(X, lgm, fa);
 #pragma unroll
   for (int q = 0; q < 16; q++) {
     const int t = tid + q * T, i = t >> 1, c = t & 1, k = k0 + c;
@@ -469,14 +607,14 @@ __global__ void __launch_bounds__(256) sg_cols_p2(FftArgs fa, int lgm, int nrows
 }
 
 // Inverse row pass + sgacc.c:138-161: normalisation, self-force.
-__global__ void __launch_bounds__(SG_BS) sg_rows_inv(FftArgs fa, int ns, int nk, const double2 *wr,
+__global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_inv(FftArgs fa, int ns, int nk, const double2 *wr,
                                                       const double2 *wt, const double *normr,
                                                       const double *normt, const double *dens,
                                                       double selfk_rstep, double selfk_tstep,
                                                       double eps, double *accr, double *acct)
 {
   extern __shared__ double2 sm[];
-  double2 *x = sm, *y = sm + ns;
+  double2 *x = sm, *y = sm + ns + ns / 16;  // padded lines
   const int i = blockIdx.x;
   for (int k = threadIdx.x; k < ns; k += blockDim.x) {
     double2 a, b;
@@ -490,16 +628,17 @@ __global__ void __launch_bounds__(SG_BS) sg_rows_inv(FftArgs fa, int ns, int nk,
       a.y = -a.y;
       b.y = -b.y;
     }
-    x[k] = make_double2(a.x - b.y, a.y + b.x);  // a + i b
+    x[pad16(k)] = make_double2(a.x - b.y, a.y + b.x);  // a + i b
   }
-  double2 *A = fft_smem(x, y, fa, 1);
+  double2 *A = fft_line_p<1>(x, y, fa);
   const double nrm_r = normr[i], nrm_t = normt[i];
   for (int j = threadIdx.x; j < ns; j += blockDim.x) {
     const size_t l = (size_t)i * ns + j;
-    double ar = A[j].x * nrm_r;
+    const double2 aj = A[pad16(j)];
+    double ar = aj.x * nrm_r;
     ar += FB_G * dens[l] * selfk_rstep * selfk_tstep / eps;
     accr[l] = ar;
-    acct[l] = A[j].y * nrm_t;
+    acct[l] = aj.y * nrm_t;
   }
 }
 
@@ -543,21 +682,36 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   if (ns % 2 != 0) { delete sg; return FB_ERR_UNSUPPORTED; }
   int rc = make_plan(&sg->prow, ns);
   if (!rc) rc = make_plan(&sg->pcol, m);
+  if (!rc) rc = make_pass_tables(&sg->frow, &sg->twr, ns);
   if (rc) { fb_sg_destroy(sg); return rc; }
-  sg->smem_row = 2 * (size_t)ns * sizeof(double2);
+  sg->smem_row = 2 * ((size_t)ns + ns / 16) * sizeof(double2);  // two padded lines
   sg->smem_col = 2 * (size_t)SG_KC * m * sizeof(double2);
-  sg->p2 = (m >= 16 && m <= 2048 && (m & (m - 1)) == 0);
+  sg->p2 = (m >= 16 && m <= 1024 && (m & (m - 1)) == 0);  // CTAs of 2m/16 <= 128 threads
   if (sg->p2) {
     FftArgs &a = sg->fc2;
     a.n = m;
-    a.tw = sg->pcol.tw;
     a.nst = 0;
     int rem = m;
     while (rem % 16 == 0) { a.radix[a.nst++] = 16; rem /= 16; }
     if (rem >= 4) { a.radix[a.nst++] = 4; rem /= 4; }
     if (rem == 2) { a.radix[a.nst++] = 2; rem /= 2; }
     for (int q = a.nst; q < SG_MAXST; q++) a.radix[q] = 1;
-    sg->smem_col2 = ((size_t)SG_KC2 * (m + m / 16) + m) * sizeof(double2);
+    // per-pass twiddle tables: entry [r][jm] = exp(-2 pi i r jm / (L R))
+    std::vector<double2> tab;
+    int L = 1;
+    for (int st = 0; st < a.nst; st++) {
+      const int R = a.radix[st];
+      for (int r = 0; r < R; r++)
+        for (int jm = 0; jm < L; jm++) {
+          const double ang = 2.0 * M_PI * (double)(r * jm) / (double)(L * R);
+          tab.push_back(make_double2(cos(ang), -sin(ang)));
+        }
+      L *= R;
+    }
+    if (cudaMalloc(&sg->tw2, tab.size() * sizeof(double2)) != cudaSuccess) { fb_sg_destroy(sg); return FB_ERR_NOMEM; }
+    cudaMemcpy(sg->tw2, tab.data(), tab.size() * sizeof(double2), cudaMemcpyHostToDevice);
+    a.tw = sg->tw2;
+    sg->smem_col2 = (size_t)SG_KC2 * (m + m / 16) * sizeof(double2);
     sg->lgm = 0;
     while ((1 << sg->lgm) < m) sg->lgm++;
   }
@@ -629,8 +783,8 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   if (!ok) { cudaFree(dkr); cudaFree(dkt); cudaFree(hr); cudaFree(ht); fb_sg_destroy(sg); return FB_ERR_NOMEM; }
   cudaMemcpy(dkr, kr.data(), kr.size() * sizeof(double), cudaMemcpyHostToDevice);
   cudaMemcpy(dkt, kt.data(), kt.size() * sizeof(double), cudaMemcpyHostToDevice);
-  FftArgs fr = fft_args(sg->prow), fc = fft_args(sg->pcol);
-  sg_rows_fwd<<<m, SG_BS, sg->smem_row, s>>>(fr, m, ns, nk, NULL, NULL, NULL, 1.0, dkr, dkt, hr, ht);
+  FftArgs fc = fft_args(sg->pcol);
+  sg_rows_fwd<<<m, SG_ROW_BS, sg->smem_row, s>>>(sg->frow, m, ns, nk, NULL, NULL, NULL, 1.0, dkr, dkt, hr, ht);
   if (sg->p2)
     sg_cols_p2<<<dim3((nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * m / 16, sg->smem_col2, s>>>(sg->fc2, sg->lgm, m, nk, 0,
                                                                                           hr, ht, sg->khr, sg->kht);
@@ -646,7 +800,7 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
 void fb_sg_destroy(fb_sg *sg)
 {
   if (!sg) return;
-  cudaFree(sg->prow.tw); cudaFree(sg->pcol.tw);
+  cudaFree(sg->prow.tw); cudaFree(sg->pcol.tw); cudaFree(sg->tw2); cudaFree(sg->twr);
   cudaFree(sg->xr); cudaFree(sg->xt); cudaFree(sg->khr); cudaFree(sg->kht);
   cudaFree(sg->sq); cudaFree(sg->rr); cudaFree(sg->nr_accr); cudaFree(sg->nr_acct);
   delete sg;
@@ -656,8 +810,7 @@ void fb_sg_destroy(fb_sg *sg)
 void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 {
   (void)k;
-  FftArgs fr = fft_args(sg->prow);
-  sg_rows_fwd<<<sg->nr, SG_BS, sg->smem_row, s>>>(fr, sg->nr, sg->ns, sg->nk, dens, sg->sq, sg->rr, sg->r0,
+  sg_rows_fwd<<<sg->nr, SG_ROW_BS, sg->smem_row, s>>>(sg->frow, sg->nr, sg->ns, sg->nk, dens, sg->sq, sg->rr, sg->r0,
                                                    NULL, NULL, sg->xr, sg->xt);
 }
 
@@ -675,8 +828,7 @@ void fb_sg_cols(fb_sg *sg, cudaStream_t s)
 
 void fb_sg_rows_inv(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 {
-  FftArgs fr = fft_args(sg->prow);
-  sg_rows_inv<<<sg->nr, SG_BS, sg->smem_row, s>>>(fr, sg->ns, sg->nk, sg->xr, sg->xt, sg->nr_accr, sg->nr_acct,
+  sg_rows_inv<<<sg->nr, SG_ROW_BS, sg->smem_row, s>>>(sg->frow, sg->ns, sg->nk, sg->xr, sg->xt, sg->nr_accr, sg->nr_acct,
                                                    dens, sg->rstep, sg->tstep, sg->eps, k.sg_accr, k.sg_acct);
 }
 
