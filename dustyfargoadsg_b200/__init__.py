@@ -110,7 +110,7 @@ class Disc:
             if entry is None:
                 return False
         t = _ffi.FbTuning(*[int(entry.get(f, 0)) for f in
-                            ("cell_block", "azi_cells_per_thread", "rad_columns", "rad_rings")])
+                            ("cell_block", "azi_cells_per_thread", "rad_columns", "rad_rings", "azi_variant")])
         check(self.lib.fb_set_tuning(self.ctx, C.byref(t)), "fb_set_tuning", self.ctx)
         return True
 

@@ -91,7 +91,8 @@ class FbDustState(C.Structure):
 
 
 class FbTuning(C.Structure):
-    _fields_ = [("cell_block", _I), ("azi_cells_per_thread", _I), ("rad_columns", _I), ("rad_rings", _I)]
+    _fields_ = [("cell_block", _I), ("azi_cells_per_thread", _I), ("rad_columns", _I), ("rad_rings", _I),
+                ("azi_variant", _I)]
 
 
 class FbStepReport(C.Structure):

@@ -1181,6 +1181,7 @@ extern "C" int fb_get_tuning(const fb_ctx *ctx, fb_tuning *t)
   t->azi_cells_per_thread = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
   t->rad_columns = k.rad_tx > 0 ? k.rad_tx : 64;
   t->rad_rings = k.rad_chunk > 0 ? k.rad_chunk : fb_rad_chunk_auto(k);
+  t->azi_variant = fb_azi_wide(k.ns, k.energy, t->azi_cells_per_thread, k.azi_variant) ? 2 : 1;
   return FB_OK;
 }
 
@@ -1193,7 +1194,11 @@ extern "C" int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t)
   if (t->azi_cells_per_thread && !fb_azi_E_valid(k.ns, k.energy, t->azi_cells_per_thread)) return FB_ERR_INVALID;
   if (t->rad_columns && (t->rad_columns < 32 || t->rad_columns > 128 || t->rad_columns % 32)) return FB_ERR_INVALID;
   if (t->rad_rings < 0 || t->rad_rings > k.nr) return FB_ERR_INVALID;
+  if (t->azi_variant < 0 || t->azi_variant > 2) return FB_ERR_INVALID;
+  const int E = t->azi_cells_per_thread ? t->azi_cells_per_thread : fb_azi_E_auto(k.ns);
+  if (t->azi_variant == 2 && !fb_azi_wide(k.ns, k.energy, E, 2)) return FB_ERR_INVALID;
   k.cell_bs = cb;
+  k.azi_variant = t->azi_variant;
   k.azi_E = t->azi_cells_per_thread;
   k.rad_tx = t->rad_columns;
   k.rad_chunk = t->rad_rings;
@@ -1219,8 +1224,9 @@ static int snapshot_take(fb_ctx *ctx, Snapshot &sn)
     const size_t np = (size_t)pp.n * sizeof(double);
     double *g[] = {k.indpot, k.rgp, k.agp, k.rind, k.aind, k.rsga, k.asga};
     for (double *f : g) sn.regions.push_back({f, nf});
-    double *a[] = {pp.r, pp.th, pp.vr, pp.vth, pp.l, pp.st};
+    double *a[] = {pp.r, pp.th, pp.vr, pp.vth, pp.l, pp.size, pp.st};  // permuted by the DT's sort
     for (double *f : a) sn.regions.push_back({f, np});
+    sn.regions.push_back({pp.orig, (size_t)pp.n * sizeof(int)});
     sn.regions.push_back({pp.dc, sizeof(fb_dust_ctl)});
   }
   for (auto &r : sn.regions) {
@@ -1300,17 +1306,22 @@ extern "C" int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_ou
     k.cell_bs = bestv;
     total += bestms;
   }
-  // 2. cells per thread of the azimuthal pass
+  // 2. cells per thread and variant of the azimuthal pass
   {
-    int bestv = k.azi_E;
+    int bestv = k.azi_E, bestvar = k.azi_variant;
     double bestms = 1e300;
     for (int E = 1; E <= 4; E++) {
       if (!fb_azi_E_valid(k.ns, k.energy, E)) continue;
-      k.azi_E = E;
-      const double ms = tune_measure(ctx, sn, substeps, azi_stage, 1);
-      if (ms >= 0.0 && ms < bestms) { bestms = ms; bestv = E; }
+      for (int var = 1; var <= 2; var++) {
+        if (var == 2 && !fb_azi_wide(k.ns, k.energy, E, 2)) continue;
+        k.azi_E = E;
+        k.azi_variant = var;
+        const double ms = tune_measure(ctx, sn, substeps, azi_stage, 1);
+        if (ms >= 0.0 && ms < bestms) { bestms = ms; bestv = E; bestvar = var; }
+      }
     }
     k.azi_E = bestv;
+    k.azi_variant = bestvar;
     total += bestms;
   }
   // 3. columns x rings per CTA of the radial pass

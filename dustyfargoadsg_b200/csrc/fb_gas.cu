@@ -1086,10 +1086,17 @@ static __device__ double block_sum_dyn(double v, double *sh)
 //
 // shared memory: NQ rings of quantities, the residual velocity, W, DQ --
 // 110.6 KB for six quantities of 1536 cells, so that two CTAs share an SM
+//
+// The wide variant (where 2 NQ + 1 rings fit) goes through the quantities
+// together: W of every quantity in place of the quantity's ring (its value
+// kept in registers), one slope ring per quantity, the updates held in
+// registers until every read of W is done -- five barriers per pass instead
+// of three per quantity, and NQ independent chains in every phase.
 #define FB_AZI_RINGS(NQ) ((NQ) + 3)
-template <int E> struct AziMaxThreads { static const int value = (E <= 2) ? 1024 : 768; };
-template <int NQ, int E, bool FULL>
-__global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal(KP k, double dtov)
+#define FB_AZI_RINGS_WIDE(NQ) (2 * (NQ) + 1)
+template <int E, bool WIDE> struct AziMaxThreads { static const int value = (E == 1 || (E == 2 && !WIDE)) ? 1024 : 768; };
+template <int NQ, int E, bool FULL, bool WIDE>
+__global__ void __launch_bounds__(AziMaxThreads<E, WIDE>::value) k_transport_azimuthal(KP k, double dtov)
 {
   extern __shared__ double smem[];
   __shared__ double sh[32];
@@ -1098,8 +1105,8 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
   const size_t base = (size_t)i * ns;
   double *Q = smem;              // NQ rings
   double *vres = Q + NQ * ns;    // residual azimuthal velocity
-  double *W = vres + ns;         // q / RhoInt
-  double *D = vres + 2 * ns;     // van Leer slopes of W
+  double *W = vres + ns;         // q / RhoInt (narrow variant)
+  double *D = vres + (WIDE ? 1 : 2) * ns;  // van Leer slopes of W (wide: NQ rings)
   double *DR = D;                // density slopes (RhoStar), read before D is rewritten
   for (int j = tid; j < ns; j += T)
     for (int q = 0; q < NQ; q++) Q[q * ns + j] = k.q[q][base + j];
@@ -1178,6 +1185,49 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
       den[e] = R[e] + 1e-20;
       rden[e] = 1.0 / den[e];
     }
+    if constexpr (WIDE) {
+      double q0[NQ][E];
+      __syncthreads();  // every read of rho and DR done: W replaces the rings, DR is D[0]
+#pragma unroll
+      for (int q = 0; q < NQ; q++)
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          if (!OWN(e)) continue;
+          double *qb = Q + q * ns;
+          q0[q][e] = qb[jj[e]];
+          qb[jj[e]] = fb_quot(q0[q][e], den[e], rden[e]);  // W = q0 / (RhoInt + 1e-20)
+        }
+      __syncthreads();  // W complete
+#pragma unroll
+      for (int q = 0; q < NQ; q++)
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          if (!OWN(e)) continue;
+          const double *Wq = Q + q * ns;
+          const double w0 = Wq[jj[e]];
+          const double dqm = (w0 - Wq[jjm[e]]), dqp = (Wq[jjp[e]] - w0);
+          D[q * ns + jj[e]] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+        }
+      __syncthreads();  // DQ complete
+#pragma unroll
+      for (int q = 0; q < NQ; q++)
+#pragma unroll
+        for (int e = 0; e < E; e++) {
+          if (!OWN(e)) continue;
+          const double *Wq = Q + q * ns, *Dq = D + q * ns;
+          const double qsl = Wq[ul[e]] + fl[e] * Dq[ul[e]];
+          const double qsh = Wq[uh[e]] + fh[e] * Dq[uh[e]];
+          double varq = dxrad * qsl * RSl[e] * Vl[e];
+          varq -= dxrad * qsh * RSh[e] * Vh[e];
+          q0[q][e] = q0[q][e] + varq * invsurf;
+        }
+      __syncthreads();  // every read of W done
+#pragma unroll
+      for (int q = 0; q < NQ; q++)
+#pragma unroll
+        for (int e = 0; e < E; e++)
+          if (OWN(e)) Q[q * ns + jj[e]] = q0[q][e];
+    } else {
 #pragma unroll
     for (int q = 0; q < NQ; q++) {
       double *qb = Q + q * ns;
@@ -1207,6 +1257,7 @@ __global__ void __launch_bounds__(AziMaxThreads<E>::value) k_transport_azimuthal
         varq -= dxrad * qsh * RSh[e] * Vh[e];
         qb[jj[e]] = q0[e] + varq * invsurf;
       }
+    }
     }
   }
 #undef OWN
@@ -1266,14 +1317,28 @@ int fb_azi_E_auto(int ns)
     if (azi_threads_for(ns, E) <= azi_max_threads(E)) return E;
   return 5;  // ring too long
 }
+static int max_smem_optin()
+{
+  int dev = 0, maxopt = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return maxopt;
+}
 int fb_azi_E_valid(int ns, int energy, int E)
 {
   if (E < 1 || E > 4 || azi_threads_for(ns, E) > azi_max_threads(E)) return 0;
   const int NQ = energy ? 6 : 5;
-  int dev = 0, maxopt = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  return (size_t)FB_AZI_RINGS(NQ) * ns * sizeof(double) + 32 * sizeof(double) <= (size_t)maxopt;
+  return (size_t)FB_AZI_RINGS(NQ) * ns * sizeof(double) + 32 * sizeof(double) <= (size_t)max_smem_optin();
+}
+// the wide variant: its rings fit and its thread limit holds (768 threads
+// for two or more cells per thread); variant 0 takes it where it can
+int fb_azi_wide(int ns, int energy, int E, int variant)
+{
+  if (variant == 1) return 0;
+  const int NQ = energy ? 6 : 5;
+  const int maxt = (E == 1) ? 1024 : 768;
+  return azi_threads_for(ns, E) <= maxt &&
+         (size_t)FB_AZI_RINGS_WIDE(NQ) * ns * sizeof(double) + 32 * sizeof(double) <= (size_t)max_smem_optin();
 }
 
 // ComputeVelocities' radial part (TransportEuler.c:531-536) needs the
@@ -1346,13 +1411,16 @@ void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
 template <int NQ>
 static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
 {
-  const size_t smem = (size_t)FB_AZI_RINGS(NQ) * k.ns * sizeof(double);
   const int E = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
+  const bool wide = fb_azi_wide(k.ns, NQ == 6, E, k.azi_variant);
+  const size_t smem = (size_t)(wide ? FB_AZI_RINGS_WIDE(NQ) : FB_AZI_RINGS(NQ)) * k.ns * sizeof(double);
   const int th = azi_threads_for(k.ns, E);
   const bool full = (th * E == k.ns);  // every thread owns E cells
-#define AZI_LAUNCH(EE)                                                            \
-  (full ? k_transport_azimuthal<NQ, EE, true><<<k.nr, th, smem, s>>>(k, dt_override) \
-        : k_transport_azimuthal<NQ, EE, false><<<k.nr, th, smem, s>>>(k, dt_override))
+#define AZI_LAUNCH(EE)                                                                                     \
+  (wide ? (full ? k_transport_azimuthal<NQ, EE, true, true><<<k.nr, th, smem, s>>>(k, dt_override)         \
+                : k_transport_azimuthal<NQ, EE, false, true><<<k.nr, th, smem, s>>>(k, dt_override))       \
+        : (full ? k_transport_azimuthal<NQ, EE, true, false><<<k.nr, th, smem, s>>>(k, dt_override)        \
+                : k_transport_azimuthal<NQ, EE, false, false><<<k.nr, th, smem, s>>>(k, dt_override)))
   switch (E) {
     case 1: AZI_LAUNCH(1); break;
     case 2: AZI_LAUNCH(2); break;
@@ -1562,10 +1630,12 @@ int fb_gas_prepare(int ns, int energy)
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (smem + 32 * sizeof(double) > (size_t)maxopt) return FB_ERR_UNSUPPORTED;
   if (fb_azi_E_auto(ns) > 4 || ns < 16) return FB_ERR_UNSUPPORTED;
-#define AZI_FNS(NQ, F)                                                                                   \
-  (const void *)k_transport_azimuthal<NQ, 1, F>, (const void *)k_transport_azimuthal<NQ, 2, F>,          \
-      (const void *)k_transport_azimuthal<NQ, 3, F>, (const void *)k_transport_azimuthal<NQ, 4, F>
-  const void *fns[] = {AZI_FNS(5, false), AZI_FNS(5, true), AZI_FNS(6, false), AZI_FNS(6, true)};
+#define AZI_FNS(NQ, F, WD)                                                                               \
+  (const void *)k_transport_azimuthal<NQ, 1, F, WD>, (const void *)k_transport_azimuthal<NQ, 2, F, WD>,  \
+      (const void *)k_transport_azimuthal<NQ, 3, F, WD>, (const void *)k_transport_azimuthal<NQ, 4, F, WD>
+  const void *fns[] = {AZI_FNS(5, false, false), AZI_FNS(5, true, false), AZI_FNS(6, false, false),
+                       AZI_FNS(6, true, false),  AZI_FNS(5, false, true),  AZI_FNS(5, true, true),
+                       AZI_FNS(6, false, true),  AZI_FNS(6, true, true)};
 #undef AZI_FNS
   for (const void *f : fns) {
     int rc = fb_allow_max_dynamic_smem(f);

@@ -22,7 +22,7 @@ from . import Disc, read_par, sweep
 from ._ffi import FbTuning, check
 
 DEFAULT_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "configs", "tuning_b200.json")
-FIELDS = ("cell_block", "azi_cells_per_thread", "rad_columns", "rad_rings")
+FIELDS = ("cell_block", "azi_cells_per_thread", "rad_columns", "rad_rings", "azi_variant")
 
 
 def grid_key(nr, ns):
