@@ -248,6 +248,7 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   ctx->err[0] = 0;
   int rc = fb_geom_fill(p, radii, &ctx->g);
   if (rc) { delete ctx; return rc; }
+  if (getenv("FB_NO_PDL")) fb_pdl = 0;  // launches without programmatic dependencies
   rc = fb_gas_prepare(ctx->ns, p->energy_equation);
   if (rc) { set_err(ctx, "ring of %d doubles does not fit in shared memory", ctx->ns); fb_geom_free(&ctx->g); delete ctx; return rc; }
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return FB_ERR_CUDA; }
@@ -648,7 +649,19 @@ static int enqueue_dt_prelude(fb_ctx *ctx)
 // Captures one DT as a graph: WHILE(cond) { substep; cond = !done }.  The
 // kernels read dt and the planets from the device control block, so one
 // capture serves every substep and every DT.
+static int build_dt_graph_once(fb_ctx *ctx);
+// Without programmatic dependent launch when a driver refuses it in a graph.
 static int build_dt_graph(fb_ctx *ctx)
+{
+  int rc = build_dt_graph_once(ctx);
+  if (rc == FB_ERR_CUDA && fb_pdl) {
+    fb_pdl = 0;
+    rc = build_dt_graph_once(ctx);
+  }
+  return rc;
+}
+
+static int build_dt_graph_once(fb_ctx *ctx)
 {
   cudaGraph_t g = NULL, body = NULL;
   cudaGraphConditionalHandle h;

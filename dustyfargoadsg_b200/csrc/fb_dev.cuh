@@ -111,6 +111,35 @@ static __device__ __forceinline__ double fb_quot(double a, double d, double r)
   return fma(e, r, y);
 }
 
+// Kernel launches of the step.  With programmatic dependent launch a
+// kernel may be scheduled while the one before it in the stream drains;
+// every kernel of the step starts with fb_grid_dependency(), which waits
+// until the previous grid has completed and its writes are visible, then
+// lets the next grid be scheduled (it only starts once every CTA of this
+// grid has started, so it never takes resources this grid still needs).
+extern int fb_pdl;  // 1: launches carry the programmatic-serialization attribute
+template <typename... KArgs, typename... Args>
+static inline void fb_launch(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                             Args... args)
+{
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cfg.attrs = at;
+  cfg.numAttrs = fb_pdl ? 1 : 0;
+  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+static __device__ __forceinline__ void fb_grid_dependency()
+{
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 struct fb_dust_ctl {
   unsigned long long x;        // drand48 state after the last draw
   long long kicks;             // calls made so far by each Gaussian generator

@@ -146,6 +146,7 @@ static __device__ double stokes_number(const PP &pp, double size, double rp, dou
 // flag = the particle gets a turbulent kick in this substep.
 __global__ void __launch_bounds__(D_BS) k_dust_drift(KP k, PP pp)
 {
+  fb_grid_dependency();
   const int q = blockIdx.x * D_BS + threadIdx.x;
   if (q == 0) pp.dc->min_ts = 1e6;  // reset by every interpolation call (Dsys.c:336)
   if (q >= pp.n) return;
@@ -179,6 +180,7 @@ static __device__ __forceinline__ int warp_incl_scan(int x)
 // exclusive scan of SCAN_BS ints per block; block totals to blocksum
 __global__ void __launch_bounds__(SCAN_BS) k_scan_block(const int *in, int *out, int *blocksum, int n)
 {
+  fb_grid_dependency();
   __shared__ int sh[SCAN_BS / 32];
   const int g = blockIdx.x * SCAN_BS + threadIdx.x;
   const int v = (g < n) ? in[g] : 0;
@@ -223,6 +225,7 @@ static __device__ int scan_top(int *blocksum, int nb)
 // Number of kicked particles K of this substep and the accepted pairs it needs.
 __global__ void __launch_bounds__(SCAN_BS) k_kick_top(PP pp, int nb)
 {
+  fb_grid_dependency();
   const int K = scan_top(pp.kick_bsum, nb);
   if (threadIdx.x == 0) {
     fb_dust_ctl *d = pp.dc;
@@ -261,6 +264,7 @@ static __device__ __forceinline__ long long candidate_limit(const PP &pp, int np
 
 __global__ void __launch_bounds__(D_BS) k_rng_count(PP pp)
 {
+  fb_grid_dependency();
   __shared__ int sh[D_BS / 32];
   const long long c = (long long)blockIdx.x * D_BS + threadIdx.x;
   const int npairs = pp.dc->npairs;
@@ -282,6 +286,7 @@ __global__ void __launch_bounds__(D_BS) k_rng_count(PP pp)
 
 __global__ void __launch_bounds__(SCAN_BS) k_rng_top(KP k, PP pp, int nb)
 {
+  fb_grid_dependency();
   const int total = scan_top(pp.cand_bsum, nb);
   if (threadIdx.x == 0) {
     fb_dust_ctl *d = pp.dc;
@@ -297,6 +302,7 @@ __global__ void __launch_bounds__(SCAN_BS) k_rng_top(KP k, PP pp, int nb)
 // Accepted candidate number g (in stream order) becomes pair g.
 __global__ void __launch_bounds__(D_BS) k_rng_scatter(PP pp)
 {
+  fb_grid_dependency();
   __shared__ int wc[D_BS / 32];
   const long long c = (long long)blockIdx.x * D_BS + threadIdx.x;
   const int npairs = pp.dc->npairs;
@@ -330,6 +336,7 @@ static __device__ __forceinline__ void record_stopping_time(const PP &pp, double
 // mode 1: the interpolation call of main.c:287 (Stokes numbers only).
 __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
 {
+  fb_grid_dependency();
   const int q = blockIdx.x * D_BS + threadIdx.x;  // storage slot
   if (q >= pp.n) return;
   const int qr = (mode == 0) ? pp.orig[q] : 0;  // the reference's index: kick flag and rank
@@ -539,6 +546,7 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
 // ----------------------------------------------------- 5. bookkeeping
 __global__ void k_dust_finish(PP pp)
 {
+  fb_grid_dependency();
   fb_dust_ctl *d = pp.dc;
   const long long G = d->kicks, K = d->K;
   if (d->npairs > 0) d->x = lcg_skip(d->x, (unsigned long long)(2 * (d->c_last + 1)));
@@ -561,6 +569,7 @@ __global__ void k_dust_finish(PP pp)
 // the particles on the grid, nr*ns for the others.
 __global__ void __launch_bounds__(D_BS) k_cell_key(KP k, PP pp)
 {
+  fb_grid_dependency();
   const int q = blockIdx.x * D_BS + threadIdx.x;
   if (q >= pp.n) return;
   const double r = pp.r[q], th = pp.th[q];
@@ -579,14 +588,17 @@ __global__ void __launch_bounds__(D_BS) k_cell_key(KP k, PP pp)
 // exclusive block offsets -> global offsets
 __global__ void __launch_bounds__(SCAN_BS) k_scan_add(int *v, const int *bsum, int n)
 {
+  fb_grid_dependency();
   const int g = blockIdx.x * SCAN_BS + threadIdx.x;
   if (g < n) v[g] += bsum[blockIdx.x];
 }
 
-__global__ void __launch_bounds__(SCAN_BS) k_scan_top_only(int *blocksum, int nb) { scan_top(blocksum, nb); }
+__global__ void __launch_bounds__(SCAN_BS) k_scan_top_only(int *blocksum, int nb) {
+  fb_grid_dependency(); scan_top(blocksum, nb); }
 
 __global__ void __launch_bounds__(D_BS) k_cell_scatter(PP pp)
 {
+  fb_grid_dependency();
   const int q = blockIdx.x * D_BS + threadIdx.x;
   if (q >= pp.n) return;
   const int pos = atomicAdd(pp.cell_count + pp.key[q], 1);  // the offsets, consumed as cursors
@@ -596,6 +608,7 @@ __global__ void __launch_bounds__(D_BS) k_cell_scatter(PP pp)
 // Moves the particles into the sorted order: slot t takes old slot perm[t].
 __global__ void __launch_bounds__(D_BS) k_cell_gather(PP pp)
 {
+  fb_grid_dependency();
   const int t = blockIdx.x * D_BS + threadIdx.x;
   if (t >= pp.n) return;
   const int s = pp.perm[t];
@@ -613,6 +626,7 @@ __global__ void __launch_bounds__(D_BS) k_cell_gather(PP pp)
 
 __global__ void __launch_bounds__(D_BS) k_cell_copy(PP pp)
 {
+  fb_grid_dependency();
   const int t = blockIdx.x * D_BS + threadIdx.x;
   if (t >= pp.n) return;
   const size_t n = pp.n;
@@ -631,36 +645,38 @@ int fb_launch_dust_sort(const KP &k, const PP &pp, cudaStream_t s)
 {
   const int nb = (pp.n + D_BS - 1) / D_BS, nc = pp.ncells, ncb = (nc + SCAN_BS - 1) / SCAN_BS;
   cudaMemsetAsync(pp.cell_count, 0, (size_t)nc * sizeof(int), s);
-  k_cell_key<<<nb, D_BS, 0, s>>>(k, pp);
-  k_scan_block<<<ncb, SCAN_BS, 0, s>>>(pp.cell_count, pp.cell_count, pp.cell_bsum, nc);
-  k_scan_top_only<<<1, SCAN_BS, 0, s>>>(pp.cell_bsum, ncb);
-  k_scan_add<<<ncb, SCAN_BS, 0, s>>>(pp.cell_count, pp.cell_bsum, nc);
-  k_cell_scatter<<<nb, D_BS, 0, s>>>(pp);
-  k_cell_gather<<<nb, D_BS, 0, s>>>(pp);
-  k_cell_copy<<<nb, D_BS, 0, s>>>(pp);
+  fb_launch(k_cell_key, nb, D_BS, 0, s, k, pp);
+  fb_launch(k_scan_block, ncb, SCAN_BS, 0, s, pp.cell_count, pp.cell_count, pp.cell_bsum, nc);
+  fb_launch(k_scan_top_only, 1, SCAN_BS, 0, s, pp.cell_bsum, ncb);
+  fb_launch(k_scan_add, ncb, SCAN_BS, 0, s, pp.cell_count, pp.cell_bsum, nc);
+  fb_launch(k_cell_scatter, nb, D_BS, 0, s, pp);
+  fb_launch(k_cell_gather, nb, D_BS, 0, s, pp);
+  fb_launch(k_cell_copy, nb, D_BS, 0, s, pp);
   return 7;
 }
 
 // storage slots in the reference's order (after an upload)
 __global__ void __launch_bounds__(D_BS) k_iota(int *v, int n)
 {
+  fb_grid_dependency();
   const int t = blockIdx.x * D_BS + threadIdx.x;
   if (t < n) v[t] = t;
 }
 void fb_launch_dust_iota(const PP &pp, cudaStream_t s)
 {
-  k_iota<<<(pp.n + D_BS - 1) / D_BS, D_BS, 0, s>>>(pp.orig, pp.n);
+  fb_launch(k_iota, (pp.n + D_BS - 1) / D_BS, D_BS, 0, s, pp.orig, pp.n);
 }
 
 // dst[orig[t]] = src[t]: one particle array back in the reference's order
 __global__ void __launch_bounds__(D_BS) k_to_reference_order(const int *orig, const double *src, double *dst, int n)
 {
+  fb_grid_dependency();
   const int t = blockIdx.x * D_BS + threadIdx.x;
   if (t < n) dst[orig[t]] = src[t];
 }
 void fb_launch_dust_to_reference_order(const PP &pp, const double *src, double *dst, cudaStream_t s)
 {
-  k_to_reference_order<<<(pp.n + D_BS - 1) / D_BS, D_BS, 0, s>>>(pp.orig, src, dst, pp.n);
+  fb_launch(k_to_reference_order, (pp.n + D_BS - 1) / D_BS, D_BS, 0, s, pp.orig, src, dst, pp.n);
 }
 
 // ---------------------------------------------------------- launchers
@@ -669,23 +685,23 @@ int fb_dust_launches(const PP &pp) { return pp.feel_turb ? 8 : 2; }
 void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s, cudaEvent_t planets_done)
 {
   const int nb = (pp.n + D_BS - 1) / D_BS;
-  k_dust_drift<<<nb, D_BS, 0, s>>>(k, pp);
+  fb_launch(k_dust_drift, nb, D_BS, 0, s, k, pp);
   if (pp.feel_turb) {
     const int nsb = (pp.n + SCAN_BS - 1) / SCAN_BS;
-    k_scan_block<<<nsb, SCAN_BS, 0, s>>>(pp.flag, pp.kidx, pp.kick_bsum, pp.n);
-    k_kick_top<<<1, SCAN_BS, 0, s>>>(pp, nsb);
+    fb_launch(k_scan_block, nsb, SCAN_BS, 0, s, pp.flag, pp.kidx, pp.kick_bsum, pp.n);
+    fb_launch(k_kick_top, 1, SCAN_BS, 0, s, pp, nsb);
     const int ncb = (pp.ncand + D_BS - 1) / D_BS;
-    k_rng_count<<<ncb, D_BS, 0, s>>>(pp);
-    k_rng_top<<<1, SCAN_BS, 0, s>>>(k, pp, ncb);
-    k_rng_scatter<<<ncb, D_BS, 0, s>>>(pp);
+    fb_launch(k_rng_count, ncb, D_BS, 0, s, pp);
+    fb_launch(k_rng_top, 1, SCAN_BS, 0, s, k, pp, ncb);
+    fb_launch(k_rng_scatter, ncb, D_BS, 0, s, pp);
   }
   if (planets_done) cudaStreamWaitEvent(s, planets_done, 0);  // positions after the planets' step
-  k_dust_update<<<nb, D_BS, 0, s>>>(k, pp, 0);
-  if (pp.feel_turb) k_dust_finish<<<1, 1, 0, s>>>(pp);
+  fb_launch(k_dust_update, nb, D_BS, 0, s, k, pp, 0);
+  if (pp.feel_turb) fb_launch(k_dust_finish, 1, 1, 0, s, pp);
 }
 
 void fb_launch_dust_interpolation_only(const KP &k, const PP &pp, cudaStream_t s)
 {
   const int nb = (pp.n + D_BS - 1) / D_BS;
-  k_dust_update<<<nb, D_BS, 0, s>>>(k, pp, 1);
+  fb_launch(k_dust_update, nb, D_BS, 0, s, k, pp, 1);
 }

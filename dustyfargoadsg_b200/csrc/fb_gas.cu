@@ -13,6 +13,8 @@
 #include <math.h>
 #include "fb_dev.cuh"
 
+int fb_pdl = 1;
+
 #define FB_BS 256
 #define FB_BS2 256  // most threads per CTA of the per-cell kernels (k.cell_bs <= FB_BS2)
 #define RING_U 6    // cells per thread and batch of k_soundspeed
@@ -149,6 +151,7 @@ static __device__ void rk5(const double *q0, double dt, const double *masses, do
 static inline int cfl_threads(int ns) { return ((ns + CFL_E - 1) / CFL_E + 31) / 32 * 32; }
 __global__ void __launch_bounds__(1024) k_cfl(KP k)
 {
+  fb_grid_dependency();
   __shared__ double sh[6 * 32];
   const int i = blockIdx.x, ns = k.ns, T = blockDim.x, tid = threadIdx.x;
   const size_t base = (size_t)i * ns;
@@ -260,7 +263,7 @@ __global__ void __launch_bounds__(1024) k_cfl(KP k)
   for (int w = tid; w < (int)(sizeof(fb_ctl) / 8); w += T) out[w] = dst[w];
 }
 
-void fb_launch_cfl(const KP &k, cudaStream_t s) { k_cfl<<<k.nr, cfl_threads(k.ns), 0, s>>>(k); }
+void fb_launch_cfl(const KP &k, cudaStream_t s) { fb_launch(k_cfl, k.nr, cfl_threads(k.ns), 0, s, k); }
 
 // The planets' step of the substep, after the controller has set dt:
 // AdvanceSystemRK5 (Pframeforce.c:163-266) and RotatePsys (Psys.c:352-372).
@@ -270,6 +273,7 @@ void fb_launch_cfl(const KP &k, cudaStream_t s) { k_cfl<<<k.nr, cfl_threads(k.ns
 // of UpdateDustVelocities (DustUpdate.c:342-352) at the new positions.
 __global__ void k_planets(KP k, fb_dust_ctl *dc, double thick, double aspect, double flaring)
 {
+  fb_grid_dependency();
   fb_ctl *c = k.ctl;
   if (c->status != FB_OK) return;
   const int np = c->np;
@@ -327,9 +331,9 @@ __global__ void k_planets(KP k, fb_dust_ctl *dc, double thick, double aspect, do
 void fb_launch_planets(const KP &k, const PP *pp, cudaStream_t s)
 {
   if (pp && pp->feel_planets)
-    k_planets<<<1, 1, 0, s>>>(k, pp->dc, pp->thicksmoothing, pp->aspectratio, pp->flaringindex);
+    fb_launch(k_planets, 1, 1, 0, s, k, pp->dc, pp->thicksmoothing, pp->aspectratio, pp->flaringindex);
   else
-    k_planets<<<1, 1, 0, s>>>(k, nullptr, 0.0, 0.0, 0.0);
+    fb_launch(k_planets, 1, 1, 0, s, k, nullptr, 0.0, 0.0, 0.0);
 }
 
 // ------------------------------------------------------------ controller
@@ -541,6 +545,7 @@ static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
 // inside ComputeViscousTerms (Viscosity.c:247-248).
 __global__ void __launch_bounds__(FB_BS) k_soundspeed(KP k, int update_gcs)
 {
+  fb_grid_dependency();
   __shared__ double sh[32];
   const int i = blockIdx.x, ns = k.ns;
   const size_t base = (size_t)i * ns;
@@ -573,13 +578,14 @@ __global__ void __launch_bounds__(FB_BS) k_soundspeed(KP k, int update_gcs)
 
 void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s)
 {
-  k_soundspeed<<<k.nr, FB_BS, 0, s>>>(k, update_gcs);
+  fb_launch(k_soundspeed, k.nr, FB_BS, 0, s, k, update_gcs);
 }
 
 // ----------------------------------------------------------- potential
 // FillForcesArrays (Pframeforce.c:44-129): star + planets + indirect terms.
 __global__ void __launch_bounds__(FB_BS2) k_potential(KP k)
 {
+  fb_grid_dependency();
   const fb_ctl *c = k.ctl;
   const int np = c->np;
   const int use_ind = (!k.discard_gas_it) && (fabs(k.pmax - k.pmin - 2. * M_PI) < 0.01);
@@ -618,7 +624,7 @@ __global__ void __launch_bounds__(FB_BS2) k_potential(KP k)
 
 void fb_launch_potential(const KP &k, cudaStream_t s)
 {
-  k_potential<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k);
+  fb_launch(k_potential, grid2d(k, k.nr), k.cell_bs, 0, s, k);
 }
 
 // ------------------------------------------------------------ SubStep1
@@ -633,6 +639,7 @@ static __device__ __forceinline__ double pressure_at(const KP &k, size_t l)
 // curvature terms into VradInt (i >= 1) and VthetaInt (all rings).
 __global__ void __launch_bounds__(FB_BS2) k_substep1(KP k)
 {
+  fb_grid_dependency();
   const int ns = k.ns;
   const double dt = k.ctl->dt;
   {
@@ -675,7 +682,7 @@ __global__ void __launch_bounds__(FB_BS2) k_substep1(KP k)
 
 void fb_launch_substep1(const KP &k, cudaStream_t s)
 {
-  k_substep1<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k);
+  fb_launch(k_substep1, grid2d(k, k.nr), k.cell_bs, 0, s, k);
 }
 
 // ------------------------------------------------------- viscous stresses
@@ -684,6 +691,7 @@ void fb_launch_substep1(const KP &k, cudaStream_t s)
 __global__ void __launch_bounds__(FB_BS2) k_viscous_terms(KP k, const double *__restrict__ vr,
                                                          const double *__restrict__ vt)
 {
+  fb_grid_dependency();
   const int ns = k.ns;
   const double invdphi = k.invdphi, onethird = 1.0 / 3.0;
   {
@@ -713,12 +721,13 @@ __global__ void __launch_bounds__(FB_BS2) k_viscous_terms(KP k, const double *__
 
 void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s)
 {
-  k_viscous_terms<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k, vr, vt);
+  fb_launch(k_viscous_terms, grid2d(k, k.nr), k.cell_bs, 0, s, k, vr, vt);
 }
 
 // UpdateVelocitiesWithViscosity (Viscosity.c:305-378)
 __global__ void __launch_bounds__(FB_BS2) k_viscous_update(KP k, double *vr, double *vt, double dtov)
 {
+  fb_grid_dependency();
   const int ns = k.ns, nr = k.nr;
   const double DeltaT = dt_of(k, dtov), invdphi = k.invdphi;
   {
@@ -744,7 +753,7 @@ __global__ void __launch_bounds__(FB_BS2) k_viscous_update(KP k, double *vr, dou
 
 void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s)
 {
-  k_viscous_update<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k, vr, vt, dt_override);
+  fb_launch(k_viscous_update, grid2d(k, k.nr), k.cell_bs, 0, s, k, vr, vt, dt_override);
 }
 
 // ------------------------------------------------------------ SubStep2
@@ -766,6 +775,7 @@ static __device__ __forceinline__ double q_t(const KP &k, size_t l, size_t ljp)
 
 __global__ void __launch_bounds__(FB_BS2) k_substep2(KP k)
 {
+  fb_grid_dependency();
   const int ns = k.ns, nr = k.nr;
   const double dt = k.ctl->dt;
   {
@@ -804,12 +814,13 @@ __global__ void __launch_bounds__(FB_BS2) k_substep2(KP k)
 
 void fb_launch_substep2(const KP &k, cudaStream_t s)
 {
-  k_substep2<<<grid2d(k, k.nr + 1), k.cell_bs, 0, s>>>(k);
+  fb_launch(k_substep2, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k);
 }
 
 // ComputeDivergenceVelocity (SourceEuler.c:2373-2412) on (Vrad, Vtheta)
 __global__ void __launch_bounds__(FB_BS2) k_divergence(KP k)
 {
+  fb_grid_dependency();
   const int ns = k.ns;
   {
     const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -825,7 +836,7 @@ __global__ void __launch_bounds__(FB_BS2) k_divergence(KP k)
 
 void fb_launch_divergence(const KP &k, cudaStream_t s)
 {
-  k_divergence<<<grid2d(k, k.nr), k.cell_bs, 0, s>>>(k);
+  fb_launch(k_divergence, grid2d(k, k.nr), k.cell_bs, 0, s, k);
 }
 
 // ------------------------------------------------------------ SubStep3
@@ -848,6 +859,7 @@ static __device__ __forceinline__ double vischeat_at(const KP &k, int i, size_t 
 // Energy = EnergyNew (ring nr of EnergyNew is never written: zero).
 __global__ void __launch_bounds__(FB_BS) k_substep3(KP k)
 {
+  fb_grid_dependency();
   __shared__ double sh[32];
   const int i = blockIdx.x, ns = k.ns, nr = k.nr;
   const double dt = k.ctl->dt;
@@ -893,7 +905,7 @@ __global__ void __launch_bounds__(FB_BS) k_substep3(KP k)
   }
 }
 
-void fb_launch_substep3(const KP &k, cudaStream_t s) { k_substep3<<<k.nr + 1, FB_BS, 0, s>>>(k); }
+void fb_launch_substep3(const KP &k, cudaStream_t s) { fb_launch(k_substep3, k.nr + 1, FB_BS, 0, s, k); }
 
 // ------------------------------------------------------------ Transport
 // Radial pass of the van Leer transport (OneWindRad, TransportEuler.c:124-220
@@ -1035,6 +1047,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
 template <int NQ>
 __global__ void __launch_bounds__(256) k_transport_radial(KP k, double dtov, int chunk)
 {
+  fb_grid_dependency();
   const double dt = dt_of(k, dtov);
   const int tx = blockDim.x >> 1, h = (threadIdx.x >= tx) ? 1 : 0;  // tx % 32 == 0: warp-uniform
   const int j = blockIdx.x * tx + threadIdx.x - h * tx;
@@ -1098,6 +1111,7 @@ template <int E, bool WIDE> struct AziMaxThreads { static const int value = (E =
 template <int NQ, int E, bool FULL, bool WIDE>
 __global__ void __launch_bounds__(AziMaxThreads<E, WIDE>::value) k_transport_azimuthal(KP k, double dtov)
 {
+  fb_grid_dependency();
   extern __shared__ double smem[];
   __shared__ double sh[32];
   const double dt = dt_of(k, dtov);
@@ -1346,6 +1360,7 @@ int fb_azi_wide(int ns, int energy, int E, int variant)
 // (SourceEuler.c:2506) and ApplyWallBoundaries (SideEuler.c:1047-1099).
 __global__ void __launch_bounds__(FB_BS2) k_transport_vr(KP k)
 {
+  fb_grid_dependency();
   const int ns = k.ns, nr = k.nr;
   const int wall = k.wall && !k.transport_only;
   const int floors = k.add_floors && !k.transport_only;
@@ -1380,6 +1395,7 @@ __global__ void __launch_bounds__(FB_BS2) k_transport_vr(KP k)
 // :213-216): the ring-0 radial fluxes summed over azimuth.
 __global__ void k_lostmass(KP k)
 {
+  fb_grid_dependency();
   double s = 0.0;
   for (int j = threadIdx.x; j < k.ns; j += 32) s += k.lost0[j];
   for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
@@ -1403,9 +1419,9 @@ void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
   const int chunk = k.rad_chunk > 0 ? k.rad_chunk : fb_rad_chunk_auto(k);
   dim3 gr(bx, (k.nr + chunk - 1) / chunk);
   if (k.energy)
-    k_transport_radial<6><<<gr, 2 * tx, 0, s>>>(k, dt_override, chunk);
+    fb_launch(k_transport_radial<6>, gr, 2 * tx, 0, s, k, dt_override, chunk);
   else
-    k_transport_radial<5><<<gr, 2 * tx, 0, s>>>(k, dt_override, chunk);
+    fb_launch(k_transport_radial<5>, gr, 2 * tx, 0, s, k, dt_override, chunk);
 }
 
 template <int NQ>
@@ -1417,10 +1433,10 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
   const int th = azi_threads_for(k.ns, E);
   const bool full = (th * E == k.ns);  // every thread owns E cells
 #define AZI_LAUNCH(EE)                                                                                     \
-  (wide ? (full ? k_transport_azimuthal<NQ, EE, true, true><<<k.nr, th, smem, s>>>(k, dt_override)         \
-                : k_transport_azimuthal<NQ, EE, false, true><<<k.nr, th, smem, s>>>(k, dt_override))       \
-        : (full ? k_transport_azimuthal<NQ, EE, true, false><<<k.nr, th, smem, s>>>(k, dt_override)        \
-                : k_transport_azimuthal<NQ, EE, false, false><<<k.nr, th, smem, s>>>(k, dt_override)))
+  (wide ? (full ? fb_launch(k_transport_azimuthal<NQ, EE, true, true>, k.nr, th, smem, s, k, dt_override)         \
+                : fb_launch(k_transport_azimuthal<NQ, EE, false, true>, k.nr, th, smem, s, k, dt_override))       \
+        : (full ? fb_launch(k_transport_azimuthal<NQ, EE, true, false>, k.nr, th, smem, s, k, dt_override)        \
+                : fb_launch(k_transport_azimuthal<NQ, EE, false, false>, k.nr, th, smem, s, k, dt_override)))
   switch (E) {
     case 1: AZI_LAUNCH(1); break;
     case 2: AZI_LAUNCH(2); break;
@@ -1440,8 +1456,8 @@ void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t
 
 void fb_launch_transport_vr(const KP &k, cudaStream_t s)
 {
-  k_transport_vr<<<grid2d(k, k.nr + 1), k.cell_bs, 0, s>>>(k);
-  k_lostmass<<<1, 32, 0, s>>>(k);
+  fb_launch(k_transport_vr, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k);
+  fb_launch(k_lostmass, 1, 32, 0, s, k);
 }
 
 // Transport (TransportEuler.c:65-87) + floors + boundaries: 4 launches
@@ -1458,6 +1474,7 @@ void fb_launch_floors_boundary(const KP &k, cudaStream_t s) { (void)k; (void)s; 
 // sub-Keplerian edge rings on the current state (stage tests).
 __global__ void k_boundary_only(KP k)
 {
+  fb_grid_dependency();
   const int ns = k.ns, nr = k.nr;
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= ns) return;
@@ -1477,13 +1494,14 @@ __global__ void k_boundary_only(KP k)
 
 void fb_launch_boundary_only(const KP &k, cudaStream_t s)
 {
-  k_boundary_only<<<(k.ns + 127) / 128, 128, 0, s>>>(k);
+  fb_launch(k_boundary_only, (k.ns + 127) / 128, 128, 0, s, k);
 }
 
 // ------------------------------------------------------------ damping
 // EvanescentBoundary (SideEuler.c:796-950), default DampToAxi or DampToIni.
 __global__ void __launch_bounds__(FB_BS) k_damping(KP k, double dtov)
 {
+  fb_grid_dependency();
   __shared__ double sh[32];
   const int i = k.damp_rings[blockIdx.x], ns = k.ns, nr = k.nr;
   const size_t base = (size_t)i * ns;
@@ -1526,13 +1544,14 @@ __global__ void __launch_bounds__(FB_BS) k_damping(KP k, double dtov)
 
 void fb_launch_damping(const KP &k, double dt_override, cudaStream_t s)
 {
-  if (k.n_damp_rings > 0) k_damping<<<k.n_damp_rings, FB_BS, 0, s>>>(k, dt_override);
+  if (k.n_damp_rings > 0) fb_launch(k_damping, k.n_damp_rings, FB_BS, 0, s, k, dt_override);
 }
 
 // ------------------------------------------------------------ diagnostics
 // GasTotalMass (SideEuler.c:15-40) and GasMomentum (SideEuler.c:114-147)
 __global__ void __launch_bounds__(FB_BS) k_diag(KP k, double *out)
 {
+  fb_grid_dependency();
   __shared__ double sh[32];
   const int ns = k.ns;
   const size_t n = (size_t)k.nr * ns;
@@ -1557,12 +1576,13 @@ __global__ void __launch_bounds__(FB_BS) k_diag(KP k, double *out)
 
 void fb_launch_diag(const KP &k, double *out2, cudaStream_t s)
 {
-  k_diag<<<k.n_partial_blocks, FB_BS, 0, s>>>(k, out2);
+  fb_launch(k_diag, k.n_partial_blocks, FB_BS, 0, s, k, out2);
 }
 
 // Derived output fields (layout (nr+1)*ns; ring nr zero)
 __global__ void __launch_bounds__(FB_BS) k_derived(KP k, int which, double *out)
 {
+  fb_grid_dependency();
   const int ns = k.ns;
   const size_t n = (size_t)k.nr * ns;
   for (size_t l = (size_t)blockIdx.x * FB_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * FB_BS) {
@@ -1587,12 +1607,13 @@ __global__ void __launch_bounds__(FB_BS) k_derived(KP k, int which, double *out)
 void fb_launch_derived(const KP &k, int which, double *out, cudaStream_t s)
 {
   const size_t n = (size_t)k.nr * k.ns;
-  k_derived<<<(int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s>>>(k, which, out);
+  fb_launch(k_derived, (int)((n + FB_BS - 1) / FB_BS), FB_BS, 0, s, k, which, out);
 }
 
 // Start of one AlgoGas call: dtemp = 0 (SourceEuler.c:333) and the loop flags.
 __global__ void k_begin_dt(KP k, double DT)
 {
+  fb_grid_dependency();
   fb_ctl *c = k.ctl;
   c->DT = DT;
   c->dtemp = 0.0;
@@ -1602,7 +1623,7 @@ __global__ void k_begin_dt(KP k, double DT)
   c->nonfinite = 0;
 }
 
-void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s) { k_begin_dt<<<1, 1, 0, s>>>(k, DT); }
+void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s) { fb_launch(k_begin_dt, 1, 1, 0, s, k, DT); }
 
 // Lets a kernel take all the dynamic shared memory the device offers beside
 // its static part.  The limit is a per-function attribute shared by every
@@ -1652,6 +1673,7 @@ int fb_gas_prepare(int ns, int energy)
 // cap bounds the loop even if the time step collapses.
 __global__ void k_loop_cond(KP k, cudaGraphConditionalHandle h, int cap)
 {
+  fb_grid_dependency();
   fb_ctl *c = k.ctl;
   int go = (!c->done && !c->status) ? 1 : 0;
   if (go && c->substeps >= cap) {
@@ -1663,5 +1685,5 @@ __global__ void k_loop_cond(KP k, cudaGraphConditionalHandle h, int cap)
 
 void fb_launch_loop_cond(const KP &k, cudaGraphConditionalHandle h, int cap, cudaStream_t s)
 {
-  k_loop_cond<<<1, 1, 0, s>>>(k, h, cap);
+  fb_launch(k_loop_cond, 1, 1, 0, s, k, h, cap);
 }

@@ -352,6 +352,7 @@ __global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_fwd(FftArgs fa, int nrow
                                                       const double *in_r, const double *in_t,
                                                       double2 *out_r, double2 *out_t)
 {
+  fb_grid_dependency();
   extern __shared__ double2 sm[];
   double2 *x = sm, *y = sm + ns + ns / 16;  // padded lines
   const int i = blockIdx.x;
@@ -388,6 +389,7 @@ __global__ void __launch_bounds__(SG_BS) sg_cols(FftArgs fa, int nrows_in, int n
                                                   double2 *data_r, double2 *data_t,
                                                   double2 *kh_r, double2 *kh_t)
 {
+  fb_grid_dependency();
   extern __shared__ double2 sm[];
   const int m = fa.n;
   double2 *x = sm, *y = sm + SG_KC * m;  // SG_KC lines each
@@ -557,6 +559,7 @@ static __device__ void col_fft(double2 *X, int lgm, const FftArgs &a)
 __global__ void __launch_bounds__(128, 4) sg_cols_p2(FftArgs fa, int lgm, int nrows_in, int nk, int mode,
                                                  double2 *data_r, double2 *data_t, double2 *kh_r, double2 *kh_t)
 {
+  fb_grid_dependency();
   extern __shared__ double2 sm[];
   const int m = 1 << lgm, mp = m + m / 16, T = blockDim.x, tid = threadIdx.x;
   const int k0 = blockIdx.x * SG_KC2;
@@ -613,6 +616,7 @@ __global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_inv(FftArgs fa, int ns, 
                                                       double selfk_rstep, double selfk_tstep,
                                                       double eps, double *accr, double *acct)
 {
+  fb_grid_dependency();
   extern __shared__ double2 sm[];
   double2 *x = sm, *y = sm + ns + ns / 16;  // padded lines
   const int i = blockIdx.x;
@@ -648,6 +652,7 @@ __global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_inv(FftArgs fa, int ns, 
 // RadSGAcc / AziSGAcc grids the particles read.
 __global__ void __launch_bounds__(SG_BS) sg_update(KP k, int refresh)
 {
+  fb_grid_dependency();
   const int ns = k.ns;
   const size_t n = (size_t)k.nr * ns;
   const double Dt = refresh ? 0.0 : k.ctl->dt;
@@ -784,12 +789,12 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   cudaMemcpy(dkr, kr.data(), kr.size() * sizeof(double), cudaMemcpyHostToDevice);
   cudaMemcpy(dkt, kt.data(), kt.size() * sizeof(double), cudaMemcpyHostToDevice);
   FftArgs fc = fft_args(sg->pcol);
-  sg_rows_fwd<<<m, SG_ROW_BS, sg->smem_row, s>>>(sg->frow, m, ns, nk, NULL, NULL, NULL, 1.0, dkr, dkt, hr, ht);
+  fb_launch(sg_rows_fwd, m, SG_ROW_BS, sg->smem_row, s, sg->frow, m, ns, nk, nullptr, nullptr, nullptr, 1.0, dkr, dkt, hr, ht);
   if (sg->p2)
-    sg_cols_p2<<<dim3((nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * m / 16, sg->smem_col2, s>>>(sg->fc2, sg->lgm, m, nk, 0,
+    fb_launch(sg_cols_p2, dim3((nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * m / 16, sg->smem_col2, s, sg->fc2, sg->lgm, m, nk, 0,
                                                                                           hr, ht, sg->khr, sg->kht);
   else
-    sg_cols<<<dim3((nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s>>>(fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
+    fb_launch(sg_cols, dim3((nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s, fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
   cudaError_t e = cudaStreamSynchronize(s);
   cudaFree(dkr); cudaFree(dkt); cudaFree(hr); cudaFree(ht);
   if (e != cudaSuccess) { fb_sg_destroy(sg); return FB_ERR_CUDA; }
@@ -810,25 +815,25 @@ void fb_sg_destroy(fb_sg *sg)
 void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 {
   (void)k;
-  sg_rows_fwd<<<sg->nr, SG_ROW_BS, sg->smem_row, s>>>(sg->frow, sg->nr, sg->ns, sg->nk, dens, sg->sq, sg->rr, sg->r0,
-                                                   NULL, NULL, sg->xr, sg->xt);
+  fb_launch(sg_rows_fwd, sg->nr, SG_ROW_BS, sg->smem_row, s, sg->frow, sg->nr, sg->ns, sg->nk, dens, sg->sq, sg->rr, sg->r0,
+                                                   nullptr, nullptr, sg->xr, sg->xt);
 }
 
 void fb_sg_cols(fb_sg *sg, cudaStream_t s)
 {
   if (sg->p2) {
-    sg_cols_p2<<<dim3((sg->nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * sg->m / 16, sg->smem_col2, s>>>(
+    fb_launch(sg_cols_p2, dim3((sg->nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * sg->m / 16, sg->smem_col2, s, 
         sg->fc2, sg->lgm, sg->nr, sg->nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
     return;
   }
   FftArgs fc = fft_args(sg->pcol);
-  sg_cols<<<dim3((sg->nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s>>>(fc, sg->nr, sg->nk, 1, sg->xr, sg->xt,
+  fb_launch(sg_cols, dim3((sg->nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s, fc, sg->nr, sg->nk, 1, sg->xr, sg->xt,
                                                                          sg->khr, sg->kht);
 }
 
 void fb_sg_rows_inv(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 {
-  sg_rows_inv<<<sg->nr, SG_ROW_BS, sg->smem_row, s>>>(sg->frow, sg->ns, sg->nk, sg->xr, sg->xt, sg->nr_accr, sg->nr_acct,
+  fb_launch(sg_rows_inv, sg->nr, SG_ROW_BS, sg->smem_row, s, sg->frow, sg->ns, sg->nk, sg->xr, sg->xt, sg->nr_accr, sg->nr_acct,
                                                    dens, sg->rstep, sg->tstep, sg->eps, k.sg_accr, k.sg_acct);
 }
 
@@ -842,7 +847,7 @@ void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 void fb_sg_update_velocities(const KP &k, cudaStream_t s, int refresh)
 {
   const size_t n = (size_t)k.nr * k.ns;
-  sg_update<<<(int)((n + SG_BS - 1) / SG_BS), SG_BS, 0, s>>>(k, refresh);
+  fb_launch(sg_update, (int)((n + SG_BS - 1) / SG_BS), SG_BS, 0, s, k, refresh);
 }
 
 int fb_sg_launches(const fb_sg *sg) { return sg ? 4 : 0; }
