@@ -642,40 +642,58 @@ __global__ void __launch_bounds__(FB_BS2) k_substep1(KP k)
   fb_grid_dependency();
   const int ns = k.ns;
   const double dt = k.ctl->dt;
-  {
-    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= ns) return;
-    const size_t l = (size_t)i * ns + j;
-    const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
-    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
-    const double Pl = pressure_at(k, l);
-    k.pres[l] = Pl;
-    if (i >= 1) {
-      const size_t lim = l - ns;
-      const double Plim = pressure_at(k, lim);
-      double gradp = (Pl - Plim) * 2.0 / (k.rho[l] + k.rho[lim]) * k.invdiffrmed[i];
-      double gradphi = (k.pot[l] - k.pot[lim]) * k.invdiffrmed[i];
-      double vt2 = k.vt[l] + k.vt[ljp] + k.vt[lim] + k.vt[ljp - ns];
-      vt2 = vt2 / 4.0 + k.rinf[i] * k.omega_frame;
-      vt2 = vt2 * vt2;
-      k.vri[l] = k.vr[l] + dt * (-gradp - gradphi + vt2 * k.invrinf[i]);
-      if (k.particles) {  // RadGradP, RadIndAcc (SourceEuler.c:875-877)
-        k.rgp[l] = (Pl - Plim) * k.invdiffrmed[i];
-        k.rind[l] = -(k.indpot[l] - k.indpot[lim]) * k.invdiffrmed[i];
-      }
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const size_t l = (size_t)i * ns + j;
+  const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+  const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+  const size_t lim = (i >= 1) ? l - ns : l;
+  // every load first (the stores below could alias them for the compiler)
+  const double Pl = pressure_at(k, l), Pjm = pressure_at(k, ljm);
+  const double rl = k.rho[l], rjm = k.rho[ljm], potl = k.pot[l], potjm = k.pot[ljm], vtl = k.vt[l];
+  const double invdxtheta = k.invdxtheta[i], torque = k.supp_torque[i];
+  double Plim = 0.0, rlim = 0.0, potlim = 0.0, vtjp = 0.0, vtlim = 0.0, vtjplim = 0.0, vrl = 0.0;
+  double invdiffrmed = 0.0, rinf = 0.0, invrinf = 0.0;
+  if (i >= 1) {
+    Plim = pressure_at(k, lim);
+    rlim = k.rho[lim];
+    potlim = k.pot[lim];
+    vtjp = k.vt[ljp];
+    vtlim = k.vt[lim];
+    vtjplim = k.vt[ljp - ns];
+    vrl = k.vr[l];
+    invdiffrmed = k.invdiffrmed[i];
+    rinf = k.rinf[i];
+    invrinf = k.invrinf[i];
+  }
+  double ipl = 0.0, iplim = 0.0, ipjm = 0.0;
+  if (k.particles) {
+    ipl = k.indpot[l];
+    ipjm = k.indpot[ljm];
+    if (i >= 1) iplim = k.indpot[lim];
+  }
+  k.pres[l] = Pl;
+  if (i >= 1) {
+    double gradp = (Pl - Plim) * 2.0 / (rl + rlim) * invdiffrmed;
+    double gradphi = (potl - potlim) * invdiffrmed;
+    double vt2 = vtl + vtjp + vtlim + vtjplim;
+    vt2 = vt2 / 4.0 + rinf * k.omega_frame;
+    vt2 = vt2 * vt2;
+    k.vri[l] = vrl + dt * (-gradp - gradphi + vt2 * invrinf);
+    if (k.particles) {  // RadGradP, RadIndAcc (SourceEuler.c:875-877)
+      k.rgp[l] = (Pl - Plim) * invdiffrmed;
+      k.rind[l] = -(ipl - iplim) * invdiffrmed;
     }
-    {
-      const double Pjm = pressure_at(k, ljm);
-      const double invdxtheta = k.invdxtheta[i];
-      double gradp = (Pl - Pjm) * 2.0 / (k.rho[l] + k.rho[ljm]) * invdxtheta;
-      double gradphi = (k.pot[l] - k.pot[ljm]) * invdxtheta;
-      double vti = k.vt[l] - dt * (gradp + gradphi);
-      vti += dt * k.supp_torque[i];
-      k.vti[l] = vti;
-      if (k.particles) {  // AziGradP, AziIndAcc (SourceEuler.c:944-951)
-        k.agp[l] = (Pl - Pjm) * invdxtheta;
-        k.aind[l] = -(k.indpot[l] - k.indpot[ljm]) * invdxtheta;
-      }
+  }
+  {
+    double gradp = (Pl - Pjm) * 2.0 / (rl + rjm) * invdxtheta;
+    double gradphi = (potl - potjm) * invdxtheta;
+    double vti = vtl - dt * (gradp + gradphi);
+    vti += dt * torque;
+    k.vti[l] = vti;
+    if (k.particles) {  // AziGradP, AziIndAcc (SourceEuler.c:944-951)
+      k.agp[l] = (Pl - Pjm) * invdxtheta;
+      k.aind[l] = -(ipl - ipjm) * invdxtheta;
     }
   }
 }
@@ -694,28 +712,38 @@ __global__ void __launch_bounds__(FB_BS2) k_viscous_terms(KP k, const double *__
   fb_grid_dependency();
   const int ns = k.ns;
   const double invdphi = k.invdphi, onethird = 1.0 / 3.0;
-  {
-    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= ns) return;
-    const size_t l = (size_t)i * ns + j;
-    const size_t lip = l + ns;
-    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
-    double div = (vr[lip] * k.rsup[i] - vr[l] * k.rinf[i]) * k.invdiffrsup[i] * k.invrmed[i];
-    div += (vt[ljp] - vt[l]) * invdphi * k.invrmed[i];
-    k.divv[l] = div;
-    const double Drr = (vr[lip] - vr[l]) * k.invdiffrsup[i];
-    const double Dpp = (vt[ljp] - vt[l]) * invdphi * k.invrmed[i] + 0.5 * (vr[lip] + vr[l]) * k.invrmed[i];
-    const double viscosity = nu_ring(k, i);
-    k.trr[l] = 2.0 * k.rho[l] * viscosity * (Drr - onethird * div);
-    k.tpp[l] = 2.0 * k.rho[l] * viscosity * (Dpp - onethird * div);
-    if (i >= 1) {
-      const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
-      const size_t lim = l - ns;
-      const size_t ljmim = ljm - ns;
-      const double Drp = 0.5 * (k.rinf[i] * (vt[l] * k.invrmed[i] - vt[lim] * k.invrmed[i - 1]) * k.invdiffrmed[i] +
-                                (vr[l] - vr[ljm]) * invdphi * k.invrinf[i]);
-      k.trp[l] = 2.0 * 0.25 * (k.rho[l] + k.rho[lim] + k.rho[ljm] + k.rho[ljmim]) * viscosity * Drp;
-    }
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const size_t l = (size_t)i * ns + j;
+  const size_t lip = l + ns;
+  const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+  const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+  // every load first
+  const double vrl = vr[l], vrip = vr[lip], vtl = vt[l], vtjp = vt[ljp], rl = k.rho[l];
+  const double rsup = k.rsup[i], rinf = k.rinf[i], invdiffrsup = k.invdiffrsup[i], invrmed = k.invrmed[i];
+  double vtim = 0.0, vrjm = 0.0, rim = 0.0, rjm = 0.0, rjmim = 0.0, invrmedm = 0.0, invdiffrmed = 0.0, invrinf = 0.0;
+  if (i >= 1) {
+    const size_t lim = l - ns, ljmim = ljm - ns;
+    vtim = vt[lim];
+    vrjm = vr[ljm];
+    rim = k.rho[lim];
+    rjm = k.rho[ljm];
+    rjmim = k.rho[ljmim];
+    invrmedm = k.invrmed[i - 1];
+    invdiffrmed = k.invdiffrmed[i];
+    invrinf = k.invrinf[i];
+  }
+  double div = (vrip * rsup - vrl * rinf) * invdiffrsup * invrmed;
+  div += (vtjp - vtl) * invdphi * invrmed;
+  k.divv[l] = div;
+  const double Drr = (vrip - vrl) * invdiffrsup;
+  const double Dpp = (vtjp - vtl) * invdphi * invrmed + 0.5 * (vrip + vrl) * invrmed;
+  const double viscosity = nu_ring(k, i);
+  k.trr[l] = 2.0 * rl * viscosity * (Drr - onethird * div);
+  k.tpp[l] = 2.0 * rl * viscosity * (Dpp - onethird * div);
+  if (i >= 1) {
+    const double Drp = 0.5 * (rinf * (vtl * invrmed - vtim * invrmedm) * invdiffrmed + (vrl - vrjm) * invdphi * invrinf);
+    k.trp[l] = 2.0 * 0.25 * (rl + rim + rjm + rjmim) * viscosity * Drp;
   }
 }
 
@@ -730,25 +758,29 @@ __global__ void __launch_bounds__(FB_BS2) k_viscous_update(KP k, double *vr, dou
   fb_grid_dependency();
   const int ns = k.ns, nr = k.nr;
   const double DeltaT = dt_of(k, dtov), invdphi = k.invdphi;
-  {
-    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= ns) return;
-    const size_t l = (size_t)i * ns + j;
-    if (i < 1) return;
-    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
-    const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
-    const size_t lim = l - ns, lip = l + ns;
-    if (i < nr - 1) {
-      vt[l] += DeltaT * k.invrmed[i] *
-               ((k.rsup[i] * k.trp[lip] - k.rinf[i] * k.trp[l]) * k.invdiffrsup[i] +
-                (k.tpp[l] - k.tpp[ljm]) * invdphi + 0.5 * (k.trp[l] + k.trp[lip])) /
-               (0.5 * (k.rho[l] + k.rho[ljm]));
-    }
-    vr[l] += DeltaT * k.invrinf[i] *
-             ((k.rmed[i] * k.trr[l] - k.rmed[i - 1] * k.trr[lim]) * k.invdiffrmed[i] +
-              (k.trp[ljp] - k.trp[l]) * invdphi - 0.5 * (k.tpp[l] + k.tpp[lim])) /
-             (0.5 * (k.rho[l] + k.rho[lim]));
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const size_t l = (size_t)i * ns + j;
+  if (i < 1) return;
+  const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+  const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+  const size_t lim = l - ns, lip = l + ns;
+  // every load first
+  const double trpl = k.trp[l], trpip = k.trp[lip], trpjp = k.trp[ljp];
+  const double tppl = k.tpp[l], tppjm = k.tpp[ljm], tppim = k.tpp[lim];
+  const double trrl = k.trr[l], trrim = k.trr[lim];
+  const double rl = k.rho[l], rjm = k.rho[ljm], rim = k.rho[lim];
+  const double vtl = vt[l], vrl = vr[l];
+  const double invrmed = k.invrmed[i], rsup = k.rsup[i], rinf = k.rinf[i], invdiffrsup = k.invdiffrsup[i];
+  const double invrinf = k.invrinf[i], rmed = k.rmed[i], rmedm = k.rmed[i - 1], invdiffrmed = k.invdiffrmed[i];
+  if (i < nr - 1) {
+    vt[l] = vtl + DeltaT * invrmed *
+                      ((rsup * trpip - rinf * trpl) * invdiffrsup + (tppl - tppjm) * invdphi + 0.5 * (trpl + trpip)) /
+                      (0.5 * (rl + rjm));
   }
+  vr[l] = vrl + DeltaT * invrinf *
+                    ((rmed * trrl - rmedm * trrim) * invdiffrmed + (trpjp - trpl) * invdphi - 0.5 * (tppl + tppim)) /
+                    (0.5 * (rl + rim));
 }
 
 void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s)
@@ -778,38 +810,41 @@ __global__ void __launch_bounds__(FB_BS2) k_substep2(KP k)
   fb_grid_dependency();
   const int ns = k.ns, nr = k.nr;
   const double dt = k.ctl->dt;
-  {
-    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= ns) return;
-    const size_t l = (size_t)i * ns + j;
-    if (i == nr) {
-      k.vr[l] = 0.0;
-      k.vt[l] = 0.0;
-      if (k.energy) k.e[l] = 0.0;
-      return;
-    }
-    const size_t lip = l + ns;
-    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
-    const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
-    const double qr = q_r(k, l, lip);
-    const double qt = q_t(k, l, ljp);
-    if (i >= 1) {
-      const size_t lim = l - ns;
-      const double qrim = q_r(k, lim, l);
-      k.vr[l] = k.vri[l] - dt * 2.0 / (k.rho[l] + k.rho[lim]) * (qr - qrim) * k.invdiffrmed[i];
-    } else {
-      k.vr[l] = 0.0;
-    }
-    {
-      const double qtjm = q_t(k, ljm, l);
-      const double invdxtheta = k.invdxtheta[i];
-      k.vt[l] = k.vti[l] - dt * 2.0 / (k.rho[l] + k.rho[ljm]) * (qt - qtjm) * invdxtheta;
-      if (k.energy) {
-        k.e[l] = k.e[l] - dt * qr * (k.vri[lip] - k.vri[l]) * k.invdiffrsup[i] -
-                 dt * qt * (k.vti[ljp] - k.vti[l]) * invdxtheta;
-      }
-    }
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const size_t l = (size_t)i * ns + j;
+  if (i == nr) {
+    k.vr[l] = 0.0;
+    k.vt[l] = 0.0;
+    if (k.energy) k.e[l] = 0.0;
+    return;
   }
+  const size_t lip = l + ns;
+  const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+  const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+  const size_t lim = (i >= 1) ? l - ns : l;
+  // every load first
+  const double qr = q_r(k, l, lip);
+  const double qt = q_t(k, l, ljp);
+  const double qtjm = q_t(k, ljm, l);
+  const double qrim = (i >= 1) ? q_r(k, lim, l) : 0.0;
+  const double rl = k.rho[l], rlim = k.rho[lim], rjm = k.rho[ljm];
+  const double vril = k.vri[l], vtil = k.vti[l];
+  const double invdxtheta = k.invdxtheta[i], invdiffrmed = k.invdiffrmed[i];
+  double el = 0.0, vrip = 0.0, vtijp = 0.0, invdiffrsup = 0.0;
+  if (k.energy) {
+    el = k.e[l];
+    vrip = k.vri[lip];
+    vtijp = k.vti[ljp];
+    invdiffrsup = k.invdiffrsup[i];
+  }
+  if (i >= 1)
+    k.vr[l] = vril - dt * 2.0 / (rl + rlim) * (qr - qrim) * invdiffrmed;
+  else
+    k.vr[l] = 0.0;
+  k.vt[l] = vtil - dt * 2.0 / (rl + rjm) * (qt - qtjm) * invdxtheta;
+  if (k.energy)
+    k.e[l] = el - dt * qr * (vrip - vril) * invdiffrsup - dt * qt * (vtijp - vtil) * invdxtheta;
 }
 
 void fb_launch_substep2(const KP &k, cudaStream_t s)

@@ -654,23 +654,32 @@ __global__ void __launch_bounds__(SG_BS) sg_update(KP k, int refresh)
 {
   fb_grid_dependency();
   const int ns = k.ns;
-  const size_t n = (size_t)k.nr * ns;
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
   const double Dt = refresh ? 0.0 : k.ctl->dt;
   double *vr = refresh ? k.vr : k.vri;
   double *vt = refresh ? k.vt : k.vti;
-  for (size_t l = (size_t)blockIdx.x * SG_BS + threadIdx.x; l < n; l += (size_t)gridDim.x * SG_BS) {
-    const int i = (int)(l / ns), j = (int)(l - (size_t)i * ns);
-    if (i > 0) {
-      const double radsgacc = ((k.rinf[i] - k.rmed[i - 1]) * k.sg_accr[l] +
-                               (k.rmed[i] - k.rinf[i]) * k.sg_accr[l - ns]) * k.invdiffrmed[i];
-      vr[l] += Dt * radsgacc;
-      if (k.particles) k.rsga[l] = radsgacc;
-    }
-    const size_t lm1 = (size_t)i * ns + (j == 0 ? ns - 1 : j - 1);
-    const double azisgacc = 0.5 * (k.sg_acct[l] + k.sg_acct[lm1]);
-    vt[l] += Dt * azisgacc;
-    if (k.particles) k.asga[l] = azisgacc;
+  const size_t l = (size_t)i * ns + j;
+  const size_t lm1 = (size_t)i * ns + (j == 0 ? ns - 1 : j - 1);
+  // every load first
+  const double at0 = k.sg_acct[l], at1 = k.sg_acct[lm1], vtl = vt[l];
+  double ar0 = 0.0, ar1 = 0.0, vrl = 0.0, c0 = 0.0, c1 = 0.0, invd = 0.0;
+  if (i > 0) {
+    ar0 = k.sg_accr[l];
+    ar1 = k.sg_accr[l - ns];
+    vrl = vr[l];
+    c0 = k.rinf[i] - k.rmed[i - 1];
+    c1 = k.rmed[i] - k.rinf[i];
+    invd = k.invdiffrmed[i];
   }
+  if (i > 0) {
+    const double radsgacc = (c0 * ar0 + c1 * ar1) * invd;
+    vr[l] = vrl + Dt * radsgacc;
+    if (k.particles) k.rsga[l] = radsgacc;
+  }
+  const double azisgacc = 0.5 * (at0 + at1);
+  vt[l] = vtl + Dt * azisgacc;
+  if (k.particles) k.asga[l] = azisgacc;
 }
 
 // ------------------------------------------------------------------- host
@@ -846,8 +855,7 @@ void fb_sg_accel(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 
 void fb_sg_update_velocities(const KP &k, cudaStream_t s, int refresh)
 {
-  const size_t n = (size_t)k.nr * k.ns;
-  fb_launch(sg_update, (int)((n + SG_BS - 1) / SG_BS), SG_BS, 0, s, k, refresh);
+  fb_launch(sg_update, dim3((k.ns + SG_BS - 1) / SG_BS, k.nr), SG_BS, 0, s, k, refresh);
 }
 
 int fb_sg_launches(const fb_sg *sg) { return sg ? 4 : 0; }
