@@ -353,6 +353,7 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.vh_l2 = log(g.rmed[1] / g.rmed[2]);
   k.ringmin = dalloc(ctx, nr);
   k.vmoy = dalloc(ctx, nr);
+  k.vt_part = dalloc(ctx, (size_t)nr * ((ns + 31) / 32));  // CTAs of >= 32 azimuths
   {
     // the CFL kernel leaves one set of force/mass partials per ring
     const int nb = nr;

@@ -67,6 +67,7 @@ struct KP {
   double vh_l1, vh_l2;     // log(r/rip), log(rip/ri2p) for ViscHeat at i=0
   // CFL / reductions
   double *ringmin, *vmoy;
+  double *vt_part;  // beta cooling: per ring, SubStep2's partial sums of vtheta (one per CTA)
   double *partials;
   int n_partial_blocks;
   fb_ctl *ctl;

@@ -811,40 +811,59 @@ __global__ void __launch_bounds__(FB_BS2) k_substep2(KP k)
   const int ns = k.ns, nr = k.nr;
   const double dt = k.ctl->dt;
   const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ns) return;
+  const bool cell = (j < ns);
   const size_t l = (size_t)i * ns + j;
-  if (i == nr) {
+  if (i == nr) {  // the whole CTA
+    if (!cell) return;
     k.vr[l] = 0.0;
     k.vt[l] = 0.0;
     if (k.energy) k.e[l] = 0.0;
     return;
   }
-  const size_t lip = l + ns;
-  const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
-  const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
-  const size_t lim = (i >= 1) ? l - ns : l;
-  // every load first
-  const double qr = q_r(k, l, lip);
-  const double qt = q_t(k, l, ljp);
-  const double qtjm = q_t(k, ljm, l);
-  const double qrim = (i >= 1) ? q_r(k, lim, l) : 0.0;
-  const double rl = k.rho[l], rlim = k.rho[lim], rjm = k.rho[ljm];
-  const double vril = k.vri[l], vtil = k.vti[l];
-  const double invdxtheta = k.invdxtheta[i], invdiffrmed = k.invdiffrmed[i];
-  double el = 0.0, vrip = 0.0, vtijp = 0.0, invdiffrsup = 0.0;
-  if (k.energy) {
-    el = k.e[l];
-    vrip = k.vri[lip];
-    vtijp = k.vti[ljp];
-    invdiffrsup = k.invdiffrsup[i];
+  double vtnew = 0.0;
+  if (cell) {
+    const size_t lip = l + ns;
+    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
+    const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
+    const size_t lim = (i >= 1) ? l - ns : l;
+    // every load first
+    const double qr = q_r(k, l, lip);
+    const double qt = q_t(k, l, ljp);
+    const double qtjm = q_t(k, ljm, l);
+    const double qrim = (i >= 1) ? q_r(k, lim, l) : 0.0;
+    const double rl = k.rho[l], rlim = k.rho[lim], rjm = k.rho[ljm];
+    const double vril = k.vri[l], vtil = k.vti[l];
+    const double invdxtheta = k.invdxtheta[i], invdiffrmed = k.invdiffrmed[i];
+    double el = 0.0, vrip = 0.0, vtijp = 0.0, invdiffrsup = 0.0;
+    if (k.energy) {
+      el = k.e[l];
+      vrip = k.vri[lip];
+      vtijp = k.vti[ljp];
+      invdiffrsup = k.invdiffrsup[i];
+    }
+    if (i >= 1)
+      k.vr[l] = vril - dt * 2.0 / (rl + rlim) * (qr - qrim) * invdiffrmed;
+    else
+      k.vr[l] = 0.0;
+    vtnew = vtil - dt * 2.0 / (rl + rjm) * (qt - qtjm) * invdxtheta;
+    k.vt[l] = vtnew;
+    if (k.energy)
+      k.e[l] = el - dt * qr * (vrip - vril) * invdiffrsup - dt * qt * (vtijp - vtil) * invdxtheta;
   }
-  if (i >= 1)
-    k.vr[l] = vril - dt * 2.0 / (rl + rlim) * (qr - qrim) * invdiffrmed;
-  else
-    k.vr[l] = 0.0;
-  k.vt[l] = vtil - dt * 2.0 / (rl + rjm) * (qt - qtjm) * invdxtheta;
-  if (k.energy)
-    k.e[l] = el - dt * qr * (vrip - vril) * invdiffrsup - dt * qt * (vtijp - vtil) * invdxtheta;
+  if (k.energy && k.beta_cooling) {
+    // SubStep3's ring mean of vtheta (SourceEuler.c:1196-1203): this CTA's
+    // part, summed in a fixed order
+    __shared__ double sh[FB_BS2 / 32];
+    double v = cell ? (vtnew + k.rmed[i] * k.omega_frame) : 0.0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += sh[w];
+      k.vt_part[(size_t)i * gridDim.x + blockIdx.x] = t;
+    }
+  }
 }
 
 void fb_launch_substep2(const KP &k, cudaStream_t s)
@@ -892,22 +911,24 @@ static __device__ __forceinline__ double vischeat_at(const KP &k, int i, size_t 
 // (SourceEuler.c:1119-1302; pdV, viscous heating, beta cooling), one CTA
 // per ring because beta cooling needs the ring mean of vtheta.  Writes
 // Energy = EnergyNew (ring nr of EnergyNew is never written: zero).
-__global__ void __launch_bounds__(FB_BS) k_substep3(KP k)
+__global__ void __launch_bounds__(FB_BS2) k_substep3(KP k)
 {
   fb_grid_dependency();
-  __shared__ double sh[32];
-  const int i = blockIdx.x, ns = k.ns, nr = k.nr;
-  const double dt = k.ctl->dt;
-  const size_t base = (size_t)i * ns;
+  const int ns = k.ns, nr = k.nr;
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const size_t l = (size_t)i * ns + j;
   if (i == nr) {
-    for (int j = threadIdx.x; j < ns; j += FB_BS) k.e[base + j] = 0.0;
+    k.e[l] = 0.0;
     return;
   }
+  const double dt = k.ctl->dt;
   double coolfac = 0.0;
   if (k.beta_cooling) {
+    // the ring mean of vtheta from SubStep2's partial sums (same CTA width)
     double s = 0.0;
-    for (int j = threadIdx.x; j < ns; j += FB_BS) s += (k.vt[base + j] + k.rmed[i] * k.omega_frame);
-    double omega = block_sum<FB_BS>(s, sh);
+    for (int b = 0; b < (int)gridDim.x; b++) s += k.vt_part[(size_t)i * gridDim.x + b];
+    double omega = s;
     omega /= (double)ns;
     omega /= k.rmed[i];
     double coolingtime = k.betatab[i] / omega;
@@ -916,31 +937,29 @@ __global__ void __launch_bounds__(FB_BS) k_substep3(KP k)
   // the i = 0 extrapolation tests the viscosity of the last ring visited by
   // the i >= 1 loop (ring nr-1), SourceEuler.c:1598
   const double visc_last = nu_ring(k, nr - 1);
-  for (int j = threadIdx.x; j < ns; j += FB_BS) {
-    const size_t l = base + j;
-    double vh = 0.0;
-    if (k.viscous_heating) {
-      if (i >= 1) {
-        vh = vischeat_at(k, i, l);
-      } else {
-        const double qpip = vischeat_at(k, 1, l + ns);
-        const double qpi2p = vischeat_at(k, 2, l + 2 * ns);
-        vh = (visc_last != 0.0) ? qpip * exp(log(qpip / qpi2p) * k.vh_l1 / k.vh_l2) : 0.0;
-      }
-      k.vischeat[l] = vh;
+  double vh = 0.0;
+  if (k.viscous_heating) {
+    if (i >= 1) {
+      vh = vischeat_at(k, i, l);
+    } else {
+      const double qpip = vischeat_at(k, 1, l + ns);
+      const double qpi2p = vischeat_at(k, 2, l + 2 * ns);
+      vh = (visc_last != 0.0) ? qpip * exp(log(qpip / qpi2p) * k.vh_l1 / k.vh_l2) : 0.0;
     }
-    double num = k.e[l] + (double)(k.viscous_heating ? 1 : 0) * vh * dt;
-    double den = 1.0 + (k.gamma - 1.0) * dt * k.divv[l];
-    double en = num / den;
-    if (k.beta_cooling) {
-      double d2 = 1.0 + dt / coolfac;
-      en = en / d2;
-    }
-    k.e[l] = en;
   }
+  const double el = k.e[l], dv = k.divv[l];
+  if (k.viscous_heating) k.vischeat[l] = vh;
+  double num = el + (double)(k.viscous_heating ? 1 : 0) * vh * dt;
+  double den = 1.0 + (k.gamma - 1.0) * dt * dv;
+  double en = num / den;
+  if (k.beta_cooling) {
+    double d2 = 1.0 + dt / coolfac;
+    en = en / d2;
+  }
+  k.e[l] = en;
 }
 
-void fb_launch_substep3(const KP &k, cudaStream_t s) { fb_launch(k_substep3, k.nr + 1, FB_BS, 0, s, k); }
+void fb_launch_substep3(const KP &k, cudaStream_t s) { fb_launch(k_substep3, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k); }
 
 // ------------------------------------------------------------ Transport
 // Radial pass of the van Leer transport (OneWindRad, TransportEuler.c:124-220
