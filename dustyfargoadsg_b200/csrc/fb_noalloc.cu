@@ -4,10 +4,10 @@
 //
 // Who needs it: a host code that embeds the step inside another GPU
 // application which owns the whole device-memory budget (its own pool or
-// allocator), or that runs the call from a latency-critical or captured
-// region where cudaMalloc/cudaFree are not acceptable (they may synchronize
-// the device and are not recorded by stream capture).  Such a caller passes
-// its own device buffers for the fields and gets no hidden allocation.
+// allocator), or that runs the call from a latency-critical region where
+// cudaMalloc/cudaFree are not acceptable (they may synchronize the device).
+// Such a caller passes its own device buffers for the fields and gets no
+// hidden allocation.
 //
 // The scratch the transport kernels need between their radial and azimuthal
 // passes (six transported quantities and the post-transport density, one
