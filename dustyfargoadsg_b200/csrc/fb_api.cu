@@ -1195,7 +1195,7 @@ extern "C" int fb_get_tuning(const fb_ctx *ctx, fb_tuning *t)
   t->azi_cells_per_thread = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
   t->rad_columns = k.rad_tx > 0 ? k.rad_tx : 64;
   t->rad_rings = k.rad_chunk > 0 ? k.rad_chunk : fb_rad_chunk_auto(k);
-  t->azi_variant = fb_azi_wide(k.ns, k.energy, t->azi_cells_per_thread, k.azi_variant) ? 2 : 1;
+  t->azi_variant = fb_azi_variant(k.ns, k.energy, t->azi_cells_per_thread, k.azi_variant);
   return FB_OK;
 }
 
@@ -1208,9 +1208,9 @@ extern "C" int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t)
   if (t->azi_cells_per_thread && !fb_azi_E_valid(k.ns, k.energy, t->azi_cells_per_thread)) return FB_ERR_INVALID;
   if (t->rad_columns && (t->rad_columns < 32 || t->rad_columns > 128 || t->rad_columns % 32)) return FB_ERR_INVALID;
   if (t->rad_rings < 0 || t->rad_rings > k.nr) return FB_ERR_INVALID;
-  if (t->azi_variant < 0 || t->azi_variant > 2) return FB_ERR_INVALID;
   const int E = t->azi_cells_per_thread ? t->azi_cells_per_thread : fb_azi_E_auto(k.ns);
-  if (t->azi_variant == 2 && !fb_azi_wide(k.ns, k.energy, E, 2)) return FB_ERR_INVALID;
+  if (t->azi_variant < 0 || t->azi_variant > 3 || !fb_azi_variant(k.ns, k.energy, E, t->azi_variant))
+    return FB_ERR_INVALID;
   k.cell_bs = cb;
   k.azi_variant = t->azi_variant;
   k.azi_E = t->azi_cells_per_thread;
@@ -1326,8 +1326,8 @@ extern "C" int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_ou
     double bestms = 1e300;
     for (int E = 1; E <= 4; E++) {
       if (!fb_azi_E_valid(k.ns, k.energy, E)) continue;
-      for (int var = 1; var <= 2; var++) {
-        if (var == 2 && !fb_azi_wide(k.ns, k.energy, E, 2)) continue;
+      for (int var = 1; var <= 3; var++) {
+        if (fb_azi_variant(k.ns, k.energy, E, var) != var) continue;
         k.azi_E = E;
         k.azi_variant = var;
         const double ms = tune_measure(ctx, sn, substeps, azi_stage, 1);

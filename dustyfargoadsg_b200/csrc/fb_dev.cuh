@@ -94,7 +94,7 @@ struct KP {
   // launch shapes (tuning): per-cell CTA width, cells per thread of the
   // azimuthal pass (0 = automatic), columns per CTA and rings per CTA of the
   // radial pass (0 = automatic), variant of the azimuthal pass (0 automatic,
-  // 1 narrow, 2 wide)
+  // 1 narrow, 2 wide, 3 packed)
   int cell_bs, azi_E, rad_tx, rad_chunk, azi_variant;
 };
 
@@ -205,7 +205,7 @@ int  fb_gas_prepare(int ns, int energy);  // kernel attributes (shared memory)
 // launch-shape candidates the tuner may try (fb_gas.cu)
 int  fb_azi_E_valid(int ns, int energy, int E);   // 1 if E cells/thread fit this ring
 int  fb_azi_E_auto(int ns);
-int  fb_azi_wide(int ns, int energy, int E, int variant);  // 1 if a launch takes the wide variant
+int  fb_azi_variant(int ns, int energy, int E, int variant);  // variant a launch takes (0: cannot run)
 int  fb_rad_chunk_auto(const KP &k);
 int  fb_allow_max_dynamic_smem(const void *func);
 void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s);

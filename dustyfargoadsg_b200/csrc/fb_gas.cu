@@ -1374,6 +1374,228 @@ __global__ void __launch_bounds__(AziMaxThreads<E, WIDE>::value) k_transport_azi
 #undef jc
 }
 
+// Packed variant of the azimuthal pass: the same phases as the wide variant,
+// with cell j's quantities side by side at P[6j .. 6j+5] (RadMomP, RadMomM,
+// ThetaMomP, ThetaMomM, [Energy,] Rho; without energy the sixth slot is
+// unused) and their slopes likewise, so one address per face serves every
+// quantity through 16-byte shared accesses, two quantities at a time
+// (48-byte cells: conflict-free per quarter warp).  Rings: 2 x 6 + 2 of
+// nsec doubles.
+#define AZP 6
+template <int NQ, int E, bool FULL>
+__global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_packed(KP k, double dtov)
+{
+  fb_grid_dependency();
+  extern __shared__ double2 smem2[];
+  __shared__ double sh[32];
+  const double dt = dt_of(k, dtov);
+  const int i = blockIdx.x, ns = k.ns, nr = k.nr, T = blockDim.x, tid = threadIdx.x;
+  const size_t base = (size_t)i * ns;
+  constexpr int RH = NQ - 1;          // slot of the density
+  double *P = (double *)smem2;        // ns cells x 6
+  double *PD = P + AZP * ns;          // slopes, ns x 6
+  double *vres = PD + AZP * ns;       // residual azimuthal velocity
+  double *DR = vres + ns;             // density slopes (RhoStar)
+  // a cell's slot pair (2h, 2h+1) as one 16-byte access: 48-byte cells keep
+  // these free of bank conflicts, single 8-byte slots would not be
+  auto pair = [&](const double *A, int j, int h) -> double2 { return ((const double2 *)(A + AZP * j))[h]; };
+  auto rho_at = [&](int j) -> double {
+    const double2 x = pair(P, j, RH / 2);
+    return (RH & 1) ? x.y : x.x;
+  };
+  for (int j = tid; j < ns; j += T) {
+    double v[AZP];
+#pragma unroll
+    for (int q = 0; q < AZP; q++) v[q] = (q < NQ) ? k.q[q][base + j] : 0.0;
+    double2 *c = (double2 *)(P + AZP * j);
+#pragma unroll
+    for (int h = 0; h < AZP / 2; h++) c[h] = make_double2(v[2 * h], v[2 * h + 1]);
+  }
+  // ComputeThetaElongations / ComputeAverageThetaVelocities / ComputeResiduals
+  const double invdt = 1.0 / dt;
+  double s = 0.0;
+  for (int j = tid; j < ns; j += T) {
+    double elong = k.vt[base + j] * dt;
+    s += elong * invdt;
+  }
+  s = block_sum_dyn(s, sh);
+  const double VMed = s / (double)ns;
+  // ComputeConstantResidual (TransportEuler.c:310-348)
+  const double dpinvns = (k.pmax - k.pmin) / (double)ns;
+  const double Ntilde = VMed * k.invrmed[i] * dt * (double)ns / (k.pmax - k.pmin);
+  const double Nround = floor(Ntilde + 0.5);
+  const long nshift = (long)Nround;
+  double vconst = (Ntilde - Nround) * k.rmed[i] * invdt * dpinvns;
+  for (int j = tid; j < ns; j += T) {
+    double elong = k.vt[base + j] * dt;
+    double v = elong * invdt - VMed;
+    if (!k.fast_transport) v = vconst + v;
+    vres[j] = v;
+  }
+  if (!k.fast_transport) vconst = 0.0;
+  const double dxtheta = k.dxtheta[i], invdxtheta = k.invdxtheta[i];
+  const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
+  const double invsurf = 1.0 / k.surf[i];
+  int jj[E], jjm[E], jjp[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    const int j = tid + e * T;
+    jj[e] = j;
+    jjm[e] = (j == 0) ? ns - 1 : j - 1;
+    jjp[e] = (j == ns - 1) ? 0 : j + 1;
+  }
+#define OWN(e) (FULL || jj[e] < ns)
+  for (int pass = 0; pass < 2; pass++) {
+    const bool uniform = (pass == 1);
+    if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
+    __syncthreads();  // P and vres complete
+    // RhoStar (ComputeStarTheta(Rho, V, RhoStar)); RhoInt in registers
+    double R[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      const double rm = rho_at(jjm[e]), r0 = rho_at(jj[e]), rp = rho_at(jjp[e]);
+      R[e] = r0;
+      const double dqm = (r0 - rm), dqp = (rp - r0);
+      DR[jj[e]] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+    }
+    __syncthreads();
+    // per face the upwind cell u and the factor f of its star value (as in
+    // the other variants)
+    double RSl[E], RSh[E], Vl[E], Vh[E], fl[E], fh[E], den[E], rden[E];
+    int ul[E], uh[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      const double vl = uniform ? vconst : vres[jj[e]], vh = uniform ? vconst : vres[jjp[e]];
+      Vl[e] = vl;
+      Vh[e] = vh;
+      const double kl = vl * dt, kh = vh * dt;
+      ul[e] = (kl > 0.0) ? jjm[e] : jj[e];
+      fl[e] = (kl > 0.0) ? (dxtheta - kl) : -(dxtheta + kl);
+      uh[e] = (kh > 0.0) ? jj[e] : jjp[e];
+      fh[e] = (kh > 0.0) ? (dxtheta - kh) : -(dxtheta + kh);
+      RSl[e] = rho_at(ul[e]) + fl[e] * DR[ul[e]];
+      RSh[e] = rho_at(uh[e]) + fh[e] * DR[uh[e]];
+      den[e] = R[e] + 1e-20;
+      rden[e] = 1.0 / den[e];
+    }
+    double q0[E][AZP];
+    __syncthreads();  // every read of rho and DR done: W replaces the cells
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      double2 *c = (double2 *)(P + AZP * jj[e]);
+#pragma unroll
+      for (int h = 0; h < AZP / 2; h++) {
+        const double2 x = c[h];
+        q0[e][2 * h] = x.x;
+        q0[e][2 * h + 1] = x.y;
+        const double wa = (2 * h < NQ) ? fb_quot(x.x, den[e], rden[e]) : 0.0;  // q0 / den
+        const double wb = (2 * h + 1 < NQ) ? fb_quot(x.y, den[e], rden[e]) : 0.0;
+        c[h] = make_double2(wa, wb);
+      }
+    }
+    __syncthreads();  // W complete
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      const double2 *cm = (const double2 *)(P + AZP * jjm[e]), *c0 = (const double2 *)(P + AZP * jj[e]),
+                    *cp = (const double2 *)(P + AZP * jjp[e]);
+      double2 *dd = (double2 *)(PD + AZP * jj[e]);
+#pragma unroll
+      for (int h = 0; h < AZP / 2; h++) {
+        const double2 wm = cm[h], w0 = c0[h], wp = cp[h];
+        const double m_[2] = {wm.x, wm.y}, z_[2] = {w0.x, w0.y}, p_[2] = {wp.x, wp.y};
+        double d2[2];
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const double dqm = (z_[u] - m_[u]), dqp = (p_[u] - z_[u]);
+          d2[u] = (2 * h + u < NQ && dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+        }
+        dd[h] = make_double2(d2[0], d2[1]);
+      }
+    }
+    __syncthreads();  // DQ complete
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      const double2 *cwl = (const double2 *)(P + AZP * ul[e]), *cdl = (const double2 *)(PD + AZP * ul[e]);
+      const double2 *cwh = (const double2 *)(P + AZP * uh[e]), *cdh = (const double2 *)(PD + AZP * uh[e]);
+#pragma unroll
+      for (int h = 0; h < AZP / 2; h++) {
+        const double2 wl = cwl[h], dl = cdl[h], wh = cwh[h], dh = cdh[h];
+        const double wl_[2] = {wl.x, wl.y}, dl_[2] = {dl.x, dl.y}, wh_[2] = {wh.x, wh.y}, dh_[2] = {dh.x, dh.y};
+#pragma unroll
+        for (int u = 0; u < 2; u++) {
+          const int q = 2 * h + u;
+          if (q >= NQ) continue;
+          const double qsl = wl_[u] + fl[e] * dl_[u];
+          const double qsh = wh_[u] + fh[e] * dh_[u];
+          double varq = dxrad * qsl * RSl[e] * Vl[e];
+          varq -= dxrad * qsh * RSh[e] * Vh[e];
+          q0[e][q] = q0[e][q] + varq * invsurf;
+        }
+      }
+    }
+    __syncthreads();  // every read of W done
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      double2 *c = (double2 *)(P + AZP * jj[e]);
+#pragma unroll
+      for (int h = 0; h < AZP / 2; h++) c[h] = make_double2(q0[e][2 * h], q0[e][2 * h + 1]);
+    }
+  }
+  __syncthreads();
+  // AdvectSHIFT (TransportEuler.c:350-373): cell j takes cell (j - nshift) mod ns
+  int shift = (int)(nshift % ns);
+  if (shift < 0) shift += ns;
+  {
+    double2 tmp[E][AZP / 2];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      int ji = jj[e] - shift;
+      if (ji < 0) ji += ns;
+      const double2 *c = (const double2 *)(P + AZP * ji);
+#pragma unroll
+      for (int h = 0; h < AZP / 2; h++) tmp[e][h] = c[h];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      double2 *c = (double2 *)(P + AZP * jj[e]);
+#pragma unroll
+      for (int h = 0; h < AZP / 2; h++) c[h] = tmp[e][h];
+    }
+  }
+#undef OWN
+  __syncthreads();
+  // ComputeVelocities, vtheta part; floors on energy; sub-Keplerian edges
+  const int subkep = (!k.transport_only) && (i == 0 || i == nr - 1);
+  for (int j = tid; j < ns; j += T) {
+    const int jm = (j == 0) ? ns - 1 : j - 1;
+    const double2 c0 = pair(P, j, 0), c1 = pair(P, j, 1), c2 = pair(P, j, 2), m1 = pair(P, jm, 1), m2 = pair(P, jm, 2);
+    const double rj = (RH & 1) ? c2.y : c2.x, rjm = (RH & 1) ? m2.y : m2.x;  // RH is 4 or 5
+    double v = (m1.x + c1.y) / (rj + rjm + 1e-20) / k.rmed[i] - k.rmed[i] * k.omega_frame;  // tp[jm] + tm[j]
+    if (subkep) v = k.vthetamed[i] - k.rmed[i] * k.omega_frame;
+    k.vt[base + j] = v;
+    k.rho_t[base + j] = rj;
+    k.q[0][base + j] = c0.x;
+    k.q[1][base + j] = c0.y;
+    if (NQ == 6) {
+      double e = c2.x;
+      if (k.add_floors && !k.transport_only) {
+        double e_bottom = 1e-3 * k.energymed[i];
+        if (e < e_bottom) e = e_bottom;
+      }
+      k.e[base + j] = e;
+    }
+  }
+}
+
 // cells per thread of the azimuthal pass (1..4): at most 1024 threads for
 // 1-2 cells each, 768 threads for 3-4 (more registers per thread).  The
 // automatic choice is the fewest cells per thread; the tuner may pick more.
@@ -1398,15 +1620,28 @@ int fb_azi_E_valid(int ns, int energy, int E)
   const int NQ = energy ? 6 : 5;
   return (size_t)FB_AZI_RINGS(NQ) * ns * sizeof(double) + 32 * sizeof(double) <= (size_t)max_smem_optin();
 }
-// the wide variant: its rings fit and its thread limit holds (768 threads
-// for two or more cells per thread); variant 0 takes it where it can
-int fb_azi_wide(int ns, int energy, int E, int variant)
+// Variants of the azimuthal pass: 1 narrow, 2 wide, 3 packed.  The wide and
+// packed ones need their rings to fit and at most 768 threads for two or
+// more cells per thread; variant 0 takes the packed one, else the wide one,
+// else the narrow one.  Returns the variant a launch takes, 0 if `variant`
+// cannot run on this ring.
+static bool azi_fits(int ns, int E, size_t rings)
 {
-  if (variant == 1) return 0;
-  const int NQ = energy ? 6 : 5;
   const int maxt = (E == 1) ? 1024 : 768;
   return azi_threads_for(ns, E) <= maxt &&
-         (size_t)FB_AZI_RINGS_WIDE(NQ) * ns * sizeof(double) + 32 * sizeof(double) <= (size_t)max_smem_optin();
+         rings * ns * sizeof(double) + 32 * sizeof(double) <= (size_t)max_smem_optin();
+}
+int fb_azi_variant(int ns, int energy, int E, int variant)
+{
+  const int NQ = energy ? 6 : 5;
+  const bool wide = azi_fits(ns, E, FB_AZI_RINGS_WIDE(NQ)), packed = azi_fits(ns, E, 2 * AZP + 2);
+  switch (variant) {
+    case 0: return packed ? 3 : wide ? 2 : 1;
+    case 1: return 1;
+    case 2: return wide ? 2 : 0;
+    case 3: return packed ? 3 : 0;
+    default: return 0;
+  }
 }
 
 // ComputeVelocities' radial part (TransportEuler.c:531-536) needs the
@@ -1482,10 +1717,26 @@ template <int NQ>
 static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
 {
   const int E = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
-  const bool wide = fb_azi_wide(k.ns, NQ == 6, E, k.azi_variant);
-  const size_t smem = (size_t)(wide ? FB_AZI_RINGS_WIDE(NQ) : FB_AZI_RINGS(NQ)) * k.ns * sizeof(double);
+  int var = fb_azi_variant(k.ns, NQ == 6, E, k.azi_variant);
+  if (var == 0) var = 1;
+  const bool wide = (var == 2);
   const int th = azi_threads_for(k.ns, E);
   const bool full = (th * E == k.ns);  // every thread owns E cells
+  if (var == 3) {
+    const size_t psmem = (size_t)(2 * AZP + 2) * k.ns * sizeof(double);
+#define AZP_LAUNCH(EE)                                                                                       \
+  (full ? fb_launch(k_transport_azimuthal_packed<NQ, EE, true>, k.nr, th, psmem, s, k, dt_override)           \
+        : fb_launch(k_transport_azimuthal_packed<NQ, EE, false>, k.nr, th, psmem, s, k, dt_override))
+    switch (E) {
+      case 1: AZP_LAUNCH(1); break;
+      case 2: AZP_LAUNCH(2); break;
+      case 3: AZP_LAUNCH(3); break;
+      default: AZP_LAUNCH(4); break;
+    }
+#undef AZP_LAUNCH
+    return;
+  }
+  const size_t smem = (size_t)(wide ? FB_AZI_RINGS_WIDE(NQ) : FB_AZI_RINGS(NQ)) * k.ns * sizeof(double);
 #define AZI_LAUNCH(EE)                                                                                     \
   (wide ? (full ? fb_launch(k_transport_azimuthal<NQ, EE, true, true>, k.nr, th, smem, s, k, dt_override)         \
                 : fb_launch(k_transport_azimuthal<NQ, EE, false, true>, k.nr, th, smem, s, k, dt_override))       \
@@ -1708,10 +1959,15 @@ int fb_gas_prepare(int ns, int energy)
 #define AZI_FNS(NQ, F, WD)                                                                               \
   (const void *)k_transport_azimuthal<NQ, 1, F, WD>, (const void *)k_transport_azimuthal<NQ, 2, F, WD>,  \
       (const void *)k_transport_azimuthal<NQ, 3, F, WD>, (const void *)k_transport_azimuthal<NQ, 4, F, WD>
+#define AZP_FNS(NQ, F)                                                                                   \
+  (const void *)k_transport_azimuthal_packed<NQ, 1, F>, (const void *)k_transport_azimuthal_packed<NQ, 2, F>, \
+      (const void *)k_transport_azimuthal_packed<NQ, 3, F>, (const void *)k_transport_azimuthal_packed<NQ, 4, F>
   const void *fns[] = {AZI_FNS(5, false, false), AZI_FNS(5, true, false), AZI_FNS(6, false, false),
                        AZI_FNS(6, true, false),  AZI_FNS(5, false, true),  AZI_FNS(5, true, true),
-                       AZI_FNS(6, false, true),  AZI_FNS(6, true, true)};
+                       AZI_FNS(6, false, true),  AZI_FNS(6, true, true),   AZP_FNS(5, false),
+                       AZP_FNS(5, true),         AZP_FNS(6, false),        AZP_FNS(6, true)};
 #undef AZI_FNS
+#undef AZP_FNS
   for (const void *f : fns) {
     int rc = fb_allow_max_dynamic_smem(f);
     if (rc) return rc;

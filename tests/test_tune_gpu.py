@@ -42,7 +42,7 @@ def test_tuning_table_lookup(tmp_path):
     table = {"iso": {"64x192": {"cell_block": 64, "azi_cells_per_thread": 2, "rad_columns": 32, "rad_rings": 8}}}
     with Disc(read_par(par), tuning=table) as d:
         assert d.tuning() == {"cell_block": 64, "azi_cells_per_thread": 2, "rad_columns": 32, "rad_rings": 8,
-                              "azi_variant": 2}
+                              "azi_variant": 3}
         with pytest.raises(FbError):
             d.set_tuning({"cell_block": 48})
         d.step()
@@ -50,19 +50,21 @@ def test_tuning_table_lookup(tmp_path):
 
 @pytest.mark.parametrize("E", [1, 2, 3])
 def test_azimuthal_variants_are_bit_identical(tmp_path, E):
-    """The narrow (three barriers per quantity) and wide (all quantities per
-    phase) azimuthal passes do the same arithmetic: whole DTs with energy,
-    cooling and self-gravity must agree to the last bit."""
+    """The narrow (three barriers per quantity), wide (all quantities per
+    phase) and packed (a cell's quantities side by side) azimuthal passes do
+    the same arithmetic: whole DTs with energy, cooling and self-gravity must
+    agree to the last bit."""
     from dustyfargoadsg_b200 import Disc, read_par
     par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "adiabatic_sg_512x1536.par"), str(tmp_path),
                             Nrad=64, Nsec=192)
     out = {}
-    for variant in (1, 2):
+    for variant in (1, 2, 3):
         with Disc(read_par(par), noise=1e-3, seed=4) as d:
             d.set_tuning({"cell_block": 128, "azi_cells_per_thread": E, "azi_variant": variant})
             assert d.tuning()["azi_variant"] == variant
             for _ in range(2):
                 d.step()
             out[variant] = d.download()
-    for k in FIELDS + ("energy",):
-        np.testing.assert_array_equal(out[1][k], out[2][k], err_msg=k)
+    for v in (2, 3):
+        for k in FIELDS + ("energy",):
+            np.testing.assert_array_equal(out[1][k], out[v][k], err_msg="%s variant %d" % (k, v))
