@@ -1379,9 +1379,13 @@ __global__ void __launch_bounds__(AziMaxThreads<E, WIDE>::value) k_transport_azi
 // ThetaMomP, ThetaMomM, [Energy,] Rho; without energy the sixth slot is
 // unused) and their slopes likewise, so one address per face serves every
 // quantity through 16-byte shared accesses, two quantities at a time
-// (48-byte cells: conflict-free per quarter warp).  Rings: 2 x 6 + 2 of
-// nsec doubles.
+// (48-byte cells: conflict-free per quarter warp).  The residual velocity
+// is recomputed from vtheta where it is needed, and without energy the
+// density slopes of RhoStar live in the unused sixth slot, so the variant
+// takes 2 x 6 (+ 1 with energy) rings of nsec doubles: 221 KB for 2304
+// isothermal cells.
 #define AZP 6
+#define AZP_RINGS(NQ) (2 * AZP + ((NQ) == 6 ? 1 : 0))
 template <int NQ, int E, bool FULL>
 __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_packed(KP k, double dtov)
 {
@@ -1394,8 +1398,11 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
   constexpr int RH = NQ - 1;          // slot of the density
   double *P = (double *)smem2;        // ns cells x 6
   double *PD = P + AZP * ns;          // slopes, ns x 6
-  double *vres = PD + AZP * ns;       // residual azimuthal velocity
-  double *DR = vres + ns;             // density slopes (RhoStar)
+  // density slopes (RhoStar): slot 5 of the cells without energy, a ring of
+  // their own with it
+  double *DRb = (NQ == 6) ? PD + AZP * ns : P + 5;
+  const int drs = (NQ == 6) ? 1 : AZP;
+#define DR_AT(j) DRb[(size_t)(j) * drs]
   // a cell's slot pair (2h, 2h+1) as one 16-byte access: 48-byte cells keep
   // these free of bank conflicts, single 8-byte slots would not be
   auto pair = [&](const double *A, int j, int h) -> double2 { return ((const double2 *)(A + AZP * j))[h]; };
@@ -1426,12 +1433,14 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
   const double Nround = floor(Ntilde + 0.5);
   const long nshift = (long)Nround;
   double vconst = (Ntilde - Nround) * k.rmed[i] * invdt * dpinvns;
-  for (int j = tid; j < ns; j += T) {
+  const double vconst0 = vconst;
+  // ComputeResiduals' value of cell j (vtheta is not written before the end)
+  auto vres_at = [&](int j) -> double {
     double elong = k.vt[base + j] * dt;
     double v = elong * invdt - VMed;
-    if (!k.fast_transport) v = vconst + v;
-    vres[j] = v;
-  }
+    if (!k.fast_transport) v = vconst0 + v;
+    return v;
+  };
   if (!k.fast_transport) vconst = 0.0;
   const double dxtheta = k.dxtheta[i], invdxtheta = k.invdxtheta[i];
   const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
@@ -1448,16 +1457,17 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
   for (int pass = 0; pass < 2; pass++) {
     const bool uniform = (pass == 1);
     if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
-    __syncthreads();  // P and vres complete
+    __syncthreads();  // P complete
     // RhoStar (ComputeStarTheta(Rho, V, RhoStar)); RhoInt in registers
     double R[E];
 #pragma unroll
     for (int e = 0; e < E; e++) {
       if (!OWN(e)) continue;
-      const double rm = rho_at(jjm[e]), r0 = rho_at(jj[e]), rp = rho_at(jjp[e]);
+      // single-slot reads: slot 5 of a neighbour may be getting its slope
+      const double rm = P[AZP * jjm[e] + RH], r0 = P[AZP * jj[e] + RH], rp = P[AZP * jjp[e] + RH];
       R[e] = r0;
       const double dqm = (r0 - rm), dqp = (rp - r0);
-      DR[jj[e]] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+      DR_AT(jj[e]) = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
     }
     __syncthreads();
     // per face the upwind cell u and the factor f of its star value (as in
@@ -1467,7 +1477,7 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
 #pragma unroll
     for (int e = 0; e < E; e++) {
       if (!OWN(e)) continue;
-      const double vl = uniform ? vconst : vres[jj[e]], vh = uniform ? vconst : vres[jjp[e]];
+      const double vl = uniform ? vconst : vres_at(jj[e]), vh = uniform ? vconst : vres_at(jjp[e]);
       Vl[e] = vl;
       Vh[e] = vh;
       const double kl = vl * dt, kh = vh * dt;
@@ -1475,13 +1485,13 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
       fl[e] = (kl > 0.0) ? (dxtheta - kl) : -(dxtheta + kl);
       uh[e] = (kh > 0.0) ? jj[e] : jjp[e];
       fh[e] = (kh > 0.0) ? (dxtheta - kh) : -(dxtheta + kh);
-      RSl[e] = rho_at(ul[e]) + fl[e] * DR[ul[e]];
-      RSh[e] = rho_at(uh[e]) + fh[e] * DR[uh[e]];
+      RSl[e] = rho_at(ul[e]) + fl[e] * DR_AT(ul[e]);
+      RSh[e] = rho_at(uh[e]) + fh[e] * DR_AT(uh[e]);
       den[e] = R[e] + 1e-20;
       rden[e] = 1.0 / den[e];
     }
     double q0[E][AZP];
-    __syncthreads();  // every read of rho and DR done: W replaces the cells
+    __syncthreads();  // every read of rho and DR done: W replaces the cells (and slot 5)
 #pragma unroll
     for (int e = 0; e < E; e++) {
       if (!OWN(e)) continue;
@@ -1572,6 +1582,7 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
     }
   }
 #undef OWN
+#undef DR_AT
   __syncthreads();
   // ComputeVelocities, vtheta part; floors on energy; sub-Keplerian edges
   const int subkep = (!k.transport_only) && (i == 0 || i == nr - 1);
@@ -1634,7 +1645,7 @@ static bool azi_fits(int ns, int E, size_t rings)
 int fb_azi_variant(int ns, int energy, int E, int variant)
 {
   const int NQ = energy ? 6 : 5;
-  const bool wide = azi_fits(ns, E, FB_AZI_RINGS_WIDE(NQ)), packed = azi_fits(ns, E, 2 * AZP + 2);
+  const bool wide = azi_fits(ns, E, FB_AZI_RINGS_WIDE(NQ)), packed = azi_fits(ns, E, AZP_RINGS(NQ));
   switch (variant) {
     case 0: return packed ? 3 : wide ? 2 : 1;
     case 1: return 1;
@@ -1723,7 +1734,7 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
   const int th = azi_threads_for(k.ns, E);
   const bool full = (th * E == k.ns);  // every thread owns E cells
   if (var == 3) {
-    const size_t psmem = (size_t)(2 * AZP + 2) * k.ns * sizeof(double);
+    const size_t psmem = (size_t)AZP_RINGS(NQ) * k.ns * sizeof(double);
 #define AZP_LAUNCH(EE)                                                                                       \
   (full ? fb_launch(k_transport_azimuthal_packed<NQ, EE, true>, k.nr, th, psmem, s, k, dt_override)           \
         : fb_launch(k_transport_azimuthal_packed<NQ, EE, false>, k.nr, th, psmem, s, k, dt_override))
