@@ -147,12 +147,21 @@ static __device__ void rk5(const double *q0, double dt, const double *masses, do
 // One CTA per ring, CFL_E cells per thread, one pass over the ring: the
 // cells' values stay in registers between the ring sums (the mean azimuthal
 // velocity the CFL limits need) and the limits themselves.
-#define CFL_E 4
-static inline int cfl_threads(int ns) { return ((ns + CFL_E - 1) / CFL_E + 31) / 32 * 32; }
-__global__ void __launch_bounds__(1024) k_cfl(KP k)
+// The cells' values kept between the ring sums and the CFL limits go
+// through shared memory (3 nsec doubles), so a ring's CTA of up to 256
+// threads fits in 64 registers a thread: four CTAs share an SM and a
+// 512-ring grid runs in one wave.
+#define CFL_BS 256
+static inline int cfl_threads(int ns)
+{
+  const int t = ((ns + 3) / 4 + 31) / 32 * 32;
+  return t < CFL_BS ? t : CFL_BS;
+}
+__global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
 {
   fb_grid_dependency();
   __shared__ double sh[6 * 32];
+  extern __shared__ double cfl_sm[];
   const int i = blockIdx.x, ns = k.ns, T = blockDim.x, tid = threadIdx.x;
   const size_t base = (size_t)i * ns;
   const double *vt = k.vt + base, *vr = k.vr + base, *rho = k.rho + base;
@@ -166,13 +175,10 @@ __global__ void __launch_bounds__(1024) k_cfl(KP k)
   // ConditionCFL's per-cell limits (SourceEuler.c:1390-1485): all but the
   // residual-velocity one are known before the ring mean; the sum under the
   // square root is evaluated in the reference's order once it is
-  double vtc[CFL_E], s12[CFL_E], s4[CFL_E];
+  double *vtc = cfl_sm, *s12 = cfl_sm + ns, *s4 = cfl_sm + 2 * ns;
   const double dxrad = k.dxrad[i], dxtheta = k.dxtheta_cfl[i];
   int neg = 0, bad = 0;
-#pragma unroll
-  for (int e = 0; e < CFL_E; e++) {
-    const int j = tid + e * T;
-    if (j >= ns) continue;
+  for (int j = tid; j < ns; j += T) {
     const double vtj = vt[j], vrj = vr[j], dens = rho[j];
     v[0] += vtj;
     if (dens < 0.0) neg = 1;
@@ -205,9 +211,9 @@ __global__ void __launch_bounds__(1024) k_cfl(KP k)
       if (dvt >= 0.0) dvt = 1e-10; else dvt = -dvt;
       double invdt4 = max2(dvr / dxrad, dvt / dxtheta);
       invdt4 *= 4.0 * FB_CVNR * FB_CVNR;
-      vtc[e] = vtj;
-      s12[e] = invdt1 * invdt1 + invdt2 * invdt2;
-      s4[e] = invdt4 * invdt4;
+      vtc[j] = vtj;
+      s12[j] = invdt1 * invdt1 + invdt2 * invdt2;
+      s4[j] = invdt4 * invdt4;
     }
   }
   block_sums<6>(v, sh);
@@ -228,12 +234,10 @@ __global__ void __launch_bounds__(1024) k_cfl(KP k)
     const double invdt5 = (viscosity != 0.0) ? viscosity * 4.0 / k.mindx2[i] : 1e-10;
     const double invdt6 = 1e-10;
     double m = 1e30;
-#pragma unroll
-    for (int e = 0; e < CFL_E; e++) {
-      if (tid + e * T >= ns) continue;
-      double vres = k.fast_transport ? vtc[e] - vmoy : vtc[e];
+    for (int j = tid; j < ns; j += T) {  // each thread reads back its own cells
+      double vres = k.fast_transport ? vtc[j] - vmoy : vtc[j];
       double invdt3 = fabs(vres) / dxtheta;
-      double dt = FB_CFLSECURITY / sqrt(s12[e] + invdt3 * invdt3 + s4[e] + invdt5 * invdt5 + invdt6 * invdt6);
+      double dt = FB_CFLSECURITY / sqrt(s12[j] + invdt3 * invdt3 + s4[j] + invdt5 * invdt5 + invdt6 * invdt6);
       if (dt < m) m = dt;
     }
     m = block_min_dyn(m, sh);
@@ -263,7 +267,10 @@ __global__ void __launch_bounds__(1024) k_cfl(KP k)
   for (int w = tid; w < (int)(sizeof(fb_ctl) / 8); w += T) out[w] = dst[w];
 }
 
-void fb_launch_cfl(const KP &k, cudaStream_t s) { fb_launch(k_cfl, k.nr, cfl_threads(k.ns), 0, s, k); }
+void fb_launch_cfl(const KP &k, cudaStream_t s)
+{
+  fb_launch(k_cfl, k.nr, cfl_threads(k.ns), 3 * (size_t)k.ns * sizeof(double), s, k);
+}
 
 // The planets' step of the substep, after the controller has set dt:
 // AdvanceSystemRK5 (Pframeforce.c:163-266) and RotatePsys (Psys.c:352-372).
@@ -1979,6 +1986,10 @@ int fb_gas_prepare(int ns, int energy)
                        AZP_FNS(5, true),         AZP_FNS(6, false),        AZP_FNS(6, true)};
 #undef AZI_FNS
 #undef AZP_FNS
+  {
+    int rc = fb_allow_max_dynamic_smem((const void *)k_cfl);  // 3 nsec doubles of cell values
+    if (rc) return rc;
+  }
   for (const void *f : fns) {
     int rc = fb_allow_max_dynamic_smem(f);
     if (rc) return rc;
