@@ -556,7 +556,7 @@ static __device__ void col_fft(double2 *X, int lgm, const FftArgs &a)
 
 // Every thread moves 16 points in each phase (T = SG_KC2 m / 16), with all
 // of a phase's global loads issued before their first use.
-__global__ void __launch_bounds__(128, 4) sg_cols_p2(FftArgs fa, int lgm, int nrows_in, int nk, int mode,
+__global__ void __launch_bounds__(128, 6) sg_cols_p2(FftArgs fa, int lgm, int nrows_in, int nk, int mode,
                                                  double2 *data_r, double2 *data_t, double2 *kh_r, double2 *kh_t)
 {
   fb_grid_dependency();
