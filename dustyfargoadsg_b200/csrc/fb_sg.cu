@@ -29,6 +29,8 @@
 #define SG_BS 256
 #define SG_ROW_BS 128  // threads of a row transform (radix-16 passes: n/16 butterflies)
 #define SG_MAXST 16
+#define SG_ROW_U 12    // points per thread per load batch of a row (1536 points: one batch)
+#define SG_INV_U 8     // wavenumbers per thread per load batch of an inverse row
 
 struct fb_fft_plan {
   int n, nst;
@@ -42,14 +44,19 @@ struct FftArgs {
   const double2 *tw;
 };
 
+struct DifArgs {
+  int lgm, npass;     // m = 2^lgm; passes of span S_p = m / 16^p >= 32, then the tail
+  const double2 *tw;  // pass p: exp(-2 pi i r j / S_p) at [r][j], r < 16, j < S_p / 16
+};
+
 struct fb_sg {
   int nr, ns, m, nk;        // m = 2 nr, nk = ns/2 + 1
   fb_fft_plan prow, pcol;
-  int p2, lgm;              // m = 2^lgm, lgm >= 4: the radix-16 column kernel
+  int p2;                   // 32 <= m = 2^lgm <= 1024: the in-place column kernel
   double2 *tw2;             // its per-pass twiddle tables
   FftArgs frow;             // the row passes (radix 16 first) and their tables
   double2 *twr;
-  FftArgs fc2;              // its passes (16, ..., 16, then 4 and/or 2)
+  DifArgs fc2;              // its passes
   double2 *xr, *xt;         // half spectra after the row pass, [i][k], i < nr
   double2 *khr, *kht;       // kernel spectra, [k][m]
   double *sq, *rr;          // sqrt(Rmed/R0), Rmed (per ring) for the densities
@@ -286,6 +293,33 @@ static __device__ __forceinline__ void dft_small(double2 *v)
 static __device__ __forceinline__ int pad16(int i) { return i + (i >> 4); }
 template <int INV> static __device__ __forceinline__ void dft16(double2 *v);
 
+// v[r] *= w^r (r = 1..15) for a radix-16 pass, w = exp(-/+ 2 pi i jm / (16 L)),
+// from the table rows r = 1, 2, 4, 8 alone (tw holds w^r at [r L + jm]); the
+// other powers are products of those, at most three deep, a few ulp.  Four
+// loads per point instead of fifteen, and fewer registers held.
+template <int INV>
+static __device__ __forceinline__ void twiddle16(double2 *v, const double2 *__restrict__ tw, int L, int jm)
+{
+  double2 w1 = tw[L + jm], w2 = tw[2 * L + jm], w4 = tw[4 * L + jm], w8 = tw[8 * L + jm];
+  if (INV) { w1.y = -w1.y; w2.y = -w2.y; w4.y = -w4.y; w8.y = -w8.y; }
+  const double2 w3 = cmul(w1, w2), w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+  v[1] = cmul(v[1], w1);
+  v[2] = cmul(v[2], w2);
+  v[3] = cmul(v[3], w3);
+  v[4] = cmul(v[4], w4);
+  v[5] = cmul(v[5], w5);
+  v[6] = cmul(v[6], w6);
+  v[7] = cmul(v[7], w7);
+  v[8] = cmul(v[8], w8);
+  v[9] = cmul(v[9], cmul(w8, w1));
+  v[10] = cmul(v[10], cmul(w8, w2));
+  v[11] = cmul(v[11], cmul(w8, w3));
+  v[12] = cmul(v[12], cmul(w8, w4));
+  v[13] = cmul(v[13], cmul(w8, w5));
+  v[14] = cmul(v[14], cmul(w8, w6));
+  v[15] = cmul(v[15], cmul(w8, w7));
+}
+
 // One radix-R Stockham pass of a line of n points between two buffers padded
 // by one slot per 16; twp is the pass's twiddle table, R rows of L entries
 // (exp(-2 pi i r jm / (L R)) at [r][jm], read with consecutive jm per warp).
@@ -298,8 +332,10 @@ static __device__ __forceinline__ void fft_pass_p(const double2 *__restrict__ x,
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; r++) v[r] = x[pad16(j + r * nb)];
-    const int jm = j % L;
-    if (L > 1) {
+    const int jm = ((L & (L - 1)) == 0) ? (j & (L - 1)) : (j % L);  // L is a power of two until a 3 or 5
+    if (R == 16 && L > 1) {
+      twiddle16<INV>(v, twp, L, jm);
+    } else if (L > 1) {
 #pragma unroll
       for (int r = 1; r < R; r++) {
         double2 w = twp[r * L + jm];
@@ -355,17 +391,28 @@ __global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_fwd(FftArgs fa, int nrow
   fb_grid_dependency();
   extern __shared__ double2 sm[];
   double2 *x = sm, *y = sm + ns + ns / 16;  // padded lines
-  const int i = blockIdx.x;
-  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-    double a, b;
-    if (in_r) {
-      a = in_r[(size_t)i * ns + j];
-      b = in_t[(size_t)i * ns + j];
-    } else {
-      a = dens[(size_t)i * ns + j] * sq[i];   // SGP_Sr = dens*sqrt(Rmed/R0)
-      b = a * rmed[i] / r0;                   // SGP_St = Sr*Rmed/R0
+  const int i = blockIdx.x, T = blockDim.x;
+  if (in_r) {
+    for (int j = threadIdx.x; j < ns; j += T) x[pad16(j)] = make_double2(in_r[(size_t)i * ns + j], in_t[(size_t)i * ns + j]);
+  } else {
+    // all of a batch's loads in flight together: one L2 round trip per
+    // SG_ROW_U * T points instead of one per T
+    const double sqi = sq[i], rmi = rmed[i];
+    for (int j0 = 0; j0 < ns; j0 += SG_ROW_U * T) {
+      double d[SG_ROW_U];
+#pragma unroll
+      for (int u = 0; u < SG_ROW_U; u++) {
+        const int j = j0 + threadIdx.x + u * T;
+        d[u] = (j < ns) ? dens[(size_t)i * ns + j] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < SG_ROW_U; u++) {
+        const int j = j0 + threadIdx.x + u * T;
+        const double a = d[u] * sqi;   // SGP_Sr = dens*sqrt(Rmed/R0)
+        const double b = a * rmi / r0;  // SGP_St = Sr*Rmed/R0
+        if (j < ns) x[pad16(j)] = make_double2(a, b);
+      }
     }
-    x[pad16(j)] = make_double2(a, b);
   }
   double2 *Z = fft_line_p<0>(x, y, fa);
   for (int k = threadIdx.x; k < nk; k += blockDim.x) {
@@ -449,13 +496,28 @@ __global__ void __launch_bounds__(SG_BS) sg_cols(FftArgs fa, int nrows_in, int n
 }
 
 // ------------------------------------------- column pass, powers of two
-// Columns of m = 2^p points (p >= 4): radix-16 passes (a 4 x 4 split with
-// the W16 twiddles in registers), then a radix-4 and/or radix-2 pass, so a
-// 1024-point column takes three passes each way instead of five.  Every
-// thread holds 16 points per pass: it loads them, the CTA synchronises, it
-// stores them -- one buffer, transformed in place.  Lines are padded by one
-// slot per 16 (index i at i + i/16), which keeps the stride-16 stores of
-// the first pass free of bank conflicts.  CTAs of SG_KC2 * m / 16 threads.
+// Columns of m = 2^lgm points, 32 <= m <= 1024, transformed in place with
+// decimation in frequency forward and decimation in time backward, so that
+// no reordering pass is needed: the forward transform leaves the spectrum
+// in a fixed permuted order, the kernel spectrum is stored in that same
+// order (it is made by the same forward code), the product is pointwise,
+// and the backward transform undoes the forward steps in reverse and
+// returns natural order.
+//   pass p (span S = m / 16^p >= 32): butterflies over the points
+//     blk S + j + (S/16) r (r < 16, j < S/16); forward: DFT16, then the
+//     outputs times exp(-2 pi i j r' / S); backward: inputs times the
+//     conjugate twiddles, then the inverse DFT16;
+//   tail (span S <= 16 left): DFTs of S consecutive points, natural order.
+// Each thread owns the 16 points of its butterfly (or its 16 consecutive
+// points in the tail) for the load and the store of a pass, so a pass
+// needs no barrier between them, and nothing is held in registers across
+// a barrier: one barrier per pass.  Rows >= m/2 of the input are the zero
+// padding (never loaded) and only rows < m/2 of the output are kept (never
+// computed past the last butterfly, stored straight to global memory).
+// Two adjacent wavenumbers per CTA (thread t: column t & 1, butterfly
+// t >> 1): a warp's global loads and stores cover 16 rows x 32 bytes.
+// Lines are padded by one slot per 16 and spaced m + m/16 + 4 slots apart,
+// which keeps every pass free of bank conflicts.
 #define SG_KC2 2
 
 template <int INV>
@@ -493,119 +555,183 @@ static __device__ __forceinline__ void dft16(double2 *v)
   for (int p = 0; p < 4; p++) dft4<INV>(v[4 * p], v[4 * p + 1], v[4 * p + 2], v[4 * p + 3]);
 }
 
-// One radix-R Stockham pass over the padded lines of m = 2^lgm points
-// (stride mp); tw is the pass's twiddle table, R rows of L entries.
-template <int R, int INV>
-static __device__ __forceinline__ void col_pass(double2 *X, int lgm, int mp, int L, const double2 *tw)
+
+// w[r] = w^r (r = 1..15), w = exp(-/+ 2 pi i j / S), from the table rows
+// r = 1, 2, 4, 8 (w^r at tw[r stride + j]): four loads instead of fifteen,
+// the other powers products at most two deep, within a few ulp.
+template <int INV>
+static __device__ __forceinline__ void pow16(double2 *w, const double2 *__restrict__ tw, int stride, int j)
 {
-  constexpr int B = 16 / R, LGR = (R == 16) ? 4 : (R == 4) ? 2 : 1;
-  const int lgnb = lgm - LGR, nb = 1 << lgnb, T = blockDim.x;
+  w[1] = tw[stride + j];
+  w[2] = tw[2 * stride + j];
+  w[4] = tw[4 * stride + j];
+  w[8] = tw[8 * stride + j];
+  if (INV) { w[1].y = -w[1].y; w[2].y = -w[2].y; w[4].y = -w[4].y; w[8].y = -w[8].y; }
+  w[3] = cmul(w[1], w[2]);
+  w[5] = cmul(w[4], w[1]);
+  w[6] = cmul(w[4], w[2]);
+  w[7] = cmul(w[4], w[3]);
+#pragma unroll
+  for (int r = 9; r < 16; r++) w[r] = cmul(w[8], w[r - 8]);
+}
+
+// 8-point DFT of v[0..7] in place, natural order (radix 2 x 4).
+template <int INV>
+static __device__ __forceinline__ void dft8(double2 *v)
+{
+  const double h = 0.70710678118654752440;
+  const double sg = INV ? -1.0 : 1.0;
+  double2 e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+  double2 o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+  dft4<INV>(e0, e1, e2, e3);
+  dft4<INV>(o0, o1, o2, o3);
+  o1 = cmul(o1, make_double2(h, -sg * h));
+  o2 = crot(o2, INV);
+  o3 = cmul(o3, make_double2(-h, -sg * h));
+  v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+  v[1] = cadd(e1, o1); v[5] = csub(e1, o1);
+  v[2] = cadd(e2, o2); v[6] = csub(e2, o2);
+  v[3] = cadd(e3, o3); v[7] = csub(e3, o3);
+}
+
+// The tail: DFTs of S consecutive points (S = 2, 4, 8, 16) over v[0..15].
+template <int INV>
+static __device__ __forceinline__ void dif_tail(double2 *v, int S)
+{
+  if (S == 16) {
+    dft16<INV>(v);
+    double2 w[16];
+#pragma unroll
+    for (int r = 0; r < 16; r++) w[r] = v[4 * (r & 3) + (r >> 2)];
+#pragma unroll
+    for (int r = 0; r < 16; r++) v[r] = w[r];
+  } else if (S == 8) {
+    dft8<INV>(v);
+    dft8<INV>(v + 8);
+  } else if (S == 4) {
+#pragma unroll
+    for (int g = 0; g < 4; g++) dft4<INV>(v[4 * g], v[4 * g + 1], v[4 * g + 2], v[4 * g + 3]);
+  } else {
+#pragma unroll
+    for (int g = 0; g < 8; g++) {
+      const double2 t0 = v[2 * g];
+      v[2 * g] = cadd(t0, v[2 * g + 1]);
+      v[2 * g + 1] = csub(t0, v[2 * g + 1]);
+    }
+  }
+}
+
+// A shared pass of span S over line x (forward: DFT16 then twiddles;
+// backward: conjugate twiddles then inverse DFT16).  q < m/16 butterflies.
+template <int INV>
+static __device__ __forceinline__ void dif_pass(double2 *x, int S, int q, const double2 *__restrict__ tw)
+{
+  const int sb = S >> 4, j = q & (sb - 1), base = (q - j) * 16 + j;  // blk S + j, blk = q / sb
   double2 v[16];
 #pragma unroll
-  for (int b = 0; b < B; b++) {
-    const int bf = threadIdx.x + b * T, line = bf >> lgnb, j = bf & (nb - 1);
-    const double2 *x = X + line * mp;
+  for (int r = 0; r < 16; r++) v[r] = x[pad16(base + r * sb)];
+  if (INV) {
 #pragma unroll
-    for (int r = 0; r < R; r++) v[b * R + r] = x[pad16(j + r * nb)];
-    if (L > 1) {
-      const int jm = j & (L - 1);
-#pragma unroll
-      for (int r = 1; r < R; r++) {
-        double2 w = tw[r * L + jm];  // exp(-2 pi i r jm / (L R)): consecutive in jm
-        if (INV) w.y = -w.y;
-        v[b * R + r] = cmul(v[b * R + r], w);
-      }
-    }
-    if (R == 16) {
-      dft16<INV>(v);
-    } else if (R == 4) {
-      dft4<INV>(v[b * 4], v[b * 4 + 1], v[b * 4 + 2], v[b * 4 + 3]);
-    } else {
-      const double2 t0 = v[b * 2];
-      v[b * 2] = cadd(t0, v[b * 2 + 1]);
-      v[b * 2 + 1] = csub(t0, v[b * 2 + 1]);
+    for (int r = 1; r < 16; r++) {
+      double2 w = tw[r * sb + j];
+      w.y = -w.y;
+      v[r] = cmul(v[r], w);
     }
   }
-  __syncthreads();
+  dft16<INV>(v);
 #pragma unroll
-  for (int b = 0; b < B; b++) {
-    const int bf = threadIdx.x + b * T, line = bf >> lgnb, j = bf & (nb - 1);
-    const int jm = j & (L - 1), idxD = (j - jm) * R + jm;
-    double2 *x = X + line * mp;
-#pragma unroll
-    for (int r = 0; r < R; r++) x[pad16(idxD + r * L)] = (R == 16) ? v[4 * (r & 3) + (r >> 2)] : v[b * R + r];
-  }
-  __syncthreads();
-}
-
-template <int INV>
-static __device__ void col_fft(double2 *X, int lgm, const FftArgs &a)
-{
-  const int m = 1 << lgm, mp = m + m / 16;
-  int L = 1, off = 0;
-  for (int st = 0; st < a.nst; st++) {
-    const int R = a.radix[st];
-    const double2 *tw = a.tw + off;  // the per-pass tables follow each other
-    if (R == 16) col_pass<16, INV>(X, lgm, mp, L, tw);
-    else if (R == 4) col_pass<4, INV>(X, lgm, mp, L, tw);
-    else col_pass<2, INV>(X, lgm, mp, L, tw);
-    off += R * L;
-    L *= R;
+  for (int r = 0; r < 16; r++) {
+    double2 o = v[4 * (r & 3) + (r >> 2)];
+    if (!INV && r > 0) o = cmul(o, tw[r * sb + j]);
+    x[pad16(base + r * sb)] = o;
   }
 }
 
-// Every thread moves 16 points in each phase (T = SG_KC2 m / 16), with all
-// of a phase's global loads issued before their first use.
-__global__ void __launch_bounds__(128, 6) sg_cols_p2(FftArgs fa, int lgm, int nrows_in, int nk, int mode,
-                                                 double2 *data_r, double2 *data_t, double2 *kh_r, double2 *kh_t)
+// MODE 0: forward transform of full columns (all m rows of data) into kh,
+// in the permuted order, the tail point r of thread q at [r][q] (setup of
+// the kernel spectra; MODE 1 reads it back the same way).  MODE 1: the
+// convolution of compute_sgacc (sgacc.c:25-38): forward transform of the
+// zero-padded half spectra, product with -G Khat, backward transform, rows
+// < m/2 written back into data.
+template <int MODE>
+__global__ void __launch_bounds__(128, 4) sg_cols_dif(DifArgs da, int nk, double2 *data_r, double2 *data_t,
+                                                  double2 *kh_r, double2 *kh_t)
 {
+  const int m = 1 << da.lgm, q16 = m >> 4, mp = m + q16 + 4, tid = threadIdx.x;
+  const int c = tid & 1, q = tid >> 1, k = blockIdx.x * SG_KC2 + c;
+  const bool live = k < nk;
+  double2 *data = blockIdx.y ? data_t : data_r;
+  double2 *kh = blockIdx.y ? kh_t : kh_r;
+  if (MODE == 1 && tid == 0) {
+    // this CTA's kernel spectra (constant: no wait on the previous grid)
+    // into L2 while the forward transform runs
+    const int k0 = blockIdx.x * SG_KC2, nc = (nk - k0 < SG_KC2) ? nk - k0 : SG_KC2;
+    const double2 *src = kh + (size_t)k0 * m;
+    const unsigned bytes = (unsigned)(nc * m * sizeof(double2));
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+  }
   fb_grid_dependency();
   extern __shared__ double2 sm[];
-  const int m = 1 << lgm, mp = m + m / 16, T = blockDim.x, tid = threadIdx.x;
-  const int k0 = blockIdx.x * SG_KC2;
-  const int which = blockIdx.y;  // 0: r, 1: t
-  double2 *data = which ? data_t : data_r;
-  double2 *kh = which ? kh_t : kh_r;
-  double2 *X = sm;
+  double2 *x = sm + c * mp;
   double2 v[16];
+  // pass 0 (span m) from global memory: points q + r m/16
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const int t = tid + q * T, i = t >> 1, c = t & 1, k = k0 + c;  // SG_KC2 == 2
-    v[q] = (i < nrows_in && k < nk) ? data[(size_t)i * nk + k] : make_double2(0.0, 0.0);
-  }
+  for (int r = 0; r < 16; r++)
+    v[r] = (live && (MODE == 0 || r < 8)) ? data[(size_t)(q + r * q16) * nk + k] : make_double2(0.0, 0.0);
+  dft16<0>(v);
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const int t = tid + q * T, i = t >> 1, c = t & 1;
-    X[c * mp + pad16(i)] = v[q];
+  for (int r = 0; r < 16; r++) {
+    double2 o = v[4 * (r & 3) + (r >> 2)];
+    if (r > 0) o = cmul(o, da.tw[r * q16 + q]);
+    x[pad16(q + r * q16)] = o;
   }
   __syncthreads();
-  col_fft<0>(X, lgm, fa);
-  if (mode == 0) {
+  int S = q16, off = m;  // the pass-0 table has 16 (m/16) entries
+  for (int p = 1; p < da.npass; p++) {
+    dif_pass<0>(x, S, q, da.tw + off);
+    __syncthreads();
+    off += S;
+    S >>= 4;
+  }
+  // tail: the thread's 16 consecutive points
 #pragma unroll
-    for (int q = 0; q < 16; q++) {
-      const int t = tid + q * T, c = t >> lgm, i = t & (m - 1), k = k0 + c;
-      if (k < nk) kh[(size_t)k * m + i] = X[c * mp + pad16(i)];
+  for (int r = 0; r < 16; r++) v[r] = x[pad16(16 * q + r)];
+  dif_tail<0>(v, S);
+  if constexpr (MODE == 0) {
+    if (live) {
+#pragma unroll
+      for (int r = 0; r < 16; r++) kh[(size_t)k * m + r * q16 + q] = v[r];  // [r][q]: coalesced
     }
-    return;
-  }
-  // product with -G Khat (sgacc.c:25-38)
+  } else {
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const int t = tid + q * T, c = t >> lgm, i = t & (m - 1), k = k0 + c;
-    v[q] = (k < nk) ? kh[(size_t)k * m + i] : make_double2(0.0, 0.0);
-  }
+    for (int r = 0; r < 16; r++) {
+      const double2 K = live ? kh[(size_t)k * m + r * q16 + q] : make_double2(0.0, 0.0), Sv = v[r];
+      v[r] = make_double2(-FB_G * (K.x * Sv.x - K.y * Sv.y), -FB_G * (K.x * Sv.y + K.y * Sv.x));
+    }
+    dif_tail<1>(v, S);
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const int t = tid + q * T, c = t >> lgm, i = t & (m - 1);
-    const double2 K = v[q], S = X[c * mp + pad16(i)];
-    X[c * mp + pad16(i)] = make_double2(-FB_G * (K.x * S.x - K.y * S.y), -FB_G * (K.x * S.y + K.y * S.x));
-  }
-  __syncthreads();
-  col_fft<1>(X, lgm, fa);
+    for (int r = 0; r < 16; r++) x[pad16(16 * q + r)] = v[r];
+    __syncthreads();
+    for (int p = da.npass - 1; p >= 1; p--) {
+      S <<= 4;
+      off -= S;
+      dif_pass<1>(x, S, q, da.tw + off);
+      __syncthreads();
+    }
+    // backward pass 0: rows q + r' m/16 for r' < 8 only
 #pragma unroll
-  for (int q = 0; q < 16; q++) {
-    const int t = tid + q * T, i = t >> 1, c = t & 1, k = k0 + c;
-    if (i < nrows_in && k < nk) data[(size_t)i * nk + k] = X[c * mp + pad16(i)];
+    for (int r = 0; r < 16; r++) v[r] = x[pad16(q + r * q16)];
+#pragma unroll
+    for (int r = 1; r < 16; r++) {
+      double2 w = da.tw[r * q16 + q];
+      w.y = -w.y;
+      v[r] = cmul(v[r], w);
+    }
+    dft16<1>(v);
+    if (live) {
+#pragma unroll
+      for (int r = 0; r < 8; r++) data[(size_t)(q + r * q16) * nk + k] = v[4 * (r & 3) + (r >> 2)];
+    }
   }
 }
 
@@ -619,30 +745,47 @@ __global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_inv(FftArgs fa, int ns, 
   fb_grid_dependency();
   extern __shared__ double2 sm[];
   double2 *x = sm, *y = sm + ns + ns / 16;  // padded lines
-  const int i = blockIdx.x;
-  for (int k = threadIdx.x; k < ns; k += blockDim.x) {
-    double2 a, b;
-    if (k < nk) {
-      a = wr[(size_t)i * nk + k];
-      b = wt[(size_t)i * nk + k];
-      if (k == 0 || 2 * k == ns) { a.y = 0.0; b.y = 0.0; }  // c2r reads only Re there
-    } else {
-      a = wr[(size_t)i * nk + (ns - k)];
-      b = wt[(size_t)i * nk + (ns - k)];
-      a.y = -a.y;
-      b.y = -b.y;
+  const int i = blockIdx.x, T = blockDim.x;
+  // each stored wavenumber k < nk is read once and gives x[k] and, for
+  // 0 < k with ns - k >= nk, its Hermitian mirror x[ns - k]
+  for (int k0 = 0; k0 < nk; k0 += SG_INV_U * T) {
+    double2 a[SG_INV_U], b[SG_INV_U];
+#pragma unroll
+    for (int u = 0; u < SG_INV_U; u++) {
+      const int k = k0 + threadIdx.x + u * T;
+      a[u] = (k < nk) ? wr[(size_t)i * nk + k] : make_double2(0.0, 0.0);
+      b[u] = (k < nk) ? wt[(size_t)i * nk + k] : make_double2(0.0, 0.0);
     }
-    x[pad16(k)] = make_double2(a.x - b.y, a.y + b.x);  // a + i b
+#pragma unroll
+    for (int u = 0; u < SG_INV_U; u++) {
+      const int k = k0 + threadIdx.x + u * T;
+      if (k >= nk) continue;
+      const double2 p = a[u], q = b[u];
+      if (k >= 1 && ns - k >= nk) x[pad16(ns - k)] = make_double2(p.x + q.y, -p.y + q.x);  // conj p + i conj q
+      if (k == 0 || 2 * k == ns) x[pad16(k)] = make_double2(p.x, q.x);  // c2r reads only Re there
+      else x[pad16(k)] = make_double2(p.x - q.y, p.y + q.x);             // p + i q
+    }
   }
   double2 *A = fft_line_p<1>(x, y, fa);
   const double nrm_r = normr[i], nrm_t = normt[i];
-  for (int j = threadIdx.x; j < ns; j += blockDim.x) {
-    const size_t l = (size_t)i * ns + j;
-    const double2 aj = A[pad16(j)];
-    double ar = aj.x * nrm_r;
-    ar += FB_G * dens[l] * selfk_rstep * selfk_tstep / eps;
-    accr[l] = ar;
-    acct[l] = aj.y * nrm_t;
+  for (int j0 = 0; j0 < ns; j0 += SG_ROW_U * T) {
+    double d[SG_ROW_U];
+#pragma unroll
+    for (int u = 0; u < SG_ROW_U; u++) {
+      const int j = j0 + threadIdx.x + u * T;
+      d[u] = (j < ns) ? dens[(size_t)i * ns + j] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < SG_ROW_U; u++) {
+      const int j = j0 + threadIdx.x + u * T;
+      if (j >= ns) continue;
+      const size_t l = (size_t)i * ns + j;
+      const double2 aj = A[pad16(j)];
+      double ar = aj.x * nrm_r;
+      ar += FB_G * d[u] * selfk_rstep * selfk_tstep / eps;
+      accr[l] = ar;
+      acct[l] = aj.y * nrm_t;
+    }
   }
 }
 
@@ -700,41 +843,34 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   if (rc) { fb_sg_destroy(sg); return rc; }
   sg->smem_row = 2 * ((size_t)ns + ns / 16) * sizeof(double2);  // two padded lines
   sg->smem_col = 2 * (size_t)SG_KC * m * sizeof(double2);
-  sg->p2 = (m >= 16 && m <= 1024 && (m & (m - 1)) == 0);  // CTAs of 2m/16 <= 128 threads
+  sg->p2 = (m >= 32 && m <= 1024 && (m & (m - 1)) == 0);  // CTAs of 2m/16 <= 128 threads
   if (sg->p2) {
-    FftArgs &a = sg->fc2;
-    a.n = m;
-    a.nst = 0;
-    int rem = m;
-    while (rem % 16 == 0) { a.radix[a.nst++] = 16; rem /= 16; }
-    if (rem >= 4) { a.radix[a.nst++] = 4; rem /= 4; }
-    if (rem == 2) { a.radix[a.nst++] = 2; rem /= 2; }
-    for (int q = a.nst; q < SG_MAXST; q++) a.radix[q] = 1;
-    // per-pass twiddle tables: entry [r][jm] = exp(-2 pi i r jm / (L R))
+    DifArgs &a = sg->fc2;
+    a.lgm = 0;
+    while ((1 << a.lgm) < m) a.lgm++;
+    // pass tables: exp(-2 pi i r j / S) at [r][j], r < 16, j < S/16, S = m, m/16, ... >= 32
     std::vector<double2> tab;
-    int L = 1;
-    for (int st = 0; st < a.nst; st++) {
-      const int R = a.radix[st];
-      for (int r = 0; r < R; r++)
-        for (int jm = 0; jm < L; jm++) {
-          const double ang = 2.0 * M_PI * (double)(r * jm) / (double)(L * R);
+    a.npass = 0;
+    for (int S = m; S >= 32; S /= 16) {
+      a.npass++;
+      for (int r = 0; r < 16; r++)
+        for (int j = 0; j < S / 16; j++) {
+          const double ang = 2.0 * M_PI * (double)((r * j) % S) / (double)S;
           tab.push_back(make_double2(cos(ang), -sin(ang)));
         }
-      L *= R;
     }
     if (cudaMalloc(&sg->tw2, tab.size() * sizeof(double2)) != cudaSuccess) { fb_sg_destroy(sg); return FB_ERR_NOMEM; }
     cudaMemcpy(sg->tw2, tab.data(), tab.size() * sizeof(double2), cudaMemcpyHostToDevice);
     a.tw = sg->tw2;
-    sg->smem_col2 = (size_t)SG_KC2 * (m + m / 16) * sizeof(double2);
-    sg->lgm = 0;
-    while ((1 << sg->lgm) < m) sg->lgm++;
+    sg->smem_col2 = (size_t)SG_KC2 * (m + m / 16 + 4) * sizeof(double2);
   }
   int dev = 0, maxopt = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxopt, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
   if (sg->smem_row > (size_t)maxopt || sg->smem_col > (size_t)maxopt) { fb_sg_destroy(sg); return FB_ERR_UNSUPPORTED; }
   if (fb_allow_max_dynamic_smem((const void *)sg_rows_fwd) || fb_allow_max_dynamic_smem((const void *)sg_rows_inv) ||
-      fb_allow_max_dynamic_smem((const void *)sg_cols) || fb_allow_max_dynamic_smem((const void *)sg_cols_p2)) {
+      fb_allow_max_dynamic_smem((const void *)sg_cols) || fb_allow_max_dynamic_smem((const void *)sg_cols_dif<0>) ||
+      fb_allow_max_dynamic_smem((const void *)sg_cols_dif<1>)) {
     fb_sg_destroy(sg);
     return FB_ERR_CUDA;
   }
@@ -800,8 +936,8 @@ int fb_sg_create(fb_sg **out, const fb_params *p, const fb_geom *g, cudaStream_t
   FftArgs fc = fft_args(sg->pcol);
   fb_launch(sg_rows_fwd, m, SG_ROW_BS, sg->smem_row, s, sg->frow, m, ns, nk, nullptr, nullptr, nullptr, 1.0, dkr, dkt, hr, ht);
   if (sg->p2)
-    fb_launch(sg_cols_p2, dim3((nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * m / 16, sg->smem_col2, s, sg->fc2, sg->lgm, m, nk, 0,
-                                                                                          hr, ht, sg->khr, sg->kht);
+    fb_launch(sg_cols_dif<0>, dim3((nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * m / 16, sg->smem_col2, s, sg->fc2, nk, hr, ht,
+              sg->khr, sg->kht);
   else
     fb_launch(sg_cols, dim3((nk + SG_KC - 1) / SG_KC, 2), SG_BS, sg->smem_col, s, fc, m, nk, 0, hr, ht, sg->khr, sg->kht);
   cudaError_t e = cudaStreamSynchronize(s);
@@ -831,8 +967,8 @@ void fb_sg_rows_fwd(fb_sg *sg, const KP &k, const double *dens, cudaStream_t s)
 void fb_sg_cols(fb_sg *sg, cudaStream_t s)
 {
   if (sg->p2) {
-    fb_launch(sg_cols_p2, dim3((sg->nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * sg->m / 16, sg->smem_col2, s, 
-        sg->fc2, sg->lgm, sg->nr, sg->nk, 1, sg->xr, sg->xt, sg->khr, sg->kht);
+    fb_launch(sg_cols_dif<1>, dim3((sg->nk + SG_KC2 - 1) / SG_KC2, 2), SG_KC2 * sg->m / 16, sg->smem_col2, s, sg->fc2,
+              sg->nk, sg->xr, sg->xt, sg->khr, sg->kht);
     return;
   }
   FftArgs fc = fft_args(sg->pcol);
