@@ -92,7 +92,7 @@ static int make_plan(fb_fft_plan *p, int n)
   return FB_OK;
 }
 
-// Passes of a line of n points, radix 16 first and then 4, 2, 3, 5, with
+// Passes of a line of n points, radix 16 first and then 4, 2, 6, 3, 5, with
 // their twiddle tables back to back: pass (R, L) holds exp(-2 pi i r jm /
 // (L R)) at [r][jm], r < R, jm < L.
 static int make_pass_tables(FftArgs *a, double2 **dtab, int n)
@@ -102,8 +102,19 @@ static int make_pass_tables(FftArgs *a, double2 **dtab, int n)
   int rem = n;
   while (rem % 16 == 0 && a->nst < SG_MAXST) { a->radix[a->nst++] = 16; rem /= 16; }
   int tail[SG_MAXST];
-  const int nt = plan_radices(rem, tail);
+  int nt = plan_radices(rem, tail);
   if (nt < 0 || a->nst + nt > SG_MAXST) return FB_ERR_UNSUPPORTED;
+  // a 2 and a 3 make one radix-6 pass instead of two
+  int i2 = -1, i3 = -1;
+  for (int q = 0; q < nt; q++) {
+    if (tail[q] == 2 && i2 < 0) i2 = q;
+    if (tail[q] == 3 && i3 < 0) i3 = q;
+  }
+  if (i2 >= 0 && i3 >= 0) {
+    tail[i2] = 6;
+    for (int q = i3; q + 1 < nt; q++) tail[q] = tail[q + 1];
+    nt--;
+  }
   for (int q = 0; q < nt; q++) a->radix[a->nst++] = tail[q];
   for (int q = a->nst; q < SG_MAXST; q++) a->radix[q] = 1;
   std::vector<double2> tab;
@@ -244,11 +255,35 @@ static __device__ double2 *fft_smem_t(double2 *x, double2 *y, const FftArgs &a)
 }
 
 
-// Radix-R DFT of v[0..R-1] in place (R = 2, 3, 4, 5), natural output order.
+// Radix-R DFT of v[0..R-1] in place (R = 2, 3, 4, 5, 6), natural output order.
+template <int R, int INV>
+static __device__ __forceinline__ void dft_small(double2 *v);
+
+// 6 = 2 x 3: DFT3 of the even and of the odd points, then
+// X[k] = E[k] + w6^k O[k], X[k + 3] = E[k] - w6^k O[k].
+template <int INV>
+static __device__ __forceinline__ void dft6(double2 *v)
+{
+  const double h = 0.86602540378443864676;  // sqrt(3)/2
+  double2 e[3] = {v[0], v[2], v[4]}, o[3] = {v[1], v[3], v[5]};
+  dft_small<3, INV>(e);
+  dft_small<3, INV>(o);
+  const double2 o1 = cmul(o[1], make_double2(0.5, INV ? h : -h));   // w6
+  const double2 o2 = cmul(o[2], make_double2(-0.5, INV ? h : -h));  // w6^2
+  v[0] = cadd(e[0], o[0]);
+  v[3] = csub(e[0], o[0]);
+  v[1] = cadd(e[1], o1);
+  v[4] = csub(e[1], o1);
+  v[2] = cadd(e[2], o2);
+  v[5] = csub(e[2], o2);
+}
+
 template <int R, int INV>
 static __device__ __forceinline__ void dft_small(double2 *v)
 {
-  if (R == 2) {
+  if (R == 6) {
+    dft6<INV>(v);
+  } else if (R == 2) {
     const double2 t0 = v[0];
     v[0] = cadd(t0, v[1]);
     v[1] = csub(t0, v[1]);
@@ -320,12 +355,13 @@ static __device__ __forceinline__ void twiddle16(double2 *v, const double2 *__re
   v[15] = cmul(v[15], cmul(w8, w7));
 }
 
-// One radix-R Stockham pass of a line of n points between two buffers padded
-// by one slot per 16; twp is the pass's twiddle table, R rows of L entries
+// One radix-R Stockham pass of a line of n points read from a buffer padded
+// by one slot per 16; output point p (natural position of this pass) goes
+// to out(p, value).  twp is the pass's twiddle table, R rows of L entries
 // (exp(-2 pi i r jm / (L R)) at [r][jm], read with consecutive jm per warp).
-template <int R, int INV>
-static __device__ __forceinline__ void fft_pass_p(const double2 *__restrict__ x, double2 *__restrict__ y, int n,
-                                                  int L, const double2 *__restrict__ twp)
+template <int R, int INV, class Out>
+static __device__ __forceinline__ void fft_pass_o(const double2 *__restrict__ x, int n, int L,
+                                                  const double2 *__restrict__ twp, Out out)
 {
   const int nb = n / R;
   for (int j = threadIdx.x; j < nb; j += blockDim.x) {
@@ -346,12 +382,26 @@ static __device__ __forceinline__ void fft_pass_p(const double2 *__restrict__ x,
     if (R == 16) dft16<INV>(v); else dft_small<R, INV>(v);
     const int idxD = (j - jm) * R + jm;
 #pragma unroll
-    for (int r = 0; r < R; r++) y[pad16(idxD + r * L)] = (R == 16) ? v[4 * (r & 3) + (r >> 2)] : v[r];
+    for (int r = 0; r < R; r++) out(idxD + r * L, (R == 16) ? v[4 * (r & 3) + (r >> 2)] : v[r]);
+  }
+}
+
+template <int INV, class Out>
+static __device__ __forceinline__ void fft_pass_any(int R, const double2 *x, int n, int L, const double2 *twp, Out out)
+{
+  switch (R) {
+    case 16: fft_pass_o<16, INV>(x, n, L, twp, out); break;
+    case 6: fft_pass_o<6, INV>(x, n, L, twp, out); break;
+    case 4: fft_pass_o<4, INV>(x, n, L, twp, out); break;
+    case 2: fft_pass_o<2, INV>(x, n, L, twp, out); break;
+    case 3: fft_pass_o<3, INV>(x, n, L, twp, out); break;
+    default: fft_pass_o<5, INV>(x, n, L, twp, out); break;
   }
 }
 
 // Stockham FFT of one line in padded shared memory with the passes of a
-// (radix 16 first, then 4, 2, 3, 5); returns the buffer holding the result.
+// (radix 16 first, then 4, 2, 6, 3, 5): the data is in x, y is scratch;
+// returns the buffer holding the result.
 template <int INV>
 static __device__ double2 *fft_line_p(double2 *x, double2 *y, const FftArgs &a)
 {
@@ -359,15 +409,9 @@ static __device__ double2 *fft_line_p(double2 *x, double2 *y, const FftArgs &a)
   int L = 1, off = 0;
   for (int st = 0; st < a.nst; st++) {
     const int R = a.radix[st];
-    const double2 *twp = a.tw + off;
     __syncthreads();
-    switch (R) {
-      case 16: fft_pass_p<16, INV>(x, y, n, L, twp); break;
-      case 4: fft_pass_p<4, INV>(x, y, n, L, twp); break;
-      case 2: fft_pass_p<2, INV>(x, y, n, L, twp); break;
-      case 3: fft_pass_p<3, INV>(x, y, n, L, twp); break;
-      default: fft_pass_p<5, INV>(x, y, n, L, twp); break;
-    }
+    double2 *yy = y;
+    fft_pass_any<INV>(R, x, n, L, a.tw + off, [=](int p, double2 v) { yy[pad16(p)] = v; });
     double2 *t = x;
     x = y;
     y = t;
@@ -416,7 +460,7 @@ __global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_fwd(FftArgs fa, int nrow
   }
   double2 *Z = fft_line_p<0>(x, y, fa);
   for (int k = threadIdx.x; k < nk; k += blockDim.x) {
-    const double2 zk = Z[pad16(k)], zc = Z[pad16((ns - k) % ns)];
+    const double2 zk = Z[pad16(k)], zc = Z[pad16(k ? ns - k : 0)];
     // A = (Z[k] + conj Z[-k]) / 2 ; B = (Z[k] - conj Z[-k]) / (2i)
     const double2 A = make_double2(0.5 * (zk.x + zc.x), 0.5 * (zk.y - zc.y));
     const double2 B = make_double2(0.5 * (zk.y + zc.y), -0.5 * (zk.x - zc.x));
@@ -746,6 +790,9 @@ __global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_inv(FftArgs fa, int ns, 
   extern __shared__ double2 sm[];
   double2 *x = sm, *y = sm + ns + ns / 16;  // padded lines
   const int i = blockIdx.x, T = blockDim.x;
+  const double nrm_r = normr[i], nrm_t = normt[i];
+  const double *di = dens + (size_t)i * ns;
+  double *ar_i = accr + (size_t)i * ns, *at_i = acct + (size_t)i * ns;
   // each stored wavenumber k < nk is read once and gives x[k] and, for
   // 0 < k with ns - k >= nk, its Hermitian mirror x[ns - k]
   for (int k0 = 0; k0 < nk; k0 += SG_INV_U * T) {
@@ -767,24 +814,22 @@ __global__ void __launch_bounds__(SG_ROW_BS, 4) sg_rows_inv(FftArgs fa, int ns, 
     }
   }
   double2 *A = fft_line_p<1>(x, y, fa);
-  const double nrm_r = normr[i], nrm_t = normt[i];
   for (int j0 = 0; j0 < ns; j0 += SG_ROW_U * T) {
     double d[SG_ROW_U];
 #pragma unroll
     for (int u = 0; u < SG_ROW_U; u++) {
       const int j = j0 + threadIdx.x + u * T;
-      d[u] = (j < ns) ? dens[(size_t)i * ns + j] : 0.0;
+      d[u] = (j < ns) ? di[j] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < SG_ROW_U; u++) {
       const int j = j0 + threadIdx.x + u * T;
       if (j >= ns) continue;
-      const size_t l = (size_t)i * ns + j;
       const double2 aj = A[pad16(j)];
       double ar = aj.x * nrm_r;
       ar += FB_G * d[u] * selfk_rstep * selfk_tstep / eps;
-      accr[l] = ar;
-      acct[l] = aj.y * nrm_t;
+      ar_i[j] = ar;
+      at_i[j] = aj.y * nrm_t;
     }
   }
 }
