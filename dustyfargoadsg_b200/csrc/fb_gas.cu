@@ -1417,19 +1417,44 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
     const double2 x = pair(P, j, RH / 2);
     return (RH & 1) ? x.y : x.x;
   };
-  for (int j = tid; j < ns; j += T) {
-    double v[AZP];
+  int jj[E], jjm[E], jjp[E];
 #pragma unroll
-    for (int q = 0; q < AZP; q++) v[q] = (q < NQ) ? k.q[q][base + j] : 0.0;
-    double2 *c = (double2 *)(P + AZP * j);
+  for (int e = 0; e < E; e++) {
+    const int j = tid + e * T;
+    jj[e] = j;
+    jjm[e] = (j == 0) ? ns - 1 : j - 1;
+    jjp[e] = (j == ns - 1) ? 0 : j + 1;
+  }
+#define OWN(e) (FULL || jj[e] < ns)
+  // every global load of the kernel at once: the own cells' quantities and
+  // vtheta of each own cell and of its upper neighbour (the residual
+  // velocities of both faces)
+  double vtc[E], vtn[E];
+  {
+    double v[E][AZP];
 #pragma unroll
-    for (int h = 0; h < AZP / 2; h++) c[h] = make_double2(v[2 * h], v[2 * h + 1]);
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+#pragma unroll
+      for (int q = 0; q < AZP; q++) v[e][q] = (q < NQ) ? k.q[q][base + jj[e]] : 0.0;
+      vtc[e] = k.vt[base + jj[e]];
+      vtn[e] = k.vt[base + jjp[e]];
+    }
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      if (!OWN(e)) continue;
+      double2 *c = (double2 *)(P + AZP * jj[e]);
+#pragma unroll
+      for (int h = 0; h < AZP / 2; h++) c[h] = make_double2(v[e][2 * h], v[e][2 * h + 1]);
+    }
   }
   // ComputeThetaElongations / ComputeAverageThetaVelocities / ComputeResiduals
   const double invdt = 1.0 / dt;
   double s = 0.0;
-  for (int j = tid; j < ns; j += T) {
-    double elong = k.vt[base + j] * dt;
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    if (!OWN(e)) continue;
+    double elong = vtc[e] * dt;
     s += elong * invdt;
   }
   s = block_sum_dyn(s, sh);
@@ -1441,9 +1466,9 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
   const long nshift = (long)Nround;
   double vconst = (Ntilde - Nround) * k.rmed[i] * invdt * dpinvns;
   const double vconst0 = vconst;
-  // ComputeResiduals' value of cell j (vtheta is not written before the end)
-  auto vres_at = [&](int j) -> double {
-    double elong = k.vt[base + j] * dt;
+  // ComputeResiduals' value of a cell of vtheta vtj
+  auto vres_of = [&](double vtj) -> double {
+    double elong = vtj * dt;
     double v = elong * invdt - VMed;
     if (!k.fast_transport) v = vconst0 + v;
     return v;
@@ -1452,15 +1477,6 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
   const double dxtheta = k.dxtheta[i], invdxtheta = k.invdxtheta[i];
   const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
   const double invsurf = 1.0 / k.surf[i];
-  int jj[E], jjm[E], jjp[E];
-#pragma unroll
-  for (int e = 0; e < E; e++) {
-    const int j = tid + e * T;
-    jj[e] = j;
-    jjm[e] = (j == 0) ? ns - 1 : j - 1;
-    jjp[e] = (j == ns - 1) ? 0 : j + 1;
-  }
-#define OWN(e) (FULL || jj[e] < ns)
   for (int pass = 0; pass < 2; pass++) {
     const bool uniform = (pass == 1);
     if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
@@ -1484,7 +1500,7 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
 #pragma unroll
     for (int e = 0; e < E; e++) {
       if (!OWN(e)) continue;
-      const double vl = uniform ? vconst : vres_at(jj[e]), vh = uniform ? vconst : vres_at(jjp[e]);
+      const double vl = uniform ? vconst : vres_of(vtc[e]), vh = uniform ? vconst : vres_of(vtn[e]);
       Vl[e] = vl;
       Vh[e] = vh;
       const double kl = vl * dt, kh = vh * dt;
@@ -1851,16 +1867,37 @@ __global__ void __launch_bounds__(FB_BS) k_damping(KP k, double dtov)
   }
   const int zero_here = k.zero_vrad &&
       (((k.rmed[i] < k.wkzrmin) && (i == 0 || i == 1)) || ((k.rmed[i] > k.wkzrmax) && (i == nr - 1)));
-  for (int j = threadIdx.x; j < ns; j += FB_BS) {
-    const size_t l = base + j;
-    k.vr[l] = (k.vr[l] + lambda * vrad0) / (1.0 + lambda);
-    k.vt[l] = (k.vt[l] + lambda * vtheta0) / (1.0 + lambda);
-    k.rho[l] = (k.rho[l] + lambda * dens0) / (1.0 + lambda);
-    if (k.energy) k.e[l] = (k.e[l] + lambda * energ0) / (1.0 + lambda);
-    if (zero_here) {
-      k.vr[l] = 0.0;
-      k.rho[l] = dens0;
-      k.vt[l] = vtheta0;
+  // one divisor per ring: each quotient is the correctly rounded x / (1 +
+  // lambda) through its reciprocal; a batch's loads are all in flight
+  // before its first store
+  const double den = 1.0 + lambda, rden = 1.0 / den;
+  for (int j0 = threadIdx.x; j0 < ns; j0 += RING_U * FB_BS) {
+    double vr[RING_U], vt[RING_U], rh[RING_U], en[RING_U];
+#pragma unroll
+    for (int u = 0; u < RING_U; u++) {
+      const int j = j0 + u * FB_BS;
+      if (j < ns) {
+        vr[u] = k.vr[base + j];
+        vt[u] = k.vt[base + j];
+        rh[u] = k.rho[base + j];
+        en[u] = k.energy ? k.e[base + j] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < RING_U; u++) {
+      const int j = j0 + u * FB_BS;
+      if (j >= ns) continue;
+      const size_t l = base + j;
+      if (zero_here) {
+        k.vr[l] = 0.0;
+        k.rho[l] = dens0;
+        k.vt[l] = vtheta0;
+      } else {
+        k.vr[l] = fb_quot(vr[u] + lambda * vrad0, den, rden);
+        k.vt[l] = fb_quot(vt[u] + lambda * vtheta0, den, rden);
+        k.rho[l] = fb_quot(rh[u] + lambda * dens0, den, rden);
+      }
+      if (k.energy) k.e[l] = fb_quot(en[u] + lambda * energ0, den, rden);
     }
   }
 }
