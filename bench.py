@@ -57,7 +57,7 @@ FALLBACK_HBM_GBS = 6650.0
 STAGE_BYTES = {
     "cfl_forces": (32, 40), "potential": (8, 8), "soundspeed": (0, 24),
     "substep1": (64, 64), "viscous_terms": (56, 56), "viscous_update": (64, 64),
-    "substep2": (40, 56), "energy_viscous_terms": (56, 56), "substep3": (0, 56),
+    "substep2": (40, 56), "substep3": (0, 80),
     "transport_radial": (64, 80), "transport_azimuthal": (80, 96),
     "transport_vr_boundary": (40, 40),
 }

@@ -604,16 +604,10 @@ static int enqueue_substep(fb_ctx *ctx)
     STAGE(ST_VUPDATE, 1, fb_launch_viscous_update(k, k.vri, k.vti, 0.0, s));
   }
   STAGE(ST_SUB2, 1, fb_launch_substep2(k, s));
-  if (k.energy) {
-    if (k.viscous_heating)
-      STAGE(ST_EVTERMS, 1, fb_launch_viscous_terms(k, k.vr, k.vt, s));
-    else
-      STAGE(ST_EVTERMS, 1, fb_launch_divergence(k, s));
-    STAGE(ST_SUB3, 1, fb_launch_substep3(k, s));
-  }
+  if (k.energy) STAGE(ST_SUB3, 1, fb_launch_substep3(k, s));  // with the stresses of the new velocities
   STAGE(ST_TRAD, 1, fb_launch_transport_radial(k, 0.0, s));
   STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s));
-  STAGE(ST_TVR, 2, fb_launch_transport_vr(k, s));
+  STAGE(ST_TVR, 1, fb_launch_transport_vr(k, s));
   if (k.evanescent && k.n_damp_rings > 0) STAGE(ST_DAMP, 1, fb_launch_damping(k, 0.0, s));
   if (!ctx->has_dust) cudaStreamWaitEvent(s, ctx->ev_planets, 0);
   if (ctx->profiling) {
@@ -1303,7 +1297,7 @@ extern "C" int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_ou
   Snapshot sn;
   rc = snapshot_take(ctx, sn);
   if (rc) { snapshot_free(sn); fb_profile(ctx, 0); return rc; }
-  const int cell_stages[] = {ST_POT, ST_SUB1, ST_VTERMS, ST_VUPDATE, ST_SUB2, ST_EVTERMS, ST_TVR};
+  const int cell_stages[] = {ST_POT, ST_SUB1, ST_VTERMS, ST_VUPDATE, ST_SUB2, ST_SUB3, ST_TVR};
   const int azi_stage[] = {ST_TAZI};
   const int rad_stage[] = {ST_TRAD};
   double total = 0.0;

@@ -190,7 +190,6 @@ void fb_launch_substep1(const KP &k, cudaStream_t s);
 void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s);
 void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s);
 void fb_launch_substep2(const KP &k, cudaStream_t s);
-void fb_launch_divergence(const KP &k, cudaStream_t s);
 void fb_launch_substep3(const KP &k, cudaStream_t s);
 void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s);

@@ -712,46 +712,71 @@ void fb_launch_substep1(const KP &k, cudaStream_t s)
 
 // ------------------------------------------------------- viscous stresses
 // ComputeViscousTerms (Viscosity.c:159-303) incl. ComputeDivergenceVelocity
-// (SourceEuler.c:2373-2412): DivV, TAUrr, TAUpp (all rings), TAUrp (i >= 1).
-__global__ void __launch_bounds__(FB_BS2) k_viscous_terms(KP k, const double *__restrict__ vr,
-                                                         const double *__restrict__ vt)
+// (SourceEuler.c:2373-2412) at cell (i, j): DivV, TAUrr, TAUpp (all rings),
+// TAUrp (i >= 1); taus = 0: DivV alone.
+struct Stress {
+  double div, trr, tpp, trp;
+};
+static __device__ __forceinline__ Stress stress_at(const KP &k, const double *__restrict__ vr,
+                                                   const double *__restrict__ vt, int i, int j, bool taus)
 {
-  fb_grid_dependency();
   const int ns = k.ns;
   const double invdphi = k.invdphi, onethird = 1.0 / 3.0;
-  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= ns) return;
   const size_t l = (size_t)i * ns + j;
   const size_t lip = l + ns;
   const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
   const size_t ljm = (j == 0) ? (size_t)i * ns + ns - 1 : l - 1;
   // every load first
-  const double vrl = vr[l], vrip = vr[lip], vtl = vt[l], vtjp = vt[ljp], rl = k.rho[l];
+  const double vrl = vr[l], vrip = vr[lip], vtl = vt[l], vtjp = vt[ljp];
   const double rsup = k.rsup[i], rinf = k.rinf[i], invdiffrsup = k.invdiffrsup[i], invrmed = k.invrmed[i];
-  double vtim = 0.0, vrjm = 0.0, rim = 0.0, rjm = 0.0, rjmim = 0.0, invrmedm = 0.0, invdiffrmed = 0.0, invrinf = 0.0;
-  if (i >= 1) {
-    const size_t lim = l - ns, ljmim = ljm - ns;
-    vtim = vt[lim];
-    vrjm = vr[ljm];
-    rim = k.rho[lim];
-    rjm = k.rho[ljm];
-    rjmim = k.rho[ljmim];
-    invrmedm = k.invrmed[i - 1];
-    invdiffrmed = k.invdiffrmed[i];
-    invrinf = k.invrinf[i];
+  double rl = 0.0, vtim = 0.0, vrjm = 0.0, rim = 0.0, rjm = 0.0, rjmim = 0.0, invrmedm = 0.0, invdiffrmed = 0.0,
+         invrinf = 0.0;
+  if (taus) {
+    rl = k.rho[l];
+    if (i >= 1) {
+      const size_t lim = l - ns, ljmim = ljm - ns;
+      vtim = vt[lim];
+      vrjm = vr[ljm];
+      rim = k.rho[lim];
+      rjm = k.rho[ljm];
+      rjmim = k.rho[ljmim];
+      invrmedm = k.invrmed[i - 1];
+      invdiffrmed = k.invdiffrmed[i];
+      invrinf = k.invrinf[i];
+    }
   }
+  Stress st;
   double div = (vrip * rsup - vrl * rinf) * invdiffrsup * invrmed;
   div += (vtjp - vtl) * invdphi * invrmed;
-  k.divv[l] = div;
-  const double Drr = (vrip - vrl) * invdiffrsup;
-  const double Dpp = (vtjp - vtl) * invdphi * invrmed + 0.5 * (vrip + vrl) * invrmed;
-  const double viscosity = nu_ring(k, i);
-  k.trr[l] = 2.0 * rl * viscosity * (Drr - onethird * div);
-  k.tpp[l] = 2.0 * rl * viscosity * (Dpp - onethird * div);
-  if (i >= 1) {
-    const double Drp = 0.5 * (rinf * (vtl * invrmed - vtim * invrmedm) * invdiffrmed + (vrl - vrjm) * invdphi * invrinf);
-    k.trp[l] = 2.0 * 0.25 * (rl + rim + rjm + rjmim) * viscosity * Drp;
+  st.div = div;
+  st.trr = st.tpp = st.trp = 0.0;
+  if (taus) {
+    const double Drr = (vrip - vrl) * invdiffrsup;
+    const double Dpp = (vtjp - vtl) * invdphi * invrmed + 0.5 * (vrip + vrl) * invrmed;
+    const double viscosity = nu_ring(k, i);
+    st.trr = 2.0 * rl * viscosity * (Drr - onethird * div);
+    st.tpp = 2.0 * rl * viscosity * (Dpp - onethird * div);
+    if (i >= 1) {
+      const double Drp = 0.5 * (rinf * (vtl * invrmed - vtim * invrmedm) * invdiffrmed + (vrl - vrjm) * invdphi * invrinf);
+      st.trp = 2.0 * 0.25 * (rl + rim + rjm + rjmim) * viscosity * Drp;
+    }
   }
+  return st;
+}
+
+__global__ void __launch_bounds__(FB_BS2) k_viscous_terms(KP k, const double *__restrict__ vr,
+                                                         const double *__restrict__ vt)
+{
+  fb_grid_dependency();
+  const int ns = k.ns;
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const size_t l = (size_t)i * ns + j;
+  const Stress st = stress_at(k, vr, vt, i, j, true);
+  k.divv[l] = st.div;
+  k.trr[l] = st.trr;
+  k.tpp[l] = st.tpp;
+  if (i >= 1) k.trp[l] = st.trp;
 }
 
 void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s)
@@ -878,46 +903,26 @@ void fb_launch_substep2(const KP &k, cudaStream_t s)
   fb_launch(k_substep2, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k);
 }
 
-// ComputeDivergenceVelocity (SourceEuler.c:2373-2412) on (Vrad, Vtheta)
-__global__ void __launch_bounds__(FB_BS2) k_divergence(KP k)
-{
-  fb_grid_dependency();
-  const int ns = k.ns;
-  {
-    const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= ns) return;
-    const size_t l = (size_t)i * ns + j;
-    const size_t lip = l + ns;
-    const size_t ljp = (j == ns - 1) ? (size_t)i * ns : l + 1;
-    double div = (k.vr[lip] * k.rsup[i] - k.vr[l] * k.rinf[i]) * k.invdiffrsup[i] * k.invrmed[i];
-    div += (k.vt[ljp] - k.vt[l]) * k.invdphi * k.invrmed[i];
-    k.divv[l] = div;
-  }
-}
-
-void fb_launch_divergence(const KP &k, cudaStream_t s)
-{
-  fb_launch(k_divergence, grid2d(k, k.nr), k.cell_bs, 0, s, k);
-}
-
 // ------------------------------------------------------------ SubStep3
-static __device__ __forceinline__ double vischeat_at(const KP &k, int i, size_t l)
+static __device__ __forceinline__ double vischeat_of(const KP &k, int i, double rho, const Stress &st)
 {
   // ComputeViscousHeating, SourceEuler.c:1570-1583 (i >= 1)
   const double viscosity = nu_ring(k, i);
   if (viscosity != 0.0) {
-    double vh = 0.5 / viscosity / k.rho[l] *
-                (k.trr[l] * k.trr[l] + 2.0 * k.trp[l] * k.trp[l] + k.tpp[l] * k.tpp[l]);
-    vh += (2.0 / 9.0) * viscosity * k.rho[l] * k.divv[l] * k.divv[l];
+    double vh = 0.5 / viscosity / rho * (st.trr * st.trr + 2.0 * st.trp * st.trp + st.tpp * st.tpp);
+    vh += (2.0 / 9.0) * viscosity * rho * st.div * st.div;
     return vh;
   }
   return 0.0;
 }
 
-// ComputeViscousHeating (SourceEuler.c:1554-1606) and SubStep3
-// (SourceEuler.c:1119-1302; pdV, viscous heating, beta cooling), one CTA
-// per ring because beta cooling needs the ring mean of vtheta.  Writes
-// Energy = EnergyNew (ring nr of EnergyNew is never written: zero).
+// ComputeViscousTerms on the new velocities (for the heating; DivergenceVelocity
+// alone without it), ComputeViscousHeating (SourceEuler.c:1554-1606) and
+// SubStep3 (SourceEuler.c:1119-1302; pdV, viscous heating, beta cooling) in
+// one pass: a cell's stresses feed its own heating, so they are evaluated
+// here (and still stored) instead of read back.  Ring 0's heating is
+// extrapolated from rings 1 and 2, whose stresses its threads evaluate too.
+// Writes Energy = EnergyNew (ring nr of EnergyNew is never written: zero).
 __global__ void __launch_bounds__(FB_BS2) k_substep3(KP k)
 {
   fb_grid_dependency();
@@ -929,6 +934,17 @@ __global__ void __launch_bounds__(FB_BS2) k_substep3(KP k)
     k.e[l] = 0.0;
     return;
   }
+  const bool heat = k.viscous_heating;
+  const Stress st = stress_at(k, k.vr, k.vt, i, j, heat);
+  Stress s1, s2;
+  double r1 = 0.0, r2 = 0.0;
+  if (heat && i == 0) {
+    s1 = stress_at(k, k.vr, k.vt, 1, j, true);
+    s2 = stress_at(k, k.vr, k.vt, 2, j, true);
+    r1 = k.rho[l + ns];
+    r2 = k.rho[l + 2 * ns];
+  }
+  const double el = k.e[l], rl = k.rho[l];
   const double dt = k.ctl->dt;
   double coolfac = 0.0;
   if (k.beta_cooling) {
@@ -941,22 +957,26 @@ __global__ void __launch_bounds__(FB_BS2) k_substep3(KP k)
     double coolingtime = k.betatab[i] / omega;
     coolfac = coolingtime;
   }
-  // the i = 0 extrapolation tests the viscosity of the last ring visited by
-  // the i >= 1 loop (ring nr-1), SourceEuler.c:1598
-  const double visc_last = nu_ring(k, nr - 1);
+  k.divv[l] = st.div;
   double vh = 0.0;
-  if (k.viscous_heating) {
+  if (heat) {
+    k.trr[l] = st.trr;
+    k.tpp[l] = st.tpp;
     if (i >= 1) {
-      vh = vischeat_at(k, i, l);
+      k.trp[l] = st.trp;
+      vh = vischeat_of(k, i, rl, st);
     } else {
-      const double qpip = vischeat_at(k, 1, l + ns);
-      const double qpi2p = vischeat_at(k, 2, l + 2 * ns);
+      // the i = 0 extrapolation tests the viscosity of the last ring visited
+      // by the i >= 1 loop (ring nr-1), SourceEuler.c:1598
+      const double visc_last = nu_ring(k, nr - 1);
+      const double qpip = vischeat_of(k, 1, r1, s1);
+      const double qpi2p = vischeat_of(k, 2, r2, s2);
       vh = (visc_last != 0.0) ? qpip * exp(log(qpip / qpi2p) * k.vh_l1 / k.vh_l2) : 0.0;
     }
+    k.vischeat[l] = vh;
   }
-  const double el = k.e[l], dv = k.divv[l];
-  if (k.viscous_heating) k.vischeat[l] = vh;
-  double num = el + (double)(k.viscous_heating ? 1 : 0) * vh * dt;
+  const double dv = st.div;
+  double num = el + (double)(heat ? 1 : 0) * vh * dt;
   double den = 1.0 + (k.gamma - 1.0) * dt * dv;
   double en = num / den;
   if (k.beta_cooling) {
@@ -1678,15 +1698,39 @@ int fb_azi_variant(int ns, int energy, int E, int variant)
   }
 }
 
+// LostMass += LostByDisk of the density's VanLeerRadial (TransportEuler.c:137,
+// :213-216): the ring-0 radial fluxes summed over azimuth by one warp, lane
+// by lane in azimuth order, then across lanes; a batch's loads all in flight.
+static __device__ __forceinline__ void lost_mass_sum(const KP &k)
+{
+  constexpr int U = 24;  // 1536 azimuths: two batches
+  double s = 0.0;
+  for (int j0 = threadIdx.x; j0 < k.ns; j0 += 32 * U) {
+    double v[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      const int j = j0 + 32 * u;
+      v[u] = (j < k.ns) ? k.lost0[j] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < U; u++)
+      if (j0 + 32 * u < k.ns) s += v[u];
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (threadIdx.x == 0) k.ctl->lost_mass += 0.0 + s;
+}
+
 // ComputeVelocities' radial part (TransportEuler.c:531-536) needs the
 // neighbouring ring after both passes; fused with AddFloorDensity
 // (SourceEuler.c:2506) and ApplyWallBoundaries (SideEuler.c:1047-1099).
+// The first warp of the first CTA also adds the lost mass.
 __global__ void __launch_bounds__(FB_BS2) k_transport_vr(KP k)
 {
   fb_grid_dependency();
   const int ns = k.ns, nr = k.nr;
   const int wall = k.wall && !k.transport_only;
   const int floors = k.add_floors && !k.transport_only;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x < 32) lost_mass_sum(k);
   {
     const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= ns) return;
@@ -1712,17 +1756,6 @@ __global__ void __launch_bounds__(FB_BS2) k_transport_vr(KP k)
     k.rho[l] = d;
     k.vr[l] = v;
   }
-}
-
-// LostMass += LostByDisk of the density's VanLeerRadial (TransportEuler.c:137,
-// :213-216): the ring-0 radial fluxes summed over azimuth.
-__global__ void k_lostmass(KP k)
-{
-  fb_grid_dependency();
-  double s = 0.0;
-  for (int j = threadIdx.x; j < k.ns; j += 32) s += k.lost0[j];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  if (threadIdx.x == 0) k.ctl->lost_mass += 0.0 + s;
 }
 
 // Rings per CTA of the radial pass when not tuned: 64-column CTAs, chunks
@@ -1796,10 +1829,9 @@ void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t
 void fb_launch_transport_vr(const KP &k, cudaStream_t s)
 {
   fb_launch(k_transport_vr, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k);
-  fb_launch(k_lostmass, 1, 32, 0, s, k);
 }
 
-// Transport (TransportEuler.c:65-87) + floors + boundaries: 4 launches
+// Transport (TransportEuler.c:65-87) + floors + boundaries: 3 launches
 void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s)
 {
   fb_launch_transport_radial(k, dt_override, s);
