@@ -177,6 +177,10 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
   // square root is evaluated in the reference's order once it is
   double *vtc = cfl_sm, *s12 = cfl_sm + ns, *s4 = cfl_sm + 2 * ns;
   const double dxrad = k.dxrad[i], dxtheta = k.dxtheta_cfl[i];
+  // the quotients by the ring's constant lengths, each correctly rounded
+  // through one reciprocal per ring
+  const double dxmin = min2(dxrad, dxtheta);
+  const double rdxmin = 1.0 / dxmin, rdxrad = 1.0 / dxrad, rdxtheta = 1.0 / dxtheta;
   int neg = 0, bad = 0;
   for (int j = tid; j < ns; j += T) {
     const double vtj = vt[j], vrj = vr[j], dens = rho[j];
@@ -203,13 +207,13 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
     v[5] += surf * dens * yc;
     if (cfl) {
       const int jp = (j == ns - 1) ? 0 : j + 1;
-      double invdt1 = k.cs[base + j] / (min2(dxrad, dxtheta));
-      double invdt2 = fabs(vrj) / dxrad;
+      double invdt1 = fb_quot(k.cs[base + j], dxmin, rdxmin);
+      double invdt2 = fb_quot(fabs(vrj), dxrad, rdxrad);
       double dvr = vr[ns + j] - vrj;
       double dvt = vt[jp] - vtj;
       if (dvr >= 0.0) dvr = 1e-10; else dvr = -dvr;
       if (dvt >= 0.0) dvt = 1e-10; else dvt = -dvt;
-      double invdt4 = max2(dvr / dxrad, dvt / dxtheta);
+      double invdt4 = max2(fb_quot(dvr, dxrad, rdxrad), fb_quot(dvt, dxtheta, rdxtheta));
       invdt4 *= 4.0 * FB_CVNR * FB_CVNR;
       vtc[j] = vtj;
       s12[j] = invdt1 * invdt1 + invdt2 * invdt2;
@@ -236,7 +240,7 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
     double m = 1e30;
     for (int j = tid; j < ns; j += T) {  // each thread reads back its own cells
       double vres = k.fast_transport ? vtc[j] - vmoy : vtc[j];
-      double invdt3 = fabs(vres) / dxtheta;
+      double invdt3 = fb_quot(fabs(vres), dxtheta, rdxtheta);
       double dt = FB_CFLSECURITY / sqrt(s12[j] + invdt3 * invdt3 + s4[j] + invdt5 * invdt5 + invdt6 * invdt6);
       if (dt < m) m = dt;
     }
@@ -980,8 +984,8 @@ __global__ void __launch_bounds__(FB_BS2) k_substep3(KP k)
   double den = 1.0 + (k.gamma - 1.0) * dt * dv;
   double en = num / den;
   if (k.beta_cooling) {
-    double d2 = 1.0 + dt / coolfac;
-    en = en / d2;
+    const double d2 = 1.0 + dt / coolfac;  // one per ring: the quotient through its reciprocal
+    en = fb_quot(en, d2, 1.0 / d2);
   }
   k.e[l] = en;
 }
