@@ -246,7 +246,7 @@ int fb_diagnostics(fb_ctx *ctx, double *mass, double *momentum);
 typedef struct fb_tuning {
   int cell_block, azi_cells_per_thread, rad_columns, rad_rings;
   int azi_variant;  /* 0 automatic, 1 narrow (NQ+3 shared rings), 2 wide (2 NQ+1 rings),
-                       3 packed (14 rings, a cell's quantities side by side) */
+                       3 packed (12 rings, 13 with energy; a cell's quantities side by side) */
 } fb_tuning;
 int fb_get_tuning(const fb_ctx *ctx, fb_tuning *t);
 int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t);
