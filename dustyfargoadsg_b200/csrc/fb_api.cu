@@ -1334,17 +1334,24 @@ extern "C" int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_ou
   }
   // 3. columns x rings per CTA of the radial pass
   {
-    const int txs[] = {32, 64, 128}, chunks[] = {4, 8, 16, 32};
+    const int txs[] = {32, 64, 128};
     int btx = k.rad_tx, bch = k.rad_chunk;
     double bestms = 1e300;
-    for (int tx : txs)
-      for (int ch : chunks) {
-        if (ch > k.nr) continue;
+    for (int tx : txs) {
+      // powers of two and the chunks that fill whole waves of this width
+      int chunks[10] = {4, 8, 16, 32};
+      int nch = 4 + fb_rad_chunks_balanced(k, tx, chunks + 4, 6);
+      for (int q = 0; q < nch; q++) {
+        const int ch = chunks[q];
+        bool seen = false;
+        for (int u = 0; u < q; u++) seen = seen || (chunks[u] == ch);
+        if (seen || ch > k.nr) continue;
         k.rad_tx = tx;
         k.rad_chunk = ch;
         const double ms = tune_measure(ctx, sn, substeps, rad_stage, 1);
         if (ms >= 0.0 && ms < bestms) { bestms = ms; btx = tx; bch = ch; }
       }
+    }
     k.rad_tx = btx;
     k.rad_chunk = bch;
     total += bestms;

@@ -206,6 +206,7 @@ int  fb_azi_E_valid(int ns, int energy, int E);   // 1 if E cells/thread fit thi
 int  fb_azi_E_auto(int ns);
 int  fb_azi_variant(int ns, int energy, int E, int variant);  // variant a launch takes (0: cannot run)
 int  fb_rad_chunk_auto(const KP &k);
+int  fb_rad_chunks_balanced(const KP &k, int tx, int *out, int max);
 int  fb_allow_max_dynamic_smem(const void *func);
 void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s);
 void fb_launch_loop_cond(const KP &k, cudaGraphConditionalHandle h, int cap, cudaStream_t s);

@@ -1762,15 +1762,60 @@ __global__ void __launch_bounds__(FB_BS2) k_transport_vr(KP k)
   }
 }
 
-// Rings per CTA of the radial pass when not tuned: 64-column CTAs, chunks
-// halving from 32 until there are >= 4 CTAs per SM (longer chunks reread
-// fewer halo rings, shorter ones fill the GPU).
+// Ring chunks of the radial pass that fill whole waves: for r = 1..6 rounds
+// of the CTAs the GPU holds at once (`tx` columns per CTA), the smallest
+// chunk whose grid takes at most r rounds.  A CTA's time grows with its
+// chunk plus the two halo rings it rereads, so a grid one CTA past a wave
+// costs a whole extra round; these chunks avoid that.  Returns how many
+// were written to out (increasing r, decreasing chunk).
+int fb_rad_chunks_balanced(const KP &k, int tx, int *out, int max)
+{
+  int dev = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 0;
+  const cudaError_t e = k.energy ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<6>, 2 * tx, 0)
+                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<5>, 2 * tx, 0);
+  if (e != cudaSuccess || per < 1 || sms < 1) {
+    cudaGetLastError();
+    return 0;
+  }
+  const int bx = (k.ns + tx - 1) / tx, slots = per * sms;
+  int n = 0;
+  for (int r = 1; r <= 6 && n < max; r++) {
+    const int rows = (r * slots) / bx;  // ring chunks that r rounds hold
+    if (rows < 1) continue;
+    int ch = (k.nr + rows - 1) / rows;
+    if (ch < 2) ch = 2;
+    if (n == 0 || out[n - 1] != ch) out[n++] = ch;
+  }
+  return n;
+}
+
+// Rings per CTA of the radial pass when not tuned: 64-column CTAs and, of
+// the wave-filling chunks, the one with the least rounds x (chunk + 2 halo
+// rings); 16 if the occupancy query fails.
 int fb_rad_chunk_auto(const KP &k)
 {
-  const int tx = k.rad_tx > 0 ? k.rad_tx : 64, bx = (k.ns + tx - 1) / tx;
-  int chunk = 32;
-  while (chunk > 4 && (long)bx * ((k.nr + chunk - 1) / chunk) < 4 * 148) chunk /= 2;
-  return chunk;
+  const int tx = k.rad_tx > 0 ? k.rad_tx : 64;
+  int ch[6];
+  const int n = fb_rad_chunks_balanced(k, tx, ch, 6);
+  if (n == 0) return 16;
+  const int bx = (k.ns + tx - 1) / tx;
+  int dev = 0, sms = 148, per = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (k.energy) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<6>, 2 * tx, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<5>, 2 * tx, 0);
+  const long slots = (long)(per > 0 ? per : 1) * sms;
+  int best = ch[0];
+  long bestcost = -1;
+  for (int q = 0; q < n; q++) {
+    const long ctas = (long)bx * ((k.nr + ch[q] - 1) / ch[q]);
+    const long rounds = (ctas + slots - 1) / slots;
+    const long cost = rounds * (ch[q] + 2);
+    if (bestcost < 0 || cost < bestcost) { bestcost = cost; best = ch[q]; }
+  }
+  return best;
 }
 
 void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
