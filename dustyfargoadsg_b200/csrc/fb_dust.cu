@@ -323,11 +323,22 @@ __global__ void __launch_bounds__(D_BS) k_rng_scatter(PP pp)
   }
 }
 
-// Minimum_Stopping_Time (Dsys.c:757-759): positive doubles order like their
-// bit patterns, so an integer atomicMin on the bits is a min on the values.
+// Minimum_Stopping_Time (Dsys.c:757-759), the smallest stopping time of the
+// substep (the dust time-step bound).  Non-negative doubles order like their
+// bit patterns, so an integer minimum on the bits is a minimum on the
+// values, exact in any order: the lanes that get here together first take their
+// minimum (high words, then low words among the lanes with the smallest
+// high word), and one of them updates the global value -- one atomic per
+// warp instead of one per particle, all on the same address.
 static __device__ __forceinline__ void record_stopping_time(const PP &pp, double Ts)
 {
-  if (Ts >= 0.0) atomicMin((long long *)&pp.dc->min_ts, __double_as_longlong(Ts));
+  const unsigned m = __activemask();
+  const unsigned long long v = (Ts >= 0.0) ? (unsigned long long)__double_as_longlong(Ts) : ~0ull;
+  const unsigned hi = (unsigned)(v >> 32), lo = (unsigned)v;
+  const unsigned mh = __reduce_min_sync(m, hi);
+  const unsigned ml = __reduce_min_sync(m, (hi == mh) ? lo : 0xffffffffu);
+  const unsigned long long w = ((unsigned long long)mh << 32) | ml;
+  if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && w != ~0ull) atomicMin((long long *)&pp.dc->min_ts, (long long)w);
 }
 
 // ----------------------------------- 4. kicks, interpolation, velocities
