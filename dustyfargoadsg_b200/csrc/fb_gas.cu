@@ -647,8 +647,9 @@ static __device__ __forceinline__ double pressure_at(const KP &k, size_t l)
 }
 
 // SubStep1 (SourceEuler.c:765-1009) without dust: pressure, potential and
-// curvature terms into VradInt (i >= 1) and VthetaInt (all rings).
-__global__ void __launch_bounds__(FB_BS2) k_substep1(KP k)
+// curvature terms into VradInt (i >= 1) and VthetaInt (all rings).  At most
+// 64 registers, so that four 256-thread CTAs share an SM (68 would allow three).
+__global__ void __launch_bounds__(FB_BS2, 4) k_substep1(KP k)
 {
   fb_grid_dependency();
   const int ns = k.ns;
