@@ -842,7 +842,9 @@ static __device__ __forceinline__ double q_t(const KP &k, size_t l, size_t ljp)
   return (dv < 0.0) ? FB_CVNR * FB_CVNR * k.rho[l] * dv * dv : 0.0;
 }
 
-__global__ void __launch_bounds__(FB_BS2) k_substep2(KP k)
+// At most 48 registers: five 256-thread CTAs per SM (SubStep2 20.6 -> 19.0 us;
+// the same cap made the stress kernels and SubStep3 slower).
+__global__ void __launch_bounds__(FB_BS2, 5) k_substep2(KP k)
 {
   fb_grid_dependency();
   const int ns = k.ns, nr = k.nr;
