@@ -1771,18 +1771,26 @@ __global__ void __launch_bounds__(FB_BS2) k_transport_vr(KP k)
 // chunk plus the two halo rings it rereads, so a grid one CTA past a wave
 // costs a whole extra round; these chunks avoid that.  Returns how many
 // were written to out (increasing r, decreasing chunk).
-int fb_rad_chunks_balanced(const KP &k, int tx, int *out, int max)
+// CTAs of the radial pass (2 tx threads) the GPU holds at once, 0 if unknown.
+static int rad_resident_ctas(int energy, int tx)
 {
   int dev = 0, sms = 0, per = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
     return 0;
-  const cudaError_t e = k.energy ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<6>, 2 * tx, 0)
-                                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<5>, 2 * tx, 0);
+  const cudaError_t e = energy ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<6>, 2 * tx, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<5>, 2 * tx, 0);
   if (e != cudaSuccess || per < 1 || sms < 1) {
     cudaGetLastError();
     return 0;
   }
-  const int bx = (k.ns + tx - 1) / tx, slots = per * sms;
+  return per * sms;
+}
+
+int fb_rad_chunks_balanced(const KP &k, int tx, int *out, int max)
+{
+  const int slots = rad_resident_ctas(k.energy, tx);
+  if (slots < 1) return 0;
+  const int bx = (k.ns + tx - 1) / tx;
   int n = 0;
   for (int r = 1; r <= 6 && n < max; r++) {
     const int rows = (r * slots) / bx;  // ring chunks that r rounds hold
@@ -1804,12 +1812,7 @@ int fb_rad_chunk_auto(const KP &k)
   const int n = fb_rad_chunks_balanced(k, tx, ch, 6);
   if (n == 0) return 16;
   const int bx = (k.ns + tx - 1) / tx;
-  int dev = 0, sms = 148, per = 1;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (k.energy) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<6>, 2 * tx, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_transport_radial<5>, 2 * tx, 0);
-  const long slots = (long)(per > 0 ? per : 1) * sms;
+  const long slots = rad_resident_ctas(k.energy, tx);
   int best = ch[0];
   long bestcost = -1;
   for (int q = 0; q < n; q++) {
