@@ -75,11 +75,17 @@ static __device__ __forceinline__ double pow15(double x) { return x * sqrt(x); }
 static __device__ __forceinline__ double powm2(double x) { return 1.0 / (x * x); }
 static __device__ __forceinline__ double powm3(double x) { return 1.0 / (x * x * x); }
 
-static __device__ __forceinline__ double tsc_weight(double d, double delta)
+// The triangular-shaped-cloud weight at distance d for a cell of width
+// delta; rdelta = 1/delta rounded, so that each quotient by delta is the
+// correctly rounded one through fb_quot (no division).
+static __device__ __forceinline__ double tsc_weight(double d, double delta, double rdelta)
 {
   double w = 0.0;
-  if (d < 0.5 * delta) w = 0.75 - d * d / delta / delta;
-  if ((d >= 0.5 * delta) && (d <= 1.5 * delta)) w = 0.5 * (1.5 - d / delta) * (1.5 - d / delta);
+  if (d < 0.5 * delta) w = 0.75 - fb_quot(fb_quot(d * d, delta, rdelta), delta, rdelta);
+  if ((d >= 0.5 * delta) && (d <= 1.5 * delta)) {
+    const double q = fb_quot(d, delta, rdelta);
+    w = 0.5 * (1.5 - q) * (1.5 - q);
+  }
   if (d > 1.5 * delta) w = 0.0;
   return w;
 }
@@ -411,6 +417,7 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
   if (jp == ns) jp = 0;
   jp = min(max(jp, 0), ns - 1);
   const double delta_phi = pp.delta_phi, delta_r = pp.delta_r;
+  const double rdelta_phi = 1.0 / delta_phi, rdelta_r = 1.0 / delta_r;
   const int want_sg = k.self_gravity && pp.feel_sg;
   double vrg = 0.0, rgp = 0.0, rind = 0.0, rsg = 0.0;
   double vtg = 0.0, agp = 0.0, aind = 0.0, asg = 0.0;
@@ -424,8 +431,10 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
   for (int t = 0; t < 3; t++) {
     const int i = ip - 1 + t;
     if (i >= 0 && i <= nr - 1) {
-      wr_inf[t] = tsc_weight(pp.log_grid ? fabs(log(rp / k.rinf[i])) : fabs(rp - k.rinf[i]), delta_r);
-      wr_med[t] = tsc_weight(pp.log_grid ? fabs(log(rp / k.rmed[i])) : fabs(rp - k.rmed[i]), delta_r);
+      wr_inf[t] = tsc_weight(pp.log_grid ? fabs(log(fb_quot(rp, k.rinf[i], k.invrinf[i]))) : fabs(rp - k.rinf[i]),
+                             delta_r, rdelta_r);
+      wr_med[t] = tsc_weight(pp.log_grid ? fabs(log(fb_quot(rp, k.rmed[i], k.invrmed[i]))) : fabs(rp - k.rmed[i]),
+                             delta_r, rdelta_r);
     } else {
       wr_inf[t] = wr_med[t] = 0.0;
     }
@@ -434,7 +443,7 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
     if (j >= 0 && j < ns) { jc[t] = j; az = pp.azimuth[j]; }
     else if (j < 0) { jc[t] = j + ns; az = pp.azimuth[0] + j * delta_phi; }
     else { jc[t] = j - ns; az = pp.azimuth[ns - 1] + (j + 1 - ns) * delta_phi; }
-    wt_c[t] = tsc_weight(fabs(tp - az), delta_phi);
+    wt_c[t] = tsc_weight(fabs(tp - az), delta_phi, rdelta_phi);
   }
   {
     const int myjp = (tp > pp.azimuth[jp]) ? jp + 1 : jp;
@@ -445,7 +454,7 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
       if (j >= 0 && j < ns) { ji[t] = j; az = pp.aziinf[j]; }
       else if (j < 0) { ji[t] = j + ns; az = pp.aziinf[0] + j * delta_phi; }
       else { ji[t] = j - ns; az = pp.aziinf[ns - 1] + (j + 1 - ns) * delta_phi; }
-      wt_i[t] = tsc_weight(fabs(tp - az), delta_phi);
+      wt_i[t] = tsc_weight(fabs(tp - az), delta_phi, rdelta_phi);
     }
   }
   // ---- 2a) vrad-staggered values: (Rinf[i], Azimuth[j]) (Dsys.c:397-487)
