@@ -2,7 +2,7 @@
 interpolation, UpdateDustVelocities) inside whole AlgoGas DTs, against the
 CPU oracle run on the same seed.
 
-Tolerances: particle positions and velocities within
+Tolerances (FP64 parity bar of this path): particle positions and velocities within
 1e-10 (scale-relative, max|gpu - ref| / max|ref|), gas fields within 1e-11,
 and the drand48 stream of the turbulent kicks at exactly the reference's
 position after every DT (the GPU draws the same Gaussian deviates, in

@@ -1,7 +1,7 @@
 """GPU parity of the gas step against the CPU oracle (the reference's own
 sequential build run on the same seeded inputs).
 
-Tolerances: fields within 1e-11 relative after one DT;
+Tolerances (FP64 parity bar of this path): fields within 1e-11 relative after one DT;
 single stages within 1e-12.  Errors are scale-relative:
 max|gpu - ref| / max|ref| per field.
 """
