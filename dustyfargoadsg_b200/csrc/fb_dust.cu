@@ -297,36 +297,48 @@ __global__ void __launch_bounds__(D_BS) k_rng_count(PP pp)
   }
 }
 
-__global__ void __launch_bounds__(SCAN_BS) k_rng_top(KP k, PP pp, int nb)
-{
-  fb_grid_dependency();
-  const int total = scan_top(pp.cand_bsum, nb);
-  if (threadIdx.x == 0) {
-    fb_dust_ctl *d = pp.dc;
-    if (d->npairs > total) {
-      // never silently wrong: the step stops with an error status
-      d->err = 1;
-      d->npairs = total;
-      k.ctl->status = FB_ERR_INVALID;
-    }
-  }
-}
-
-// Accepted candidate number g (in stream order) becomes pair g.
-__global__ void __launch_bounds__(D_BS) k_rng_scatter(PP pp)
+// Accepted candidate number g (in stream order) becomes pair g.  The
+// blocks' counts are summed here: only the blocks below the candidate limit
+// have any (a handful), and each of those adds the counts before it; block 0
+// also checks that the candidates cover the pairs needed -- never silently
+// wrong: the step stops with an error status.
+__global__ void __launch_bounds__(D_BS) k_rng_scatter(KP k, PP pp, int nb)
 {
   fb_grid_dependency();
   __shared__ int wc[D_BS / 32];
-  const long long c = (long long)blockIdx.x * D_BS + threadIdx.x;
-  const int npairs = pp.dc->npairs;
-  const int acc = (npairs > 0 && c < pp.ncand) ? pp.cand_flag[c] : 0;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int npairs = pp.dc->npairs;
+  // sum of the counts of blocks [0, upto): every thread gets it
+  auto block_count = [&](int upto) -> int {
+    int v = 0;
+    for (int q = threadIdx.x; q < upto; q += D_BS) v += pp.cand_bsum[q];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    __syncthreads();
+    if (lane == 0) wc[w] = v;
+    __syncthreads();
+    int t = 0;
+    for (int q = 0; q < D_BS / 32; q++) t += wc[q];
+    __syncthreads();
+    return t;
+  };
+  if (blockIdx.x == 0) {
+    const int total = block_count(nb);
+    if (threadIdx.x == 0 && npairs > total) {
+      pp.dc->err = 1;
+      k.ctl->status = FB_ERR_INVALID;
+    }
+  }
+  const long long c0 = (long long)blockIdx.x * D_BS;
+  if (npairs <= 0 || c0 >= candidate_limit(pp, npairs)) return;  // no accepted candidate here
+  const int prefix = block_count(blockIdx.x);
+  const long long c = c0 + threadIdx.x;
+  const int acc = (c < pp.ncand) ? pp.cand_flag[c] : 0;
   const unsigned b = __ballot_sync(0xffffffffu, acc);
   if (lane == 0) wc[w] = __popc(b);
   __syncthreads();
   int off = 0;
   for (int q = 0; q < w; q++) off += wc[q];
-  const int g = pp.cand_bsum[blockIdx.x] + off + __popc(b & ((1u << lane) - 1u));
+  const int g = prefix + off + __popc(b & ((1u << lane) - 1u));
   if (acc && g < npairs) {
     double u1, u2, ww;
     candidate(pp.dc->x, c, &u1, &u2, &ww);
@@ -707,7 +719,7 @@ void fb_launch_dust_to_reference_order(const PP &pp, const double *src, double *
 }
 
 // ---------------------------------------------------------- launchers
-int fb_dust_launches(const PP &pp) { return pp.feel_turb ? 8 : 2; }
+int fb_dust_launches(const PP &pp) { return pp.feel_turb ? 7 : 2; }
 
 void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s, cudaEvent_t planets_done)
 {
@@ -719,8 +731,7 @@ void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s, cudaEvent
     fb_launch(k_kick_top, 1, SCAN_BS, 0, s, pp, nsb);
     const int ncb = (pp.ncand + D_BS - 1) / D_BS;
     fb_launch(k_rng_count, ncb, D_BS, 0, s, pp);
-    fb_launch(k_rng_top, 1, SCAN_BS, 0, s, k, pp, ncb);
-    fb_launch(k_rng_scatter, ncb, D_BS, 0, s, pp);
+    fb_launch(k_rng_scatter, ncb, D_BS, 0, s, k, pp, ncb);
   }
   if (planets_done) cudaStreamWaitEvent(s, planets_done, 0);  // positions after the planets' step
   fb_launch(k_dust_update, nb, D_BS, 0, s, k, pp, 0);
