@@ -1928,24 +1928,41 @@ void fb_launch_boundary_only(const KP &k, cudaStream_t s)
 __global__ void __launch_bounds__(FB_BS) k_damping(KP k, double dtov)
 {
   fb_grid_dependency();
-  __shared__ double sh[32];
+  __shared__ double shm[4 * 32];
   const int i = k.damp_rings[blockIdx.x], ns = k.ns, nr = k.nr;
   const size_t base = (size_t)i * ns;
   const double step = dt_of(k, dtov);
   const double lambda = k.damp_lam[i] * step / k.damp_tau[i];
   double vrad0, vtheta0, dens0, energ0;
   if (k.damp_axi) {
-    double a = 0.0, b = 0.0, c = 0.0, d = 0.0;
-    for (int j = threadIdx.x; j < ns; j += FB_BS) {
-      a += k.vr[base + j];
-      b += k.vt[base + j];
-      c += k.rho[base + j];
-      d += k.e[base + j];
+    // the four ring means: each thread's partial sums in azimuth order (a
+    // batch's loads in flight together), then one four-value tree, the same
+    // order as four single sums
+    double m[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int j0 = threadIdx.x; j0 < ns; j0 += RING_U * FB_BS) {
+      double v[RING_U][4];
+#pragma unroll
+      for (int u = 0; u < RING_U; u++) {
+        const int j = j0 + u * FB_BS;
+        if (j < ns) {
+          v[u][0] = k.vr[base + j];
+          v[u][1] = k.vt[base + j];
+          v[u][2] = k.rho[base + j];
+          v[u][3] = k.e[base + j];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < RING_U; u++)
+        if (j0 + u * FB_BS < ns) {
+#pragma unroll
+          for (int q = 0; q < 4; q++) m[q] += v[u][q];
+        }
     }
-    vrad0 = block_sum<FB_BS>(a, sh) / (double)ns;
-    vtheta0 = block_sum<FB_BS>(b, sh) / (double)ns;
-    dens0 = block_sum<FB_BS>(c, sh) / (double)ns;
-    energ0 = block_sum<FB_BS>(d, sh) / (double)ns;
+    block_sums<4>(m, shm);
+    vrad0 = m[0] / (double)ns;
+    vtheta0 = m[1] / (double)ns;
+    dens0 = m[2] / (double)ns;
+    energ0 = m[3] / (double)ns;
   } else {
     vtheta0 = k.vthetamed[i] - k.rmed[i] * k.omega_frame;
     vrad0 = k.vradmed[i];
