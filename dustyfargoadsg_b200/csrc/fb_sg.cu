@@ -600,25 +600,6 @@ static __device__ __forceinline__ void dft16(double2 *v)
 }
 
 
-// w[r] = w^r (r = 1..15), w = exp(-/+ 2 pi i j / S), from the table rows
-// r = 1, 2, 4, 8 (w^r at tw[r stride + j]): four loads instead of fifteen,
-// the other powers products at most two deep, within a few ulp.
-template <int INV>
-static __device__ __forceinline__ void pow16(double2 *w, const double2 *__restrict__ tw, int stride, int j)
-{
-  w[1] = tw[stride + j];
-  w[2] = tw[2 * stride + j];
-  w[4] = tw[4 * stride + j];
-  w[8] = tw[8 * stride + j];
-  if (INV) { w[1].y = -w[1].y; w[2].y = -w[2].y; w[4].y = -w[4].y; w[8].y = -w[8].y; }
-  w[3] = cmul(w[1], w[2]);
-  w[5] = cmul(w[4], w[1]);
-  w[6] = cmul(w[4], w[2]);
-  w[7] = cmul(w[4], w[3]);
-#pragma unroll
-  for (int r = 9; r < 16; r++) w[r] = cmul(w[8], w[r - 8]);
-}
-
 // 8-point DFT of v[0..7] in place, natural order (radix 2 x 4).
 template <int INV>
 static __device__ __forceinline__ void dft8(double2 *v)
