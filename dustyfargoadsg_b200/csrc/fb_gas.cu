@@ -48,31 +48,6 @@ static __device__ double block_sum(double v, double *sh)
   return r;
 }
 
-template <int BS>
-static __device__ double block_min(double v, double *sh)
-{
-  for (int o = 16; o > 0; o >>= 1) {
-    double u = __shfl_down_sync(0xffffffffu, v, o);
-    v = (u < v) ? u : v;
-  }
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  __syncthreads();
-  if (lane == 0) sh[w] = v;
-  __syncthreads();
-  if (w == 0) {
-    v = (lane < BS / 32) ? sh[lane] : 1e300;
-    for (int o = 16; o > 0; o >>= 1) {
-      double u = __shfl_down_sync(0xffffffffu, v, o);
-      v = (u < v) ? u : v;
-    }
-    if (lane == 0) sh[0] = v;
-  }
-  __syncthreads();
-  double r = sh[0];
-  __syncthreads();
-  return r;
-}
-
 static __device__ __forceinline__ double nu_ring(const KP &k, int i)
 {
   // FViscosity(Rmed[i]) (Viscosity.c:23-69) for the supported laws:
