@@ -119,13 +119,11 @@ static __device__ void rk5(const double *q0, double dt, const double *masses, do
 // azimuthal mean Vmoy[i] and the smallest per-cell limit of the ring; the
 // controller takes the minimum over rings, adds the shear limit and returns
 // ceil(deltaT/newdt).  DetectCrash (SourceEuler.c:51-69) rides along.
-// One CTA per ring, CFL_E cells per thread, one pass over the ring: the
-// cells' values stay in registers between the ring sums (the mean azimuthal
-// velocity the CFL limits need) and the limits themselves.
-// The cells' values kept between the ring sums and the CFL limits go
-// through shared memory (3 nsec doubles), so a ring's CTA of up to 256
-// threads fits in 64 registers a thread: four CTAs share an SM and a
-// 512-ring grid runs in one wave.
+// One pass over the ring: the values each cell needs after the ring sums
+// (the mean azimuthal velocity the CFL limits need) are kept in shared
+// memory (3 nsec doubles), so a ring's CTA of up to 256 threads fits in 64
+// registers a thread: four CTAs share an SM and a 512-ring grid runs in one
+// wave.
 #define CFL_BS 256
 static inline int cfl_threads(int ns)
 {
