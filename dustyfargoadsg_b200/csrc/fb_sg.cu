@@ -5,16 +5,20 @@
 // St = Sr r/r0 with the kernels Kr, Kt on a (2 Nr) x Ns periodic grid (the
 // radial direction zero-padded), through unnormalised FFTW transforms:
 //     A = IFFT2( -G FFT2(K) . FFT2(S) ),   normalised by rstep tstep/(2Nr Ns).
-// Here the transforms are our own Stockham mixed-radix FFTs (radix 16 in
-// registers first, then 4, 2, 3, 5; lines padded by one slot per 16 in
-// shared memory against bank conflicts; per-pass twiddle tables read with
-// consecutive entries per warp), one CTA per 1-D transform or pair:
+// Here the transforms are our own, one CTA per 1-D transform or pair:
 //   1. sg_rows_fwd : per ring i < Nr, one complex FFT of z = Sr + i St along
-//      phi, split into the two half spectra (rows >= Nr are zero, so they
-//      are never transformed);
-//   2. sg_cols     : per azimuthal wavenumber k and per quantity, forward FFT
-//      along the 2 Nr radial points, product with the kernel spectrum,
-//      inverse FFT; only the Nr physical rows are written back;
+//      phi (Stockham, radix 16 in registers first, then 4, 2, 6, 3, 5; lines
+//      padded by one slot per 16 in shared memory against bank conflicts;
+//      per-pass twiddle tables read with consecutive entries per warp),
+//      split into the two half spectra (rows >= Nr are zero, so they are
+//      never transformed);
+//   2. sg_cols_dif : per pair of azimuthal wavenumbers k and per quantity,
+//      the 2 Nr radial points transformed in place (decimation in frequency
+//      forward, in time backward, so the spectrum stays in one permuted
+//      order in which the kernel spectrum is also stored), product with the
+//      kernel spectrum, backward transform; only the Nr physical rows are
+//      computed in the last pass and written back (sg_cols, Stockham, for
+//      column lengths other than powers of two up to 1024);
 //   3. sg_rows_inv : per ring, one inverse complex FFT of Wr + i Wt (both
 //      Hermitian), whose real and imaginary parts are the two accelerations,
 //      with the normalisation and self-force term of sgacc.c:138-161 fused;
