@@ -515,8 +515,6 @@ static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
   if (!k.indirect_term) { c->ind_x = 0.0; c->ind_y = 0.0; }
   // AdvanceSystemRK5 and RotatePsys follow in k_planets, which runs beside
   // the next kernels of the substep
-  // LostMass of the previous substep's ring-0 radial mass fluxes
-  // (VanLeerRadial's LostByDisk, TransportEuler.c:213-216).
   c->physical_time += dt;  // SourceEuler.c:714 (no kernel in this substep reads it)
   c->substeps += 1;
   c->done = (c->dtemp < 0.999999999 * c->DT) ? 0 : 1;
