@@ -50,6 +50,7 @@ WORKLOADS = {
 }
 BATCH_DISCS, BATCH_SEED = 64, 2  # the batched sweep: 64 discs drawn from seed 2
 DEFAULT_WORKLOAD = "adiabatic_sg_512x1536"
+CONFIG_DIR = os.path.join(REPO, "dustyfargoadsg_b200", "configs")
 FALLBACK_HBM_GBS = 6650.0
 
 # Algorithmic bytes per cell of each stage (distinct fields read + written,
@@ -61,6 +62,18 @@ STAGE_BYTES = {
     "transport_radial": (64, 80), "transport_azimuthal": (80, 96),
     "transport_vr_boundary": (40, 40),
 }
+
+
+def par_grid(path):
+    """(NRAD, NSEC) of a .par file, read with the reference's rules
+    (case-insensitive keys, '#' comments; src/Interpret.c:82-130)."""
+    grid = {"NRAD": 64, "NSEC": 64}  # the reference's defaults, src/var.c
+    with open(path) as f:
+        for line in f:
+            tok = line.replace("\t", " ").split()
+            if len(tok) >= 2 and not tok[0].startswith("#") and tok[0].upper() in grid:
+                grid[tok[0].upper()] = int(float(tok[1]))
+    return grid["NRAD"], grid["NSEC"]
 
 
 def _env_int(name, dflt):
@@ -227,19 +240,23 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload is None:
+        args.workload = DEFAULT_WORKLOAD
+    wl = dict(WORKLOADS[args.workload])
+    par_path = os.path.join(CONFIG_DIR, wl["par"])
+
+    if args.impl == "reference":
+        # the reference arm runs the reference's own build only: the package
+        # (and its shared library) is not imported in this process
+        grid = par_grid(par_path)
+        wl["nrad"], wl["nsec"] = grid
+        run_reference(args, par_path, wl, grid[0] * grid[1])
+        return
 
     import dustyfargoadsg_b200 as fb
-    if args.workload is None:
-        args.workload = DEFAULT_WORKLOAD if _supported(fb, DEFAULT_WORKLOAD) else "iso_128x384"
-    wl = dict(WORKLOADS[args.workload])
-    par_path = os.path.join(fb.CONFIG_DIR, wl["par"])
     p = fb.read_par(par_path)
     wl["nrad"], wl["nsec"] = p.nrad, p.nsec
     cells = p.nrad * p.nsec
-
-    if args.impl == "reference":
-        run_reference(args, par_path, wl, cells)
-        return
 
     import numpy as np
     import torch
@@ -435,23 +452,6 @@ def measure_batch(fb, table, flush, warmup=2, steps=3):
     finally:
         for d in discs:
             d.close()
-
-
-def _supported(fb, name):
-    try:
-        p = fb.read_par(os.path.join(fb.CONFIG_DIR, WORKLOADS[name]["par"]))
-    except Exception:
-        return False
-    return p.unsupported == 0 and os.environ.get("FB_BENCH_SG", "1") == "1" and _sg_built(fb)
-
-
-def _sg_built(fb):
-    # self-gravity is available once fb_create accepts it
-    try:
-        lib = fb.load()
-        return hasattr(lib, "fb_sg_ready") and lib.fb_sg_ready() == 1
-    except Exception:
-        return False
 
 
 if __name__ == "__main__":

@@ -188,10 +188,31 @@ class Disc:
         check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx)
 
     def step(self):
-        """One DT (AlgoGas) on the device; returns the step report."""
+        """One DT (AlgoGas) on the device; returns the step report.
+
+        A DT in which the reference's crash test fired (negative energy,
+        SourceEuler.c:545-566) completes like the reference's and is not an
+        error here: rep.status is then FB_ERR_NEGATIVE and rep.crashes,
+        rep.crash_substeps and rep.crash_time say what happened
+        (crash_state() gives the state at the first crash)."""
         rep = FbStepReport()
-        check(self.lib.fb_algogas(self.ctx, C.byref(rep)), "fb_algogas", self.ctx)
+        rc = self.lib.fb_algogas(self.ctx, C.byref(rep))
+        if rc != _ffi.FB_ERR_NEGATIVE:
+            check(rc, "fb_algogas", self.ctx)
         return rep
+
+    def crash_state(self):
+        """The state at the first crash (rings 0..nrad-1), what the reference
+        writes as gas*999.dat: {dens, vrad, vtheta, energy, crash_time}."""
+        n = self.nr * self.ns
+        out = {k: np.zeros(n) for k in ("dens", "vrad", "vtheta", "energy")}
+        st = FbState()
+        for k, a in out.items():
+            setattr(st, k, _ptr(a))
+        t = C.c_double()
+        check(self.lib.fb_download_crash(self.ctx, C.byref(st), C.byref(t)), "fb_download_crash", self.ctx)
+        out["crash_time"] = t.value
+        return out
 
     def stage(self, stage, dt):
         check(self.lib.fb_stage(self.ctx, int(stage), float(dt)), "fb_stage", self.ctx)
@@ -275,7 +296,9 @@ class Batch:
 
     def step(self):
         """One DT of every disc; returns the per-disc step reports."""
-        check(self.lib.fb_batch_algogas(self.b, self.reps), "fb_batch_algogas")
+        rc = self.lib.fb_batch_algogas(self.b, self.reps)
+        if rc != _ffi.FB_ERR_NEGATIVE:  # a crash is reported per disc, as in Disc.step
+            check(rc, "fb_batch_algogas")
         return list(self.reps)
 
     def close(self):

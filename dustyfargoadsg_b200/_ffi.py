@@ -9,6 +9,7 @@ import os
 
 FB_MAX_PLANETS = 16
 FB_OK = 0
+FB_ERR_NEGATIVE = -6  # the crash test fired during a DT that still completed
 FB_ERR = {
     -1: "FB_ERR_INVALID", -2: "FB_ERR_UNSUPPORTED", -3: "FB_ERR_CUDA", -4: "FB_ERR_NOMEM",
     -5: "FB_ERR_NAN", -6: "FB_ERR_NEGATIVE", -7: "FB_ERR_SUBSTEPS", -8: "FB_ERR_TIMEOUT",
@@ -98,7 +99,8 @@ class FbTuning(C.Structure):
 class FbStepReport(C.Structure):
     _fields_ = [
         ("substeps", _I), ("status", _I), ("physical_time", _D), ("mindt", _D), ("maxdt", _D),
-        ("lost_mass", _D), ("gpu_ms", _D),
+        ("lost_mass", _D), ("gpu_ms", _D), ("crashes", _I), ("crash_substeps", _I),
+        ("neg_density_substeps", _I), ("crash_time", _D),
     ]
 
 
@@ -108,7 +110,7 @@ LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libfargo_b2
 EXPORTS = (
     "fb_params_default", "fb_params_read_par", "fb_unsupported_name", "fb_planets_read_cfg",
     "fb_init_state", "fb_create", "fb_destroy", "fb_upload", "fb_algogas", "fb_download",
-    "fb_download_derived", "fb_diagnostics", "fb_strerror", "fb_last_error", "fb_stage",
+    "fb_download_derived", "fb_download_crash", "fb_diagnostics", "fb_strerror", "fb_last_error", "fb_stage",
     "fb_build_info", "fb_struct_size", "fb_kernel_launches", "fb_profile", "fb_profile_read",
     "fb_select_device", "fb_transport_noalloc", "fb_noalloc_last_error", "fb_init_dust",
     "fb_dust_upload", "fb_dust_download", "fb_vortensity", "fb_batch_create", "fb_batch_algogas",

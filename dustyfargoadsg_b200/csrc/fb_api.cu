@@ -278,6 +278,10 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
     if (!*fields[f]) { fb_destroy(ctx); return FB_ERR_NOMEM; }
   }
   k.lost0 = dalloc(ctx, ns);
+  if (p->energy_equation) {  // only the energy test can crash (DetectCrash as AlgoGas uses it)
+    k.crash_snap = dalloc(ctx, (size_t)4 * nr * ns);
+    if (!k.crash_snap) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+  }
   // 1-D tables (host, glibc libm; see fb_host.c)
   const fb_geom &g = ctx->g;
   std::vector<double> cs_ring(nr), p15(nr), dxrad(nr), dxth(nr), invdxth(nr), dxth_cfl(nr), mindx2(nr);
@@ -737,6 +741,15 @@ extern "C" int fb_profile_read(const fb_ctx *ctx, int idx, const char **name, do
   return FB_NSTAGE;
 }
 
+// The DetectCrash bookkeeping of one DT (SourceEuler.c:545-566).
+static void report_crash(const fb_ctl *c, fb_step_report *rep)
+{
+  rep->crashes = c->crashes;
+  rep->crash_substeps = c->crash_substeps;
+  rep->neg_density_substeps = c->neg_dens_substeps;
+  rep->crash_time = c->crashes > 0 ? c->crash_time : 0.0;
+}
+
 extern "C" int fb_algogas(fb_ctx *ctx, fb_step_report *rep)
 {
   if (!ctx) return FB_ERR_INVALID;
@@ -780,8 +793,17 @@ extern "C" int fb_algogas(fb_ctx *ctx, fb_step_report *rep)
     rep->maxdt = c->maxdt;
     rep->lost_mass = c->lost_mass;
     rep->gpu_ms = ms;
+    report_crash(c, rep);
   }
-  if (status) set_err(ctx, "AlgoGas stopped: %s", fb_strerror(status));
+  if (status) {
+    set_err(ctx, "AlgoGas stopped: %s", fb_strerror(status));
+  } else if (c->crash_substeps > 0) {
+    // the DT ran to its end, as the reference's does after a crash
+    set_err(ctx, "DetectCrash: negative energy in %d substep(s) of this DT; first crash at time %.12g",
+            c->crash_substeps, c->crash_time);
+    status = FB_ERR_NEGATIVE;
+    if (rep) rep->status = status;
+  }
   return status;
 }
 
@@ -816,6 +838,24 @@ extern "C" int fb_download(fb_ctx *ctx, fb_state *s, unsigned mask)
     s->planets.vx[q] = c->pvx[q];
     s->planets.vy[q] = c->pvy[q];
   }
+  return FB_OK;
+}
+
+extern "C" int fb_download_crash(fb_ctx *ctx, fb_state *s, double *crash_time)
+{
+  if (!ctx || !s) return FB_ERR_INVALID;
+  const fb_ctl *c = ctx->h_ctl;
+  if (!ctx->k.crash_snap || !c->crash_snapped) {
+    set_err(ctx, "no crash has been detected");
+    return FB_ERR_STATE;
+  }
+  const size_t n = (size_t)ctx->nr * ctx->ns;
+  double *dst[4] = {s->dens, s->vrad, s->vtheta, s->energy};
+  for (int q = 0; q < 4; q++)
+    if (dst[q]) CK(cudaMemcpyAsync(dst[q], ctx->k.crash_snap + q * n, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                   ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  if (crash_time) *crash_time = c->crash_time;
   return FB_OK;
 }
 
@@ -1162,6 +1202,13 @@ extern "C" int fb_batch_algogas(fb_batch *b, fb_step_report *reps)
       reps[d].maxdt = h->maxdt;
       reps[d].lost_mass = h->lost_mass;
       reps[d].gpu_ms = ms;  // the whole batch
+      report_crash(h, &reps[d]);
+    }
+    if (!h->status && h->crash_substeps > 0) {  // the disc's DT ran to its end (see fb_algogas)
+      set_err(c, "DetectCrash: negative energy in %d substep(s) of this DT; first crash at time %.12g",
+              h->crash_substeps, h->crash_time);
+      if (reps) reps[d].status = FB_ERR_NEGATIVE;
+      if (!status) status = FB_ERR_NEGATIVE;
     }
   }
   return status;

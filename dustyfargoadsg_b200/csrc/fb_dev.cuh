@@ -23,7 +23,18 @@ struct fb_ctl {
   double ind_x, ind_y;                       // IndirectTerm (Pframeforce.c:25)
   double bary_x[3], bary_y[3];               // stardiscbarycenter_{x,y}
   double mdisc;
-  int substeps, done, status, crash_count, nonfinite;
+  int substeps, done, status, nonfinite;
+  // DetectCrash (SourceEuler.c:51-69) as AlgoGas uses it (:545-566): the
+  // CFL kernel's CTAs raise the flags for the state at the start of the
+  // substep, the controller consumes them.  Only the energy test decides a
+  // crash there (its result overwrites the density test's, :546-548).
+  int neg_dens_flag, neg_energy_flag;
+  int crashes;            // AlreadyCrashed: crashed substeps since creation
+  int crash_substeps;     // crashed substeps of this DT
+  int neg_dens_substeps;  // substeps of this DT that began with a negative density
+  int crash_snap_now;     // this substep's starting state is the first crash's
+  int crash_snapped;      // the first crash's state is held (fb_download_crash)
+  double crash_time;      // timeCRASH (SourceEuler.c:551)
   int np;
   unsigned int cfl_done;                     // CTAs of the CFL kernel finished this substep
   double pm[FB_MAX_PLANETS], px[FB_MAX_PLANETS], py[FB_MAX_PLANETS];
@@ -47,6 +58,7 @@ struct KP {
   double *divv, *trr, *tpp, *trp, *vischeat;
   double *q[6];        // transport: RadMomP, RadMomM, ThetaMomP, ThetaMomM, Energy, Rho
   double *rho_t;       // density after transport, before floors
+  double *crash_snap;  // 4 x nr*ns: density, vrad, vtheta, energy of the first crash
   double *lost0;       // ns: ring-0 radial mass fluxes of the last substep
   double *sg_accr, *sg_acct;  // SG accelerations (nf)
   // per-ring tables (nr or nr+1 entries)
@@ -200,7 +212,8 @@ void fb_launch_damping(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_diag(const KP &k, double *out2, cudaStream_t s);
 void fb_launch_derived(const KP &k, int which, double *out, cudaStream_t s);
 void fb_launch_boundary_only(const KP &k, cudaStream_t s);
-int  fb_gas_prepare(int ns, int energy);  // kernel attributes (shared memory)
+int  fb_gas_prepare(int ns, int energy);  // kernel attributes (shared memory); loads the azimuthal kernels
+int  fb_transport_preload(void);          // loads the radial and vr transport kernels
 // launch-shape candidates the tuner may try (fb_gas.cu)
 int  fb_azi_E_valid(int ns, int energy, int E);   // 1 if E cells/thread fit this ring
 int  fb_azi_E_auto(int ns);

@@ -375,6 +375,10 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
   fb_grid_dependency();
   const int q = blockIdx.x * D_BS + threadIdx.x;  // storage slot
   if (q >= pp.n) return;
+  // a candidate shortfall (k_rng_scatter) leaves pairs unset: the substep's
+  // particles are not advanced, the step stops with an error status and
+  // fb_dust_download refuses the state from then on
+  if (mode == 0 && pp.dc->err) return;
   const int qr = (mode == 0) ? pp.orig[q] : 0;  // the reference's index: kick flag and rank
   const int ns = k.ns, nr = k.nr;
   const double rinf0 = k.rinf[0], rsupl = k.rsup[nr - 1];
@@ -588,6 +592,11 @@ __global__ void k_dust_finish(PP pp)
   fb_grid_dependency();
   fb_dust_ctl *d = pp.dc;
   const long long G = d->kicks, K = d->K;
+  if (d->err) {  // the stream position is unknown after a shortfall: leave it
+    d->K = 0;
+    d->npairs = 0;
+    return;
+  }
   if (d->npairs > 0) d->x = lcg_skip(d->x, (unsigned long long)(2 * (d->c_last + 1)));
   if (K > 0 && ((G + K) & 1ll)) {
     // an odd number of calls in total: each generator keeps the second

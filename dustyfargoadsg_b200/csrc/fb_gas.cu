@@ -154,15 +154,15 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
   // through one reciprocal per ring
   const double dxmin = min2(dxrad, dxtheta);
   const double rdxmin = 1.0 / dxmin, rdxrad = 1.0 / dxrad, rdxtheta = 1.0 / dxtheta;
-  int neg = 0, bad = 0;
+  int negd = 0, nege = 0, bad = 0;
   for (int j = tid; j < ns; j += T) {
     const double vtj = vt[j], vrj = vr[j], dens = rho[j];
     v[0] += vtj;
-    if (dens < 0.0) neg = 1;
+    if (dens < 0.0) negd = 1;
     if (!isfinite(dens) || !isfinite(vtj) || !isfinite(vrj)) bad = 1;
     if (k.energy) {
       const double en = k.e[base + j];
-      if (en < 0.0) neg = 1;
+      if (en < 0.0) nege = 1;
       if (!isfinite(en)) bad = 1;
     }
     const double xc = rmi * k.cosaz[j];
@@ -200,10 +200,12 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
     double *pp = k.partials + (size_t)i * 5;  // summed by the controller in ring order
     for (int q = 0; q < 5; q++) pp[q] = v[1 + q];
   }
-  neg = __syncthreads_or(neg);
+  negd = __syncthreads_or(negd);
+  nege = __syncthreads_or(nege);
   bad = __syncthreads_or(bad);
   if (tid == 0) {
-    if (neg) atomicAdd(&k.ctl->crash_count, 1);
+    if (negd) atomicOr(&k.ctl->neg_dens_flag, 1);
+    if (nege) atomicOr(&k.ctl->neg_energy_flag, 1);
     if (bad) atomicOr(&k.ctl->nonfinite, 1);
   }
   if (cfl) {
@@ -472,6 +474,24 @@ static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
   block_sums<5>(f, sh);
   if (tid != 0) return;
   const double dtnbody = c->dtnbody;  // planet_prelude
+  // DetectCrash of the substep's starting state (SourceEuler.c:545-566):
+  // Crashed is the energy test alone (it overwrites the density test's
+  // result; an isothermal run's energy grid holds EnergyMed >= 0 and never
+  // crashes).  The first crash's time is kept and its state copied by the
+  // potential kernel of this substep, which runs before anything changes it.
+  c->crash_snap_now = 0;
+  if (c->neg_dens_flag) c->neg_dens_substeps += 1;
+  if (k.energy && c->neg_energy_flag) {
+    if (c->crashes == 0) {
+      c->crash_time = c->physical_time;
+      c->crash_snap_now = k.crash_snap ? 1 : 0;
+      c->crash_snapped = c->crash_snap_now;
+    }
+    c->crashes += 1;
+    c->crash_substeps += 1;
+  }
+  c->neg_dens_flag = 0;
+  c->neg_energy_flag = 0;
   // ConditionCFL reduction (SourceEuler.c:1336-1497) and substep count
   const double deltaT = c->DT - c->dtemp;
   double newdt = newdt_cells;
@@ -601,6 +621,13 @@ __global__ void __launch_bounds__(FB_BS2) k_potential(KP k)
     }
     k.pot[l] = P;
     if (k.particles) k.indpot[l] = IP;  // IndPotential (Pframeforce.c:55-121)
+    if (c->crash_snap_now) {  // the first crash's state (WriteDiskPolar ..., 999)
+      const size_t n = (size_t)k.nr * k.ns;
+      k.crash_snap[l] = k.rho[l];
+      k.crash_snap[n + l] = k.vr[l];
+      k.crash_snap[2 * n + l] = k.vt[l];
+      if (k.energy) k.crash_snap[3 * n + l] = k.e[l];
+    }
   }
 }
 
@@ -1857,6 +1884,20 @@ void fb_launch_transport_vr(const KP &k, cudaStream_t s)
   fb_launch(k_transport_vr, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k);
 }
 
+// Makes the driver load the radial and vr transport kernels now (asking
+// for a function's attributes loads it under lazy module loading), so that
+// their first launch later needs no module load.  fb_gas_prepare does the
+// same for every azimuthal variant.
+int fb_transport_preload(void)
+{
+  const void *fns[] = {(const void *)k_transport_radial<5>, (const void *)k_transport_radial<6>,
+                       (const void *)k_transport_vr};
+  cudaFuncAttributes fa;
+  for (const void *f : fns)
+    if (cudaFuncGetAttributes(&fa, f) != cudaSuccess) return FB_ERR_CUDA;
+  return FB_OK;
+}
+
 // Transport (TransportEuler.c:65-87) + floors + boundaries: 3 launches
 void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s)
 {
@@ -2056,6 +2097,8 @@ __global__ void k_begin_dt(KP k, double DT)
   c->substeps = 0;
   c->status = 0;
   c->nonfinite = 0;
+  c->crash_substeps = 0;
+  c->neg_dens_substeps = 0;
 }
 
 void fb_launch_begin_dt(const KP &k, double DT, cudaStream_t s) { fb_launch(k_begin_dt, 1, 1, 0, s, k, DT); }

@@ -12,8 +12,13 @@
 // The scratch the transport kernels need between their radial and azimuthal
 // passes (six transported quantities and the post-transport density, one
 // field each, plus one ring of outflow fluxes) lives in a file-scope
-// __device__ array of fixed size: every GPU that loads this library holds it
-// (about 7.4 MB) until the process exits.  Calls share that array and it
+// __device__ array of fixed size (about 7.4 MB): a GPU holds it from the
+// first call on it (when the driver loads this file's module) until the
+// process exits.  The first call on a device also loads every transport
+// kernel, so it is the only call that may make the driver allocate; later
+// calls allocate nothing.  A call copies the grid tables from pageable host
+// memory and synchronizes its stream, so it must never be made while that
+// stream is being captured into a CUDA graph.  Calls share that array and it
 // keeps the last call's contents; the only value that must start at zero
 // (the outflow accumulator) is cleared on every call.  Calls that overlap on
 // the GPU (different streams, or different host threads) race on the shared
@@ -30,6 +35,7 @@
 #define FB_NA_MAX_NSEC 3072
 #define FB_NA_NTAB 10
 #define FB_NA_MAX_DEVICES 64
+#define FB_NA_MIN_NSEC 16
 
 static __device__ __align__(256) double fb_na_scratch[7 * (size_t)FB_NA_MAX_CELLS + FB_NA_MAX_NSEC];
 static __device__ __align__(256) double fb_na_tables[FB_NA_NTAB * (FB_NA_MAX_NRAD + 1)];
@@ -57,7 +63,11 @@ static int na_fail(int code, const char *msg)
 }
 
 // Once per device, with that device current: device addresses of the
-// file-scope arrays.  Host code must not use the symbols themselves.
+// file-scope arrays (host code must not use the symbols themselves), and
+// every kernel a call can launch loaded now.  Under lazy module loading
+// (CUDA's default) the driver loads a kernel, and may allocate device memory
+// for it, the first time the kernel is used; doing all of that here confines
+// it to the first call on each device.
 static int na_setup(int dev)
 {
   na_device &d = g_na[dev];
@@ -67,6 +77,12 @@ static int na_setup(int dev)
       cudaGetSymbolAddress((void **)&d.ctl, fb_na_ctl) != cudaSuccess) {
     cudaGetLastError();
     return na_fail(FB_ERR_CUDA, "cudaGetSymbolAddress failed for the no-alloc scratch");
+  }
+  // the azimuthal variants (all of them, whatever the grid) and the radial
+  // and vr passes
+  if (fb_gas_prepare(FB_NA_MIN_NSEC, 1) != FB_OK || fb_transport_preload() != FB_OK) {
+    cudaGetLastError();
+    return na_fail(FB_ERR_CUDA, "loading the transport kernels failed");
   }
   d.ready = 1;
   return FB_OK;
@@ -79,7 +95,7 @@ extern "C" int fb_transport_noalloc(const fb_params *p, double *dens, double *vr
     return na_fail(FB_ERR_INVALID, "null argument");
   if (!(dt > 0.0)) return na_fail(FB_ERR_INVALID, "dt must be > 0");
   const int nr = p->nrad, ns = p->nsec;
-  if (nr < 4 || ns < 16) return na_fail(FB_ERR_INVALID, "grid too small (nrad >= 4, nsec >= 16)");
+  if (nr < 4 || ns < FB_NA_MIN_NSEC) return na_fail(FB_ERR_INVALID, "grid too small (nrad >= 4, nsec >= 16)");
   if ((size_t)(nr + 1) * ns > FB_NA_MAX_CELLS || nr > FB_NA_MAX_NRAD || ns > FB_NA_MAX_NSEC)
     return na_fail(FB_ERR_INVALID,
                    "grid too large for the no-alloc scratch: (nrad+1)*nsec must be <= 131072, "

@@ -15,7 +15,9 @@
  * drand48 stream and the scalar globals (PhysicalTime, LostMass, MINDT,
  * MAXDT, stardiscbarycenter) are refreshed so that the reference's
  * SendOutput, planet and particle logs and -a monitor see the state they
- * expect.  Errors print a message and call prs_exit(1),
+ * expect.  A crash (the reference's negative-energy test) is reported as the
+ * reference does: "Crash!" and the *999.dat dumps once, a 'c' per crashed
+ * substep, and the run goes on.  Errors print a message and call prs_exit(1),
  * the reference's own way of stopping (src/LowTasks.c:32).
  */
 #include "mp.h"
@@ -36,6 +38,7 @@ extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensi
 extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
 
 static fb_ctx *g_ctx = NULL;
+static int g_crashes = 0;  /* AlreadyCrashed as last reported */
 
 static void dropin_fail(const char *what, int rc)
 {
@@ -199,6 +202,41 @@ static void state_views(fb_state *st, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid
   st->energy = Energy->Field;
 }
 
+/* The reference's reaction to its first crash (SourceEuler.c:549-561):
+   "Crash! at time ..." and the state of that substep written as
+   gas{dens,vrad,vtheta,energy}999.dat by its own WriteDiskPolar, here from
+   the copy the GPU kept (fb_download_crash). */
+static void write_crash_dumps(PolarGrid *Rho, PolarGrid *Vrad, PolarGrid *Vtheta, PolarGrid *Energy)
+{
+  PolarGrid *g[4];
+  double *buf[4];
+  real *keep;
+  fb_state cs;
+  double t = 0.0;
+  const size_t n = (size_t)NRAD * NSEC;
+  int q, rc;
+  g[0] = Rho; g[1] = Vrad; g[2] = Vtheta; g[3] = Energy;
+  for (q = 0; q < 4; q++) {
+    buf[q] = (double *)malloc(n * sizeof(double));
+    if (!buf[q]) dropin_fail("crash dump buffer", FB_ERR_NOMEM);
+  }
+  memset(&cs, 0, sizeof cs);
+  cs.dens = buf[0];
+  cs.vrad = buf[1];
+  cs.vtheta = buf[2];
+  cs.energy = buf[3];
+  rc = fb_download_crash(g_ctx, &cs, &t);
+  if (rc) dropin_fail("fb_download_crash", rc);
+  fprintf(stdout, "\nCrash! at time %.12g\n", t);
+  for (q = 0; q < 4; q++) {
+    keep = g[q]->Field;
+    g[q]->Field = buf[q];
+    WriteDiskPolar(g[q], 999);
+    g[q]->Field = keep;
+    free(buf[q]);
+  }
+}
+
 void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid *Vtheta,
                        PolarGrid *Energy, PolarGrid *Label, PolarGrid *DRho,
                        PolarGrid *dustpcdens, PolarGrid *DVrad, PolarGrid *DVtheta,
@@ -262,7 +300,7 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
     }
   }
   rc = fb_algogas(g_ctx, &rep);
-  if (rc) dropin_fail("fb_algogas", rc);
+  if (rc && rc != FB_ERR_NEGATIVE) dropin_fail("fb_algogas", rc);  /* a crash is not fatal */
   rc = fb_download(g_ctx, &st, FB_F_ALL);
   if (rc) dropin_fail("fb_download", rc);
   if (EnergyEquation || Write_Temperature) fb_download_derived(g_ctx, 0, Temperature->Field);
@@ -288,7 +326,11 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
     sys->vx[k] = st.planets.vx[k];
     sys->vy[k] = st.planets.vy[k];
   }
-  /* one '.' per substep, as the reference prints (SourceEuler.c:567) */
-  for (k = 0; k < rep.substeps; k++) masterprint(".");
+  if (rep.crashes > 0 && g_crashes == 0) write_crash_dumps(Rho, Vrad, Vtheta, Energy);
+  g_crashes = rep.crashes;
+  /* one mark per substep as the reference prints them (SourceEuler.c:564-567):
+     '.', or 'c' for a crashed substep */
+  for (k = 0; k < rep.substeps - rep.crash_substeps; k++) masterprint(".");
+  for (k = 0; k < rep.crash_substeps; k++) masterprint("c");
   masterprint("\n");
 }

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define FB_ABI_VERSION 1
+#define FB_ABI_VERSION 2
 
 #define FB_OK               0
 #define FB_ERR_INVALID     -1   /* bad argument or parameter value          */
@@ -37,8 +37,9 @@ extern "C" {
 #define FB_ERR_CUDA        -3   /* CUDA runtime error                        */
 #define FB_ERR_NOMEM       -4   /* device or host allocation failed          */
 #define FB_ERR_NAN         -5   /* NaN/Inf found in the gas state            */
-#define FB_ERR_NEGATIVE    -6   /* negative density or energy (the reference's
-                                   DetectCrash, src/SourceEuler.c:51-69)     */
+#define FB_ERR_NEGATIVE    -6   /* the reference's crash test fired during the
+                                   DT (DetectCrash, src/SourceEuler.c:51-69,
+                                   545-566): a warning, the DT is complete   */
 #define FB_ERR_SUBSTEPS    -7   /* CFL substep count above the cap           */
 #define FB_ERR_TIMEOUT     -8   /* a bounded device wait gave up             */
 #define FB_ERR_IO          -9   /* file could not be read or written         */
@@ -146,7 +147,16 @@ typedef struct fb_profiles {
   double *global_soundspeed;
 } fb_profiles;
 
-/* What one fb_algogas call did. */
+/* What one fb_algogas call did.
+   Crash bookkeeping follows AlgoGas (src/SourceEuler.c:545-566): at every
+   substep the state is tested for negative values before the gas update, and
+   the substep "crashes" when the energy is negative somewhere (the density
+   test runs too, but its result is overwritten by the energy test's, so an
+   isothermal run never crashes).  The first crash's time is timeCRASH and its
+   state (density, vrad, vtheta, energy of rings 0..nrad-1) is kept on the
+   device for fb_download_crash, the reference's *999.dat dumps.  Like the
+   reference, the step carries on after a crash: fb_algogas completes the DT
+   and returns FB_ERR_NEGATIVE (status too) when any of its substeps crashed. */
 typedef struct fb_step_report {
   int substeps;          /* CFL substeps taken in this DT                 */
   int status;            /* FB_OK or the first error seen                 */
@@ -154,6 +164,14 @@ typedef struct fb_step_report {
   double mindt, maxdt;   /* MINDT / MAXDT (src/SourceEuler.c:457-460)     */
   double lost_mass;      /* LostMass (src/TransportEuler.c:137)            */
   double gpu_ms;         /* device time of the DT (CUDA events)            */
+  int crashes;           /* AlreadyCrashed: crashed substeps so far (since
+                            fb_create), src/SourceEuler.c:563           */
+  int crash_substeps;    /* crashed substeps of this DT (the 'c' marks of
+                            src/SourceEuler.c:564)                       */
+  int neg_density_substeps; /* substeps of this DT that began with a negative
+                            density somewhere (not a crash for AlgoGas)  */
+  double crash_time;     /* timeCRASH: PhysicalTime of the first crash
+                            (src/SourceEuler.c:551); 0 if none           */
 } fb_step_report;
 
 /* Lagrangian dust particles (src/types.h:114-146, the fields the step
@@ -227,6 +245,12 @@ int fb_download(fb_ctx *ctx, fb_state *st, unsigned mask);
    interpolation call, src/main.c:287), download when writing outputs. */
 int fb_dust_upload(fb_ctx *ctx, const fb_dust_state *st);
 int fb_dust_download(fb_ctx *ctx, fb_dust_state *st);
+/* The state at the first crash (see fb_step_report), nrad*nsec doubles per
+   non-NULL field of st (density, vrad, vtheta, energy; ring nrad untouched):
+   what the reference writes as gasdens999.dat, gasvrad999.dat,
+   gasvtheta999.dat and gasenergy999.dat (src/SourceEuler.c:549-561).
+   FB_ERR_STATE if no crash happened. */
+int fb_download_crash(fb_ctx *ctx, fb_state *st, double *crash_time);
 /* Derived output fields at the current state (reference layout, (nrad+1)*nsec):
    which = 0 Temperature (src/SourceEuler.c:2440), 1 Potential, 2 Pressure,
    3 SoundSpeed, 4 DivergenceVelocity, 5 ViscHeat, 6 SG radial acceleration
@@ -342,18 +366,20 @@ int fb_stage(fb_ctx *ctx, int stage, double dt);
    fb_stage(ctx, FB_STAGE_TRANSPORT, dt) (Transport, src/TransportEuler.c:65)
    without a context and without allocating anything: the inter-pass scratch
    is a fixed file-scope device array of at most FB_NOALLOC_MAX_CELLS cells
-   (about 7.4 MB), held on every GPU that loads the library until exit.
+   (about 7.4 MB), held on a GPU from the first call there until exit.
    dens, vrad, vtheta, energy are DEVICE pointers to (nrad+1)*nsec doubles in
    the PolarGrid layout, updated in place (energy only with the energy
    equation); stream is a cudaStream_t (NULL: default stream); lost_mass, if
    not NULL, receives the ring-0 outflow of this call (the stream is then
    synchronized).  Grids with (nrad+1)*nsec > FB_NOALLOC_MAX_CELLS, nrad >
    4096 or nsec > 3072 are refused with FB_ERR_INVALID.  The first call on a
-   device (and the first with a larger nsec) sets up the device addresses and
-   kernel attributes; make it before any stream capture.  Every call
-   synchronizes the stream once after uploading the grid tables.  All calls
-   share the scratch, so calls that overlap on the GPU race.  The reason for
-   a failure is in fb_noalloc_last_error(). */
+   device sets up the device addresses and loads every kernel a call can
+   launch: it is the only call that may make the CUDA driver allocate (module
+   loading); later calls allocate nothing.  Every call copies the grid tables
+   from host memory and synchronizes the stream, so no call may be made while
+   its stream is being captured into a CUDA graph.  All calls share the
+   scratch, so calls that overlap on the GPU race.  The reason for a failure
+   is in fb_noalloc_last_error(). */
 #define FB_NOALLOC_MAX_CELLS 131072
 int fb_transport_noalloc(const fb_params *p, double *dens, double *vrad, double *vtheta,
                          double *energy, double dt, void *stream, double *lost_mass);

@@ -24,6 +24,8 @@
  *       leaving the first Transport, ComputeViscousTerms,
  *       UpdateVelocitiesWithViscosity, ApplyBoundaryCondition and
  *       EvanescentBoundary calls of the run.
+ *       With ORACLE_NEGATE_ENERGY=l the energy of cell l changes sign
+ *       before the first call (crash-report tests).
  *   DumpSources      (LowTasks.c:133) becomes a no-op (it shells out to cp).
  *
  * At exit it prints one line "ORACLE_TIMING {json}" on stderr with the
@@ -342,7 +344,14 @@ void __wrap_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad,
   long every = ev ? atol(ev) : 1;
   char tag[64];
   ensure_atexit();
-  if (h_calls == 0) dump_state("state_init", Rho, Vrad, Vtheta, Energy, sys, dsys);
+  if (h_calls == 0) {
+    /* ORACLE_NEGATE_ENERGY=l flips the sign of the energy of cell l before
+       the first DT: the input of the crash-report tests (DetectCrash,
+       SourceEuler.c:545-566) */
+    const char *neg = getenv("ORACLE_NEGATE_ENERGY");
+    if (neg) Energy->Field[atol(neg)] = -Energy->Field[atol(neg)];
+    dump_state("state_init", Rho, Vrad, Vtheta, Energy, sys, dsys);
+  }
   h_call_start = now_s();
   h_in_algogas = 1;
 #ifdef FB_DROPIN

@@ -69,9 +69,12 @@ def write_par(src_par, dst_dir, **keys):
 
 
 def run_oracle(par, steps, noise=0.0, seed=0, dump_every=1, stage=False, workdir=None,
-               timeout=3600, max_substeps=None, keep=False, extra_keys=None, binary=None):
+               timeout=3600, max_substeps=None, keep=False, extra_keys=None, binary=None, flags=()):
     """Run the reference for `steps` AlgoGas calls (NTOT = steps-1) and
-    return (dumps, timing, workdir).  dumps maps tag -> dict of arrays."""
+    return (dumps, timing, workdir).  dumps maps tag -> dict of arrays.
+    `flags` are the reference's own command-line switches (e.g. "-a" for
+    the per-DT mass and momentum lines of main.c:390-395); the run's
+    standard output is kept in workdir/stdout.txt."""
     binary = binary or ORACLE_BIN
     if not os.path.exists(binary):
         raise RuntimeError("%s missing: run `make -C oracle all dropin` where the reference is present" % binary)
@@ -92,8 +95,10 @@ def run_oracle(par, steps, noise=0.0, seed=0, dump_every=1, stage=False, workdir
         env["ORACLE_STAGE_DUMP"] = "1"
     if max_substeps:
         env["ORACLE_MAX_SUBSTEPS"] = str(int(max_substeps))
-    r = subprocess.run([binary, p], cwd=wd, env=env, stdout=subprocess.PIPE, stderr=subprocess.PIPE,
-                       timeout=timeout)
+    r = subprocess.run([binary] + list(flags) + [p], cwd=wd, env=env, stdout=subprocess.PIPE,
+                       stderr=subprocess.PIPE, timeout=timeout)
+    with open(os.path.join(wd, "stdout.txt"), "wb") as f:
+        f.write(r.stdout)
     if r.returncode != 0:
         raise RuntimeError("oracle failed (%d): %s" % (r.returncode, r.stderr[-2000:].decode(errors="replace")))
     dumps = {}
@@ -122,3 +127,11 @@ def rel_err(a, b, floor=0.0):
     if scale == 0.0:
         return float(np.max(np.abs(a - b)))
     return float(np.max(np.abs(a - b)) / scale)
+
+
+def cell_rel_err(a, b):
+    """max over cells of |a-b| / |b|, for strictly positive fields (density,
+    energy): the per-cell relative error."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.max(np.abs(a - b) / np.abs(b)))

@@ -53,3 +53,31 @@ def test_dropin_matches_reference(tmp_path, par_name, keys):
     pa = np.loadtxt(os.path.join(wa, "out", "planet0.dat"))
     pb = np.loadtxt(os.path.join(wb, "out", "planet0.dat"))
     np.testing.assert_allclose(pb, pa, rtol=1e-10, atol=1e-14)
+
+
+def test_dropin_crash_report(tmp_path):
+    """The reference's crash report through the drop-in: the same "Crash!"
+    line and the same gas*999.dat files as the reference's own AlgoGas, from
+    a start with one negative-energy cell; the run goes on."""
+    nr, ns, cell = 48, 144, 20 * 144 + 50
+    par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "adiabatic_sg_512x1536.par"), str(tmp_path),
+                            Nrad=nr, Nsec=ns, SelfGravity="No", AlphaViscosity="0.0")
+    wa, wb = str(tmp_path / "ref"), str(tmp_path / "gpu")
+    os.makedirs(wa)
+    os.makedirs(wb)
+    os.environ["ORACLE_NEGATE_ENERGY"] = str(cell)
+    try:
+        ref, _, _ = _oracle.run_oracle(par, 2, noise=1e-4, seed=3, workdir=wa, keep=True)
+        gpu, _, _ = _oracle.run_oracle(par, 2, noise=1e-4, seed=3, workdir=wb, keep=True,
+                                       binary=_oracle.DROPIN_BIN)
+    finally:
+        del os.environ["ORACLE_NEGATE_ENERGY"]
+    crash = [[line for line in open(os.path.join(w, "stdout.txt")).read().splitlines() if "Crash!" in line]
+             for w in (wa, wb)]
+    assert crash[0] and crash[0] == crash[1]
+    for name in ("gasdens", "gasvrad", "gasvtheta", "gasenergy"):
+        xa = np.fromfile(os.path.join(wa, "out", "%s999.dat" % name))
+        xb = np.fromfile(os.path.join(wb, "out", "%s999.dat" % name))
+        assert xa.size == nr * ns and np.array_equal(xa, xb), name
+    for k in ("dens", "vrad", "vtheta", "energy"):
+        assert _oracle.rel_err(gpu["state_00002"][k], ref["state_00002"][k]) <= 1e-11, k

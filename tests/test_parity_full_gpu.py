@@ -1,0 +1,110 @@
+"""GPU parity against the CPU oracle (the reference's own sequential build)
+at the benchmark workloads' full sizes and on the grid variants the smaller
+tests do not cover.
+
+Tolerances (the FP64 parity bar of this path): gas fields within 1e-11 after
+each DT, both scale-relative (max|gpu-ref| / max|ref| per field) and, for the
+strictly positive density and energy, per cell (max |gpu-ref|/|ref|);
+particle positions and velocities within 1e-10 with the drand48 stream at
+exactly the reference's position; equal substep counts.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from tests import _oracle
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not _oracle.have_oracle(), reason="oracle not built")]
+
+CFG = _oracle.CONFIG_DIR
+TOL_DT = 1e-11
+TOL_DUST = 1e-10
+
+
+def _check_dt(rep, out, ref, prev_substeps, fields):
+    assert rep.substeps == int(ref["substeps"]) - prev_substeps, "substep count differs"
+    errs = {k: _oracle.rel_err(out[k], ref[k]) for k in fields}
+    cell = {k: _oracle.cell_rel_err(out[k], ref[k]) for k in ("dens", "energy") if k in fields}
+    print("substeps", rep.substeps, "scale-relative", errs, "per cell", cell)
+    assert all(e <= TOL_DT for e in errs.values()), errs
+    assert all(e <= TOL_DT for e in cell.values()), cell
+    assert abs(out["PhysicalTime"] - ref["PhysicalTime"]) <= 1e-13 * abs(ref["PhysicalTime"])
+    return int(ref["substeps"])
+
+
+def _run(par, steps, noise, seed, fields, dust=False, dust_seed=None):
+    from dustyfargoadsg_b200 import Disc, read_par
+    dumps, _, _ = _oracle.run_oracle(par, steps=steps, noise=noise, seed=seed, timeout=3000)
+    p = read_par(par)
+    assert p.unsupported == 0
+    with Disc(p, noise=noise, seed=seed, dust_seed=dust_seed) as disc:
+        init = disc.download()
+        for k in fields:
+            assert _oracle.rel_err(init[k], dumps["state_init"][k]) <= (1e-13 if p.self_gravity else 0.0), k
+        prev = 0
+        for s in range(1, steps + 1):
+            rep = disc.step()
+            ref = dumps["state_%05d" % s]
+            prev = _check_dt(rep, disc.download(), ref, prev, fields)
+            if dust:
+                d = disc.dust()
+                errs = {k: _oracle.rel_err(d[k], ref[k]) for k in ("pc_r", "pc_th", "pc_vr", "pc_vth", "pc_stokes")}
+                print("particles", errs, "kicks", d["pc_kicks"])
+                assert all(e <= TOL_DUST for e in errs.values()), errs
+                assert d["pc_rng_x"] == int(ref["rng_state"]), "random stream out of step"
+    return dumps
+
+
+def test_headline_workload_two_dts(tmp_path):
+    """The benchmark's default workload as it is: 512 x 1536, adiabatic with
+    beta cooling, alpha viscosity and self-gravity, two whole DTs."""
+    par = _oracle.write_par(os.path.join(CFG, "adiabatic_sg_512x1536.par"), str(tmp_path))
+    _run(par, 2, 1e-4, 0, ("dens", "vrad", "vtheta", "energy"))
+
+
+def test_dust_workload_full_size(tmp_path):
+    """The particle workload as it is: 256 x 768 gas with 200,000 particles
+    and turbulent kicks, one whole DT."""
+    par = _oracle.write_par(os.path.join(CFG, "dust_256x768.par"), str(tmp_path))
+    _run(par, 1, 1e-4, 0, ("dens", "vrad", "vtheta"), dust=True, dust_seed=0)
+
+
+@pytest.mark.parametrize("case", ["gas", "particles"])
+def test_arithmetic_radii(tmp_path, case):
+    """RadialSpacing A: evenly spaced interfaces (SourceEuler.c:88-96)."""
+    if case == "gas":
+        par = _oracle.write_par(os.path.join(CFG, "iso_128x384.par"), str(tmp_path), RadialSpacing="A")
+        _run(par, 2, 1e-4, 0, ("dens", "vrad", "vtheta"))
+    else:
+        par = _oracle.write_par(os.path.join(CFG, "dust_256x768.par"), str(tmp_path), RadialSpacing="A",
+                                Nrad=64, Nsec=192, NbPart=2000, RminDust=0.6, RmaxDust=1.8)
+        _run(par, 2, 1e-4, 1, ("dens", "vrad", "vtheta"), dust=True, dust_seed=1)
+
+
+def test_alternative_indirect_term(tmp_path):
+    """AlternativeGasIndirectTerm: the disc's pull on the star from the
+    finite-difference acceleration of the star-disc barycentre
+    (ComputeOppositeAccelerationOfBarycenter, SideEuler.c:91-112)."""
+    from dustyfargoadsg_b200 import Disc, read_par
+    par = _oracle.write_par(os.path.join(CFG, "iso_128x384.par"), str(tmp_path), Nrad=64, Nsec=192,
+                            AlternativeGasIndirectTerm="Yes")
+    p = read_par(par)
+    assert p.alternative_gas_indirect_term == 1 and p.unsupported == 0
+    steps = 3
+    dumps, _, _ = _oracle.run_oracle(par, steps=steps, noise=1e-3, seed=6)
+    with Disc(p, noise=1e-3, seed=6) as disc:
+        prev = 0
+        for s in range(1, steps + 1):
+            rep = disc.step()
+            ref = dumps["state_%05d" % s]
+            out = disc.download()
+            prev = _check_dt(rep, out, ref, prev, ("dens", "vrad", "vtheta"))
+            st = disc.st
+            for q in range(3):
+                for name in ("stardiscbarycenter_x", "stardiscbarycenter_y"):
+                    a, b = getattr(st, name)[q], ref[name][q]
+                    # sums over the disc's cells that cancel to ~1e-8: the
+                    # summation order shows at ~1e-18
+                    assert abs(a - b) <= 1e-12 * abs(b) + 1e-17, (name, q, a, b)

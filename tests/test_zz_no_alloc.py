@@ -5,9 +5,12 @@ GPU application that owns the device-memory budget, or called from a region
 where an allocation (which may synchronize the device) is not acceptable.
 Its scratch is a fixed file-scope device array shared by all calls, so the
 test makes two calls in a row (the second one sees the first one's leftover
-scratch) on each of two grids, and checks every result against the
-allocating path through a context, fb_stage(ctx, FB_STAGE_TRANSPORT, dt),
-within the stage tolerance the other GPU tests use.
+scratch) on each of two grids, and checks every result, and the ring-0
+outflow it reports, against the allocating path through a context,
+fb_stage(ctx, FB_STAGE_TRANSPORT, dt), within the stage tolerance the other
+GPU tests use.  Only the first call on a device may make the driver allocate
+(it loads the kernels); the test checks that the device's free memory is the
+same before and after every later call.
 """
 import ctypes as C
 import os
@@ -21,6 +24,7 @@ pytestmark = pytest.mark.gpu
 
 TOL_STAGE = 1e-12
 FIELDS = ("dens", "vrad", "vtheta", "energy")
+_setup_done = [False]  # the first call of this process on the device has been made
 
 
 def _run_pair(par, dt):
@@ -39,18 +43,26 @@ def _run_pair(par, dt):
     torch.cuda.synchronize()
     t = {k: torch.tensor(start[k], dtype=torch.float64, device="cuda") for k in FIELDS}
     ptr = {k: C.c_void_p(t[k].data_ptr()) for k in FIELDS}
+    prev_lost = start["LostMass"]
     for ref in (ref1, ref2):
         torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         lost = C.c_double(0.0)
         rc = lib.fb_transport_noalloc(C.byref(p), ptr["dens"], ptr["vrad"], ptr["vtheta"], ptr["energy"],
                                       dt, None, C.byref(lost))
         assert rc == 0, lib.fb_noalloc_last_error().decode()
         torch.cuda.synchronize()
+        if _setup_done[0]:
+            assert torch.cuda.mem_get_info()[0] == free0, "a call after the first one allocated device memory"
+        _setup_done[0] = True
         for k in FIELDS:
             got = t[k].cpu().numpy()
             err = _oracle.rel_err(got, ref[k])
             assert err <= TOL_STAGE, (k, err)
-        assert np.isfinite(lost.value)
+        # the ring-0 outflow of this call, as the context accumulates it
+        want = ref["LostMass"] - prev_lost
+        prev_lost = ref["LostMass"]
+        assert abs(lost.value - want) <= TOL_STAGE * max(abs(want), abs(ref["LostMass"])), (lost.value, want)
 
 
 def test_transport_noalloc_matches_context_path(tmp_path):
