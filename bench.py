@@ -236,6 +236,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=None, choices=sorted(WORKLOADS))
+    ap.add_argument("--mode", default=None, choices=["parity", "fast"],
+                    help="library build: parity (exact divisions, unfused multiply-adds, the reference's "
+                         "rounding) or fast (fused multiply-adds, approximate-reciprocal slopes); both "
+                         "meet the same parity tests")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep measurement")
     args = ap.parse_args()
@@ -253,7 +257,11 @@ def main():
         run_reference(args, par_path, wl, grid[0] * grid[1])
         return
 
+    if args.mode is not None:
+        os.environ["FB_MODE"] = args.mode  # read by every library load below
     import dustyfargoadsg_b200 as fb
+    from dustyfargoadsg_b200 import _ffi
+    args.mode = _ffi.default_mode()
     p = fb.read_par(par_path)
     wl["nrad"], wl["nsec"] = p.nrad, p.nsec
     cells = p.nrad * p.nsec
@@ -392,7 +400,7 @@ def main():
 
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
-        batch = measure_batch(fb, table, flush)
+        batch = measure_batch(fb, table, flush, cpu_baseline=not args.no_cpu_baseline)
 
     if rank == 0:
         line = {
@@ -402,7 +410,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded white noise on the initial density)",
             "config": {"workload": args.workload, "nrad": p.nrad, "nsec": p.nsec,
                        "substeps_per_step": sub_all / world / args.steps,
-                       "parallelism": "replicas%d" % world,
+                       "parallelism": "replicas%d" % world, "build": args.mode,
                        "l2": "flushed (256 MB write) before every timed step"},
             "e2e": {"value": e2e_value, "unit": "cell-updates/s", "h2d_bytes_per_step": fbytes,
                     "d2h_bytes_per_step": fbytes + d2h_extra},
@@ -424,7 +432,7 @@ def main():
         dist.destroy_process_group()
 
 
-def measure_batch(fb, table, flush, warmup=2, steps=3):
+def measure_batch(fb, table, flush, warmup=2, steps=3, cpu_baseline=True):
     """The batched sweep: 64 discs of uneven grids and parameters (seed 2),
     one graph launch per DT for all of them; orbits/s summed over discs."""
     import torch
@@ -443,15 +451,54 @@ def measure_batch(fb, table, flush, warmup=2, steps=3):
                 ms += reps[0].gpu_ms
                 cell_updates += sum(r.substeps * d.nr * d.ns for r, d in zip(reps, discs))
             launches = sum(d.kernel_launches() for d in discs) - launches0
+            subs_per_dt = [r.substeps for r in reps]
         orbits = BATCH_DISCS * steps * sweep.orbits_per_dt(discs[0].p)
-        return {"metric": "batched orbits/s", "value": orbits / (ms / 1e3), "unit": "orbits/s",
-                "discs": BATCH_DISCS, "seed": BATCH_SEED, "steps": steps, "warmup": warmup,
-                "cell_updates_per_s": cell_updates / (ms / 1e3), "ms_per_step": ms / steps,
-                "gpu_launches": launches, "graph_launches_per_step": 1,
-                "grids": sorted({"%dx%d" % (d.nr, d.ns) for d in discs})}
+        out = {"metric": "batched orbits/s", "value": orbits / (ms / 1e3), "unit": "orbits/s",
+               "discs": BATCH_DISCS, "seed": BATCH_SEED, "steps": steps, "warmup": warmup,
+               "cell_updates_per_s": cell_updates / (ms / 1e3), "ms_per_step": ms / steps,
+               "gpu_launches": launches, "graph_launches_per_step": 1,
+               "grids": sorted({"%dx%d" % (d.nr, d.ns) for d in discs})}
+        if cpu_baseline:
+            cells = [d.nr * d.ns for d in discs]
+            out["cpu_baseline"] = batch_cpu_baseline(wd, cells, subs_per_dt, sweep.orbits_per_dt(discs[0].p))
+        return out
     finally:
         for d in discs:
             d.close()
+
+
+def batch_cpu_baseline(wd, cells, subs_per_dt, orbits_per_dt, budget_s=24.0):
+    """The batched sweep on the host: one process of the reference's own
+    build (oracle/_ref) per disc, as many at once as there are cores, each
+    timed on a bounded sample of its own substeps (time inside AlgoGas).
+    A disc's orbits/s is its substep rate over its substeps per DT (as the
+    GPU took them) times the orbits per DT; the sweep's rate on all cores is
+    the sum over discs times min(1, cores / discs)."""
+    import concurrent.futures as cf
+
+    from tests import _oracle  # test infrastructure: the CPU baseline only
+    if not _oracle.have_oracle():
+        return {"value": None, "unit": "orbits/s", "kind": "reference", "sample": "oracle binary not built"}
+    cores = os.cpu_count() or 1
+    n = len(cells)
+    per_disc = budget_s * min(cores, n) / n
+    guess = 4.0e6  # cell-updates/s of one core, only to size the samples
+
+    def one(d):
+        nsub = max(2, int(per_disc * guess / cells[d]))
+        w = tempfile.mkdtemp(prefix="fb_bcpu_")
+        _, t, _ = _oracle.run_oracle(os.path.join(wd, "disc%03d.par" % d), steps=10 ** 6, noise=1e-4, seed=0,
+                                     dump_every=10 ** 9, max_substeps=nsub, workdir=w, keep=True, timeout=1800)
+        return t
+
+    with cf.ThreadPoolExecutor(max_workers=cores) as ex:
+        timings = list(ex.map(one, range(n)))
+    rates = [t["substeps"] / t["wall_s"] / max(s, 1) * orbits_per_dt for t, s in zip(timings, subs_per_dt)]
+    value = sum(rates) * min(1.0, cores / n)
+    return {"value": value, "unit": "orbits/s", "cores": cores, "kind": "reference",
+            "sample": "each of the %d discs run alone by the reference's build for about %.1f s of substeps "
+                      "(%d at a time); orbits/s per disc from its substep rate and the GPU's substeps per DT"
+                      % (n, per_disc, min(cores, n))}
 
 
 if __name__ == "__main__":

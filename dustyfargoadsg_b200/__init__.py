@@ -55,8 +55,10 @@ class Disc:
 
     DUST_ARRAYS = ("r", "th", "vr", "vth", "l", "size", "stokes")
 
-    def __init__(self, params, noise=0.0, seed=0, state=None, dust_seed=None, tuning=None):
-        self.lib = load()
+    def __init__(self, params, noise=0.0, seed=0, state=None, dust_seed=None, tuning=None, mode=None):
+        """mode: the library build, "parity" or "fast" (default: FB_MODE, else parity)."""
+        self.lib = load(mode)
+        self.mode = self.lib.fb_mode
         if isinstance(params, (str, os.PathLike)):
             params = read_par(params)
         self.p = params
@@ -86,18 +88,18 @@ class Disc:
                 setattr(self.dst, k, _ptr(a))
         if state is None:
             check(self.lib.fb_init_state(C.byref(self.p), self.ctx, float(noise), int(seed),
-                                         C.byref(self.st), C.byref(self.pr)), "fb_init_state", self.ctx)
+                                         C.byref(self.st), C.byref(self.pr)), "fb_init_state", self.ctx, self.lib)
         else:
             self.set_state(state)
             if self.npart > 0 and "pc_r" in state:
                 self.set_dust(state)
             return
-        check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx)
+        check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx, self.lib)
         if self.npart > 0:
             # InitDustSystem reseeds the stream (Dsys.c:173)
             check(self.lib.fb_init_dust(C.byref(self.p), self.ctx, int(seed if dust_seed is None else dust_seed),
-                                        C.byref(self.dst)), "fb_init_dust", self.ctx)
-            check(self.lib.fb_dust_upload(self.ctx, C.byref(self.dst)), "fb_dust_upload", self.ctx)
+                                        C.byref(self.dst)), "fb_init_dust", self.ctx, self.lib)
+            check(self.lib.fb_dust_upload(self.ctx, C.byref(self.dst)), "fb_dust_upload", self.ctx, self.lib)
 
     # -- launch shapes --------------------------------------------------
     def set_tuning(self, tuning):
@@ -111,12 +113,12 @@ class Disc:
                 return False
         t = _ffi.FbTuning(*[int(entry.get(f, 0)) for f in
                             ("cell_block", "azi_cells_per_thread", "rad_columns", "rad_rings", "azi_variant")])
-        check(self.lib.fb_set_tuning(self.ctx, C.byref(t)), "fb_set_tuning", self.ctx)
+        check(self.lib.fb_set_tuning(self.ctx, C.byref(t)), "fb_set_tuning", self.ctx, self.lib)
         return True
 
     def tuning(self):
         t = _ffi.FbTuning()
-        check(self.lib.fb_get_tuning(self.ctx, C.byref(t)), "fb_get_tuning", self.ctx)
+        check(self.lib.fb_get_tuning(self.ctx, C.byref(t)), "fb_get_tuning", self.ctx, self.lib)
         return {f: getattr(t, f) for f, _ in t._fields_}
 
     # -- particles ------------------------------------------------------
@@ -134,11 +136,11 @@ class Disc:
         carry = state.get("pc_carry", (0.0, 0.0))
         self.dst.carry[0], self.dst.carry[1] = float(carry[0]), float(carry[1])
         self.dst.particles_mass = 0.0
-        check(self.lib.fb_dust_upload(self.ctx, C.byref(self.dst)), "fb_dust_upload", self.ctx)
+        check(self.lib.fb_dust_upload(self.ctx, C.byref(self.dst)), "fb_dust_upload", self.ctx, self.lib)
 
     def dust(self):
         """Download the particles: {pc_r, ..., pc_stokes, pc_rng_x, pc_kicks}."""
-        check(self.lib.fb_dust_download(self.ctx, C.byref(self.dst)), "fb_dust_download", self.ctx)
+        check(self.lib.fb_dust_download(self.ctx, C.byref(self.dst)), "fb_dust_download", self.ctx, self.lib)
         out = {"pc_" + k: v.copy() for k, v in self.dust_arrays.items()}
         out.update(pc_rng_x=int(self.dst.rng_x), pc_kicks=int(self.dst.kicks),
                    pc_carry=(self.dst.carry[0], self.dst.carry[1]))
@@ -185,7 +187,7 @@ class Disc:
                 pl.feeldisk[q] = cfg.feeldisk[q]
                 pl.feelothers[q] = cfg.feelothers[q]
                 pl.binary[q] = cfg.binary[q]
-        check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx)
+        check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx, self.lib)
 
     def step(self):
         """One DT (AlgoGas) on the device; returns the step report.
@@ -198,7 +200,7 @@ class Disc:
         rep = FbStepReport()
         rc = self.lib.fb_algogas(self.ctx, C.byref(rep))
         if rc != _ffi.FB_ERR_NEGATIVE:
-            check(rc, "fb_algogas", self.ctx)
+            check(rc, "fb_algogas", self.ctx, self.lib)
         return rep
 
     def crash_state(self):
@@ -210,15 +212,15 @@ class Disc:
         for k, a in out.items():
             setattr(st, k, _ptr(a))
         t = C.c_double()
-        check(self.lib.fb_download_crash(self.ctx, C.byref(st), C.byref(t)), "fb_download_crash", self.ctx)
+        check(self.lib.fb_download_crash(self.ctx, C.byref(st), C.byref(t)), "fb_download_crash", self.ctx, self.lib)
         out["crash_time"] = t.value
         return out
 
     def stage(self, stage, dt):
-        check(self.lib.fb_stage(self.ctx, int(stage), float(dt)), "fb_stage", self.ctx)
+        check(self.lib.fb_stage(self.ctx, int(stage), float(dt)), "fb_stage", self.ctx, self.lib)
 
     def download(self, mask=FB_F_ALL):
-        check(self.lib.fb_download(self.ctx, C.byref(self.st), C.c_uint(mask)), "fb_download", self.ctx)
+        check(self.lib.fb_download(self.ctx, C.byref(self.st), C.c_uint(mask)), "fb_download", self.ctx, self.lib)
         out = {k: v.copy() for k, v in self.fields.items()}
         st = self.st
         out.update(PhysicalTime=st.physical_time, LostMass=st.lost_mass, MINDT=st.mindt, MAXDT=st.maxdt,
@@ -232,7 +234,7 @@ class Disc:
         return int(self.lib.fb_kernel_launches(self.ctx))
 
     def profile(self, enable=True):
-        check(self.lib.fb_profile(self.ctx, 1 if enable else 0), "fb_profile", self.ctx)
+        check(self.lib.fb_profile(self.ctx, 1 if enable else 0), "fb_profile", self.ctx, self.lib)
 
     def profile_read(self):
         """{stage name: (device ms, launches)} accumulated since profile()."""
@@ -246,7 +248,7 @@ class Disc:
 
     def derived(self, which):
         out = np.zeros(self.nf)
-        check(self.lib.fb_download_derived(self.ctx, int(which), _ptr(out)), "fb_download_derived", self.ctx)
+        check(self.lib.fb_download_derived(self.ctx, int(which), _ptr(out)), "fb_download_derived", self.ctx, self.lib)
         return out
 
     def vortensity(self, field=False):
@@ -255,12 +257,12 @@ class Disc:
         sm, vm = np.zeros(self.nr), np.zeros(self.nr)
         f = np.zeros(self.nf) if field else None
         check(self.lib.fb_vortensity(self.ctx, _ptr(f) if field else None, _ptr(sm), _ptr(vm)),
-              "fb_vortensity", self.ctx)
+              "fb_vortensity", self.ctx, self.lib)
         return (sm, vm, f) if field else (sm, vm)
 
     def diagnostics(self):
         m, p = C.c_double(), C.c_double()
-        check(self.lib.fb_diagnostics(self.ctx, C.byref(m), C.byref(p)), "fb_diagnostics", self.ctx)
+        check(self.lib.fb_diagnostics(self.ctx, C.byref(m), C.byref(p)), "fb_diagnostics", self.ctx, self.lib)
         return m.value, p.value
 
     def close(self):
@@ -286,19 +288,21 @@ class Batch:
     (fb_batch_*); the discs stay usable on their own."""
 
     def __init__(self, discs):
-        self.lib = load()
         self.discs = list(discs)
+        self.lib = self.discs[0].lib
+        if any(d.lib is not self.lib for d in self.discs):
+            raise ValueError("the discs of a batch must use the same library build")
         n = len(self.discs)
         arr = (C.c_void_p * n)(*[d.ctx for d in self.discs])
         self.b = C.c_void_p()
-        check(self.lib.fb_batch_create(arr, n, C.byref(self.b)), "fb_batch_create")
+        check(self.lib.fb_batch_create(arr, n, C.byref(self.b)), "fb_batch_create", None, self.lib)
         self.reps = (FbStepReport * n)()
 
     def step(self):
         """One DT of every disc; returns the per-disc step reports."""
         rc = self.lib.fb_batch_algogas(self.b, self.reps)
         if rc != _ffi.FB_ERR_NEGATIVE:  # a crash is reported per disc, as in Disc.step
-            check(rc, "fb_batch_algogas")
+            check(rc, "fb_batch_algogas", None, self.lib)
         return list(self.reps)
 
     def close(self):

@@ -104,7 +104,22 @@ class FbStepReport(C.Structure):
     ]
 
 
-LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libfargo_b200.so")
+_HERE = os.path.dirname(os.path.abspath(__file__))
+#: the two builds of the library (same C ABI): "parity" divides exactly and
+#: rounds every multiply-add twice like the reference's build; "fast" fuses
+#: multiply-adds and takes the van Leer slopes through a refined approximate
+#: reciprocal
+LIB_PATHS = {"parity": os.path.join(_HERE, "libfargo_b200.so"),
+             "fast": os.path.join(_HERE, "libfargo_b200_fast.so")}
+LIB_PATH = LIB_PATHS["parity"]
+
+
+def default_mode():
+    """The build used when none is named: FB_MODE from the environment, else parity."""
+    mode = os.environ.get("FB_MODE", "parity")
+    if mode not in LIB_PATHS:
+        raise ValueError("FB_MODE must be one of %s, not %r" % (sorted(LIB_PATHS), mode))
+    return mode
 
 #: every symbol include/fargo_b200.h declares
 EXPORTS = (
@@ -121,19 +136,22 @@ EXPORTS = (
     "fb_closure_set_gain",
 )
 
-_lib = None
+_lib = None   # the first library loaded (error details for contexts without a known library)
+_libs = {}
 
 
-def load():
-    """Load libfargo_b200.so (built by `make -C dustyfargoadsg_b200`)."""
+def load(mode=None):
+    """Load the library of `mode` ("parity" or "fast"; default_mode() when
+    None), built by `make -C dustyfargoadsg_b200`."""
     global _lib
-    if _lib is not None:
-        return _lib
-    if not os.path.exists(LIB_PATH):
+    mode = mode or default_mode()
+    if mode in _libs:
+        return _libs[mode]
+    path = LIB_PATHS[mode]
+    if not os.path.exists(path):
         raise RuntimeError(
-            "libfargo_b200.so is not built (%s); run `make -C dustyfargoadsg_b200` or "
-            "__graft_entry__.build()" % LIB_PATH)
-    lib = C.CDLL(LIB_PATH)
+            "%s is not built; run `make -C dustyfargoadsg_b200` or __graft_entry__.build()" % path)
+    lib = C.CDLL(path)
     vp = C.c_void_p
     sig = {
         "fb_params_default": (_I, [C.POINTER(FbParams)]),
@@ -188,8 +206,11 @@ def load():
         f = getattr(lib, name)
         f.restype = res
         f.argtypes = args
-    _lib = lib
     check_layout(lib)
+    lib.fb_mode = mode
+    _libs[mode] = lib
+    if _lib is None:
+        _lib = lib
     return lib
 
 
@@ -207,9 +228,10 @@ class FbError(RuntimeError):
         super().__init__("%s failed: %s%s" % (where, name, (" (" + detail + ")") if detail else ""))
 
 
-def check(code, where, ctx=None):
+def check(code, where, ctx=None, lib=None):
     if code != FB_OK:
         detail = ""
-        if ctx is not None and _lib is not None:
-            detail = (_lib.fb_last_error(ctx) or b"").decode(errors="replace")
+        lib = lib or _lib
+        if ctx is not None and lib is not None:
+            detail = (lib.fb_last_error(ctx) or b"").decode(errors="replace")
         raise FbError(code, where, detail)

@@ -49,7 +49,7 @@ class Closure:
     """The network and its device-side training set (fb_closure)."""
 
     def __init__(self, coarse_disc, capacity=256, batch=8, seed=0):
-        self.lib = load()
+        self.lib = coarse_disc.lib
         self.c = C.c_void_p()
         check(self.lib.fb_closure_create(coarse_disc.ctx, int(capacity), int(batch), int(seed), C.byref(self.c)),
               "fb_closure_create")

@@ -132,7 +132,11 @@ extern "C" const char *fb_last_error(const fb_ctx *ctx) { return ctx ? ctx->err 
 
 extern "C" const char *fb_build_info(void)
 {
-  return "libfargo_b200 sm_100a fp64 --fmad=false abi " "1";
+#if FB_FAST
+  return "libfargo_b200_fast sm_100a fp64 --fmad=true approximate-reciprocal slopes abi 2";
+#else
+  return "libfargo_b200 sm_100a fp64 --fmad=false abi 2";
+#endif
 }
 
 // Particle arrays, the grids the gas step leaves for them, and the constants

@@ -124,6 +124,29 @@ static __device__ __forceinline__ double fb_quot(double a, double d, double r)
   return fma(e, r, y);
 }
 
+// Quotient of a van Leer slope, dq+ dq- / (dq+ + dq-), taken only where
+// dq+ dq- > 0 (so the divisor is non-zero and of the numerator's sign).
+// Parity build: the exact (IEEE, correctly rounded) division of the
+// reference.  Fast build (FB_FAST): the hardware's approximate reciprocal
+// (PTX rcp.approx.ftz.f64) refined by two Newton-Raphson steps,
+// r <- r + r (1 - b r), each of which doubles the correct bits, then one
+// product: a few ulp from the exact quotient, without the division's
+// range-check branch.
+static __device__ __forceinline__ double fb_vl_quot(double a, double b)
+{
+#if FB_FAST
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(b));
+  double e = fma(-b, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-b, r, 1.0);
+  r = fma(r, e, r);
+  return a * r;
+#else
+  return a / b;
+#endif
+}
+
 // Kernel launches of the step.  With programmatic dependent launch a
 // kernel may be scheduled while the one before it in the stream drains;
 // every kernel of the step starts with fb_grid_dependency(), which waits

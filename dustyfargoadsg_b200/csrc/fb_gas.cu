@@ -1063,7 +1063,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
     if (kk <= 0 || kk >= nr - 1) return 0.0;
     double dqm = (a0 - am) * k.invdiffrmed[kk];
     double dqp = (ap - a0) * k.invdiffrmed[kk + 1];
-    if (dqp * dqm > 0.0) return 2.0 * dqp * dqm / (dqp + dqm);
+    if (dqp * dqm > 0.0) return fb_vl_quot(2.0 * dqp * dqm, dqp + dqm);
     return 0.0;
   };
   int kstart = max(i0 - 1, 0);
@@ -1260,7 +1260,7 @@ __global__ void __launch_bounds__(AziMaxThreads<E, WIDE>::value) k_transport_azi
       const double rm = rho[jjm[e]], r0 = rho[jj[e]], rp = rho[jjp[e]];
       R[e] = r0;
       const double dqm = (r0 - rm), dqp = (rp - r0);
-      DR[jj[e]] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+      DR[jj[e]] = (dqp * dqm > 0.0) ? fb_vl_quot(dqp * dqm, dqp + dqm) * invdxtheta : 0.0;
     }
     __syncthreads();
     // Per face, the upwind cell u and the factor f of its star value:
@@ -1306,7 +1306,7 @@ __global__ void __launch_bounds__(AziMaxThreads<E, WIDE>::value) k_transport_azi
           const double *Wq = Q + q * ns;
           const double w0 = Wq[jj[e]];
           const double dqm = (w0 - Wq[jjm[e]]), dqp = (Wq[jjp[e]] - w0);
-          D[q * ns + jj[e]] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+          D[q * ns + jj[e]] = (dqp * dqm > 0.0) ? fb_vl_quot(dqp * dqm, dqp + dqm) * invdxtheta : 0.0;
         }
       __syncthreads();  // DQ complete
 #pragma unroll
@@ -1345,7 +1345,7 @@ __global__ void __launch_bounds__(AziMaxThreads<E, WIDE>::value) k_transport_azi
         if (!OWN(e)) continue;
         const double w0 = W[jj[e]];
         const double dqm = (w0 - W[jjm[e]]), dqp = (W[jjp[e]] - w0);
-        D[jj[e]] = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+        D[jj[e]] = (dqp * dqm > 0.0) ? fb_vl_quot(dqp * dqm, dqp + dqm) * invdxtheta : 0.0;
       }
       __syncthreads();  // DQ complete
 #pragma unroll
@@ -1515,7 +1515,7 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
       const double rm = P[AZP * jjm[e] + RH], r0 = P[AZP * jj[e] + RH], rp = P[AZP * jjp[e] + RH];
       R[e] = r0;
       const double dqm = (r0 - rm), dqp = (rp - r0);
-      DR_AT(jj[e]) = (dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+      DR_AT(jj[e]) = (dqp * dqm > 0.0) ? fb_vl_quot(dqp * dqm, dqp + dqm) * invdxtheta : 0.0;
     }
     __syncthreads();
     // per face the upwind cell u and the factor f of its star value (as in
@@ -1569,7 +1569,7 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
 #pragma unroll
         for (int u = 0; u < 2; u++) {
           const double dqm = (z_[u] - m_[u]), dqp = (p_[u] - z_[u]);
-          d2[u] = (2 * h + u < NQ && dqp * dqm > 0.0) ? dqp * dqm / (dqp + dqm) * invdxtheta : 0.0;
+          d2[u] = (2 * h + u < NQ && dqp * dqm > 0.0) ? fb_vl_quot(dqp * dqm, dqp + dqm) * invdxtheta : 0.0;
         }
         dd[h] = make_double2(d2[0], d2[1]);
       }

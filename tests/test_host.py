@@ -13,21 +13,25 @@ REPO = _oracle.REPO
 CFG = _oracle.CONFIG_DIR
 
 
-def test_library_exports_every_declared_symbol():
+@pytest.mark.parametrize("mode", ["parity", "fast"])
+def test_library_exports_every_declared_symbol(mode):
     from dustyfargoadsg_b200 import _ffi
-    lib = _ffi.load()
+    lib = _ffi.load(mode)
     header = open(os.path.join(REPO, "include", "fargo_b200.h")).read()
     declared = set(re.findall(r"\b(fb_[a-z0-9_]+)\s*\(", header))
     assert declared, "no declarations parsed"
     for name in sorted(declared):
         assert hasattr(lib, name), name
     assert set(_ffi.EXPORTS) == declared
-    assert b"sm_100a" in lib.fb_build_info()
+    info = lib.fb_build_info()
+    assert b"sm_100a" in info
+    assert (b"--fmad=true" in info) == (mode == "fast")
 
 
-def test_struct_layout_matches_ctypes():
+@pytest.mark.parametrize("mode", ["parity", "fast"])
+def test_struct_layout_matches_ctypes(mode):
     from dustyfargoadsg_b200 import _ffi
-    _ffi.check_layout(_ffi.load())
+    _ffi.check_layout(_ffi.load(mode))
 
 
 def test_params_defaults_and_switches():

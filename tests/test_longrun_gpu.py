@@ -27,11 +27,15 @@ TOL_FIELD = 1e-8
 TOL_TRACK = 1e-10
 
 
-def test_hundred_orbits_match_oracle():
+@pytest.mark.parametrize("mode", ["parity", "fast"])
+def test_hundred_orbits_match_oracle(mode):
+    """Both builds of the library: the parity one, and the fast one (fused
+    multiply-adds, approximate-reciprocal slopes) against the same bar."""
     from dustyfargoadsg_b200 import Disc, read_par
     g = np.load(GOLDEN)
     steps = int(g["steps"])
-    with Disc(read_par(os.path.join(_oracle.CONFIG_DIR, "iso_128x384.par")), noise=1e-4, seed=0) as disc:
+    with Disc(read_par(os.path.join(_oracle.CONFIG_DIR, "iso_128x384.par")), noise=1e-4, seed=0,
+              mode=mode) as disc:
         m0, j0 = disc.diagnostics()
         mass, mom, substeps = np.zeros(steps), np.zeros(steps), 0
         for s in range(steps):
@@ -49,7 +53,7 @@ def test_hundred_orbits_match_oracle():
     track_j = float(np.max(np.abs(mom - g["momentum"]))) / ref_j0
     drift = {"mass gpu": (mass[-1] - m0) / m0, "mass ref": (g["mass"][-1] - ref_m0) / ref_m0,
              "momentum gpu": (mom[-1] - j0) / j0, "momentum ref": (g["momentum"][-1] - ref_j0) / ref_j0}
-    print("100 orbits:", substeps, "substeps; errors", errs, "tracking", track_m, track_j, "drift", drift)
+    print(mode, "100 orbits:", substeps, "substeps; errors", errs, "tracking", track_m, track_j, "drift", drift)
     assert all(e <= TOL_FIELD for e in errs.values()), errs
     assert abs(m0 - ref_m0) <= 1e-14 * ref_m0 and abs(j0 - ref_j0) <= 1e-14 * abs(ref_j0)
     assert track_m <= TOL_TRACK and track_j <= TOL_TRACK, (track_m, track_j)

@@ -34,12 +34,13 @@ def _check_dt(rep, out, ref, prev_substeps, fields):
     return int(ref["substeps"])
 
 
-def _run(par, steps, noise, seed, fields, dust=False, dust_seed=None):
+def _run(par, steps, noise, seed, fields, dust=False, dust_seed=None, dumps=None, mode="parity"):
     from dustyfargoadsg_b200 import Disc, read_par
-    dumps, _, _ = _oracle.run_oracle(par, steps=steps, noise=noise, seed=seed, timeout=3000)
+    if dumps is None:
+        dumps, _, _ = _oracle.run_oracle(par, steps=steps, noise=noise, seed=seed, timeout=3000)
     p = read_par(par)
     assert p.unsupported == 0
-    with Disc(p, noise=noise, seed=seed, dust_seed=dust_seed) as disc:
+    with Disc(p, noise=noise, seed=seed, dust_seed=dust_seed, mode=mode) as disc:
         init = disc.download()
         for k in fields:
             assert _oracle.rel_err(init[k], dumps["state_init"][k]) <= (1e-13 if p.self_gravity else 0.0), k
@@ -57,11 +58,21 @@ def _run(par, steps, noise, seed, fields, dust=False, dust_seed=None):
     return dumps
 
 
-def test_headline_workload_two_dts(tmp_path):
+@pytest.fixture(scope="module")
+def headline(tmp_path_factory):
+    par = _oracle.write_par(os.path.join(CFG, "adiabatic_sg_512x1536.par"), str(tmp_path_factory.mktemp("head")))
+    dumps, _, _ = _oracle.run_oracle(par, steps=2, noise=1e-4, seed=0, timeout=3000)
+    return par, dumps
+
+
+@pytest.mark.parametrize("mode", ["parity", "fast"])
+def test_headline_workload_two_dts(headline, mode):
     """The benchmark's default workload as it is: 512 x 1536, adiabatic with
-    beta cooling, alpha viscosity and self-gravity, two whole DTs."""
-    par = _oracle.write_par(os.path.join(CFG, "adiabatic_sg_512x1536.par"), str(tmp_path))
-    _run(par, 2, 1e-4, 0, ("dens", "vrad", "vtheta", "energy"))
+    beta cooling, alpha viscosity and self-gravity, two whole DTs, with both
+    builds of the library (the fast one fuses multiply-adds and takes the
+    van Leer slopes through an approximate reciprocal: the same bar)."""
+    par, dumps = headline
+    _run(par, 2, 1e-4, 0, ("dens", "vrad", "vtheta", "energy"), dumps=dumps, mode=mode)
 
 
 def test_dust_workload_full_size(tmp_path):
