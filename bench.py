@@ -242,6 +242,8 @@ def main():
                          "meet the same parity tests")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-sweep measurement")
+    ap.add_argument("--no-dropin", action="store_true",
+                    help="skip the measurement through the reference's own main (drop-in AlgoGas)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.workload is None:
@@ -257,8 +259,9 @@ def main():
         run_reference(args, par_path, wl, grid[0] * grid[1])
         return
 
-    if args.mode is not None:
-        os.environ["FB_MODE"] = args.mode  # read by every library load below
+    # the fast build is the benchmarked one: it meets the same parity tests
+    # (one DT at 1e-11, 100 orbits at 1e-8, the full-size workloads)
+    os.environ["FB_MODE"] = args.mode or os.environ.get("FB_MODE", "fast")
     import dustyfargoadsg_b200 as fb
     from dustyfargoadsg_b200 import _ffi
     args.mode = _ffi.default_mode()
@@ -398,6 +401,10 @@ def main():
         else:
             cpu = {"value": None, "unit": "cell-updates/s", "cores": 1, "kind": "reference", "sample": desc}
 
+    dropin = None
+    if rank == 0 and world == 1 and not args.no_dropin:
+        dropin = measure_dropin(par_path, wl, cells, steps=max(3, min(args.steps, 10)))
+
     batch = None
     if rank == 0 and world == 1 and not args.no_batch:
         batch = measure_batch(fb, table, flush, cpu_baseline=not args.no_cpu_baseline)
@@ -425,6 +432,8 @@ def main():
             line["particle_updates_per_s"] = disc.npart * sub_all / t_max
         if batch is not None:
             line["batched"] = batch
+        if dropin is not None:
+            line["dropin"] = dropin
         print(json.dumps(line))
     disc.close()
     if dist is not None:
@@ -465,6 +474,34 @@ def measure_batch(fb, table, flush, warmup=2, steps=3, cpu_baseline=True):
     finally:
         for d in discs:
             d.close()
+
+
+def measure_dropin(par_path, wl, cells, steps, warmup=2):
+    """The workload through the reference's own main() with AlgoGas answered
+    by the library (oracle/_ref/fargo_dropin, built from
+    dustyfargoadsg_b200/host/algogas_dropin.c): wall time of the reference's
+    time loop per DT, its planet logs and every host-side step between the
+    AlgoGas calls included, after `warmup` DTs (graph capture, first SG)."""
+    from tests import _oracle  # test infrastructure: runs the drop-in binary
+    if not os.path.exists(_oracle.DROPIN_BIN):
+        return {"unavailable": "drop-in binary not built"}
+    env = dict(os.environ, ORACLE_TIMING_SKIP=str(warmup))
+    keep = dict(os.environ)
+    os.environ.update(env)
+    try:
+        _, t, _ = _oracle.run_oracle(par_path, steps=warmup + steps, noise=wl["noise"], seed=wl["seed"],
+                                     dump_every=10 ** 9, binary=_oracle.DROPIN_BIN, timeout=1800,
+                                     extra_keys={"Ninterm": 10 ** 6})
+    finally:
+        os.environ.clear()
+        os.environ.update(keep)
+    wall, calls, sub = t["loop_wall_s"], t["loop_calls"], t["loop_substeps"]
+    return {"metric": "gas cell-updates/s FP64 through the reference's main", "value": sub * cells / wall,
+            "unit": "cell-updates/s", "ms_per_dt": wall * 1e3 / calls, "dts": calls, "warmup_dts": warmup,
+            "substeps": sub,
+            "how": "oracle/_ref/fargo_dropin: the reference's main(), per-DT planet logs (UpdateLog, and "
+                   "UpdateLogSG after the loop's self-gravity call, both fed by the GPU) and the host fields "
+                   "downloaded only where the loop reads them; wall clock of the loop"}
 
 
 def batch_cpu_baseline(wd, cells, subs_per_dt, orbits_per_dt, budget_s=24.0):

@@ -100,7 +100,8 @@ class FbStepReport(C.Structure):
     _fields_ = [
         ("substeps", _I), ("status", _I), ("physical_time", _D), ("mindt", _D), ("maxdt", _D),
         ("lost_mass", _D), ("gpu_ms", _D), ("crashes", _I), ("crash_substeps", _I),
-        ("neg_density_substeps", _I), ("crash_time", _D),
+        ("neg_density_substeps", _I), ("crash_time", _D), ("disk_on_primary", _D * 2),
+        ("disk_on_primary_alt", _D * 2),
     ]
 
 
@@ -125,7 +126,7 @@ def default_mode():
 EXPORTS = (
     "fb_params_default", "fb_params_read_par", "fb_unsupported_name", "fb_planets_read_cfg",
     "fb_init_state", "fb_create", "fb_destroy", "fb_upload", "fb_algogas", "fb_download",
-    "fb_download_derived", "fb_download_crash", "fb_diagnostics", "fb_strerror", "fb_last_error", "fb_stage",
+    "fb_download_derived", "fb_download_crash", "fb_download_sgacc", "fb_diagnostics", "fb_planet_force", "fb_strerror", "fb_last_error", "fb_stage",
     "fb_build_info", "fb_struct_size", "fb_kernel_launches", "fb_profile", "fb_profile_read",
     "fb_select_device", "fb_transport_noalloc", "fb_noalloc_last_error", "fb_init_dust",
     "fb_dust_upload", "fb_dust_download", "fb_vortensity", "fb_batch_create", "fb_batch_algogas",
@@ -166,6 +167,9 @@ def load(mode=None):
         "fb_download": (_I, [vp, C.POINTER(FbState), C.c_uint]),
         "fb_download_derived": (_I, [vp, _I, _P]),
         "fb_diagnostics": (_I, [vp, _P, _P]),
+        "fb_planet_force": (_I, [vp, _D, _D, _D, _D, _P]),
+        "fb_download_sgacc": (_I, [vp, _I, _I, _P, _P]),
+        "fb_download_crash": (_I, [vp, C.POINTER(FbState), _P]),
         "fb_strerror": (C.c_char_p, [_I]),
         "fb_last_error": (C.c_char_p, [vp]),
         "fb_stage": (_I, [vp, _I, _D]),

@@ -367,8 +367,9 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
     const int nb = nr;
     k.n_partial_blocks = nb;
     k.partials = dalloc(ctx, (size_t)nb * 5);
-    ctx->d_diag = dalloc(ctx, (size_t)nb * 2);
-    if (cudaMallocHost((void **)&ctx->h_diag, (size_t)nb * 2 * sizeof(double)) != cudaSuccess) {
+    // per-ring partials of the diagnostics (2 per ring) and of fb_planet_force (4)
+    ctx->d_diag = dalloc(ctx, (size_t)nb * 4);
+    if (cudaMallocHost((void **)&ctx->h_diag, (size_t)nb * 4 * sizeof(double)) != cudaSuccess) {
       fb_destroy(ctx);
       return FB_ERR_NOMEM;
     }
@@ -745,9 +746,14 @@ extern "C" int fb_profile_read(const fb_ctx *ctx, int idx, const char **name, do
   return FB_NSTAGE;
 }
 
-// The DetectCrash bookkeeping of one DT (SourceEuler.c:545-566).
+// The DetectCrash bookkeeping of one DT (SourceEuler.c:545-566), and the
+// disc's pull on the star that AlgoGas leaves in DiskOnPrimaryAcceleration.
 static void report_crash(const fb_ctl *c, fb_step_report *rep)
 {
+  rep->disk_on_primary[0] = c->disk_acc_x;  // DiskOnPrimaryAcceleration of the last substep
+  rep->disk_on_primary[1] = c->disk_acc_y;
+  rep->disk_on_primary_alt[0] = c->disk_acc_alt_x;
+  rep->disk_on_primary_alt[1] = c->disk_acc_alt_y;
   rep->crashes = c->crashes;
   rep->crash_substeps = c->crash_substeps;
   rep->neg_density_substeps = c->neg_dens_substeps;
@@ -890,6 +896,45 @@ extern "C" int fb_diagnostics(fb_ctx *ctx, double *mass, double *momentum)
   }
   if (mass) *mass = m;
   if (momentum) *momentum = p;
+  return FB_OK;
+}
+
+extern "C" int fb_download_sgacc(fb_ctx *ctx, int ring0, int nrings, double *accr, double *acct)
+{
+  if (!ctx || ring0 < 0 || nrings < 0 || ring0 + nrings > ctx->nr) return FB_ERR_INVALID;
+  if (!ctx->sg) return FB_ERR_STATE;
+  const size_t off = (size_t)ring0 * ctx->ns, n = (size_t)nrings * ctx->ns * sizeof(double);
+  if (accr) CK(cudaMemcpyAsync(accr + off, ctx->k.sg_accr + off, n, cudaMemcpyDeviceToHost, ctx->st));
+  if (acct) CK(cudaMemcpyAsync(acct + off, ctx->k.sg_acct + off, n, cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return FB_OK;
+}
+
+extern "C" int fb_planet_force(fb_ctx *ctx, double x, double y, double rsmoothing, double mass, double *out)
+{
+  if (!ctx || !out) return FB_ERR_INVALID;
+  if (!ctx->uploaded) return FB_ERR_STATE;
+  const int nr = ctx->nr;
+  // ComputeForce (Force.c:118-119): star-planet distance and Hill radius
+  const double a = sqrt(x * x + y * y);
+  const double rh = pow(mass / 3., 1. / 3.) * a + 1e-15;
+  const double cutoff = ctx->p.excludehillfactor * rh;  // hillcutfactor of k = 1 (dimfxy = 2)
+  fb_launch_body_force(ctx->k, x, y, rsmoothing, cutoff, ctx->d_diag, ctx->st);
+  ctx->launches += 1;
+  CK(cudaMemcpyAsync(ctx->h_diag, ctx->d_diag, (size_t)nr * 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  // the rings in order, each into the inner or the outer sums (Force.c:218-226)
+  double fxi[2] = {0., 0.}, fxo[2] = {0., 0.}, fyi[2] = {0., 0.}, fyo[2] = {0., 0.};
+  for (int i = 0; i < nr; i++) {
+    const double *p = ctx->h_diag + (size_t)i * 4;
+    if (ctx->g.rmed[i] < a) {
+      fxi[0] += p[0]; fxi[1] += p[1]; fyi[0] += p[2]; fyi[1] += p[3];
+    } else {
+      fxo[0] += p[0]; fxo[1] += p[1]; fyo[0] += p[2]; fyo[1] += p[3];
+    }
+  }
+  out[0] = fxi[0]; out[1] = fxi[1]; out[2] = fxo[0]; out[3] = fxo[1];
+  out[4] = fyi[0]; out[5] = fyi[1]; out[6] = fyo[0]; out[7] = fyo[1];
   return FB_OK;
 }
 

@@ -260,6 +260,8 @@ cudaStream_t fb_ctx_stream(const fb_ctx *ctx);
 void fb_ctx_count_launches(fb_ctx *ctx, int n);
 // diagnostics (fb_diag.cu)
 void fb_launch_vortensity(const KP &k, double *xi, cudaStream_t s);
+void fb_launch_body_force(const KP &k, double x, double y, double rsmoothing, double cutoff, double *part,
+                          cudaStream_t s);
 void fb_launch_ring_mean(const double *f, int nr, int ns, double *out, cudaStream_t s);
 // Lagrangian particles (fb_dust.cu)
 void fb_launch_dust_substep(const KP &k, const PP &pp, cudaStream_t s, cudaEvent_t planets_done);

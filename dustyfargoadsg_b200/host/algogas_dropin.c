@@ -36,9 +36,17 @@ extern boolean BM08, DustFeedback, Write_Temperature, Write_Potential;
 extern boolean DustFeelDisk, DustFeelPlanets, DustFeelTurb, DustFeelSG, DustFeelSGZeroMode;
 extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensity, ZZIntegrator;
 extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
+extern boolean CompareSGAndSummationTorques;
+extern Pair DiskOnPrimaryAcceleration, DiskOnPrimaryAcceleration_alt;
 
 static fb_ctx *g_ctx = NULL;
 static int g_crashes = 0;  /* AlreadyCrashed as last reported */
+static long g_substeps = 0; /* CFL substeps of all DTs so far */
+/* the host state the last DT left behind: downloaded on demand */
+static int g_host_stale = 0, g_sync_always = 0;
+static PolarGrid *g_rho, *g_vrad, *g_vtheta, *g_energy;
+static DustSystem *g_dsys;
+static PlanetarySystem *g_sys;
 
 static void dropin_fail(const char *what, int rc)
 {
@@ -237,6 +245,37 @@ static void write_crash_dumps(PolarGrid *Rho, PolarGrid *Vrad, PolarGrid *Vtheta
   }
 }
 
+long fb_dropin_substeps(void) { return g_substeps; }
+
+/* Brings the fields the last DT left on the GPU (and the particles with the
+   position of the drand48 stream) back into the reference's host arrays. */
+void fb_dropin_sync_host(void)
+{
+  fb_state st;
+  fb_dust_state dst;
+  int rc;
+  if (!g_ctx || !g_host_stale) return;
+  state_views(&st, g_rho, g_vrad, g_vtheta, g_energy);
+  rc = fb_download(g_ctx, &st, FB_F_ALL);
+  if (rc) dropin_fail("fb_download", rc);
+  if (EnergyEquation || Write_Temperature) {
+    rc = fb_download_derived(g_ctx, 0, Temperature->Field);
+    if (rc) dropin_fail("fb_download_derived", rc);
+  }
+  if (Write_Potential) {
+    rc = fb_download_derived(g_ctx, 1, Potential->Field);
+    if (rc) dropin_fail("fb_download_derived", rc);
+  }
+  if (NBPART != 0) {
+    dust_views(&dst, g_dsys);
+    rc = fb_dust_download(g_ctx, &dst);
+    if (rc) dropin_fail("fb_dust_download", rc);
+    rand48_set(dst.rng_x);
+  }
+  g_host_stale = 0;
+}
+#define sync_host fb_dropin_sync_host
+
 void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid *Vtheta,
                        PolarGrid *Energy, PolarGrid *Label, PolarGrid *DRho,
                        PolarGrid *dustpcdens, PolarGrid *DVrad, PolarGrid *DVtheta,
@@ -248,7 +287,10 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
   fb_dust_state dst;
   (void)force; (void)Label; (void)DRho; (void)dustpcdens; (void)DVrad; (void)DVtheta;
   state_views(&st, Rho, Vrad, Vtheta, Energy);
+  g_sys = sys;
   if (!g_ctx) {
+    const char *sync = getenv("FB_DROPIN_SYNC");
+    g_sync_always = (sync && atoi(sync) != 0);
     fb_params p;
     fb_profiles prof;
     params_from_globals(&p);
@@ -301,23 +343,25 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
   }
   rc = fb_algogas(g_ctx, &rep);
   if (rc && rc != FB_ERR_NEGATIVE) dropin_fail("fb_algogas", rc);  /* a crash is not fatal */
-  rc = fb_download(g_ctx, &st, FB_F_ALL);
+  g_substeps += rep.substeps;
+  /* the scalars and the planets every DT; the fields only when a reference
+     routine is about to read them (sync_host, called by the wrappers below) */
+  rc = fb_download(g_ctx, &st, 0u);
   if (rc) dropin_fail("fb_download", rc);
-  if (EnergyEquation || Write_Temperature) fb_download_derived(g_ctx, 0, Temperature->Field);
-  if (Write_Potential) fb_download_derived(g_ctx, 1, Potential->Field);
+  g_rho = Rho; g_vrad = Vrad; g_vtheta = Vtheta; g_energy = Energy; g_dsys = dsys;
+  g_host_stale = 1;
+  if (g_sync_always) sync_host();
   PhysicalTime = st.physical_time;
   LostMass = st.lost_mass;
   MINDT = st.mindt;
   MAXDT = st.maxdt;
+  DiskOnPrimaryAcceleration.x = rep.disk_on_primary[0];
+  DiskOnPrimaryAcceleration.y = rep.disk_on_primary[1];
+  DiskOnPrimaryAcceleration_alt.x = rep.disk_on_primary_alt[0];
+  DiskOnPrimaryAcceleration_alt.y = rep.disk_on_primary_alt[1];
   for (k = 0; k < 3; k++) {
     stardiscbarycenter_x[k] = st.stardiscbarycenter_x[k];
     stardiscbarycenter_y[k] = st.stardiscbarycenter_y[k];
-  }
-  if (NBPART != 0) {
-    dust_views(&dst, dsys);
-    rc = fb_dust_download(g_ctx, &dst);
-    if (rc) dropin_fail("fb_dust_download", rc);
-    rand48_set(dst.rng_x);
   }
   for (k = 0; k < sys->nb; k++) {
     sys->mass[k] = st.planets.mass[k];
@@ -333,4 +377,182 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
   for (k = 0; k < rep.substeps - rep.crash_substeps; k++) masterprint(".");
   for (k = 0; k < rep.crash_substeps; k++) masterprint("c");
   masterprint("\n");
+}
+
+/* ---------------------------------------------------------------------------
+ * The rest of the reference's time loop (main.c:302-397) reads the state
+ * between AlgoGas calls only through the routines below.  Linked with
+ * -Wl,--wrap=<name> for each of them (the drop-in build of oracle/Makefile
+ * does so), the host fields are downloaded only when one of them is about to
+ * read them (outputs, -a monitoring, Stockholm logs), and the two per-DT
+ * planet logs are fed from the GPU instead:
+ *   UpdateLog            the disc's force on each planet by fb_planet_force
+ *                        (ComputeForce on the device density), written
+ *                        exactly as src/Force.c:266-328 writes tqwk*.dat and
+ *                        indtq*.dat;
+ *   compute_selfgravity  the loop's logging call (DeltaT = 0, main.c:316,
+ *                        which only computes the accelerations) on the GPU,
+ *                        with the rings next to the planets brought back for
+ *                        UpdateLogSG.
+ * Before the first AlgoGas (no context yet) every wrapper calls the
+ * reference's own routine.  FB_DROPIN_SYNC=1 in the environment downloads
+ * every field after every DT instead. */
+void __real_SendOutput();
+void __real_UpdateLog();
+void __real_UpdateLogStockholm();
+void __real_compute_selfgravity();
+void __real_CompareSGandSummationTorques();
+void __real_WriteBarycentrePosition();
+void __real_CheckMomentumConservation();
+real __real_GasMomentum();
+real __real_GasTotalMass();
+real __real_GasTotalEnergy();
+void __real_WriteDustSystemFile();
+void __real_WriteJacobi();
+
+void __wrap_SendOutput(int index, PolarGrid *dens, PolarGrid *gasvr, PolarGrid *gasvt, PolarGrid *gasenerg,
+                       PolarGrid *label, PolarGrid *pcdens, PolarGrid *dustdens, PolarGrid *dustvr,
+                       PolarGrid *dustvt, DustSystem *dsys)
+{
+  sync_host();
+  __real_SendOutput(index, dens, gasvr, gasvt, gasenerg, label, pcdens, dustdens, dustvr, dustvt, dsys);
+}
+
+void __wrap_UpdateLog(Force *fc, PlanetarySystem *psys, PolarGrid *Rho, int outputnb, real time)
+{
+  int i, rc;
+  real x, y, r, m, vx, vy, smoothing, f[8];
+  FILE *out;
+  char filename[MAX1D];
+  if (!g_ctx || !g_host_stale) {
+    __real_UpdateLog(fc, psys, Rho, outputnb, time);
+    return;
+  }
+  for (i = 0; i < psys->nb; i++) {
+    x = psys->x[i];
+    y = psys->y[i];
+    vx = psys->vx[i];
+    vy = psys->vy[i];
+    r = sqrt(x * x + y * y);
+    m = psys->mass[i];
+    if (RocheSmoothing)
+      smoothing = r * pow(m / 3., 1. / 3.) * ROCHESMOOTHING;
+    else
+      smoothing = compute_smoothing(r);
+    rc = fb_planet_force(g_ctx, x, y, smoothing, m, f);
+    if (rc) dropin_fail("fb_planet_force", rc);
+    fc->fx_inner = f[0]; fc->fx_ex_inner = f[1]; fc->fx_outer = f[2]; fc->fx_ex_outer = f[3];
+    fc->fy_inner = f[4]; fc->fy_ex_inner = f[5]; fc->fy_outer = f[6]; fc->fy_ex_outer = f[7];
+    sprintf(filename, "%stqwk%d.dat", OUTPUTDIR, i);
+    out = fopen(filename, "a");
+    if (out == NULL) {
+      fprintf(stderr, "Can't open %s\n", filename);
+      prs_exit(1);
+    }
+    fprintf(out, "%d\t%.18g\t%.18g\t%.18g\t%.18g\t%.18g\t%.18g\t%.18g\t%.18g\t%.18g\n", outputnb,
+            x * fc->fy_inner - y * fc->fx_inner, x * fc->fy_outer - y * fc->fx_outer,
+            x * fc->fy_ex_inner - y * fc->fx_ex_inner, x * fc->fy_ex_outer - y * fc->fx_ex_outer,
+            vx * fc->fx_inner + vy * fc->fy_inner, vx * fc->fx_outer + vy * fc->fy_outer,
+            vx * fc->fx_ex_inner + vy * fc->fy_ex_inner, vx * fc->fx_ex_outer + vy * fc->fy_ex_outer, time);
+    fclose(out);
+    sprintf(filename, "%sindtq%d.dat", OUTPUTDIR, i);
+    out = fopen(filename, "a");
+    if (out == NULL) {
+      fprintf(stderr, "Can't open %s\n", filename);
+      prs_exit(1);
+    }
+    fprintf(out, "%d\t%.18g\t%.18g\n", outputnb,
+            -x * DiskOnPrimaryAcceleration.y + y * DiskOnPrimaryAcceleration.x, time);
+    fclose(out);
+  }
+}
+
+void __wrap_UpdateLogStockholm(PlanetarySystem *sys, PolarGrid *Rho, int outputnb, real time)
+{
+  sync_host();
+  __real_UpdateLogStockholm(sys, Rho, outputnb, time);
+}
+
+void __wrap_compute_selfgravity(PolarGrid *Rho, PolarGrid *Vr, PolarGrid *Vt, PolarGrid *DVr, PolarGrid *DVt,
+                                real DeltaT, boolean SGUpdate)
+{
+  int k, ip, lo, hi, rc;
+  real rp;
+  if (!g_ctx || DeltaT != 0.0 || SGZeroMode || !g_host_stale) {
+    sync_host();
+    __real_compute_selfgravity(Rho, Vr, Vt, DVr, DVt, DeltaT, SGUpdate);
+    return;
+  }
+  /* the accelerations of the current density (compute_fftdensity and
+     compute_sgacc, src/sgmain.c:23-28); the velocity update with DeltaT = 0
+     changes nothing */
+  rc = fb_stage(g_ctx, FB_STAGE_SELFGRAV, 0.0);
+  if (rc) dropin_fail("fb_stage(SELFGRAV)", rc);
+  if (CompareSGAndSummationTorques) {
+    rc = fb_download_sgacc(g_ctx, 0, NRAD, gr->Field, gtheta->Field);
+    if (rc) dropin_fail("fb_download_sgacc", rc);
+  } else if (g_sys) {
+    /* UpdateLogSG (src/Force.c:369-420) reads the rings ip-1 .. ip+1 around
+       each planet inside the grid */
+    for (k = 0; k < g_sys->nb; k++) {
+      rp = sqrt(g_sys->x[k] * g_sys->x[k] + g_sys->y[k] * g_sys->y[k]);
+      if (rp < Rinf[0] || rp >= Rsup[NRAD - 1]) continue;
+      ip = 0;
+      while (ip < NRAD && rp >= Rinf[ip]) ip++;
+      ip--;
+      lo = ip - 2 < 0 ? 0 : ip - 2;
+      hi = ip + 2 > NRAD - 1 ? NRAD - 1 : ip + 2;
+      rc = fb_download_sgacc(g_ctx, lo, hi - lo + 1, gr->Field, gtheta->Field);
+      if (rc) dropin_fail("fb_download_sgacc", rc);
+    }
+  }
+  SG_initcounter++;
+}
+
+void __wrap_CompareSGandSummationTorques(Force *force, PolarGrid *Rho, PlanetarySystem *sys)
+{
+  sync_host();
+  __real_CompareSGandSummationTorques(force, Rho, sys);
+}
+
+void __wrap_WriteBarycentrePosition(PolarGrid *Rho)
+{
+  sync_host();
+  __real_WriteBarycentrePosition(Rho);
+}
+
+void __wrap_CheckMomentumConservation(PolarGrid *Density, PolarGrid *Vtheta, PlanetarySystem *sys)
+{
+  sync_host();
+  __real_CheckMomentumConservation(Density, Vtheta, sys);
+}
+
+real __wrap_GasMomentum(PolarGrid *Density, PolarGrid *Vtheta)
+{
+  sync_host();
+  return __real_GasMomentum(Density, Vtheta);
+}
+
+real __wrap_GasTotalMass(PolarGrid *array)
+{
+  sync_host();
+  return __real_GasTotalMass(array);
+}
+
+real __wrap_GasTotalEnergy(PolarGrid *Rho, PolarGrid *Vr, PolarGrid *Vt, PolarGrid *Energy)
+{
+  sync_host();
+  return __real_GasTotalEnergy(Rho, Vr, Vt, Energy);
+}
+
+void __wrap_WriteDustSystemFile(DustSystem *dsys, int index)
+{
+  sync_host();
+  __real_WriteDustSystemFile(dsys, index);
+}
+
+void __wrap_WriteJacobi(DustSystem *dsys, PlanetarySystem *sys, int k)
+{
+  sync_host();
+  __real_WriteJacobi(dsys, sys, k);
 }

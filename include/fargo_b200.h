@@ -172,6 +172,13 @@ typedef struct fb_step_report {
                             density somewhere (not a crash for AlgoGas)  */
   double crash_time;     /* timeCRASH: PhysicalTime of the first crash
                             (src/SourceEuler.c:551); 0 if none           */
+  double disk_on_primary[2]; /* DiskOnPrimaryAcceleration (x, y) of the last
+                            substep (src/SourceEuler.c:482), which the
+                            reference's planet logs read after AlgoGas    */
+  double disk_on_primary_alt[2]; /* DiskOnPrimaryAcceleration_alt (x, y), the
+                            barycentre's finite-difference version
+                            (src/SideEuler.c:91-112), for the
+                            compindirectterm.dat output (src/Output.c)   */
 } fb_step_report;
 
 /* Lagrangian dust particles (src/types.h:114-146, the fields the step
@@ -256,9 +263,24 @@ int fb_download_crash(fb_ctx *ctx, fb_state *st, double *crash_time);
    3 SoundSpeed, 4 DivergenceVelocity, 5 ViscHeat, 6 SG radial acceleration
    (SG_Accr, src/sgacc.c:152-161), 7 SG azimuthal acceleration (SG_Acct). */
 int fb_download_derived(fb_ctx *ctx, int which, double *out);
+/* Rings [ring0, ring0+nrings) of the self-gravity accelerations last
+   computed (by the step, or by fb_stage(.., FB_STAGE_SELFGRAV, ..)): SG_Accr
+   and SG_Acct of src/sgacc.c:152-161, into accr / acct (either may be NULL)
+   at their own offsets of (nrad+1)*nsec arrays.  The reference's planet log
+   UpdateLogSG (src/Force.c:331) reads only the rings next to each planet. */
+int fb_download_sgacc(fb_ctx *ctx, int ring0, int nrings, double *accr, double *acct);
 /* Diagnostics on the device state: GasTotalMass (src/SideEuler.c:15) and
    GasMomentum (src/SideEuler.c:114). */
 int fb_diagnostics(fb_ctx *ctx, double *mass, double *momentum);
+/* ComputeForce (src/Force.c:77-253) of the disc's current density on a body
+   at (x, y) with smoothing length rsmoothing and mass `mass`, with the Hill
+   cut of EXCLUDEHILLFACTOR: out[8] = fx_inner, fx_ex_inner, fx_outer,
+   fx_ex_outer, fy_inner, fy_ex_inner, fy_outer, fy_ex_outer (the Force
+   fields).  Summed per ring on the device, then over the rings in ring
+   order (about 1e-16 relative from the reference's single sequential sum).
+   It serves the per-DT planet logs (UpdateLog, src/Force.c:266-328) without
+   a download of the density. */
+int fb_planet_force(fb_ctx *ctx, double x, double y, double rsmoothing, double mass, double *out);
 /* ---- launch shapes (no counterpart in the reference) ---------------------
    CTA width of the per-cell kernels (32..256, multiple of 32), cells per
    thread of the azimuthal transport (1..4), columns (32/64/128) and rings

@@ -29,7 +29,9 @@
  *   DumpSources      (LowTasks.c:133) becomes a no-op (it shells out to cp).
  *
  * At exit it prints one line "ORACLE_TIMING {json}" on stderr with the
- * wall time spent inside AlgoGas, the substep count and cell-updates/s.
+ * wall time spent inside AlgoGas, the substep count, cell-updates/s and the
+ * wall time of the time loop from the first AlgoGas call to the end of the
+ * last one (AlgoGas plus the loop's logs and outputs between the calls).
  *
  * Dump format ("FBD1"): one ASCII JSON header line, then raw little-endian
  * doubles.  The header lists {"name": [offset_in_doubles, count], ...} and
@@ -46,6 +48,8 @@ void __real_UpdateVelocitiesWithViscosity();
 void __real_ApplyBoundaryCondition();
 void __real_EvanescentBoundary();
 #ifdef FB_DROPIN
+long fb_dropin_substeps(void);
+void fb_dropin_sync_host(void);
 void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad,
                        PolarGrid *Vtheta, PolarGrid *Energy, PolarGrid *Label,
                        PolarGrid *DRho, PolarGrid *dustpcdens,
@@ -58,6 +62,8 @@ extern boolean SelfGravity, SGZeroMode;
 
 static double h_time_in_algogas = 0.0;
 static double h_call_start = 0.0;
+static double h_loop_start = -1.0, h_loop_end = 0.0;  /* first timed AlgoGas start, last AlgoGas end */
+static long h_loop_calls0 = 0, h_loop_substeps0 = 0;
 static long h_substeps = 0;
 static long h_calls = 0;
 static int h_atexit_set = 0;
@@ -80,8 +86,11 @@ static void print_timing(void)
   const char *tf = getenv("ORACLE_TIMING_FILE");
   snprintf(line, sizeof line,
            "{\"wall_s\": %.9g, \"substeps\": %ld, \"algogas_calls\": %ld, "
-           "\"nrad\": %d, \"nsec\": %d, \"cell_updates_per_s\": %.9g}",
-           h_time_in_algogas, h_substeps, h_calls, GLOBALNRAD, NSEC, rate);
+           "\"nrad\": %d, \"nsec\": %d, \"cell_updates_per_s\": %.9g, \"loop_wall_s\": %.9g, "
+           "\"loop_calls\": %ld, \"loop_substeps\": %ld}",
+           h_time_in_algogas, h_substeps, h_calls, GLOBALNRAD, NSEC, rate,
+           h_loop_start >= 0.0 ? h_loop_end - h_loop_start : 0.0, h_calls - h_loop_calls0,
+           h_substeps - h_loop_substeps0);
   fprintf(stderr, "ORACLE_TIMING %s\n", line);
   if (tf && (f = fopen(tf, "w")) != NULL) {
     fprintf(f, "%s\n", line);
@@ -353,6 +362,15 @@ void __wrap_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad,
     dump_state("state_init", Rho, Vrad, Vtheta, Energy, sys, dsys);
   }
   h_call_start = now_s();
+  {
+    /* ORACLE_TIMING_SKIP=W starts the loop clock at call W (warm-up calls) */
+    const char *sk = getenv("ORACLE_TIMING_SKIP");
+    if (h_loop_start < 0.0 && h_calls >= (sk ? atol(sk) : 0L)) {
+      h_loop_start = h_call_start;
+      h_loop_calls0 = h_calls;
+      h_loop_substeps0 = h_substeps;
+    }
+  }
   h_in_algogas = 1;
 #ifdef FB_DROPIN
   fb_dropin_AlgoGas(force, Rho, Vrad, Vtheta, Energy, Label, DRho, dustpcdens,
@@ -361,11 +379,18 @@ void __wrap_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad,
   __real_AlgoGas(force, Rho, Vrad, Vtheta, Energy, Label, DRho, dustpcdens,
                  DVrad, DVtheta, sys, dsys);
 #endif
-  h_time_in_algogas += now_s() - h_call_start;
+  h_loop_end = now_s();
+  h_time_in_algogas += h_loop_end - h_call_start;
   h_in_algogas = 0;
   h_calls++;
+#ifdef FB_DROPIN
+  h_substeps = fb_dropin_substeps();  /* the drop-in's count: Transport is not called */
+#endif
   if (every > 0 && (h_calls % every) == 0) {
     snprintf(tag, sizeof tag, "state_%05ld", h_calls);
+#ifdef FB_DROPIN
+    fb_dropin_sync_host();  /* the drop-in brings fields back only on demand */
+#endif
     dump_state(tag, Rho, Vrad, Vtheta, Energy, sys, dsys);
   }
 }
