@@ -508,9 +508,10 @@ def batch_cpu_baseline(wd, cells, subs_per_dt, orbits_per_dt, budget_s=24.0):
     """The batched sweep on the host: one process of the reference's own
     build (oracle/_ref) per disc, as many at once as there are cores, each
     timed on a bounded sample of its own substeps (time inside AlgoGas).
-    A disc's orbits/s is its substep rate over its substeps per DT (as the
-    GPU took them) times the orbits per DT; the sweep's rate on all cores is
-    the sum over discs times min(1, cores / discs)."""
+    One DT of a disc costs its substeps per DT (as the GPU took them) at its
+    measured substep rate; the cores share the discs, so one DT of every disc
+    takes the sum of those costs over the cores.  Orbits/s counts the orbits
+    of all discs, like the GPU figure."""
     import concurrent.futures as cf
 
     from tests import _oracle  # test infrastructure: the CPU baseline only
@@ -530,12 +531,15 @@ def batch_cpu_baseline(wd, cells, subs_per_dt, orbits_per_dt, budget_s=24.0):
 
     with cf.ThreadPoolExecutor(max_workers=cores) as ex:
         timings = list(ex.map(one, range(n)))
-    rates = [t["substeps"] / t["wall_s"] / max(s, 1) * orbits_per_dt for t, s in zip(timings, subs_per_dt)]
-    value = sum(rates) * min(1.0, cores / n)
+    # seconds one core needs for one DT of each disc; the cores share the
+    # discs, so one DT of all of them takes their sum over the cores
+    t_dt = [max(s, 1) * t["wall_s"] / t["substeps"] for t, s in zip(timings, subs_per_dt)]
+    value = n * orbits_per_dt / (sum(t_dt) / min(cores, n))
     return {"value": value, "unit": "orbits/s", "cores": cores, "kind": "reference",
             "sample": "each of the %d discs run alone by the reference's build for about %.1f s of substeps "
-                      "(%d at a time); orbits/s per disc from its substep rate and the GPU's substeps per DT"
-                      % (n, per_disc, min(cores, n))}
+                      "(%d at a time); a DT of a disc costs its substeps per DT (as the GPU took them) at its "
+                      "measured substep rate, and the %d cores share the %d discs' DTs"
+                      % (n, per_disc, min(cores, n), min(cores, n), n)}
 
 
 if __name__ == "__main__":

@@ -1299,7 +1299,7 @@ extern "C" int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t)
   if (t->rad_columns && (t->rad_columns < 32 || t->rad_columns > 128 || t->rad_columns % 32)) return FB_ERR_INVALID;
   if (t->rad_rings < 0 || t->rad_rings > k.nr) return FB_ERR_INVALID;
   const int E = t->azi_cells_per_thread ? t->azi_cells_per_thread : fb_azi_E_auto(k.ns);
-  if (t->azi_variant < 0 || t->azi_variant > 3 || !fb_azi_variant(k.ns, k.energy, E, t->azi_variant))
+  if (t->azi_variant < 0 || t->azi_variant > 5 || !fb_azi_variant(k.ns, k.energy, E, t->azi_variant))
     return FB_ERR_INVALID;
   k.cell_bs = cb;
   k.azi_variant = t->azi_variant;
@@ -1416,7 +1416,7 @@ extern "C" int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_ou
     double bestms = 1e300;
     for (int E = 1; E <= 4; E++) {
       if (!fb_azi_E_valid(k.ns, k.energy, E)) continue;
-      for (int var = 1; var <= 3; var++) {
+      for (int var = 1; var <= 5; var++) {
         if (fb_azi_variant(k.ns, k.energy, E, var) != var) continue;
         k.azi_E = E;
         k.azi_variant = var;

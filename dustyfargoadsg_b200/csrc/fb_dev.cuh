@@ -111,7 +111,8 @@ struct KP {
 };
 
 // Device state of the particles' random stream (src/DustUpdate.c:438-485).
-// a / d rounded to nearest, given r = 1/d rounded to nearest: y = RN(a r) is
+// a / d rounded to nearest, given r = 1/d rounded to nearest (fb_rcp in the
+// parity build): y = RN(a r) is
 // within one ulp of a/d, its remainder a - d y is exact in one fma, and
 // RN(y + r (a - d y)) = RN(a / d) (Markstein's theorem: P. Markstein, IBM J.
 // Res. Dev. 34(1), 1990; J.-M. Muller et al., Handbook of Floating-Point
@@ -144,6 +145,40 @@ static __device__ __forceinline__ double fb_vl_quot(double a, double b)
   return a * r;
 #else
   return a / b;
+#endif
+}
+
+// 1/d for the shared-divisor quotients fb_quot.  Parity build: correctly
+// rounded (IEEE division), which makes fb_quot exact.  Fast build: the
+// approximate reciprocal refined by two Newton-Raphson steps (a few ulp), so
+// that fb_quot is within a few ulp of the quotient.
+static __device__ __forceinline__ double fb_rcp(double d)
+{
+#if FB_FAST
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(d));
+  double e = fma(-d, r, 1.0);
+  r = fma(r, e, r);
+  e = fma(-d, r, 1.0);
+  return fma(r, e, r);
+#else
+  return 1.0 / d;
+#endif
+}
+
+// The van Leer slope of the azimuthal pass from the differences dq- and dq+
+// of a quantity across a cell, times invdx: dq+ dq- / (dq+ + dq-) invdx where
+// dq+ dq- > 0, else 0 (TransportEuler.c:392-433).  The fast build evaluates
+// the quotient in every lane and selects afterwards, so that the slopes of a
+// thread's cells run side by side instead of behind a branch each.
+static __device__ __forceinline__ double fb_vl_slope(double dqm, double dqp, double invdx)
+{
+#if FB_FAST
+  const double num = dqp * dqm;
+  const double v = fb_vl_quot(num, dqp + dqm) * invdx;
+  return (num > 0.0) ? v : 0.0;
+#else
+  return (dqp * dqm > 0.0) ? fb_vl_quot(dqp * dqm, dqp + dqm) * invdx : 0.0;
 #endif
 }
 

@@ -1054,7 +1054,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
       if (NQ == 6) qv[1] = w.u1;
       qv[NH - 1] = r;
     }
-    const double den = r + 1e-20, rden = 1.0 / den;
+    const double den = r + 1e-20, rden = fb_rcp(den);
 #pragma unroll
     for (int q = 0; q < NH; q++) { Qo[q][slot] = qv[q]; W[q][slot] = fb_quot(qv[q], den, rden); }  // qv / den
     R[slot] = r;
@@ -1655,6 +1655,412 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
   }
 }
 
+// Register variant of the azimuthal pass (variant 4).  Thread t owns the E
+// contiguous cells c0 = t E .. t E + E - 1 of its ring (nsec = E T with T a
+// multiple of 32); every quantity of its cells stays in registers, loaded as
+// 16-byte pairs along the azimuth.  A neighbour's value crosses lanes by a
+// warp shuffle and warps through a small double-buffered halo in shared
+// memory (one barrier per exchange).  Each face flux is evaluated once, by the
+// owner of the cell above the face, and reaches the cell below through the
+// next exchange; the quantities are advanced one after another, so only one
+// quantity's quotients, slopes and fluxes are live at a time.  The arithmetic
+// is that of the other variants, operation for operation, and the ring mean
+// adds the same cells in the same order (thread t's cells t, t + T, ...), so
+// for the same E the results agree to the last bit.
+#define AZR_MAXW 32  // warps per CTA
+#define AZR_NV 2     // values per exchange and side
+#define AZR_MAXT 768  // threads per CTA (each kernel instance is bounded by its own MT <= 768)
+
+// The left neighbour's last-cell values rL (nl of them, from sL of the thread
+// before) and the right neighbour's first-cell values rR (from sR of the
+// thread after), around the ring.
+template <int NL, int NR>
+static __device__ __forceinline__ void azr_exchange(double (*hal)[2][AZR_MAXW][AZR_NV], int &xb, int lane, int w,
+                                                    int wl, int wr, const double *sL, double *rL, const double *sR,
+                                                    double *rR)
+{
+#pragma unroll
+  for (int v = 0; v < NL; v++) rL[v] = __shfl_up_sync(0xffffffffu, sL[v], 1);
+#pragma unroll
+  for (int v = 0; v < NR; v++) rR[v] = __shfl_down_sync(0xffffffffu, sR[v], 1);
+  if (lane == 31)
+#pragma unroll
+    for (int v = 0; v < NL; v++) hal[xb][0][w][v] = sL[v];
+  if (lane == 0)
+#pragma unroll
+    for (int v = 0; v < NR; v++) hal[xb][1][w][v] = sR[v];
+  __syncthreads();
+  if (lane == 0)
+#pragma unroll
+    for (int v = 0; v < NL; v++) rL[v] = hal[xb][0][wl][v];
+  if (lane == 31)
+#pragma unroll
+    for (int v = 0; v < NR; v++) rR[v] = hal[xb][1][wr][v];
+  xb ^= 1;
+}
+
+template <int E>
+static __device__ __forceinline__ void azr_load(const double *p, double (&v)[E])
+{
+  if ((E & 1) == 0) {
+#pragma unroll
+    for (int h = 0; h < E / 2; h++) {
+      const double2 x = ((const double2 *)p)[h];
+      v[2 * h] = x.x;
+      v[2 * h + 1] = x.y;
+    }
+  } else {
+#pragma unroll
+    for (int e = 0; e < E; e++) v[e] = p[e];
+  }
+}
+
+// One ring of the register variant: the quantities q0 and vtheta vt of the
+// thread's own cells (loaded by the caller), vs = vtheta of cells tid, tid + T,
+// ... (the ring mean's order).  The results of own cell c0 + e land at cell
+// p = c0 + e + nshift (mod nsec): out(e, p, vtheta, density, RadMomP,
+// RadMomM, energy).
+template <int NQ, int E, class Out>
+static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, double (&q0)[NQ][E],
+                                                const double (&vt)[E], const double (&vs)[E], double *sh,
+                                                double (*hal)[2][AZR_MAXW][AZR_NV], int &xb, Out out)
+{
+  const int ns = k.ns, nr = k.nr, T = blockDim.x, tid = threadIdx.x;
+  const int lane = tid & 31, w = tid >> 5, nw = T >> 5;
+  const int wl = (w == 0) ? nw - 1 : w - 1, wr = (w == nw - 1) ? 0 : w + 1;
+  const int c0 = tid * E;
+  constexpr int RH = NQ - 1;  // the density is the last quantity
+#define AZR_X(NL, NR, sL, rL, sR, rR) azr_exchange<NL, NR>(hal, xb, lane, w, wl, wr, sL, rL, sR, rR)
+  // ComputeThetaElongations / ComputeAverageThetaVelocities / ComputeResiduals
+  const double invdt = 1.0 / dt;
+  double s = 0.0;
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    double elong = vs[e] * dt;
+    s += elong * invdt;
+  }
+  s = block_sum_dyn(s, sh);
+  const double VMed = s / (double)ns;
+  // ComputeConstantResidual (TransportEuler.c:310-348)
+  const double dpinvns = (k.pmax - k.pmin) / (double)ns;
+  const double Ntilde = VMed * k.invrmed[i] * dt * (double)ns / (k.pmax - k.pmin);
+  const double Nround = floor(Ntilde + 0.5);
+  const long nshift = (long)Nround;
+  double vconst = (Ntilde - Nround) * k.rmed[i] * invdt * dpinvns;
+  const double vconst0 = vconst;
+  auto vres_of = [&](double vtj) -> double {
+    double elong = vtj * dt;
+    double v = elong * invdt - VMed;
+    if (!k.fast_transport) v = vconst0 + v;
+    return v;
+  };
+  if (!k.fast_transport) vconst = 0.0;
+  const double dxtheta = k.dxtheta[i], invdxtheta = k.invdxtheta[i];
+  const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
+  const double invsurf = 1.0 / k.surf[i];
+  for (int pass = 0; pass < 2; pass++) {
+    const bool uniform = (pass == 1);
+    if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
+    // lower face e of the own cell c0 + e: velocity, upwind side (left when
+    // the displacement is positive) and the factor of its star value
+    double V[E], f[E];
+    bool upl[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      V[e] = uniform ? vconst : vres_of(vt[e]);
+      const double kf = V[e] * dt;
+      upl[e] = (kf > 0.0);
+      f[e] = upl[e] ? (dxtheta - kf) : -(dxtheta + kf);
+    }
+    // RhoStar (ComputeStarTheta(Rho, V, RhoStar)): density slopes
+    double rL[1], rR[1];
+    {
+      const double sL[1] = {q0[RH][E - 1]}, sR[1] = {q0[RH][0]};
+      AZR_X(1, 1, sL, rL, sR, rR);
+    }
+    double DR[E], den[E], rden[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const double rm = (e == 0) ? rL[0] : q0[RH][e - 1], r0 = q0[RH][e];
+      const double rp = (e == E - 1) ? rR[0] : q0[RH][e + 1];
+      const double dqm = (r0 - rm), dqp = (rp - r0);
+      DR[e] = fb_vl_slope(dqm, dqp, invdxtheta);
+      den[e] = r0 + 1e-20;
+      rden[e] = fb_rcp(den[e]);
+    }
+    // quotients q / (rho + 1e-20) of the first quantity, with the left
+    // neighbour's density slope
+    double W[E], WL, WR;
+#pragma unroll
+    for (int e = 0; e < E; e++) W[e] = fb_quot(q0[0][e], den[e], rden[e]);
+    double DRL;
+    {
+      const double sL[2] = {W[E - 1], DR[E - 1]}, sR[1] = {W[0]};
+      double xl[2], xr[1];
+      AZR_X(2, 1, sL, xl, sR, xr);
+      WL = xl[0];
+      DRL = xl[1];
+      WR = xr[0];
+    }
+    double RS[E];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      const double ru = upl[e] ? ((e == 0) ? rL[0] : q0[RH][e - 1]) : q0[RH][e];
+      const double du = upl[e] ? ((e == 0) ? DRL : DR[e - 1]) : DR[e];
+      RS[e] = ru + f[e] * du;
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      // van Leer slopes of the quotients (ComputeStarTheta)
+      double D[E];
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const double wm = (e == 0) ? WL : W[e - 1], w0 = W[e], wp = (e == E - 1) ? WR : W[e + 1];
+        const double dqm = (w0 - wm), dqp = (wp - w0);
+        D[e] = fb_vl_slope(dqm, dqp, invdxtheta);
+      }
+      double DL;
+      {
+        const double sL[1] = {D[E - 1]};
+        double xl[1];
+        AZR_X(1, 0, sL, xl, sL, xl);
+        DL = xl[0];
+      }
+      // star value and flux at each own lower face (VanLeerTheta)
+      double F[E];
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const double ws = upl[e] ? ((e == 0) ? WL : W[e - 1]) : W[e];
+        const double ds = upl[e] ? ((e == 0) ? DL : D[e - 1]) : D[e];
+        const double qs = ws + f[e] * ds;
+        F[e] = dxrad * qs * RS[e] * V[e];
+      }
+      // the next quantity's quotients travel with this one's first flux
+      double Wn[E], WnL = 0.0, WnR = 0.0, FR;
+      if (q + 1 < NQ) {
+#pragma unroll
+        for (int e = 0; e < E; e++) Wn[e] = fb_quot(q0[(q + 1 < NQ) ? q + 1 : q][e], den[e], rden[e]);
+        const double sL[1] = {Wn[E - 1]}, sR[2] = {F[0], Wn[0]};
+        double xl[1], xr[2];
+        AZR_X(1, 2, sL, xl, sR, xr);
+        FR = xr[0];
+        WnR = xr[1];
+        WnL = xl[0];
+      } else {
+        const double sR[1] = {F[0]};
+        double xr[1];
+        AZR_X(0, 1, sR, xr, sR, xr);
+        FR = xr[0];
+      }
+#pragma unroll
+      for (int e = 0; e < E; e++) {
+        const double Fh = (e == E - 1) ? FR : F[e + 1];
+        double varq = F[e];
+        varq -= Fh;
+        q0[q][e] = q0[q][e] + varq * invsurf;
+      }
+      if (q + 1 < NQ) {
+#pragma unroll
+        for (int e = 0; e < E; e++) W[e] = Wn[e];
+        WL = WnL;
+        WR = WnR;
+      }
+    }
+  }
+  // AdvectSHIFT (TransportEuler.c:350-373): cell c goes to c + nshift (mod
+  // ns); ComputeVelocities' vtheta (TransportEuler.c:515-547) from the
+  // pre-shift neighbours, floors on energy, sub-Keplerian edges
+  int shift = (int)(nshift % ns);
+  if (shift < 0) shift += ns;
+  double xl[2];
+  {
+    const double sL[2] = {q0[2][E - 1], q0[RH][E - 1]};  // ThetaMomP and the density of the cell before
+    AZR_X(2, 0, sL, xl, sL, xl);
+  }
+#undef AZR_X
+  const int subkep = (!k.transport_only) && (i == 0 || i == nr - 1);
+  const double rmi = k.rmed[i];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    int p = c0 + e + shift;
+    if (p >= ns) p -= ns;
+    const double tpm = (e == 0) ? xl[0] : q0[2][e - 1], rm = (e == 0) ? xl[1] : q0[RH][e - 1];
+    double v = (tpm + q0[3][e]) / (q0[RH][e] + rm + 1e-20) / rmi - rmi * k.omega_frame;
+    if (subkep) v = k.vthetamed[i] - rmi * k.omega_frame;
+    double en = 0.0;
+    if (NQ == 6) {
+      en = q0[(NQ == 6) ? 4 : 0][e];
+      if (k.add_floors && !k.transport_only) {
+        double e_bottom = 1e-3 * k.energymed[i];
+        if (en < e_bottom) en = e_bottom;
+      }
+    }
+    out(p, v, q0[RH][e], q0[0][e], q0[1][e], en);
+  }
+}
+
+template <int NQ, int E, int MT>
+__global__ void __launch_bounds__(MT) k_transport_azimuthal_reg(KP k, double dtov)
+{
+  fb_grid_dependency();
+  __shared__ double sh[32];
+  __shared__ double hal[2][2][AZR_MAXW][AZR_NV];  // [buffer][0 last cells, 1 first cells][warp][value]
+  const double dt = dt_of(k, dtov);
+  const int i = blockIdx.x, ns = k.ns, T = blockDim.x, tid = threadIdx.x;
+  const size_t base = (size_t)i * ns;
+  const int c0 = tid * E;
+  int xb = 0;
+  // every global load at once: the own cells' quantities and vtheta, and
+  // vtheta of the cells the ring mean of the other variants gives this thread
+  double q0[NQ][E], vt[E], vs[E];
+#pragma unroll
+  for (int q = 0; q < NQ; q++) azr_load<E>(k.q[q] + base + c0, q0[q]);
+  azr_load<E>(k.vt + base + c0, vt);
+#pragma unroll
+  for (int e = 0; e < E; e++) vs[e] = k.vt[base + tid + e * T];
+  azr_ring<NQ, E>(k, dt, i, q0, vt, vs, sh, hal, xb,
+                  [&](int p, double v, double r, double a, double b, double en) {
+                    k.vt[base + p] = v;
+                    k.rho_t[base + p] = r;
+                    k.q[0][base + p] = a;
+                    k.q[1][base + p] = b;
+                    if (NQ == 6) k.e[base + p] = en;
+                  });
+}
+
+// Staged variant of the azimuthal pass (variant 5): the register variant's
+// arithmetic in a persistent kernel (one CTA per SM, rings i = blockIdx.x,
+// blockIdx.x + gridDim.x, ...).  A ring's NQ quantities and vtheta arrive in
+// shared memory by bulk asynchronous copies (cp.async.bulk, completion on an
+// mbarrier) issued one ring ahead, so the next ring's loads overlap this
+// ring's arithmetic; the results are written back into the same buffer at
+// their shifted cells and leave by bulk copies too, one contiguous row per
+// field.  Two buffers of NQ + 1 rows of nsec doubles.  Every wait is bounded:
+// a copy that never completes sets FB_ERR_TIMEOUT in the control block and the
+// CTA stops.
+static __device__ __forceinline__ unsigned azs_smem(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+static __device__ __forceinline__ void azs_expect(unsigned long long *bar, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(azs_smem(bar)), "r"(bytes)
+               : "memory");
+}
+static __device__ __forceinline__ void azs_load(void *dst, const void *src, unsigned bytes, unsigned long long *bar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   azs_smem(dst)),
+               "l"(src), "r"(bytes), "r"(azs_smem(bar))
+               : "memory");
+}
+static __device__ __forceinline__ void azs_store(void *dst, const void *src, unsigned bytes)
+{
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(azs_smem(src)),
+               "r"(bytes)
+               : "memory");
+}
+// bounded wait for phase `parity` of the mbarrier: false after `limit` tries
+static __device__ __forceinline__ bool azs_wait(unsigned long long *bar, unsigned parity, long long limit)
+{
+  for (long long it = 0; it < limit; it++) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(azs_smem(bar)), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+#define AZS_WAIT_LIMIT (1LL << 22)  // try_wait calls (each may suspend for a while): seconds, not forever
+
+template <int NQ, int E, int MT>
+__global__ void __launch_bounds__(MT) k_transport_azimuthal_staged(KP k, double dtov)
+{
+  fb_grid_dependency();
+  extern __shared__ double2 azs_dyn[];
+  __shared__ double sh[32];
+  __shared__ double hal[2][2][AZR_MAXW][AZR_NV];
+  __shared__ __align__(8) unsigned long long bar[2];
+  __shared__ int failed;
+  const double dt = dt_of(k, dtov);
+  const int ns = k.ns, nr = k.nr, T = blockDim.x, tid = threadIdx.x;
+  const int c0 = tid * E;
+  constexpr int NB = NQ + 1;  // rows per ring: the quantities and vtheta
+  double *buf = (double *)azs_dyn;
+  const unsigned row_bytes = (unsigned)ns * 8u;
+  int xb = 0;
+  // the rows of ring r into buffer b (one thread)
+  auto issue = [&](int r, int b) {
+    const size_t base = (size_t)r * ns;
+    azs_expect(&bar[b], NB * row_bytes);
+#pragma unroll
+    for (int q = 0; q < NQ; q++) azs_load(buf + (size_t)(b * NB + q) * ns, k.q[q] + base, row_bytes, &bar[b]);
+    azs_load(buf + (size_t)(b * NB + NQ) * ns, k.vt + base, row_bytes, &bar[b]);
+  };
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(azs_smem(&bar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(azs_smem(&bar[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    failed = 0;
+    if ((int)blockIdx.x < nr) issue(blockIdx.x, 0);
+  }
+  __syncthreads();
+  int it = 0;
+  for (int i = blockIdx.x; i < nr; i += gridDim.x, it++) {
+    const int b = it & 1;
+    const size_t base = (size_t)i * ns;
+    // the next ring into the other buffer, once the bulk stores of the ring
+    // it held last have read it
+    if (tid == 0 && i + (int)gridDim.x < nr) {
+      asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+      issue(i + gridDim.x, b ^ 1);
+    }
+    if (!azs_wait(&bar[b], (unsigned)((it >> 1) & 1), AZS_WAIT_LIMIT)) failed = 1;
+    __syncthreads();
+    if (failed) break;
+    const double *rows = buf + (size_t)b * NB * ns;
+    double q0[NQ][E], vt[E], vs[E];
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+#pragma unroll
+      for (int e = 0; e < E; e++) q0[q][e] = rows[(size_t)q * ns + c0 + e];
+#pragma unroll
+    for (int e = 0; e < E; e++) {
+      vt[e] = rows[(size_t)NQ * ns + c0 + e];
+      vs[e] = rows[(size_t)NQ * ns + tid + e * T];
+    }
+    __syncthreads();  // every row read: the buffer takes the results
+    double *o = buf + (size_t)b * NB * ns;
+    azr_ring<NQ, E>(k, dt, i, q0, vt, vs, sh, hal, xb,
+                    [&](int p, double v, double r, double a, double bb, double en) {
+                      o[p] = v;
+                      o[(size_t)ns + p] = r;
+                      o[(size_t)2 * ns + p] = a;
+                      o[(size_t)3 * ns + p] = bb;
+                      if (NQ == 6) o[(size_t)4 * ns + p] = en;
+                    });
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the results, visible to the bulk copies
+    __syncthreads();
+    if (tid == 0) {
+      azs_store(k.vt + base, o, row_bytes);
+      azs_store(k.rho_t + base, o + ns, row_bytes);
+      azs_store(k.q[0] + base, o + (size_t)2 * ns, row_bytes);
+      azs_store(k.q[1] + base, o + (size_t)3 * ns, row_bytes);
+      if (NQ == 6) azs_store(k.e + base, o + (size_t)4 * ns, row_bytes);
+      asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+    }
+  }
+  if (tid == 0) {
+    if (failed) {
+      k.ctl->status = FB_ERR_TIMEOUT;
+      // a load still in flight lands in this CTA's buffer: give it a bounded
+      // time to arrive before the CTA's shared memory goes away
+      azs_wait(&bar[it & 1], (unsigned)((it >> 1) & 1), AZS_WAIT_LIMIT);
+    }
+    asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");  // the results are in global memory
+  }
+}
+
 // cells per thread of the azimuthal pass (1..4): at most 1024 threads for
 // 1-2 cells each, 768 threads for 3-4 (more registers per thread).  The
 // automatic choice is the fewest cells per thread; the tuner may pick more.
@@ -1690,6 +2096,41 @@ static bool azi_fits(int ns, int E, size_t rings)
   return azi_threads_for(ns, E) <= maxt &&
          rings * ns * sizeof(double) + 32 * sizeof(double) <= (size_t)max_smem_optin();
 }
+// The register variant needs E >= 2 contiguous cells per thread with
+// nsec = E T, T a multiple of 32 within the kernel's thread limit.
+static bool azr_fits(int ns, int E)
+{
+  if (E < 2 || E > 4 || ns % E != 0) return false;
+  const int T = ns / E;
+  return T % 32 == 0 && T <= AZR_MAXT && T / 32 <= AZR_MAXW;
+}
+// The staged variant: two buffers of NQ + 1 rows of nsec doubles, rows of a
+// whole number of 16-byte units (even nsec), 16-byte aligned fields.
+static size_t azs_smem_bytes(int ns, int NQ) { return (size_t)2 * (NQ + 1) * ns * sizeof(double); }
+static bool azs_fits(int ns, int energy, int E)
+{
+  const int NQ = energy ? 6 : 5;
+  return azr_fits(ns, E) && ns % 2 == 0 &&
+         azs_smem_bytes(ns, NQ) + 4096 <= (size_t)max_smem_optin();
+}
+static bool azs_pointers_aligned(const KP &k, int NQ)
+{
+  auto al = [](const void *p) { return ((unsigned long long)p & 15ull) == 0; };
+  bool ok = al(k.vt) && al(k.rho_t) && (NQ != 6 || al(k.e));
+  for (int q = 0; q < NQ; q++) ok = ok && al(k.q[q]);
+  return ok;
+}
+// one CTA per ring up to the CTAs the GPU holds at once
+static int azs_grid(const void *fn, int threads, size_t smem, int nr)
+{
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const int g = sms * per_sm;
+  return g < nr ? g : nr;
+}
 int fb_azi_variant(int ns, int energy, int E, int variant)
 {
   const int NQ = energy ? 6 : 5;
@@ -1699,6 +2140,8 @@ int fb_azi_variant(int ns, int energy, int E, int variant)
     case 1: return 1;
     case 2: return wide ? 2 : 0;
     case 3: return packed ? 3 : 0;
+    case 4: return azr_fits(ns, E) ? 4 : 0;
+    case 5: return azs_fits(ns, energy, E) ? 5 : 0;
     default: return 0;
   }
 }
@@ -1842,6 +2285,40 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
   const bool wide = (var == 2);
   const int th = azi_threads_for(k.ns, E);
   const bool full = (th * E == k.ns);  // every thread owns E cells
+  if (var == 5 && !azs_pointers_aligned(k, NQ)) var = 4;  // bulk copies need 16-byte aligned rows
+  if (var == 5) {
+    const int T = k.ns / E;
+    const size_t smem = azs_smem_bytes(k.ns, NQ);
+#define AZS_LAUNCH(EE, MM)                                                                                \
+  fb_launch(k_transport_azimuthal_staged<NQ, EE, MM>,                                                   \
+            azs_grid((const void *)k_transport_azimuthal_staged<NQ, EE, MM>, MM, smem, k.nr), T, smem, s, k, \
+            dt_override)
+#define AZS_E(EE) (T <= 256 ? AZS_LAUNCH(EE, 256) : T <= 512 ? AZS_LAUNCH(EE, 512) : AZS_LAUNCH(EE, 768))
+    switch (E) {
+      case 2: AZS_E(2); break;
+      case 3: AZS_E(3); break;
+      default: AZS_E(4); break;
+    }
+#undef AZS_E
+#undef AZS_LAUNCH
+    return;
+  }
+  if (var == 4) {
+    // the instance bounded by the smallest of 256 / 512 / 768 threads that
+    // holds T: the fewer threads, the more registers each may use
+    const int T = k.ns / E;
+#define AZR_LAUNCH(EE)                                                                                   \
+  (T <= 256 ? fb_launch(k_transport_azimuthal_reg<NQ, EE, 256>, k.nr, T, 0, s, k, dt_override)            \
+   : T <= 512 ? fb_launch(k_transport_azimuthal_reg<NQ, EE, 512>, k.nr, T, 0, s, k, dt_override)          \
+              : fb_launch(k_transport_azimuthal_reg<NQ, EE, 768>, k.nr, T, 0, s, k, dt_override))
+    switch (E) {
+      case 2: AZR_LAUNCH(2); break;
+      case 3: AZR_LAUNCH(3); break;
+      default: AZR_LAUNCH(4); break;
+    }
+#undef AZR_LAUNCH
+    return;
+  }
   if (var == 3) {
     const size_t psmem = (size_t)AZP_RINGS(NQ) * k.ns * sizeof(double);
 #define AZP_LAUNCH(EE)                                                                                       \
@@ -2145,6 +2622,18 @@ int fb_gas_prepare(int ns, int energy)
     int rc = fb_allow_max_dynamic_smem((const void *)k_cfl);  // 3 nsec doubles of cell values
     if (rc) return rc;
   }
+#define AZS_FNS(NQ, EE)                                                                  \
+  (const void *)k_transport_azimuthal_staged<NQ, EE, 256>,                               \
+      (const void *)k_transport_azimuthal_staged<NQ, EE, 512>,                           \
+      (const void *)k_transport_azimuthal_staged<NQ, EE, 768>
+  {
+    const void *sfns[] = {AZS_FNS(5, 2), AZS_FNS(5, 3), AZS_FNS(5, 4), AZS_FNS(6, 2), AZS_FNS(6, 3), AZS_FNS(6, 4)};
+    for (const void *f : sfns) {
+      int rc = fb_allow_max_dynamic_smem(f);
+      if (rc) return rc;
+    }
+  }
+#undef AZS_FNS
   for (const void *f : fns) {
     int rc = fb_allow_max_dynamic_smem(f);
     if (rc) return rc;

@@ -292,7 +292,11 @@ int fb_planet_force(fb_ctx *ctx, double x, double y, double rsmoothing, double m
 typedef struct fb_tuning {
   int cell_block, azi_cells_per_thread, rad_columns, rad_rings;
   int azi_variant;  /* 0 automatic, 1 narrow (NQ+3 shared rings), 2 wide (2 NQ+1 rings),
-                       3 packed (12 rings, 13 with energy; a cell's quantities side by side) */
+                       3 packed (12 rings, 13 with energy; a cell's quantities side by side),
+                       4 register (E = 2..4 contiguous cells per thread, quantities in
+                       registers; nsec = E T with T a multiple of 32), 5 staged (the
+                       register variant in a persistent kernel whose rings arrive and
+                       leave by bulk asynchronous copies, one ring ahead) */
 } fb_tuning;
 int fb_get_tuning(const fb_ctx *ctx, fb_tuning *t);
 int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t);

@@ -54,14 +54,22 @@ def test_dropin_matches_reference(tmp_path, par_name, keys):
     pb = np.loadtxt(os.path.join(wb, "out", "planet0.dat"))
     np.testing.assert_allclose(pb, pa, rtol=1e-10, atol=1e-14)
     # the per-DT planet logs of UpdateLog (Force.c:266-328), fed by the GPU's
-    # ComputeForce: each column within 1e-10 of its largest value (the force
-    # sums are added in another order, and torques cancel)
+    # ComputeForce, and the indirect terms of compindirectterm.dat
+    # (Output.c): each column within 1e-10 of its largest value (the force
+    # sums are added in another order, and torques cancel).  The last two
+    # columns of compindirectterm.dat, the barycentre's second difference
+    # (SideEuler.c:91-112), divide sums that cancel to ~1e-8 by dt^2: their
+    # summation order shows at 1e-6 of the direct term's size.
     for name in ("tqwk0.dat", "indtq0.dat", "compindirectterm.dat"):
         la = np.atleast_2d(np.loadtxt(os.path.join(wa, "out", name)))
         lb = np.atleast_2d(np.loadtxt(os.path.join(wb, "out", name)))
         assert la.shape == lb.shape and la.shape[0] >= 2, (name, la.shape, lb.shape)
         scale = np.maximum(np.max(np.abs(la), axis=0), 1e-300)
-        assert np.all(np.abs(lb - la) <= 1e-10 * scale), name
+        tol = 1e-10 * scale
+        if name == "compindirectterm.dat":
+            tol[3:] = 1e-6 * max(scale[1], scale[2])
+        bad = np.abs(lb - la) > tol
+        assert not np.any(bad), (name, la[np.any(bad, axis=1)], lb[np.any(bad, axis=1)])
 
 
 def test_dropin_crash_report(tmp_path):
@@ -94,24 +102,31 @@ def test_dropin_crash_report(tmp_path):
 
 def test_dropin_restart(tmp_path):
     """-s N restart (Init.c:93-211, main.c:97-100) through the drop-in: the
-    reference's own restart reads the N-th outputs of an earlier run, the
-    GPU continues from them, and its next output matches the uninterrupted
-    reference run's within 1e-11."""
+    reference's own restart code reads the N-th outputs of an earlier run and
+    the GPU continues from what it read.  The reference's restart is not
+    exact itself (it does not restore everything the run carried, e.g. the
+    barycentre history), so the drop-in's next output is compared with the
+    reference restarted from the same files: within 1e-11."""
     import shutil
     nr, ns = 64, 192
     par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "adiabatic_sg_512x1536.par"), str(tmp_path),
                             Nrad=nr, Nsec=ns)
-    wa, wb = str(tmp_path / "ref"), str(tmp_path / "gpu")
+    wa = str(tmp_path / "first")
     os.makedirs(wa)
     extra = {"Ninterm": 2}
     _oracle.run_oracle(par, 5, noise=1e-4, seed=2, workdir=wa, keep=True, extra_keys=extra)
-    shutil.copytree(os.path.join(wa, "out"), os.path.join(wb, "out"))
-    for name in ("gasdens2.dat", "gasvrad2.dat", "gasvtheta2.dat", "gasenergy2.dat"):
-        os.remove(os.path.join(wb, "out", name))
-    _oracle.run_oracle(par, 5, noise=1e-4, seed=2, workdir=wb, keep=True, extra_keys=extra,
-                       binary=_oracle.DROPIN_BIN, flags=["-s", "1"])
-    for name in ("gasdens", "gasvrad", "gasvtheta", "gasenergy"):
-        xa = np.fromfile(os.path.join(wa, "out", "%s2.dat" % name))
-        xb = np.fromfile(os.path.join(wb, "out", "%s2.dat" % name))
+    names = ("gasdens", "gasvrad", "gasvtheta", "Temperature")
+    runs = {}
+    for tag, binary in (("ref", _oracle.ORACLE_BIN), ("gpu", _oracle.DROPIN_BIN)):
+        w = str(tmp_path / tag)
+        shutil.copytree(os.path.join(wa, "out"), os.path.join(w, "out"))
+        for name in names:
+            os.remove(os.path.join(w, "out", "%s2.dat" % name))
+        _oracle.run_oracle(par, 5, noise=1e-4, seed=2, workdir=w, keep=True, extra_keys=extra, binary=binary,
+                           flags=["-s", "1"])
+        runs[tag] = w
+    for name in names:
+        xa = np.fromfile(os.path.join(runs["ref"], "out", "%s2.dat" % name))
+        xb = np.fromfile(os.path.join(runs["gpu"], "out", "%s2.dat" % name))
         assert xa.size == nr * ns and xb.size == nr * ns, name
         assert _oracle.rel_err(xb, xa) <= 1e-11, name

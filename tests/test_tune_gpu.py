@@ -49,16 +49,21 @@ def test_tuning_table_lookup(tmp_path):
 
 
 @pytest.mark.parametrize("cfg", ["adiabatic_sg_512x1536.par", "iso_128x384.par"])
-@pytest.mark.parametrize("E", [1, 2, 3])
+@pytest.mark.parametrize("E", [1, 2, 3, 4])
 def test_azimuthal_variants_are_bit_identical(tmp_path, E, cfg):
     """The narrow (three barriers per quantity), wide (all quantities per
-    phase) and packed (a cell's quantities side by side) azimuthal passes do
-    the same arithmetic: whole DTs, isothermal or with energy, cooling and
-    self-gravity, must agree to the last bit."""
+    phase), packed (a cell's quantities side by side), register (E
+    contiguous cells per thread, quantities in registers, each face flux
+    evaluated once; E >= 2) and staged (the register variant fed and drained
+    by bulk asynchronous copies) azimuthal passes do the same arithmetic: whole
+    DTs, isothermal or with energy, cooling and self-gravity, must agree to
+    the last bit."""
     from dustyfargoadsg_b200 import Disc, read_par
-    par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, cfg), str(tmp_path), Nrad=64, Nsec=192)
+    nsec = 256 if E == 4 else 192  # the register variant needs nsec / E threads, a multiple of 32
+    par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, cfg), str(tmp_path), Nrad=64, Nsec=nsec)
     out = {}
-    for variant in (1, 2, 3):
+    variants = (1, 2, 3, 4, 5) if E >= 2 else (1, 2, 3)
+    for variant in variants:
         with Disc(read_par(par), noise=1e-3, seed=4) as d:
             d.set_tuning({"cell_block": 128, "azi_cells_per_thread": E, "azi_variant": variant})
             assert d.tuning()["azi_variant"] == variant
@@ -66,6 +71,6 @@ def test_azimuthal_variants_are_bit_identical(tmp_path, E, cfg):
                 d.step()
             out[variant] = d.download()
     fields = FIELDS + (("energy",) if read_par(par).energy_equation else ())
-    for v in (2, 3):
+    for v in variants[1:]:
         for k in fields:
             np.testing.assert_array_equal(out[1][k], out[v][k], err_msg="%s variant %d" % (k, v))
