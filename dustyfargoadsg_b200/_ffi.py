@@ -43,7 +43,8 @@ class FbParams(C.Structure):
         ("fast_transport", _I), ("wall_boundary", _I), ("evanescent", _I),
         ("wkzrmin", _D), ("wkzrmax", _D), ("dampingtodynamicaltimeratio", _D),
         ("damp_to_axi", _I), ("damp_to_ini", _I), ("add_floors", _I),
-        ("densityfloor", _D), ("zero_vrad_bc", _I),
+        ("densityfloor", _D), ("zero_vrad_bc", _I), ("open_inner", _I), ("kn_open", _I),
+        ("non_reflecting", _I),
         ("mindt", _D), ("maxdt", _D), ("imposeddiskdrift", _D),
         ("factorunitmass", _D), ("factorunitlength", _D), ("factormmw", _D),
         ("nbpart", _I),

@@ -157,6 +157,34 @@ def record_samples(net, fine, coarse, first_slot, nsamples, every=1):
     return slot
 
 
+def record_rollout_samples(net, fine, coarse, first_slot, nsamples, every=1, horizon=4):
+    """Samples on the states the corrected solver itself visits (data
+    aggregation: S. Ross, G. Gordon, D. Bagnell, AISTATS 2011): the coarse
+    disc starts from the coarse-grained fine state and runs `horizon` DTs of
+    the plain method, each followed by the network's correction, beside the
+    fine disc; from that corrected state one sample is taken as
+    record_samples takes it (features, the plain DT, the coarse-grained fine
+    DT), so its target also undoes the drift the corrected run has
+    gathered."""
+    slot = first_slot
+    for _ in range(nsamples):
+        downsample(fine, coarse)
+        for _ in range(horizon):
+            coarse.step()
+            net.apply(coarse)
+            fine.step()
+        net.record(coarse, slot, 0)
+        coarse.step()
+        net.record(coarse, slot, 1)
+        fine.step()
+        downsample(fine, coarse)
+        net.record(coarse, slot, 2)
+        slot += 1
+        for _ in range(every - 1):
+            fine.step()
+    return slot
+
+
 def train_small(workdir, coarse_nr=16, coarse_ns=64, factor=4, samples=6, iters=60, seed=0):
     """A small end-to-end training run (tests): one disc, a few samples."""
     draw = dict(q=1e-3, AlphaViscosity=1e-3, AspectRatio=0.05, SigmaSlope=0.5)
@@ -268,6 +296,10 @@ def main(argv=None):
     ap.add_argument("--samples-per-disc", type=int, default=24)
     ap.add_argument("--every", type=int, default=10, help="fine DTs between samples")
     ap.add_argument("--iters", type=int, default=2000)
+    ap.add_argument("--rollout-rounds", type=int, default=0,
+                    help="rounds of samples taken on the corrected solver's own states, each followed by "
+                         "more training (data aggregation)")
+    ap.add_argument("--rollout-horizon", type=int, default=4, help="corrected DTs before such a sample")
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--eval-discs", type=int, default=4)
     ap.add_argument("--eval-dt", type=int, default=400)
@@ -277,7 +309,7 @@ def main(argv=None):
     args = ap.parse_args(argv)
     wd = tempfile.mkdtemp(prefix="fb_closure_")
     draws = sweep.draw_discs(args.train_discs, seed=3)
-    cap = args.train_discs * args.samples_per_disc
+    cap = args.train_discs * args.samples_per_disc * (1 + args.rollout_rounds)
     report = {"coarse": [args.coarse_nr, 3 * args.coarse_nr], "factor": args.factor}
     t0 = time.perf_counter()
     net = None
@@ -315,6 +347,41 @@ def main(argv=None):
         if v < best_val:
             best_val, best = v, net.get_params()
     net.set_params(best)
+    # data aggregation: samples on the corrected solver's own states, then
+    # more training on everything (the held-out discs stay held out)
+    report["rollout"] = []
+    ntrain_disc = args.train_discs - args.val_discs
+    for rnd in range(args.rollout_rounds):
+        t2 = time.perf_counter()
+        first_new = slot
+        for d, draw in enumerate(draws[:ntrain_disc]):
+            draw = dict(draw)
+            draw.pop("Nrad"), draw.pop("Nsec")
+            fine, coarse = disc_pair(draw, wd, "roll%02d_%02d" % (rnd, d), args.coarse_nr, args.factor)
+            for _ in range(args.spinup_dt):
+                fine.step()
+            try:
+                slot = record_rollout_samples(net, fine, coarse, slot, args.samples_per_disc, args.every,
+                                              args.rollout_horizon)
+            except FbError as exc:  # a corrected run that fails contributes no samples
+                print("rollout disc", d, "failed:", exc, flush=True)
+            fine.close()
+            coarse.close()
+        # the new samples go behind the validation block: train on both ranges
+        for it in range(0, args.iters, chunk):
+            n = min(chunk, args.iters - it)
+            losses.extend(net.train(0, ntrain, (n + 1) // 2, lr=args.lr, seed=100 * rnd + it).tolist())
+            if slot > first_new:
+                losses.extend(net.train(first_new, slot - first_new, n // 2, lr=args.lr,
+                                        seed=100 * rnd + it + 1).tolist())
+            v = val_loss()
+            curve.append([len(losses), float(np.mean(losses[-chunk:])), v])
+            if v < best_val:
+                best_val, best = v, net.get_params()
+        net.set_params(best)
+        report["rollout"].append({"round": rnd, "samples": slot - first_new, "t_s": time.perf_counter() - t2,
+                                  "loss_val_best": best_val})
+        print("rollout round", rnd, report["rollout"][-1], flush=True)
     report["t_train_s"] = time.perf_counter() - t1
     report["loss_train_first"], report["loss_train_last"] = float(losses[0]), float(np.mean(losses[-50:]))
     report["loss_val_best"] = best_val

@@ -241,6 +241,7 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   *out = NULL;
   if (p->unsupported) return FB_ERR_UNSUPPORTED;
   if (p->nrad < 4 || p->nsec < 2) return FB_ERR_INVALID;
+  if ((p->open_inner || p->non_reflecting) && p->nrad < 8) return FB_ERR_INVALID;  // the edges span 4 rings each
   if (p->self_gravity && !p->log_grid) return FB_ERR_INVALID;  // sginit.c:6-7
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return FB_ERR_NODEVICE;
@@ -397,6 +398,22 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.beta_cooling = p->beta_cooling;
   k.fast_transport = p->fast_transport;
   k.wall = p->wall_boundary;
+  k.open_inner = p->open_inner;
+  k.kn_open = p->kn_open;
+  k.non_reflecting = p->non_reflecting;
+  k.sigmaslope = p->sigmaslope;
+  if (p->open_inner || p->non_reflecting) {  // the edges' constants, as the reference evaluates them
+    const fb_geom &gg = ctx->g;
+    k.ob_vt1 = sqrt(gg.rmed[2] / gg.rmed[1]);
+    k.ob_vt0 = sqrt(gg.rmed[2] / gg.rmed[0]);
+    k.ob_vtout = pow(gg.rmed[nr - 1] / gg.rmed[nr - 2], -0.5);
+    k.nrb_om1 = pow(gg.rinf[1], -1.5);
+    k.nrb_omn2 = pow(gg.rinf[nr - 2], -1.5);
+    k.nrb_csinit0 = sqrt(p->adiabaticindex) * p->aspectratio * pow(gg.rmed[0], -0.5 + p->flaringindex);
+    k.nrb_csinit1 = sqrt(p->adiabaticindex) * p->aspectratio * pow(gg.rmed[1], -0.5 + p->flaringindex);
+    k.radii0 = gg.radii[0];
+    k.radiin = gg.radii[nr];
+  }
   k.evanescent = p->evanescent;
   k.add_floors = p->add_floors;
   k.damp_axi = p->damp_to_axi;
@@ -617,6 +634,14 @@ static int enqueue_substep(fb_ctx *ctx)
   STAGE(ST_TRAD, 1, fb_launch_transport_radial(k, 0.0, s));
   STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s));
   STAGE(ST_TVR, 1, fb_launch_transport_vr(k, s));
+  if (k.open_inner || k.non_reflecting) {
+    // ApplyBoundaryCondition's other edges (SideEuler.c:1102-1131); the
+    // non-reflecting edge reads the planets' new positions and, with the
+    // energy equation, the sound speed of the transported state
+    if (k.non_reflecting && !ctx->has_dust) cudaStreamWaitEvent(s, ctx->ev_planets, 0);
+    if (k.non_reflecting && k.energy) STAGE(ST_TVR, 1, fb_launch_soundspeed(k, 0, s));
+    STAGE(ST_TVR, 1, fb_launch_edges(k, s));
+  }
   if (k.evanescent && k.n_damp_rings > 0) STAGE(ST_DAMP, 1, fb_launch_damping(k, 0.0, s));
   if (!ctx->has_dust) cudaStreamWaitEvent(s, ctx->ev_planets, 0);
   if (ctx->profiling) {

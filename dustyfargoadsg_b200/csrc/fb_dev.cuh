@@ -89,6 +89,14 @@ struct KP {
   int visc_mode;           // 0 inviscid, 1 alpha, 2 constant nu
   int energy, viscous_heating, beta_cooling, fast_transport;
   int wall, evanescent, add_floors, damp_axi, zero_vrad;
+  // open and non-reflecting edges (SideEuler.c:300-410, 569-794) and the
+  // constants they take from the 1-D tables (glibc pow on the host):
+  // sqrt(Rmed2/Rmed1), sqrt(Rmed2/Rmed0), pow(Rmed[nr-1]/Rmed[nr-2], -0.5),
+  // pow(Rinf[1], -1.5), pow(Rinf[nr-2], -1.5), the initial sound speeds of
+  // rings 0 and 1 (adiabatic), SIGMASLOPE, Radii[0] and Radii[nr]
+  int open_inner, kn_open, non_reflecting;
+  double ob_vt1, ob_vt0, ob_vtout, nrb_om1, nrb_omn2, nrb_csinit0, nrb_csinit1, sigmaslope;
+  double radii0, radiin;
   double floordens, wkzrmin, wkzrmax;
   int indirect_term, discard_gas_it, alt_gas_it, exclude_hill, roche, forced_circular;
   double indirect_smoothing, rochesmoothing, thicksmoothing, aspectratio, flaringindex;
@@ -265,6 +273,7 @@ void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_transport_vr(const KP &k, cudaStream_t s);
+void fb_launch_edges(const KP &k, cudaStream_t s);  // open / non-reflecting edges
 void fb_launch_floors_boundary(const KP &k, cudaStream_t s);
 void fb_launch_damping(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_diag(const KP &k, double *out2, cudaStream_t s);

@@ -2361,6 +2361,205 @@ void fb_launch_transport_vr(const KP &k, cudaStream_t s)
   fb_launch(k_transport_vr, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k);
 }
 
+// ------------------------------------------- open and non-reflecting edges
+// ApplyBoundaryCondition's edges other than the wall (SideEuler.c:1102-1131),
+// after the transport and floors and before the damping, as AlgoGas calls it
+// (SourceEuler.c:695): OpenBoundary (SideEuler.c:300-410; with INNERBOUNDARY
+// K, Kley & Nelson's outflow of :325-338) and NonReflectingBoundary
+// (SideEuler.c:569-794).  One CTA per edge: blockIdx.x 0 the inner edge, 1 the
+// outer.  The ring means the non-reflecting edge takes are summed by one
+// fixed tree (the reference sums sequentially: ~1e-16 relative).  Where the
+// reference leaves the innermost (outermost) planet's radius undefined (no
+// planet inside the grid), the planets' frequency term is 0 here.
+#define EDGE_BS 256
+__global__ void __launch_bounds__(EDGE_BS) k_edges(KP k)
+{
+  fb_grid_dependency();
+  __shared__ double sh[32];
+  const int ns = k.ns, nr = k.nr, tid = threadIdx.x, T = blockDim.x;
+  const bool inner = (blockIdx.x == 0);
+  double *rho = k.rho, *vr = k.vr, *vt = k.vt, *en = k.e;
+  const double *cs = k.cs;
+  if (k.open_inner) {
+    if (inner) {
+      const int i = 2;
+      for (int j = tid; j < ns; j += T) {
+        const size_t l = (size_t)j + (size_t)i * ns;
+        if (k.kn_open) {
+          rho[l - ns] = rho[l] * k.rmed[1] / k.rmed[0];
+          if (k.energy) en[l - ns] = en[l];
+          if (vr[l + ns] > 0.0) {
+            vr[l] = 0.0;
+          } else {
+            const double vri = -3. * nu_ring(k, i) / k.rmed[i] * 3. * (-k.sigmaslope + 1. + 2. * k.flaringindex);
+            if (fabs(vr[l + ns]) > fabs(vri))
+              vr[l] = vri;
+            else
+              vr[l] = vr[l + ns];
+          }
+        } else {
+          rho[l - ns] = rho[l];
+          rho[l - 2 * ns] = rho[l];
+          if (k.energy) {
+            en[l - ns] = en[l];
+            en[l - 2 * ns] = en[l];
+          }
+          vt[l - ns] = vt[l] * k.ob_vt1;
+          vt[l - 2 * ns] = vt[l] * k.ob_vt0;
+          if ((vr[l + ns] >= 0.0) || (rho[l] < k.sigmamed[0])) {
+            vr[l] = 0.0;
+            vr[l - ns] = 0.0;
+          } else {
+            vr[l] = vr[l + ns];
+            vr[l - ns] = vr[l + ns];
+          }
+        }
+      }
+    } else {
+      const int i = nr - 1;
+      for (int j = tid; j < ns; j += T) {
+        const size_t l = (size_t)j + (size_t)i * ns;
+        rho[l] = rho[l - ns];
+        if (k.energy) en[l] = en[l - ns];
+        vt[l] = vt[l - ns] * k.ob_vtout;
+        if (k.kn_open) {
+          if (vr[l - ns] < 0.0)
+            vr[l] = 0.0;
+          else
+            vr[l] = vr[l - ns];
+        } else {
+          if ((vr[l - ns] < 0.0) || (rho[l] < k.sigmamed[nr - 2]))
+            vr[l] = 0.0;
+          else
+            vr[l] = vr[l - ns];
+        }
+      }
+    }
+  }
+  if (!k.non_reflecting) return;
+  const fb_ctl *c = k.ctl;
+  if (inner) {
+    // innermost planet inside the grid (SideEuler.c:589-599)
+    double buf = k.radiin, omega_in = 0.0;
+    for (int q = 0; q < c->np; q++) {
+      const double rp = sqrt(c->px[q] * c->px[q] + c->py[q] * c->py[q]);
+      if ((rp < buf) && (rp >= k.radii0)) {
+        buf = rp;
+        omega_in = pow(rp, -1.5);
+      }
+    }
+    const int i = 1;
+    if (!k.energy) {
+      double cs0 = 0.0, cs1 = 0.0, d0 = 0.0, d1 = 0.0;
+      for (int j = tid; j < ns; j += T) {
+        cs0 += cs[j];
+        cs1 += cs[ns + j];
+        d0 += rho[j];
+        d1 += rho[ns + j];
+      }
+      cs0 = block_sum_dyn(cs0, sh) / (double)ns;
+      cs1 = block_sum_dyn(cs1, sh) / (double)ns;
+      d0 = block_sum_dyn(d0, sh) / (double)ns;  // dens0: unused without an accreting edge
+      d1 = block_sum_dyn(d1, sh) / (double)ns;
+      (void)d0;
+      double dangle = (k.nrb_om1 - omega_in) / (.5 * (cs0 + cs1));
+      dangle *= (k.rmed[1] - k.rmed[0]);
+      const int i_angle = (int)(dangle / (k.pmax - k.pmin) * (double)ns + .5);
+      for (int j = tid; j < ns; j += T) {
+        const size_t l = (size_t)j + (size_t)i * ns;
+        int jp = j + i_angle;
+        if (jp >= ns) jp -= ns;
+        if (jp < 0) jp += ns;
+        rho[jp] = rho[l];
+        const double vr_med = -cs1 * (rho[l] - d1) / d1;
+        vr[l] = 2. * vr_med - vr[l + ns];
+      }
+      __syncthreads();
+      double mean = 0.0;
+      for (int j = tid; j < ns; j += T) mean += rho[j];
+      mean = block_sum_dyn(mean, sh) / (double)ns;
+      for (int j = tid; j < ns; j += T) rho[j] += (k.sigmamed[0] - mean);
+    } else {
+      const double csinit0 = k.nrb_csinit0, csinit1 = k.nrb_csinit1;
+      double dangle = (k.nrb_om1 - omega_in) / (.5 * (csinit0 + csinit1));
+      dangle *= (k.rmed[1] - k.rmed[0]);
+      const int i_angle = (int)(dangle / (k.pmax - k.pmin) * (double)ns + .5);
+      for (int j = tid; j < ns; j += T) {
+        const size_t l = (size_t)j + (size_t)i * ns;
+        int jp = j + i_angle;
+        if (jp >= ns) jp -= ns;
+        if (jp < 0) jp += ns;
+        en[jp] = en[l];
+        const double vr_med = -csinit1 * (rho[l] - k.sigmamed[1]) / k.sigmamed[1];
+        vr[l] = 2. * vr_med - vr[l + ns];
+      }
+      __syncthreads();
+      for (int j = tid; j < ns; j += T)
+        rho[j] = k.sigmamed[0] + (k.gamma - 1.0) * (en[j] - k.energymed[0]) / csinit0 / csinit0;
+      __syncthreads();
+      double mean = 0.0;
+      for (int j = tid; j < ns; j += T) mean += rho[j];
+      mean = block_sum_dyn(mean, sh) / (double)ns;
+      for (int j = tid; j < ns; j += T) rho[j] += (k.sigmamed[0] - mean);
+      __syncthreads();
+      mean = 0.0;
+      for (int j = tid; j < ns; j += T) mean += en[j];
+      mean = block_sum_dyn(mean, sh) / (double)ns;
+      for (int j = tid; j < ns; j += T) en[j] += (k.energymed[0] - mean);
+    }
+  } else {
+    // outermost planet inside the grid (SideEuler.c:718-728)
+    double buf = k.radii0, omega_out = 0.0;
+    for (int q = 0; q < c->np; q++) {
+      const double rp = sqrt(c->px[q] * c->px[q] + c->py[q] * c->py[q]);
+      if ((rp > buf) && (rp <= k.radiin)) {
+        buf = rp;
+        omega_out = pow(rp, -1.5);
+      }
+    }
+    const size_t b1 = (size_t)(nr - 1) * ns, b2 = (size_t)(nr - 2) * ns;
+    double c2 = 0.0, c1 = 0.0, d1 = 0.0, d2 = 0.0;
+    for (int j = tid; j < ns; j += T) {
+      c2 += cs[b2 + j];
+      c1 += cs[b1 + j];
+      d1 += rho[b1 + j];
+      d2 += rho[b2 + j];
+    }
+    const double csnrm2 = block_sum_dyn(c2, sh) / (double)ns;
+    const double csnrm1 = block_sum_dyn(c1, sh) / (double)ns;
+    const double densnrm1 = block_sum_dyn(d1, sh) / (double)ns;  // unused without an accreting edge
+    const double densnrm2 = block_sum_dyn(d2, sh) / (double)ns;
+    (void)densnrm1;
+    double dangle = (k.nrb_omn2 - omega_out) / (.5 * (csnrm1 + csnrm2));
+    dangle *= (k.rmed[nr - 1] - k.rmed[nr - 2]);
+    const int i_angle = (int)(dangle / (k.pmax - k.pmin) * (double)ns + .5);
+    for (int j = tid; j < ns; j += T) {
+      const size_t l = (size_t)j + b1;
+      int jp = j - i_angle;
+      if (jp >= ns) jp -= ns;
+      if (jp < 0) jp += ns;
+      const size_t lp = (size_t)jp + b2;
+      rho[l] = rho[lp];
+      en[l] = en[lp];
+      const double vr_med = (!k.energy) ? csnrm1 * (rho[l - ns] - densnrm2) / densnrm2
+                                        : cs[l] * (rho[l - ns] - densnrm2) / densnrm2;
+      vr[l] = 2. * vr_med - vr[l - ns];
+    }
+    __syncthreads();
+    double mean = 0.0;
+    for (int j = tid; j < ns; j += T) mean += rho[b1 + j];
+    mean = block_sum_dyn(mean, sh) / (double)ns;
+    for (int j = tid; j < ns; j += T) rho[b1 + j] += k.sigmamed[nr - 1] - mean;
+    __syncthreads();
+    mean = 0.0;
+    for (int j = tid; j < ns; j += T) mean += en[b1 + j];
+    mean = block_sum_dyn(mean, sh) / (double)ns;
+    for (int j = tid; j < ns; j += T) en[b1 + j] += k.energymed[nr - 1] - mean;
+  }
+}
+
+void fb_launch_edges(const KP &k, cudaStream_t s) { fb_launch(k_edges, 2, EDGE_BS, 0, s, k); }
+
 // Makes the driver load the radial and vr transport kernels now (asking
 // for a function's attributes loads it under lazy module loading), so that
 // their first launch later needs no module load.  fb_gas_prepare does the

@@ -100,6 +100,9 @@ int fb_params_default(fb_params *p)
   p->damp_to_ini = 0;
   p->add_floors = 1;
   p->zero_vrad_bc = 0;
+  p->open_inner = 0;
+  p->kn_open = 0;
+  p->non_reflecting = 0;
   p->dust_feel_disk = 1;
   p->dust_feel_planets = 1;
   p->dust_feel_turb = 0;
@@ -257,8 +260,10 @@ int fb_params_read_par(fb_params *p, const char *path)
   if (is_c(c, 'S')) p->fast_transport = 0;
   c = kv_c(&set, "INNERBOUNDARY", 'W');
   p->wall_boundary = is_c(c, 'W');
-  if (is_c(c, 'O') || is_c(c, 'N') || is_c(c, 'A') || is_c(c, 'K'))
-    p->unsupported |= FB_U_BOUNDARY;
+  p->open_inner = is_c(c, 'O') || is_c(c, 'K');
+  p->kn_open = is_c(c, 'K');
+  p->non_reflecting = is_c(c, 'N');
+  if (is_c(c, 'A')) p->unsupported |= FB_U_BOUNDARY;  /* the accreting boundary is not built */
   c = kv_c(&set, "WAVEKILLINGZONES", 'N');
   p->evanescent = is_c(c, 'Y');
   if (is_c(kv_c(&set, "DAMPTOINI", 'N'), 'Y')) { p->damp_to_ini = 1; p->damp_to_axi = 0; }
@@ -354,7 +359,7 @@ const char *fb_unsupported_name(const fb_params *p)
 {
   static const struct { unsigned long long bit; const char *name; } names[] = {
     {FB_U_CENTRIFUGAL, "CentrifugalBalance/CavityTorque"}, {FB_U_TAILOFF, "TailOff"},
-    {FB_U_DUSTFLUID, "DustFluid"}, {FB_U_BOUNDARY, "InnerBoundary other than Wall"},
+    {FB_U_DUSTFLUID, "DustFluid"}, {FB_U_BOUNDARY, "InnerBoundary Accreting"},
     {FB_U_OUTERSOURCE, "OuterSourceMass"}, {FB_U_DAMPTOVISCOUS, "DampToViscous"},
     {FB_U_ADDMASS, "AddMass"}, {FB_U_EVAPORATION, "DiscEvaporation"},
     {FB_U_PHOTOEVAP, "PhotoEvaporation"}, {FB_U_SGZEROMODE, "SelfGravity Z (zero mode)"},

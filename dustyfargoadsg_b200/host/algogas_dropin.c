@@ -36,7 +36,7 @@ extern boolean BM08, DustFeedback, Write_Temperature, Write_Potential;
 extern boolean DustFeelDisk, DustFeelPlanets, DustFeelTurb, DustFeelSG, DustFeelSGZeroMode;
 extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensity, ZZIntegrator;
 extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
-extern boolean CompareSGAndSummationTorques;
+extern boolean CompareSGAndSummationTorques, KNOpen;
 extern Pair DiskOnPrimaryAcceleration, DiskOnPrimaryAcceleration_alt;
 
 static fb_ctx *g_ctx = NULL;
@@ -114,7 +114,10 @@ static void params_from_globals(fb_params *p)
   p->factormmw = FACTORMMW;
   p->nbpart = NBPART;
   /* features the GPU build does not implement are refused by fb_create */
-  if (OpenInner || NonReflecting || AccBoundary) p->unsupported |= FB_U_BOUNDARY;
+  p->open_inner = OpenInner;
+  p->kn_open = KNOpen;
+  p->non_reflecting = NonReflecting;
+  if (AccBoundary) p->unsupported |= FB_U_BOUNDARY;
   if (OuterSourceMass) p->unsupported |= FB_U_OUTERSOURCE;
   if (DampToViscous) p->unsupported |= FB_U_DAMPTOVISCOUS;
   if (AddMass) p->unsupported |= FB_U_ADDMASS;

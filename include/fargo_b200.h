@@ -84,7 +84,7 @@ typedef struct fb_params {
   int forced_circular, exclude_hill;
   double excludehillfactor, eccentricity, releasedate, releaseradius;
   /* transport and boundaries: TRANSPORT (FARGO/Standard), INNERBOUNDARY
-     (Wall), WAVEKILLINGZONES, WKZRMIN, WKZRMAX,
+     (Wall, Open, KNOpen, NonReflecting), WAVEKILLINGZONES, WKZRMIN, WKZRMAX,
      DAMPINGTODYNAMICALTIMERATIO, DAMPTOAXI/DAMPTOINI, ADDFLOORS,
      DENSITYFLOOR, ZEROVRADBC */
   int fast_transport, wall_boundary, evanescent;
@@ -92,6 +92,10 @@ typedef struct fb_params {
   int damp_to_axi, damp_to_ini, add_floors;
   double densityfloor;
   int zero_vrad_bc;
+  /* INNERBOUNDARY other than WALL (src/Interpret.c:168-175): OPEN (open_inner),
+     KNOPEN (open_inner and kn_open: Kley & Nelson's outflow), NONREFLECTING
+     (non_reflecting); ACCRETING is refused */
+  int open_inner, kn_open, non_reflecting;
   /* MINDT, MAXDT: initial values of the running min/max substep (the
      reference keeps them as .par variables, src/var.c:145-146) */
   double mindt, maxdt;

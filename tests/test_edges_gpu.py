@@ -1,0 +1,54 @@
+"""The inner and outer edges other than the wall (ApplyBoundaryCondition,
+SideEuler.c:1102-1131): OpenBoundary (SideEuler.c:300-410), its Kley &
+Nelson variant (INNERBOUNDARY K) and NonReflectingBoundary
+(SideEuler.c:569-794), isothermal and adiabatic, against the CPU oracle (the
+reference's own build) on the same seeded start.
+
+Tolerance (the one-DT parity bar of this path): fields within 1e-11
+(scale-relative) after each DT, equal substep counts.  The non-reflecting
+edge takes ring means, which the GPU sums in a tree order: its rounding
+stays at the 1e-16 level of those means.
+"""
+import os
+
+import pytest
+
+from tests import _oracle
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not _oracle.have_oracle(), reason="oracle not built")]
+
+CFG = _oracle.CONFIG_DIR
+TOL_DT = 1e-11
+
+CASES = {
+    "open_iso": ("iso_128x384.par", dict(InnerBoundary="OPEN")),
+    "knopen_iso": ("iso_128x384.par", dict(InnerBoundary="KNOPEN")),
+    "nonreflecting_iso": ("iso_128x384.par", dict(InnerBoundary="NONREFLECTING")),
+    "open_adiabatic": ("adiabatic_sg_512x1536.par", dict(InnerBoundary="OPEN", SelfGravity="No")),
+    "nonreflecting_adiabatic": ("adiabatic_sg_512x1536.par", dict(InnerBoundary="NONREFLECTING",
+                                                                  SelfGravity="No")),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_edges_match_oracle(tmp_path, case):
+    from dustyfargoadsg_b200 import Disc, read_par
+    name, keys = CASES[case]
+    par = _oracle.write_par(os.path.join(CFG, name), str(tmp_path), Nrad=64, Nsec=192, **keys)
+    p = read_par(par)
+    assert p.unsupported == 0 and p.wall_boundary == 0
+    steps = 3
+    dumps, _, _ = _oracle.run_oracle(par, steps=steps, noise=1e-3, seed=7)
+    fields = ("dens", "vrad", "vtheta") + (("energy",) if p.energy_equation else ())
+    with Disc(p, noise=1e-3, seed=7) as disc:
+        prev = 0
+        for s in range(1, steps + 1):
+            rep = disc.step()
+            ref = dumps["state_%05d" % s]
+            out = disc.download()
+            assert rep.substeps == int(ref["substeps"]) - prev, "substep count differs"
+            prev = int(ref["substeps"])
+            errs = {k: _oracle.rel_err(out[k], ref[k]) for k in fields + ("energy",)}
+            print(case, "DT", s, rep.substeps, errs)
+            assert all(e <= TOL_DT for e in errs.values()), errs

@@ -49,7 +49,7 @@ def test_params_defaults_and_switches():
 def test_unsupported_features_are_refused(tmp_path):
     from dustyfargoadsg_b200 import Disc, FbError, read_par
     src = os.path.join(CFG, "iso_128x384.par")
-    for key, val in (("InnerBoundary", "Non-Reflecting"), ("Frame", "C"), ("DustFluid", "Yes"),
+    for key, val in (("InnerBoundary", "Accreting"), ("Frame", "C"), ("DustFluid", "Yes"),
                      ("ThermalCooling", "Yes")):
         par = _oracle.write_par(src, str(tmp_path), **{key: val})
         p = read_par(par)
@@ -125,3 +125,18 @@ def test_initial_particles_bit_identical(tmp_path, keys):
     np.testing.assert_array_equal(arrays["l"], arrays["r"] * arrays["vth"])
     assert st.rng_x == int(ref["rng_state"])
     assert st.kicks == 0
+
+
+def test_inner_boundary_switches():
+    """INNERBOUNDARY by first letter (src/Interpret.c:168-175): W wall, O open,
+    K Kley & Nelson open, N non-reflecting; A (accreting) is refused."""
+    import tempfile
+
+    from dustyfargoadsg_b200 import read_par
+    src = os.path.join(CFG, "iso_128x384.par")
+    want = {"Wall": (1, 0, 0, 0), "Open": (0, 1, 0, 0), "KNOpen": (0, 1, 1, 0), "Non-Reflecting": (0, 0, 0, 1)}
+    with tempfile.TemporaryDirectory() as wd:
+        for val, flags in want.items():
+            p = read_par(_oracle.write_par(src, wd, InnerBoundary=val))
+            assert (p.wall_boundary, p.open_inner, p.kn_open, p.non_reflecting) == flags, val
+            assert p.unsupported == 0, val
