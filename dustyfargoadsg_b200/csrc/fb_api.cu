@@ -230,6 +230,14 @@ static int dust_create(fb_ctx *ctx)
   pp.ring_inv_r0 = 1.0 / g.rinf[0];
   pp.ring_inv_step = p->log_grid ? (double)ctx->nr / log(g.rsup[ctx->nr - 1] / g.rinf[0])
                                  : (double)ctx->nr / (g.rsup[ctx->nr - 1] - g.rinf[0]);
+  {
+    std::vector<double> lri(ctx->nr + 1), lrm(ctx->nr);
+    for (int i = 0; i <= ctx->nr; i++) lri[i] = log(g.rinf[i]);
+    for (int i = 0; i < ctx->nr; i++) lrm[i] = log(g.rmed[i]);
+    pp.log_rinf = dtable(ctx, lri.data(), ctx->nr + 1);
+    pp.log_rmed = dtable(ctx, lrm.data(), ctx->nr);
+    if (!pp.log_rinf || !pp.log_rmed) return FB_ERR_NOMEM;
+  }
   ctx->has_dust = 1;
   return FB_OK;
 }

@@ -257,6 +257,9 @@ struct PP {
   // first guess of a particle's ring from the grid law (log or arithmetic),
   // corrected exactly against the radii
   double ring_r0, ring_inv_r0, ring_inv_step;
+  // log of the interface and centre radii (glibc log on the host): the fast
+  // build takes a TSC weight's |log(rp / R)| as |log rp - log R|
+  const double *log_rinf, *log_rmed;
 };
 
 // launchers (fb_gas.cu)

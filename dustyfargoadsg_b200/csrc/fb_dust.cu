@@ -443,14 +443,23 @@ __global__ void __launch_bounds__(D_BS, 3) k_dust_update(KP k, PP pp, int mode)
   // is computed once and reused, as the same values enter the sums.
   double wr_inf[3], wr_med[3], wt_c[3], wt_i[3];
   int jc[3], ji[3];
+#if FB_FAST
+  // one logarithm per particle: |log(rp / R)| as |log rp - log R|
+  const double lrp = pp.log_grid ? log(rp) : 0.0;
+#endif
 #pragma unroll
   for (int t = 0; t < 3; t++) {
     const int i = ip - 1 + t;
     if (i >= 0 && i <= nr - 1) {
+#if FB_FAST
+      wr_inf[t] = tsc_weight(pp.log_grid ? fabs(lrp - pp.log_rinf[i]) : fabs(rp - k.rinf[i]), delta_r, rdelta_r);
+      wr_med[t] = tsc_weight(pp.log_grid ? fabs(lrp - pp.log_rmed[i]) : fabs(rp - k.rmed[i]), delta_r, rdelta_r);
+#else
       wr_inf[t] = tsc_weight(pp.log_grid ? fabs(log(fb_quot(rp, k.rinf[i], k.invrinf[i]))) : fabs(rp - k.rinf[i]),
                              delta_r, rdelta_r);
       wr_med[t] = tsc_weight(pp.log_grid ? fabs(log(fb_quot(rp, k.rmed[i], k.invrmed[i]))) : fabs(rp - k.rmed[i]),
                              delta_r, rdelta_r);
+#endif
     } else {
       wr_inf[t] = wr_med[t] = 0.0;
     }

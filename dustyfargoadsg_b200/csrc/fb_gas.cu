@@ -1720,10 +1720,30 @@ static __device__ __forceinline__ void azr_load(const double *p, double (&v)[E])
 // ... (the ring mean's order).  The results of own cell c0 + e land at cell
 // p = c0 + e + nshift (mod nsec): out(e, p, vtheta, density, RadMomP,
 // RadMomM, energy).
+// The ring's entries of the 1-D tables, loaded together with the ring's
+// fields (not one by one where the arithmetic first needs them).
+struct AzrTab {
+  double invrmed, rmed, dxtheta, invdxtheta, rsup, rinf, surf, vthetamed, energymed;
+};
+static __device__ __forceinline__ AzrTab azr_tab(const KP &k, int i)
+{
+  AzrTab t;
+  t.invrmed = k.invrmed[i];
+  t.rmed = k.rmed[i];
+  t.dxtheta = k.dxtheta[i];
+  t.invdxtheta = k.invdxtheta[i];
+  t.rsup = k.rsup[i];
+  t.rinf = k.rinf[i];
+  t.surf = k.surf[i];
+  t.vthetamed = k.vthetamed ? k.vthetamed[i] : 0.0;
+  t.energymed = (k.energy && k.energymed) ? k.energymed[i] : 0.0;
+  return t;
+}
+
 template <int NQ, int E, class Out>
-static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, double (&q0)[NQ][E],
-                                                const double (&vt)[E], const double (&vs)[E], double *sh,
-                                                double (*hal)[2][AZR_MAXW][AZR_NV], int &xb, Out out)
+static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, const AzrTab &tb,
+                                                double (&q0)[NQ][E], const double (&vt)[E], const double (&vs)[E],
+                                                double *sh, double (*hal)[2][AZR_MAXW][AZR_NV], int &xb, Out out)
 {
   const int ns = k.ns, nr = k.nr, T = blockDim.x, tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5, nw = T >> 5;
@@ -1743,10 +1763,10 @@ static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, d
   const double VMed = s / (double)ns;
   // ComputeConstantResidual (TransportEuler.c:310-348)
   const double dpinvns = (k.pmax - k.pmin) / (double)ns;
-  const double Ntilde = VMed * k.invrmed[i] * dt * (double)ns / (k.pmax - k.pmin);
+  const double Ntilde = VMed * tb.invrmed * dt * (double)ns / (k.pmax - k.pmin);
   const double Nround = floor(Ntilde + 0.5);
   const long nshift = (long)Nround;
-  double vconst = (Ntilde - Nround) * k.rmed[i] * invdt * dpinvns;
+  double vconst = (Ntilde - Nround) * tb.rmed * invdt * dpinvns;
   const double vconst0 = vconst;
   auto vres_of = [&](double vtj) -> double {
     double elong = vtj * dt;
@@ -1755,9 +1775,9 @@ static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, d
     return v;
   };
   if (!k.fast_transport) vconst = 0.0;
-  const double dxtheta = k.dxtheta[i], invdxtheta = k.invdxtheta[i];
-  const double dxrad = (k.rsup[i] - k.rinf[i]) * dt;
-  const double invsurf = 1.0 / k.surf[i];
+  const double dxtheta = tb.dxtheta, invdxtheta = tb.invdxtheta;
+  const double dxrad = (tb.rsup - tb.rinf) * dt;
+  const double invsurf = 1.0 / tb.surf;
   for (int pass = 0; pass < 2; pass++) {
     const bool uniform = (pass == 1);
     if (uniform && !k.fast_transport) break;  // NoSplitAdvection: no update
@@ -1879,19 +1899,19 @@ static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, d
   }
 #undef AZR_X
   const int subkep = (!k.transport_only) && (i == 0 || i == nr - 1);
-  const double rmi = k.rmed[i];
+  const double rmi = tb.rmed;
 #pragma unroll
   for (int e = 0; e < E; e++) {
     int p = c0 + e + shift;
     if (p >= ns) p -= ns;
     const double tpm = (e == 0) ? xl[0] : q0[2][e - 1], rm = (e == 0) ? xl[1] : q0[RH][e - 1];
     double v = (tpm + q0[3][e]) / (q0[RH][e] + rm + 1e-20) / rmi - rmi * k.omega_frame;
-    if (subkep) v = k.vthetamed[i] - rmi * k.omega_frame;
+    if (subkep) v = tb.vthetamed - rmi * k.omega_frame;
     double en = 0.0;
     if (NQ == 6) {
       en = q0[(NQ == 6) ? 4 : 0][e];
       if (k.add_floors && !k.transport_only) {
-        double e_bottom = 1e-3 * k.energymed[i];
+        double e_bottom = 1e-3 * tb.energymed;
         if (en < e_bottom) en = e_bottom;
       }
     }
@@ -1918,7 +1938,8 @@ __global__ void __launch_bounds__(MT) k_transport_azimuthal_reg(KP k, double dto
   azr_load<E>(k.vt + base + c0, vt);
 #pragma unroll
   for (int e = 0; e < E; e++) vs[e] = k.vt[base + tid + e * T];
-  azr_ring<NQ, E>(k, dt, i, q0, vt, vs, sh, hal, xb,
+  const AzrTab tb = azr_tab(k, i);
+  azr_ring<NQ, E>(k, dt, i, tb, q0, vt, vs, sh, hal, xb,
                   [&](int p, double v, double r, double a, double b, double en) {
                     k.vt[base + p] = v;
                     k.rho_t[base + p] = r;
@@ -2009,6 +2030,7 @@ __global__ void __launch_bounds__(MT) k_transport_azimuthal_staged(KP k, double 
   for (int i = blockIdx.x; i < nr; i += gridDim.x, it++) {
     const int b = it & 1;
     const size_t base = (size_t)i * ns;
+    const AzrTab tb = azr_tab(k, i);  // in flight while the copies complete
     // the next ring into the other buffer, once the bulk stores of the ring
     // it held last have read it
     if (tid == 0 && i + (int)gridDim.x < nr) {
@@ -2031,7 +2053,7 @@ __global__ void __launch_bounds__(MT) k_transport_azimuthal_staged(KP k, double 
     }
     __syncthreads();  // every row read: the buffer takes the results
     double *o = buf + (size_t)b * NB * ns;
-    azr_ring<NQ, E>(k, dt, i, q0, vt, vs, sh, hal, xb,
+    azr_ring<NQ, E>(k, dt, i, tb, q0, vt, vs, sh, hal, xb,
                     [&](int p, double v, double r, double a, double bb, double en) {
                       o[p] = v;
                       o[(size_t)ns + p] = r;

@@ -75,11 +75,20 @@ def test_headline_workload_two_dts(headline, mode):
     _run(par, 2, 1e-4, 0, ("dens", "vrad", "vtheta", "energy"), dumps=dumps, mode=mode)
 
 
-def test_dust_workload_full_size(tmp_path):
+@pytest.fixture(scope="module")
+def dust_full(tmp_path_factory):
+    par = _oracle.write_par(os.path.join(CFG, "dust_256x768.par"), str(tmp_path_factory.mktemp("dust")))
+    dumps, _, _ = _oracle.run_oracle(par, steps=1, noise=1e-4, seed=0, timeout=3000)
+    return par, dumps
+
+
+@pytest.mark.parametrize("mode", ["parity", "fast"])
+def test_dust_workload_full_size(dust_full, mode):
     """The particle workload as it is: 256 x 768 gas with 200,000 particles
-    and turbulent kicks, one whole DT."""
-    par = _oracle.write_par(os.path.join(CFG, "dust_256x768.par"), str(tmp_path))
-    _run(par, 1, 1e-4, 0, ("dens", "vrad", "vtheta"), dust=True, dust_seed=0)
+    and turbulent kicks, one whole DT, with both builds (the fast one takes
+    the TSC weights' |log(rp/R)| as |log rp - log R|)."""
+    par, dumps = dust_full
+    _run(par, 1, 1e-4, 0, ("dens", "vrad", "vtheta"), dust=True, dust_seed=0, dumps=dumps, mode=mode)
 
 
 @pytest.mark.parametrize("case", ["gas", "particles"])
