@@ -34,6 +34,8 @@ class FbParams(C.Structure):
         ("alphaviscosity", _D), ("viscosity", _D),
         ("adiabaticindex", _D), ("energy_equation", _I), ("viscous_heating", _I),
         ("beta_cooling", _I), ("betacoolingtime", _D), ("betacoolingslope", _D),
+        ("thermal_cooling", _I), ("constant_opacity", _I), ("imposedconstantopacity", _D),
+        ("factoropacities", _D),
         ("self_gravity", _I), ("sgthicknesssmoothing", _D),
         ("thicknesssmoothing", _D), ("rochesmoothing", _D), ("indirecttermsmoothing", _D),
         ("masstaper", _D), ("omegaframe", _D),

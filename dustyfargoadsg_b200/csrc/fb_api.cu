@@ -406,6 +406,13 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.beta_cooling = p->beta_cooling;
   k.fast_transport = p->fast_transport;
   k.wall = p->wall_boundary;
+  k.thermal_cooling = p->energy_equation && p->thermal_cooling;
+  if (k.thermal_cooling) {
+    // sigma_SB in code units (LowTasks.c:215)
+    k.sigma_sb = 5.6704e-8 * pow(fb_unit_mass(p), -1) * pow(fb_unit_time(p), 3.) * pow(fb_unit_temperature(p), 4.);
+    k.opacity = dalloc(ctx, nf);
+    if (!k.opacity) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+  }
   k.open_inner = p->open_inner;
   k.kn_open = p->kn_open;
   k.non_reflecting = p->non_reflecting;
@@ -528,6 +535,14 @@ extern "C" int fb_upload(fb_ctx *ctx, const fb_state *s, const fb_profiles *prof
     k_fill_cs_iso<<<256, 256, 0, ctx->st>>>(k);
   } else {
     fb_launch_soundspeed(k, 0, ctx->st);
+  }
+  if (k.thermal_cooling) {
+    // the opacity of the uploaded state, which the step keeps, as the
+    // reference computes it once in InitEuler (SourceEuler.c:275)
+    const fb_params *pp = &ctx->p;
+    const double um = fb_unit_mass(pp), ul = fb_unit_length(pp);
+    fb_launch_opacity(k, pp->constant_opacity, pp->imposedconstantopacity, pp->factoropacities,
+                      fb_unit_temperature(pp), um, pow(ul, -3.), 0.1 * pow(ul, -2.0) * pow(um, 1.0), ctx->st);
   }
   // scalar state
   fb_ctl *c = ctx->h_ctl;

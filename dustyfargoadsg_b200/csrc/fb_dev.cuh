@@ -95,6 +95,12 @@ struct KP {
   // pow(Rinf[1], -1.5), pow(Rinf[nr-2], -1.5), the initial sound speeds of
   // rings 0 and 1 (adiabatic), SIGMASLOPE, Radii[0] and Radii[nr]
   int open_inner, kn_open, non_reflecting;
+  // thermal cooling (SourceEuler.c:1201-1290): the opacity field, set once
+  // from the uploaded state as InitEuler sets it (SourceEuler.c:275), and
+  // the Stefan-Boltzmann constant in code units (LowTasks.c:215)
+  int thermal_cooling;
+  double *opacity;
+  double sigma_sb;
   double ob_vt1, ob_vt0, ob_vtout, nrb_om1, nrb_omn2, nrb_csinit0, nrb_csinit1, sigmaslope;
   double radii0, radiin;
   double floordens, wkzrmin, wkzrmax;
@@ -277,6 +283,10 @@ void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
 void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_transport_vr(const KP &k, cudaStream_t s);
 void fb_launch_edges(const KP &k, cudaStream_t s);  // open / non-reflecting edges
+// ComputeOpacities (SourceEuler.c:1608-1701) of the current state:
+// constant = SETCONSTANTOPACITY; conv = 0.1 unit_length^-2 unit_mass
+void fb_launch_opacity(const KP &k, int constant, double imposed, double factor, double unit_temperature,
+                       double unit_mass, double inv_l3, double conv, cudaStream_t s);
 void fb_launch_floors_boundary(const KP &k, cudaStream_t s);
 void fb_launch_damping(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_diag(const KP &k, double *out2, cudaStream_t s);

@@ -981,14 +981,80 @@ __global__ void __launch_bounds__(FB_BS2) k_substep3(KP k)
     k.vischeat[l] = vh;
   }
   const double dv = st.div;
-  double num = el + (double)(heat ? 1 : 0) * vh * dt;
-  double den = 1.0 + (k.gamma - 1.0) * dt * dv;
-  double en = num / den;
-  if (k.beta_cooling) {
-    const double d2 = 1.0 + dt / coolfac;  // one per ring: the quotient through its reciprocal
-    en = fb_quot(en, d2, 1.0 / d2);
+  double en;
+  if (k.thermal_cooling) {
+    // implicit update with thermal cooling, without stellar irradiation
+    // (SourceEuler.c:1201-1290); beta cooling does not apply then
+    const double tau = 0.5 * k.opacity[l] * rl;
+    const double tau_eff = 0.375 * tau + 0.25 * sqrt(3.0) + 0.25 / tau;
+    const double temp = (k.gamma - 1.0) * el * (1.0 / rl);
+    const double num = el + dt * (vh * (double)(heat ? 1 : 0) + (6.0 * k.sigma_sb / tau_eff) * pow(temp, 4.0));
+    const double den = 1.0 + (k.gamma - 1.0) * dt * dv +
+                       8.0 * dt * (k.sigma_sb / tau_eff) * (k.gamma - 1.0) * pow(temp, 3.0) * (1.0 / rl);
+    en = num / den;
+  } else {
+    double num = el + (double)(heat ? 1 : 0) * vh * dt;
+    double den = 1.0 + (k.gamma - 1.0) * dt * dv;
+    en = num / den;
+    if (k.beta_cooling) {
+      const double d2 = 1.0 + dt / coolfac;  // one per ring: the quotient through its reciprocal
+      en = fb_quot(en, d2, 1.0 / d2);
+    }
   }
   k.e[l] = en;
+}
+
+// ComputeOpacities (SourceEuler.c:1608-1701): Bell & Lin (1994) opacities of
+// the cells of rings 0..nr-1 from their temperature and 3-D density, or the
+// imposed constant, in code units.
+__global__ void __launch_bounds__(FB_BS2) k_opacity(KP k, int constant, double imposed, double factor,
+                                                   double unit_temperature, double unit_mass, double inv_l3,
+                                                   double conv)
+{
+  fb_grid_dependency();
+  const int ns = k.ns;
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= ns) return;
+  const size_t l = (size_t)i * ns + j;
+  double op;
+  if (!constant) {
+    const double energ = k.e[l], dens = k.rho[l];
+    const double temp = (k.gamma - 1.0) * energ * (1.0 / dens);
+    const double phys_temp = temp * unit_temperature;
+    const double roversigma = k.rmed[i] / dens;
+    const double buf = k.gamma * (k.gamma - 1.0) * energ * pow(roversigma, 3.);
+    const double rho3D = 0.5 * pow(buf, -0.5);
+    double phys_dens = rho3D * unit_mass * inv_l3;  // kg m^-3 (inv_l3 = pow(unit_length, -3.))
+    phys_dens *= 1e-3;                                // g cm^-3
+    if (phys_temp < 167.0) {
+      op = 2e-4 * pow(phys_temp, 2.0);
+    } else if (phys_temp < 203.0) {
+      op = 2e16 * pow(phys_temp, -7.0);
+    } else if (phys_temp < pow(2e82 * phys_dens, 2. / 49)) {
+      op = 0.1 * pow(phys_temp, 0.5);
+    } else if (phys_temp < pow(2e89 * pow(phys_dens, 1. / 3), 1. / 27)) {
+      op = 2e81 * pow(phys_dens, 1.0) * pow(phys_temp, -24.);
+    } else if (phys_temp < pow(1e28 * pow(phys_dens, 1. / 3), 1. / 7)) {
+      op = 1e-8 * pow(phys_dens, 2. / 3) * pow(phys_temp, 3.);
+    } else if (phys_temp < pow(1.5e56 * pow(phys_dens, 2. / 3), 0.08)) {
+      op = 1e-36 * pow(phys_dens, 1. / 3) * pow(phys_temp, 10.);
+    } else if (phys_temp < pow(4.31e20 * phys_dens, 2. / 5)) {
+      op = 1.5e20 * pow(phys_dens, 1.) * pow(phys_temp, -2.5);
+    } else {
+      op = 0.348;
+    }
+    op *= factor;
+  } else {
+    op = imposed;
+  }
+  k.opacity[l] = op * conv;
+}
+
+void fb_launch_opacity(const KP &k, int constant, double imposed, double factor, double unit_temperature,
+                       double unit_mass, double inv_l3, double conv, cudaStream_t s)
+{
+  fb_launch(k_opacity, grid2d(k, k.nr), k.cell_bs, 0, s, k, constant, imposed, factor, unit_temperature, unit_mass,
+            inv_l3, conv);
 }
 
 void fb_launch_substep3(const KP &k, cudaStream_t s) { fb_launch(k_substep3, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k); }
@@ -2315,7 +2381,9 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
   fb_launch(k_transport_azimuthal_staged<NQ, EE, MM>,                                                   \
             azs_grid((const void *)k_transport_azimuthal_staged<NQ, EE, MM>, MM, smem, k.nr), T, smem, s, k, \
             dt_override)
-#define AZS_E(EE) (T <= 256 ? AZS_LAUNCH(EE, 256) : T <= 512 ? AZS_LAUNCH(EE, 512) : AZS_LAUNCH(EE, 768))
+#define AZS_E(EE)                                                                                   \
+  (T <= 256 ? AZS_LAUNCH(EE, 256) : T <= 384 ? AZS_LAUNCH(EE, 384) : T <= 512 ? AZS_LAUNCH(EE, 512)  \
+                                                                   : AZS_LAUNCH(EE, 768))
     switch (E) {
       case 2: AZS_E(2); break;
       case 3: AZS_E(3); break;
@@ -2326,11 +2394,12 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
     return;
   }
   if (var == 4) {
-    // the instance bounded by the smallest of 256 / 512 / 768 threads that
-    // holds T: the fewer threads, the more registers each may use
+    // the instance bounded by the smallest of 256 / 384 / 512 / 768 threads
+    // that holds T: the fewer threads, the more registers each may use
     const int T = k.ns / E;
 #define AZR_LAUNCH(EE)                                                                                   \
   (T <= 256 ? fb_launch(k_transport_azimuthal_reg<NQ, EE, 256>, k.nr, T, 0, s, k, dt_override)            \
+   : T <= 384 ? fb_launch(k_transport_azimuthal_reg<NQ, EE, 384>, k.nr, T, 0, s, k, dt_override)          \
    : T <= 512 ? fb_launch(k_transport_azimuthal_reg<NQ, EE, 512>, k.nr, T, 0, s, k, dt_override)          \
               : fb_launch(k_transport_azimuthal_reg<NQ, EE, 768>, k.nr, T, 0, s, k, dt_override))
     switch (E) {
@@ -2845,6 +2914,7 @@ int fb_gas_prepare(int ns, int energy)
   }
 #define AZS_FNS(NQ, EE)                                                                  \
   (const void *)k_transport_azimuthal_staged<NQ, EE, 256>,                               \
+      (const void *)k_transport_azimuthal_staged<NQ, EE, 384>,                           \
       (const void *)k_transport_azimuthal_staged<NQ, EE, 512>,                           \
       (const void *)k_transport_azimuthal_staged<NQ, EE, 768>
   {

@@ -64,6 +64,10 @@ int fb_params_default(fb_params *p)
   p->adiabaticindex = 1.4;
   p->betacoolingtime = 10.0;
   p->betacoolingslope = 0.0;
+  p->thermal_cooling = 0;          /* THERMALCOOLING NO, SETCONSTANTOPACITY NO */
+  p->constant_opacity = 0;
+  p->imposedconstantopacity = 0.1; /* src/var.c:193-195 */
+  p->factoropacities = 1.0;
   p->dampingtodynamicaltimeratio = 0.3;
   p->wkzrmin = 0.0;
   p->wkzrmax = 0.0;
@@ -227,6 +231,8 @@ int fb_params_read_par(fb_params *p, const char *path)
   p->adiabaticindex = kv_num(&set, "ADIABATICINDEX", p->adiabaticindex);
   p->betacoolingtime = kv_num(&set, "BETACOOLINGTIME", p->betacoolingtime);
   p->betacoolingslope = kv_num(&set, "BETACOOLINGSLOPE", p->betacoolingslope);
+  p->imposedconstantopacity = kv_num(&set, "IMPOSEDCONSTANTOPACITY", p->imposedconstantopacity);
+  p->factoropacities = kv_num(&set, "FACTOROPACITIES", p->factoropacities);
   p->dampingtodynamicaltimeratio = kv_num(&set, "DAMPINGTODYNAMICALTIMERATIO", p->dampingtodynamicaltimeratio);
   p->wkzrmin = kv_num(&set, "WKZRMIN", p->wkzrmin);
   p->wkzrmax = kv_num(&set, "WKZRMAX", p->wkzrmax);
@@ -285,7 +291,10 @@ int fb_params_read_par(fb_params *p, const char *path)
   if (is_c(kv_c(&set, "ENTROPYDIFFUSION", 'N'), 'Y')) p->unsupported |= FB_U_THERMALDIFF;
   c = kv_c(&set, "RADIATIVEDIFFUSION", 'N');
   if (is_c(c, 'E') || is_c(c, 'I')) p->unsupported |= FB_U_THERMALDIFF;
-  if (is_c(kv_c(&set, "THERMALCOOLING", 'N'), 'Y')) p->unsupported |= FB_U_THERMALCOOLING;
+  if (is_c(kv_c(&set, "THERMALCOOLING", 'N'), 'Y')) p->thermal_cooling = 1;
+  if (is_c(kv_c(&set, "SETCONSTANTOPACITY", 'N'), 'Y')) p->constant_opacity = 1;
+  c = kv_c(&set, "STELLARIRRADIATION", 'N');
+  if (is_c(c, 'Y') || is_c(c, 'L')) p->unsupported |= FB_U_IRRADIATION;
   if (is_c(kv_c(&set, "TEMPPRESC", 'N'), 'Y')) p->unsupported |= FB_U_TEMPPRESC;
   if (is_c(kv_c(&set, "FORCEDCIRCULAR", 'N'), 'Y')) p->forced_circular = 1;
   if (is_c(kv_c(&set, "FORCEDINNERCIRCULAR", 'N'), 'Y')) p->unsupported |= FB_U_FORCEDINNER;
@@ -364,7 +373,7 @@ const char *fb_unsupported_name(const fb_params *p)
     {FB_U_ADDMASS, "AddMass"}, {FB_U_EVAPORATION, "DiscEvaporation"},
     {FB_U_PHOTOEVAP, "PhotoEvaporation"}, {FB_U_SGZEROMODE, "SelfGravity Z (zero mode)"},
     {FB_U_ZMPLUS, "ZMPlus"}, {FB_U_MHDLSA, "MHD LSA turbulence"},
-    {FB_U_THERMALDIFF, "Entropy/radiative diffusion"}, {FB_U_THERMALCOOLING, "ThermalCooling"},
+    {FB_U_THERMALDIFF, "Entropy/radiative diffusion"}, {FB_U_THERMALCOOLING, "ThermalCooling"}, {FB_U_IRRADIATION, "StellarIrradiation"},
     {FB_U_TEMPPRESC, "TempPresc"}, {FB_U_COROTATING, "Corotating frame"},
     {FB_U_CICPLANET, "CICPlanet"}, {FB_U_BM08, "BM08Trick"}, {FB_U_CPDMASS, "ComputeCPDMass"},
     {FB_U_LABEL, "LabelAdvection"}, {FB_U_IMPOSEDDENSITY, "ImposedDensity"},
@@ -722,6 +731,15 @@ done:
 /* ComputeCodeUnits (src/LowTasks.c:202-213) */
 double fb_unit_length(const fb_params *p) { return 1.49598e11 * p->factorunitlength; }
 double fb_unit_mass(const fb_params *p) { return 1.9891e30 * p->factorunitmass; }
+double fb_unit_time(const fb_params *p)
+{
+  return sqrt(pow(fb_unit_length(p), 3.) / 6.673e-11 / fb_unit_mass(p));
+}
+double fb_unit_temperature(const fb_params *p)
+{
+  const double mmw = 2.35 * p->factormmw;
+  return mmw * 8.0841643e-15 * fb_unit_mass(p) / fb_unit_length(p);
+}
 
 /* InitDustSystem (src/Dsys.c:128-262), new particles, one process. */
 int fb_init_dust(const fb_params *p, fb_ctx *ctx, long seed, fb_dust_state *st)

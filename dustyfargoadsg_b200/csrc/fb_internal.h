@@ -59,6 +59,7 @@ extern "C" {
 #define FB_U_INTERPOLATION    (1ull << 40)
 #define FB_U_DUSTSGZERO       (1ull << 41)
 #define FB_U_SOFTWRITING      (1ull << 42)
+#define FB_U_IRRADIATION      (1ull << 43)
 
 /* 1-D geometry of FillPolar1DArrays (src/SourceEuler.c:71-188) for one
  * process holding all rings (IMIN = 0, GLOBALNRAD = NRAD). */
@@ -94,6 +95,8 @@ int fb_sg_axisym_accel(fb_ctx *ctx, const double *dens, double *axi_out);
 int fb_sg_axisym_accel_device(fb_ctx *ctx, double *axi_out);
 /* Units of ComputeCodeUnits (src/LowTasks.c:202-229). */
 double fb_unit_length(const fb_params *p);
+double fb_unit_time(const fb_params *p);         /* LowTasks.c:212 */
+double fb_unit_temperature(const fb_params *p);  /* LowTasks.c:213 */
 double fb_unit_mass(const fb_params *p);
 /* Geometry held by a context (NULL if none). */
 const fb_geom *fb_ctx_geom(const fb_ctx *ctx);

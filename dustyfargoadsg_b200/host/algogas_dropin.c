@@ -36,7 +36,7 @@ extern boolean BM08, DustFeedback, Write_Temperature, Write_Potential;
 extern boolean DustFeelDisk, DustFeelPlanets, DustFeelTurb, DustFeelSG, DustFeelSGZeroMode;
 extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensity, ZZIntegrator;
 extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
-extern boolean CompareSGAndSummationTorques, KNOpen;
+extern boolean CompareSGAndSummationTorques, KNOpen, SetConstantOpacity, StellarIrradiation;
 extern Pair DiskOnPrimaryAcceleration, DiskOnPrimaryAcceleration_alt;
 
 static fb_ctx *g_ctx = NULL;
@@ -127,7 +127,11 @@ static void params_from_globals(fb_params *p)
   if (ZMPlus) p->unsupported |= FB_U_ZMPLUS;
   if (MHDLSA) p->unsupported |= FB_U_MHDLSA;
   if (EntropyDiffusion || RadiativeDiffusion) p->unsupported |= FB_U_THERMALDIFF;
-  if (ThermalCooling) p->unsupported |= FB_U_THERMALCOOLING;
+  p->thermal_cooling = ThermalCooling;
+  p->constant_opacity = SetConstantOpacity;
+  p->imposedconstantopacity = IMPOSEDCONSTANTOPACITY;
+  p->factoropacities = FACTOROPACITIES;
+  if (StellarIrradiation) p->unsupported |= FB_U_IRRADIATION;
   if (TempPresc) p->unsupported |= FB_U_TEMPPRESC;
   if (Corotating) p->unsupported |= FB_U_COROTATING;
   if (BM08) p->unsupported |= FB_U_BM08;

@@ -66,10 +66,14 @@ typedef struct fb_params {
   /* ALPHAVISCOSITY, VISCOSITY */
   double alphaviscosity, viscosity;
   /* thermodynamics: ADIABATICINDEX, ENERGYEQUATION, VISCOUSHEATING,
-     BETACOOLING, BETACOOLINGTIME, BETACOOLINGSLOPE */
+     BETACOOLING, BETACOOLINGTIME, BETACOOLINGSLOPE; thermal cooling below */
   double adiabaticindex;
   int energy_equation, viscous_heating, beta_cooling;
   double betacoolingtime, betacoolingslope;
+  /* THERMALCOOLING (radiative cooling with Bell & Lin opacities),
+     SETCONSTANTOPACITY, IMPOSEDCONSTANTOPACITY, FACTOROPACITIES */
+  int thermal_cooling, constant_opacity;
+  double imposedconstantopacity, factoropacities;
   /* self-gravity: SELFGRAVITY (Yes), SGTHICKNESSSMOOTHING */
   int self_gravity;
   double sgthicknesssmoothing;

@@ -52,3 +52,32 @@ def test_edges_match_oracle(tmp_path, case):
             errs = {k: _oracle.rel_err(out[k], ref[k]) for k in fields + ("energy",)}
             print(case, "DT", s, rep.substeps, errs)
             assert all(e <= TOL_DT for e in errs.values()), errs
+
+
+@pytest.mark.parametrize("opacity", ["BellLin", "constant"])
+def test_thermal_cooling_matches_oracle(tmp_path, opacity):
+    """Radiative cooling in SubStep3 (SourceEuler.c:1201-1290, without stellar
+    irradiation), with the Bell & Lin opacities of the initial state
+    (ComputeOpacities, SourceEuler.c:1608-1701, which the reference computes
+    once, in InitEuler) or an imposed constant one; adiabatic 64 x 192 disc,
+    3 DTs, fields within 1e-11."""
+    from dustyfargoadsg_b200 import Disc, read_par
+    keys = dict(Nrad=64, Nsec=192, SelfGravity="No", BetaCooling="No", ThermalCooling="Yes")
+    if opacity == "constant":
+        keys.update(SetConstantOpacity="Yes", ImposedConstantOpacity="0.5")
+    par = _oracle.write_par(os.path.join(CFG, "adiabatic_sg_512x1536.par"), str(tmp_path), **keys)
+    p = read_par(par)
+    assert p.unsupported == 0 and p.thermal_cooling == 1
+    steps = 3
+    dumps, _, _ = _oracle.run_oracle(par, steps=steps, noise=1e-3, seed=8)
+    with Disc(p, noise=1e-3, seed=8) as disc:
+        prev = 0
+        for s in range(1, steps + 1):
+            rep = disc.step()
+            ref = dumps["state_%05d" % s]
+            out = disc.download()
+            assert rep.substeps == int(ref["substeps"]) - prev, "substep count differs"
+            prev = int(ref["substeps"])
+            errs = {k: _oracle.rel_err(out[k], ref[k]) for k in ("dens", "vrad", "vtheta", "energy")}
+            print("thermal cooling", opacity, "DT", s, rep.substeps, errs)
+            assert all(e <= TOL_DT for e in errs.values()), errs
