@@ -35,7 +35,8 @@ class FbParams(C.Structure):
         ("adiabaticindex", _D), ("energy_equation", _I), ("viscous_heating", _I),
         ("beta_cooling", _I), ("betacoolingtime", _D), ("betacoolingslope", _D),
         ("thermal_cooling", _I), ("constant_opacity", _I), ("imposedconstantopacity", _D),
-        ("factoropacities", _D),
+        ("factoropacities", _D), ("stellar_irradiation", _I), ("backgroundtemperature", _D),
+        ("slopebackgroundtemperature", _D), ("stellarluminosity", _D),
         ("self_gravity", _I), ("sgthicknesssmoothing", _D),
         ("thicknesssmoothing", _D), ("rochesmoothing", _D), ("indirecttermsmoothing", _D),
         ("masstaper", _D), ("omegaframe", _D),

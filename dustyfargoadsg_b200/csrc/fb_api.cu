@@ -412,6 +412,18 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
     k.sigma_sb = 5.6704e-8 * pow(fb_unit_mass(p), -1) * pow(fb_unit_time(p), 3.) * pow(fb_unit_temperature(p), 4.);
     k.opacity = dalloc(ctx, nf);
     if (!k.opacity) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+    k.irradiation = p->stellar_irradiation;
+    if (k.irradiation) {  // per ring, as SubStep3 evaluates them (SourceEuler.c:1204-1268)
+      const double um = fb_unit_mass(p), ul = fb_unit_length(p), ut = fb_unit_time(p);
+      const double Lstar = p->stellarluminosity * 3.8e26 * pow(um, -1.0) * pow(ul, -2.0) * pow(ut, 3.0);
+      std::vector<double> irr(nr);
+      for (int i = 0; i < nr; i++)
+        irr[i] = (k.irradiation == 1)
+                     ? (p->backgroundtemperature / fb_unit_temperature(p)) * pow(ctx->g.rmed[i], p->slopebackgroundtemperature)
+                     : Lstar / 4.0 / M_PI / ctx->g.rmed[i] / ctx->g.rmed[i];
+      k.irr_ring = dtable(ctx, irr.data(), nr);
+      if (!k.irr_ring) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+    }
   }
   k.open_inner = p->open_inner;
   k.kn_open = p->kn_open;

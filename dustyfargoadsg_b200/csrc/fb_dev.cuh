@@ -101,6 +101,11 @@ struct KP {
   int thermal_cooling;
   double *opacity;
   double sigma_sb;
+  // stellar irradiation: 0 none, 1 background temperature (irr_ring[i] =
+  // its value at Rmed[i]), 2 imposed luminosity (irr_ring[i] =
+  // Lstar/4/pi/Rmed[i]/Rmed[i])
+  int irradiation;
+  const double *irr_ring;
   double ob_vt1, ob_vt0, ob_vtout, nrb_om1, nrb_omn2, nrb_csinit0, nrb_csinit1, sigmaslope;
   double radii0, radiin;
   double floordens, wkzrmin, wkzrmax;

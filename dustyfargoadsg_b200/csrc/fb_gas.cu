@@ -983,12 +983,29 @@ __global__ void __launch_bounds__(FB_BS2) k_substep3(KP k)
   const double dv = st.div;
   double en;
   if (k.thermal_cooling) {
-    // implicit update with thermal cooling, without stellar irradiation
+    // implicit update with thermal cooling and stellar irradiation
     // (SourceEuler.c:1201-1290); beta cooling does not apply then
     const double tau = 0.5 * k.opacity[l] * rl;
     const double tau_eff = 0.375 * tau + 0.25 * sqrt(3.0) + 0.25 / tau;
     const double temp = (k.gamma - 1.0) * el * (1.0 / rl);
-    const double num = el + dt * (vh * (double)(heat ? 1 : 0) + (6.0 * k.sigma_sb / tau_eff) * pow(temp, 4.0));
+    double num;
+    if (k.irradiation) {
+      double temp_irr;
+      if (k.irradiation == 1) {
+        temp_irr = k.irr_ring[i];
+      } else {
+        // the grazing angle as the reference finally sets it (:1257; the
+        // radial temperature gradient computed before it is not used)
+        const double albedo = 0.1;
+        const double costheta = 0.5 * sqrt(k.rmed[i] * temp) * (2.0 * k.flaringindex);
+        const double buf = 0.5 * (tau_eff / k.sigma_sb) * (1.0 - albedo) * k.irr_ring[i] * costheta;
+        temp_irr = pow(buf, 0.25);  // NaN stops the step (FB_ERR_NAN); the reference exits
+      }
+      num = el + dt * (vh * (double)(heat ? 1 : 0) +
+                       (2.0 * k.sigma_sb / tau_eff) * (3.0 * pow(temp, 4.0) + pow(temp_irr, 4.0)));
+    } else {
+      num = el + dt * (vh * (double)(heat ? 1 : 0) + (6.0 * k.sigma_sb / tau_eff) * pow(temp, 4.0));
+    }
     const double den = 1.0 + (k.gamma - 1.0) * dt * dv +
                        8.0 * dt * (k.sigma_sb / tau_eff) * (k.gamma - 1.0) * pow(temp, 3.0) * (1.0 / rl);
     en = num / den;

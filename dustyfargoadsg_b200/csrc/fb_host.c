@@ -68,6 +68,10 @@ int fb_params_default(fb_params *p)
   p->constant_opacity = 0;
   p->imposedconstantopacity = 0.1; /* src/var.c:193-195 */
   p->factoropacities = 1.0;
+  p->stellar_irradiation = 0;          /* src/var.c:88-91 */
+  p->backgroundtemperature = 50.0;
+  p->slopebackgroundtemperature = -0.5;
+  p->stellarluminosity = 1.0;
   p->dampingtodynamicaltimeratio = 0.3;
   p->wkzrmin = 0.0;
   p->wkzrmax = 0.0;
@@ -233,6 +237,9 @@ int fb_params_read_par(fb_params *p, const char *path)
   p->betacoolingslope = kv_num(&set, "BETACOOLINGSLOPE", p->betacoolingslope);
   p->imposedconstantopacity = kv_num(&set, "IMPOSEDCONSTANTOPACITY", p->imposedconstantopacity);
   p->factoropacities = kv_num(&set, "FACTOROPACITIES", p->factoropacities);
+  p->backgroundtemperature = kv_num(&set, "BACKGROUNDTEMPERATURE", p->backgroundtemperature);
+  p->slopebackgroundtemperature = kv_num(&set, "SLOPEBACKGROUNDTEMPERATURE", p->slopebackgroundtemperature);
+  p->stellarluminosity = kv_num(&set, "STELLARLUMINOSITY", p->stellarluminosity);
   p->dampingtodynamicaltimeratio = kv_num(&set, "DAMPINGTODYNAMICALTIMERATIO", p->dampingtodynamicaltimeratio);
   p->wkzrmin = kv_num(&set, "WKZRMIN", p->wkzrmin);
   p->wkzrmax = kv_num(&set, "WKZRMAX", p->wkzrmax);
@@ -294,7 +301,8 @@ int fb_params_read_par(fb_params *p, const char *path)
   if (is_c(kv_c(&set, "THERMALCOOLING", 'N'), 'Y')) p->thermal_cooling = 1;
   if (is_c(kv_c(&set, "SETCONSTANTOPACITY", 'N'), 'Y')) p->constant_opacity = 1;
   c = kv_c(&set, "STELLARIRRADIATION", 'N');
-  if (is_c(c, 'Y') || is_c(c, 'L')) p->unsupported |= FB_U_IRRADIATION;
+  if (is_c(c, 'Y')) p->stellar_irradiation = 1;
+  if (is_c(c, 'L')) p->stellar_irradiation = 2;
   if (is_c(kv_c(&set, "TEMPPRESC", 'N'), 'Y')) p->unsupported |= FB_U_TEMPPRESC;
   if (is_c(kv_c(&set, "FORCEDCIRCULAR", 'N'), 'Y')) p->forced_circular = 1;
   if (is_c(kv_c(&set, "FORCEDINNERCIRCULAR", 'N'), 'Y')) p->unsupported |= FB_U_FORCEDINNER;

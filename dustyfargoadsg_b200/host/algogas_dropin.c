@@ -36,7 +36,7 @@ extern boolean BM08, DustFeedback, Write_Temperature, Write_Potential;
 extern boolean DustFeelDisk, DustFeelPlanets, DustFeelTurb, DustFeelSG, DustFeelSGZeroMode;
 extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensity, ZZIntegrator;
 extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
-extern boolean CompareSGAndSummationTorques, KNOpen, SetConstantOpacity, StellarIrradiation;
+extern boolean CompareSGAndSummationTorques, KNOpen, SetConstantOpacity, StellarIrradiation, ImposedStellarLuminosity;
 extern Pair DiskOnPrimaryAcceleration, DiskOnPrimaryAcceleration_alt;
 
 static fb_ctx *g_ctx = NULL;
@@ -131,7 +131,10 @@ static void params_from_globals(fb_params *p)
   p->constant_opacity = SetConstantOpacity;
   p->imposedconstantopacity = IMPOSEDCONSTANTOPACITY;
   p->factoropacities = FACTOROPACITIES;
-  if (StellarIrradiation) p->unsupported |= FB_U_IRRADIATION;
+  p->stellar_irradiation = StellarIrradiation ? (ImposedStellarLuminosity ? 2 : 1) : 0;
+  p->backgroundtemperature = BACKGROUNDTEMPERATURE;
+  p->slopebackgroundtemperature = SLOPEBACKGROUNDTEMPERATURE;
+  p->stellarluminosity = STELLARLUMINOSITY;
   if (TempPresc) p->unsupported |= FB_U_TEMPPRESC;
   if (Corotating) p->unsupported |= FB_U_COROTATING;
   if (BM08) p->unsupported |= FB_U_BM08;

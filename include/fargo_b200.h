@@ -71,9 +71,14 @@ typedef struct fb_params {
   int energy_equation, viscous_heating, beta_cooling;
   double betacoolingtime, betacoolingslope;
   /* THERMALCOOLING (radiative cooling with Bell & Lin opacities),
-     SETCONSTANTOPACITY, IMPOSEDCONSTANTOPACITY, FACTOROPACITIES */
+     SETCONSTANTOPACITY, IMPOSEDCONSTANTOPACITY, FACTOROPACITIES;
+     STELLARIRRADIATION (0 No, 1 Yes: a background temperature
+     BACKGROUNDTEMPERATURE r^SLOPEBACKGROUNDTEMPERATURE, 2 L: heating by a
+     star of STELLARLUMINOSITY solar luminosities) */
   int thermal_cooling, constant_opacity;
   double imposedconstantopacity, factoropacities;
+  int stellar_irradiation;
+  double backgroundtemperature, slopebackgroundtemperature, stellarluminosity;
   /* self-gravity: SELFGRAVITY (Yes), SGTHICKNESSSMOOTHING */
   int self_gravity;
   double sgthicknesssmoothing;

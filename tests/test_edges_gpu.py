@@ -54,17 +54,22 @@ def test_edges_match_oracle(tmp_path, case):
             assert all(e <= TOL_DT for e in errs.values()), errs
 
 
-@pytest.mark.parametrize("opacity", ["BellLin", "constant"])
+@pytest.mark.parametrize("opacity", ["BellLin", "constant", "irradiated", "luminosity"])
 def test_thermal_cooling_matches_oracle(tmp_path, opacity):
-    """Radiative cooling in SubStep3 (SourceEuler.c:1201-1290, without stellar
-    irradiation), with the Bell & Lin opacities of the initial state
+    """Radiative cooling in SubStep3 (SourceEuler.c:1201-1290), with the Bell &
+    Lin opacities of the initial state
     (ComputeOpacities, SourceEuler.c:1608-1701, which the reference computes
-    once, in InitEuler) or an imposed constant one; adiabatic 64 x 192 disc,
-    3 DTs, fields within 1e-11."""
+    once, in InitEuler) or an imposed constant one, and with the star's
+    irradiation as a background temperature or from its luminosity;
+    adiabatic 64 x 192 disc, 3 DTs, fields within 1e-11."""
     from dustyfargoadsg_b200 import Disc, read_par
     keys = dict(Nrad=64, Nsec=192, SelfGravity="No", BetaCooling="No", ThermalCooling="Yes")
     if opacity == "constant":
         keys.update(SetConstantOpacity="Yes", ImposedConstantOpacity="0.5")
+    if opacity == "irradiated":  # a background temperature profile (SourceEuler.c:1218-1226)
+        keys.update(StellarIrradiation="Yes", BackgroundTemperature="30.0", SlopeBackgroundTemperature="-0.5")
+    if opacity == "luminosity":  # heating by the star's imposed luminosity (SourceEuler.c:1227-1268)
+        keys.update(StellarIrradiation="L", StellarLuminosity="1.0", FlaringIndex="0.25")
     par = _oracle.write_par(os.path.join(CFG, "adiabatic_sg_512x1536.par"), str(tmp_path), **keys)
     p = read_par(par)
     assert p.unsupported == 0 and p.thermal_cooling == 1

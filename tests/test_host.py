@@ -50,7 +50,7 @@ def test_unsupported_features_are_refused(tmp_path):
     from dustyfargoadsg_b200 import Disc, FbError, read_par
     src = os.path.join(CFG, "iso_128x384.par")
     for key, val in (("InnerBoundary", "Accreting"), ("Frame", "C"), ("DustFluid", "Yes"),
-                     ("StellarIrradiation", "Yes")):
+                     ("EntropyDiffusion", "Yes")):
         par = _oracle.write_par(src, str(tmp_path), **{key: val})
         p = read_par(par)
         assert p.unsupported != 0, key
