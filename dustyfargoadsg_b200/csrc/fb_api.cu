@@ -1019,6 +1019,10 @@ extern "C" int fb_stage(fb_ctx *ctx, int stage, double dt)
       break;
     case FB_STAGE_BOUNDARY:
       fb_launch_boundary_only(k, s);
+      if (k.open_inner || k.non_reflecting) {  // ApplyBoundaryCondition's other edges, as in the substep
+        if (k.non_reflecting && k.energy) fb_launch_soundspeed(k, 0, s);
+        fb_launch_edges(k, s);
+      }
       break;
     case FB_STAGE_DAMPING:
       if (!(dt > 0.0)) return FB_ERR_INVALID;

@@ -392,7 +392,8 @@ const char *fb_last_error(const fb_ctx *ctx);
 #define FB_STAGE_TRANSPORT  1  /* Transport (src/TransportEuler.c:65)       */
 #define FB_STAGE_VISCOSITY  2  /* ComputeViscousTerms + UpdateVelocitiesWithViscosity
                                   on (vrad, vtheta, dens) (src/Viscosity.c:159-378) */
-#define FB_STAGE_BOUNDARY   3  /* ApplyBoundaryCondition (src/SideEuler.c:1102) */
+#define FB_STAGE_BOUNDARY   3  /* ApplyBoundaryCondition (src/SideEuler.c:1102): walls,
+                                  sub-Keplerian edges, open and non-reflecting edges */
 #define FB_STAGE_DAMPING    4  /* EvanescentBoundary (src/SideEuler.c:796)  */
 #define FB_STAGE_SELFGRAV   5  /* compute_sgacc only: fills SG accelerations */
 int fb_stage(fb_ctx *ctx, int stage, double dt);
