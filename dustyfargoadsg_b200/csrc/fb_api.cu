@@ -285,12 +285,15 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.nf = nf;
   double **fields[] = {&k.rho, &k.vr, &k.vt, &k.e, &k.cs, &k.pres, &k.pot, &k.vri, &k.vti,
                        &k.divv, &k.trr, &k.tpp, &k.trp, &k.vischeat, &k.q[0], &k.q[1], &k.q[2],
-                       &k.q[3], &k.q[4], &k.q[5], &k.rho_t, &k.sg_accr, &k.sg_acct};
+                       &k.q[3], &k.q[4], &k.q[5], &k.rho_t, &k.sg_accr, &k.sg_acct,
+                       &k.azt_buf[0], &k.azt_buf[1], &k.azt_buf[2]};
   for (size_t f = 0; f < sizeof fields / sizeof fields[0]; f++) {
     *fields[f] = dalloc(ctx, nf);
     if (!*fields[f]) { fb_destroy(ctx); return FB_ERR_NOMEM; }
   }
   k.lost0 = dalloc(ctx, ns);
+  k.azt_vmed = dalloc(ctx, nr);
+  if (!k.lost0 || !k.azt_vmed) { fb_destroy(ctx); return FB_ERR_NOMEM; }
   if (p->energy_equation) {  // only the energy test can crash (DetectCrash as AlgoGas uses it)
     k.crash_snap = dalloc(ctx, (size_t)4 * nr * ns);
     if (!k.crash_snap) { fb_destroy(ctx); return FB_ERR_NOMEM; }
@@ -429,6 +432,10 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.kn_open = p->kn_open;
   k.non_reflecting = p->non_reflecting;
   k.sigmaslope = p->sigmaslope;
+  if (p->non_reflecting) {
+    k.edge_buf = dalloc(ctx, (size_t)3 * ns);
+    if (!k.edge_buf) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+  }
   if (p->open_inner || p->non_reflecting) {  // the edges' constants, as the reference evaluates them
     const fb_geom &gg = ctx->g;
     k.ob_vt1 = sqrt(gg.rmed[2] / gg.rmed[1]);
@@ -668,6 +675,7 @@ static int enqueue_substep(fb_ctx *ctx)
   if (k.energy) STAGE(ST_SUB3, 1, fb_launch_substep3(k, s));  // with the stresses of the new velocities
   STAGE(ST_TRAD, 1, fb_launch_transport_radial(k, 0.0, s));
   STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s));
+  ctx->launches += fb_azi_launches(k) - 1;  // the tile variant's ring means: one pass, two kernels
   STAGE(ST_TVR, 1, fb_launch_transport_vr(k, s));
   if (k.open_inner || k.non_reflecting) {
     // ApplyBoundaryCondition's other edges (SideEuler.c:1102-1131); the
@@ -1363,7 +1371,7 @@ extern "C" int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t)
   if (t->rad_columns && (t->rad_columns < 32 || t->rad_columns > 128 || t->rad_columns % 32)) return FB_ERR_INVALID;
   if (t->rad_rings < 0 || t->rad_rings > k.nr) return FB_ERR_INVALID;
   const int E = t->azi_cells_per_thread ? t->azi_cells_per_thread : fb_azi_E_auto(k.ns);
-  if (t->azi_variant < 0 || t->azi_variant > 5 || !fb_azi_variant(k.ns, k.energy, E, t->azi_variant))
+  if (t->azi_variant < 0 || t->azi_variant > 7 || !fb_azi_variant(k.ns, k.energy, E, t->azi_variant))
     return FB_ERR_INVALID;
   k.cell_bs = cb;
   k.azi_variant = t->azi_variant;
@@ -1480,7 +1488,7 @@ extern "C" int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_ou
     double bestms = 1e300;
     for (int E = 1; E <= 4; E++) {
       if (!fb_azi_E_valid(k.ns, k.energy, E)) continue;
-      for (int var = 1; var <= 5; var++) {
+      for (int var = 1; var <= 7; var++) {
         if (fb_azi_variant(k.ns, k.energy, E, var) != var) continue;
         k.azi_E = E;
         k.azi_variant = var;

@@ -58,6 +58,11 @@ struct KP {
   double *divv, *trr, *tpp, *trp, *vischeat;
   double *q[6];        // transport: RadMomP, RadMomM, ThetaMomP, ThetaMomM, Energy, Rho
   double *rho_t;       // density after transport, before floors
+  // tile variant of the azimuthal pass: RadMomP and RadMomM after the radial
+  // pass and a copy of vtheta (three fields), and the ring means of vtheta
+  // (nr); vt_copy is azt_buf[2] in the radial pass feeding the tile variant,
+  // else NULL
+  double *azt_buf[3], *azt_vmed, *vt_copy;
   double *crash_snap;  // 4 x nr*ns: density, vrad, vtheta, energy of the first crash
   double *lost0;       // ns: ring-0 radial mass fluxes of the last substep
   double *sg_accr, *sg_acct;  // SG accelerations (nf)
@@ -95,6 +100,7 @@ struct KP {
   // pow(Rinf[1], -1.5), pow(Rinf[nr-2], -1.5), the initial sound speeds of
   // rings 0 and 1 (adiabatic), SIGMASLOPE, Radii[0] and Radii[nr]
   int open_inner, kn_open, non_reflecting;
+  double *edge_buf;  // 3 nsec: the non-reflecting edges' copies, read before written
   // thermal cooling (SourceEuler.c:1201-1290): the opacity field, set once
   // from the uploaded state as InitEuler sets it (SourceEuler.c:275), and
   // the Stefan-Boltzmann constant in code units (LowTasks.c:215)
@@ -125,7 +131,7 @@ struct KP {
   // launch shapes (tuning): per-cell CTA width, cells per thread of the
   // azimuthal pass (0 = automatic), columns per CTA and rings per CTA of the
   // radial pass (0 = automatic), variant of the azimuthal pass (0 automatic,
-  // 1 narrow, 2 wide, 3 packed)
+  // 1 narrow, 2 wide, 3 packed, 4 register, 5 staged, 6 tile)
   int cell_bs, azi_E, rad_tx, rad_chunk, azi_variant;
 };
 
@@ -302,6 +308,7 @@ int  fb_transport_preload(void);          // loads the radial and vr transport k
 // launch-shape candidates the tuner may try (fb_gas.cu)
 int  fb_azi_E_valid(int ns, int energy, int E);   // 1 if E cells/thread fit this ring
 int  fb_azi_E_auto(int ns);
+int  fb_azi_launches(const KP &k);  // kernel launches of one azimuthal pass
 int  fb_azi_variant(int ns, int energy, int E, int variant);  // variant a launch takes (0: cannot run)
 int  fb_rad_chunk_auto(const KP &k);
 int  fb_rad_chunks_balanced(const KP &k, int tx, int *out, int max);

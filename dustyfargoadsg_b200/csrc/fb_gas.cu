@@ -1112,6 +1112,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
       } else {
         w.u0 = k.vt[l];
         if (NQ == 6) w.u1 = k.e[l];
+        if (k.vt_copy && kk >= i0 && kk < i1) k.vt_copy[l] = w.u0;  // for the tile variant
       }
     }
     if (kk >= 0 && kk <= nr) w.v = k.vr[(size_t)kk * ns + j];
@@ -1823,27 +1824,53 @@ static __device__ __forceinline__ AzrTab azr_tab(const KP &k, int i)
   return t;
 }
 
-template <int NQ, int E, class Out>
+// Neighbour values within one warp only (the tile variant): lane 0's left
+// and lane 31's right neighbours are its own values, which only the tile's
+// halo cells read.
+template <int NL, int NR>
+static __device__ __forceinline__ void azt_exchange(const double *sL, double *rL, const double *sR, double *rR)
+{
+#pragma unroll
+  for (int v = 0; v < NL; v++) rL[v] = __shfl_up_sync(0xffffffffu, sL[v], 1);
+#pragma unroll
+  for (int v = 0; v < NR; v++) rR[v] = __shfl_down_sync(0xffffffffu, sR[v], 1);
+}
+
+// TILE = false: the register variant, one CTA per ring, c0 = tid E, the ring
+// mean from vs by one CTA reduction, neighbours across warps through hal.
+// TILE = true: the tile variant, one warp per tile of the ring, c0 = the
+// ring cell of the warp's first loaded cell plus lane E (any integer: taken
+// modulo nsec), the ring mean vmed_in given, no barrier at all.
+template <int NQ, int E, bool TILE, class Out>
 static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, const AzrTab &tb,
                                                 double (&q0)[NQ][E], const double (&vt)[E], const double (&vs)[E],
-                                                double *sh, double (*hal)[2][AZR_MAXW][AZR_NV], int &xb, Out out)
+                                                double vmed_in, int c0, double *sh,
+                                                double (*hal)[2][AZR_MAXW][AZR_NV], int &xb, Out out)
 {
   const int ns = k.ns, nr = k.nr, T = blockDim.x, tid = threadIdx.x;
   const int lane = tid & 31, w = tid >> 5, nw = T >> 5;
   const int wl = (w == 0) ? nw - 1 : w - 1, wr = (w == nw - 1) ? 0 : w + 1;
-  const int c0 = tid * E;
   constexpr int RH = NQ - 1;  // the density is the last quantity
-#define AZR_X(NL, NR, sL, rL, sR, rR) azr_exchange<NL, NR>(hal, xb, lane, w, wl, wr, sL, rL, sR, rR)
+#define AZR_X(NL, NR, sL, rL, sR, rR)                                       \
+  do {                                                                      \
+    if (TILE)                                                               \
+      azt_exchange<NL, NR>(sL, rL, sR, rR);                                 \
+    else                                                                    \
+      azr_exchange<NL, NR>(hal, xb, lane, w, wl, wr, sL, rL, sR, rR);       \
+  } while (0)
   // ComputeThetaElongations / ComputeAverageThetaVelocities / ComputeResiduals
   const double invdt = 1.0 / dt;
-  double s = 0.0;
+  double VMed = vmed_in;
+  if (!TILE) {
+    double s = 0.0;
 #pragma unroll
-  for (int e = 0; e < E; e++) {
-    double elong = vs[e] * dt;
-    s += elong * invdt;
+    for (int e = 0; e < E; e++) {
+      double elong = vs[e] * dt;
+      s += elong * invdt;
+    }
+    s = block_sum_dyn(s, sh);
+    VMed = s / (double)ns;
   }
-  s = block_sum_dyn(s, sh);
-  const double VMed = s / (double)ns;
   // ComputeConstantResidual (TransportEuler.c:310-348)
   const double dpinvns = (k.pmax - k.pmin) / (double)ns;
   const double Ntilde = VMed * tb.invrmed * dt * (double)ns / (k.pmax - k.pmin);
@@ -1985,7 +2012,14 @@ static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, c
   const double rmi = tb.rmed;
 #pragma unroll
   for (int e = 0; e < E; e++) {
-    int p = c0 + e + shift;
+    int p;
+    if (TILE) {
+      int g = (c0 + e) % ns;
+      if (g < 0) g += ns;
+      p = g + shift;
+    } else {
+      p = c0 + e + shift;
+    }
     if (p >= ns) p -= ns;
     const double tpm = (e == 0) ? xl[0] : q0[2][e - 1], rm = (e == 0) ? xl[1] : q0[RH][e - 1];
     double v = (tpm + q0[3][e]) / (q0[RH][e] + rm + 1e-20) / rmi - rmi * k.omega_frame;
@@ -1998,7 +2032,7 @@ static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, c
         if (en < e_bottom) en = e_bottom;
       }
     }
-    out(p, v, q0[RH][e], q0[0][e], q0[1][e], en);
+    out(e, p, v, q0[RH][e], q0[0][e], q0[1][e], en);
   }
 }
 
@@ -2022,14 +2056,93 @@ __global__ void __launch_bounds__(MT) k_transport_azimuthal_reg(KP k, double dto
 #pragma unroll
   for (int e = 0; e < E; e++) vs[e] = k.vt[base + tid + e * T];
   const AzrTab tb = azr_tab(k, i);
-  azr_ring<NQ, E>(k, dt, i, tb, q0, vt, vs, sh, hal, xb,
-                  [&](int p, double v, double r, double a, double b, double en) {
+  azr_ring<NQ, E, false>(k, dt, i, tb, q0, vt, vs, 0.0, c0, sh, hal, xb,
+                         [&](int, int p, double v, double r, double a, double b, double en) {
                     k.vt[base + p] = v;
                     k.rho_t[base + p] = r;
                     k.q[0][base + p] = a;
                     k.q[1][base + p] = b;
                     if (NQ == 6) k.e[base + p] = en;
                   });
+}
+
+// Tile variant of the azimuthal pass (variant 6): the register variant's
+// arithmetic with no barrier.  A ring is cut into tiles of AZT_CO(E) = 32 E -
+// 9 cells, one warp each (AZT_WPC warps of any rings per CTA).  A warp loads
+// 32 E consecutive cells, the tile with 5 cells before it and 4 after, and
+// advances all of them: a van Leer pass changes a cell from its neighbours
+// up to two cells away, so after the residual and the uniform pass the
+// cells 4 .. 32 E - 5 are exact, and ComputeVelocities' vtheta, which reads
+// the cell before, is exact on the 32 E - 9 cells from the sixth on.  The
+// halo costs 9 / (32 E) of redundant arithmetic; in exchange every
+// neighbour value moves by a warp shuffle and the warps of an SM run
+// independently.  Tiles of one ring run in different CTAs, so the pass
+// cannot work in place: the radial pass leaves RadMomP, RadMomM and a copy
+// of vtheta in three scratch fields (azt_buf) and this pass writes the usual
+// outputs.  The ring mean of vtheta comes from k_azi_vmed, summed in the
+// order of the register variant's CTA of azi_threads_for(nsec, E) threads,
+// so for the same E the results agree to the last bit.
+#define AZT_WPC 4
+#define AZT_LEFT 5
+#define AZT_HALO 9
+#define AZT_CO(E) (32 * (E) - AZT_HALO)
+
+__global__ void __launch_bounds__(1024) k_azi_vmed(KP k, double dtov)
+{
+  fb_grid_dependency();
+  __shared__ double sh[32];
+  const double dt = dt_of(k, dtov);
+  const int i = blockIdx.x, ns = k.ns, T = blockDim.x;
+  const double *vt = k.vt + (size_t)i * ns;
+  const double invdt = 1.0 / dt;
+  double s = 0.0;
+  for (int j = threadIdx.x; j < ns; j += T) {
+    double elong = vt[j] * dt;
+    s += elong * invdt;
+  }
+  s = block_sum_dyn(s, sh);
+  if (threadIdx.x == 0) k.azt_vmed[i] = s / (double)ns;
+}
+
+template <int NQ, int E, int MINB>
+__global__ void __launch_bounds__(AZT_WPC * 32, MINB) k_transport_azimuthal_tile(KP k, double dtov)
+{
+  fb_grid_dependency();
+  const double dt = dt_of(k, dtov);
+  const int ns = k.ns;
+  constexpr int CO = AZT_CO(E);
+  const int ntiles = (ns + CO - 1) / CO;
+  const int gw = blockIdx.x * AZT_WPC + (threadIdx.x >> 5);
+  if (gw >= k.nr * ntiles) return;  // the whole warp
+  const int i = gw / ntiles, t = gw - i * ntiles;
+  const int lane = threadIdx.x & 31;
+  const size_t base = (size_t)i * ns;
+  const int c0 = t * CO - AZT_LEFT + lane * E;
+  double q0[NQ][E], vt[E], vs[E];
+#pragma unroll
+  for (int e = 0; e < E; e++) {
+    int g = (c0 + e) % ns;
+    if (g < 0) g += ns;
+    const size_t l = base + g;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) q0[q][e] = (q < 2 ? k.azt_buf[q] : k.q[q])[l];
+    vt[e] = k.azt_buf[2][l];
+    vs[e] = 0.0;
+  }
+  const AzrTab tb = azr_tab(k, i);
+  const double vmed = k.azt_vmed[i];
+  int xb = 0;
+  const int m0 = lane * E - AZT_LEFT, tcell = t * CO;  // tile cell of own cell e: m0 + e
+  azr_ring<NQ, E, true>(k, dt, i, tb, q0, vt, vs, vmed, c0, nullptr, nullptr, xb,
+                        [&](int e, int p, double v, double r, double a, double b, double en) {
+                          const int m = m0 + e;
+                          if (m < 0 || m >= CO || tcell + m >= ns) return;
+                          k.vt[base + p] = v;
+                          k.rho_t[base + p] = r;
+                          k.q[0][base + p] = a;
+                          k.q[1][base + p] = b;
+                          if (NQ == 6) k.e[base + p] = en;
+                        });
 }
 
 // Staged variant of the azimuthal pass (variant 5): the register variant's
@@ -2136,8 +2249,8 @@ __global__ void __launch_bounds__(MT) k_transport_azimuthal_staged(KP k, double 
     }
     __syncthreads();  // every row read: the buffer takes the results
     double *o = buf + (size_t)b * NB * ns;
-    azr_ring<NQ, E>(k, dt, i, tb, q0, vt, vs, sh, hal, xb,
-                    [&](int p, double v, double r, double a, double bb, double en) {
+    azr_ring<NQ, E, false>(k, dt, i, tb, q0, vt, vs, 0.0, tid * E, sh, hal, xb,
+                           [&](int, int p, double v, double r, double a, double bb, double en) {
                       o[p] = v;
                       o[(size_t)ns + p] = r;
                       o[(size_t)2 * ns + p] = a;
@@ -2236,6 +2349,9 @@ static int azs_grid(const void *fn, int threads, size_t smem, int nr)
   const int g = sms * per_sm;
   return g < nr ? g : nr;
 }
+// The tile variant: 2 to 4 cells per lane, and the ring-mean kernel's CTA
+// of azi_threads_for(nsec, E) threads within 1024.
+static bool azt_fits(int ns, int E) { return E >= 2 && E <= 4 && azi_threads_for(ns, E) <= 1024; }
 int fb_azi_variant(int ns, int energy, int E, int variant)
 {
   const int NQ = energy ? 6 : 5;
@@ -2247,9 +2363,28 @@ int fb_azi_variant(int ns, int energy, int E, int variant)
     case 3: return packed ? 3 : 0;
     case 4: return azr_fits(ns, E) ? 4 : 0;
     case 5: return azs_fits(ns, energy, E) ? 5 : 0;
+    case 6: return azt_fits(ns, E) ? 6 : 0;
+    case 7: return azt_fits(ns, E) ? 7 : 0;
     default: return 0;
   }
 }
+// The variant and cells per thread a launch of this KP's azimuthal pass
+// takes: the tuned ones where they can run, the staged variant only on
+// 16-byte aligned fields, the tile variant only with its scratch fields.
+static int azi_resolve(const KP &k, int *Eout)
+{
+  const int NQ = k.energy ? 6 : 5;
+  const int E = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
+  int var = fb_azi_variant(k.ns, k.energy, E, k.azi_variant);
+  if (var == 0) var = 1;
+  if (var == 5 && !azs_pointers_aligned(k, NQ)) var = 4;  // bulk copies need 16-byte aligned rows
+  if ((var == 6 || var == 7) && !(k.azt_buf[0] && k.azt_buf[1] && k.azt_buf[2] && k.azt_vmed))
+    var = azr_fits(k.ns, E) ? 4 : 1;
+  if (Eout) *Eout = E;
+  return var;
+}
+static bool azt_variant(int var) { return var == 6 || var == 7; }
+int fb_azi_launches(const KP &k) { return azt_variant(azi_resolve(k, nullptr)) ? 2 : 1; }
 
 // LostMass += LostByDisk of the density's VanLeerRadial (TransportEuler.c:137,
 // :213-216): the ring-0 radial fluxes summed over azimuth by one warp, lane
@@ -2370,8 +2505,17 @@ int fb_rad_chunk_auto(const KP &k)
   return best;
 }
 
-void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
+void fb_launch_transport_radial(const KP &k0, double dt_override, cudaStream_t s)
 {
+  // before the tile variant: RadMomP, RadMomM and a copy of vtheta into its
+  // scratch fields (it cannot update them in place)
+  KP k = k0;
+  k.vt_copy = nullptr;
+  if (azt_variant(azi_resolve(k0, nullptr))) {
+    k.q[0] = k0.azt_buf[0];
+    k.q[1] = k0.azt_buf[1];
+    k.vt_copy = k0.azt_buf[2];
+  }
   const int tx = k.rad_tx > 0 ? k.rad_tx : 64, bx = (k.ns + tx - 1) / tx;
   const int chunk = k.rad_chunk > 0 ? k.rad_chunk : fb_rad_chunk_auto(k);
   dim3 gr(bx, (k.nr + chunk - 1) / chunk);
@@ -2384,13 +2528,32 @@ void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s)
 template <int NQ>
 static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
 {
-  const int E = k.azi_E > 0 ? k.azi_E : fb_azi_E_auto(k.ns);
-  int var = fb_azi_variant(k.ns, NQ == 6, E, k.azi_variant);
-  if (var == 0) var = 1;
+  int E = 1;
+  const int var = azi_resolve(k, &E);
   const bool wide = (var == 2);
   const int th = azi_threads_for(k.ns, E);
   const bool full = (th * E == k.ns);  // every thread owns E cells
-  if (var == 5 && !azs_pointers_aligned(k, NQ)) var = 4;  // bulk copies need 16-byte aligned rows
+  if (var == 6 || var == 7) {
+    fb_launch(k_azi_vmed, k.nr, th, 0, s, k, dt_override);
+    const int CO = AZT_CO(E), ntiles = (k.ns + CO - 1) / CO;
+    const int grid = (int)(((long)k.nr * ntiles + AZT_WPC - 1) / AZT_WPC);
+#define AZT_LAUNCH(EE, MB) fb_launch(k_transport_azimuthal_tile<NQ, EE, MB>, grid, AZT_WPC * 32, 0, s, k, dt_override)
+    if (var == 6) {
+      switch (E) {
+        case 2: AZT_LAUNCH(2, 4); break;
+        case 3: AZT_LAUNCH(3, 4); break;
+        default: AZT_LAUNCH(4, 4); break;
+      }
+    } else {
+      switch (E) {
+        case 2: AZT_LAUNCH(2, 3); break;
+        case 3: AZT_LAUNCH(3, 3); break;
+        default: AZT_LAUNCH(4, 3); break;
+      }
+    }
+#undef AZT_LAUNCH
+    return;
+  }
   if (var == 5) {
     const int T = k.ns / E;
     const size_t smem = azs_smem_bytes(k.ns, NQ);
@@ -2557,8 +2720,11 @@ __global__ void __launch_bounds__(EDGE_BS) k_edges(KP k)
       }
     }
     const int i = 1;
+    // the ring means and the shift (SideEuler.c:607-626 isothermal,
+    // :662-674 adiabatic)
+    double cs1 = 0.0, d1 = 0.0, dangle;
     if (!k.energy) {
-      double cs0 = 0.0, cs1 = 0.0, d0 = 0.0, d1 = 0.0;
+      double cs0 = 0.0, d0 = 0.0;
       for (int j = tid; j < ns; j += T) {
         cs0 += cs[j];
         cs1 += cs[ns + j];
@@ -2570,38 +2736,50 @@ __global__ void __launch_bounds__(EDGE_BS) k_edges(KP k)
       d0 = block_sum_dyn(d0, sh) / (double)ns;  // dens0: unused without an accreting edge
       d1 = block_sum_dyn(d1, sh) / (double)ns;
       (void)d0;
-      double dangle = (k.nrb_om1 - omega_in) / (.5 * (cs0 + cs1));
-      dangle *= (k.rmed[1] - k.rmed[0]);
-      const int i_angle = (int)(dangle / (k.pmax - k.pmin) * (double)ns + .5);
-      for (int j = tid; j < ns; j += T) {
-        const size_t l = (size_t)j + (size_t)i * ns;
-        int jp = j + i_angle;
-        if (jp >= ns) jp -= ns;
-        if (jp < 0) jp += ns;
-        rho[jp] = rho[l];
-        const double vr_med = -cs1 * (rho[l] - d1) / d1;
-        vr[l] = 2. * vr_med - vr[l + ns];
-      }
-      __syncthreads();
+      dangle = (k.nrb_om1 - omega_in) / (.5 * (cs0 + cs1));
+    } else {
+      dangle = (k.nrb_om1 - omega_in) / (.5 * (k.nrb_csinit0 + k.nrb_csinit1));
+    }
+    dangle *= (k.rmed[1] - k.rmed[0]);
+    const int i_angle = (int)(dangle / (k.pmax - k.pmin) * (double)ns + .5);
+    // The reference's loop copies ring 1 into ring 0 shifted by i_angle
+    // cells, wrapping once: a shift beyond one turn writes cells of ring 1
+    // the loop has already read (the same values result when every read is
+    // done before any write).  A shift beyond two turns, or one that writes
+    // below ring 0, is not reproduced: the DT stops with
+    // FB_ERR_UNSUPPORTED.  The density (isothermal) or the energy
+    // (adiabatic) is copied; vrad from the old density of ring 1.
+    double *f = k.energy ? en : rho, *ebuf = k.edge_buf;
+    int bad = 0;
+    for (int j = tid; j < ns; j += T) {
+      const size_t l = (size_t)j + (size_t)i * ns;
+      int jp = j + i_angle;
+      if (jp >= ns) jp -= ns;
+      if (jp < 0) jp += ns;
+      if (jp < 0 || jp >= 2 * ns || (jp >= ns && jp - ns > j)) bad = 1;
+      ebuf[j] = f[l];
+      const double vr_med = k.energy ? -k.nrb_csinit1 * (rho[l] - k.sigmamed[1]) / k.sigmamed[1]
+                                     : -cs1 * (rho[l] - d1) / d1;
+      vr[l] = 2. * vr_med - vr[l + ns];
+    }
+    if (__syncthreads_or(bad)) {
+      if (tid == 0) k.ctl->status = FB_ERR_UNSUPPORTED;
+      return;
+    }
+    for (int j = tid; j < ns; j += T) {
+      int jp = j + i_angle;
+      if (jp >= ns) jp -= ns;
+      if (jp < 0) jp += ns;
+      f[jp] = ebuf[j];
+    }
+    __syncthreads();
+    if (!k.energy) {
       double mean = 0.0;
       for (int j = tid; j < ns; j += T) mean += rho[j];
       mean = block_sum_dyn(mean, sh) / (double)ns;
       for (int j = tid; j < ns; j += T) rho[j] += (k.sigmamed[0] - mean);
     } else {
-      const double csinit0 = k.nrb_csinit0, csinit1 = k.nrb_csinit1;
-      double dangle = (k.nrb_om1 - omega_in) / (.5 * (csinit0 + csinit1));
-      dangle *= (k.rmed[1] - k.rmed[0]);
-      const int i_angle = (int)(dangle / (k.pmax - k.pmin) * (double)ns + .5);
-      for (int j = tid; j < ns; j += T) {
-        const size_t l = (size_t)j + (size_t)i * ns;
-        int jp = j + i_angle;
-        if (jp >= ns) jp -= ns;
-        if (jp < 0) jp += ns;
-        en[jp] = en[l];
-        const double vr_med = -csinit1 * (rho[l] - k.sigmamed[1]) / k.sigmamed[1];
-        vr[l] = 2. * vr_med - vr[l + ns];
-      }
-      __syncthreads();
+      const double csinit0 = k.nrb_csinit0;
       for (int j = tid; j < ns; j += T)
         rho[j] = k.sigmamed[0] + (k.gamma - 1.0) * (en[j] - k.energymed[0]) / csinit0 / csinit0;
       __syncthreads();
@@ -2625,6 +2803,7 @@ __global__ void __launch_bounds__(EDGE_BS) k_edges(KP k)
         omega_out = pow(rp, -1.5);
       }
     }
+    const int i = nr - 1;
     const size_t b1 = (size_t)(nr - 1) * ns, b2 = (size_t)(nr - 2) * ns;
     double c2 = 0.0, c1 = 0.0, d1 = 0.0, d2 = 0.0;
     for (int j = tid; j < ns; j += T) {
@@ -2641,17 +2820,52 @@ __global__ void __launch_bounds__(EDGE_BS) k_edges(KP k)
     double dangle = (k.nrb_omn2 - omega_out) / (.5 * (csnrm1 + csnrm2));
     dangle *= (k.rmed[nr - 1] - k.rmed[nr - 2]);
     const int i_angle = (int)(dangle / (k.pmax - k.pmin) * (double)ns + .5);
+    // The reference's loop sets cell j of ring nr-1 from cell j - i_angle of
+    // ring nr-2, wrapping once: a shift beyond one turn reads cells of ring
+    // nr-1 itself, the new value where the loop has already written the cell
+    // (followed back to its own source), else the old one.  Every source is
+    // resolved and read before any cell is written.  A source outside rings
+    // 3 .. nr-1 is not reproduced (FB_ERR_UNSUPPORTED).
+    double *bufr = k.edge_buf + ns, *bufe = k.edge_buf + 2 * (size_t)ns;
+    int bad = 0;
     for (int j = tid; j < ns; j += T) {
       const size_t l = (size_t)j + b1;
-      int jp = j - i_angle;
-      if (jp >= ns) jp -= ns;
-      if (jp < 0) jp += ns;
-      const size_t lp = (size_t)jp + b2;
-      rho[l] = rho[lp];
-      en[l] = en[lp];
+      long src = -1;
+      int jj = j;
+      for (int it = 0; it <= ns; it++) {
+        int jp = jj - i_angle;
+        if (jp >= ns) jp -= ns;
+        if (jp < 0) jp += ns;
+        if (jp < ns) {
+          src = (long)(i - 1) * ns + jp;
+          break;
+        }
+        const int cc = jp - ns;  // a cell of ring nr-1
+        if (cc >= ns) break;
+        if (cc < jj) {
+          jj = cc;
+          continue;
+        }
+        src = (long)i * ns + cc;
+        break;
+      }
+      if (src < 3L * ns || src >= (long)nr * ns) {
+        bad = 1;
+        src = (long)l;
+      }
+      bufr[j] = rho[src];
+      bufe[j] = en[src];
       const double vr_med = (!k.energy) ? csnrm1 * (rho[l - ns] - densnrm2) / densnrm2
                                         : cs[l] * (rho[l - ns] - densnrm2) / densnrm2;
       vr[l] = 2. * vr_med - vr[l - ns];
+    }
+    if (__syncthreads_or(bad)) {
+      if (tid == 0) k.ctl->status = FB_ERR_UNSUPPORTED;
+      return;
+    }
+    for (int j = tid; j < ns; j += T) {
+      rho[b1 + j] = bufr[j];
+      en[b1 + j] = bufe[j];
     }
     __syncthreads();
     double mean = 0.0;

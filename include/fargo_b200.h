@@ -309,7 +309,11 @@ typedef struct fb_tuning {
                        4 register (E = 2..4 contiguous cells per thread, quantities in
                        registers; nsec = E T with T a multiple of 32), 5 staged (the
                        register variant in a persistent kernel whose rings arrive and
-                       leave by bulk asynchronous copies, one ring ahead) */
+                       leave by bulk asynchronous copies, one ring ahead), 6 tile (the
+                       register variant's arithmetic with one warp per tile of
+                       32 E - 9 cells and no barrier; E = 2..4; four CTAs of four
+                       warps per SM), 7 (the tile variant with up to 168
+                       registers a thread: three CTAs per SM) */
 } fb_tuning;
 int fb_get_tuning(const fb_ctx *ctx, fb_tuning *t);
 int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t);

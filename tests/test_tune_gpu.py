@@ -54,15 +54,17 @@ def test_azimuthal_variants_are_bit_identical(tmp_path, E, cfg):
     """The narrow (three barriers per quantity), wide (all quantities per
     phase), packed (a cell's quantities side by side), register (E
     contiguous cells per thread, quantities in registers, each face flux
-    evaluated once; E >= 2) and staged (the register variant fed and drained
-    by bulk asynchronous copies) azimuthal passes do the same arithmetic: whole
+    evaluated once; E >= 2), staged (the register variant fed and drained
+    by bulk asynchronous copies) and tile (one warp per tile of 32 E - 9
+    cells with a halo, no barrier; here 3 or 4 tiles per ring, the last one
+    wrapping around the ring; 128 or 168 registers) azimuthal passes do the same arithmetic: whole
     DTs, isothermal or with energy, cooling and self-gravity, must agree to
     the last bit."""
     from dustyfargoadsg_b200 import Disc, read_par
     nsec = 256 if E == 4 else 192  # the register variant needs nsec / E threads, a multiple of 32
     par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, cfg), str(tmp_path), Nrad=64, Nsec=nsec)
     out = {}
-    variants = (1, 2, 3, 4, 5) if E >= 2 else (1, 2, 3)
+    variants = (1, 2, 3, 4, 5, 6, 7) if E >= 2 else (1, 2, 3)
     for variant in variants:
         with Disc(read_par(par), noise=1e-3, seed=4) as d:
             d.set_tuning({"cell_block": 128, "azi_cells_per_thread": E, "azi_variant": variant})
@@ -73,4 +75,26 @@ def test_azimuthal_variants_are_bit_identical(tmp_path, E, cfg):
     fields = FIELDS + (("energy",) if read_par(par).energy_equation else ())
     for v in variants[1:]:
         for k in fields:
+            np.testing.assert_array_equal(out[1][k], out[v][k], err_msg="%s variant %d" % (k, v))
+
+
+@pytest.mark.parametrize("E", [2, 3, 4])
+def test_tile_variant_on_short_rings(tmp_path, E):
+    """Rings shorter than one tile's 32 E loaded cells (nsec 64): the tile
+    wraps around its ring more than once and must still give the narrow
+    variant's results to the last bit (adiabatic disc with cooling and
+    self-gravity, two DTs)."""
+    from dustyfargoadsg_b200 import Disc, read_par
+    par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "adiabatic_sg_512x1536.par"), str(tmp_path),
+                            Nrad=48, Nsec=64)
+    out = {}
+    for variant in (1, 6, 7):
+        with Disc(read_par(par), noise=1e-3, seed=5) as d:
+            d.set_tuning({"cell_block": 128, "azi_cells_per_thread": E, "azi_variant": variant})
+            assert d.tuning()["azi_variant"] == variant
+            for _ in range(2):
+                d.step()
+            out[variant] = d.download()
+    for v in (6, 7):
+        for k in FIELDS + ("energy",):
             np.testing.assert_array_equal(out[1][k], out[v][k], err_msg="%s variant %d" % (k, v))
