@@ -95,11 +95,27 @@ class Disc:
                 self.set_dust(state)
             return
         check(self.lib.fb_upload(self.ctx, C.byref(self.st), C.byref(self.pr)), "fb_upload", self.ctx, self.lib)
+        if self.p.mhd_lsa and self.p.nbturbmodes > 0:
+            # the turbulent modes draw from the reference's global drand48
+            # stream: seeded when the .par is read (Interpret.c:404-407),
+            # reseeded and advanced by the initial noise when there is some
+            self.set_lsa_stream(self.lib.fb_rand48_state(int(seed), self.nr * self.ns if noise else 0))
         if self.npart > 0:
             # InitDustSystem reseeds the stream (Dsys.c:173)
             check(self.lib.fb_init_dust(C.byref(self.p), self.ctx, int(seed if dust_seed is None else dust_seed),
                                         C.byref(self.dst)), "fb_init_dust", self.ctx, self.lib)
             check(self.lib.fb_dust_upload(self.ctx, C.byref(self.dst)), "fb_dust_upload", self.ctx, self.lib)
+
+    # -- turbulent potential -------------------------------------------
+    def lsa_stream(self):
+        """48-bit drand48 state the turbulent modes draw from next."""
+        x = C.c_ulonglong()
+        check(self.lib.fb_lsa_stream(self.ctx, C.byref(x), 0), "fb_lsa_stream", self.ctx, self.lib)
+        return x.value
+
+    def set_lsa_stream(self, x):
+        v = C.c_ulonglong(int(x))
+        check(self.lib.fb_lsa_stream(self.ctx, C.byref(v), 1), "fb_lsa_stream", self.ctx, self.lib)
 
     # -- launch shapes --------------------------------------------------
     def set_tuning(self, tuning):

@@ -58,6 +58,9 @@ class FbParams(C.Structure):
         ("sfta", _I), ("interpolation", _I), ("write_dust_density", _I),
         ("unsupported", C.c_ulonglong),
         ("planetconfig", C.c_char * 512), ("outputdir", C.c_char * 512),
+        ("mhd_lsa", _I), ("nbturbmodes", _I), ("high_m_cutoff", _I),
+        ("gammaturb", _D), ("lsamodespeedup", _D), ("turbrmin", _D), ("turbrmax", _D),
+        ("cavityradius", _D), ("cavityratio", _D), ("cavitywidth", _D),
     ]
 
 
@@ -138,7 +141,7 @@ EXPORTS = (
     "fb_closure_create", "fb_closure_destroy", "fb_closure_num_params", "fb_closure_params",
     "fb_closure_scales", "fb_closure_autoscale", "fb_closure_record", "fb_closure_set_sample",
     "fb_closure_loss_grad", "fb_closure_train", "fb_closure_infer", "fb_closure_apply", "fb_downsample",
-    "fb_closure_set_gain",
+    "fb_closure_set_gain", "fb_lsa_stream", "fb_rand48_state",
 )
 
 _lib = None   # the first library loaded (error details for contexts without a known library)
@@ -209,6 +212,8 @@ def load(mode=None):
         "fb_closure_apply": (_I, [vp, vp]),
         "fb_downsample": (_I, [vp, vp]),
         "fb_closure_set_gain": (_I, [vp, _D]),
+        "fb_lsa_stream": (_I, [vp, C.POINTER(C.c_ulonglong), _I]),
+        "fb_rand48_state": (C.c_ulonglong, [C.c_long, C.c_longlong]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -432,6 +432,24 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.kn_open = p->kn_open;
   k.non_reflecting = p->non_reflecting;
   k.sigmaslope = p->sigmaslope;
+  if (p->mhd_lsa && p->nbturbmodes > 0) {  // turbulent potential (src/turb.c)
+    k.lsa = 1;
+    k.lsa_nm = p->nbturbmodes;
+    k.lsa_highm = p->high_m_cutoff;
+    k.lsa_gamma = p->gammaturb;
+    k.lsa_speedup = p->lsamodespeedup;
+    k.lsa_rmin = p->turbrmin;
+    k.lsa_rmax = p->turbrmax;
+    k.cav_rmin = p->cavityradius - p->cavitywidth * p->aspectratio;  // turb.c:82-83
+    k.cav_rmax = p->cavityradius + p->cavitywidth * p->aspectratio;
+    k.cav_ratio = p->cavityratio;
+    k.lsa_st = (fb_lsa *)dalloc(ctx, (sizeof(fb_lsa) + sizeof(double) - 1) / sizeof(double));
+    k.lsa_cs = dalloc(ctx, (size_t)2 * k.lsa_nm * ns);
+    k.lsa_g = dalloc(ctx, (size_t)k.lsa_nm * nr);
+    if (!k.lsa_st || !k.lsa_cs || !k.lsa_g) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+    const unsigned long long x0 = fb_rand48_state(0, 0);  // every tf = 0: all modes drawn at the first substep
+    cudaMemcpy(&k.lsa_st->x, &x0, sizeof x0, cudaMemcpyHostToDevice);
+  }
   if (p->non_reflecting) {
     k.edge_buf = dalloc(ctx, (size_t)3 * ns);
     if (!k.edge_buf) { fb_destroy(ctx); return FB_ERR_NOMEM; }
@@ -655,7 +673,9 @@ static int enqueue_substep(fb_ctx *ctx)
   if (ctx->has_dust)
     STAGE(ST_DUST, fb_dust_launches(ctx->pp), fb_launch_dust_substep(k, ctx->pp, s, ctx->ev_planets));
   if (k.energy) STAGE(ST_SOUND, 1, fb_launch_soundspeed(k, k.visc_mode == 1, s));
+  if (k.lsa) STAGE(ST_POT, 2, fb_launch_lsa_modes(k, s));  // the turbulent modes at the substep's start
   STAGE(ST_POT, 1, fb_launch_potential(k, s));
+  if (k.lsa) STAGE(ST_POT, 1, fb_launch_lsa_add(k, s));
   STAGE(ST_SUB1, 1, fb_launch_substep1(k, s));
   if (k.self_gravity) {
     if (sg_branch) {
@@ -947,6 +967,25 @@ extern "C" int fb_download_derived(fb_ctx *ctx, int which, double *out)
   CK(cudaMemcpyAsync(out, tmp, ctx->nf * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
   CK(cudaFreeAsync(tmp, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
+  return FB_OK;
+}
+
+extern "C" int fb_lsa_stream(fb_ctx *ctx, unsigned long long *x, int set)
+{
+  if (!ctx || !x) return FB_ERR_INVALID;
+  if (!ctx->k.lsa) {
+    set_err(ctx, "fb_lsa_stream: the context has no turbulent potential (MHD L)");
+    return FB_ERR_STATE;
+  }
+  unsigned long long *dx = &ctx->k.lsa_st->x;
+  if (set) {
+    const unsigned long long v = *x & 0xFFFFFFFFFFFFull;
+    CK(cudaMemcpyAsync(dx, &v, sizeof v, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  } else {
+    CK(cudaMemcpyAsync(x, dx, sizeof *x, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+  }
   return FB_OK;
 }
 

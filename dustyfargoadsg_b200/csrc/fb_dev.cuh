@@ -44,6 +44,23 @@ struct fb_ctl {
   // planets as seen by FillForcesArrays in the current substep
   double pot_m[FB_MAX_PLANETS], pot_x[FB_MAX_PLANETS], pot_y[FB_MAX_PLANETS];
   double pot_smooth2[FB_MAX_PLANETS], pot_invd3[FB_MAX_PLANETS];
+  double t_sub;  // PhysicalTime at the start of the substep (FillForcesArrays' time)
+};
+
+// Turbulent potential (ApplyLSAOnPotential, src/turb.c:13-135): the modes'
+// parameters, the drand48 stream they are drawn from, and per substep each
+// mode's time factor sin(pi ttilde / deltat) and the cosine and sine of its
+// phase phic + (omegac - OmegaFrame) ttilde.  act[0 .. nact) lists the modes
+// that add to the potential (all of them unless HIGHMCUTOFF, then m <= 6),
+// in mode order.
+struct fb_lsa {
+  unsigned long long x;
+  int nact, status;
+  int m[FB_LSA_MAX_MODES], redraw[FB_LSA_MAX_MODES], act[FB_LSA_MAX_MODES];
+  double rc[FB_LSA_MAX_MODES], phic[FB_LSA_MAX_MODES], xi[FB_LSA_MAX_MODES];
+  double omegac[FB_LSA_MAX_MODES], sigma[FB_LSA_MAX_MODES], deltat[FB_LSA_MAX_MODES];
+  double t0[FB_LSA_MAX_MODES], tf[FB_LSA_MAX_MODES];
+  double s[FB_LSA_MAX_MODES], cp[FB_LSA_MAX_MODES], sp[FB_LSA_MAX_MODES];
 };
 
 // Everything a kernel needs, passed by value (well under the 32 KB limit).
@@ -128,6 +145,13 @@ struct KP {
   // DUSTFEEDBACK: the substep is also bounded by half the particles' minimum
   // stopping time (SourceEuler.c:1501-1507); NULL otherwise
   const double *dust_min_ts;
+  // turbulent potential (MHD L): modes, their azimuthal factors
+  // cos/sin(m Azimuth[j]) (2 x nm x ns, recomputed for redrawn modes) and
+  // radial envelopes mygamma/r xi exp(-(r-rc)^2/sigma^2) (nm x nr)
+  int lsa, lsa_nm, lsa_highm;
+  double lsa_gamma, lsa_speedup, lsa_rmin, lsa_rmax, cav_rmin, cav_rmax, cav_ratio;
+  fb_lsa *lsa_st;
+  double *lsa_cs, *lsa_g;
   // launch shapes (tuning): per-cell CTA width, cells per thread of the
   // azimuthal pass (0 = automatic), columns per CTA and rings per CTA of the
   // radial pass (0 = automatic), variant of the azimuthal pass (0 automatic,
@@ -284,6 +308,10 @@ void fb_launch_cfl(const KP &k, cudaStream_t s);
 void fb_launch_planets(const KP &k, const PP *pp, cudaStream_t s);
 void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s);
 void fb_launch_potential(const KP &k, cudaStream_t s);
+// turbulent potential: mode draws and tables after the controller, the
+// modes' sum added to the potential after k_potential (two and one launches)
+void fb_launch_lsa_modes(const KP &k, cudaStream_t s);
+void fb_launch_lsa_add(const KP &k, cudaStream_t s);
 void fb_launch_substep1(const KP &k, cudaStream_t s);
 void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s);
 void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s);

@@ -535,6 +535,7 @@ static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c)
   if (!k.indirect_term) { c->ind_x = 0.0; c->ind_y = 0.0; }
   // AdvanceSystemRK5 and RotatePsys follow in k_planets, which runs beside
   // the next kernels of the substep
+  c->t_sub = c->physical_time;  // what FillForcesArrays' turbulent potential sees
   c->physical_time += dt;  // SourceEuler.c:714 (no kernel in this substep reads it)
   c->substeps += 1;
   c->done = (c->dtemp < 0.999999999 * c->DT) ? 0 : 1;
@@ -1098,6 +1099,13 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
   // window: index 0 = ring k-1, 1 = ring k, 2 = ring k+1
   double W[NH][3], Qo[NH][3], R[3], VW[3];
   double DQ[NH][2], DR[2], QS[NH][2], RS[2], VR[2];
+  // flux through the inner face of the cell being updated: the outer-face
+  // flux of the cell below, carried from the previous iteration (the face
+  // radius Rsup[i-1] is Rinf[i], the same double), so each face's flux is
+  // evaluated once
+  double FI[NH];
+#pragma unroll
+  for (int q = 0; q < NH; q++) FI[q] = 0.0;
   // the inputs of one ring, loaded one iteration before they are used
   struct Raw { double r, u0, u1, u2, v; };
   auto fetch = [&](int kk) -> Raw {
@@ -1185,18 +1193,24 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
     }
     VR[1] = vrk;
     const int io = kk - 1;
+    // VanLeerRadial (TransportEuler.c:205-212): varq = dt dtheta Rinf[i]
+    // QStar RhoStar Vrad at face i minus the same at face i+1
+    const double b = dt * dtheta * k.rinf[kk];  // face kk = outer face of cell io
+    double FO[NH];
+#pragma unroll
+    for (int q = 0; q < NH; q++) FO[q] = b * QS[q][1] * RS[1] * VR[1];
     if (io >= i0 && io < i1) {
       const size_t l = (size_t)io * ns + j;
-      const double a = dt * dtheta * k.rinf[io];
-      const double b = dt * dtheta * k.rsup[io];
 #pragma unroll
       for (int q = 0; q < NH; q++) {
-        double varq = a * QS[q][0] * RS[0] * VR[0];
-        varq -= b * QS[q][1] * RS[1] * VR[1];
+        double varq = FI[q];
+        varq -= FO[q];
         k.q[LO + q][l] = Qo[q][0] + varq * k.invsurf[io];
         if (LO + q == NQ - 1 && io == 0) k.lost0[j] = varq;
       }
     }
+#pragma unroll
+    for (int q = 0; q < NH; q++) FI[q] = FO[q];
     // shift windows
 #pragma unroll
     for (int q = 0; q < NH; q++) {

@@ -30,6 +30,14 @@ double fb_drand48(fb_rand48 *s)
   return ldexp((double)s->x, -48);
 }
 
+unsigned long long fb_rand48_state(long seed, long long draws)
+{
+  fb_rand48 r;
+  fb_srand48(&r, seed);
+  for (long long n = 0; n < draws; n++) r.x = (0x5DEECE66Dull * r.x + 0xBull) & 0xFFFFFFFFFFFFull;
+  return r.x;
+}
+
 /* ---------------------------------------------------------------- defaults */
 int fb_params_default(fb_params *p)
 {
@@ -121,6 +129,17 @@ int fb_params_default(fb_params *p)
   p->interpolation = 2;
   strcpy(p->planetconfig, "Systems/SolarSystem.cfg");
   strcpy(p->outputdir, "~masset");
+  /* turbulent potential (src/var.c:70-72, 99-102, 133-134) */
+  p->mhd_lsa = 0;
+  p->nbturbmodes = 50;
+  p->high_m_cutoff = 0;
+  p->gammaturb = 0.00001;
+  p->lsamodespeedup = 0.1;
+  p->turbrmin = 0.0;
+  p->turbrmax = 0.0;
+  p->cavityradius = 0.0;
+  p->cavityratio = 1.0;
+  p->cavitywidth = 1.0;
   return FB_OK;
 }
 
@@ -329,7 +348,22 @@ int fb_params_read_par(fb_params *p, const char *path)
   if (is_c(kv_c(&set, "ADDMASS", 'N'), 'Y')) p->unsupported |= FB_U_ADDMASS;
   if (is_c(kv_c(&set, "DISCEVAPORATION", 'N'), 'Y')) p->unsupported |= FB_U_EVAPORATION;
   if (is_c(kv_c(&set, "PHOTOEVAPORATION", 'N'), 'Y')) p->unsupported |= FB_U_PHOTOEVAP;
-  if (is_c(kv_c(&set, "MHD", 'N'), 'L')) p->unsupported |= FB_U_MHDLSA;
+  /* MHD L: the turbulent potential (src/Interpret.c:404-410); it draws from
+     the drand48 stream the particles' kicks and initial draws share, so the
+     two together are refused */
+  p->nbturbmodes = kv_int(&set, "NBTURBMODES", p->nbturbmodes);
+  p->gammaturb = kv_num(&set, "GAMMATURB", p->gammaturb);
+  p->lsamodespeedup = kv_num(&set, "LSAMODESPEEDUP", p->lsamodespeedup);
+  p->turbrmin = kv_num(&set, "TURBRMIN", p->turbrmin);
+  p->turbrmax = kv_num(&set, "TURBRMAX", p->turbrmax);
+  p->cavityradius = kv_num(&set, "CAVITYRADIUS", p->cavityradius);
+  p->cavityratio = kv_num(&set, "CAVITYRATIO", p->cavityratio);
+  p->cavitywidth = kv_num(&set, "CAVITYWIDTH", p->cavitywidth);
+  if (is_c(kv_c(&set, "HIGHMCUTOFF", 'N'), 'Y')) p->high_m_cutoff = 1;
+  if (is_c(kv_c(&set, "MHD", 'N'), 'L')) {
+    p->mhd_lsa = 1;
+    if (p->nbturbmodes < 0 || p->nbturbmodes > FB_LSA_MAX_MODES || p->nbpart > 0) p->unsupported |= FB_U_MHDLSA;
+  }
   if (kv_num(&set, "CAVITYRADIUS", 0.0) != 0.0 || kv_num(&set, "CAVITYRATIO", 1.0) != 1.0)
     p->unsupported |= FB_U_CAVITY;
   if (kv_num(&set, "TRANSITIONRADIUS", 0.0) != 0.0 || kv_num(&set, "TRANSITIONRATIO", 1.0) != 1.0)

@@ -37,6 +37,7 @@ extern boolean DustFeelDisk, DustFeelPlanets, DustFeelTurb, DustFeelSG, DustFeel
 extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensity, ZZIntegrator;
 extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
 extern boolean CompareSGAndSummationTorques, KNOpen, SetConstantOpacity, StellarIrradiation, ImposedStellarLuminosity;
+extern boolean HighMCutoff;
 extern Pair DiskOnPrimaryAcceleration, DiskOnPrimaryAcceleration_alt;
 
 static fb_ctx *g_ctx = NULL;
@@ -125,7 +126,19 @@ static void params_from_globals(fb_params *p)
   if (PhotoEvaporation) p->unsupported |= FB_U_PHOTOEVAP;
   if (SelfGravity && SGZeroMode) p->unsupported |= FB_U_SGZEROMODE;
   if (ZMPlus) p->unsupported |= FB_U_ZMPLUS;
-  if (MHDLSA) p->unsupported |= FB_U_MHDLSA;
+  /* the turbulent potential (src/turb.c); it shares the drand48 stream
+     with the particles, so the two together are refused */
+  p->mhd_lsa = MHDLSA;
+  p->nbturbmodes = NBTURBMODES;
+  p->high_m_cutoff = HighMCutoff;
+  p->gammaturb = GAMMATURB;
+  p->lsamodespeedup = LSAMODESPEEDUP;
+  p->turbrmin = TURBRMIN;
+  p->turbrmax = TURBRMAX;
+  p->cavityradius = CAVITYRADIUS;
+  p->cavityratio = CAVITYRATIO;
+  p->cavitywidth = CAVITYWIDTH;
+  if (MHDLSA && (NBPART != 0 || NBTURBMODES < 0 || NBTURBMODES > FB_LSA_MAX_MODES)) p->unsupported |= FB_U_MHDLSA;
   if (EntropyDiffusion || RadiativeDiffusion) p->unsupported |= FB_U_THERMALDIFF;
   p->thermal_cooling = ThermalCooling;
   p->constant_opacity = SetConstantOpacity;
@@ -339,6 +352,12 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
     prof.global_soundspeed = GLOBAL_SoundSpeed;
     rc = fb_upload(g_ctx, &st, &prof);
     if (rc) dropin_fail("fb_upload", rc);
+    if (MHDLSA && NBTURBMODES > 0) {
+      /* the turbulent modes continue the drand48 stream where main.c left it */
+      unsigned long long x = rand48_get();
+      rc = fb_lsa_stream(g_ctx, &x, 1);
+      if (rc) dropin_fail("fb_lsa_stream", rc);
+    }
     if (NBPART != 0) {
       /* the particles as main.c left them, and the position of the drand48
          stream the turbulent kicks continue; the Gaussian generators have not
@@ -358,6 +377,12 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
      routine is about to read them (sync_host, called by the wrappers below) */
   rc = fb_download(g_ctx, &st, 0u);
   if (rc) dropin_fail("fb_download", rc);
+  if (MHDLSA && NBTURBMODES > 0) {  /* the stream as the modes' draws left it */
+    unsigned long long x = 0;
+    rc = fb_lsa_stream(g_ctx, &x, 0);
+    if (rc) dropin_fail("fb_lsa_stream", rc);
+    rand48_set(x);
+  }
   g_rho = Rho; g_vrad = Vrad; g_vtheta = Vtheta; g_energy = Energy; g_dsys = dsys;
   g_host_stale = 1;
   if (g_sync_always) sync_host();

@@ -130,7 +130,17 @@ typedef struct fb_params {
   /* PLANETCONFIG and OUTPUTDIR, as written in the .par file */
   char planetconfig[512];
   char outputdir[512];
+  /* stochastic turbulent potential of Laughlin et al. (2004) as modified by
+     Baruteau & Lin (2010) (src/turb.c:13-135, MHD L): NBTURBMODES modes
+     (at most FB_LSA_MAX_MODES), GAMMATURB, LSAMODESPEEDUP, TURBRMIN,
+     TURBRMAX, HIGHMCUTOFF (only modes m <= 6), and the cavity profile of
+     the forcing amplitude CAVITYRADIUS, CAVITYRATIO, CAVITYWIDTH */
+  int mhd_lsa, nbturbmodes, high_m_cutoff;
+  double gammaturb, lsamodespeedup, turbrmin, turbrmax;
+  double cavityradius, cavityratio, cavitywidth;
 } fb_params;
+
+#define FB_LSA_MAX_MODES 256
 
 /* Planetary system (src/types.h:96-108).  initial_mass/final_mass are the
    reference's InitialPlanetMass/FinalPlanetMass (src/global.h). */
@@ -265,6 +275,17 @@ int fb_download(fb_ctx *ctx, fb_state *st, unsigned mask);
    interpolation call, src/main.c:287), download when writing outputs. */
 int fb_dust_upload(fb_ctx *ctx, const fb_dust_state *st);
 int fb_dust_download(fb_ctx *ctx, fb_dust_state *st);
+/* Turbulent potential (MHD L, ApplyLSAOnPotential, src/turb.c:13-135): the
+   modes are drawn on the device from the POSIX drand48 stream, the
+   reference's global one (seeded at src/Interpret.c:404-407, then used by
+   whatever draws before the time loop).  The stream's 48-bit state is read
+   (set = 0) or written (set = 1) here; a context starts with srand48(0)'s.
+   fb_rand48_state gives srand48(seed)'s state advanced by `draws` draws
+   (with noise, fb_init_state draws nrad*nsec numbers after seeding).
+   Every mode is redrawn at the first substep after fb_create, as the
+   reference's zeroed mode lifetimes make it do at the start of a run. */
+int fb_lsa_stream(fb_ctx *ctx, unsigned long long *x, int set);
+unsigned long long fb_rand48_state(long seed, long long draws);
 /* The state at the first crash (see fb_step_report), nrad*nsec doubles per
    non-NULL field of st (density, vrad, vtheta, energy; ring nrad untouched):
    what the reference writes as gasdens999.dat, gasvrad999.dat,

@@ -140,3 +140,33 @@ def test_inner_boundary_switches():
             p = read_par(_oracle.write_par(src, wd, InnerBoundary=val))
             assert (p.wall_boundary, p.open_inner, p.kn_open, p.non_reflecting) == flags, val
             assert p.unsupported == 0, val
+
+
+def test_turbulent_potential_parameters(tmp_path):
+    """MHD L reads the turbulent potential's keys (src/var.c:99-102, 133-134)
+    and is refused together with particles, whose kicks share the reference's
+    drand48 stream with the modes."""
+    from dustyfargoadsg_b200 import read_par
+    lsa = dict(MHD="L", NbTurbModes="40", GammaTurb="2e-3", TurbRmin="0.6", TurbRmax="2.0", HighMCutoff="Yes")
+    p = read_par(_oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "iso_128x384.par"), str(tmp_path), **lsa))
+    assert p.unsupported == 0 and p.mhd_lsa == 1 and p.nbturbmodes == 40 and p.high_m_cutoff == 1
+    assert p.gammaturb == 2e-3 and p.turbrmin == 0.6 and p.turbrmax == 2.0 and p.lsamodespeedup == 0.1
+    os.makedirs(str(tmp_path / "d"))
+    d = read_par(_oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "dust_256x768.par"), str(tmp_path / "d"),
+                                   NbPart=100, **lsa))
+    assert d.unsupported != 0
+    os.makedirs(str(tmp_path / "m"))
+    m = read_par(_oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "iso_128x384.par"), str(tmp_path / "m"),
+                                   **dict(lsa, NbTurbModes="1000")))
+    assert m.unsupported != 0
+
+
+def test_rand48_state_helper():
+    """fb_rand48_state is srand48(seed) advanced by `draws` drand48 calls."""
+    from dustyfargoadsg_b200 import load
+    lib = load()
+    x = (7 << 16) | 0x330E
+    for _ in range(1000):
+        x = (0x5DEECE66D * x + 0xB) & ((1 << 48) - 1)
+    assert lib.fb_rand48_state(7, 1000) == x
+    assert lib.fb_rand48_state(0, 0) == 0x330E

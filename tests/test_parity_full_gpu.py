@@ -128,3 +128,31 @@ def test_alternative_indirect_term(tmp_path):
                     # sums over the disc's cells that cancel to ~1e-8: the
                     # summation order shows at ~1e-18
                     assert abs(a - b) <= 1e-12 * abs(b) + 1e-17, (name, q, a, b)
+
+
+def test_density_floor_lifts_cells(tmp_path):
+    """AddFloorDensity (SourceEuler.c:2506-2521) with DensityFloor 5e-4 above
+    the outer disc's density (6.3e-4 r^-0.5 falls below it beyond r = 1.6):
+    the floor lifts every such cell after the transport of each substep;
+    fields within 1e-11 after each of 3 DTs, and the floor must have acted."""
+    from dustyfargoadsg_b200 import Disc, read_par
+    par = _oracle.write_par(os.path.join(CFG, "iso_128x384.par"), str(tmp_path), Nrad=64, Nsec=192,
+                            DensityFloor="5e-4")
+    p = read_par(par)
+    assert p.densityfloor == 5e-4 and p.unsupported == 0
+    steps = 3
+    dumps, _, _ = _oracle.run_oracle(par, steps=steps, noise=1e-3, seed=9)
+    with Disc(p, noise=1e-3, seed=9) as disc:
+        below = int(np.sum(disc.fields["dens"][: p.nrad * p.nsec] < 5e-4))
+        prev = 0
+        for s in range(1, steps + 1):
+            rep = disc.step()
+            ref = dumps["state_%05d" % s]
+            out = disc.download()
+            prev = _check_dt(rep, out, ref, prev, ("dens", "vrad", "vtheta"))
+        dens = out["dens"][2 * p.nsec: (p.nrad - 2) * p.nsec]  # the walls reset two rings per edge
+    assert below > 1000, below
+    # the damping zone relaxes floored cells toward ring means (a rounding
+    # below the floor is possible there); between it and the disc, cells sit
+    # exactly on the floor
+    assert np.min(dens) >= 5e-4 * (1 - 1e-12) and np.sum(dens == 5e-4) > 100, (np.min(dens), np.sum(dens == 5e-4))
