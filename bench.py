@@ -368,23 +368,32 @@ def main():
     peak, peak_kind = measured_peak()
     best = None
     stages = {}
+    # one radial pass per substep: the substeps of the profiled DTs (a stage
+    # may launch several kernels per substep, so its time per pass is its
+    # total over the substeps, not over its launches)
+    nsub = prof.get("transport_radial", (0.0, 0))[1]
     for name, (ms, cnt) in prof.items():
         if cnt <= 0 or ms <= 0:
             continue
         per_launch_ms = ms / cnt
         stages[name] = {"ms_per_launch": per_launch_ms, "launches": cnt}
+        if nsub > 0:
+            stages[name]["ms_per_substep"] = ms / nsub
         if best is None or ms > prof[best][0]:
             best = name
     roofline = None
     if best is not None:
         bpc = STAGE_BYTES.get(best, (None, None))[energy]
         ms, cnt = prof[best]
+        if nsub > 0:
+            cnt = nsub  # the time of one pass of the stage
         units = cells
         if best == "dust_particles":
             # per particle and substep: read r, th, vr, vth, size, St, flag and
             # write r, th, vr, vth, St (96 B); the grid gathers are L2 hits
             bpc, units = 96, disc.npart
-            cnt = cnt / (8 if p.dust_feel_turb else 2)  # launches per substep
+            if nsub <= 0:
+                cnt = cnt / (8 if p.dust_feel_turb else 2)  # launches per substep
         achieved = (bpc * units / (ms / cnt * 1e-3) / 1e9) if bpc else None
         roofline = {"bound": "hbm", "kernel": best, "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": (achieved / peak) if achieved else None,

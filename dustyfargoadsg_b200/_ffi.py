@@ -61,6 +61,7 @@ class FbParams(C.Structure):
         ("mhd_lsa", _I), ("nbturbmodes", _I), ("high_m_cutoff", _I),
         ("gammaturb", _D), ("lsamodespeedup", _D), ("turbrmin", _D), ("turbrmax", _D),
         ("cavityradius", _D), ("cavityratio", _D), ("cavitywidth", _D),
+        ("entropy_diffusion", _I), ("radiative_diffusion", _I), ("diffusivity", _D),
     ]
 
 

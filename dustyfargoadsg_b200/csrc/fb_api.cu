@@ -9,13 +9,14 @@
 #include <vector>
 #include "fb_dev.cuh"
 
+#define FB_PROFILE_POINTS 64
 enum {
-  ST_CFL, ST_FORCE, ST_CONTROL, ST_SOUND, ST_POT, ST_SUB1, ST_SG, ST_SGCOLS, ST_SGINV, ST_SGUPD,
+  ST_CFL, ST_SUB0, ST_CONTROL, ST_SOUND, ST_POT, ST_SUB1, ST_SG, ST_SGCOLS, ST_SGINV, ST_SGUPD,
   ST_VTERMS, ST_VUPDATE,
   ST_SUB2, ST_EVTERMS, ST_SUB3, ST_TRAD, ST_TAZI, ST_TVR, ST_DAMP, ST_DUST, FB_NSTAGE
 };
 static const char *stage_names[FB_NSTAGE] = {
-  "cfl_forces", "unused", "controller", "soundspeed", "potential", "substep1", "sg_rows_fwd",
+  "cfl_forces", "substep0", "controller", "soundspeed", "potential", "substep1", "sg_rows_fwd",
   "sg_cols", "sg_rows_inv", "sg_update",
   "viscous_terms", "viscous_update", "substep2", "energy_viscous_terms", "substep3",
   "transport_radial", "transport_azimuthal", "transport_vr_boundary", "damping", "dust_particles"};
@@ -31,6 +32,7 @@ struct fb_ctx {
   cudaEvent_t ev_fork, ev_planets;    // its start and end within a substep
   cudaStream_t st_sg;                 // branch of the self-gravity convolution
   cudaEvent_t ev_sg_fork, ev_sg_done;
+  cudaEvent_t ev_vm_fork, ev_vm_done;  // the tile variant's ring means, on the SG stream beside SubStep3 / radial
   KP k;
   std::vector<void *> allocs;
   fb_ctl *d_ctl;
@@ -272,7 +274,9 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
       cudaEventCreateWithFlags(&ctx->ev_planets, cudaEventDisableTiming) != cudaSuccess ||
       cudaStreamCreateWithFlags(&ctx->st_sg, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&ctx->ev_sg_fork, cudaEventDisableTiming) != cudaSuccess ||
-      cudaEventCreateWithFlags(&ctx->ev_sg_done, cudaEventDisableTiming) != cudaSuccess) {
+      cudaEventCreateWithFlags(&ctx->ev_sg_done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_vm_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&ctx->ev_vm_done, cudaEventDisableTiming) != cudaSuccess) {
     fb_destroy(ctx);
     return FB_ERR_CUDA;
   }
@@ -410,10 +414,41 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.fast_transport = p->fast_transport;
   k.wall = p->wall_boundary;
   k.thermal_cooling = p->energy_equation && p->thermal_cooling;
+  if (p->energy_equation && (p->entropy_diffusion || p->radiative_diffusion)) {
+    // thermal diffusion (SubStep0): its scratch fields, and for radiative
+    // diffusion the opacity of every substep with ComputeOpacities' constants
+    k.ent_diff = p->entropy_diffusion;
+    k.rad_diff = p->radiative_diffusion;
+    k.diffusivity = p->diffusivity;
+    double **tf[] = {&k.td_s, &k.td_t, &k.td_k, &k.td_ent, &k.td_rad};
+    for (double **f : tf)
+      if (!(*f = dalloc(ctx, nf))) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+    if (k.rad_diff) {
+      const double um = fb_unit_mass(p), ul = fb_unit_length(p);
+      k.sigma_sb = 5.6704e-8 * pow(um, -1) * pow(fb_unit_time(p), 3.) * pow(fb_unit_temperature(p), 4.);
+      k.op_constant = p->constant_opacity;
+      k.op_imposed = p->imposedconstantopacity;
+      k.op_factor = p->factoropacities;
+      k.op_utemp = fb_unit_temperature(p);
+      k.op_umass = um;
+      k.op_invl3 = pow(ul, -3.);
+      k.op_conv = 0.1 * pow(ul, -2.0) * pow(um, 1.0);
+      if (!k.opacity && !(k.opacity = dalloc(ctx, nf))) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+    }
+    if (k.rad_diff == 2) {
+      k.sor_grid = fb_sor_grid();
+      if (k.sor_grid < 1) { set_err(ctx, "no resident CTA for the radiative diffusion solver"); fb_destroy(ctx); return FB_ERR_CUDA; }
+      for (int q = 0; q < 6; q++)
+        if (!(k.sor_c[q] = dalloc(ctx, nf))) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+      k.sor_part = dalloc(ctx, (size_t)3 * k.sor_grid);
+      k.sor_bar = (unsigned int *)dalloc(ctx, 1);
+      if (!k.sor_part || !k.sor_bar) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+    }
+  }
   if (k.thermal_cooling) {
     // sigma_SB in code units (LowTasks.c:215)
     k.sigma_sb = 5.6704e-8 * pow(fb_unit_mass(p), -1) * pow(fb_unit_time(p), 3.) * pow(fb_unit_temperature(p), 4.);
-    k.opacity = dalloc(ctx, nf);
+    if (!k.opacity) k.opacity = dalloc(ctx, nf);
     if (!k.opacity) { fb_destroy(ctx); return FB_ERR_NOMEM; }
     k.irradiation = p->stellar_irradiation;
     if (k.irradiation) {  // per ring, as SubStep3 evaluates them (SourceEuler.c:1204-1268)
@@ -527,6 +562,8 @@ extern "C" int fb_destroy(fb_ctx *ctx)
   if (ctx->st_planets) cudaStreamDestroy(ctx->st_planets);
   if (ctx->ev_sg_fork) cudaEventDestroy(ctx->ev_sg_fork);
   if (ctx->ev_sg_done) cudaEventDestroy(ctx->ev_sg_done);
+  if (ctx->ev_vm_fork) cudaEventDestroy(ctx->ev_vm_fork);
+  if (ctx->ev_vm_done) cudaEventDestroy(ctx->ev_vm_done);
   if (ctx->st_sg) cudaStreamDestroy(ctx->st_sg);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->gdt_exec) cudaGraphExecDestroy(ctx->gdt_exec);
@@ -573,7 +610,7 @@ extern "C" int fb_upload(fb_ctx *ctx, const fb_state *s, const fb_profiles *prof
   } else {
     fb_launch_soundspeed(k, 0, ctx->st);
   }
-  if (k.thermal_cooling) {
+  if (k.thermal_cooling || k.rad_diff) {
     // the opacity of the uploaded state, which the step keeps, as the
     // reference computes it once in InitEuler (SourceEuler.c:275)
     const fb_params *pp = &ctx->p;
@@ -589,6 +626,10 @@ extern "C" int fb_upload(fb_ctx *ctx, const fb_state *s, const fb_profiles *prof
   c->physical_time_initial = s->physical_time_initial;
   c->omega_frame = s->omega_frame;
   c->lost_mass = s->lost_mass;
+  if (!ctx->uploaded) {  // the implicit solver's statics (SourceEuler.c:43, 47)
+    c->sor_omega = FB_SOR_OMEGA0;
+    c->sor_niterbuf = FB_SOR_MAXITS;
+  }
   c->mindt = s->mindt;
   c->maxdt = s->maxdt;
   for (int q = 0; q < 3; q++) {
@@ -626,7 +667,7 @@ extern "C" int fb_upload(fb_ctx *ctx, const fb_state *s, const fb_profiles *prof
 // stage when profiling and counts the kernel launches it issues.
 #define STAGE(id, nlaunch, call)                                 \
   do {                                                           \
-    if (ctx->profiling) {                                        \
+    if (ctx->profiling && npt < FB_PROFILE_POINTS - 1) {         \
       cudaEventRecord(ctx->pev[npt], s);                         \
       ctx->pseq[npt] = (id);                                     \
       npt++;                                                     \
@@ -658,6 +699,13 @@ static int enqueue_substep(fb_ctx *ctx)
     ctx->pcount[ST_SGCOLS] += 1;
     ctx->pcount[ST_SGINV] += 1;
   }
+  // explicit radiative diffusion: the opacity of the substep's starting
+  // state, which ConditionCFL and ComputeRadiativeDiffusion both compute
+  // (SourceEuler.c:1326, 1809) and SubStep3's cooling then uses
+  if (k.energy && k.rad_diff == 1) {
+    STAGE(ST_CFL, 1, fb_launch_opacity_now(k, s));
+    STAGE(ST_CFL, 1, fb_launch_td_cfl(k, s));
+  }
   STAGE(ST_CFL, 1, fb_launch_cfl(k, s));  // ConditionCFL + the controller (last CTA)
   // the planets' step on a branch of its own: no gas kernel of the substep
   // reads the positions it writes; joined before the particles' velocity
@@ -672,6 +720,11 @@ static int enqueue_substep(fb_ctx *ctx)
   // (SourceEuler.c:504-531)
   if (ctx->has_dust)
     STAGE(ST_DUST, fb_dust_launches(ctx->pp), fb_launch_dust_substep(k, ctx->pp, s, ctx->ev_planets));
+  // SubStep0: thermal diffusion, before the sound speed (SourceEuler.c:577-586)
+  if (k.energy && (k.ent_diff || k.rad_diff)) {
+    int n0 = 0;  // the stage's kernel launches
+    STAGE(ST_SUB0, n0, n0 = fb_launch_substep0(k, s));
+  }
   if (k.energy) STAGE(ST_SOUND, 1, fb_launch_soundspeed(k, k.visc_mode == 1, s));
   if (k.lsa) STAGE(ST_POT, 2, fb_launch_lsa_modes(k, s));  // the turbulent modes at the substep's start
   STAGE(ST_POT, 1, fb_launch_potential(k, s));
@@ -692,10 +745,26 @@ static int enqueue_substep(fb_ctx *ctx)
     STAGE(ST_VUPDATE, 1, fb_launch_viscous_update(k, k.vri, k.vti, 0.0, s));
   }
   STAGE(ST_SUB2, 1, fb_launch_substep2(k, s));
+  // the tile variant's ring means of vtheta, which SubStep2 has just
+  // written for the last time before the transport: on a branch beside
+  // SubStep3 and the radial pass (in line when profiling stage by stage)
+  const bool vm_branch = !ctx->profiling && fb_azi_launches(k) == 2;
+  if (vm_branch) {
+    cudaEventRecord(ctx->ev_vm_fork, s);
+    cudaStreamWaitEvent(ctx->st_sg, ctx->ev_vm_fork, 0);
+    fb_launch_azi_vmed(k, 0.0, ctx->st_sg);
+    cudaEventRecord(ctx->ev_vm_done, ctx->st_sg);
+    ctx->launches += 1;
+    ctx->pcount[ST_TAZI] += 1;
+  }
   if (k.energy) STAGE(ST_SUB3, 1, fb_launch_substep3(k, s));  // with the stresses of the new velocities
   STAGE(ST_TRAD, 1, fb_launch_transport_radial(k, 0.0, s));
-  STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s));
-  ctx->launches += fb_azi_launches(k) - 1;  // the tile variant's ring means: one pass, two kernels
+  if (vm_branch) {
+    cudaStreamWaitEvent(s, ctx->ev_vm_done, 0);
+    STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s, true));
+  } else {
+    STAGE(ST_TAZI, fb_azi_launches(k), fb_launch_transport_azimuthal(k, 0.0, s));  // ring means + tiles
+  }
   STAGE(ST_TVR, 1, fb_launch_transport_vr(k, s));
   if (k.open_inner || k.non_reflecting) {
     // ApplyBoundaryCondition's other edges (SideEuler.c:1102-1131); the
@@ -815,8 +884,8 @@ extern "C" int fb_profile(fb_ctx *ctx, int enable)
 {
   if (!ctx) return FB_ERR_INVALID;
   if (enable && ctx->pev.empty()) {
-    ctx->pev.resize(FB_NSTAGE + 2);
-    ctx->pseq.resize(FB_NSTAGE + 2);
+    ctx->pev.resize(FB_PROFILE_POINTS);  // the recorded points of one substep, with room to spare
+    ctx->pseq.resize(FB_PROFILE_POINTS);
     for (auto &e : ctx->pev) CK(cudaEventCreate(&e));
   }
   ctx->profiling = enable ? 1 : 0;

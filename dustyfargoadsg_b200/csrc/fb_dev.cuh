@@ -45,7 +45,15 @@ struct fb_ctl {
   double pot_m[FB_MAX_PLANETS], pot_x[FB_MAX_PLANETS], pot_y[FB_MAX_PLANETS];
   double pot_smooth2[FB_MAX_PLANETS], pot_invd3[FB_MAX_PLANETS];
   double t_sub;  // PhysicalTime at the start of the substep (FillForcesArrays' time)
+  // implicit radiative diffusion (SubStep0, SourceEuler.c:749-760): the
+  // relaxation parameter omegaSOR and the previous solve's iteration count
+  // niterbuf, both carried from solve to solve; sor_iters = the last solve's
+  double sor_omega;
+  int sor_niterbuf, sor_iters;
 };
+#define FB_SOR_MAXITS 100000  // MAXITS of SourceEuler.c:20
+#define FB_SOR_OMEGA0 1.97    // omegaSOR's initial value (SourceEuler.c:47)
+#define FB_SOR_EPS 1e-4       // epsilonSOR (SourceEuler.c:48)
 
 // Turbulent potential (ApplyLSAOnPotential, src/turb.c:13-135): the modes'
 // parameters, the drand48 stream they are drawn from, and per substep each
@@ -152,6 +160,21 @@ struct KP {
   double lsa_gamma, lsa_speedup, lsa_rmin, lsa_rmax, cav_rmin, cav_rmax, cav_ratio;
   fb_lsa *lsa_st;
   double *lsa_cs, *lsa_g;
+  // thermal diffusion (energy equation): entropy diffusion (DIFFUSIVITY),
+  // radiative diffusion 1 explicit / 2 implicit; per-cell scratch: the
+  // entropy logarithm, the temperature (TempInt, updated in place by the
+  // solver), the diffusion coefficient K or chi, the two explicit source
+  // fields, the solver's coefficients a..f (6 fields), per-CTA residual
+  // partial sums and the solver's grid barrier {count, generation}
+  int ent_diff, rad_diff;
+  double diffusivity;
+  double *td_s, *td_t, *td_k, *td_ent, *td_rad, *sor_c[6], *sor_part;
+  unsigned int *sor_bar;
+  int sor_grid;
+  // ComputeOpacities' constants (SourceEuler.c:1608-1701), for the opacity
+  // of the current state at every substep when radiative diffusion is on
+  int op_constant;
+  double op_imposed, op_factor, op_utemp, op_umass, op_invl3, op_conv;
   // launch shapes (tuning): per-cell CTA width, cells per thread of the
   // azimuthal pass (0 = automatic), columns per CTA and rings per CTA of the
   // radial pass (0 = automatic), variant of the azimuthal pass (0 automatic,
@@ -312,6 +335,13 @@ void fb_launch_potential(const KP &k, cudaStream_t s);
 // modes' sum added to the potential after k_potential (two and one launches)
 void fb_launch_lsa_modes(const KP &k, cudaStream_t s);
 void fb_launch_lsa_add(const KP &k, cudaStream_t s);
+// thermal diffusion: the opacity of the current state (before the CFL
+// kernel with explicit radiative diffusion) and SubStep0 after the
+// controller; each returns its kernel launches
+int fb_launch_opacity_now(const KP &k, cudaStream_t s);
+int fb_launch_substep0(const KP &k, cudaStream_t s);
+int fb_launch_td_cfl(const KP &k, cudaStream_t s);  // explicit radiative diffusion's CFL limits
+int fb_sor_grid(void);  // CTAs of the solver kernel the GPU holds at once
 void fb_launch_substep1(const KP &k, cudaStream_t s);
 void fb_launch_viscous_terms(const KP &k, const double *vr, const double *vt, cudaStream_t s);
 void fb_launch_viscous_update(const KP &k, double *vr, double *vt, double dt_override, cudaStream_t s);
@@ -319,7 +349,9 @@ void fb_launch_substep2(const KP &k, cudaStream_t s);
 void fb_launch_substep3(const KP &k, cudaStream_t s);
 void fb_launch_transport(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_transport_radial(const KP &k, double dt_override, cudaStream_t s);
-void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s);
+// vmed_done: the tile variant's ring means are already taken (fb_launch_azi_vmed)
+void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s, bool vmed_done = false);
+int  fb_launch_azi_vmed(const KP &k, double dt_override, cudaStream_t s);
 void fb_launch_transport_vr(const KP &k, cudaStream_t s);
 void fb_launch_edges(const KP &k, cudaStream_t s);  // open / non-reflecting edges
 // ComputeOpacities (SourceEuler.c:1608-1701) of the current state:

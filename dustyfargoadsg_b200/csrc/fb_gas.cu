@@ -211,11 +211,16 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
   if (cfl) {
     const double viscosity = nu_ring(k, i);
     const double invdt5 = (viscosity != 0.0) ? viscosity * 4.0 / k.mindx2[i] : 1e-10;
-    const double invdt6 = 1e-10;
+    // thermal diffusion's limit (SourceEuler.c:1411-1428): entropy
+    // diffusion's per ring; explicit radiative diffusion's per cell (below),
+    // which replaces it when both are on
+    const double invdt6_ring = (k.energy && k.ent_diff) ? k.diffusivity * 4.0 / k.mindx2[i] : 1e-10;
     double m = 1e30;
     for (int j = tid; j < ns; j += T) {  // each thread reads back its own cells
       double vres = k.fast_transport ? vtc[j] - vmoy : vtc[j];
       double invdt3 = fb_quot(fabs(vres), dxtheta, rdxtheta);
+      double invdt6 = invdt6_ring;
+      if (k.energy && k.rad_diff == 1) invdt6 = k.td_rad[base + j];  // k_td_cfl, just before this kernel
       double dt = FB_CFLSECURITY / sqrt(s12[j] + invdt3 * invdt3 + s4[j] + invdt5 * invdt5 + invdt6 * invdt6);
       if (dt < m) m = dt;
     }
@@ -1075,6 +1080,17 @@ void fb_launch_opacity(const KP &k, int constant, double imposed, double factor,
             inv_l3, conv);
 }
 
+// ComputeOpacities of the current state with the constants held in KP:
+// radiative diffusion recomputes the opacity at every substep (in
+// ConditionCFL and ComputeRadiativeDiffusion, or in the implicit solver),
+// and SubStep3's cooling then uses that one (SourceEuler.c:1326, 1809, 1901)
+int fb_launch_opacity_now(const KP &k, cudaStream_t s)
+{
+  fb_launch(k_opacity, grid2d(k, k.nr), k.cell_bs, 0, s, k, k.op_constant, k.op_imposed, k.op_factor, k.op_utemp,
+            k.op_umass, k.op_invl3, k.op_conv);
+  return 1;
+}
+
 void fb_launch_substep3(const KP &k, cudaStream_t s) { fb_launch(k_substep3, grid2d(k, k.nr + 1), k.cell_bs, 0, s, k); }
 
 // ------------------------------------------------------------ Transport
@@ -1106,10 +1122,20 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
   double FI[NH];
 #pragma unroll
   for (int q = 0; q < NH; q++) FI[q] = 0.0;
-  // the inputs of one ring, loaded one iteration before they are used
-  struct Raw { double r, u0, u1, u2, v; };
+  // the inputs of one ring, loaded one iteration before they are used,
+  // with the ring's table entries: Rmed, InvDiffRmed, Rinf and the
+  // InvSurf of the cell below (the one whose update reads this ring's face)
+  struct Raw { double r, u0, u1, u2, v, tm, ti, tr, ts; };
+  // table windows (slot 1 = ring kk, slot 2 = ring kk+1, TM slot 0 = kk-1)
+  double TM[3], TI[3], TR[3], TS[3];
   auto fetch = [&](int kk) -> Raw {
-    Raw w = {0.0, 0.0, 0.0, 0.0, 0.0};
+    Raw w = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (kk >= 0 && kk <= nr) {
+      w.tm = k.rmed[kk];
+      w.ti = k.invdiffrmed[kk];
+      w.tr = k.rinf[kk];
+      if (kk >= 1) w.ts = k.invsurf[kk - 1];
+    }
     if (kk >= 0 && kk <= nr - 1) {
       const size_t l = (size_t)kk * ns + j;
       w.r = k.rho[l];
@@ -1128,6 +1154,10 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
   };
   auto put = [&](const Raw &w, int kk, int slot) {
     VW[slot] = w.v;
+    TM[slot] = w.tm;
+    TI[slot] = w.ti;
+    TR[slot] = w.tr;
+    TS[slot] = w.ts;
     if (kk < 0 || kk > nr - 1) {
 #pragma unroll
       for (int q = 0; q < NH; q++) { W[q][slot] = 0.0; Qo[q][slot] = 0.0; }
@@ -1135,7 +1165,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
       return;
     }
     const double r = w.r;
-    const double Rm = k.rmed[kk];
+    const double Rm = w.tm;
     double qv[NH];
     if (H == 0) {
       qv[0] = r * w.u0;                    // rp = rho*vr[lip]
@@ -1153,8 +1183,8 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
   };
   auto slope = [&](double am, double a0, double ap, int kk) -> double {
     if (kk <= 0 || kk >= nr - 1) return 0.0;
-    double dqm = (a0 - am) * k.invdiffrmed[kk];
-    double dqp = (ap - a0) * k.invdiffrmed[kk + 1];
+    double dqm = (a0 - am) * TI[1];  // InvDiffRmed[kk]
+    double dqp = (ap - a0) * TI[2];  // InvDiffRmed[kk + 1]
     if (dqp * dqm > 0.0) return fb_vl_quot(2.0 * dqp * dqm, dqp + dqm);
     return 0.0;
   };
@@ -1170,8 +1200,8 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
     nxt = fetch(kk + 2);
     put(cur, kk + 1, 2);
     const double vrk = VW[1];  // vr of ring kk
-    const double rmk = k.rmed[kk];
-    const double rmkm = (kk >= 1) ? k.rmed[kk - 1] : 0.0;
+    const double rmk = TM[1];
+    const double rmkm = TM[0];  // 0 below ring 0
 #pragma unroll
     for (int q = 0; q < NH; q++) DQ[q][1] = slope(W[q][0], W[q][1], W[q][2], kk);
     DR[1] = slope(R[0], R[1], R[2], kk);
@@ -1185,7 +1215,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
       for (int q = 0; q < NH; q++) QS[q][1] = W[q][0] + (rmk - rmkm - vrk * dt) * 0.5 * DQ[q][0];
       RS[1] = R[0] + f * DR[0];
     } else {
-      const double rmkp = k.rmed[kk + 1];
+      const double rmkp = TM[2];
       const double f = (rmkp - rmk + vrk * dt) * 0.5;
 #pragma unroll
       for (int q = 0; q < NH; q++) QS[q][1] = W[q][1] - (rmkp - rmk + vrk * dt) * 0.5 * DQ[q][1];
@@ -1195,7 +1225,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
     const int io = kk - 1;
     // VanLeerRadial (TransportEuler.c:205-212): varq = dt dtheta Rinf[i]
     // QStar RhoStar Vrad at face i minus the same at face i+1
-    const double b = dt * dtheta * k.rinf[kk];  // face kk = outer face of cell io
+    const double b = dt * dtheta * TR[1];  // Rinf[kk]: face kk = outer face of cell io
     double FO[NH];
 #pragma unroll
     for (int q = 0; q < NH; q++) FO[q] = b * QS[q][1] * RS[1] * VR[1];
@@ -1205,7 +1235,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
       for (int q = 0; q < NH; q++) {
         double varq = FI[q];
         varq -= FO[q];
-        k.q[LO + q][l] = Qo[q][0] + varq * k.invsurf[io];
+        k.q[LO + q][l] = Qo[q][0] + varq * TS[1];  // InvSurf[io]
         if (LO + q == NQ - 1 && io == 0) k.lost0[j] = varq;
       }
     }
@@ -1221,6 +1251,10 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
     }
     R[0] = R[1]; R[1] = R[2];
     VW[0] = VW[1]; VW[1] = VW[2];
+    TM[0] = TM[1]; TM[1] = TM[2];
+    TI[1] = TI[2];
+    TR[1] = TR[2];
+    TS[1] = TS[2];
     DR[0] = DR[1];
     RS[0] = RS[1];
     VR[0] = VR[1];
@@ -1229,7 +1263,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
 
 // CTAs of 2 tx threads: columns blockIdx.x tx .. + tx, rings of one chunk
 template <int NQ>
-__global__ void __launch_bounds__(256) k_transport_radial(KP k, double dtov, int chunk)
+__global__ void __launch_bounds__(256, 2) k_transport_radial(KP k, double dtov, int chunk)
 {
   fb_grid_dependency();
   const double dt = dt_of(k, dtov);
@@ -2539,8 +2573,19 @@ void fb_launch_transport_radial(const KP &k0, double dt_override, cudaStream_t s
     fb_launch(k_transport_radial<5>, gr, 2 * tx, 0, s, k, dt_override, chunk);
 }
 
+// The tile variant's ring means of vtheta (k_azi_vmed): nothing between
+// SubStep2 and the azimuthal pass changes vtheta, so the step may run them
+// on a branch beside SubStep3 and the radial pass.  Returns the launches.
+int fb_launch_azi_vmed(const KP &k, double dt_override, cudaStream_t s)
+{
+  int E = 1;
+  if (!azt_variant(azi_resolve(k, &E))) return 0;
+  fb_launch(k_azi_vmed, k.nr, azi_threads_for(k.ns, E), 0, s, k, dt_override);
+  return 1;
+}
+
 template <int NQ>
-static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
+static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s, bool vmed_done)
 {
   int E = 1;
   const int var = azi_resolve(k, &E);
@@ -2548,7 +2593,7 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
   const int th = azi_threads_for(k.ns, E);
   const bool full = (th * E == k.ns);  // every thread owns E cells
   if (var == 6 || var == 7) {
-    fb_launch(k_azi_vmed, k.nr, th, 0, s, k, dt_override);
+    if (!vmed_done) fb_launch(k_azi_vmed, k.nr, th, 0, s, k, dt_override);
     const int CO = AZT_CO(E), ntiles = (k.ns + CO - 1) / CO;
     const int grid = (int)(((long)k.nr * ntiles + AZT_WPC - 1) / AZT_WPC);
 #define AZT_LAUNCH(EE, MB) fb_launch(k_transport_azimuthal_tile<NQ, EE, MB>, grid, AZT_WPC * 32, 0, s, k, dt_override)
@@ -2633,12 +2678,12 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s)
 #undef AZI_LAUNCH
 }
 
-void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s)
+void fb_launch_transport_azimuthal(const KP &k, double dt_override, cudaStream_t s, bool vmed_done)
 {
   if (k.energy)
-    launch_azimuthal<6>(k, dt_override, s);
+    launch_azimuthal<6>(k, dt_override, s, vmed_done);
   else
-    launch_azimuthal<5>(k, dt_override, s);
+    launch_azimuthal<5>(k, dt_override, s, vmed_done);
 }
 
 void fb_launch_transport_vr(const KP &k, cudaStream_t s)

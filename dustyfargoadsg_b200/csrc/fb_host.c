@@ -140,6 +140,10 @@ int fb_params_default(fb_params *p)
   p->cavityradius = 0.0;
   p->cavityratio = 1.0;
   p->cavitywidth = 1.0;
+  /* thermal diffusion (src/var.c:85-86, 93) */
+  p->entropy_diffusion = 0;
+  p->radiative_diffusion = 0;
+  p->diffusivity = 0.000001;
   return FB_OK;
 }
 
@@ -314,9 +318,15 @@ int fb_params_read_par(fb_params *p, const char *path)
   if (p->energy_equation && p->adiabaticindex == 1) p->energy_equation = 0; /* Interpret.c:426-429 */
   if (is_c(kv_c(&set, "VISCOUSHEATING", 'Y'), 'N')) p->viscous_heating = 0;
   if (is_c(kv_c(&set, "BETACOOLING", 'N'), 'Y')) p->beta_cooling = 1;
-  if (is_c(kv_c(&set, "ENTROPYDIFFUSION", 'N'), 'Y')) p->unsupported |= FB_U_THERMALDIFF;
+  /* thermal diffusion (src/Interpret.c:381-388); the implicit solver's
+     red-black sweep equals the reference's sequential one only when the
+     two cells either side of the azimuthal wrap have different colours */
+  if (is_c(kv_c(&set, "ENTROPYDIFFUSION", 'N'), 'Y')) p->entropy_diffusion = 1;
   c = kv_c(&set, "RADIATIVEDIFFUSION", 'N');
-  if (is_c(c, 'E') || is_c(c, 'I')) p->unsupported |= FB_U_THERMALDIFF;
+  if (is_c(c, 'E')) p->radiative_diffusion = 1;
+  if (is_c(c, 'I')) p->radiative_diffusion = 2;
+  p->diffusivity = kv_num(&set, "DIFFUSIVITY", p->diffusivity);
+  if (p->radiative_diffusion == 2 && (p->nsec % 2) != 0) p->unsupported |= FB_U_THERMALDIFF;
   if (is_c(kv_c(&set, "THERMALCOOLING", 'N'), 'Y')) p->thermal_cooling = 1;
   if (is_c(kv_c(&set, "SETCONSTANTOPACITY", 'N'), 'Y')) p->constant_opacity = 1;
   c = kv_c(&set, "STELLARIRRADIATION", 'N');

@@ -37,7 +37,7 @@ extern boolean DustFeelDisk, DustFeelPlanets, DustFeelTurb, DustFeelSG, DustFeel
 extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensity, ZZIntegrator;
 extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
 extern boolean CompareSGAndSummationTorques, KNOpen, SetConstantOpacity, StellarIrradiation, ImposedStellarLuminosity;
-extern boolean HighMCutoff;
+extern boolean HighMCutoff, ImplicitRadiativeDiffusion;
 extern Pair DiskOnPrimaryAcceleration, DiskOnPrimaryAcceleration_alt;
 
 static fb_ctx *g_ctx = NULL;
@@ -139,7 +139,10 @@ static void params_from_globals(fb_params *p)
   p->cavityratio = CAVITYRATIO;
   p->cavitywidth = CAVITYWIDTH;
   if (MHDLSA && (NBPART != 0 || NBTURBMODES < 0 || NBTURBMODES > FB_LSA_MAX_MODES)) p->unsupported |= FB_U_MHDLSA;
-  if (EntropyDiffusion || RadiativeDiffusion) p->unsupported |= FB_U_THERMALDIFF;
+  p->entropy_diffusion = EntropyDiffusion;
+  p->radiative_diffusion = RadiativeDiffusion ? (ImplicitRadiativeDiffusion ? 2 : 1) : 0;
+  p->diffusivity = DIFFUSIVITY;
+  if (p->radiative_diffusion == 2 && (NSEC % 2) != 0) p->unsupported |= FB_U_THERMALDIFF;
   p->thermal_cooling = ThermalCooling;
   p->constant_opacity = SetConstantOpacity;
   p->imposedconstantopacity = IMPOSEDCONSTANTOPACITY;

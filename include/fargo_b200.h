@@ -138,6 +138,13 @@ typedef struct fb_params {
   int mhd_lsa, nbturbmodes, high_m_cutoff;
   double gammaturb, lsamodespeedup, turbrmin, turbrmax;
   double cavityradius, cavityratio, cavitywidth;
+  /* thermal diffusion with the energy equation (src/SourceEuler.c:722-762,
+     1740-2052): ENTROPYDIFFUSION (explicit, coefficient DIFFUSIVITY) and
+     RADIATIVEDIFFUSION, 0 No, 1 E (explicit, flux-limited, Bell & Lin
+     opacities of the current state), 2 I (implicit: red-black successive
+     over-relaxation, needs an even NSEC) */
+  int entropy_diffusion, radiative_diffusion;
+  double diffusivity;
 } fb_params;
 
 #define FB_LSA_MAX_MODES 256

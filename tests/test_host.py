@@ -49,9 +49,10 @@ def test_params_defaults_and_switches():
 def test_unsupported_features_are_refused(tmp_path):
     from dustyfargoadsg_b200 import Disc, FbError, read_par
     src = os.path.join(CFG, "iso_128x384.par")
-    for key, val in (("InnerBoundary", "Accreting"), ("Frame", "C"), ("DustFluid", "Yes"),
-                     ("EntropyDiffusion", "Yes")):
-        par = _oracle.write_par(src, str(tmp_path), **{key: val})
+    for keys in ({"InnerBoundary": "Accreting"}, {"Frame": "C"}, {"DustFluid": "Yes"},
+                 {"EnergyEquation": "Yes", "RadiativeDiffusion": "Implicit", "Nsec": "385"}):
+        key = ",".join(keys)
+        par = _oracle.write_par(src, str(tmp_path), **keys)
         p = read_par(par)
         assert p.unsupported != 0, key
         with pytest.raises(FbError):
@@ -170,3 +171,16 @@ def test_rand48_state_helper():
         x = (0x5DEECE66D * x + 0xB) & ((1 << 48) - 1)
     assert lib.fb_rand48_state(7, 1000) == x
     assert lib.fb_rand48_state(0, 0) == 0x330E
+
+
+def test_thermal_diffusion_parameters(tmp_path):
+    """ENTROPYDIFFUSION, RADIATIVEDIFFUSION (E explicit, I implicit) and
+    DIFFUSIVITY (src/var.c:85-93, src/Interpret.c:381-388)."""
+    from dustyfargoadsg_b200 import read_par
+    src = os.path.join(CFG, "adiabatic_sg_512x1536.par")
+    p = read_par(_oracle.write_par(src, str(tmp_path), EntropyDiffusion="Yes", Diffusivity="2e-5",
+                                   RadiativeDiffusion="Explicit"))
+    assert p.entropy_diffusion == 1 and p.radiative_diffusion == 1 and p.diffusivity == 2e-5 and p.unsupported == 0
+    os.makedirs(str(tmp_path / "i"))
+    q = read_par(_oracle.write_par(src, str(tmp_path / "i"), RadiativeDiffusion="Implicit"))
+    assert q.radiative_diffusion == 2 and q.entropy_diffusion == 0 and q.diffusivity == 1e-6 and q.unsupported == 0
