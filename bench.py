@@ -60,7 +60,7 @@ STAGE_BYTES = {
     "substep1": (64, 64), "viscous_terms": (56, 56), "viscous_update": (64, 64),
     "substep2": (40, 56), "substep3": (0, 80),
     "transport_radial": (64, 80), "transport_azimuthal": (80, 96),
-    "transport_vr_boundary": (40, 40),
+    "transport_vr_boundary": (40, 40), "transport_ring_means": (8, 8),
 }
 
 

@@ -99,7 +99,8 @@ class Disc:
             # the turbulent modes draw from the reference's global drand48
             # stream: seeded when the .par is read (Interpret.c:404-407),
             # reseeded and advanced by the initial noise when there is some
-            self.set_lsa_stream(self.lib.fb_rand48_state(int(seed), self.nr * self.ns if noise else 0))
+            draws = self.nr * self.ns if (noise or self.p.add_noise) else 0
+            self.set_lsa_stream(self.lib.fb_rand48_state(int(seed), draws))
         if self.npart > 0:
             # InitDustSystem reseeds the stream (Dsys.c:173)
             check(self.lib.fb_init_dust(C.byref(self.p), self.ctx, int(seed if dust_seed is None else dust_seed),

@@ -62,6 +62,7 @@ class FbParams(C.Structure):
         ("gammaturb", _D), ("lsamodespeedup", _D), ("turbrmin", _D), ("turbrmax", _D),
         ("cavityradius", _D), ("cavityratio", _D), ("cavitywidth", _D),
         ("entropy_diffusion", _I), ("radiative_diffusion", _I), ("diffusivity", _D),
+        ("corotating", _I), ("add_noise", _I), ("temppresc", _I), ("presctime0", _D),
     ]
 
 

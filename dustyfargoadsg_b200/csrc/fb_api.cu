@@ -13,13 +13,14 @@
 enum {
   ST_CFL, ST_SUB0, ST_CONTROL, ST_SOUND, ST_POT, ST_SUB1, ST_SG, ST_SGCOLS, ST_SGINV, ST_SGUPD,
   ST_VTERMS, ST_VUPDATE,
-  ST_SUB2, ST_EVTERMS, ST_SUB3, ST_TRAD, ST_TAZI, ST_TVR, ST_DAMP, ST_DUST, FB_NSTAGE
+  ST_SUB2, ST_EVTERMS, ST_SUB3, ST_TRAD, ST_TAZI, ST_TVR, ST_DAMP, ST_DUST, ST_TVMED, FB_NSTAGE
 };
 static const char *stage_names[FB_NSTAGE] = {
   "cfl_forces", "substep0", "controller", "soundspeed", "potential", "substep1", "sg_rows_fwd",
   "sg_cols", "sg_rows_inv", "sg_update",
   "viscous_terms", "viscous_update", "substep2", "energy_viscous_terms", "substep3",
-  "transport_radial", "transport_azimuthal", "transport_vr_boundary", "damping", "dust_particles"};
+  "transport_radial", "transport_azimuthal", "transport_vr_boundary", "damping", "dust_particles",
+  "transport_ring_means"};
 
 struct fb_ctx {
   fb_params p;
@@ -404,6 +405,7 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.dphi = (p->pmax - p->pmin) / (double)ns;
   k.invdphi = 1.0 / k.dphi;
   k.omega_frame = p->omegaframe;
+  k.corot = p->corotating;
   k.gamma = p->adiabaticindex;
   k.alpha = p->alphaviscosity;
   k.nu_const = p->viscosity;
@@ -414,6 +416,16 @@ extern "C" int fb_create(const fb_params *p, const double *radii, fb_ctx **out)
   k.fast_transport = p->fast_transport;
   k.wall = p->wall_boundary;
   k.thermal_cooling = p->energy_equation && p->thermal_cooling;
+  if (p->energy_equation && p->temppresc && !k.thermal_cooling) {
+    // FillPrescTime (Theo.c:200-212) or PRESCTIME0 / pow(Rmed, -1.5)
+    std::vector<double> pt(nr);
+    for (int i = 0; i < nr; i++)
+      pt[i] = (p->viscosity > 0.0) ? p->presctime0 * pow(ctx->g.rmed[i], 2.0 + 2.0 * p->flaringindex)
+                                   : p->presctime0 / pow(ctx->g.rmed[i], -1.5);
+    k.temppresc = 1;
+    k.presc = dtable(ctx, pt.data(), nr);
+    if (!k.presc) { fb_destroy(ctx); return FB_ERR_NOMEM; }
+  }
   if (p->energy_equation && (p->entropy_diffusion || p->radiative_diffusion)) {
     // thermal diffusion (SubStep0): its scratch fields, and for radiative
     // diffusion the opacity of every substep with ComputeOpacities' constants
@@ -653,7 +665,7 @@ extern "C" int fb_upload(fb_ctx *ctx, const fb_state *s, const fb_profiles *prof
     c->pfinal[q] = pl.final_mass[q];
     c->pfeelothers[q] = pl.feelothers[q];
   }
-  if (ctx->p.omegaframe != s->omega_frame) {
+  if (!ctx->p.corotating && ctx->p.omegaframe != s->omega_frame) {
     set_err(ctx, "OmegaFrame must stay OMEGAFRAME (non-rotating frame)");
     return FB_ERR_UNSUPPORTED;
   }
@@ -707,15 +719,25 @@ static int enqueue_substep(fb_ctx *ctx)
     STAGE(ST_CFL, 1, fb_launch_td_cfl(k, s));
   }
   STAGE(ST_CFL, 1, fb_launch_cfl(k, s));  // ConditionCFL + the controller (last CTA)
-  // the planets' step on a branch of its own: no gas kernel of the substep
-  // reads the positions it writes; joined before the particles' velocity
-  // update, else at the end of the substep
-  cudaEventRecord(ctx->ev_fork, s);
-  cudaStreamWaitEvent(ctx->st_planets, ctx->ev_fork, 0);
-  fb_launch_planets(k, ctx->has_dust ? &ctx->pp : NULL, ctx->st_planets);
-  cudaEventRecord(ctx->ev_planets, ctx->st_planets);
-  ctx->launches += 1;
-  ctx->pcount[ST_CFL] += 1;
+  if (k.corot) {
+    // corotating frame: FillForcesArrays' turbulent modes still see the old
+    // OmegaFrame; then the planets' step sets the new one and CorrectVtheta
+    // applies its change before the gas update (SourceEuler.c:476-525)
+    if (k.lsa) STAGE(ST_POT, 2, fb_launch_lsa_modes(k, s));
+    STAGE(ST_CFL, 1, fb_launch_planets(k, NULL, s));
+    STAGE(ST_CFL, 1, fb_launch_correct_vtheta(k, s));
+    cudaEventRecord(ctx->ev_planets, s);
+  } else {
+    // the planets' step on a branch of its own: no gas kernel of the substep
+    // reads the positions it writes; joined before the particles' velocity
+    // update, else at the end of the substep
+    cudaEventRecord(ctx->ev_fork, s);
+    cudaStreamWaitEvent(ctx->st_planets, ctx->ev_fork, 0);
+    fb_launch_planets(k, ctx->has_dust ? &ctx->pp : NULL, ctx->st_planets);
+    cudaEventRecord(ctx->ev_planets, ctx->st_planets);
+    ctx->launches += 1;
+    ctx->pcount[ST_CFL] += 1;
+  }
   // particles after the planets' RK5 step and before the gas update
   // (SourceEuler.c:504-531)
   if (ctx->has_dust)
@@ -726,7 +748,7 @@ static int enqueue_substep(fb_ctx *ctx)
     STAGE(ST_SUB0, n0, n0 = fb_launch_substep0(k, s));
   }
   if (k.energy) STAGE(ST_SOUND, 1, fb_launch_soundspeed(k, k.visc_mode == 1, s));
-  if (k.lsa) STAGE(ST_POT, 2, fb_launch_lsa_modes(k, s));  // the turbulent modes at the substep's start
+  if (k.lsa && !k.corot) STAGE(ST_POT, 2, fb_launch_lsa_modes(k, s));  // the turbulent modes at the substep's start
   STAGE(ST_POT, 1, fb_launch_potential(k, s));
   if (k.lsa) STAGE(ST_POT, 1, fb_launch_lsa_add(k, s));
   STAGE(ST_SUB1, 1, fb_launch_substep1(k, s));
@@ -755,7 +777,7 @@ static int enqueue_substep(fb_ctx *ctx)
     fb_launch_azi_vmed(k, 0.0, ctx->st_sg);
     cudaEventRecord(ctx->ev_vm_done, ctx->st_sg);
     ctx->launches += 1;
-    ctx->pcount[ST_TAZI] += 1;
+    ctx->pcount[ST_TVMED] += 1;
   }
   if (k.energy) STAGE(ST_SUB3, 1, fb_launch_substep3(k, s));  // with the stresses of the new velocities
   STAGE(ST_TRAD, 1, fb_launch_transport_radial(k, 0.0, s));
@@ -763,7 +785,9 @@ static int enqueue_substep(fb_ctx *ctx)
     cudaStreamWaitEvent(s, ctx->ev_vm_done, 0);
     STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s, true));
   } else {
-    STAGE(ST_TAZI, fb_azi_launches(k), fb_launch_transport_azimuthal(k, 0.0, s));  // ring means + tiles
+    // the tile variant's ring means as a stage of their own, then the pass
+    if (fb_azi_launches(k) == 2) STAGE(ST_TVMED, 1, fb_launch_azi_vmed(k, 0.0, s));
+    STAGE(ST_TAZI, 1, fb_launch_transport_azimuthal(k, 0.0, s, true));
   }
   STAGE(ST_TVR, 1, fb_launch_transport_vr(k, s));
   if (k.open_inner || k.non_reflecting) {
@@ -1479,7 +1503,7 @@ extern "C" int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t)
   if (t->rad_columns && (t->rad_columns < 32 || t->rad_columns > 128 || t->rad_columns % 32)) return FB_ERR_INVALID;
   if (t->rad_rings < 0 || t->rad_rings > k.nr) return FB_ERR_INVALID;
   const int E = t->azi_cells_per_thread ? t->azi_cells_per_thread : fb_azi_E_auto(k.ns);
-  if (t->azi_variant < 0 || t->azi_variant > 7 || !fb_azi_variant(k.ns, k.energy, E, t->azi_variant))
+  if (t->azi_variant < 0 || t->azi_variant > 8 || !fb_azi_variant(k.ns, k.energy, E, t->azi_variant))
     return FB_ERR_INVALID;
   k.cell_bs = cb;
   k.azi_variant = t->azi_variant;
@@ -1596,7 +1620,7 @@ extern "C" int fb_tune(fb_ctx *ctx, int substeps, fb_tuning *best, double *ms_ou
     double bestms = 1e300;
     for (int E = 1; E <= 4; E++) {
       if (!fb_azi_E_valid(k.ns, k.energy, E)) continue;
-      for (int var = 1; var <= 7; var++) {
+      for (int var = 1; var <= 8; var++) {
         if (fb_azi_variant(k.ns, k.energy, E, var) != var) continue;
         k.azi_E = E;
         k.azi_variant = var;

@@ -45,6 +45,7 @@ struct fb_ctl {
   double pot_m[FB_MAX_PLANETS], pot_x[FB_MAX_PLANETS], pot_y[FB_MAX_PLANETS];
   double pot_smooth2[FB_MAX_PLANETS], pot_invd3[FB_MAX_PLANETS];
   double t_sub;  // PhysicalTime at the start of the substep (FillForcesArrays' time)
+  double domega; // corotating frame: this substep's change of OmegaFrame (CorrectVtheta)
   // implicit radiative diffusion (SubStep0, SourceEuler.c:749-760): the
   // relaxation parameter omegaSOR and the previous solve's iteration count
   // niterbuf, both carried from solve to solve; sor_iters = the last solve's
@@ -102,6 +103,10 @@ struct KP {
   const double *supp_torque;
   const double *sigmamed, *energymed, *vthetamed, *vradmed;
   const double *betatab;   // ComputeBetaCooling(Rmed)
+  // TEMPPRESC: per ring the relaxation time (PrescTimeMed, or PRESCTIME0 /
+  // Omega without VISCOSITY), SourceEuler.c:1162-1168
+  int temppresc;
+  const double *presc;
   const double *damp_lam;  // damping*damping per ring (0 outside the zones)
   const double *damp_tau;  // DAMPINGTODYNAMICALTIMERATIO*pow(Rmed,1.5)
   const int *damp_rings;   // list of rings inside the wave-killing zones
@@ -115,6 +120,9 @@ struct KP {
   fb_ctl *ctl;
   // scalars
   double pmin, pmax, dphi, invdphi, omega_frame;
+  // frame corotating with the first planet (FRAME C): OmegaFrame changes
+  // every substep and lives in the control block; kernels read it via omf()
+  int corot;
   double gamma, alpha, nu_const;
   int visc_mode;           // 0 inviscid, 1 alpha, 2 constant nu
   int energy, viscous_heating, beta_cooling, fast_transport;
@@ -181,6 +189,10 @@ struct KP {
   // 1 narrow, 2 wide, 3 packed, 4 register, 5 staged, 6 tile)
   int cell_bs, azi_E, rad_tx, rad_chunk, azi_variant;
 };
+
+// OmegaFrame as the current substep sees it: the control block's in a
+// corotating frame (updated by the planets' step), else the constant
+static __device__ __forceinline__ double omf(const KP &k) { return k.corot ? k.ctl->omega_frame : k.omega_frame; }
 
 // Device state of the particles' random stream (src/DustUpdate.c:438-485).
 // a / d rounded to nearest, given r = 1/d rounded to nearest (fb_rcp in the
@@ -329,6 +341,7 @@ struct PP {
 // launchers (fb_gas.cu)
 void fb_launch_cfl(const KP &k, cudaStream_t s);
 void fb_launch_planets(const KP &k, const PP *pp, cudaStream_t s);
+void fb_launch_correct_vtheta(const KP &k, cudaStream_t s);  // corotating frame: CorrectVtheta
 void fb_launch_soundspeed(const KP &k, int update_gcs, cudaStream_t s);
 void fb_launch_potential(const KP &k, cudaStream_t s);
 // turbulent potential: mode draws and tables after the controller, the

@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(DG_BS) k_vortensity(KP k, double *xi)
   const size_t limjm = ljm - ns;
   const double drvt = (k.rmed[i] * k.vt[l] - k.rmed[i - 1] * k.vt[lim]) / (k.rmed[i] - k.rmed[i - 1]);
   const double dvr = (k.vr[l] - k.vr[ljm]) * k.invdphi;
-  const double omega = (drvt - dvr) / k.rinf[i] + 2.0 * k.omega_frame;
+  const double omega = (drvt - dvr) / k.rinf[i] + 2.0 * omf(k);
   const double sig = 0.25 * (k.rho[l] + k.rho[lim] + k.rho[ljm] + k.rho[limjm]);
   xi[l] = omega / sig;
 }

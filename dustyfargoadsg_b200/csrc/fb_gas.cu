@@ -111,8 +111,20 @@ static __device__ double block_min_dyn(double v, double *sh)
 
 static __device__ void controller_body(const KP &k, double *sh, fb_ctl *c);
 static __device__ void planet_prelude(const KP &k, fb_ctl *c);
+// Work arrays of the planets' step.  k_planets is one thread and keeps them
+// in shared memory: with them as local arrays of the thread, the device
+// compiler of this toolkit produced stage derivatives whose x component read
+// the distance array instead of the positions (found by comparing one step
+// of a free planet with the reference's; the shared-memory form matches it
+// to the last bit).
+struct RkWork {
+  double k[6][4 * FB_MAX_PLANETS];
+  double dist[FB_MAX_PLANETS];
+  double q0[4 * FB_MAX_PLANETS], q1[4 * FB_MAX_PLANETS], masses[FB_MAX_PLANETS];
+};
+
 static __device__ void rk5(const double *q0, double dt, const double *masses, double *q1, int n,
-                           const int *feelothers, int indirect);
+                           const int *feelothers, int indirect, RkWork &w);
 
 // ---------------------------------------------------------------- CFL
 // ConditionCFL (SourceEuler.c:1304-1552): one CTA per ring computes the
@@ -266,17 +278,22 @@ __global__ void k_planets(KP k, fb_dust_ctl *dc, double thick, double aspect, do
 {
   fb_grid_dependency();
   fb_ctl *c = k.ctl;
+  c->domega = 0.0;
   if (c->status != FB_OK) return;
   const int np = c->np;
   const double dt = c->dt;
+  // corotating frame: GetPsysInfo(sys, MARK) (SourceEuler.c:476, Psys.c:
+  // 323-326): the first planet's position at the start of the substep
+  const double xmark = (np > 0) ? c->px[0] : 0.0, ymark = (np > 0) ? c->py[0] : 0.0;
   // AdvanceSystemRK5 (Pframeforce.c:163-266)
   if (!k.forced_circular) {
-    double q0[4 * FB_MAX_PLANETS], q1[4 * FB_MAX_PLANETS], masses[FB_MAX_PLANETS];
+    __shared__ RkWork rw;
+    double *q0 = rw.q0, *q1 = rw.q1, *masses = rw.masses;
     for (int i = 0; i < np; i++) {
       q0[i] = c->px[i]; q0[i + np] = c->py[i]; q0[i + 2 * np] = c->pvx[i]; q0[i + 3 * np] = c->pvy[i];
       masses[i] = c->pm[i];
     }
-    if (np > 0) rk5(q0, dt, masses, q1, np, c->pfeelothers, k.indirect_term);
+    if (np > 0) rk5(q0, dt, masses, q1, np, c->pfeelothers, k.indirect_term, rw);
     for (int i = 0; i < np; i++) {
       c->px[i] = q1[i]; c->py[i] = q1[i + np]; c->pvx[i] = q1[i + 2 * np]; c->pvy[i] = q1[i + 3 * np];
     }
@@ -294,6 +311,18 @@ __global__ void k_planets(KP k, fb_dust_ctl *dc, double thick, double aspect, do
       c->pvx[i] = -v * sin(theta + dtheta);
       c->pvy[i] = v * cos(theta + dtheta);
     }
+  }
+  // corotating frame (SourceEuler.c:516-524): OmegaFrame becomes the angle
+  // the first planet turned through during the step (GetPsysInfo GET,
+  // Psys.c:327-337) over dt; CorrectVtheta follows with the change
+  if (k.corot && np > 0) {
+    const double x = c->px[0], y = c->py[0];
+    const double d2 = sqrt(x * x + y * y);
+    const double d1 = sqrt(xmark * xmark + ymark * ymark);
+    const double cross = xmark * y - x * ymark;
+    const double omega_new = asin(cross / (d1 * d2)) / dt;
+    c->domega = omega_new - c->omega_frame;
+    c->omega_frame = omega_new;
   }
   // RotatePsys (Psys.c:352-372) with angle OmegaFrame*dt
   {
@@ -319,6 +348,22 @@ __global__ void k_planets(KP k, fb_dust_ctl *dc, double thick, double aspect, do
   }
 }
 
+// CorrectVtheta (SideEuler.c:1133-1147): vtheta -= domega Rmed on rings
+// 0..nr-1 after the frame's angular velocity changed by domega
+__global__ void __launch_bounds__(FB_BS2) k_correct_vtheta(KP k)
+{
+  fb_grid_dependency();
+  const int i = blockIdx.y, j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= k.ns) return;
+  const double domega = k.ctl->domega;
+  k.vt[(size_t)i * k.ns + j] -= domega * k.rmed[i];
+}
+
+void fb_launch_correct_vtheta(const KP &k, cudaStream_t s)
+{
+  fb_launch(k_correct_vtheta, grid2d(k, k.nr), k.cell_bs, 0, s, k);
+}
+
 void fb_launch_planets(const KP &k, const PP *pp, cudaStream_t s)
 {
   if (pp && pp->feel_planets)
@@ -339,11 +384,10 @@ static __device__ double dev_aspect_ratio(const KP &k, double rad)
 
 // DerivMotionRK5 (RungeKunta.c:13-53)
 static __device__ void rk5_deriv(const double *q, const double *masses, double *deriv, int n,
-                                 double dt, const int *feelothers, int indirect)
+                                 double dt, const int *feelothers, int indirect, double *Dist)
 {
   const double *x = q, *y = q + n, *vx = q + 2 * n, *vy = q + 3 * n;
   double *dx = deriv, *dy = deriv + n, *dvx = deriv + 2 * n, *dvy = deriv + 3 * n;
-  double Dist[FB_MAX_PLANETS];
   for (int i = 0; i < n; i++) Dist[i] = sqrt(x[i] * x[i] + y[i] * y[i]);
   for (int i = 0; i < n; i++) {
     dx[i] = vx[i];
@@ -368,28 +412,30 @@ static __device__ void rk5_deriv(const double *q, const double *masses, double *
 
 // RungeKunta (RungeKunta.c:64-91)
 static __device__ void rk5(const double *q0, double dt, const double *masses, double *q1, int n,
-                           const int *feelothers, int indirect)
+                           const int *feelothers, int indirect, RkWork &w)
 {
   // k2..k5 enter the first translations multiplied by 0.0; the reference
   // seeds them with the previous call's k6 (RungeKunta.c:73-75), which is
   // finite, so zeros give the same sums.
-  double k1[4 * FB_MAX_PLANETS] = {0}, k2[4 * FB_MAX_PLANETS] = {0}, k3[4 * FB_MAX_PLANETS] = {0};
-  double k4[4 * FB_MAX_PLANETS] = {0}, k5[4 * FB_MAX_PLANETS] = {0}, k6[4 * FB_MAX_PLANETS] = {0};
+  double *k1 = w.k[0], *k2 = w.k[1], *k3 = w.k[2], *k4 = w.k[3], *k5 = w.k[4], *k6 = w.k[5];
+  for (int s = 0; s < 6; s++)
+    for (int i = 0; i < 4 * FB_MAX_PLANETS; i++) w.k[s][i] = 0.0;
+  double *Dist = w.dist;
   const int m = 4 * n;
-  rk5_deriv(q0, masses, k1, n, dt, feelothers, indirect);
+  rk5_deriv(q0, masses, k1, n, dt, feelothers, indirect, Dist);
   for (int i = 0; i < m; i++) q1[i] = q0[i] + 0.2 * k1[i] + 0.0 * k2[i] + 0.0 * k3[i] + 0.0 * k4[i] + 0.0 * k5[i];
-  rk5_deriv(q1, masses, k2, n, dt, feelothers, indirect);
+  rk5_deriv(q1, masses, k2, n, dt, feelothers, indirect, Dist);
   for (int i = 0; i < m; i++) q1[i] = q0[i] + 0.075 * k1[i] + 0.225 * k2[i] + 0.0 * k3[i] + 0.0 * k4[i] + 0.0 * k5[i];
-  rk5_deriv(q1, masses, k3, n, dt, feelothers, indirect);
+  rk5_deriv(q1, masses, k3, n, dt, feelothers, indirect, Dist);
   for (int i = 0; i < m; i++) q1[i] = q0[i] + 0.3 * k1[i] + -0.9 * k2[i] + 1.2 * k3[i] + 0.0 * k4[i] + 0.0 * k5[i];
-  rk5_deriv(q1, masses, k4, n, dt, feelothers, indirect);
+  rk5_deriv(q1, masses, k4, n, dt, feelothers, indirect, Dist);
   for (int i = 0; i < m; i++)
     q1[i] = q0[i] + -11.0 / 54.0 * k1[i] + 2.5 * k2[i] + -70.0 / 27.0 * k3[i] + 35.0 / 27.0 * k4[i] + 0.0 * k5[i];
-  rk5_deriv(q1, masses, k5, n, dt, feelothers, indirect);
+  rk5_deriv(q1, masses, k5, n, dt, feelothers, indirect, Dist);
   for (int i = 0; i < m; i++)
     q1[i] = q0[i] + 1631.0 / 55296.0 * k1[i] + 175.0 / 512.0 * k2[i] + 575.0 / 13824.0 * k3[i] +
             44275.0 / 110592.0 * k4[i] + 253.0 / 4096.0 * k5[i];
-  rk5_deriv(q1, masses, k6, n, dt, feelothers, indirect);
+  rk5_deriv(q1, masses, k6, n, dt, feelothers, indirect, Dist);
   for (int i = 0; i < m; i++)
     q1[i] = q0[i] + 37.0 / 378.0 * k1[i] + 250.0 / 621.0 * k3[i] + 125.0 / 594.0 * k4[i] + 512.0 / 1771.0 * k6[i];
 }
@@ -693,7 +739,7 @@ __global__ void __launch_bounds__(FB_BS2, 4) k_substep1(KP k)
     double gradp = (Pl - Plim) * 2.0 / (rl + rlim) * invdiffrmed;
     double gradphi = (potl - potlim) * invdiffrmed;
     double vt2 = vtl + vtjp + vtlim + vtjplim;
-    vt2 = vt2 / 4.0 + rinf * k.omega_frame;
+    vt2 = vt2 / 4.0 + rinf * omf(k);
     vt2 = vt2 * vt2;
     k.vri[l] = vrl + dt * (-gradp - gradphi + vt2 * invrinf);
     if (k.particles) {  // RadGradP, RadIndAcc (SourceEuler.c:875-877)
@@ -897,7 +943,7 @@ __global__ void __launch_bounds__(FB_BS2, 5) k_substep2(KP k)
     // SubStep3's ring mean of vtheta (SourceEuler.c:1196-1203): this CTA's
     // part, summed in a fixed order
     __shared__ double sh[FB_BS2 / 32];
-    double v = cell ? (vtnew + k.rmed[i] * k.omega_frame) : 0.0;
+    double v = cell ? (vtnew + k.rmed[i] * omf(k)) : 0.0;
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
     __syncthreads();
@@ -1019,6 +1065,12 @@ __global__ void __launch_bounds__(FB_BS2) k_substep3(KP k)
     double num = el + (double)(heat ? 1 : 0) * vh * dt;
     double den = 1.0 + (k.gamma - 1.0) * dt * dv;
     en = num / den;
+    if (k.temppresc) {  // relaxation towards the initial profile (SourceEuler.c:1162-1175)
+      const double coolingtime = k.presc[i];
+      num = en + k.energymed[i] * (rl / k.sigmamed[i]) * (dt / coolingtime);
+      den = 1.0 + dt / coolingtime;
+      en = num / den;
+    }
     if (k.beta_cooling) {
       const double d2 = 1.0 + dt / coolfac;  // one per ring: the quotient through its reciprocal
       en = fb_quot(en, d2, 1.0 / d2);
@@ -1110,7 +1162,7 @@ static __device__ __forceinline__ void radial_column(const KP &k, double dt, int
   constexpr int LO = H ? 3 : 0, NH = (H ? NQ : 3) - LO;
   const int ns = k.ns, nr = k.nr;
   const int jp = (j == ns - 1) ? 0 : j + 1;
-  const double Om = k.omega_frame;
+  const double Om = omf(k);
   const double dtheta = (k.pmax - k.pmin) / (double)ns;
   // window: index 0 = ring k-1, 1 = ring k, 2 = ring k+1
   double W[NH][3], Qo[NH][3], R[3], VW[3];
@@ -1520,8 +1572,8 @@ __global__ void __launch_bounds__(AziMaxThreads<E, WIDE>::value) k_transport_azi
   const int subkep = (!k.transport_only) && (i == 0 || i == nr - 1);
   for (int j = tid; j < ns; j += T) {
     const int jm = (j == 0) ? ns - 1 : j - 1;
-    double v = (tp[jm] + tm[j]) / (rho[j] + rho[jm] + 1e-20) / k.rmed[i] - k.rmed[i] * k.omega_frame;
-    if (subkep) v = k.vthetamed[i] - k.rmed[i] * k.omega_frame;
+    double v = (tp[jm] + tm[j]) / (rho[j] + rho[jm] + 1e-20) / k.rmed[i] - k.rmed[i] * omf(k);
+    if (subkep) v = k.vthetamed[i] - k.rmed[i] * omf(k);
     k.vt[base + j] = v;
     k.rho_t[base + j] = rho[j];
     k.q[0][base + j] = Q[j];
@@ -1770,8 +1822,8 @@ __global__ void __launch_bounds__((E == 1) ? 1024 : 768) k_transport_azimuthal_p
     const int jm = (j == 0) ? ns - 1 : j - 1;
     const double2 c0 = pair(P, j, 0), c1 = pair(P, j, 1), c2 = pair(P, j, 2), m1 = pair(P, jm, 1), m2 = pair(P, jm, 2);
     const double rj = (RH & 1) ? c2.y : c2.x, rjm = (RH & 1) ? m2.y : m2.x;  // RH is 4 or 5
-    double v = (m1.x + c1.y) / (rj + rjm + 1e-20) / k.rmed[i] - k.rmed[i] * k.omega_frame;  // tp[jm] + tm[j]
-    if (subkep) v = k.vthetamed[i] - k.rmed[i] * k.omega_frame;
+    double v = (m1.x + c1.y) / (rj + rjm + 1e-20) / k.rmed[i] - k.rmed[i] * omf(k);  // tp[jm] + tm[j]
+    if (subkep) v = k.vthetamed[i] - k.rmed[i] * omf(k);
     k.vt[base + j] = v;
     k.rho_t[base + j] = rj;
     k.q[0][base + j] = c0.x;
@@ -2070,8 +2122,8 @@ static __device__ __forceinline__ void azr_ring(const KP &k, double dt, int i, c
     }
     if (p >= ns) p -= ns;
     const double tpm = (e == 0) ? xl[0] : q0[2][e - 1], rm = (e == 0) ? xl[1] : q0[RH][e - 1];
-    double v = (tpm + q0[3][e]) / (q0[RH][e] + rm + 1e-20) / rmi - rmi * k.omega_frame;
-    if (subkep) v = tb.vthetamed - rmi * k.omega_frame;
+    double v = (tpm + q0[3][e]) / (q0[RH][e] + rm + 1e-20) / rmi - rmi * omf(k);
+    if (subkep) v = tb.vthetamed - rmi * omf(k);
     double en = 0.0;
     if (NQ == 6) {
       en = q0[(NQ == 6) ? 4 : 0][e];
@@ -2413,6 +2465,7 @@ int fb_azi_variant(int ns, int energy, int E, int variant)
     case 5: return azs_fits(ns, energy, E) ? 5 : 0;
     case 6: return azt_fits(ns, E) ? 6 : 0;
     case 7: return azt_fits(ns, E) ? 7 : 0;
+    case 8: return azt_fits(ns, E) ? 8 : 0;
     default: return 0;
   }
 }
@@ -2426,12 +2479,12 @@ static int azi_resolve(const KP &k, int *Eout)
   int var = fb_azi_variant(k.ns, k.energy, E, k.azi_variant);
   if (var == 0) var = 1;
   if (var == 5 && !azs_pointers_aligned(k, NQ)) var = 4;  // bulk copies need 16-byte aligned rows
-  if ((var == 6 || var == 7) && !(k.azt_buf[0] && k.azt_buf[1] && k.azt_buf[2] && k.azt_vmed))
+  if ((var == 6 || var == 7 || var == 8) && !(k.azt_buf[0] && k.azt_buf[1] && k.azt_buf[2] && k.azt_vmed))
     var = azr_fits(k.ns, E) ? 4 : 1;
   if (Eout) *Eout = E;
   return var;
 }
-static bool azt_variant(int var) { return var == 6 || var == 7; }
+static bool azt_variant(int var) { return var == 6 || var == 7 || var == 8; }
 int fb_azi_launches(const KP &k) { return azt_variant(azi_resolve(k, nullptr)) ? 2 : 1; }
 
 // LostMass += LostByDisk of the density's VanLeerRadial (TransportEuler.c:137,
@@ -2592,7 +2645,7 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s, bo
   const bool wide = (var == 2);
   const int th = azi_threads_for(k.ns, E);
   const bool full = (th * E == k.ns);  // every thread owns E cells
-  if (var == 6 || var == 7) {
+  if (var == 6 || var == 7 || var == 8) {
     if (!vmed_done) fb_launch(k_azi_vmed, k.nr, th, 0, s, k, dt_override);
     const int CO = AZT_CO(E), ntiles = (k.ns + CO - 1) / CO;
     const int grid = (int)(((long)k.nr * ntiles + AZT_WPC - 1) / AZT_WPC);
@@ -2602,6 +2655,12 @@ static void launch_azimuthal(const KP &k, double dt_override, cudaStream_t s, bo
         case 2: AZT_LAUNCH(2, 4); break;
         case 3: AZT_LAUNCH(3, 4); break;
         default: AZT_LAUNCH(4, 4); break;
+      }
+    } else if (var == 8) {  // five CTAs per SM (at most 102 registers)
+      switch (E) {
+        case 2: AZT_LAUNCH(2, 5); break;
+        case 3: AZT_LAUNCH(3, 5); break;
+        default: AZT_LAUNCH(4, 5); break;
       }
     } else {
       switch (E) {
@@ -2983,8 +3042,8 @@ __global__ void k_boundary_only(KP k)
     k.rho[(size_t)(nr - 2) * ns + j] = k.sigmamed[nr - 2];
     k.rho[(size_t)(nr - 1) * ns + j] = k.sigmamed[nr - 1];
   }
-  k.vt[j] = k.vthetamed[0] - k.rmed[0] * k.omega_frame;
-  k.vt[(size_t)(nr - 1) * ns + j] = k.vthetamed[nr - 1] - k.rmed[nr - 1] * k.omega_frame;
+  k.vt[j] = k.vthetamed[0] - k.rmed[0] * omf(k);
+  k.vt[(size_t)(nr - 1) * ns + j] = k.vthetamed[nr - 1] - k.rmed[nr - 1] * omf(k);
 }
 
 void fb_launch_boundary_only(const KP &k, cudaStream_t s)
@@ -3033,7 +3092,7 @@ __global__ void __launch_bounds__(FB_BS) k_damping(KP k, double dtov)
     dens0 = m[2] / (double)ns;
     energ0 = m[3] / (double)ns;
   } else {
-    vtheta0 = k.vthetamed[i] - k.rmed[i] * k.omega_frame;
+    vtheta0 = k.vthetamed[i] - k.rmed[i] * omf(k);
     vrad0 = k.vradmed[i];
     dens0 = k.sigmamed[i];
     energ0 = k.energymed[i];
@@ -3094,9 +3153,9 @@ __global__ void __launch_bounds__(FB_BS) k_diag(KP k, double *out)
     m += k.surf[i] * k.rho[l];
     double vt_cent;
     if (j < ns - 1)
-      vt_cent = 0.5 * (k.vt[l] + k.vt[l + 1]) + k.rmed[i] * k.omega_frame;
+      vt_cent = 0.5 * (k.vt[l] + k.vt[l + 1]) + k.rmed[i] * omf(k);
     else
-      vt_cent = 0.5 * (k.vt[l] + k.vt[(size_t)i * ns]) + k.rmed[i] * k.omega_frame;
+      vt_cent = 0.5 * (k.vt[l] + k.vt[(size_t)i * ns]) + k.rmed[i] * omf(k);
     p += k.surf[i] * k.rho[l] * k.rmed[i] * vt_cent;
   }
   m = block_sum<FB_BS>(m, sh);

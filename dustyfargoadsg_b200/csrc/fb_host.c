@@ -144,6 +144,10 @@ int fb_params_default(fb_params *p)
   p->entropy_diffusion = 0;
   p->radiative_diffusion = 0;
   p->diffusivity = 0.000001;
+  p->corotating = 0;
+  p->add_noise = 0;
+  p->temppresc = 0;
+  p->presctime0 = 6.28;  /* src/var.c:95 */
   return FB_OK;
 }
 
@@ -332,12 +336,15 @@ int fb_params_read_par(fb_params *p, const char *path)
   c = kv_c(&set, "STELLARIRRADIATION", 'N');
   if (is_c(c, 'Y')) p->stellar_irradiation = 1;
   if (is_c(c, 'L')) p->stellar_irradiation = 2;
-  if (is_c(kv_c(&set, "TEMPPRESC", 'N'), 'Y')) p->unsupported |= FB_U_TEMPPRESC;
+  if (is_c(kv_c(&set, "TEMPPRESC", 'N'), 'Y')) p->temppresc = 1;  /* Interpret.c:397 */
+  p->presctime0 = kv_num(&set, "PRESCTIME0", p->presctime0);
   if (is_c(kv_c(&set, "FORCEDCIRCULAR", 'N'), 'Y')) p->forced_circular = 1;
   if (is_c(kv_c(&set, "FORCEDINNERCIRCULAR", 'N'), 'Y')) p->unsupported |= FB_U_FORCEDINNER;
   if (is_c(kv_c(&set, "EXCLUDEHILL", 'N'), 'Y')) p->exclude_hill = 1;
   c = kv_c(&set, "FRAME", 'F');
-  if (is_c(c, 'C') || is_c(c, 'G') || is_c(c, 'B')) p->unsupported |= FB_U_COROTATING;
+  if (is_c(c, 'C')) p->corotating = 1;  /* Interpret.c:225-232 */
+  if (is_c(c, 'G') || is_c(c, 'B')) p->unsupported |= FB_U_COROTATING;
+  if (p->corotating && is_c(kv_c(&set, "COROTATEWITHOUTERPLANET", 'N'), 'Y')) p->unsupported |= FB_U_COROTATING;
   if (is_c(kv_c(&set, "CICPLANET", 'N'), 'Y')) p->unsupported |= FB_U_CICPLANET;
   if (is_c(kv_c(&set, "BM08TRICK", 'N'), 'Y')) p->unsupported |= FB_U_BM08;
   if (is_c(kv_c(&set, "COMPUTECPDMASS", 'N'), 'Y')) p->unsupported |= FB_U_CPDMASS;
@@ -347,7 +354,7 @@ int fb_params_read_par(fb_params *p, const char *path)
   if (is_c(c, 'Y') || is_c(c, 'B')) p->unsupported |= FB_U_ADDM;
   if (is_c(kv_c(&set, "ADDM2", 'N'), 'Y')) p->unsupported |= FB_U_ADDM;
   if (is_c(kv_c(&set, "ADDM1TOM10", 'N'), 'Y')) p->unsupported |= FB_U_ADDM;
-  if (is_c(kv_c(&set, "ADDNOISE", 'N'), 'Y')) p->unsupported |= FB_U_ADDNOISE;
+  if (is_c(kv_c(&set, "ADDNOISE", 'N'), 'Y')) p->add_noise = 1;  /* Interpret.c:373-376 */
   c = kv_c(&set, "TAILOFF", 'N');
   if (is_c(c, 'G') || is_c(c, 'H') || is_c(c, 'E') || is_c(c, 'A') || is_c(c, 'B') ||
       is_c(c, 'S') || is_c(c, 'I'))
@@ -401,7 +408,7 @@ int fb_params_read_par(fb_params *p, const char *path)
     if (is_c(kv_c(&set, "REMOVEDUSTFROMPLANETSHILLRADIUS", 'N'), 'Y')) p->unsupported |= FB_U_HILLREMOVAL;
     if (p->interpolation != 2) p->unsupported |= FB_U_INTERPOLATION;
     if (is_c(kv_c(&set, "DUSTFEELSG", 'Y'), 'Z')) p->unsupported |= FB_U_DUSTSGZERO;
-    if (p->omegaframe != 0.0) p->unsupported |= FB_U_COROTATING;
+    if (p->omegaframe != 0.0 || p->corotating) p->unsupported |= FB_U_COROTATING;
   }
   if (is_c(kv_c(&set, "DUSTFEELSG", 'Y'), 'N')) p->dust_feel_sg = 0;
   if (!is_c(kv_c(&set, "WRITEDUSTDENSITY", 'N'), 'N')) p->write_dust_density = 1;  /* Interpret.c:255-258 */
@@ -644,6 +651,14 @@ int fb_init_state(const fb_params *p, fb_ctx *ctx, double noise_amp, long noise_
   }
   for (i = 0; i < nr; i++)
     for (j = 0; j < ns; j++) st->dens[j + i * ns] = prof->sigma_med[i];
+  if (p->add_noise) {
+    /* AddNoise (Pframeforce.c:317-320): 1e-3 relative, drand48 from the seed */
+    fb_rand48 r48;
+    fb_srand48(&r48, noise_seed);
+    for (i = 0; i < nr; i++)
+      for (j = 0; j < ns; j++)
+        st->dens[j + i * ns] += 1e-3 * prof->sigma_med[i] * (2.0 * fb_drand48(&r48) - 1.0);
+  }
   if (noise_amp != 0.0) {
     fb_rand48 r48;
     fb_srand48(&r48, noise_seed);
@@ -685,6 +700,25 @@ int fb_init_state(const fb_params *p, fb_ctx *ctx, double noise_amp, long noise_
     }
   }
   st->omega_frame = p->omegaframe;
+  if (p->corotating && st->planets.nb > 0) {
+    /* main.c:228-247: the first planet's angular frequency, from its orbit
+       (GetPsysInfo FREQUENCY, Psys.c:281-297) or, with self-gravity, v / r */
+    const double x = st->planets.x[0], y = st->planets.y[0];
+    const double vx = st->planets.vx[0], vy = st->planets.vy[0];
+    if (!p->self_gravity) {
+      const double m = st->planets.mass[0] + 1.;
+      const double h = x * vy - y * vx;
+      const double d = sqrt(x * x + y * y);
+      const double Ax = x * vy * vy - y * vx * vy - FB_G * m * x / d;
+      const double Ay = y * vx * vx - x * vx * vy - FB_G * m * y / d;
+      const double e = sqrt(Ax * Ax + Ay * Ay) / m;
+      const double a = h * h / FB_G / m / (1. - e * e);
+      st->omega_frame = sqrt(m / a / a / a);
+    } else {
+      const double r = sqrt(x * x + y * y), v = sqrt(vx * vx + vy * vy);
+      st->omega_frame = v / r;
+    }
+  }
 
   /* InitEuler: ComputeSoundSpeed (src/SourceEuler.c:2323-2343) */
   cs = (double *)calloc(nf, sizeof(double));

@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(256) k_lsa_modes(KP k)
     }
     const double ttilde = t - L->t0[q];
     L->s[q] = sin(M_PI * ttilde / L->deltat[q]);
-    const double P = L->phic[q] + (L->omegac[q] - k.omega_frame) * ttilde;
+    const double P = L->phic[q] + (L->omegac[q] - omf(k)) * ttilde;
     double sp, cp;
     sincos(P, &sp, &cp);
     L->cp[q] = cp;

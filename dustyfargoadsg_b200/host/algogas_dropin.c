@@ -37,7 +37,7 @@ extern boolean DustFeelDisk, DustFeelPlanets, DustFeelTurb, DustFeelSG, DustFeel
 extern boolean ShortFrictionTimeApproximation, TSCInterpolation, Write_DustDensity, ZZIntegrator;
 extern boolean DustGrowth, RemoveDustFromPlanetsHillRadius, NoTimestepConstraintByParticles, SoftWriting;
 extern boolean CompareSGAndSummationTorques, KNOpen, SetConstantOpacity, StellarIrradiation, ImposedStellarLuminosity;
-extern boolean HighMCutoff, ImplicitRadiativeDiffusion;
+extern boolean HighMCutoff, ImplicitRadiativeDiffusion, GuidingCenter, BinaryCenter, CorotateWithOuterPlanet;
 extern Pair DiskOnPrimaryAcceleration, DiskOnPrimaryAcceleration_alt;
 
 static fb_ctx *g_ctx = NULL;
@@ -151,8 +151,11 @@ static void params_from_globals(fb_params *p)
   p->backgroundtemperature = BACKGROUNDTEMPERATURE;
   p->slopebackgroundtemperature = SLOPEBACKGROUNDTEMPERATURE;
   p->stellarluminosity = STELLARLUMINOSITY;
-  if (TempPresc) p->unsupported |= FB_U_TEMPPRESC;
-  if (Corotating) p->unsupported |= FB_U_COROTATING;
+  p->temppresc = TempPresc;
+  p->presctime0 = PRESCTIME0;
+  p->corotating = Corotating;
+  if (GuidingCenter || BinaryCenter || CorotateWithOuterPlanet || (Corotating && NBPART != 0))
+    p->unsupported |= FB_U_COROTATING;
   if (BM08) p->unsupported |= FB_U_BM08;
   if (ComputeCPDMass) p->unsupported |= FB_U_CPDMASS;
   if (AdvecteLabel) p->unsupported |= FB_U_LABEL;

@@ -145,6 +145,20 @@ typedef struct fb_params {
      over-relaxation, needs an even NSEC) */
   int entropy_diffusion, radiative_diffusion;
   double diffusivity;
+  /* FRAME C: a frame corotating with the first planet (OMEGAFRAME is then
+     the planet's angular frequency at the start and follows it at every
+     substep, src/main.c:228-247, src/SourceEuler.c:476-525); the guiding-
+     centre and binary-centre frames (G, B) are refused */
+  int corotating;
+  /* ADDNOISE: white noise of relative amplitude 1e-3 on the initial density
+     (src/Pframeforce.c:317-320), drawn by fb_init_state from the drand48
+     stream seeded with its noise_seed (the reference seeds it from the wall
+     clock, src/Interpret.c:373-376); TEMPPRESC: relaxation of the energy
+     towards its initial profile in SubStep3 (src/SourceEuler.c:1159-1175)
+     on the time PRESCTIME0 r^(2+2 FLARINGINDEX) (with VISCOSITY > 0) or
+     PRESCTIME0 / Omega */
+  int add_noise, temppresc;
+  double presctime0;
 } fb_params;
 
 #define FB_LSA_MAX_MODES 256
@@ -341,7 +355,8 @@ typedef struct fb_tuning {
                        register variant's arithmetic with one warp per tile of
                        32 E - 9 cells and no barrier; E = 2..4; four CTAs of four
                        warps per SM), 7 (the tile variant with up to 168
-                       registers a thread: three CTAs per SM) */
+                       registers a thread: three CTAs per SM), 8 (the tile
+                       variant at five CTAs per SM, 96 registers) */
 } fb_tuning;
 int fb_get_tuning(const fb_ctx *ctx, fb_tuning *t);
 int fb_set_tuning(fb_ctx *ctx, const fb_tuning *t);

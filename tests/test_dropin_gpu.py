@@ -21,6 +21,9 @@ pytestmark = [pytest.mark.gpu,
     ("dust_256x768.par", dict(Nrad=64, Nsec=192, NbPart=2000, RminDust=0.6, RmaxDust=1.8)),
     ("iso_128x384.par", dict(Nrad=64, Nsec=192, MHD="L", NbTurbModes=50, GammaTurb="1e-3", TurbRmin=0.6,
                              TurbRmax=2.0)),
+    ("iso_128x384.par", dict(Nrad=64, Nsec=192, Frame="C", InnerBoundary="NONREFLECTING")),
+    ("adiabatic_sg_512x1536.par", dict(Nrad=64, Nsec=192, AddNoise="Yes", TempPresc="Yes", BetaCooling="No",
+                                       InnerBoundary="OPEN", EntropyDiffusion="Yes", Diffusivity="1e-4")),
 ])
 def test_dropin_matches_reference(tmp_path, par_name, keys):
     src = os.path.join(_oracle.CONFIG_DIR, par_name)

@@ -49,7 +49,7 @@ def test_params_defaults_and_switches():
 def test_unsupported_features_are_refused(tmp_path):
     from dustyfargoadsg_b200 import Disc, FbError, read_par
     src = os.path.join(CFG, "iso_128x384.par")
-    for keys in ({"InnerBoundary": "Accreting"}, {"Frame": "C"}, {"DustFluid": "Yes"},
+    for keys in ({"InnerBoundary": "Accreting"}, {"Frame": "G"}, {"DustFluid": "Yes"},
                  {"EnergyEquation": "Yes", "RadiativeDiffusion": "Implicit", "Nsec": "385"}):
         key = ",".join(keys)
         par = _oracle.write_par(src, str(tmp_path), **keys)
@@ -60,12 +60,16 @@ def test_unsupported_features_are_refused(tmp_path):
 
 
 @pytest.mark.skipif(not _oracle.have_oracle(), reason="oracle not built")
-@pytest.mark.parametrize("noise,seed", [(0.0, 0), (1e-4, 0), (1e-3, 7)])
-def test_initial_state_bit_identical(tmp_path, noise, seed):
-    """fb_init_state == the reference's main.c initialisation, bit for bit."""
+@pytest.mark.parametrize("noise,seed,keys", [(0.0, 0, {}), (1e-4, 0, {}), (1e-3, 7, {}),
+                                             (0.0, 5, {"AddNoise": "Yes", "Frame": "C"}),
+                                             (1e-3, 3, {"AddNoise": "Yes", "Frame": "C", "ForcedCircular": "No"})])
+def test_initial_state_bit_identical(tmp_path, noise, seed, keys):
+    """fb_init_state == the reference's main.c initialisation, bit for bit,
+    also with the reference's own AddNoise perturbation (seeded) and in the
+    frame corotating with the planet (OmegaFrame from its orbit)."""
     from dustyfargoadsg_b200 import _ffi, read_par
     src = os.path.join(CFG, "iso_128x384.par")
-    par = _oracle.write_par(src, str(tmp_path), Nrad=48, Nsec=96)
+    par = _oracle.write_par(src, str(tmp_path), Nrad=48, Nsec=96, **keys)
     dumps, _, _ = _oracle.run_oracle(par, steps=1, noise=noise, seed=seed, dump_every=1000)
     ref = dumps["state_init"]
     lib = _ffi.load()
@@ -91,6 +95,7 @@ def test_initial_state_bit_identical(tmp_path, noise, seed):
     assert st.planets.nb == 1
     assert st.planets.x[0] == ref["pl_x"][0] and st.planets.vy[0] == ref["pl_vy"][0]
     assert st.planets.mass[0] == ref["pl_mass"][0]
+    assert st.omega_frame == ref["OmegaFrame"]
 
 
 DUST_PAR = os.path.join(CFG, "dust_256x768.par")
@@ -184,3 +189,21 @@ def test_thermal_diffusion_parameters(tmp_path):
     os.makedirs(str(tmp_path / "i"))
     q = read_par(_oracle.write_par(src, str(tmp_path / "i"), RadiativeDiffusion="Implicit"))
     assert q.radiative_diffusion == 2 and q.entropy_diffusion == 0 and q.diffusivity == 1e-6 and q.unsupported == 0
+
+
+REF_IN = os.path.join(os.environ.get("FB_REFERENCE_DIR", os.path.join(os.path.dirname(REPO), "reference")), "in")
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_IN), reason="the reference's example parameter files are not here")
+def test_reference_example_parameter_files_are_accepted():
+    """Every example parameter file the reference ships (in/*.par: a
+    corotating disc with non-reflecting edges, its energy-equation variant,
+    the gas-only one, and the self-gravitating disc with AddNoise and
+    TempPresc) is accepted as it is: no feature it sets is refused."""
+    from dustyfargoadsg_b200 import _ffi, read_par
+    lib = _ffi.load()
+    pars = sorted(f for f in os.listdir(REF_IN) if f.endswith(".par"))
+    assert pars
+    for f in pars:
+        p = read_par(os.path.join(REF_IN, f))
+        assert p.unsupported == 0, (f, lib.fb_unsupported_name(C.byref(p)).decode())

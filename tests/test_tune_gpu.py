@@ -64,7 +64,7 @@ def test_azimuthal_variants_are_bit_identical(tmp_path, E, cfg):
     nsec = 256 if E == 4 else 192  # the register variant needs nsec / E threads, a multiple of 32
     par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, cfg), str(tmp_path), Nrad=64, Nsec=nsec)
     out = {}
-    variants = (1, 2, 3, 4, 5, 6, 7) if E >= 2 else (1, 2, 3)
+    variants = (1, 2, 3, 4, 5, 6, 7, 8) if E >= 2 else (1, 2, 3)
     for variant in variants:
         with Disc(read_par(par), noise=1e-3, seed=4) as d:
             d.set_tuning({"cell_block": 128, "azi_cells_per_thread": E, "azi_variant": variant})
@@ -88,13 +88,13 @@ def test_tile_variant_on_short_rings(tmp_path, E):
     par = _oracle.write_par(os.path.join(_oracle.CONFIG_DIR, "adiabatic_sg_512x1536.par"), str(tmp_path),
                             Nrad=48, Nsec=64)
     out = {}
-    for variant in (1, 6, 7):
+    for variant in (1, 6, 7, 8):
         with Disc(read_par(par), noise=1e-3, seed=5) as d:
             d.set_tuning({"cell_block": 128, "azi_cells_per_thread": E, "azi_variant": variant})
             assert d.tuning()["azi_variant"] == variant
             for _ in range(2):
                 d.step()
             out[variant] = d.download()
-    for v in (6, 7):
+    for v in (6, 7, 8):
         for k in FIELDS + ("energy",):
             np.testing.assert_array_equal(out[1][k], out[v][k], err_msg="%s variant %d" % (k, v))
