@@ -393,6 +393,7 @@ void fb_dropin_AlgoGas(Force *force, PolarGrid *Rho, PolarGrid *Vrad, PolarGrid 
   g_host_stale = 1;
   if (g_sync_always) sync_host();
   PhysicalTime = st.physical_time;
+  OmegaFrame = st.omega_frame;  /* follows the planet in a corotating frame */
   LostMass = st.lost_mass;
   MINDT = st.mindt;
   MAXDT = st.maxdt;

@@ -22,6 +22,7 @@ pytestmark = [pytest.mark.gpu,
     ("iso_128x384.par", dict(Nrad=64, Nsec=192, MHD="L", NbTurbModes=50, GammaTurb="1e-3", TurbRmin=0.6,
                              TurbRmax=2.0)),
     ("iso_128x384.par", dict(Nrad=64, Nsec=192, Frame="C", InnerBoundary="NONREFLECTING")),
+    ("iso_128x384.par", dict(Nrad=64, Nsec=192, Frame="C", ForcedCircular="No", MassTaper="5.0")),
     ("adiabatic_sg_512x1536.par", dict(Nrad=64, Nsec=192, AddNoise="Yes", TempPresc="Yes", BetaCooling="No",
                                        InnerBoundary="OPEN", EntropyDiffusion="Yes", Diffusivity="1e-4")),
 ])
@@ -41,6 +42,8 @@ def test_dropin_matches_reference(tmp_path, par_name, keys):
         for k in ("dens", "vrad", "vtheta", "energy"):
             assert _oracle.rel_err(a[k], b[k]) <= 1e-11, (s, k)
         assert abs(a["PhysicalTime"] - b["PhysicalTime"]) <= 1e-13 * b["PhysicalTime"]
+        # the frame's angular velocity the binding hands back (planet*.dat prints it)
+        assert abs(a["OmegaFrame"] - b["OmegaFrame"]) <= 1e-12 * max(abs(b["OmegaFrame"]), 1.0), s
         if "pc_r" in b:  # particles
             for k in ("pc_r", "pc_th", "pc_vr", "pc_vth", "pc_stokes"):
                 assert _oracle.rel_err(a[k], b[k]) <= 1e-10, (s, k)
