@@ -153,6 +153,13 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
   const bool cfl = (i >= 1);  // ConditionCFL's rings: One_or_active..Max_or_active-1
   if (i == 0 && tid == 0) planet_prelude(k, k.ctl);
   const double rmi = k.rmed[i], surf = k.surf[i], rs = k.indirect_smoothing;
+#if FB_FAST
+  // fast build: every cell of the ring lies rmed[i] from the star, so the
+  // smoothed 1/d^3 of the star's sums is the ring's (within a few ulp of
+  // the reference's per-cell value): one root and two divisions per ring
+  const double dist2_ring = rmi * rmi + rs * rs;
+  const double invd3_ring = 1.0 / dist2_ring / sqrt(dist2_ring);
+#endif
   // ring sums: vtheta; ComputeForce (Force.c:77-253) for the star (x = y = 0,
   // mass 0) with rsmoothing = INDIRECTTERMSMOOTHING (SourceEuler.c:482);
   // GasTotalMass (SideEuler.c:15) and the barycentre sums (SideEuler.c:42-89)
@@ -181,10 +188,14 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
     const double yc = rmi * k.sinaz[j];
     const double cellmass = surf * dens;
     const double dx = xc - 0.0, dy = yc - 0.0;
+#if FB_FAST
+    const double InvDist3 = invd3_ring;
+#else
     const double d2 = dx * dx + dy * dy;
     const double dist2 = d2 + rs * rs;
     const double distance = sqrt(dist2);
     const double InvDist3 = 1.0 / dist2 / distance;
+#endif
     v[1] += FB_G * cellmass * dx * InvDist3 * 1.0;
     v[2] += FB_G * cellmass * dy * InvDist3 * 1.0;
     v[3] += surf * dens;
@@ -227,17 +238,22 @@ __global__ void __launch_bounds__(CFL_BS, 4) k_cfl(KP k)
     // diffusion's per ring; explicit radiative diffusion's per cell (below),
     // which replaces it when both are on
     const double invdt6_ring = (k.energy && k.ent_diff) ? k.diffusivity * 4.0 / k.mindx2[i] : 1e-10;
-    double m = 1e30;
+    // the ring's limit is the smallest CFLSECURITY / sqrt(S) over its cells;
+    // a correctly rounded square root and quotient are monotone, so it is
+    // the limit of the largest S, to the last bit: one root and one division
+    // per ring.  A NaN sum is skipped as the reference's `dt < newdt` skips
+    // it; S >= invdt5^2 >= 1e-20 otherwise.
+    double smax = -1.0;
     for (int j = tid; j < ns; j += T) {  // each thread reads back its own cells
       double vres = k.fast_transport ? vtc[j] - vmoy : vtc[j];
       double invdt3 = fb_quot(fabs(vres), dxtheta, rdxtheta);
       double invdt6 = invdt6_ring;
       if (k.energy && k.rad_diff == 1) invdt6 = k.td_rad[base + j];  // k_td_cfl, just before this kernel
-      double dt = FB_CFLSECURITY / sqrt(s12[j] + invdt3 * invdt3 + s4[j] + invdt5 * invdt5 + invdt6 * invdt6);
-      if (dt < m) m = dt;
+      const double S = s12[j] + invdt3 * invdt3 + s4[j] + invdt5 * invdt5 + invdt6 * invdt6;
+      if (S > smax) smax = S;
     }
-    m = block_min_dyn(m, sh);
-    if (tid == 0) k.ringmin[i] = m;
+    smax = -block_min_dyn(-smax, sh);
+    if (tid == 0) k.ringmin[i] = (smax > 0.0) ? FB_CFLSECURITY / sqrt(smax) : 1e30;
   }
   // the last CTA to finish runs the controller (no waiting: whoever comes
   // last sees every other ring's results)
