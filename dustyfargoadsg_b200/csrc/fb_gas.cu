@@ -679,7 +679,7 @@ __global__ void __launch_bounds__(FB_BS2) k_potential(KP k)
       P += pot;
     }
     {
-      const double InvDistance = 1.0 / k.rmed[i];
+      const double InvDistance = k.invrmed[i];  // 1.0 / Rmed[i], correctly rounded on the host
       double pot = -FB_G * 1.0 * InvDistance;
       if (use_ind) {
         pot -= c->ind_x * x + c->ind_y * y;
